@@ -1,0 +1,362 @@
+"""Benchmark of the ct2 gravity step on B200: particles/s per kick+drift.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one kick+drift at rung 0 through the reference-facing kick_step
+entry point (bin -> P2M -> FFT -> Green's multiply -> IFFT -> L2P + direct sum
+-> kick -> drift), on seeded synthetic particles resident in HBM.  Default
+workload: 128^3 = 2,097,152 particles, 70% in 512 Plummer spheres (a = 0.005,
+log-uniform masses over 10x) plus 30% uniform, 256^3 mesh, Plummer softening
+eps = 1/(50*128), dt = 1e-3.
+
+`value` is whole-job particles/s (device time, CUDA events, max over ranks);
+`e2e` is the same metric through the public API with the particle state copied
+host->device before and device->host after every step.  `roofline` is for the
+kernel with the largest share of the step; `cpu_baseline` is the CPU oracle
+timed on a bounded sample.  Under torchrun (N>1) every rank runs an
+independent box (replicas; the step has no exchange), value = all particles /
+max rank time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particles/s per kick+drift at 128^3 (rms force err <=1e-4 vs FP64 direct sum)"
+UNIT = "particles/s"
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return dict(hbm=float(d["hbm_gbs"]), sm_max_mhz=float(d.get("sm_max_mhz", 1965.0)),
+                    source="measured")
+    return dict(hbm=6650.0, sm_max_mhz=1965.0, source="fallback")
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", "clocks_rank%d.csv" % device)
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device),
+                                          "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                c = [s.strip() for s in line.split(",")]
+                if len(c) >= 9:
+                    rows.append(c)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k] == "Active"})
+        loaded = [s for s in sm if s > 0.5 * (max(sm) if sm else 1)]
+        return {"sm_mhz": statistics.median(loaded) if loaded else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def workload(args, rank):
+    from ct2_b200 import ics
+    n = args.ngrid ** 3
+    P = ics.plummer_spheres(n, seed=args.seed + rank, nspheres=args.nspheres, a=args.a)
+    return P, n
+
+
+def cpu_baseline(args):
+    """CPU oracle (C + numpy, all host threads) on a bounded sample of the
+    workload: the same generator scaled to 1/64 of the particles and mesh
+    cells (same particles per cell and sphere size in cells)."""
+    from ct2_b200 import ics
+    from oracle import oracle as O
+    ng = args.ngrid // 4
+    mesh = args.mesh // 4
+    mbits = int(np.log2(mesh))
+    nsph = max(1, args.nspheres // 64)
+    P = ics.plummer_spheres(ng ** 3, seed=args.seed, nspheres=nsph, a=args.a * 4)
+    n = ng ** 3
+    soft = 1.0 / (50 * args.ngrid) * 4
+    Gk = O.greens_k(mbits, args.order, 0, soft, args.bwidth)  # cached per mesh, not timed
+    times = []
+    for _ in range(2):
+        t = time.perf_counter()
+        r = O.method_forces(P["x"], P["y"], P["z"], mbits, args.order, 0, soft, args.bwidth,
+                            1.0 / n, Gk=Gk)
+        f = (r["ffar"] + r["fnear"]).astype(np.float32)
+        perm = r["perm"]
+        vx, vy, vz, rung, mr = O.kick_update(P["vx"][perm], P["vy"][perm], P["vz"][perm],
+                                             P["rung"][perm], f[:, 0], f[:, 1], f[:, 2],
+                                             ascending=1, descending=1, top=1, first=0, prung=0,
+                                             t0=args.dt, eta=0.15, max_dt=0.01, scale=1.0,
+                                             hsoft=soft)
+        O.drift(r["xs"], r["ys"], r["zs"], vx, vy, vz, args.dt, 1.0)
+        times.append(time.perf_counter() - t)
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count()))
+    return {"value": n / min(times), "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": "CPU oracle, one full kick+drift on the workload generator scaled to "
+                      "%d^3 particles, %d spheres, %d^3 mesh, order %d, bwidth %g (1/64 of the "
+                      "particles and cells); Green's table excluded (cached per mesh)"
+                      % (ng, nsph, mesh, args.order, args.bwidth)}
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference path's CPU restatement (the reference
+    itself does not build: HPX/sfmm absent, 3D FFT drivers empty), all host
+    threads, a bounded sample per step."""
+    if rank != 0:
+        return
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
+    for _ in range(args.warmup):
+        cpu_baseline(args)
+    vals = []
+    for _ in range(args.steps):
+        vals.append(cpu_baseline(args))
+    v = min(x["value"] for x in vals)
+    cb = dict(vals[0])
+    cb["value"] = v
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": _config(args, world), "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def _config(args, world):
+    return {"workload": "plummer_spheres_128cubed_mesh256" if args.ngrid == 128 else
+            "plummer_spheres_%dcubed_mesh%d" % (args.ngrid, args.mesh),
+            "particles_per_gpu": args.ngrid ** 3, "mesh": args.mesh, "order": args.order,
+            "bwidth": args.bwidth, "softening": "plummer eps=1/(50*%d)" % args.ngrid,
+            "dt": args.dt, "parallelism": "replicas" if world > 1 else "single",
+            "l2": "inputs larger than L2 (particle store + mesh grids >> 126 MB)"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ngrid", type=int, default=128)
+    ap.add_argument("--mesh", type=int, default=256)
+    ap.add_argument("--order", type=int, default=5)
+    ap.add_argument("--bwidth", type=float, default=3.0)
+    ap.add_argument("--nspheres", type=int, default=512)
+    ap.add_argument("--a", type=float, default=0.005)
+    ap.add_argument("--dt", type=float, default=1e-3)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--accuracy-sinks", type=int, default=4096)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+
+    from ct2_b200.gravity import Gravity
+    from ct2_b200 import _lib
+
+    P, n = workload(args, rank)
+    soft = 1.0 / (50 * args.ngrid)
+    g = Gravity(mesh=args.mesh, order=args.order, bwidth=args.bwidth, hsoft=soft,
+                GM=1.0 / n, device=local, max_particles=n)
+    g.upload_dict(P)
+    stream = torch.cuda.ExternalStream(g.stream(), device=local)
+
+    def step():
+        return g.kick_step(0, 0, 1.0, 1.0, 1.0, args.dt, 0)
+
+    # accuracy on the initial state: forces vs the FP64 Ewald direct sum
+    g.particle_to_grid()
+    g.compute_forces()
+    f, _ = g.forces()
+    d = g.download()
+    rng = np.random.Generator(np.random.PCG64(123))
+    sel = np.sort(rng.choice(n, size=min(args.accuracy_sinks, n), replace=False))
+    truth = g.ewald_direct(d["x"][sel], d["y"][sel], d["z"][sel])
+    diff = np.linalg.norm(f[sel] - truth, axis=1)
+    tn = np.linalg.norm(truth, axis=1)
+    acc = {"rms_rel": float(np.sqrt(np.mean((diff / tn) ** 2))),
+           "max_rel": float((diff / tn).max()),
+           "rms_norm": float(np.sqrt(np.mean(diff ** 2) / np.mean(tn ** 2))),
+           "sinks": int(len(sel))}
+    g.upload_dict(P)
+
+    for _ in range(args.warmup):
+        step()
+    g.synchronize()
+    stage_sum = np.zeros(7)
+    l0 = g.launch_count()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    inter = 0
+    for _ in range(args.steps):
+        step()
+        stage_sum += g.stage_times()
+        inter += g.interaction_count()
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    ck = clocks.stop()
+    launches = g.launch_count() - l0
+    ms = e0.elapsed_time(e1) / args.steps
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    value = n * world / (ms * 1e-3)
+
+    # end to end through the public API: host state in, step, host state out
+    e2e = None
+    if not args.no_e2e:
+        def pinned(a):
+            v = np.ascontiguousarray(a)
+            view = v.view(np.int32) if v.dtype == np.uint32 else v
+            return torch.from_numpy(view).pin_memory().numpy().view(v.dtype)
+        pin = {k: pinned(P[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "rung")}
+        outb = {k: torch.empty(n, dtype={"x": torch.int32, "y": torch.int32, "z": torch.int32,
+                                         "vx": torch.float32, "vy": torch.float32,
+                                         "vz": torch.float32, "rung": torch.int8}[k]).pin_memory()
+                for k in pin}
+        outn = {k: v.numpy() for k, v in outb.items()}
+        for k in ("x", "y", "z"):
+            outn[k] = outn[k].view(np.uint32)
+        import ctypes
+        lib = _lib.load()
+
+        def e2e_step():
+            g.upload(pin["x"], pin["y"], pin["z"], pin["vx"], pin["vy"], pin["vz"], pin["rung"])
+            step()
+            vp = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+            rc = lib.ct2g_download_particles(g.handle, vp(outn["x"]), vp(outn["y"]), vp(outn["z"]),
+                                             vp(outn["vx"]), vp(outn["vy"]), vp(outn["vz"]),
+                                             vp(outn["rung"]), None)
+            assert rc == 0
+        for _ in range(2):
+            e2e_step()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            e2e_step()
+        e1.record(stream)
+        e1.synchronize()
+        ems = e0.elapsed_time(e1) / args.steps
+        if dist:
+            t = torch.tensor([ems], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        e2e = {"value": n * world / (ems * 1e-3), "unit": UNIT,
+               "h2d_bytes_per_step": int(n * 25), "d2h_bytes_per_step": int(n * 25)}
+
+    # roofline of the dominant stage
+    st = stage_sum / args.steps
+    names = ["bin", "p2m", "fft_fwd", "mg2l", "fft_inv", "forces", "update_drift"]
+    peaks = _peaks()
+    M, nc = args.mesh, (args.order + 1) * (args.order + 2) * (args.order + 3) // 6
+    CK = M * M * (M // 2 + 1)
+    algo_bytes = {"bin": 66.0 * n, "p2m": 12.0 * n + 4.0 * nc * M ** 3,
+                  "fft_fwd": nc * (4.0 * M ** 3 + 8.0 * CK), "mg2l": 20.0 * nc * CK,
+                  "fft_inv": nc * (4.0 * M ** 3 + 8.0 * CK), "update_drift": 61.0 * n}
+    k = int(np.argmax(st))
+    dom = names[k]
+    if dom == "forces":
+        flops = 20.0 * inter / args.steps
+        sms = torch.cuda.get_device_properties(local).multi_processor_count
+        peak = sms * 128 * 2 * peaks["sm_max_mhz"] * 1e6 / 1e12
+        ach = flops / (st[k] * 1e-3) / 1e12
+        roof = {"kernel": "forces (direct sum)", "bound": "fp32", "achieved": ach, "peak": peak,
+                "unit": "TFLOP/s", "frac": ach / peak, "traffic": None,
+                "peak_source": "derived: SMs x 128 x 2 x max SM clock (no measured FP32 peak)"}
+    else:
+        ach = algo_bytes[dom] / (st[k] * 1e-3) / 1e9
+        roof = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": peaks["hbm"],
+                "unit": "GB/s", "frac": ach / peaks["hbm"], "traffic": None,
+                "peak_source": peaks["source"]}
+    stages = {nm: float(t) for nm, t in zip(names, st)}
+
+    cb = None
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            cb = cpu_baseline(args)
+        except Exception as ex:  # reported, not fatal
+            cb = {"value": None, "error": repr(ex)}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic: seeded Plummer spheres + uniform background",
+                "config": _config(args, world), "e2e": e2e, "gpu_launches": int(launches),
+                "roofline": roof, "cpu_baseline": cb, "clocks": ck, "accuracy": acc,
+                "stage_ms": stages, "interactions_per_step": inter / args.steps}
+        print(json.dumps(line), flush=True)
+    g.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

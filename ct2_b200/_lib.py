@@ -1,0 +1,111 @@
+"""ctypes binding of libct2g.so (the C ABI declared in include/ct2g.h).
+
+The library is the only compute path: if it is missing or cannot load, every
+call raises -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libct2g.so")
+
+CT2G_OK = 0
+SOFT_PLUMMER = 0
+SOFT_SPHERE = 1
+MAX_ORDER = 6
+
+
+class Options(ctypes.Structure):
+    _fields_ = [("bwidth", ctypes.c_float), ("hsoft", ctypes.c_float), ("eta", ctypes.c_float),
+                ("GM", ctypes.c_float), ("mesh", ctypes.c_int), ("order", ctypes.c_int),
+                ("kernel", ctypes.c_int), ("device", ctypes.c_int),
+                ("max_particles", ctypes.c_size_t)]
+
+
+class KickParams(ctypes.Structure):
+    _fields_ = [("ascending", ctypes.c_int), ("descending", ctypes.c_int), ("top", ctypes.c_int),
+                ("first", ctypes.c_int), ("rung", ctypes.c_int), ("t0", ctypes.c_float),
+                ("eta", ctypes.c_float), ("max_dt", ctypes.c_float), ("scale", ctypes.c_float)]
+
+
+# (name, restype, argtypes) for every symbol of include/ct2g.h
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_SZ = ctypes.c_size_t
+_F = ctypes.c_float
+_D = ctypes.c_double
+SYMBOLS = [
+    ("ct2g_default_options", None, [_P]),
+    ("ct2g_create", _I, [_P, _P]),
+    ("ct2g_destroy", _I, [_P]),
+    ("ct2g_last_error", ctypes.c_char_p, [_P]),
+    ("ct2g_status_string", ctypes.c_char_p, [_I]),
+    ("ct2g_get_options", _I, [_P, _P]),
+    ("ct2g_set_params", _I, [_P, _F, _F, _F]),
+    ("ct2g_upload_particles", _I, [_P, _P, _P, _P, _P, _P, _P, _P, _SZ]),
+    ("ct2g_download_particles", _I, [_P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    ("ct2g_particle_count", _SZ, [_P]),
+    ("ct2g_particle_to_grid", _I, [_P]),
+    ("ct2g_download_cells", _I, [_P, _P, _P]),
+    ("ct2g_compute_multipoles", _I, [_P]),
+    ("ct2g_download_multipoles", _I, [_P, _P]),
+    ("ct2g_compute_expansions", _I, [_P]),
+    ("ct2g_download_expansions", _I, [_P, _P]),
+    ("ct2g_download_greens", _I, [_P, _P]),
+    ("ct2g_compute_forces", _I, [_P]),
+    ("ct2g_download_forces", _I, [_P, _P, _P, _P, _P]),
+    ("ct2g_upload_forces", _I, [_P, _P, _P, _P]),
+    ("ct2g_kick_update", _I, [_P, _P, _P]),
+    ("ct2g_kick", _I, [_P, _P, _P]),
+    ("ct2g_drift", _I, [_P, _F, _F]),
+    ("ct2g_kick_step", _I, [_P, _P, _I, _D, _D, _D, _D, _I, _I, _P]),
+    ("ct2g_sort_by_rung", _I, [_P, _I]),
+    ("ct2g_push_rungs", _I, [_P]),
+    ("ct2g_pop_rungs", _I, [_P]),
+    ("ct2g_set_minrung", _I, [_P, _I]),
+    ("ct2g_current_range", _I, [_P, _P, _P]),
+    ("ct2g_rung_counts", _I, [_P, _P, _I, _P]),
+    ("ct2g_fft_r2c_3d", _I, [_P, _P, _P, _I, _I]),
+    ("ct2g_fft_c2r_3d", _I, [_P, _P, _P, _I, _I]),
+    ("ct2g_fft3d_f32_dev", _I, [_P, _I, _P, _P, _I, _I]),
+    ("ct2g_ewald_direct", _I, [_P, _P, _P, _P, _SZ, _D, _D, _I, _P, _P]),
+    ("ct2g_stream", _P, [_P]),
+    ("ct2g_synchronize", _I, [_P]),
+    ("ct2g_stage_times", _I, [_P, _P, _I]),
+    ("ct2g_launch_count", ctypes.c_uint64, [_P]),
+    ("ct2g_interaction_count", ctypes.c_uint64, [_P]),
+]
+
+_lib = None
+
+
+def load():
+    """Load libct2g.so, raising if it is missing (no fallback exists)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError("libct2g.so is not built (run python -m ct2_b200.build); "
+                           "the gravity step has no CPU fallback")
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, res, args in SYMBOLS:
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+class CT2GError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__("ct2g status %d (%s): %s" % (status, _status_str(status), msg))
+        self.status = status
+
+
+def _status_str(s):
+    try:
+        return load().ct2g_status_string(s).decode()
+    except Exception:  # pragma: no cover
+        return "?"

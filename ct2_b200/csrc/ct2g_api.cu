@@ -1,0 +1,771 @@
+// C ABI: context lifetime, particle store, stage entry points, the
+// rung-hierarchical kick_step driver (src/main.cpp:8-92) and rung bookkeeping
+// (src/particle.cpp:31-57,320-347).
+#include <cstdio>
+#include <cstring>
+
+#include "ct2g_internal.cuh"
+
+int ct2g_upload_stencil(ct2g_ctx *ctx, const std::vector<int> &st4);
+
+int ct2g_fail(ct2g_ctx *ctx, int code, const std::string &msg) {
+  if (ctx) ctx->err = msg;
+  return code;
+}
+
+int ct2g_cuda_fail(ct2g_ctx *ctx, cudaError_t e, const char *what) {
+  std::string m = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+  if (ctx) ctx->err = m;
+  return e == cudaErrorMemoryAllocation ? CT2G_ENOMEM : CT2G_ECUDA;
+}
+
+namespace {
+
+// stable partition of [b, e) by rung < minrung (front) / >= minrung (back)
+__global__ void rung_flag_kernel(const int8_t *__restrict__ rung, size_t b, size_t nr,
+                                 int minrung, uint32_t *__restrict__ flags) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nr) flags[i] = rung[b + i] < minrung ? 1u : 0u;
+}
+
+__global__ void rung_scatter_kernel(const uint32_t *__restrict__ flags,
+                                    const uint32_t *__restrict__ fscan, size_t b, size_t nr,
+                                    uint32_t nlow, uint32_t *__restrict__ perm) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nr) return;
+  uint32_t dst = flags[i] ? fscan[i] : nlow + ((uint32_t)i - fscan[i]);
+  perm[dst] = (uint32_t)i;
+}
+
+template <typename T>
+__global__ void permute_kernel(const uint32_t *__restrict__ perm, size_t b, size_t nr,
+                               const T *__restrict__ in, T *__restrict__ out) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nr) out[b + i] = in[b + perm[i]];
+}
+
+__global__ void rung_count_kernel(const int8_t *__restrict__ rung, size_t n,
+                                  unsigned long long *__restrict__ counts) {
+  __shared__ unsigned int c[128];
+  if (threadIdx.x < 128) c[threadIdx.x] = 0;
+  __syncthreads();
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    int r = rung[i];
+    atomicAdd(&c[r & 127], 1u);
+  }
+  __syncthreads();
+  if (threadIdx.x < 128 && c[threadIdx.x]) atomicAdd(&counts[threadIdx.x], (unsigned long long)c[threadIdx.x]);
+}
+
+__global__ void set_minrung_kernel(int8_t *__restrict__ rung, size_t n, int minrung) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && rung[i] < minrung) rung[i] = (int8_t)minrung;
+}
+
+__global__ void iota_kernel(uint32_t *__restrict__ id, size_t n) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) id[i] = (uint32_t)i;
+}
+
+bool is_pow2(int v) { return v > 0 && (v & (v - 1)) == 0; }
+
+void free_particles(ct2g_ctx *ctx) {
+  void *ptrs[] = {ctx->x, ctx->y, ctx->z, ctx->id, ctx->vx, ctx->vy, ctx->vz, ctx->rung,
+                  ctx->x2, ctx->y2, ctx->z2, ctx->id2, ctx->vx2, ctx->vy2, ctx->vz2, ctx->rung2,
+                  ctx->keys, ctx->keys2, ctx->vals, ctx->vals2, ctx->hist, ctx->src,
+                  ctx->chunk_begin, ctx->flags, ctx->fx, ctx->fy, ctx->fz, ctx->pot};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  ctx->x = ctx->y = ctx->z = ctx->id = nullptr;
+  ctx->vx = ctx->vy = ctx->vz = nullptr;
+  ctx->rung = nullptr;
+  ctx->x2 = ctx->y2 = ctx->z2 = ctx->id2 = nullptr;
+  ctx->vx2 = ctx->vy2 = ctx->vz2 = nullptr;
+  ctx->rung2 = nullptr;
+  ctx->keys = ctx->keys2 = ctx->vals = ctx->vals2 = ctx->hist = nullptr;
+  ctx->src = nullptr;
+  ctx->chunk_begin = ctx->flags = nullptr;
+  ctx->fx = ctx->fy = ctx->fz = ctx->pot = nullptr;
+  ctx->cap = 0;
+}
+
+int check(ct2g_ctx *ctx) {
+  if (!ctx) return CT2G_EINVAL;
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return ct2g_cuda_fail(ctx, e, "cudaSetDevice");
+  return CT2G_OK;
+}
+
+int ensure_grid(ct2g_ctx *ctx) {
+  if (!ctx->has_particles) return ct2g_fail(ctx, CT2G_ESTATE, "no particles uploaded");
+  if (!ctx->grid_valid) return ct2g_fail(ctx, CT2G_ESTATE, "particle_to_grid has not run since the particles moved");
+  return CT2G_OK;
+}
+
+int ensure_expansions(ct2g_ctx *ctx) {
+  CT2G_TRY(ensure_grid(ctx));
+  if (!ctx->moments_valid && !ctx->expansions_valid) {
+    cudaEventRecord(ctx->ev[1], ctx->stream);
+    CT2G_TRY(ct2g_p2m(ctx));
+    ctx->moments_valid = true;
+  } else {
+    cudaEventRecord(ctx->ev[1], ctx->stream);
+  }
+  if (!ctx->expansions_valid) {
+    CT2G_TRY(ct2g_mesh_solve(ctx));
+    ctx->moments_valid = false;  // grid now holds expansions
+    ctx->expansions_valid = true;
+  } else {
+    for (int k = 2; k <= 5; k++) cudaEventRecord(ctx->ev[k], ctx->stream);
+  }
+  return CT2G_OK;
+}
+
+}  // namespace
+
+int ct2g_alloc_particles(ct2g_ctx *ctx, size_t n) {
+  if (n <= ctx->cap) return CT2G_OK;
+  free_particles(ctx);
+  const size_t cap = n;
+  const size_t ntiles = (cap + 4095) / 4096;
+#define A(ptr, bytes) CT2G_CUDA(ctx, cudaMalloc(&(ptr), (bytes)))
+  A(ctx->x, cap * 4);
+  A(ctx->y, cap * 4);
+  A(ctx->z, cap * 4);
+  A(ctx->id, cap * 4);
+  A(ctx->vx, cap * 4);
+  A(ctx->vy, cap * 4);
+  A(ctx->vz, cap * 4);
+  A(ctx->rung, cap);
+  A(ctx->x2, cap * 4);
+  A(ctx->y2, cap * 4);
+  A(ctx->z2, cap * 4);
+  A(ctx->id2, cap * 4);
+  A(ctx->vx2, cap * 4);
+  A(ctx->vy2, cap * 4);
+  A(ctx->vz2, cap * 4);
+  A(ctx->rung2, cap);
+  A(ctx->keys, cap * 4);
+  A(ctx->keys2, cap * 4);
+  A(ctx->vals, cap * 4);
+  A(ctx->vals2, cap * 4);
+  A(ctx->hist, ntiles * 256 * 4);
+  A(ctx->src, cap * sizeof(float4));
+  A(ctx->chunk_begin, cap * 4);
+  A(ctx->flags, cap * 4);
+  A(ctx->fx, cap * 4);
+  A(ctx->fy, cap * 4);
+  A(ctx->fz, cap * 4);
+  A(ctx->pot, cap * 4);
+#undef A
+  ctx->cap = cap;
+  return CT2G_OK;
+}
+
+int ct2g_alloc_mesh(ct2g_ctx *ctx) {
+  CT2G_CUDA(ctx, cudaMalloc(&ctx->cell_start, sizeof(uint32_t) * (ctx->C + 1)));
+  CT2G_CUDA(ctx, cudaMalloc(&ctx->grid, sizeof(float) * ctx->nc * ctx->C));
+  CT2G_CUDA(ctx, cudaMalloc(&ctx->spec, sizeof(float2) * ctx->nc * ctx->CK));
+  CT2G_CUDA(ctx, cudaMalloc(&ctx->greens, sizeof(float) * ctx->nc * ctx->CK));
+  return CT2G_OK;
+}
+
+extern "C" {
+
+void ct2g_default_options(ct2g_options *o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->bwidth = 3.0f;
+  o->hsoft = 1.0f / 50.0f;
+  o->eta = 0.15f;
+  o->GM = 0.0f;
+  o->mesh = 64;
+  o->order = 4;
+  o->kernel = CT2G_SOFT_PLUMMER;
+  o->device = 0;
+  o->max_particles = 0;
+}
+
+const char *ct2g_status_string(int s) {
+  switch (s) {
+    case CT2G_OK: return "ok";
+    case CT2G_EINVAL: return "invalid argument";
+    case CT2G_ENOMEM: return "out of device memory";
+    case CT2G_ECUDA: return "CUDA error";
+    case CT2G_ESTATE: return "call out of order";
+    case CT2G_ETIMEOUT: return "device wait timed out";
+    case CT2G_ENODEV: return "no usable sm_100 device";
+  }
+  return "unknown status";
+}
+
+const char *ct2g_last_error(const ct2g_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int ct2g_create(const ct2g_options *opt, ct2g_ctx **out) {
+  if (!opt || !out) return CT2G_EINVAL;
+  *out = nullptr;
+  if (!is_pow2(opt->mesh) || opt->mesh < 8 || opt->mesh > 512) return CT2G_EINVAL;
+  if (opt->order < 1 || opt->order > CT2G_MAX_ORDER) return CT2G_EINVAL;
+  if (!(opt->bwidth >= 0.f) || 2.0f * opt->bwidth + 1.0f > (float)opt->mesh || opt->bwidth > 4.0f)
+    return CT2G_EINVAL;
+  if (!(opt->hsoft > 0.f)) return CT2G_EINVAL;
+  if (opt->kernel != CT2G_SOFT_PLUMMER && opt->kernel != CT2G_SOFT_SPHERE) return CT2G_EINVAL;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= opt->device || opt->device < 0) {
+    cudaGetLastError();
+    return CT2G_ENODEV;
+  }
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, opt->device) != cudaSuccess || prop.major < 10) return CT2G_ENODEV;
+  ct2g_ctx *ctx = new ct2g_ctx();
+  ctx->opt = *opt;
+  ctx->device = opt->device;
+  ctx->num_sms = prop.multiProcessorCount;
+  ctx->M = opt->mesh;
+  while ((1 << ctx->mbits) < ctx->M) ctx->mbits++;
+  ctx->C = (int64_t)ctx->M * ctx->M * ctx->M;
+  ctx->CK = (int64_t)ctx->M * ctx->M * (ctx->M / 2 + 1);
+  ctx->p = opt->order;
+  ctx->nc = ct2g_ncomp(ctx->p);
+  int rc = CT2G_OK;
+  do {
+    if (cudaSetDevice(ctx->device) != cudaSuccess) { rc = CT2G_ENODEV; break; }
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) { rc = CT2G_ECUDA; break; }
+    for (auto &e : ctx->ev)
+      if (cudaEventCreate(&e) != cudaSuccess) { rc = CT2G_ECUDA; break; }
+    if (rc) break;
+    if (cudaMallocHost(&ctx->h_pinned, 64) != cudaSuccess) { rc = CT2G_ECUDA; break; }
+    if (cudaMalloc(&ctx->d_maxrung, sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&ctx->d_inter, sizeof(unsigned long long)) != cudaSuccess) { rc = CT2G_ENOMEM; break; }
+    if ((rc = ct2g_alloc_mesh(ctx)) != CT2G_OK) break;
+    // near-field stencil: integer offsets |o|^2 <= bwidth^2 (the fixed form
+    // of particle_cell_neighbors, src/particle.cpp:302-318)
+    std::vector<int> st;
+    const int B = (int)std::floor(opt->bwidth);
+    const double bw2 = (double)opt->bwidth * (double)opt->bwidth;
+    for (int i = -B; i <= B; i++)
+      for (int j = -B; j <= B; j++)
+        for (int k = -B; k <= B; k++)
+          if ((double)(i * i + j * j + k * k) <= bw2) {
+            st.push_back(i);
+            st.push_back(j);
+            st.push_back(k);
+            st.push_back(0);
+          }
+    ctx->nstencil = (int)(st.size() / 4);
+    if ((rc = ct2g_upload_stencil(ctx, st)) != CT2G_OK) break;
+    if (opt->max_particles && (rc = ct2g_alloc_particles(ctx, opt->max_particles)) != CT2G_OK) break;
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) { rc = CT2G_ECUDA; break; }
+  } while (0);
+  if (rc != CT2G_OK) {
+    cudaGetLastError();
+    ct2g_destroy(ctx);
+    return rc;
+  }
+  *out = ctx;
+  return CT2G_OK;
+}
+
+int ct2g_destroy(ct2g_ctx *ctx) {
+  if (!ctx) return CT2G_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  free_particles(ctx);
+  void *ptrs[] = {ctx->cell_start, ctx->grid, ctx->spec, ctx->greens, ctx->tw32, ctx->tw64,
+                  ctx->d_maxrung, ctx->d_inter, ctx->scan_tmp};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
+  for (auto &e : ctx->ev)
+    if (e) cudaEventDestroy(e);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return CT2G_OK;
+}
+
+int ct2g_get_options(const ct2g_ctx *ctx, ct2g_options *out) {
+  if (!ctx || !out) return CT2G_EINVAL;
+  *out = ctx->opt;
+  return CT2G_OK;
+}
+
+int ct2g_set_params(ct2g_ctx *ctx, float hsoft, float eta, float GM) {
+  if (!ctx) return CT2G_EINVAL;
+  if (!(hsoft > 0.f) || !(eta > 0.f)) return ct2g_fail(ctx, CT2G_EINVAL, "hsoft and eta must be > 0");
+  if (hsoft != ctx->opt.hsoft) {
+    ctx->greens_valid = false;  // the far-field kernel depends on the softening
+    ctx->expansions_valid = false;
+  }
+  ctx->opt.hsoft = hsoft;
+  ctx->opt.eta = eta;
+  if (GM > 0.f) ctx->opt.GM = GM;
+  ctx->forces_valid = false;
+  return CT2G_OK;
+}
+
+int ct2g_upload_particles(ct2g_ctx *ctx, const uint32_t *x, const uint32_t *y, const uint32_t *z,
+                          const float *vx, const float *vy, const float *vz, const int8_t *rung,
+                          size_t n) {
+  CT2G_TRY(check(ctx));
+  if (!x || !y || !z || !vx || !vy || !vz) return ct2g_fail(ctx, CT2G_EINVAL, "null particle array");
+  if (n >= 0x7fffffffu) return ct2g_fail(ctx, CT2G_EINVAL, "too many particles");
+  CT2G_TRY(ct2g_alloc_particles(ctx, std::max<size_t>(n, 1)));
+  cudaStream_t st = ctx->stream;
+  CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->x, x, n * 4, cudaMemcpyHostToDevice, st));
+  CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->y, y, n * 4, cudaMemcpyHostToDevice, st));
+  CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->z, z, n * 4, cudaMemcpyHostToDevice, st));
+  CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->vx, vx, n * 4, cudaMemcpyHostToDevice, st));
+  CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->vy, vy, n * 4, cudaMemcpyHostToDevice, st));
+  CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->vz, vz, n * 4, cudaMemcpyHostToDevice, st));
+  if (rung)
+    CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->rung, rung, n, cudaMemcpyHostToDevice, st));
+  else
+    CT2G_CUDA(ctx, cudaMemsetAsync(ctx->rung, 0, n, st));
+  if (n) {
+    iota_kernel<<<ct2g_div_up(n, 256), 256, 0, st>>>(ctx->id, n);
+    CT2G_LAUNCHED(ctx);
+  }
+  CT2G_CUDA(ctx, cudaStreamSynchronize(st));
+  ctx->n = n;
+  if (!(ctx->opt.GM > 0.f)) ctx->opt.GM = n ? 1.0f / (float)n : 0.f;
+  ctx->rung_begin = 0;
+  ctx->rung_stack.clear();
+  ctx->has_particles = true;
+  ctx->grid_valid = ctx->moments_valid = ctx->expansions_valid = ctx->forces_valid = false;
+  return CT2G_OK;
+}
+
+int ct2g_download_particles(ct2g_ctx *ctx, uint32_t *x, uint32_t *y, uint32_t *z, float *vx,
+                            float *vy, float *vz, int8_t *rung, uint32_t *ids) {
+  CT2G_TRY(check(ctx));
+  const size_t n = ctx->n;
+  cudaStream_t st = ctx->stream;
+  if (x) CT2G_CUDA(ctx, cudaMemcpyAsync(x, ctx->x, n * 4, cudaMemcpyDeviceToHost, st));
+  if (y) CT2G_CUDA(ctx, cudaMemcpyAsync(y, ctx->y, n * 4, cudaMemcpyDeviceToHost, st));
+  if (z) CT2G_CUDA(ctx, cudaMemcpyAsync(z, ctx->z, n * 4, cudaMemcpyDeviceToHost, st));
+  if (vx) CT2G_CUDA(ctx, cudaMemcpyAsync(vx, ctx->vx, n * 4, cudaMemcpyDeviceToHost, st));
+  if (vy) CT2G_CUDA(ctx, cudaMemcpyAsync(vy, ctx->vy, n * 4, cudaMemcpyDeviceToHost, st));
+  if (vz) CT2G_CUDA(ctx, cudaMemcpyAsync(vz, ctx->vz, n * 4, cudaMemcpyDeviceToHost, st));
+  if (rung) CT2G_CUDA(ctx, cudaMemcpyAsync(rung, ctx->rung, n, cudaMemcpyDeviceToHost, st));
+  if (ids) CT2G_CUDA(ctx, cudaMemcpyAsync(ids, ctx->id, n * 4, cudaMemcpyDeviceToHost, st));
+  CT2G_CUDA(ctx, cudaStreamSynchronize(st));
+  return CT2G_OK;
+}
+
+size_t ct2g_particle_count(const ct2g_ctx *ctx) { return ctx ? ctx->n : 0; }
+
+int ct2g_particle_to_grid(ct2g_ctx *ctx) {
+  CT2G_TRY(check(ctx));
+  if (!ctx->has_particles) return ct2g_fail(ctx, CT2G_ESTATE, "no particles uploaded");
+  cudaEventRecord(ctx->ev[0], ctx->stream);
+  return ct2g_bin_range(ctx);
+}
+
+int ct2g_download_cells(ct2g_ctx *ctx, int64_t *cell_begin, int64_t *cell_end) {
+  CT2G_TRY(check(ctx));
+  if (!cell_begin || !cell_end) return ct2g_fail(ctx, CT2G_EINVAL, "null output");
+  CT2G_TRY(ensure_grid(ctx));
+  std::vector<uint32_t> h(ctx->C + 1);
+  CT2G_CUDA(ctx, cudaMemcpyAsync(h.data(), ctx->cell_start, sizeof(uint32_t) * h.size(),
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+  CT2G_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  const uint32_t M = (uint32_t)ctx->M;
+  for (uint32_t i = 0; i < M; i++)
+    for (uint32_t j = 0; j < M; j++)
+      for (uint32_t k = 0; k < M; k++) {
+        const uint32_t key = ct2g_morton(i, j, k);
+        const size_t c = ((size_t)i * M + j) * M + k;
+        cell_begin[c] = h[key];
+        cell_end[c] = h[key + 1];
+      }
+  return CT2G_OK;
+}
+
+int ct2g_compute_multipoles(ct2g_ctx *ctx) {
+  CT2G_TRY(check(ctx));
+  CT2G_TRY(ensure_grid(ctx));
+  CT2G_TRY(ct2g_p2m(ctx));
+  ctx->moments_valid = true;
+  ctx->expansions_valid = false;
+  return CT2G_OK;
+}
+
+int ct2g_download_multipoles(ct2g_ctx *ctx, float *out) {
+  CT2G_TRY(check(ctx));
+  if (!out) return ct2g_fail(ctx, CT2G_EINVAL, "null output");
+  if (!ctx->moments_valid) return ct2g_fail(ctx, CT2G_ESTATE, "moments not computed (or already transformed)");
+  CT2G_CUDA(ctx, cudaMemcpyAsync(out, ctx->grid, sizeof(float) * ctx->nc * ctx->C,
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+  CT2G_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return CT2G_OK;
+}
+
+int ct2g_compute_expansions(ct2g_ctx *ctx) {
+  CT2G_TRY(check(ctx));
+  CT2G_TRY(ensure_grid(ctx));
+  if (!ctx->moments_valid) CT2G_TRY(ct2g_compute_multipoles(ctx));
+  CT2G_TRY(ct2g_mesh_solve(ctx));
+  ctx->moments_valid = false;
+  ctx->expansions_valid = true;
+  return CT2G_OK;
+}
+
+int ct2g_download_expansions(ct2g_ctx *ctx, float *out) {
+  CT2G_TRY(check(ctx));
+  if (!out) return ct2g_fail(ctx, CT2G_EINVAL, "null output");
+  if (!ctx->expansions_valid) return ct2g_fail(ctx, CT2G_ESTATE, "expansions not computed");
+  CT2G_CUDA(ctx, cudaMemcpyAsync(out, ctx->grid, sizeof(float) * ctx->nc * ctx->C,
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+  CT2G_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return CT2G_OK;
+}
+
+int ct2g_download_greens(ct2g_ctx *ctx, float *out) {
+  CT2G_TRY(check(ctx));
+  if (!out) return ct2g_fail(ctx, CT2G_EINVAL, "null output");
+  CT2G_TRY(ct2g_build_greens(ctx));
+  CT2G_CUDA(ctx, cudaMemcpyAsync(out, ctx->greens, sizeof(float) * ctx->nc * ctx->CK,
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+  CT2G_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return CT2G_OK;
+}
+
+int ct2g_compute_forces(ct2g_ctx *ctx) {
+  CT2G_TRY(check(ctx));
+  CT2G_TRY(ensure_expansions(ctx));
+  CT2G_TRY(ct2g_forces(ctx));
+  ctx->forces_valid = true;
+  return CT2G_OK;
+}
+
+int ct2g_download_forces(ct2g_ctx *ctx, float *fx, float *fy, float *fz, float *pot) {
+  CT2G_TRY(check(ctx));
+  const size_t n = ctx->n;
+  cudaStream_t st = ctx->stream;
+  if (fx) CT2G_CUDA(ctx, cudaMemcpyAsync(fx, ctx->fx, n * 4, cudaMemcpyDeviceToHost, st));
+  if (fy) CT2G_CUDA(ctx, cudaMemcpyAsync(fy, ctx->fy, n * 4, cudaMemcpyDeviceToHost, st));
+  if (fz) CT2G_CUDA(ctx, cudaMemcpyAsync(fz, ctx->fz, n * 4, cudaMemcpyDeviceToHost, st));
+  if (pot) CT2G_CUDA(ctx, cudaMemcpyAsync(pot, ctx->pot, n * 4, cudaMemcpyDeviceToHost, st));
+  CT2G_CUDA(ctx, cudaStreamSynchronize(st));
+  return CT2G_OK;
+}
+
+int ct2g_upload_forces(ct2g_ctx *ctx, const float *fx, const float *fy, const float *fz) {
+  CT2G_TRY(check(ctx));
+  if (!fx || !fy || !fz) return ct2g_fail(ctx, CT2G_EINVAL, "null force array");
+  const size_t n = ctx->n;
+  cudaStream_t st = ctx->stream;
+  CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->fx, fx, n * 4, cudaMemcpyHostToDevice, st));
+  CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->fy, fy, n * 4, cudaMemcpyHostToDevice, st));
+  CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->fz, fz, n * 4, cudaMemcpyHostToDevice, st));
+  CT2G_CUDA(ctx, cudaStreamSynchronize(st));
+  ctx->forces_valid = true;
+  return CT2G_OK;
+}
+
+int ct2g_kick_update(ct2g_ctx *ctx, const ct2g_kick_params *p, int *max_rung) {
+  CT2G_TRY(check(ctx));
+  if (!p) return ct2g_fail(ctx, CT2G_EINVAL, "null kick params");
+  if (p->rung < 0 || p->rung > 30) return ct2g_fail(ctx, CT2G_EINVAL, "rung out of range");
+  if (!ctx->forces_valid) return ct2g_fail(ctx, CT2G_ESTATE, "no forces to apply");
+  return ct2g_update(ctx, p, max_rung, false, 0.f, 1.f);
+}
+
+int ct2g_kick(ct2g_ctx *ctx, const ct2g_kick_params *p, int *max_rung) {
+  CT2G_TRY(check(ctx));
+  if (!p) return ct2g_fail(ctx, CT2G_EINVAL, "null kick params");
+  if (p->rung < 0 || p->rung > 30) return ct2g_fail(ctx, CT2G_EINVAL, "rung out of range");
+  CT2G_TRY(ensure_expansions(ctx));
+  CT2G_TRY(ct2g_forces(ctx));
+  cudaEventRecord(ctx->ev[6], ctx->stream);
+  ctx->forces_valid = true;
+  CT2G_TRY(ct2g_update(ctx, p, max_rung, false, 0.f, 1.f));
+  cudaEventRecord(ctx->ev[7], ctx->stream);
+  return CT2G_OK;
+}
+
+int ct2g_drift(ct2g_ctx *ctx, float dt, float scale) {
+  CT2G_TRY(check(ctx));
+  if (!(scale != 0.f)) return ct2g_fail(ctx, CT2G_EINVAL, "scale must be nonzero");
+  return ct2g_drift_all(ctx, dt, scale);
+}
+
+int ct2g_sort_by_rung(ct2g_ctx *ctx, int minrung) {
+  CT2G_TRY(check(ctx));
+  if (minrung == 0) {
+    ctx->rung_begin = 0;
+    return CT2G_OK;
+  }
+  const size_t b = ctx->rung_begin, nr = ctx->n - b;
+  if (nr == 0) return CT2G_OK;
+  CT2G_TRY(ct2g_alloc_particles(ctx, ctx->n));
+  cudaStream_t st = ctx->stream;
+  const unsigned T = 256, G = ct2g_div_up(nr, T);
+  rung_flag_kernel<<<G, T, 0, st>>>(ctx->rung, b, nr, minrung, ctx->flags);
+  CT2G_LAUNCHED(ctx);
+  uint32_t nlow = 0;
+  CT2G_TRY(ct2g_scan_exclusive(ctx, ctx->flags, ctx->vals2, nr, &nlow));
+  rung_scatter_kernel<<<G, T, 0, st>>>(ctx->flags, ctx->vals2, b, nr, nlow, ctx->vals);
+  CT2G_LAUNCHED(ctx);
+  permute_kernel<uint32_t><<<G, T, 0, st>>>(ctx->vals, b, nr, ctx->x, ctx->x2);
+  permute_kernel<uint32_t><<<G, T, 0, st>>>(ctx->vals, b, nr, ctx->y, ctx->y2);
+  permute_kernel<uint32_t><<<G, T, 0, st>>>(ctx->vals, b, nr, ctx->z, ctx->z2);
+  permute_kernel<uint32_t><<<G, T, 0, st>>>(ctx->vals, b, nr, ctx->id, ctx->id2);
+  permute_kernel<float><<<G, T, 0, st>>>(ctx->vals, b, nr, ctx->vx, ctx->vx2);
+  permute_kernel<float><<<G, T, 0, st>>>(ctx->vals, b, nr, ctx->vy, ctx->vy2);
+  permute_kernel<float><<<G, T, 0, st>>>(ctx->vals, b, nr, ctx->vz, ctx->vz2);
+  permute_kernel<int8_t><<<G, T, 0, st>>>(ctx->vals, b, nr, ctx->rung, ctx->rung2);
+  ctx->launches += 7;
+  CT2G_LAUNCHED(ctx);
+  if (b > 0) {
+    CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->x2, ctx->x, b * 4, cudaMemcpyDeviceToDevice, st));
+    CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->y2, ctx->y, b * 4, cudaMemcpyDeviceToDevice, st));
+    CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->z2, ctx->z, b * 4, cudaMemcpyDeviceToDevice, st));
+    CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->id2, ctx->id, b * 4, cudaMemcpyDeviceToDevice, st));
+    CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->vx2, ctx->vx, b * 4, cudaMemcpyDeviceToDevice, st));
+    CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->vy2, ctx->vy, b * 4, cudaMemcpyDeviceToDevice, st));
+    CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->vz2, ctx->vz, b * 4, cudaMemcpyDeviceToDevice, st));
+    CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->rung2, ctx->rung, b, cudaMemcpyDeviceToDevice, st));
+  }
+  std::swap(ctx->x, ctx->x2);
+  std::swap(ctx->y, ctx->y2);
+  std::swap(ctx->z, ctx->z2);
+  std::swap(ctx->id, ctx->id2);
+  std::swap(ctx->vx, ctx->vx2);
+  std::swap(ctx->vy, ctx->vy2);
+  std::swap(ctx->vz, ctx->vz2);
+  std::swap(ctx->rung, ctx->rung2);
+  ctx->rung_begin = b + nlow;
+  ctx->grid_valid = ctx->moments_valid = ctx->expansions_valid = ctx->forces_valid = false;
+  return CT2G_OK;
+}
+
+int ct2g_push_rungs(ct2g_ctx *ctx) {
+  if (!ctx) return CT2G_EINVAL;
+  ctx->rung_stack.push_back(ctx->rung_begin);
+  return CT2G_OK;
+}
+
+int ct2g_pop_rungs(ct2g_ctx *ctx) {
+  if (!ctx) return CT2G_EINVAL;
+  if (ctx->rung_stack.empty()) return ct2g_fail(ctx, CT2G_ESTATE, "rung stack empty");
+  ctx->rung_begin = ctx->rung_stack.back();
+  ctx->rung_stack.pop_back();
+  ctx->grid_valid = ctx->moments_valid = ctx->expansions_valid = ctx->forces_valid = false;
+  return CT2G_OK;
+}
+
+int ct2g_set_minrung(ct2g_ctx *ctx, int minrung) {
+  CT2G_TRY(check(ctx));
+  if (ctx->n == 0) return CT2G_OK;
+  set_minrung_kernel<<<ct2g_div_up(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->rung, ctx->n, minrung);
+  CT2G_LAUNCHED(ctx);
+  return CT2G_OK;
+}
+
+int ct2g_current_range(ct2g_ctx *ctx, size_t *begin, size_t *end) {
+  if (!ctx) return CT2G_EINVAL;
+  if (begin) *begin = ctx->rung_begin;
+  if (end) *end = ctx->n;
+  return CT2G_OK;
+}
+
+int ct2g_rung_counts(ct2g_ctx *ctx, size_t *counts, int nmax, int *nrungs) {
+  CT2G_TRY(check(ctx));
+  unsigned long long *d = nullptr;
+  CT2G_CUDA(ctx, cudaMalloc(&d, sizeof(unsigned long long) * 128));
+  cudaMemsetAsync(d, 0, sizeof(unsigned long long) * 128, ctx->stream);
+  if (ctx->n) {
+    rung_count_kernel<<<std::min<unsigned>(ct2g_div_up(ctx->n, 256), 1024), 256, 0, ctx->stream>>>(ctx->rung, ctx->n, d);
+    ctx->launches++;
+  }
+  unsigned long long h[128];
+  cudaError_t e = cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(d);
+  if (e != cudaSuccess) return ct2g_cuda_fail(ctx, e, "rung counts");
+  int top = 0;
+  for (int r = 0; r < 128; r++)
+    if (h[r]) top = r + 1;
+  if (nrungs) *nrungs = top;
+  for (int r = 0; r < nmax && counts; r++) counts[r] = r < 128 ? (size_t)h[r] : 0;
+  return CT2G_OK;
+}
+
+// kick_step, src/main.cpp:8-92, with the GPU stages; the level bookkeeping,
+// clip_top rule and push/pop order are the reference's.
+int ct2g_kick_step(ct2g_ctx *ctx, int *minrung_io, int max_rung, double scale, double adot,
+                   double tau, double t0, int minrung0, int nocrop, int *out_max_rung) {
+  CT2G_TRY(check(ctx));
+  if (!minrung_io) return ct2g_fail(ctx, CT2G_EINVAL, "null minrung");
+  int &minrung = *minrung_io;
+  std::vector<int> levels(std::max(max_rung - minrung, 0) + 1);
+  int k = 0;
+  for (int i = max_rung; i > minrung; i--) levels[k++] = i;
+  levels[k++] = minrung;
+  bool ascending = true, clip_top = false, top = false;
+  int mr = 0;
+  for (size_t li = 0; li < levels.size(); li++) {
+    if (levels[li] == minrung) {
+      ascending = false;
+      top = true;
+    } else {
+      top = false;
+    }
+    if (!ascending && !top) CT2G_TRY(ct2g_push_rungs(ctx));
+    if (!ascending) CT2G_TRY(ct2g_sort_by_rung(ctx, levels[li]));
+    if (top && minrung == minrung0) {
+      size_t counts[128];
+      int nr = 0;
+      CT2G_TRY(ct2g_rung_counts(ctx, counts, 128, &nr));
+      if (nr > minrung0 + 1) {
+        size_t fast = 0, slow = counts[minrung0];
+        for (int i = minrung0 + 1; i < nr; i++) fast += counts[i];
+        if (3 * fast > slow) clip_top = !nocrop;
+      }
+    }
+    CT2G_TRY(ct2g_particle_to_grid(ctx));
+    ct2g_kick_params kp;
+    kp.top = (clip_top && levels[li] == minrung0 + 1) ? 1 : (top ? 1 : 0);
+    kp.ascending = (ascending || top) ? 1 : 0;
+    kp.descending = (clip_top && top) ? 0 : ((!ascending || top) ? 1 : 0);
+    kp.eta = ctx->opt.eta;
+    kp.scale = (float)scale;
+    kp.first = tau == 0.0 ? 1 : 0;
+    kp.rung = levels[li];
+    kp.t0 = (float)t0;
+    kp.max_dt = (float)(0.01f / adot);
+    CT2G_TRY(ct2g_kick(ctx, &kp, &mr));
+    if (clip_top && top) CT2G_TRY(ct2g_set_minrung(ctx, minrung0 + 1));
+    if (clip_top && top) {
+      levels.push_back(minrung0 + 1);
+    } else if (!ascending || top) {
+      if (mr > levels[li]) levels.push_back(levels[li] + 1);
+    }
+    if ((!ascending || top) && !(clip_top && top)) {
+      const double dt = t0 / (double)(1 << levels[li]);
+      CT2G_TRY(ct2g_drift(ctx, (float)dt, (float)scale));
+    }
+    if (ascending && !top) CT2G_TRY(ct2g_pop_rungs(ctx));
+  }
+  if (clip_top) minrung++;
+  if (out_max_rung) *out_max_rung = mr;
+  return CT2G_OK;
+}
+
+int ct2g_fft_r2c_3d(ct2g_ctx *ctx, const double *xin, double *xout, int N, int batch) {
+  CT2G_TRY(check(ctx));
+  if (!xin || !xout || batch < 1 || !is_pow2(N) || N < 4 || N > 512)
+    return ct2g_fail(ctx, CT2G_EINVAL, "fft_r2c_3d: bad arguments");
+  const size_t n3 = (size_t)N * N * N, nk = (size_t)N * N * (N / 2 + 1);
+  double *din = nullptr;
+  double2 *dout = nullptr;
+  CT2G_CUDA(ctx, cudaMalloc(&din, sizeof(double) * n3 * batch));
+  cudaError_t e = cudaMalloc(&dout, sizeof(double2) * nk * batch);
+  if (e != cudaSuccess) {
+    cudaFree(din);
+    return ct2g_cuda_fail(ctx, e, "fft_r2c_3d alloc");
+  }
+  int rc = CT2G_OK;
+  std::vector<double2> h(nk * batch);
+  e = cudaMemcpyAsync(din, xin, sizeof(double) * n3 * batch, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) {
+    rc = ct2g_fft_r2c_f64(ctx, din, dout, N, batch);
+    if (rc == CT2G_OK) {
+      e = cudaMemcpyAsync(h.data(), dout, sizeof(double2) * nk * batch, cudaMemcpyDeviceToHost, ctx->stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    }
+  }
+  cudaFree(din);
+  cudaFree(dout);
+  if (rc != CT2G_OK) return rc;
+  if (e != cudaSuccess) return ct2g_cuda_fail(ctx, e, "fft_r2c_3d");
+  // split planes: re at [0,dimag), im at [dimag, 2 dimag)
+  for (int b = 0; b < batch; b++) {
+    double *o = xout + (size_t)b * 2 * nk;
+    for (size_t q = 0; q < nk; q++) {
+      o[q] = h[b * nk + q].x;
+      o[nk + q] = h[b * nk + q].y;
+    }
+  }
+  return CT2G_OK;
+}
+
+int ct2g_fft_c2r_3d(ct2g_ctx *ctx, const double *xin, double *xout, int N, int batch) {
+  CT2G_TRY(check(ctx));
+  if (!xin || !xout || batch < 1 || !is_pow2(N) || N < 4 || N > 512)
+    return ct2g_fail(ctx, CT2G_EINVAL, "fft_c2r_3d: bad arguments");
+  const size_t n3 = (size_t)N * N * N, nk = (size_t)N * N * (N / 2 + 1);
+  std::vector<double2> h(nk * batch);
+  for (int b = 0; b < batch; b++) {
+    const double *i = xin + (size_t)b * 2 * nk;
+    for (size_t q = 0; q < nk; q++) h[b * nk + q] = make_double2(i[q], i[nk + q]);
+  }
+  double *dout = nullptr;
+  double2 *din = nullptr;
+  CT2G_CUDA(ctx, cudaMalloc(&din, sizeof(double2) * nk * batch));
+  cudaError_t e = cudaMalloc(&dout, sizeof(double) * n3 * batch);
+  if (e != cudaSuccess) {
+    cudaFree(din);
+    return ct2g_cuda_fail(ctx, e, "fft_c2r_3d alloc");
+  }
+  int rc = CT2G_OK;
+  e = cudaMemcpyAsync(din, h.data(), sizeof(double2) * nk * batch, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) {
+    rc = ct2g_fft_c2r_f64(ctx, din, dout, N, batch);
+    if (rc == CT2G_OK) {
+      e = cudaMemcpyAsync(xout, dout, sizeof(double) * n3 * batch, cudaMemcpyDeviceToHost, ctx->stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    }
+  }
+  cudaFree(din);
+  cudaFree(dout);
+  if (rc != CT2G_OK) return rc;
+  if (e != cudaSuccess) return ct2g_cuda_fail(ctx, e, "fft_c2r_3d");
+  return CT2G_OK;
+}
+
+int ct2g_fft3d_f32_dev(ct2g_ctx *ctx, int dir, void *d_real, void *d_complex, int N, int batch) {
+  CT2G_TRY(check(ctx));
+  if (!d_real || !d_complex || batch < 1 || !is_pow2(N) || N < 4 || N > 512)
+    return ct2g_fail(ctx, CT2G_EINVAL, "fft3d_f32_dev: bad arguments");
+  if (dir > 0) return ct2g_fft_r2c_f32(ctx, (const float *)d_real, (float2 *)d_complex, N, batch);
+  return ct2g_fft_c2r_f32(ctx, (float2 *)d_complex, (float *)d_real, N, batch);
+}
+
+void *ct2g_stream(ct2g_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+int ct2g_synchronize(ct2g_ctx *ctx) {
+  CT2G_TRY(check(ctx));
+  CT2G_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return CT2G_OK;
+}
+
+int ct2g_stage_times(ct2g_ctx *ctx, float *ms, int n) {
+  CT2G_TRY(check(ctx));
+  if (!ms || n < 7) return ct2g_fail(ctx, CT2G_EINVAL, "need 7 slots");
+  CT2G_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  for (int k = 0; k < 7; k++) {
+    float t = 0.f;
+    if (cudaEventElapsedTime(&t, ctx->ev[k], ctx->ev[k + 1]) != cudaSuccess) {
+      cudaGetLastError();
+      t = -1.f;
+    }
+    ms[k] = t;
+  }
+  return CT2G_OK;
+}
+
+uint64_t ct2g_launch_count(const ct2g_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+uint64_t ct2g_interaction_count(const ct2g_ctx *ctx) {
+  if (!ctx || !ctx->d_inter) return 0;
+  unsigned long long v = 0;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  cudaMemcpy(&v, ctx->d_inter, sizeof(v), cudaMemcpyDeviceToHost);
+  return v;
+}
+
+}  // extern "C"

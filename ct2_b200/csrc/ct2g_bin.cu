@@ -1,0 +1,377 @@
+// Particle binning (particle_to_grid, src/particle.cpp:69-114,349-362):
+// Morton cell keys from the top mesh bits of the fixed-point positions, a
+// stable LSD radix sort of (key, index) pairs, cell ranges, the gather of the
+// SoA into cell order, per-particle float offsets from the cell centre for
+// the direct sum, and the sink-chunk list.
+//
+// The reference partitions recursively (a Hoare partition per level,
+// dimension depth%3); for a power-of-two mesh every particle lands in the
+// same leaf as here, because the split point fixed32((I+N/2)/Ncell) equals
+// (I+N/2) << (32-mbits), and the leaves come out in the same (Morton) order.
+// Only the order inside a cell differs: the reference's partition leaves it
+// arbitrary, here it is the stable (previous) order, so the sort is
+// deterministic.
+#include "ct2g_internal.cuh"
+
+namespace {
+
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 4;  // per thread
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__device__ __forceinline__ uint32_t warp_incl_scan(uint32_t v) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t t = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += t;
+  }
+  return v;
+}
+
+// block-wide exclusive scan of one value per thread; returns block total
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t *smem32,
+                                                    uint32_t &total) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  uint32_t inc = warp_incl_scan(v);
+  if (lane == 31) smem32[w] = inc;
+  __syncthreads();
+  if (w == 0) {
+    uint32_t s = lane < nw ? smem32[lane] : 0;
+    uint32_t si = warp_incl_scan(s);
+    if (lane < nw) smem32[lane] = si - s;
+    if (lane == nw - 1) smem32[32] = si;
+  }
+  __syncthreads();
+  uint32_t res = inc - v + smem32[w];
+  total = smem32[32];
+  __syncthreads();
+  return res;
+}
+
+__global__ void scan_reduce_kernel(const uint32_t *__restrict__ in, size_t n,
+                                   uint32_t *__restrict__ bsum) {
+  __shared__ uint32_t sm[33];
+  size_t base = (size_t)blockIdx.x * kScanTile;
+  uint32_t s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; k++) {
+    size_t i = base + (size_t)k * kScanThreads + threadIdx.x;
+    if (i < n) s += in[i];
+  }
+  uint32_t tot;
+  block_excl_scan(s, sm, tot);
+  if (threadIdx.x == 0) bsum[blockIdx.x] = tot;
+}
+
+// single block: exclusive scan of bsum[nb] in place (nb arbitrary)
+__global__ void scan_single_kernel(uint32_t *__restrict__ a, size_t nb, uint32_t *total) {
+  __shared__ uint32_t sm[33];
+  uint32_t carry = 0;
+  for (size_t base = 0; base < nb; base += blockDim.x) {
+    size_t i = base + threadIdx.x;
+    uint32_t v = i < nb ? a[i] : 0;
+    uint32_t tot;
+    uint32_t ex = block_excl_scan(v, sm, tot);
+    if (i < nb) a[i] = ex + carry;
+    carry += tot;
+  }
+  if (threadIdx.x == 0 && total) *total = carry;
+}
+
+__global__ void scan_apply_kernel(const uint32_t *__restrict__ in, size_t n,
+                                  const uint32_t *__restrict__ boff, uint32_t *__restrict__ out) {
+  __shared__ uint32_t sm[33];
+  size_t base = (size_t)blockIdx.x * kScanTile + (size_t)threadIdx.x * kScanItems;
+  uint32_t v[kScanItems];
+  uint32_t s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; k++) {
+    v[k] = (base + k < n) ? in[base + k] : 0;
+    s += v[k];
+  }
+  uint32_t tot;
+  uint32_t ex = block_excl_scan(s, sm, tot) + boff[blockIdx.x];
+#pragma unroll
+  for (int k = 0; k < kScanItems; k++) {
+    if (base + k < n) out[base + k] = ex;
+    ex += v[k];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// radix sort, 8-bit digits, tiles of 256 threads x 16 items (striped per warp)
+// ---------------------------------------------------------------------------
+constexpr int kRadixThreads = 256;
+constexpr int kRadixItems = 16;
+constexpr int kRadixTile = kRadixThreads * kRadixItems;
+constexpr int kRadixWarps = kRadixThreads / 32;
+
+__device__ __forceinline__ size_t radix_item(int slot) {
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  return (size_t)blockIdx.x * kRadixTile + (size_t)w * 32 * kRadixItems + slot * 32 + lane;
+}
+
+__global__ void radix_hist_kernel(const uint32_t *__restrict__ keys, size_t n, int shift,
+                                  uint32_t ntiles, uint32_t *__restrict__ hist) {
+  __shared__ uint32_t cnt[256];
+  cnt[threadIdx.x] = 0;
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < kRadixItems; k++) {
+    size_t i = radix_item(k);
+    if (i < n) atomicAdd(&cnt[(keys[i] >> shift) & 255u], 1u);
+  }
+  __syncthreads();
+  hist[(size_t)threadIdx.x * ntiles + blockIdx.x] = cnt[threadIdx.x];
+}
+
+__global__ void radix_scatter_kernel(const uint32_t *__restrict__ keys,
+                                     const uint32_t *__restrict__ vals, size_t n, int shift,
+                                     uint32_t ntiles, const uint32_t *__restrict__ hscan,
+                                     uint32_t *__restrict__ okeys, uint32_t *__restrict__ ovals) {
+  __shared__ uint32_t wcnt[kRadixWarps][256];
+  __shared__ uint32_t base[256];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int i = threadIdx.x; i < kRadixWarps * 256; i += kRadixThreads) (&wcnt[0][0])[i] = 0;
+  base[threadIdx.x] = hscan[(size_t)threadIdx.x * ntiles + blockIdx.x];
+  __syncthreads();
+  uint32_t k_[kRadixItems], v_[kRadixItems], r_[kRadixItems];
+  const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+  for (int k = 0; k < kRadixItems; k++) {
+    size_t i = radix_item(k);
+    bool valid = i < n;
+    uint32_t key = valid ? keys[i] : 0u;
+    uint32_t d = (key >> shift) & 255u;
+    k_[k] = key;
+    v_[k] = valid ? vals[i] : 0u;
+    unsigned act = __ballot_sync(0xffffffffu, valid);
+    unsigned peers = __match_any_sync(0xffffffffu, valid ? d : 256u + lane) & act;
+    uint32_t before = valid ? wcnt[w][d] : 0u;
+    __syncwarp();
+    if (valid) {
+      r_[k] = before + __popc(peers & lt);
+      if ((peers & lt) == 0) wcnt[w][d] = before + __popc(peers);
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+  {  // exclusive prefix over warps for digit threadIdx.x
+    uint32_t run = 0;
+    for (int ww = 0; ww < kRadixWarps; ww++) {
+      uint32_t t = wcnt[ww][threadIdx.x];
+      wcnt[ww][threadIdx.x] = run;
+      run += t;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < kRadixItems; k++) {
+    size_t i = radix_item(k);
+    if (i < n) {
+      uint32_t d = (k_[k] >> shift) & 255u;
+      uint32_t pos = base[d] + wcnt[w][d] + r_[k];
+      okeys[pos] = k_[k];
+      ovals[pos] = v_[k];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+__global__ void keys_kernel(const uint32_t *__restrict__ x, const uint32_t *__restrict__ y,
+                            const uint32_t *__restrict__ z, size_t begin, size_t nr, int mbits,
+                            uint32_t *__restrict__ keys, uint32_t *__restrict__ vals) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nr) return;
+  const int sh = 32 - mbits;
+  size_t g = begin + i;
+  keys[i] = ct2g_morton(x[g] >> sh, y[g] >> sh, z[g] >> sh);
+  vals[i] = (uint32_t)i;
+}
+
+// cell_start from sorted Morton keys: keys (key[i-1], key[i]] start at begin+i
+__global__ void cell_start_kernel(const uint32_t *__restrict__ skeys, size_t nr, size_t begin,
+                                  uint32_t C, uint32_t *__restrict__ cs) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > nr) return;
+  uint32_t lo = (i == 0) ? 0u : skeys[i - 1] + 1u;
+  uint32_t hi = (i == nr) ? C : skeys[i];
+  for (uint32_t c = lo; c <= hi && c < C + 1; c++) cs[c] = (uint32_t)(begin + i);
+  if (i == nr) cs[C] = (uint32_t)(begin + nr);
+}
+
+// gather the active range into cell order; write the direct-sum source records
+__global__ void gather_kernel(const uint32_t *__restrict__ perm, size_t begin, size_t nr,
+                              int mbits, const uint32_t *__restrict__ x,
+                              const uint32_t *__restrict__ y, const uint32_t *__restrict__ z,
+                              const float *__restrict__ vx, const float *__restrict__ vy,
+                              const float *__restrict__ vz, const int8_t *__restrict__ rung,
+                              const uint32_t *__restrict__ id, uint32_t *__restrict__ x2,
+                              uint32_t *__restrict__ y2, uint32_t *__restrict__ z2,
+                              float *__restrict__ vx2, float *__restrict__ vy2,
+                              float *__restrict__ vz2, int8_t *__restrict__ rung2,
+                              uint32_t *__restrict__ id2, float4 *__restrict__ src) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nr) return;
+  size_t s = begin + perm[i], d = begin + i;
+  uint32_t px = x[s], py = y[s], pz = z[s];
+  x2[d] = px;
+  y2[d] = py;
+  z2[d] = pz;
+  vx2[d] = vx[s];
+  vy2[d] = vy[s];
+  vz2[d] = vz[s];
+  rung2[d] = rung[s];
+  id2[d] = id[s];
+  // offset from the cell centre: low (32-mbits) bits minus half a cell,
+  // exact in float (|value| < 2^(31-mbits) <= 2^24)
+  const int sh = 32 - mbits;
+  const uint32_t mask = (sh == 32) ? 0xffffffffu : ((1u << sh) - 1u);
+  const int32_t half = (int32_t)(1u << (sh - 1));
+  const float sc = (float)CT2G_TWO_M32;
+  src[d] = make_float4((float)((int32_t)(px & mask) - half) * sc,
+                       (float)((int32_t)(py & mask) - half) * sc,
+                       (float)((int32_t)(pz & mask) - half) * sc, 0.f);
+}
+
+// chunk starts: every 32nd particle of a cell (counted from the cell start)
+__global__ void chunk_flag_kernel(const uint32_t *__restrict__ skeys,
+                                  const uint32_t *__restrict__ cs, size_t begin, size_t nr,
+                                  uint32_t *__restrict__ flags) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nr) return;
+  uint32_t c0 = cs[skeys[i]];
+  flags[i] = (((uint32_t)(begin + i) - c0) & 31u) == 0 ? 1u : 0u;
+}
+
+__global__ void chunk_fill_kernel(const uint32_t *__restrict__ flags,
+                                  const uint32_t *__restrict__ fscan, size_t begin, size_t nr,
+                                  uint32_t *__restrict__ chunk_begin) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nr) return;
+  if (flags[i]) chunk_begin[fscan[i]] = (uint32_t)(begin + i);
+}
+
+}  // namespace
+
+// exclusive scan of n uint32 values (in may equal out); optional host total
+int ct2g_scan_exclusive(ct2g_ctx *ctx, const uint32_t *in, uint32_t *out, size_t n,
+                        uint32_t *total_host) {
+  if (n == 0) {
+    if (total_host) *total_host = 0;
+    return CT2G_OK;
+  }
+  unsigned nb = ct2g_div_up(n, kScanTile);
+  if (ctx->scan_tmp_words < (size_t)nb + 1) {
+    if (ctx->scan_tmp) cudaFree(ctx->scan_tmp);
+    ctx->scan_tmp = nullptr;
+    ctx->scan_tmp_words = 0;
+    CT2G_CUDA(ctx, cudaMalloc(&ctx->scan_tmp, sizeof(uint32_t) * ((size_t)nb + 1)));
+    ctx->scan_tmp_words = (size_t)nb + 1;
+  }
+  uint32_t *bsum = ctx->scan_tmp;
+  scan_reduce_kernel<<<nb, kScanThreads, 0, ctx->stream>>>(in, n, bsum);
+  CT2G_LAUNCHED(ctx);
+  scan_single_kernel<<<1, 1024, 0, ctx->stream>>>(bsum, nb, bsum + nb);
+  CT2G_LAUNCHED(ctx);
+  scan_apply_kernel<<<nb, kScanThreads, 0, ctx->stream>>>(in, n, bsum, out);
+  CT2G_LAUNCHED(ctx);
+  if (total_host) {
+    CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->h_pinned, bsum + nb, sizeof(uint32_t),
+                                   cudaMemcpyDeviceToHost, ctx->stream));
+    CT2G_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    *total_host = ctx->h_pinned[0];
+  }
+  return CT2G_OK;
+}
+
+// Sort the current range [rung_begin, n) by cell; build cell ranges, source
+// records and sink chunks.
+int ct2g_bin_range(ct2g_ctx *ctx) {
+  const size_t begin = ctx->rung_begin, nr = ctx->n - ctx->rung_begin;
+  const int mbits = ctx->mbits;
+  cudaStream_t st = ctx->stream;
+  const unsigned T = 256;
+  if (nr > 0) {
+    keys_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(ctx->x, ctx->y, ctx->z, begin, nr, mbits,
+                                                    ctx->keys, ctx->vals);
+    CT2G_LAUNCHED(ctx);
+    const int bits = 3 * mbits;
+    const uint32_t ntiles = ct2g_div_up(nr, kRadixTile);
+    uint32_t *ka = ctx->keys, *va = ctx->vals, *kb = ctx->keys2, *vb = ctx->vals2;
+    for (int shift = 0; shift < bits; shift += 8) {
+      radix_hist_kernel<<<ntiles, kRadixThreads, 0, st>>>(ka, nr, shift, ntiles, ctx->hist);
+      CT2G_LAUNCHED(ctx);
+      CT2G_TRY(ct2g_scan_exclusive(ctx, ctx->hist, ctx->hist, (size_t)256 * ntiles, nullptr));
+      radix_scatter_kernel<<<ntiles, kRadixThreads, 0, st>>>(ka, va, nr, shift, ntiles,
+                                                             ctx->hist, kb, vb);
+      CT2G_LAUNCHED(ctx);
+      uint32_t *t = ka;
+      ka = kb;
+      kb = t;
+      t = va;
+      va = vb;
+      vb = t;
+    }
+    // sorted keys/perm now in (ka, va); keep them addressable as keys/vals
+    if (ka != ctx->keys) {
+      uint32_t *t = ctx->keys;
+      ctx->keys = ka;
+      ctx->keys2 = t;
+      t = ctx->vals;
+      ctx->vals = va;
+      ctx->vals2 = t;
+    }
+    cell_start_kernel<<<ct2g_div_up(nr + 1, T), T, 0, st>>>(ctx->keys, nr, begin,
+                                                           (uint32_t)ctx->C, ctx->cell_start);
+    CT2G_LAUNCHED(ctx);
+    gather_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(
+        ctx->vals, begin, nr, mbits, ctx->x, ctx->y, ctx->z, ctx->vx, ctx->vy, ctx->vz,
+        ctx->rung, ctx->id, ctx->x2, ctx->y2, ctx->z2, ctx->vx2, ctx->vy2, ctx->vz2, ctx->rung2,
+        ctx->id2, ctx->src);
+    CT2G_LAUNCHED(ctx);
+    // particles outside the range keep their place
+    if (begin > 0) {
+      CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->x2, ctx->x, begin * 4, cudaMemcpyDeviceToDevice, st));
+      CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->y2, ctx->y, begin * 4, cudaMemcpyDeviceToDevice, st));
+      CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->z2, ctx->z, begin * 4, cudaMemcpyDeviceToDevice, st));
+      CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->vx2, ctx->vx, begin * 4, cudaMemcpyDeviceToDevice, st));
+      CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->vy2, ctx->vy, begin * 4, cudaMemcpyDeviceToDevice, st));
+      CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->vz2, ctx->vz, begin * 4, cudaMemcpyDeviceToDevice, st));
+      CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->rung2, ctx->rung, begin, cudaMemcpyDeviceToDevice, st));
+      CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->id2, ctx->id, begin * 4, cudaMemcpyDeviceToDevice, st));
+    }
+    std::swap(ctx->x, ctx->x2);
+    std::swap(ctx->y, ctx->y2);
+    std::swap(ctx->z, ctx->z2);
+    std::swap(ctx->vx, ctx->vx2);
+    std::swap(ctx->vy, ctx->vy2);
+    std::swap(ctx->vz, ctx->vz2);
+    std::swap(ctx->rung, ctx->rung2);
+    std::swap(ctx->id, ctx->id2);
+    // sink chunks
+    chunk_flag_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(ctx->keys, ctx->cell_start, begin, nr,
+                                                        ctx->flags);
+    CT2G_LAUNCHED(ctx);
+    uint32_t total = 0;
+    CT2G_TRY(ct2g_scan_exclusive(ctx, ctx->flags, ctx->vals2, nr, &total));
+    chunk_fill_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(ctx->flags, ctx->vals2, begin, nr,
+                                                        ctx->chunk_begin);
+    CT2G_LAUNCHED(ctx);
+    ctx->nchunks = total;
+  } else {
+    // empty range: every cell empty
+    uint32_t v = (uint32_t)begin;
+    std::vector<uint32_t> h(ctx->C + 1, v);
+    CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->cell_start, h.data(), sizeof(uint32_t) * h.size(),
+                                   cudaMemcpyHostToDevice, st));
+    CT2G_CUDA(ctx, cudaStreamSynchronize(st));
+    ctx->nchunks = 0;
+  }
+  ctx->grid_valid = true;
+  ctx->moments_valid = false;
+  ctx->expansions_valid = false;
+  ctx->forces_valid = false;
+  return CT2G_OK;
+}

@@ -1,0 +1,187 @@
+// Internal declarations shared by the ct2g CUDA translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "../../include/ct2g.h"
+
+#define CT2G_TWO_M32 2.3283064365386963e-10
+
+// ---------------------------------------------------------------------------
+// Multi-indices n = (nx, ny, nz), |n| <= P: ordered by degree, then nx
+// descending, then ny descending.  idx = T(d) + (d-nx)(d-nx+1)/2 + nz with
+// T(d) = d(d+1)(d+2)/6.  (The same ordering as the CPU oracle.)
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr int ct2g_ncomp(int p) { return (p + 1) * (p + 2) * (p + 3) / 6; }
+__host__ __device__ constexpr int ct2g_mi_index(int nx, int ny, int nz) {
+  return (nx + ny + nz) * (nx + ny + nz + 1) * (nx + ny + nz + 2) / 6 +
+         (ny + nz) * (ny + nz + 1) / 2 + nz;
+}
+
+// ---------------------------------------------------------------------------
+// Morton keys: cell (i,j,k) -> bits interleaved from the most significant, x
+// first.  The reference's recursive bisection (src/particle.cpp:89-114,
+// depth d splitting dimension d%3) lays its leaves out in exactly this order.
+// ---------------------------------------------------------------------------
+__host__ __device__ __forceinline__ uint32_t ct2g_spread3(uint32_t v) {
+  v &= 0x3ffu;
+  v = (v | (v << 16)) & 0x030000ffu;
+  v = (v | (v << 8)) & 0x0300f00fu;
+  v = (v | (v << 4)) & 0x030c30c3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+__host__ __device__ __forceinline__ uint32_t ct2g_compact3(uint32_t v) {
+  v &= 0x09249249u;
+  v = (v | (v >> 2)) & 0x030c30c3u;
+  v = (v | (v >> 4)) & 0x0300f00fu;
+  v = (v | (v >> 8)) & 0x030000ffu;
+  v = (v | (v >> 16)) & 0x3ffu;
+  return v;
+}
+__host__ __device__ __forceinline__ uint32_t ct2g_morton(uint32_t i, uint32_t j, uint32_t k) {
+  return (ct2g_spread3(i) << 2) | (ct2g_spread3(j) << 1) | ct2g_spread3(k);
+}
+
+template <int P>
+struct MiTable {
+  static constexpr int NC = ct2g_ncomp(P);
+  int nx[NC];
+  int ny[NC];
+  int nz[NC];
+  int deg[NC];
+  constexpr MiTable() : nx(), ny(), nz(), deg() {
+    int k = 0;
+    for (int d = 0; d <= P; d++)
+      for (int a = d; a >= 0; a--)
+        for (int b = d - a; b >= 0; b--) {
+          nx[k] = a;
+          ny[k] = b;
+          nz[k] = d - a - b;
+          deg[k] = d;
+          k++;
+        }
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Context
+// ---------------------------------------------------------------------------
+struct FftPlanBufs;
+
+struct ct2g_ctx {
+  ct2g_options opt;
+  int mbits = 0;
+  int M = 0;       // mesh cells per dim
+  int64_t C = 0;   // mesh^3
+  int64_t CK = 0;  // mesh*mesh*(mesh/2+1)
+  int p = 0;
+  int nc = 0;      // ncomp(p)
+  int device = 0;
+  int num_sms = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[8] = {};
+  float stage_ms[8] = {};
+  std::string err;
+  uint64_t launches = 0;
+  uint64_t interactions = 0;
+
+  // particle store (current order) and the sort target buffers
+  size_t n = 0, cap = 0;
+  uint32_t *x = nullptr, *y = nullptr, *z = nullptr, *id = nullptr;
+  float *vx = nullptr, *vy = nullptr, *vz = nullptr;
+  int8_t *rung = nullptr;
+  uint32_t *x2 = nullptr, *y2 = nullptr, *z2 = nullptr, *id2 = nullptr;
+  float *vx2 = nullptr, *vy2 = nullptr, *vz2 = nullptr;
+  int8_t *rung2 = nullptr;
+  // binning scratch
+  uint32_t *keys = nullptr, *keys2 = nullptr, *vals = nullptr, *vals2 = nullptr;
+  uint32_t *hist = nullptr;   // radix digit histograms
+  uint32_t *scan_tmp = nullptr;
+  size_t scan_tmp_words = 0;
+  uint32_t *cell_start = nullptr;  // [C+1] indexed by Morton key, absolute indices
+  float4 *src = nullptr;           // per sorted particle: offset from own cell centre
+  uint32_t *chunk_begin = nullptr; // sink chunks (<=32 particles of one cell)
+  uint32_t *flags = nullptr;
+  uint32_t nchunks = 0;
+  // forces
+  float *fx = nullptr, *fy = nullptr, *fz = nullptr, *pot = nullptr;
+  int *d_maxrung = nullptr;
+  unsigned long long *d_inter = nullptr;
+  uint32_t *h_pinned = nullptr;  // small pinned host scratch
+  // mesh
+  float *grid = nullptr;    // [nc][C] real: moments, then expansions
+  float2 *spec = nullptr;   // [nc][CK] complex
+  float *greens = nullptr;  // [nc][CK] real-or-imag
+  float2 *tw32 = nullptr;   // twiddles exp(-2 pi i k/M), k < M/2
+  double2 *tw64 = nullptr;
+  int tw_n = 0;
+  // stencil
+  int nstencil = 0;
+  int *d_stencil = nullptr;  // [nstencil][3]
+
+  // state
+  size_t rung_begin = 0;
+  std::vector<size_t> rung_stack;
+  bool grid_valid = false;     // cell_start / src / chunks valid for current range
+  bool moments_valid = false;
+  bool expansions_valid = false;
+  bool greens_valid = false;
+  bool forces_valid = false;
+  bool has_particles = false;
+};
+
+// ---------------------------------------------------------------------------
+// Error plumbing
+// ---------------------------------------------------------------------------
+int ct2g_fail(ct2g_ctx *ctx, int code, const std::string &msg);
+int ct2g_cuda_fail(ct2g_ctx *ctx, cudaError_t e, const char *what);
+
+#define CT2G_CUDA(ctx, call)                                       \
+  do {                                                             \
+    cudaError_t e_ = (call);                                       \
+    if (e_ != cudaSuccess) return ct2g_cuda_fail((ctx), e_, #call); \
+  } while (0)
+
+#define CT2G_LAUNCHED(ctx)                                                 \
+  do {                                                                     \
+    (ctx)->launches++;                                                     \
+    cudaError_t e_ = cudaGetLastError();                                   \
+    if (e_ != cudaSuccess) return ct2g_cuda_fail((ctx), e_, "kernel launch"); \
+  } while (0)
+
+#define CT2G_TRY(expr)        \
+  do {                        \
+    int rc_ = (expr);         \
+    if (rc_ != CT2G_OK) return rc_; \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// Stage entry points (implemented across the .cu files)
+// ---------------------------------------------------------------------------
+int ct2g_alloc_particles(ct2g_ctx *ctx, size_t n);
+int ct2g_alloc_mesh(ct2g_ctx *ctx);
+int ct2g_scan_exclusive(ct2g_ctx *ctx, const uint32_t *in, uint32_t *out, size_t n,
+                        uint32_t *total_host);
+int ct2g_bin_range(ct2g_ctx *ctx);
+int ct2g_build_greens(ct2g_ctx *ctx);
+int ct2g_p2m(ct2g_ctx *ctx);
+int ct2g_mesh_solve(ct2g_ctx *ctx);
+int ct2g_forces(ct2g_ctx *ctx);
+int ct2g_update(ct2g_ctx *ctx, const ct2g_kick_params *p, int *max_rung, bool fuse_drift,
+                float drift_dt, float drift_scale);
+int ct2g_drift_all(ct2g_ctx *ctx, float dt, float scale);
+int ct2g_twiddles(ct2g_ctx *ctx, int N);
+// batched 3D FFTs on device buffers, on ctx->stream
+int ct2g_fft_r2c_f32(ct2g_ctx *ctx, const float *in, float2 *out, int N, int batch);
+int ct2g_fft_c2r_f32(ct2g_ctx *ctx, float2 *in, float *out, int N, int batch);
+int ct2g_fft_r2c_f64(ct2g_ctx *ctx, const double *in, double2 *out, int N, int batch);
+int ct2g_fft_c2r_f64(ct2g_ctx *ctx, double2 *in, double *out, int N, int batch);
+
+static inline unsigned ct2g_div_up(size_t a, size_t b) { return (unsigned)((a + b - 1) / b); }

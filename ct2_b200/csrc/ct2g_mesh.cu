@@ -1,0 +1,418 @@
+// Mesh stages of the gravity step:
+//   P2M    per-cell moments about the cell centre, FP64 accumulate
+//          (particle_compute_multipoles, src/particle.cpp:180-209)
+//   Green  k-space Green's tensor with the near zone zeroed and Ewald images
+//          (particle_greens, src/particle.cpp:116-178), built once per context
+//   MG2L   per-k contraction L_a = sum_b G_{a+b} M_b (src/particle.cpp:244-250)
+//   solve  forward FFT -> MG2L -> inverse FFT (particle_compute_expansions,
+//          src/particle.cpp:211-271)
+//
+// The reference takes the multipole algebra from the un-vendored sfmm
+// library.  Here it is the Cartesian Taylor form: with s = x_j - centre(src),
+// t = x - centre(sink), R = centre(sink) - centre(src),
+//   M_b = sum_j (-s_j)^b / b!,   L_a = sum_b D^{a+b} phi(R) M_b,
+//   phi(x) = -GM sum_a L_a t^a/a!,   F_i = GM sum_a L_{a+e_i} t^a/a!,
+// truncated at |a|+|b| <= p, the cell-centre sums done as one periodic
+// convolution per (a, b) on the mesh.
+#include "ct2g_internal.cuh"
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// P2M: one thread per cell (particles are cell-sorted, so no atomics)
+// ---------------------------------------------------------------------------
+template <int P>
+__global__ void __launch_bounds__(128) p2m_kernel(const uint32_t *__restrict__ x,
+                                                  const uint32_t *__restrict__ y,
+                                                  const uint32_t *__restrict__ z,
+                                                  const uint32_t *__restrict__ cs, int mbits,
+                                                  int64_t C, float *__restrict__ grid) {
+  constexpr MiTable<P> T{};
+  constexpr int NC = MiTable<P>::NC;
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;  // row-major cell
+  if (c >= C) return;
+  const uint32_t M1 = (1u << mbits) - 1u;
+  const uint32_t cx = (uint32_t)(c >> (2 * mbits)), cy = (uint32_t)(c >> mbits) & M1,
+                 cz = (uint32_t)c & M1;
+  const uint32_t key = ct2g_morton(cx, cy, cz);
+  const uint32_t b = cs[key], e = cs[key + 1];
+  double acc[NC];
+#pragma unroll
+  for (int k = 0; k < NC; k++) acc[k] = 0.0;
+  const int sh = 32 - mbits;
+  const uint32_t halfc = 1u << (sh - 1);
+  const uint32_t ux = (cx << sh) + halfc, uy = (cy << sh) + halfc, uz = (cz << sh) + halfc;
+  for (uint32_t i = b; i < e; i++) {
+    // -s, exactly from the fixed-point difference
+    const double sx = -(double)(int32_t)(x[i] - ux) * CT2G_TWO_M32;
+    const double sy = -(double)(int32_t)(y[i] - uy) * CT2G_TWO_M32;
+    const double sz = -(double)(int32_t)(z[i] - uz) * CT2G_TWO_M32;
+    double px[P + 1], py[P + 1], pz[P + 1];
+    px[0] = py[0] = pz[0] = 1.0;
+#pragma unroll
+    for (int q = 1; q <= P; q++) {
+      px[q] = px[q - 1] * sx * (1.0 / q);
+      py[q] = py[q - 1] * sy * (1.0 / q);
+      pz[q] = pz[q - 1] * sz * (1.0 / q);
+    }
+#pragma unroll
+    for (int k = 0; k < NC; k++) acc[k] += px[T.nx[k]] * py[T.ny[k]] * pz[T.nz[k]];
+  }
+#pragma unroll
+  for (int k = 0; k < NC; k++) grid[(int64_t)k * C + c] = (float)acc[k];
+}
+
+// ---------------------------------------------------------------------------
+// MG2L: one thread per k-point, in place on the spectrum.
+// G_n is real for even |n| and i*g for odd |n| (parity of D^n phi).
+// ---------------------------------------------------------------------------
+template <int P>
+__global__ void __launch_bounds__(128) mg2l_kernel(float2 *__restrict__ spec,
+                                                   const float *__restrict__ G, int64_t CK) {
+  constexpr MiTable<P> T{};
+  constexpr int NC = MiTable<P>::NC;
+  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= CK) return;
+  float2 m[NC];
+  float g[NC];
+#pragma unroll
+  for (int k = 0; k < NC; k++) {
+    m[k] = spec[(int64_t)k * CK + q];
+    g[k] = G[(int64_t)k * CK + q];
+  }
+#pragma unroll
+  for (int a = 0; a < NC; a++) {
+    float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int b = 0; b < NC; b++) {
+      if (T.deg[a] + T.deg[b] <= P) {
+        const int ab = ct2g_mi_index(T.nx[a] + T.nx[b], T.ny[a] + T.ny[b], T.nz[a] + T.nz[b]);
+        const float gv = g[ab];
+        if (((T.deg[a] + T.deg[b]) & 1) == 0) {
+          acc.x = fmaf(gv, m[b].x, acc.x);
+          acc.y = fmaf(gv, m[b].y, acc.y);
+        } else {  // i*g*(mx + i my) = (-g my, g mx)
+          acc.x = fmaf(-gv, m[b].y, acc.x);
+          acc.y = fmaf(gv, m[b].x, acc.y);
+        }
+      }
+    }
+    spec[(int64_t)a * CK + q] = acc;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Green's tensor, FP64, runtime tables (built once per context)
+// ---------------------------------------------------------------------------
+constexpr int kMaxTerms = 16;
+struct DTerm {
+  int mx, my, mz, j;
+  double coef;
+};
+
+// f^[j] = (r^-1 d/dr)^j f for the softened kernels and erf(alpha r)/r
+__device__ void radial_plummer(double r2, double eps, int jmax, double *f) {
+  double s2 = r2 + eps * eps;
+  double inv = 1.0 / s2, base = 1.0 / sqrt(s2);
+  double df = 1.0;  // (2j-1)!!
+  for (int j = 0; j <= jmax; j++) {
+    if (j > 0) df *= (2 * j - 1);
+    f[j] = ((j & 1) ? -df : df) * base;
+    base *= inv;
+  }
+}
+
+__device__ void radial_sphere(double r2, double h, int jmax, double *f) {
+  if (r2 >= h * h) {
+    radial_plummer(r2, 0.0, jmax, f);
+    return;
+  }
+  const double h3 = h * h * h;
+  for (int j = 0; j <= jmax; j++) f[j] = 0.0;
+  f[0] = 1.5 / h - 0.5 * r2 / h3;
+  if (jmax >= 1) f[1] = -1.0 / h3;
+}
+
+__device__ void radial_erf(double r2, double alpha, int jmax, double *f) {
+  const double a2 = alpha * alpha;
+  const double spi = 1.7724538509055160273;
+  if (a2 * r2 < 4.0) {
+    // power series in u = r^2
+    const double pre = 2.0 * alpha / spi;
+    double p2 = 1.0;
+    for (int j = 0; j <= jmax; j++) {
+      double sum = 0.0, term = 1.0;
+      for (int k = j; k < j + 80; k++) {
+        double t = term / (2 * k + 1);
+        sum += (k & 1) ? -t : t;
+        term *= a2 * r2 / (k - j + 1);
+        if (term < 1e-30 * fabs(sum) && k > j + 4) break;
+      }
+      f[j] = pre * p2 * sum;
+      p2 *= 2.0 * a2;
+    }
+  } else {
+    // 1/r - erfc(alpha r)/r with Smith's recursion for the erfc part
+    const double r = sqrt(r2);
+    const double ex = exp(-a2 * r2);
+    double B = erfc(alpha * r) / r;
+    double Aj = 1.0 / r;
+    double twoa2j = 1.0;
+    for (int j = 0; j <= jmax; j++) {
+      if (j > 0) {
+        twoa2j *= 2.0 * a2;
+        B = ((2 * j - 1) * B + twoa2j / (alpha * spi) * ex) / r2;
+        Aj *= (2 * j - 1) / r2;
+      }
+      f[j] = ((j & 1) ? -1.0 : 1.0) * (Aj - B);
+    }
+  }
+}
+
+__device__ __forceinline__ double ipow(double x, int e) {
+  double r = 1.0;
+  for (int i = 0; i < e; i++) r *= x;
+  return r;
+}
+
+// real-space part for components [k0, k0+K) at every lattice offset
+__global__ void greens_real_kernel(int mbits, int p, int kernel, double soft, double bw2,
+                                   double alpha, const DTerm *__restrict__ terms,
+                                   const int *__restrict__ nterms, int k0, int K,
+                                   double *__restrict__ out) {
+  const int M = 1 << mbits;
+  const int64_t C = (int64_t)M * M * M;
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= C) return;
+  int o[3] = {(int)(c >> (2 * mbits)), (int)((c >> mbits) & (M - 1)), (int)(c & (M - 1))};
+  for (int d = 0; d < 3; d++)
+    if (o[d] >= M / 2) o[d] -= M;
+  const double h = 1.0 / M;
+  const double R[3] = {o[0] * h, o[1] * h, o[2] * h};
+  const double r2 = R[0] * R[0] + R[1] * R[1] + R[2] * R[2];
+  const bool near = (double)(o[0] * o[0] + o[1] * o[1] + o[2] * o[2]) <= bw2;
+  double fe[CT2G_MAX_ORDER + 1], fk[CT2G_MAX_ORDER + 1], f[CT2G_MAX_ORDER + 1];
+  radial_erf(r2, alpha, p, fe);
+  if (!near) {
+    if (kernel == CT2G_SOFT_SPHERE)
+      radial_sphere(r2, soft, p, fk);
+    else
+      radial_plummer(r2, soft, p, fk);
+  }
+  for (int j = 0; j <= p; j++) f[j] = (near ? 0.0 : fk[j]) - fe[j];
+  for (int kk = 0; kk < K; kk++) {
+    const int k = k0 + kk;
+    double g = 0.0;
+    for (int t = 0; t < nterms[k]; t++) {
+      const DTerm d = terms[k * kMaxTerms + t];
+      g += d.coef * ipow(R[0], d.mx) * ipow(R[1], d.my) * ipow(R[2], d.mz) * f[d.j];
+    }
+    if (k == 0) g -= 3.14159265358979323846 / (alpha * alpha);
+    out[(int64_t)kk * C + c] = g;
+  }
+}
+
+// combine the FFT of the real-space part with the folded Ewald k-space sum
+__global__ void greens_finish_kernel(int mbits, int p, double alpha, int kmax,
+                                     const int *__restrict__ mi, int k0, int K,
+                                     const double2 *__restrict__ spec64, float *__restrict__ G) {
+  const int M = 1 << mbits;
+  const int NH = M / 2 + 1;
+  const int64_t CK = (int64_t)M * M * NH;
+  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= CK) return;
+  const int qx = (int)(q / ((int64_t)M * NH)), qy = (int)((q / NH) % M), qz = (int)(q % NH);
+  const double norm = 1.0 / ((double)M * M * M);
+  double acc[64];
+  for (int kk = 0; kk < K; kk++) {
+    const int k = k0 + kk;
+    const int deg = mi[3 * k] + mi[3 * k + 1] + mi[3 * k + 2];
+    const double2 v = spec64[(int64_t)kk * CK + q];
+    acc[kk] = ((deg & 1) ? v.y : v.x) * norm;
+  }
+  // aliases kv == q (mod M) with |kv| <= kmax, kv != 0
+  const double pi = 3.14159265358979323846;
+  const double K2 = (double)kmax * kmax;
+  auto first = [&](int qd) {  // smallest alias of qd (in [0,M)) that is >= -kmax
+    int t = qd;
+    while (t - M >= -kmax) t -= M;
+    return t;
+  };
+  for (int kx = first(qx); kx <= kmax; kx += M)
+    for (int ky = first(qy); ky <= kmax; ky += M)
+      for (int kz = first(qz); kz <= kmax; kz += M) {
+        const double k2 = (double)kx * kx + (double)ky * ky + (double)kz * kz;
+        if (k2 == 0.0 || k2 > K2) continue;
+        const double w = exp(-pi * pi * k2 / (alpha * alpha)) / (pi * k2);
+        const double kv[3] = {2 * pi * kx, 2 * pi * ky, 2 * pi * kz};
+        for (int kk = 0; kk < K; kk++) {
+          const int k = k0 + kk;
+          const int *n = mi + 3 * k;
+          const int deg = n[0] + n[1] + n[2];
+          const double s = ((deg / 2) & 1) ? -1.0 : 1.0;
+          acc[kk] += s * w * ipow(kv[0], n[0]) * ipow(kv[1], n[1]) * ipow(kv[2], n[2]);
+        }
+      }
+  for (int kk = 0; kk < K; kk++) G[(int64_t)(k0 + kk) * CK + q] = (float)acc[kk];
+}
+
+double factd(int n) {
+  double r = 1.0;
+  for (int i = 2; i <= n; i++) r *= i;
+  return r;
+}
+
+template <int P>
+int launch_p2m(ct2g_ctx *ctx) {
+  const unsigned T = 128;
+  p2m_kernel<P><<<ct2g_div_up(ctx->C, T), T, 0, ctx->stream>>>(
+      ctx->x, ctx->y, ctx->z, ctx->cell_start, ctx->mbits, ctx->C, ctx->grid);
+  CT2G_LAUNCHED(ctx);
+  return CT2G_OK;
+}
+
+template <int P>
+int launch_mg2l(ct2g_ctx *ctx) {
+  const unsigned T = 128;
+  mg2l_kernel<P><<<ct2g_div_up(ctx->CK, T), T, 0, ctx->stream>>>(ctx->spec, ctx->greens,
+                                                                  ctx->CK);
+  CT2G_LAUNCHED(ctx);
+  return CT2G_OK;
+}
+
+}  // namespace
+
+// Green's-table Ewald split (box units), as in the CPU oracle
+static const double kGreensAlpha = 12.0;
+static const int kGreensKmax = 36;
+
+int ct2g_build_greens(ct2g_ctx *ctx) {
+  if (ctx->greens_valid) return CT2G_OK;
+  const int p = ctx->p, nc = ctx->nc, M = ctx->M;
+  // D^n term tables and multi-indices
+  std::vector<DTerm> terms((size_t)nc * kMaxTerms);
+  std::vector<int> nterms(nc), mi(3 * nc);
+  {
+    int k = 0;
+    for (int d = 0; d <= p; d++)
+      for (int a = d; a >= 0; a--)
+        for (int b = d - a; b >= 0; b--) {
+          int n[3] = {a, b, d - a - b};
+          mi[3 * k] = n[0];
+          mi[3 * k + 1] = n[1];
+          mi[3 * k + 2] = n[2];
+          int t = 0;
+          for (int mx = 0; 2 * mx <= n[0]; mx++)
+            for (int my = 0; 2 * my <= n[1]; my++)
+              for (int mz = 0; 2 * mz <= n[2]; mz++) {
+                int m[3] = {mx, my, mz};
+                double c = 1.0;
+                for (int q = 0; q < 3; q++)
+                  c *= factd(n[q]) / (factd(m[q]) * factd(n[q] - 2 * m[q]));
+                c /= (double)(1 << (mx + my + mz));
+                DTerm &dt = terms[(size_t)k * kMaxTerms + t];
+                dt.mx = n[0] - 2 * mx;
+                dt.my = n[1] - 2 * my;
+                dt.mz = n[2] - 2 * mz;
+                dt.j = d - mx - my - mz;
+                dt.coef = c;
+                t++;
+              }
+          nterms[k] = t;
+          k++;
+        }
+  }
+  DTerm *d_terms = nullptr;
+  int *d_nterms = nullptr, *d_mi = nullptr;
+  double *rs = nullptr;
+  double2 *sp = nullptr;
+  int rc = CT2G_OK;
+  const int K = std::min(nc, M >= 512 ? 2 : (M >= 256 ? 8 : 16));
+  auto cleanup = [&]() {
+    cudaStreamSynchronize(ctx->stream);
+    if (d_terms) cudaFree(d_terms);
+    if (d_nterms) cudaFree(d_nterms);
+    if (d_mi) cudaFree(d_mi);
+    if (rs) cudaFree(rs);
+    if (sp) cudaFree(sp);
+  };
+  do {
+    cudaError_t e;
+    if ((e = cudaMalloc(&d_terms, sizeof(DTerm) * terms.size())) != cudaSuccess ||
+        (e = cudaMalloc(&d_nterms, sizeof(int) * nc)) != cudaSuccess ||
+        (e = cudaMalloc(&d_mi, sizeof(int) * 3 * nc)) != cudaSuccess ||
+        (e = cudaMalloc(&rs, sizeof(double) * (size_t)K * ctx->C)) != cudaSuccess ||
+        (e = cudaMalloc(&sp, sizeof(double2) * (size_t)K * ctx->CK)) != cudaSuccess) {
+      rc = ct2g_cuda_fail(ctx, e, "greens scratch allocation");
+      break;
+    }
+    cudaMemcpyAsync(d_terms, terms.data(), sizeof(DTerm) * terms.size(), cudaMemcpyHostToDevice,
+                    ctx->stream);
+    cudaMemcpyAsync(d_nterms, nterms.data(), sizeof(int) * nc, cudaMemcpyHostToDevice,
+                    ctx->stream);
+    cudaMemcpyAsync(d_mi, mi.data(), sizeof(int) * 3 * nc, cudaMemcpyHostToDevice, ctx->stream);
+    const double soft = ctx->opt.hsoft;
+    const double bw2 = (double)ctx->opt.bwidth * (double)ctx->opt.bwidth;
+    for (int k0 = 0; k0 < nc && rc == CT2G_OK; k0 += K) {
+      const int kk = std::min(K, nc - k0);
+      greens_real_kernel<<<ct2g_div_up(ctx->C, 128), 128, 0, ctx->stream>>>(
+          ctx->mbits, p, ctx->opt.kernel, soft, bw2, kGreensAlpha, d_terms, d_nterms, k0, kk,
+          rs);
+      ctx->launches++;
+      if ((e = cudaGetLastError()) != cudaSuccess) {
+        rc = ct2g_cuda_fail(ctx, e, "greens_real_kernel");
+        break;
+      }
+      rc = ct2g_fft_r2c_f64(ctx, rs, sp, M, kk);
+      if (rc != CT2G_OK) break;
+      greens_finish_kernel<<<ct2g_div_up(ctx->CK, 128), 128, 0, ctx->stream>>>(
+          ctx->mbits, p, kGreensAlpha, kGreensKmax, d_mi, k0, kk, sp, ctx->greens);
+      ctx->launches++;
+      if ((e = cudaGetLastError()) != cudaSuccess) {
+        rc = ct2g_cuda_fail(ctx, e, "greens_finish_kernel");
+        break;
+      }
+    }
+  } while (0);
+  cleanup();
+  if (rc == CT2G_OK) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return ct2g_cuda_fail(ctx, e, "greens build");
+    ctx->greens_valid = true;
+  }
+  return rc;
+}
+
+int ct2g_p2m(ct2g_ctx *ctx) {
+  switch (ctx->p) {
+    case 1: return launch_p2m<1>(ctx);
+    case 2: return launch_p2m<2>(ctx);
+    case 3: return launch_p2m<3>(ctx);
+    case 4: return launch_p2m<4>(ctx);
+    case 5: return launch_p2m<5>(ctx);
+    case 6: return launch_p2m<6>(ctx);
+  }
+  return ct2g_fail(ctx, CT2G_EINVAL, "unsupported order");
+}
+
+// forward FFT of the moment grids, MG2L, inverse FFT into the expansions
+// (which overwrite the moments in ctx->grid)
+int ct2g_mesh_solve(ct2g_ctx *ctx) {
+  CT2G_TRY(ct2g_build_greens(ctx));
+  cudaEventRecord(ctx->ev[2], ctx->stream);
+  CT2G_TRY(ct2g_fft_r2c_f32(ctx, ctx->grid, ctx->spec, ctx->M, ctx->nc));
+  cudaEventRecord(ctx->ev[3], ctx->stream);
+  switch (ctx->p) {
+    case 1: CT2G_TRY(launch_mg2l<1>(ctx)); break;
+    case 2: CT2G_TRY(launch_mg2l<2>(ctx)); break;
+    case 3: CT2G_TRY(launch_mg2l<3>(ctx)); break;
+    case 4: CT2G_TRY(launch_mg2l<4>(ctx)); break;
+    case 5: CT2G_TRY(launch_mg2l<5>(ctx)); break;
+    case 6: CT2G_TRY(launch_mg2l<6>(ctx)); break;
+    default: return ct2g_fail(ctx, CT2G_EINVAL, "unsupported order");
+  }
+  cudaEventRecord(ctx->ev[4], ctx->stream);
+  CT2G_TRY(ct2g_fft_c2r_f32(ctx, ctx->spec, ctx->grid, ctx->M, ctx->nc));
+  cudaEventRecord(ctx->ev[5], ctx->stream);
+  return CT2G_OK;
+}

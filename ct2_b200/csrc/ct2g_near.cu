@@ -1,0 +1,267 @@
+// Forces, kick update and drift.
+//
+//   forces  L2P far field + direct-sum near field per sink chunk
+//           (kick_cell, src/kick.cpp:3-74): one warp per chunk of <= 32
+//           sinks of one cell; every source of each stencil cell is a
+//           warp-uniform (broadcast) load of a float4 offset from its cell
+//           centre, so the inner loop is 3 FADD + 3 FFMA + RSQRT + 2 FMUL +
+//           3 FFMA per interaction in FP32.
+//   update  velocity + rung update (src/kick.cpp:75-99), FP64 arithmetic,
+//           stored FP32; ceil(log2(t0/dt)) taken exactly from the exponent bits
+//   drift   x += fixed32(v * dt/scale) (src/drift.cpp:4-18)
+//
+// Defects of the reference fixed here: the source loop advanced by one but
+// loaded eight sources (kick.cpp:38-43), the near-field force was reduced
+// from the far-field accumulator (kick.cpp:72), and the update indexed the
+// SIMD lane with the absolute particle index (kick.cpp:82-98).
+#include "ct2g_internal.cuh"
+
+namespace {
+
+__constant__ int c_stencil[4 * 729];  // (ox, oy, oz, unused) per offset
+
+template <int P>
+__device__ __forceinline__ void l2p(const float *__restrict__ grid, int64_t C, int64_t cell,
+                                    float tx, float ty, float tz, float &fx, float &fy,
+                                    float &fz, float &pot) {
+  constexpr MiTable<P> T{};
+  constexpr int NC = MiTable<P>::NC;
+  float L[NC];
+#pragma unroll
+  for (int k = 0; k < NC; k++) L[k] = __ldg(grid + (int64_t)k * C + cell);
+  float px[P + 1], py[P + 1], pz[P + 1];
+  px[0] = py[0] = pz[0] = 1.f;
+#pragma unroll
+  for (int q = 1; q <= P; q++) {
+    px[q] = px[q - 1] * tx * (1.f / q);
+    py[q] = py[q - 1] * ty * (1.f / q);
+    pz[q] = pz[q - 1] * tz * (1.f / q);
+  }
+  float ax = 0.f, ay = 0.f, az = 0.f, ph = 0.f;
+#pragma unroll
+  for (int k = 0; k < NC; k++) {
+    const float mono = px[T.nx[k]] * py[T.ny[k]] * pz[T.nz[k]];
+    ph = fmaf(-L[k], mono, ph);
+    if (T.deg[k] < P) {
+      ax = fmaf(L[ct2g_mi_index(T.nx[k] + 1, T.ny[k], T.nz[k])], mono, ax);
+      ay = fmaf(L[ct2g_mi_index(T.nx[k], T.ny[k] + 1, T.nz[k])], mono, ay);
+      az = fmaf(L[ct2g_mi_index(T.nx[k], T.ny[k], T.nz[k] + 1)], mono, az);
+    }
+  }
+  fx = ax;
+  fy = ay;
+  fz = az;
+  pot = ph;
+}
+
+template <int P, int KERNEL, bool POT>
+__global__ void __launch_bounds__(256) forces_kernel(
+    const uint32_t *__restrict__ chunk_begin, uint32_t nchunks, const uint32_t *__restrict__ cs,
+    const uint32_t *__restrict__ skeys, uint32_t rbegin, const float4 *__restrict__ src,
+    const float *__restrict__ grid, int mbits, int nstencil, float soft, float GM,
+    float *__restrict__ ofx, float *__restrict__ ofy, float *__restrict__ ofz,
+    float *__restrict__ opot, unsigned long long *__restrict__ inter) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t ch = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (ch >= nchunks) return;
+  const int M = 1 << mbits;
+  const int64_t C = (int64_t)M * M * M;
+  const uint32_t b = chunk_begin[ch];
+  const uint32_t key = skeys[b - rbegin];  // Morton key of the sink cell
+  const uint32_t cend = min(cs[key + 1], b + 32u);
+  const uint32_t i = b + lane;
+  const bool act = i < cend;
+  const float4 si = src[act ? i : b];
+  const int cx = (int)ct2g_compact3(key >> 2), cy = (int)ct2g_compact3(key >> 1),
+            cz = (int)ct2g_compact3(key);
+  const int64_t cell = ((int64_t)cx * M + cy) * M + cz;  // row-major grid index
+  float fx = 0.f, fy = 0.f, fz = 0.f, ph = 0.f;
+  if (P > 0) l2p<P>(grid, C, cell, si.x, si.y, si.z, fx, fy, fz, ph);
+  const float hc = 1.0f / (float)M;
+  const float h2 = soft * soft, hinv = 1.f / soft, hinv3 = hinv * hinv * hinv;
+  float nx = 0.f, ny = 0.f, nz = 0.f, np = 0.f;
+  uint32_t nsrc = 0;
+  for (int s = 0; s < nstencil; s++) {
+    const int ox = c_stencil[4 * s], oy = c_stencil[4 * s + 1], oz = c_stencil[4 * s + 2];
+    const uint32_t nb = ct2g_morton((uint32_t)((cx + ox) & (M - 1)),
+                                    (uint32_t)((cy + oy) & (M - 1)),
+                                    (uint32_t)((cz + oz) & (M - 1)));
+    const uint32_t j0 = cs[nb], j1 = cs[nb + 1];
+    nsrc += j1 - j0;
+    // sink position relative to the neighbour cell's centre
+    const float xs = si.x - (float)ox * hc, ys = si.y - (float)oy * hc,
+                zs = si.z - (float)oz * hc;
+    for (uint32_t j = j0; j < j1; j++) {
+      const float4 q = __ldg(src + j);
+      const float dx = xs - q.x, dy = ys - q.y, dz = zs - q.z;
+      const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+      float g;
+      if (KERNEL == CT2G_SOFT_PLUMMER) {
+        const float ri = rsqrtf(r2 + h2);
+        g = ri * ri * ri;
+        if (POT) np -= ri;
+      } else {
+        if (r2 < h2) {
+          g = hinv3;
+          if (POT) np -= 1.5f * hinv - 0.5f * r2 * hinv3;
+        } else {
+          const float ri = rsqrtf(r2);
+          g = ri * ri * ri;
+          if (POT) np -= ri;
+        }
+      }
+      nx = fmaf(-dx, g, nx);
+      ny = fmaf(-dy, g, ny);
+      nz = fmaf(-dz, g, nz);
+    }
+  }
+  if (act) {
+    ofx[i] = GM * (fx + nx);
+    ofy[i] = GM * (fy + ny);
+    ofz[i] = GM * (fz + nz);
+    if (POT) opot[i] = GM * (ph + np);
+  }
+  if (lane == 0 && inter) atomicAdd(inter, (unsigned long long)(cend - b) * nsrc);
+}
+
+__device__ __forceinline__ int ceil_log2_exact(float v) {
+  // exact ceil(log2(v)) for finite normal v > 0
+  const uint32_t u = __float_as_uint(v);
+  const int e = (int)((u >> 23) & 255u) - 127;
+  return (u & 0x7fffffu) ? e + 1 : e;
+}
+
+__global__ void update_kernel(size_t begin, size_t end, const float *__restrict__ fx,
+                              const float *__restrict__ fy, const float *__restrict__ fz,
+                              float *__restrict__ vx, float *__restrict__ vy,
+                              float *__restrict__ vz, int8_t *__restrict__ rung,
+                              ct2g_kick_params p, float hsoft, int *__restrict__ maxrung) {
+  const size_t i = begin + (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int mr = 0;
+  if (i < end) {
+    const float f[3] = {fx[i], fy[i], fz[i]};
+    double v[3] = {vx[i], vy[i], vz[i]};
+    const double sgn = p.top ? 1.0 : -1.0;
+    const float dth = __fdiv_rn(__fmul_rn(0.5f, p.t0), (float)(1 << p.rung));
+    if (p.ascending && !p.first) {
+#pragma unroll
+      for (int d = 0; d < 3; d++) v[d] = __dadd_rn(v[d], __dmul_rn(__dmul_rn(sgn, (double)f[d]), (double)dth));
+    }
+    if (p.descending) {
+      float g2 = __fmul_rn(f[0], f[0]);
+      g2 = __fadd_rn(g2, __fmul_rn(f[1], f[1]));
+      g2 = __fadd_rn(g2, __fmul_rn(f[2], f[2]));
+      float dt = fminf(__fmul_rn(p.eta, __fsqrt_rn(__fdiv_rn(__fmul_rn(p.scale, hsoft),
+                                                              __fsqrt_rn(g2)))),
+                       p.t0);
+      dt = fminf(p.max_dt, dt);
+      int r = rung[i];
+      int up = (ceil_log2_exact(__fdiv_rn(p.t0, dt)) > p.rung) ? 1 : 0;
+      int nr = max(p.rung + up, r - 1);
+      rung[i] = (int8_t)nr;
+      mr = nr;
+#pragma unroll
+      for (int d = 0; d < 3; d++) v[d] = __dadd_rn(v[d], __dmul_rn(__dmul_rn(sgn, (double)f[d]), (double)dth));
+    }
+    vx[i] = (float)v[0];
+    vy[i] = (float)v[1];
+    vz[i] = (float)v[2];
+  }
+  // block max -> global
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mr = max(mr, __shfl_xor_sync(0xffffffffu, mr, o));
+  if ((threadIdx.x & 31) == 0 && mr > 0) atomicMax(maxrung, mr);
+}
+
+__global__ void drift_kernel(size_t n, uint32_t *__restrict__ x, uint32_t *__restrict__ y,
+                             uint32_t *__restrict__ z, const float *__restrict__ vx,
+                             const float *__restrict__ vy, const float *__restrict__ vz,
+                             float lambda) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float two32 = 4294967296.0f;
+  x[i] += (uint32_t)__float2ll_rz(__fmul_rn(__fmul_rn(vx[i], lambda), two32));
+  y[i] += (uint32_t)__float2ll_rz(__fmul_rn(__fmul_rn(vy[i], lambda), two32));
+  z[i] += (uint32_t)__float2ll_rz(__fmul_rn(__fmul_rn(vz[i], lambda), two32));
+}
+
+template <int P, int K, bool POT>
+int launch_forces_t(ct2g_ctx *ctx) {
+  const unsigned T = 256;
+  const size_t threads = (size_t)ctx->nchunks * 32;
+  forces_kernel<P, K, POT><<<ct2g_div_up(threads, T), T, 0, ctx->stream>>>(
+      ctx->chunk_begin, ctx->nchunks, ctx->cell_start, ctx->keys, (uint32_t)ctx->rung_begin,
+      ctx->src, ctx->grid, ctx->mbits, ctx->nstencil, ctx->opt.hsoft, ctx->opt.GM, ctx->fx,
+      ctx->fy, ctx->fz, ctx->pot, ctx->d_inter);
+  CT2G_LAUNCHED(ctx);
+  return CT2G_OK;
+}
+
+template <int P>
+int launch_forces_p(ct2g_ctx *ctx) {
+  if (ctx->opt.kernel == CT2G_SOFT_SPHERE) return launch_forces_t<P, CT2G_SOFT_SPHERE, true>(ctx);
+  return launch_forces_t<P, CT2G_SOFT_PLUMMER, true>(ctx);
+}
+
+}  // namespace
+
+int ct2g_upload_stencil(ct2g_ctx *ctx, const std::vector<int> &st4) {
+  CT2G_CUDA(ctx, cudaMemcpyToSymbolAsync(c_stencil, st4.data(), sizeof(int) * st4.size(), 0,
+                                         cudaMemcpyHostToDevice, ctx->stream));
+  return CT2G_OK;
+}
+
+int ct2g_forces(ct2g_ctx *ctx) {
+  const size_t n = ctx->n;
+  // entries outside the range read as zero
+  CT2G_CUDA(ctx, cudaMemsetAsync(ctx->fx, 0, n * 4, ctx->stream));
+  CT2G_CUDA(ctx, cudaMemsetAsync(ctx->fy, 0, n * 4, ctx->stream));
+  CT2G_CUDA(ctx, cudaMemsetAsync(ctx->fz, 0, n * 4, ctx->stream));
+  CT2G_CUDA(ctx, cudaMemsetAsync(ctx->pot, 0, n * 4, ctx->stream));
+  CT2G_CUDA(ctx, cudaMemsetAsync(ctx->d_inter, 0, sizeof(unsigned long long), ctx->stream));
+  if (ctx->nchunks == 0) return CT2G_OK;
+  switch (ctx->p) {
+    case 1: return launch_forces_p<1>(ctx);
+    case 2: return launch_forces_p<2>(ctx);
+    case 3: return launch_forces_p<3>(ctx);
+    case 4: return launch_forces_p<4>(ctx);
+    case 5: return launch_forces_p<5>(ctx);
+    case 6: return launch_forces_p<6>(ctx);
+  }
+  return ct2g_fail(ctx, CT2G_EINVAL, "unsupported order");
+}
+
+int ct2g_update(ct2g_ctx *ctx, const ct2g_kick_params *p, int *max_rung, bool fuse_drift,
+                float drift_dt, float drift_scale) {
+  const size_t b = ctx->rung_begin, e = ctx->n;
+  CT2G_CUDA(ctx, cudaMemsetAsync(ctx->d_maxrung, 0, sizeof(int), ctx->stream));
+  if (e > b) {
+    update_kernel<<<ct2g_div_up(e - b, 256), 256, 0, ctx->stream>>>(
+        b, e, ctx->fx, ctx->fy, ctx->fz, ctx->vx, ctx->vy, ctx->vz, ctx->rung, *p,
+        ctx->opt.hsoft, ctx->d_maxrung);
+    CT2G_LAUNCHED(ctx);
+  }
+  if (fuse_drift) CT2G_TRY(ct2g_drift_all(ctx, drift_dt, drift_scale));
+  if (max_rung) {
+    CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->h_pinned, ctx->d_maxrung, sizeof(int),
+                                   cudaMemcpyDeviceToHost, ctx->stream));
+    CT2G_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    *max_rung = (int)ctx->h_pinned[0];
+  }
+  return CT2G_OK;
+}
+
+int ct2g_drift_all(ct2g_ctx *ctx, float dt, float scale) {
+  if (ctx->n == 0) return CT2G_OK;
+  const float lambda = dt / scale;
+  drift_kernel<<<ct2g_div_up(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->n, ctx->x, ctx->y, ctx->z,
+                                                                   ctx->vx, ctx->vy, ctx->vz,
+                                                                   lambda);
+  CT2G_LAUNCHED(ctx);
+  // positions changed: the cell structure is stale
+  ctx->grid_valid = false;
+  ctx->moments_valid = false;
+  ctx->expansions_valid = false;
+  ctx->forces_valid = false;
+  return CT2G_OK;
+}

@@ -1,0 +1,268 @@
+"""Python host layer over the ct2g C ABI, mirroring the reference's
+operator interface for the gravity step (dmarce1/ct2):
+
+  particle store   particle_allocate / SoA accessors (src/particle.cpp:273-288,
+                   cosmictiger/particle.hpp:22-56)  -> Gravity.upload / download
+  particle_to_grid (src/particle.cpp:349-362)      -> Gravity.particle_to_grid
+  particle_compute_multipoles / _expansions         -> compute_multipoles /
+                   (src/particle.cpp:180-271)          compute_expansions
+  kick(const kick_params&) (src/kick.cpp:105-125)   -> Gravity.kick
+  drift(float dt, float scale) (src/drift.cpp:4-18) -> Gravity.drift
+  kick_step(...) (src/main.cpp:8-92)                -> Gravity.kick_step
+  fft_r2c_3d / fft_c2r_3d (cosmictiger/fft.hpp:28-29) -> fft_r2c_3d / fft_c2r_3d
+
+Arrays are numpy; every call goes to libct2g.so on the GPU.  Errors raise
+CT2GError with the library's message (the reference aborts or has none).
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from ._lib import CT2GError, KickParams, Options
+
+
+def ncomp(p: int) -> int:
+    return (p + 1) * (p + 2) * (p + 3) // 6
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+@dataclass
+class kick_params:
+    """Field for field cosmictiger/kick.hpp:10-20."""
+    ascending: bool = True
+    descending: bool = True
+    top: bool = True
+    first: bool = False
+    rung: int = 0
+    t0: float = 1e-3
+    eta: float = 0.15
+    max_dt: float = 0.01
+    scale: float = 1.0
+
+    def _c(self):
+        return KickParams(int(self.ascending), int(self.descending), int(self.top),
+                          int(self.first), int(self.rung), self.t0, self.eta, self.max_dt,
+                          self.scale)
+
+
+class Gravity:
+    """One GPU context: particle store, mesh, Green's tensor, stream."""
+
+    def __init__(self, mesh=64, order=4, bwidth=3.0, hsoft=1.0 / 50.0, eta=0.15, GM=0.0,
+                 kernel=_lib.SOFT_PLUMMER, device=0, max_particles=0):
+        self._l = _lib.load()
+        o = Options()
+        self._l.ct2g_default_options(ctypes.byref(o))
+        o.mesh, o.order, o.bwidth, o.hsoft, o.eta, o.GM = mesh, order, bwidth, hsoft, eta, GM
+        o.kernel, o.device, o.max_particles = kernel, device, max_particles
+        h = ctypes.c_void_p()
+        rc = self._l.ct2g_create(ctypes.byref(o), ctypes.byref(h))
+        if rc != 0:
+            raise CT2GError(rc, "ct2g_create(mesh=%d, order=%d, bwidth=%g)" % (mesh, order, bwidth))
+        self._h = h
+        self.mesh, self.order, self.bwidth, self.kernel = mesh, order, bwidth, kernel
+        self.nc = ncomp(order)
+
+    # -- plumbing -----------------------------------------------------------
+    def _chk(self, rc):
+        if rc != 0:
+            raise CT2GError(rc, self._l.ct2g_last_error(self._h).decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._l.ct2g_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def options(self):
+        o = Options()
+        self._chk(self._l.ct2g_get_options(self._h, ctypes.byref(o)))
+        return o
+
+    def set_params(self, hsoft, eta, GM=0.0):
+        self._chk(self._l.ct2g_set_params(self._h, hsoft, eta, GM))
+
+    # -- particle store -----------------------------------------------------
+    def upload(self, x, y, z, vx, vy, vz, rung=None):
+        arrs = [np.ascontiguousarray(a, t) for a, t in
+                ((x, np.uint32), (y, np.uint32), (z, np.uint32), (vx, np.float32),
+                 (vy, np.float32), (vz, np.float32))]
+        r = None if rung is None else np.ascontiguousarray(rung, np.int8)
+        n = len(arrs[0])
+        self._chk(self._l.ct2g_upload_particles(self._h, *[_ptr(a) for a in arrs], _ptr(r), n))
+
+    def upload_dict(self, d):
+        self.upload(d["x"], d["y"], d["z"], d["vx"], d["vy"], d["vz"], d.get("rung"))
+
+    def count(self):
+        return int(self._l.ct2g_particle_count(self._h))
+
+    def download(self):
+        n = self.count()
+        out = dict(x=np.empty(n, np.uint32), y=np.empty(n, np.uint32), z=np.empty(n, np.uint32),
+                   vx=np.empty(n, np.float32), vy=np.empty(n, np.float32),
+                   vz=np.empty(n, np.float32), rung=np.empty(n, np.int8),
+                   id=np.empty(n, np.uint32))
+        self._chk(self._l.ct2g_download_particles(
+            self._h, *[_ptr(out[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "rung", "id")]))
+        return out
+
+    # -- stages -------------------------------------------------------------
+    def particle_to_grid(self):
+        self._chk(self._l.ct2g_particle_to_grid(self._h))
+
+    def cells(self):
+        """(begin, end) per row-major cell (i*mesh+j)*mesh+k."""
+        b = np.empty(self.mesh ** 3, np.int64)
+        e = np.empty(self.mesh ** 3, np.int64)
+        self._chk(self._l.ct2g_download_cells(self._h, _ptr(b), _ptr(e)))
+        return b, e
+
+    def compute_multipoles(self):
+        self._chk(self._l.ct2g_compute_multipoles(self._h))
+
+    def multipoles(self):
+        out = np.empty((self.nc, self.mesh, self.mesh, self.mesh), np.float32)
+        self._chk(self._l.ct2g_download_multipoles(self._h, _ptr(out)))
+        return out
+
+    def compute_expansions(self):
+        self._chk(self._l.ct2g_compute_expansions(self._h))
+
+    def expansions(self):
+        out = np.empty((self.nc, self.mesh, self.mesh, self.mesh), np.float32)
+        self._chk(self._l.ct2g_download_expansions(self._h, _ptr(out)))
+        return out
+
+    def greens(self):
+        m = self.mesh
+        out = np.empty((self.nc, m, m, m // 2 + 1), np.float32)
+        self._chk(self._l.ct2g_download_greens(self._h, _ptr(out)))
+        return out
+
+    def compute_forces(self):
+        self._chk(self._l.ct2g_compute_forces(self._h))
+
+    def forces(self):
+        n = self.count()
+        f = [np.empty(n, np.float32) for _ in range(4)]
+        self._chk(self._l.ct2g_download_forces(self._h, *[_ptr(a) for a in f]))
+        return np.stack(f[:3], 1), f[3]
+
+    def upload_forces(self, f):
+        f = np.asarray(f, np.float32)
+        cols = [np.ascontiguousarray(f[:, k]) for k in range(3)]
+        self._chk(self._l.ct2g_upload_forces(self._h, *[_ptr(c) for c in cols]))
+
+    def kick_update(self, params: kick_params) -> int:
+        mr = ctypes.c_int(0)
+        self._chk(self._l.ct2g_kick_update(self._h, ctypes.byref(params._c()), ctypes.byref(mr)))
+        return mr.value
+
+    def kick(self, params: kick_params) -> int:
+        """int kick(const kick_params&): returns the max rung."""
+        mr = ctypes.c_int(0)
+        self._chk(self._l.ct2g_kick(self._h, ctypes.byref(params._c()), ctypes.byref(mr)))
+        return mr.value
+
+    def drift(self, dt: float, scale: float):
+        self._chk(self._l.ct2g_drift(self._h, dt, scale))
+
+    def kick_step(self, minrung, max_rung, scale, adot, tau, t0, minrung0, nocrop=False):
+        """Returns (max_rung, minrung) -- the reference returns max_rung and
+        updates minrung through its reference argument."""
+        mr = ctypes.c_int(minrung)
+        out = ctypes.c_int(0)
+        self._chk(self._l.ct2g_kick_step(self._h, ctypes.byref(mr), max_rung, scale, adot, tau,
+                                         t0, minrung0, int(nocrop), ctypes.byref(out)))
+        return out.value, mr.value
+
+    # rung bookkeeping
+    def sort_by_rung(self, minrung):
+        self._chk(self._l.ct2g_sort_by_rung(self._h, minrung))
+
+    def push_rungs(self):
+        self._chk(self._l.ct2g_push_rungs(self._h))
+
+    def pop_rungs(self):
+        self._chk(self._l.ct2g_pop_rungs(self._h))
+
+    def set_minrung(self, minrung):
+        self._chk(self._l.ct2g_set_minrung(self._h, minrung))
+
+    def current_range(self):
+        b, e = ctypes.c_size_t(), ctypes.c_size_t()
+        self._chk(self._l.ct2g_current_range(self._h, ctypes.byref(b), ctypes.byref(e)))
+        return b.value, e.value
+
+    def rung_counts(self):
+        c = np.zeros(128, np.uint64)
+        nr = ctypes.c_int(0)
+        self._chk(self._l.ct2g_rung_counts(self._h, _ptr(c), 128, ctypes.byref(nr)))
+        return c[:nr.value].astype(np.int64)
+
+    # -- FFT ----------------------------------------------------------------
+    def fft_r2c_3d(self, x):
+        """x: float64 [batch,]N,N,N -> split planes float64 [batch,] 2*N*N*(N/2+1)."""
+        x = np.ascontiguousarray(x, np.float64)
+        N = x.shape[-1]
+        b = 1 if x.ndim == 3 else x.shape[0]
+        out = np.empty((b, 2 * N * N * (N // 2 + 1)), np.float64)
+        self._chk(self._l.ct2g_fft_r2c_3d(self._h, _ptr(x), _ptr(out), N, b))
+        return out[0] if x.ndim == 3 else out
+
+    def fft_c2r_3d(self, y, N):
+        y = np.ascontiguousarray(y, np.float64)
+        b = 1 if y.ndim == 1 else y.shape[0]
+        out = np.empty((b, N, N, N), np.float64)
+        self._chk(self._l.ct2g_fft_c2r_3d(self._h, _ptr(y), _ptr(out), N, b))
+        return out[0] if y.ndim == 1 else out
+
+    # -- diagnostics --------------------------------------------------------
+    def ewald_direct(self, sx, sy, sz, alpha=10.5, rcut=0.5, kmax=20, with_pot=False):
+        sx, sy, sz = (np.ascontiguousarray(a, np.uint32) for a in (sx, sy, sz))
+        ns = len(sx)
+        f = np.empty((ns, 3), np.float64)
+        pot = np.empty(ns, np.float64) if with_pot else None
+        self._chk(self._l.ct2g_ewald_direct(self._h, _ptr(sx), _ptr(sy), _ptr(sz), ns, alpha,
+                                            rcut, kmax, _ptr(f), _ptr(pot)))
+        return (f, pot) if with_pot else f
+
+    def stage_times(self):
+        t = np.zeros(7, np.float32)
+        self._chk(self._l.ct2g_stage_times(self._h, _ptr(t), 7))
+        return t
+
+    def synchronize(self):
+        self._chk(self._l.ct2g_synchronize(self._h))
+
+    def stream(self):
+        return self._l.ct2g_stream(self._h)
+
+    def launch_count(self):
+        return int(self._l.ct2g_launch_count(self._h))
+
+    def interaction_count(self):
+        return int(self._l.ct2g_interaction_count(self._h))

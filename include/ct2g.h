@@ -1,0 +1,211 @@
+/*
+ * ct2g.h -- C ABI of the B200-native ct2 gravity step.
+ *
+ * Plain C types only (pointers, sizes, scalars); no torch or C++ types.  One
+ * context owns one GPU's particle store (SoA, resident in HBM), the mesh
+ * buffers, the cached Green's tensor and one CUDA stream.  A context is not
+ * thread-safe; separate contexts are independent.  Every entry point returns
+ * a status (CT2G_OK == 0) and ct2g_last_error() describes the last failure.
+ *
+ * Each declaration names the reference interface it replaces (dmarce1/ct2,
+ * file:line within that project).  The reference keeps its particles in
+ * process-global arrays (src/particle.cpp:17-25, cosmictiger/particle.hpp:22-56)
+ * mutated in place by particle_to_grid / kick / drift; here they live in the
+ * context and cross the boundary through ct2g_upload_* / ct2g_download_*.
+ * Like the reference, particle_to_grid leaves the store in cell order; the ids
+ * returned by ct2g_download_particles map it back to upload order.
+ */
+#ifndef CT2G_H_
+#define CT2G_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define CT2G_OK 0
+#define CT2G_EINVAL 1   /* bad argument or option                              */
+#define CT2G_ENOMEM 2   /* device allocation failed                            */
+#define CT2G_ECUDA 3    /* CUDA runtime error                                  */
+#define CT2G_ESTATE 4   /* call out of order (e.g. kick before particle_to_grid)*/
+#define CT2G_ETIMEOUT 5 /* a bounded device-side wait gave up                  */
+#define CT2G_ENODEV 6   /* no usable sm_100 device                             */
+
+/* softening kernels */
+#define CT2G_SOFT_PLUMMER 0 /* 1/sqrt(r^2+h^2) for every pair                      */
+#define CT2G_SOFT_SPHERE 1  /* the reference's compact uniform-sphere kernel,      */
+                            /* src/kick.cpp:52-60: Newtonian beyond r = h          */
+
+#define CT2G_MAX_ORDER 6
+
+/* Options: the fields of the reference's struct options read by the gravity
+ * step (cosmictiger/options.hpp:14-32; defaults src/options.cpp:50-62,88),
+ * plus the mesh / order / kernel choices the reference leaves to Ncell and to
+ * sfmm.  Ncell = cbrt(count/ppcell)+4 (src/particle.cpp:355) becomes an
+ * explicit power-of-two `mesh`; PORDER (cosmictiger/cosmictiger.hpp:16)
+ * becomes the runtime `order`. */
+typedef struct {
+  float bwidth;         /* direct-sum stencil: cell offsets |o|^2 <= bwidth^2      */
+  float hsoft;          /* softening length, box units                             */
+  float eta;            /* rung accuracy parameter                                 */
+  float GM;             /* G * particle mass; 0 -> 1/nparts at upload              */
+  int mesh;             /* cells per dimension: power of two, 8..512               */
+  int order;            /* multipole expansion order p, 1..CT2G_MAX_ORDER          */
+  int kernel;           /* CT2G_SOFT_*                                             */
+  int device;           /* CUDA device ordinal                                     */
+  size_t max_particles; /* capacity reserved at create (0: sized by first upload)  */
+} ct2g_options;
+
+/* kick parameters, field for field cosmictiger/kick.hpp:10-20 */
+typedef struct {
+  int ascending;
+  int descending;
+  int top;
+  int first;
+  int rung;
+  float t0;
+  float eta;
+  float max_dt;
+  float scale;
+} ct2g_kick_params;
+
+typedef struct ct2g_ctx ct2g_ctx;
+
+/* Reference defaults (src/options.cpp:50-62): bwidth 3, hsoft 1/50, eta 0.15;
+ * plus mesh 64, order 4, Plummer kernel, device 0. */
+void ct2g_default_options(ct2g_options *opt);
+
+/* Context lifetime; replaces the reference's process-global particle and
+ * option state (src/particle.cpp:17-25, src/options.cpp:14,36-42). */
+int ct2g_create(const ct2g_options *opt, ct2g_ctx **out);
+int ct2g_destroy(ct2g_ctx *ctx);
+const char *ct2g_last_error(const ct2g_ctx *ctx);
+const char *ct2g_status_string(int status);
+/* get_options() (cosmictiger/options.hpp:34) */
+int ct2g_get_options(const ct2g_ctx *ctx, ct2g_options *out);
+/* change hsoft / eta / GM without rebuilding (GM <= 0 keeps the current value) */
+int ct2g_set_params(ct2g_ctx *ctx, float hsoft, float eta, float GM);
+
+/* Particle store: replaces particle_allocate + particles_init + the SoA
+ * accessors (src/particle.cpp:273-288,364-374; cosmictiger/particle.hpp:22-56).
+ * Host pointers; rung may be NULL (all 0).  Assigns ids 0..n-1. */
+int ct2g_upload_particles(ct2g_ctx *ctx, const uint32_t *x, const uint32_t *y,
+                          const uint32_t *z, const float *vx, const float *vy,
+                          const float *vz, const int8_t *rung, size_t n);
+/* Host pointers; any may be NULL.  Current (cell-sorted) order. */
+int ct2g_download_particles(ct2g_ctx *ctx, uint32_t *x, uint32_t *y, uint32_t *z,
+                            float *vx, float *vy, float *vz, int8_t *rung,
+                            uint32_t *ids);
+/* particle_count() (src/particle.cpp:27) */
+size_t ct2g_particle_count(const ct2g_ctx *ctx);
+
+/* particle_to_grid() (src/particle.cpp:349-362; cosmictiger/particle.hpp:62):
+ * stable sort of the current range [rung_begin, n) by cell.  Each particle
+ * lands in the leaf the reference's bisection (particle.cpp:69-114) reaches,
+ * and the cells follow one another in the bisection's (Morton, x-major bit
+ * interleave) order; inside a cell the previous order is kept. */
+int ct2g_particle_to_grid(ct2g_ctx *ctx);
+/* particle_get_cell(i,j,k) (cosmictiger/particle.hpp:70) for every cell at
+ * once: host int64 [mesh^3] each, indexed (i*mesh+j)*mesh+k, absolute
+ * particle index ranges [begin, end). */
+int ct2g_download_cells(ct2g_ctx *ctx, int64_t *cell_begin, int64_t *cell_end);
+
+/* particle_compute_multipoles (src/particle.cpp:180-209): per-cell Cartesian
+ * moments about the cell centre, accumulated in FP64, stored FP32. */
+int ct2g_compute_multipoles(ct2g_ctx *ctx);
+/* host float[ncomp(order)][mesh^3] */
+int ct2g_download_multipoles(ct2g_ctx *ctx, float *out);
+
+/* particle_compute_expansions (src/particle.cpp:211-271): forward r2c FFT of
+ * every moment grid, Green's multiply (MG2L, particle.cpp:244-250) with the
+ * cached k-space Green's tensor (particle_greens, particle.cpp:116-178),
+ * inverse c2r FFT into per-cell local expansions. */
+int ct2g_compute_expansions(ct2g_ctx *ctx);
+/* host float[ncomp(order)][mesh^3]: particle_get_expansion
+ * (cosmictiger/particle.hpp:71) for every cell */
+int ct2g_download_expansions(ct2g_ctx *ctx, float *out);
+/* host float[ncomp(order)][mesh][mesh][mesh/2+1]: the k-space Green's tensor,
+ * normalised by 1/mesh^3; real part for even |n|, imaginary part for odd |n| */
+int ct2g_download_greens(ct2g_ctx *ctx, float *out);
+
+/* Forces of the current range (L2P far field + direct-sum near field,
+ * src/kick.cpp:19-74), without touching velocities. */
+int ct2g_compute_forces(ct2g_ctx *ctx);
+/* host float[n] each, current order; pot may be NULL.  Accelerations include
+ * GM.  Entries outside the current range are zero. */
+int ct2g_download_forces(ct2g_ctx *ctx, float *fx, float *fy, float *fz, float *pot);
+/* host float[n] each: replaces the force buffer (for update-only tests) */
+int ct2g_upload_forces(ct2g_ctx *ctx, const float *fx, const float *fy, const float *fz);
+/* velocity + rung update of kick_cell (src/kick.cpp:75-99) from the force
+ * buffer, over the current range; *max_rung receives the largest new rung */
+int ct2g_kick_update(ct2g_ctx *ctx, const ct2g_kick_params *p, int *max_rung);
+
+/* int kick(const kick_params&) (cosmictiger/kick.hpp:24, src/kick.cpp:105-125):
+ * forces + update over the current range; returns the max rung in *max_rung.
+ * Requires ct2g_particle_to_grid (and the mesh stages, which it runs if the
+ * expansions are stale). */
+int ct2g_kick(ct2g_ctx *ctx, const ct2g_kick_params *p, int *max_rung);
+
+/* void drift(float dt, float scale) (cosmictiger/drift.hpp:12,
+ * src/drift.cpp:4-18): x += fixed32(v * dt/scale) for every particle */
+int ct2g_drift(ct2g_ctx *ctx, float dt, float scale);
+
+/* int kick_step(int& minrung, int max_rung, double scale, double adot,
+ * double tau, double t0, int minrung0, bool nocrop) (cosmictiger/kick.hpp:23,
+ * src/main.cpp:8-92): the rung-hierarchical KDK step, GPU-resident.
+ * *minrung is updated like the reference's reference argument; the return
+ * value of the reference goes to *out_max_rung. */
+int ct2g_kick_step(ct2g_ctx *ctx, int *minrung, int max_rung, double scale, double adot,
+                   double tau, double t0, int minrung0, int nocrop, int *out_max_rung);
+
+/* Rung bookkeeping (src/particle.cpp:31-57,320-347). */
+int ct2g_sort_by_rung(ct2g_ctx *ctx, int minrung);        /* particle_sort_by_rung   */
+int ct2g_push_rungs(ct2g_ctx *ctx);                       /* particle_push_rungs     */
+int ct2g_pop_rungs(ct2g_ctx *ctx);                        /* particle_pop_rungs      */
+int ct2g_set_minrung(ct2g_ctx *ctx, int minrung);         /* particle_set_minrung    */
+int ct2g_current_range(ct2g_ctx *ctx, size_t *begin, size_t *end); /* particle_current_range */
+/* particle_rung_counts: counts[0..nmax) (host); *nrungs = highest rung + 1 */
+int ct2g_rung_counts(ct2g_ctx *ctx, size_t *counts, int nmax, int *nrungs);
+
+/* 3D FFTs, replacing fft_r2c_3d / fft_c2r_3d (cosmictiger/fft.hpp:28-29;
+ * src/fft/fft_r2c_3d.cpp, src/fft/fft_c2r_3d.cpp) in FP64 with the
+ * reference's split-plane halfcomplex layout (src/particle.cpp:220,236-237):
+ * xin[N^3] real, index (i*N+j)*N+k; xout[2*dimag], dimag = N*N*(N/2+1), real
+ * parts at [0,dimag) and imaginary parts at [dimag,2*dimag), index
+ * (i*N+j)*(N/2+1)+k.  Forward: X(q) = sum_r x(r) exp(-2 pi i q.r/N).
+ * c2r is the unnormalised inverse (c2r(r2c(x)) = N^3 x).  Host pointers;
+ * batch transforms of consecutive arrays.  N: power of two, 4..512. */
+int ct2g_fft_r2c_3d(ct2g_ctx *ctx, const double *xin, double *xout, int N, int batch);
+int ct2g_fft_c2r_3d(ct2g_ctx *ctx, const double *xin, double *xout, int N, int batch);
+/* FP32 device-pointer variant on the context stream, interleaved complex
+ * output (float2[batch][N][N][N/2+1]); dir = +1 forward r2c, -1 inverse c2r */
+int ct2g_fft3d_f32_dev(ct2g_ctx *ctx, int dir, void *d_real, void *d_complex, int N,
+                       int batch);
+
+/* FP64 Ewald direct sum over ALL particles of the context as sources, at the
+ * given sink positions (host, fixed32): the force truth.  f: host double[3*ns]
+ * (interleaved xyz), pot: host double[ns] or NULL.  Same kernel/softening/GM
+ * as the context. */
+int ct2g_ewald_direct(ct2g_ctx *ctx, const uint32_t *sx, const uint32_t *sy,
+                      const uint32_t *sz, size_t ns, double alpha, double rcut, int kmax,
+                      double *f, double *pot);
+
+/* Stream and timing helpers. */
+void *ct2g_stream(ct2g_ctx *ctx);   /* the context's cudaStream_t */
+int ct2g_synchronize(ct2g_ctx *ctx);
+/* Per-stage device times (ms) of the last ct2g_kick / ct2g_kick_step call:
+ * [0] bin, [1] P2M, [2] forward FFT, [3] MG2L, [4] inverse FFT, [5] forces,
+ * [6] kick update + drift.  n >= 7. */
+int ct2g_stage_times(ct2g_ctx *ctx, float *ms, int n);
+/* Number of kernel launches issued by this context since creation. */
+uint64_t ct2g_launch_count(const ct2g_ctx *ctx);
+/* Near-field pair interactions of the last force computation (exact count). */
+uint64_t ct2g_interaction_count(const ct2g_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CT2G_H_ */
