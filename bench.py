@@ -2,9 +2,10 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-A step is one kick+drift at rung 0 through the reference-facing kick_step
-entry point (bin -> P2M -> FFT -> Green's multiply -> IFFT -> L2P + direct sum
--> kick -> drift), on seeded synthetic particles resident in HBM.  Default
+A step is one kick+drift at rung 0 through the reference-facing entry points
+particle_to_grid -> kick -> drift (the first level of kick_step,
+src/main.cpp:49-82): bin -> P2M -> FFT -> Green's multiply -> IFFT -> L2P +
+direct sum -> kick -> drift, on seeded synthetic particles resident in HBM.  Default
 workload: 128^3 = 2,097,152 particles, 70% in 512 Plummer spheres (a = 0.005,
 log-uniform masses over 10x) plus 30% uniform, 256^3 mesh, Plummer softening
 eps = 1/(50*128), dt = 1e-3.
@@ -217,8 +218,16 @@ def main():
     g.upload_dict(P)
     stream = torch.cuda.ExternalStream(g.stream(), device=local)
 
+    from ct2_b200.gravity import kick_params
+    kp = kick_params(ascending=True, descending=True, top=True, first=False, rung=0,
+                     t0=args.dt, eta=0.15, max_dt=0.01, scale=1.0)
+
     def step():
-        return g.kick_step(0, 0, 1.0, 1.0, 1.0, args.dt, 0)
+        # one kick+drift at rung 0: the first level of kick_step
+        # (src/main.cpp:49-82): particle_to_grid, kick, drift
+        g.particle_to_grid()
+        g.kick(kp)
+        g.drift(args.dt, 1.0)
 
     # accuracy on the initial state: forces vs the FP64 Ewald direct sum
     g.particle_to_grid()

@@ -7,6 +7,7 @@
 #include "ct2g_internal.cuh"
 
 int ct2g_upload_stencil(ct2g_ctx *ctx, const std::vector<int> &st4);
+int ct2g_fft_init(ct2g_ctx *ctx);
 
 int ct2g_fail(ct2g_ctx *ctx, int code, const std::string &msg) {
   if (ctx) ctx->err = msg;
@@ -239,6 +240,7 @@ int ct2g_create(const ct2g_options *opt, ct2g_ctx **out) {
     if (cudaMalloc(&ctx->d_maxrung, sizeof(int)) != cudaSuccess ||
         cudaMalloc(&ctx->d_inter, sizeof(unsigned long long)) != cudaSuccess) { rc = CT2G_ENOMEM; break; }
     if ((rc = ct2g_alloc_mesh(ctx)) != CT2G_OK) break;
+    if ((rc = ct2g_fft_init(ctx)) != CT2G_OK) break;
     // near-field stencil: integer offsets |o|^2 <= bwidth^2 (the fixed form
     // of particle_cell_neighbors, src/particle.cpp:302-318)
     std::vector<int> st;
@@ -505,7 +507,7 @@ int ct2g_sort_by_rung(ct2g_ctx *ctx, int minrung) {
   rung_flag_kernel<<<G, T, 0, st>>>(ctx->rung, b, nr, minrung, ctx->flags);
   CT2G_LAUNCHED(ctx);
   uint32_t nlow = 0;
-  CT2G_TRY(ct2g_scan_exclusive(ctx, ctx->flags, ctx->vals2, nr, &nlow));
+  CT2G_TRY(ct2g_scan_exclusive(ctx, ctx->flags, ctx->vals2, nr, &nlow, 0));
   rung_scatter_kernel<<<G, T, 0, st>>>(ctx->flags, ctx->vals2, b, nr, nlow, ctx->vals);
   CT2G_LAUNCHED(ctx);
   permute_kernel<uint32_t><<<G, T, 0, st>>>(ctx->vals, b, nr, ctx->x, ctx->x2);

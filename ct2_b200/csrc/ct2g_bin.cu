@@ -80,7 +80,8 @@ __global__ void scan_single_kernel(uint32_t *__restrict__ a, size_t nb, uint32_t
 }
 
 __global__ void scan_apply_kernel(const uint32_t *__restrict__ in, size_t n,
-                                  const uint32_t *__restrict__ boff, uint32_t *__restrict__ out) {
+                                  const uint32_t *__restrict__ boff, uint32_t offset,
+                                  uint32_t *__restrict__ out) {
   __shared__ uint32_t sm[33];
   size_t base = (size_t)blockIdx.x * kScanTile + (size_t)threadIdx.x * kScanItems;
   uint32_t v[kScanItems];
@@ -91,7 +92,7 @@ __global__ void scan_apply_kernel(const uint32_t *__restrict__ in, size_t n,
     s += v[k];
   }
   uint32_t tot;
-  uint32_t ex = block_excl_scan(s, sm, tot) + boff[blockIdx.x];
+  uint32_t ex = block_excl_scan(s, sm, tot) + boff[blockIdx.x] + offset;
 #pragma unroll
   for (int k = 0; k < kScanItems; k++) {
     if (base + k < n) out[base + k] = ex;
@@ -190,15 +191,19 @@ __global__ void keys_kernel(const uint32_t *__restrict__ x, const uint32_t *__re
   vals[i] = (uint32_t)i;
 }
 
-// cell_start from sorted Morton keys: keys (key[i-1], key[i]] start at begin+i
-__global__ void cell_start_kernel(const uint32_t *__restrict__ skeys, size_t nr, size_t begin,
-                                  uint32_t C, uint32_t *__restrict__ cs) {
+// per-cell particle counts of the sorted range (cell_start = begin + their
+// exclusive scan)
+__global__ void cell_count_kernel(const uint32_t *__restrict__ skeys, size_t nr,
+                                  uint32_t *__restrict__ counts) {
   size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i > nr) return;
-  uint32_t lo = (i == 0) ? 0u : skeys[i - 1] + 1u;
-  uint32_t hi = (i == nr) ? C : skeys[i];
-  for (uint32_t c = lo; c <= hi && c < C + 1; c++) cs[c] = (uint32_t)(begin + i);
-  if (i == nr) cs[C] = (uint32_t)(begin + nr);
+  if (i >= nr) return;
+  const uint32_t k = skeys[i];
+  // one atomic per run of equal keys
+  if (i == 0 || skeys[i - 1] != k) {
+    size_t e = i + 1;
+    while (e < nr && skeys[e] == k) e++;
+    counts[k] = (uint32_t)(e - i);
+  }
 }
 
 // gather the active range into cell order; write the direct-sum source records
@@ -257,7 +262,7 @@ __global__ void chunk_fill_kernel(const uint32_t *__restrict__ flags,
 
 // exclusive scan of n uint32 values (in may equal out); optional host total
 int ct2g_scan_exclusive(ct2g_ctx *ctx, const uint32_t *in, uint32_t *out, size_t n,
-                        uint32_t *total_host) {
+                        uint32_t *total_host, uint32_t offset) {
   if (n == 0) {
     if (total_host) *total_host = 0;
     return CT2G_OK;
@@ -275,7 +280,7 @@ int ct2g_scan_exclusive(ct2g_ctx *ctx, const uint32_t *in, uint32_t *out, size_t
   CT2G_LAUNCHED(ctx);
   scan_single_kernel<<<1, 1024, 0, ctx->stream>>>(bsum, nb, bsum + nb);
   CT2G_LAUNCHED(ctx);
-  scan_apply_kernel<<<nb, kScanThreads, 0, ctx->stream>>>(in, n, bsum, out);
+  scan_apply_kernel<<<nb, kScanThreads, 0, ctx->stream>>>(in, n, bsum, offset, out);
   CT2G_LAUNCHED(ctx);
   if (total_host) {
     CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->h_pinned, bsum + nb, sizeof(uint32_t),
@@ -303,7 +308,7 @@ int ct2g_bin_range(ct2g_ctx *ctx) {
     for (int shift = 0; shift < bits; shift += 8) {
       radix_hist_kernel<<<ntiles, kRadixThreads, 0, st>>>(ka, nr, shift, ntiles, ctx->hist);
       CT2G_LAUNCHED(ctx);
-      CT2G_TRY(ct2g_scan_exclusive(ctx, ctx->hist, ctx->hist, (size_t)256 * ntiles, nullptr));
+      CT2G_TRY(ct2g_scan_exclusive(ctx, ctx->hist, ctx->hist, (size_t)256 * ntiles, nullptr, 0));
       radix_scatter_kernel<<<ntiles, kRadixThreads, 0, st>>>(ka, va, nr, shift, ntiles,
                                                              ctx->hist, kb, vb);
       CT2G_LAUNCHED(ctx);
@@ -323,9 +328,11 @@ int ct2g_bin_range(ct2g_ctx *ctx) {
       ctx->vals = va;
       ctx->vals2 = t;
     }
-    cell_start_kernel<<<ct2g_div_up(nr + 1, T), T, 0, st>>>(ctx->keys, nr, begin,
-                                                           (uint32_t)ctx->C, ctx->cell_start);
+    CT2G_CUDA(ctx, cudaMemsetAsync(ctx->cell_start, 0, sizeof(uint32_t) * (ctx->C + 1), st));
+    cell_count_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(ctx->keys, nr, ctx->cell_start);
     CT2G_LAUNCHED(ctx);
+    CT2G_TRY(ct2g_scan_exclusive(ctx, ctx->cell_start, ctx->cell_start, (size_t)ctx->C + 1,
+                                 nullptr, (uint32_t)begin));
     gather_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(
         ctx->vals, begin, nr, mbits, ctx->x, ctx->y, ctx->z, ctx->vx, ctx->vy, ctx->vz,
         ctx->rung, ctx->id, ctx->x2, ctx->y2, ctx->z2, ctx->vx2, ctx->vy2, ctx->vz2, ctx->rung2,
@@ -355,7 +362,7 @@ int ct2g_bin_range(ct2g_ctx *ctx) {
                                                         ctx->flags);
     CT2G_LAUNCHED(ctx);
     uint32_t total = 0;
-    CT2G_TRY(ct2g_scan_exclusive(ctx, ctx->flags, ctx->vals2, nr, &total));
+    CT2G_TRY(ct2g_scan_exclusive(ctx, ctx->flags, ctx->vals2, nr, &total, 0));
     chunk_fill_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(ctx->flags, ctx->vals2, begin, nr,
                                                         ctx->chunk_begin);
     CT2G_LAUNCHED(ctx);

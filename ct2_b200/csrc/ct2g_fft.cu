@@ -12,11 +12,16 @@
 //
 // Three passes, each one read and one write of the array:
 //   Z: r2c along the contiguous axis, two real lines packed as one complex line
-//   Y: complex FFT along j, tiles of W contiguous qk columns staged in smem
+//   Y: complex FFT along j, tiles of W contiguous qk columns
 //   X: complex FFT along i, tiles of W contiguous (qj,qk) columns
-// Each 1D transform is radix-2 decimation in time on bit-reversed input, the
-// order the reference's scramble() produces (src/fft/scramble.cpp:26-43),
-// computed in shared memory.
+// A tile is staged in shared memory with coalesced loads.  Each line of
+// N = R1*R2 points is transformed in two register stages (the "four-step"
+// factorisation): R1 threads each do an R2-point DFT in registers over a
+// stride-R1 subsequence, multiply by exp(-2 pi i n1 k2/N), and exchange
+// through shared memory; R2 threads each then do an R1-point DFT.  The
+// in-register DFTs are radix-2 decimation-in-frequency butterflies with
+// compile-time twiddles.  Row tiles pad one word pair every R1 points so both
+// exchange patterns are free of bank conflicts.
 #include "ct2g_internal.cuh"
 
 namespace {
@@ -25,6 +30,14 @@ template <typename T> struct Cplx;
 template <> struct Cplx<float> { using type = float2; };
 template <> struct Cplx<double> { using type = double2; };
 
+// exp(-2 pi i k/32), k < 32, set at context creation from host FP64 cos/sin
+__constant__ float2 c_w32f[32];
+__constant__ double2 c_w32d[32];
+
+template <typename C2> __device__ __forceinline__ C2 w32(int k);
+template <> __device__ __forceinline__ float2 w32<float2>(int k) { return c_w32f[k]; }
+template <> __device__ __forceinline__ double2 w32<double2>(int k) { return c_w32d[k]; }
+
 template <typename C2>
 __device__ __forceinline__ C2 cmul(C2 a, C2 b) {
   C2 r;
@@ -32,168 +45,248 @@ __device__ __forceinline__ C2 cmul(C2 a, C2 b) {
   r.y = a.x * b.y + a.y * b.x;
   return r;
 }
-
-// In-place radix-2 DIT on `nlines` lines of length N=2^logN held in smem,
-// element (l, r) at s[l*ls + r*es], input in bit-reversed order.  The
-// twiddles tw[k] = exp(-2 pi i k/N), k < N/2, are in smem.
 template <typename C2>
-__device__ __forceinline__ void smem_fft(C2 *s, int logN, int nlines, int ls, int es,
-                                         const C2 *tw, bool inv) {
-  const int N = 1 << logN, half = N >> 1;
-  const int total = nlines * half;
-  for (int lh = 0; lh < logN; lh++) {
-    const int h = 1 << lh;
-    const int tstep = logN - 1 - lh;  // twiddle index = pos << tstep
-    for (int b = threadIdx.x; b < total; b += blockDim.x) {
-      int j = b & (half - 1);
-      int l = b >> (logN - 1);
-      int pos = j & (h - 1);
-      int i0 = ((j >> lh) << (lh + 1)) + pos;
-      int i1 = i0 + h;
-      C2 w = tw[pos << tstep];
-      if (inv) w.y = -w.y;
-      C2 *p0 = s + l * ls + i0 * es;
-      C2 *p1 = s + l * ls + i1 * es;
-      C2 a = *p0;
-      C2 m = cmul(w, *p1);
-      C2 r0, r1;
-      r0.x = a.x + m.x;
-      r0.y = a.y + m.y;
-      r1.x = a.x - m.x;
-      r1.y = a.y - m.y;
-      *p0 = r0;
-      *p1 = r1;
+__device__ __forceinline__ C2 cadd(C2 a, C2 b) {
+  C2 r;
+  r.x = a.x + b.x;
+  r.y = a.y + b.y;
+  return r;
+}
+template <typename C2>
+__device__ __forceinline__ C2 csub(C2 a, C2 b) {
+  C2 r;
+  r.x = a.x - b.x;
+  r.y = a.y - b.y;
+  return r;
+}
+
+constexpr int ilog2c(int n) { return n <= 1 ? 0 : 1 + ilog2c(n / 2); }
+constexpr int brevc(int v, int bits) {
+  int r = 0;
+  for (int i = 0; i < bits; i++) r |= ((v >> i) & 1) << (bits - 1 - i);
+  return r;
+}
+
+// In-register R-point DFT (R <= 32), natural order in and out.
+// Radix-2 DIF: span h from R/2 down to 1, butterfly (a, b) ->
+// (a + b, (a - b) W_{2h}^j); the result lands in bit-reversed order and is
+// permuted back at compile time.
+template <int R, typename C2, bool INV>
+__device__ __forceinline__ void reg_dft(C2 (&v)[R]) {
+#pragma unroll
+  for (int h = R / 2; h >= 1; h >>= 1) {
+#pragma unroll
+    for (int blk = 0; blk < R; blk += 2 * h) {
+#pragma unroll
+      for (int j = 0; j < h; j++) {
+        const C2 a = v[blk + j], b = v[blk + j + h];
+        v[blk + j] = cadd(a, b);
+        C2 d = csub(a, b);
+        if (j != 0) {
+          C2 w = w32<C2>(j * (32 / (2 * h)));
+          if (INV) w.y = -w.y;
+          d = cmul(d, w);
+        }
+        v[blk + j + h] = d;
+      }
+    }
+  }
+  C2 t[R];
+#pragma unroll
+  for (int k = 0; k < R; k++) t[k] = v[brevc(k, ilog2c(R))];
+#pragma unroll
+  for (int k = 0; k < R; k++) v[k] = t[k];
+}
+
+// Line FFTs on smem lines.  Layout ROWS: element (l, r) at
+// l*(N + N/R1) + r + r/R1 (one pad every R1 points); layout COLS: element
+// (l, r) at r*W + l.
+template <int N, bool ROWS>
+struct LineLayout {
+  static constexpr int R2 = N >= 4 ? (1 << (ilog2c(N) / 2)) : 1;
+  static constexpr int R1 = N / R2;  // R1 >= R2
+  static constexpr int LS = N + N / R1;
+  __device__ __forceinline__ static int at(int l, int r, int W) {
+    return ROWS ? l * LS + r + r / R1 : r * W + l;
+  }
+};
+
+// Transform `nlines` lines (nlines*R1 and nlines*R2 jobs spread over the block).
+// stw: N twiddles exp(-2 pi i k/N) in smem.
+template <int N, bool ROWS, typename C2, bool INV>
+__device__ __forceinline__ void tile_fft(C2 *s, int nlines, int W, const C2 *stw) {
+  using LL = LineLayout<N, ROWS>;
+  constexpr int R1 = LL::R1, R2 = LL::R2;
+  // step 1: job (line, n1): R2-point DFT over r = n1 + R1*n2, twiddle.  The
+  // block has 256 threads.
+  for (int job = threadIdx.x; job < nlines * R1; job += blockDim.x) {
+    int l, n1;
+    if (ROWS) {
+      n1 = job % R1;
+      l = job / R1;
+    } else {
+      l = job % nlines;
+      n1 = job / nlines;
+    }
+    C2 v[R2];
+#pragma unroll
+    for (int n2 = 0; n2 < R2; n2++) v[n2] = s[LL::at(l, n1 + R1 * n2, W)];
+    reg_dft<R2, C2, INV>(v);
+#pragma unroll
+    for (int k2 = 1; k2 < R2; k2++) {
+      C2 w = stw[(n1 * k2) & (N - 1)];
+      if (INV) w.y = -w.y;
+      v[k2] = cmul(v[k2], w);
+    }
+    // Y[n1][k2] back into the slots just read (slot n1 + R1*k2)
+#pragma unroll
+    for (int k2 = 0; k2 < R2; k2++) s[LL::at(l, n1 + R1 * k2, W)] = v[k2];
+  }
+  __syncthreads();
+  // step 2: job (line, k2): R1-point DFT over n1 -> X[k2 + R2*k1].  Jobs go
+  // in rounds of whole lines (LW lines per round), so a round's writes never
+  // touch slots that a later round still has to read.
+  constexpr int LW = 256 / R2;
+  for (int l0 = 0; l0 < nlines; l0 += LW) {
+    int l, k2;
+    if (ROWS) {
+      k2 = threadIdx.x % R2;
+      l = l0 + threadIdx.x / R2;
+    } else {
+      l = l0 + threadIdx.x % LW;
+      k2 = threadIdx.x / LW;
+    }
+    const bool on = l < nlines;
+    C2 v[R1];
+    if (on) {
+#pragma unroll
+      for (int n1 = 0; n1 < R1; n1++) v[n1] = s[LL::at(l, n1 + R1 * k2, W)];
+      reg_dft<R1, C2, INV>(v);
+    }
+    __syncthreads();  // all reads of this round before any write
+    if (on) {
+#pragma unroll
+      for (int k1 = 0; k1 < R1; k1++) s[LL::at(l, k2 + R2 * k1, W)] = v[k1];
     }
     __syncthreads();
   }
 }
 
 template <typename C2>
-__device__ __forceinline__ void load_twiddles(C2 *stw, const C2 *tw, int half) {
-  for (int k = threadIdx.x; k < half; k += blockDim.x) stw[k] = tw[k];
-}
-
-__device__ __forceinline__ int bitrev(int j, int logN) {
-  return (int)(__brev((unsigned)j) >> (32 - logN));
+__device__ __forceinline__ void load_twiddles(C2 *stw, const C2 *tw, int n) {
+  for (int k = threadIdx.x; k < n; k += blockDim.x) stw[k] = tw[k];
 }
 
 // ---- pass Z forward: pairs of real lines -> half spectra -------------------
-// lines: total number of real lines (even); LP complex (packed) lines per block
-template <typename T>
-__global__ void fftz_r2c_kernel(const T *__restrict__ in, typename Cplx<T>::type *__restrict__ out,
-                                int logN, size_t npairs, int LP,
-                                const typename Cplx<T>::type *__restrict__ tw) {
+// LP complex (packed) lines per block; npairs = number of real-line pairs
+template <typename T, int N>
+__global__ void __launch_bounds__(256) fftz_r2c_kernel(const T *__restrict__ in,
+                                                       typename Cplx<T>::type *__restrict__ out,
+                                                       size_t npairs, int LP,
+                                                       const typename Cplx<T>::type *__restrict__ tw) {
   using C2 = typename Cplx<T>::type;
-  extern __shared__ unsigned char smraw[];
-  const int N = 1 << logN, NH = N / 2 + 1;
+  using LL = LineLayout<N, true>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  constexpr int NH = N / 2 + 1;
   C2 *stw = reinterpret_cast<C2 *>(smraw);
-  C2 *s = stw + N / 2;
-  const int ls = N + 1;  // padded line stride
-  load_twiddles(stw, tw, N / 2);
+  C2 *s = stw + N;
+  load_twiddles(stw, tw, N);
   const size_t pair0 = (size_t)blockIdx.x * LP;
   const int np = (int)min((size_t)LP, npairs - pair0);
+  const T *src = in + pair0 * 2 * N;
   for (int e = threadIdx.x; e < np * N; e += blockDim.x) {
-    int l = e >> logN, j = e & (N - 1);
-    size_t line = 2 * (pair0 + l);
+    const int l = e / N, r = e % N;
     C2 v;
-    v.x = in[line * N + j];
-    v.y = in[(line + 1) * N + j];
-    s[l * ls + bitrev(j, logN)] = v;
+    v.x = src[(size_t)(2 * l) * N + r];
+    v.y = src[(size_t)(2 * l + 1) * N + r];
+    s[LL::at(l, r, 0)] = v;
   }
   __syncthreads();
-  smem_fft(s, logN, np, ls, 1, stw, false);
+  tile_fft<N, true, C2, false>(s, np, 0, stw);
+  C2 *dst = out + pair0 * 2 * NH;
   for (int e = threadIdx.x; e < np * NH; e += blockDim.x) {
-    int l = e / NH, k = e - l * NH;
-    size_t line = 2 * (pair0 + l);
-    C2 zk = s[l * ls + (k & (N - 1))];
-    C2 zc = s[l * ls + ((N - k) & (N - 1))];
+    const int l = e / NH, k = e % NH;
+    const C2 zk = s[LL::at(l, k & (N - 1), 0)];
+    const C2 zc = s[LL::at(l, (N - k) & (N - 1), 0)];
     // A_k = (Z_k + conj Z_{N-k})/2, B_k = (Z_k - conj Z_{N-k})/(2i)
     C2 a, b;
     a.x = (T)0.5 * (zk.x + zc.x);
     a.y = (T)0.5 * (zk.y - zc.y);
     b.x = (T)0.5 * (zk.y + zc.y);
     b.y = (T)0.5 * (zc.x - zk.x);
-    out[line * NH + k] = a;
-    out[(line + 1) * NH + k] = b;
+    dst[(size_t)(2 * l) * NH + k] = a;
+    dst[(size_t)(2 * l + 1) * NH + k] = b;
   }
 }
 
 // ---- pass Z inverse: pairs of half spectra -> real lines --------------------
-template <typename T>
-__global__ void fftz_c2r_kernel(const typename Cplx<T>::type *__restrict__ in, T *__restrict__ out,
-                                int logN, size_t npairs, int LP,
-                                const typename Cplx<T>::type *__restrict__ tw) {
+template <typename T, int N>
+__global__ void __launch_bounds__(256) fftz_c2r_kernel(const typename Cplx<T>::type *__restrict__ in,
+                                                       T *__restrict__ out, size_t npairs, int LP,
+                                                       const typename Cplx<T>::type *__restrict__ tw) {
   using C2 = typename Cplx<T>::type;
-  extern __shared__ unsigned char smraw[];
-  const int N = 1 << logN, NH = N / 2 + 1;
+  using LL = LineLayout<N, true>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  constexpr int NH = N / 2 + 1;
   C2 *stw = reinterpret_cast<C2 *>(smraw);
-  C2 *s = stw + N / 2;
-  const int ls = N + 1;
-  load_twiddles(stw, tw, N / 2);
+  C2 *s = stw + N;
+  load_twiddles(stw, tw, N);
   const size_t pair0 = (size_t)blockIdx.x * LP;
   const int np = (int)min((size_t)LP, npairs - pair0);
+  const C2 *src = in + pair0 * 2 * NH;
   for (int e = threadIdx.x; e < np * N; e += blockDim.x) {
-    int l = e >> logN, k = e & (N - 1);
-    size_t line = 2 * (pair0 + l);
+    const int l = e / N, k = e % N;
     // Z_k = A_k + i B_k, with A_{N-k} = conj(A_k) for the upper half
     C2 a, b, z;
     if (k < NH) {
-      a = in[line * NH + k];
-      b = in[(line + 1) * NH + k];
+      a = src[(size_t)(2 * l) * NH + k];
+      b = src[(size_t)(2 * l + 1) * NH + k];
     } else {
-      a = in[line * NH + (N - k)];
-      b = in[(line + 1) * NH + (N - k)];
+      a = src[(size_t)(2 * l) * NH + (N - k)];
+      b = src[(size_t)(2 * l + 1) * NH + (N - k)];
       a.y = -a.y;
       b.y = -b.y;
     }
     z.x = a.x - b.y;
     z.y = a.y + b.x;
-    s[l * ls + bitrev(k, logN)] = z;
+    s[LL::at(l, k, 0)] = z;
   }
   __syncthreads();
-  smem_fft(s, logN, np, ls, 1, stw, true);
+  tile_fft<N, true, C2, true>(s, np, 0, stw);
+  T *dst = out + pair0 * 2 * N;
   for (int e = threadIdx.x; e < np * N; e += blockDim.x) {
-    int l = e >> logN, j = e & (N - 1);
-    size_t line = 2 * (pair0 + l);
-    C2 z = s[l * ls + j];
-    out[line * N + j] = z.x;
-    out[(line + 1) * N + j] = z.y;
+    const int l = e / N, r = e % N;
+    const C2 z = s[LL::at(l, r, 0)];
+    dst[(size_t)(2 * l) * N + r] = z.x;
+    dst[(size_t)(2 * l + 1) * N + r] = z.y;
   }
 }
 
 // ---- strided passes: FFT along rows for tiles of W contiguous columns -------
 // array: outer blocks of `ostride` elements; inside, rows of `rstride`; ncols
 // valid columns per row.  grid.x = nouter * ntiles.
-template <typename C2>
-__global__ void fft_cols_kernel(C2 *__restrict__ a, int logN, size_t nouter, size_t ostride,
-                                size_t rstride, size_t ncols, int W, int ntiles, bool inv,
-                                const C2 *__restrict__ tw) {
-  extern __shared__ unsigned char smraw[];
-  const int N = 1 << logN;
+template <typename C2, int N, bool INV>
+__global__ void __launch_bounds__(256) fft_cols_kernel(C2 *__restrict__ a, size_t ostride,
+                                                       size_t rstride, size_t ncols, int W,
+                                                       int ntiles, const C2 *__restrict__ tw) {
+  extern __shared__ __align__(16) unsigned char smraw[];
   C2 *stw = reinterpret_cast<C2 *>(smraw);
-  C2 *s = stw + N / 2;
-  load_twiddles(stw, tw, N / 2);
+  C2 *s = stw + N;
+  load_twiddles(stw, tw, N);
   const size_t outer = blockIdx.x / ntiles;
   const size_t col0 = (size_t)(blockIdx.x % ntiles) * W;
   const int wv = (int)min((size_t)W, ncols - col0);
   C2 *base = a + outer * ostride + col0;
-  const int logW = __ffs(W) - 1;
   for (int e = threadIdx.x; e < N * W; e += blockDim.x) {
-    int r = e >> logW, w = e & (W - 1);
-    if (w < wv) s[bitrev(r, logN) * W + w] = base[(size_t)r * rstride + w];
+    const int r = e / W, w = e % W;
+    if (w < wv) s[r * W + w] = base[(size_t)r * rstride + w];
   }
   __syncthreads();
-  smem_fft(s, logN, W, 1, W, stw, inv);
+  tile_fft<N, false, C2, INV>(s, W, W, stw);
   for (int e = threadIdx.x; e < N * W; e += blockDim.x) {
-    int r = e >> logW, w = e & (W - 1);
+    const int r = e / W, w = e % W;
     if (w < wv) base[(size_t)r * rstride + w] = s[r * W + w];
   }
-}
-
-int ilog2(int n) {
-  int l = 0;
-  while ((1 << l) < n) l++;
-  return l;
 }
 
 template <typename C2>
@@ -203,20 +296,19 @@ const float2 *twiddle_ptr<float2>(ct2g_ctx *ctx) { return ctx->tw32; }
 template <>
 const double2 *twiddle_ptr<double2>(ct2g_ctx *ctx) { return ctx->tw64; }
 
-template <typename T>
-int run_cols(ct2g_ctx *ctx, typename Cplx<T>::type *spec, int N, int batch, bool inv) {
+template <typename T, int N>
+int run_cols(ct2g_ctx *ctx, typename Cplx<T>::type *spec, int batch, bool inv) {
   using C2 = typename Cplx<T>::type;
-  const int logN = ilog2(N);
   const size_t NH = N / 2 + 1;
-  const int W = 16;
-  const size_t smem = sizeof(C2) * ((size_t)N / 2 + (size_t)N * W);
-  auto kern = fft_cols_kernel<C2>;
-  CT2G_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem));
+  const int W = std::max(16, 4096 / N);
+  const size_t smem = sizeof(C2) * ((size_t)N + (size_t)N * W);
+  auto kf = fft_cols_kernel<C2, N, false>;
+  auto ki = fft_cols_kernel<C2, N, true>;
+  CT2G_CUDA(ctx, cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CT2G_CUDA(ctx, cudaFuncSetAttribute(ki, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const C2 *tw = twiddle_ptr<C2>(ctx);
-  // X pass first on inverse, Y first on forward (order does not matter)
   for (int pass = 0; pass < 2; pass++) {
-    bool ypass = (pass == 0) != inv;
+    const bool ypass = (pass == 0) != inv;
     size_t nouter, ostride, rstride, ncols;
     if (ypass) {
       nouter = (size_t)batch * N;
@@ -229,53 +321,94 @@ int run_cols(ct2g_ctx *ctx, typename Cplx<T>::type *spec, int N, int batch, bool
       rstride = (size_t)N * NH;
       ncols = (size_t)N * NH;
     }
-    int ntiles = (int)((ncols + W - 1) / W);
-    size_t nblocks = nouter * ntiles;
-    kern<<<(unsigned)nblocks, 256, smem, ctx->stream>>>(spec, logN, nouter, ostride, rstride,
-                                                         ncols, W, ntiles, inv, tw);
+    const int ntiles = (int)((ncols + W - 1) / W);
+    const size_t nblocks = nouter * ntiles;
+    (inv ? ki : kf)<<<(unsigned)nblocks, 256, smem, ctx->stream>>>(spec, ostride, rstride, ncols,
+                                                                     W, ntiles, tw);
     CT2G_LAUNCHED(ctx);
   }
   return CT2G_OK;
 }
 
-template <typename T>
-int fft_r2c(ct2g_ctx *ctx, const T *in, typename Cplx<T>::type *out, int N, int batch) {
+template <typename T, int N>
+int fft_r2c_n(ct2g_ctx *ctx, const T *in, typename Cplx<T>::type *out, int batch) {
   using C2 = typename Cplx<T>::type;
-  CT2G_TRY(ct2g_twiddles(ctx, N));
-  const int logN = ilog2(N);
   const size_t npairs = (size_t)batch * N * N / 2;
-  const int LP = (int)std::max<size_t>(1, (size_t)8192 / N);
-  const size_t smem = sizeof(C2) * ((size_t)N / 2 + (size_t)LP * (N + 1));
-  auto kern = fftz_r2c_kernel<T>;
-  CT2G_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem));
-  kern<<<ct2g_div_up(npairs, LP), 256, smem, ctx->stream>>>(in, out, logN, npairs, LP,
+  const int LP = std::max(1, 4096 / N);
+  const size_t smem = sizeof(C2) * ((size_t)N + (size_t)LP * LineLayout<N, true>::LS);
+  auto kern = fftz_r2c_kernel<T, N>;
+  CT2G_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  kern<<<ct2g_div_up(npairs, LP), 256, smem, ctx->stream>>>(in, out, npairs, LP,
                                                             twiddle_ptr<C2>(ctx));
   CT2G_LAUNCHED(ctx);
-  return run_cols<T>(ctx, out, N, batch, false);
+  return run_cols<T, N>(ctx, out, batch, false);
 }
 
-template <typename T>
-int fft_c2r(ct2g_ctx *ctx, typename Cplx<T>::type *in, T *out, int N, int batch) {
+template <typename T, int N>
+int fft_c2r_n(ct2g_ctx *ctx, typename Cplx<T>::type *in, T *out, int batch) {
   using C2 = typename Cplx<T>::type;
-  CT2G_TRY(ct2g_twiddles(ctx, N));
-  CT2G_TRY(run_cols<T>(ctx, in, N, batch, true));
-  const int logN = ilog2(N);
+  CT2G_TRY((run_cols<T, N>(ctx, in, batch, true)));
   const size_t npairs = (size_t)batch * N * N / 2;
-  const int LP = (int)std::max<size_t>(1, (size_t)8192 / N);
-  const size_t smem = sizeof(C2) * ((size_t)N / 2 + (size_t)LP * (N + 1));
-  auto kern = fftz_c2r_kernel<T>;
-  CT2G_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem));
-  kern<<<ct2g_div_up(npairs, LP), 256, smem, ctx->stream>>>(in, out, logN, npairs, LP,
+  const int LP = std::max(1, 4096 / N);
+  const size_t smem = sizeof(C2) * ((size_t)N + (size_t)LP * LineLayout<N, true>::LS);
+  auto kern = fftz_c2r_kernel<T, N>;
+  CT2G_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  kern<<<ct2g_div_up(npairs, LP), 256, smem, ctx->stream>>>(in, out, npairs, LP,
                                                             twiddle_ptr<C2>(ctx));
   CT2G_LAUNCHED(ctx);
   return CT2G_OK;
 }
 
+template <typename T>
+int fft_r2c(ct2g_ctx *ctx, const T *in, typename Cplx<T>::type *out, int N, int batch) {
+  CT2G_TRY(ct2g_twiddles(ctx, N));
+  switch (N) {
+    case 4: return fft_r2c_n<T, 4>(ctx, in, out, batch);
+    case 8: return fft_r2c_n<T, 8>(ctx, in, out, batch);
+    case 16: return fft_r2c_n<T, 16>(ctx, in, out, batch);
+    case 32: return fft_r2c_n<T, 32>(ctx, in, out, batch);
+    case 64: return fft_r2c_n<T, 64>(ctx, in, out, batch);
+    case 128: return fft_r2c_n<T, 128>(ctx, in, out, batch);
+    case 256: return fft_r2c_n<T, 256>(ctx, in, out, batch);
+    case 512: return fft_r2c_n<T, 512>(ctx, in, out, batch);
+  }
+  return ct2g_fail(ctx, CT2G_EINVAL, "FFT size must be a power of two in [4, 512]");
+}
+
+template <typename T>
+int fft_c2r(ct2g_ctx *ctx, typename Cplx<T>::type *in, T *out, int N, int batch) {
+  CT2G_TRY(ct2g_twiddles(ctx, N));
+  switch (N) {
+    case 4: return fft_c2r_n<T, 4>(ctx, in, out, batch);
+    case 8: return fft_c2r_n<T, 8>(ctx, in, out, batch);
+    case 16: return fft_c2r_n<T, 16>(ctx, in, out, batch);
+    case 32: return fft_c2r_n<T, 32>(ctx, in, out, batch);
+    case 64: return fft_c2r_n<T, 64>(ctx, in, out, batch);
+    case 128: return fft_c2r_n<T, 128>(ctx, in, out, batch);
+    case 256: return fft_c2r_n<T, 256>(ctx, in, out, batch);
+    case 512: return fft_c2r_n<T, 512>(ctx, in, out, batch);
+  }
+  return ct2g_fail(ctx, CT2G_EINVAL, "FFT size must be a power of two in [4, 512]");
+}
+
 }  // namespace
 
-// twiddles exp(-2 pi i k/N), k < N/2, computed on the host in FP64
+// constant twiddles of the in-register DFTs, once per context (device)
+int ct2g_fft_init(ct2g_ctx *ctx) {
+  float2 wf[32];
+  double2 wd[32];
+  const double twopi = 6.283185307179586476925286766559;
+  for (int k = 0; k < 32; k++) {
+    const double a = -twopi * (double)k / 32.0;
+    wd[k] = make_double2(std::cos(a), std::sin(a));
+    wf[k] = make_float2((float)wd[k].x, (float)wd[k].y);
+  }
+  CT2G_CUDA(ctx, cudaMemcpyToSymbol(c_w32f, wf, sizeof(wf)));
+  CT2G_CUDA(ctx, cudaMemcpyToSymbol(c_w32d, wd, sizeof(wd)));
+  return CT2G_OK;
+}
+
+// twiddles exp(-2 pi i k/N), k < N, computed on the host in FP64
 int ct2g_twiddles(ct2g_ctx *ctx, int N) {
   if (ctx->tw_n == N) return CT2G_OK;
   if (ctx->tw32) cudaFree(ctx->tw32);
@@ -283,20 +416,19 @@ int ct2g_twiddles(ct2g_ctx *ctx, int N) {
   ctx->tw32 = nullptr;
   ctx->tw64 = nullptr;
   ctx->tw_n = 0;
-  const int h = N / 2;
-  std::vector<float2> t32(h);
-  std::vector<double2> t64(h);
+  std::vector<float2> t32(N);
+  std::vector<double2> t64(N);
   const double twopi = 6.283185307179586476925286766559;
-  for (int k = 0; k < h; k++) {
-    double a = -twopi * (double)k / (double)N;
+  for (int k = 0; k < N; k++) {
+    const double a = -twopi * (double)k / (double)N;
     t64[k] = make_double2(std::cos(a), std::sin(a));
     t32[k] = make_float2((float)t64[k].x, (float)t64[k].y);
   }
-  CT2G_CUDA(ctx, cudaMalloc(&ctx->tw32, sizeof(float2) * h));
-  CT2G_CUDA(ctx, cudaMalloc(&ctx->tw64, sizeof(double2) * h));
-  CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->tw32, t32.data(), sizeof(float2) * h,
+  CT2G_CUDA(ctx, cudaMalloc(&ctx->tw32, sizeof(float2) * N));
+  CT2G_CUDA(ctx, cudaMalloc(&ctx->tw64, sizeof(double2) * N));
+  CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->tw32, t32.data(), sizeof(float2) * N,
                                  cudaMemcpyHostToDevice, ctx->stream));
-  CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->tw64, t64.data(), sizeof(double2) * h,
+  CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->tw64, t64.data(), sizeof(double2) * N,
                                  cudaMemcpyHostToDevice, ctx->stream));
   CT2G_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   ctx->tw_n = N;

@@ -167,8 +167,9 @@ int ct2g_cuda_fail(ct2g_ctx *ctx, cudaError_t e, const char *what);
 // ---------------------------------------------------------------------------
 int ct2g_alloc_particles(ct2g_ctx *ctx, size_t n);
 int ct2g_alloc_mesh(ct2g_ctx *ctx);
+// exclusive scan (+ offset) of n uint32 values; in may equal out
 int ct2g_scan_exclusive(ct2g_ctx *ctx, const uint32_t *in, uint32_t *out, size_t n,
-                        uint32_t *total_host);
+                        uint32_t *total_host, uint32_t offset);
 int ct2g_bin_range(ct2g_ctx *ctx);
 int ct2g_build_greens(ct2g_ctx *ctx);
 int ct2g_p2m(ct2g_ctx *ctx);

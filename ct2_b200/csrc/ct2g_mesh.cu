@@ -14,6 +14,8 @@
 //   phi(x) = -GM sum_a L_a t^a/a!,   F_i = GM sum_a L_{a+e_i} t^a/a!,
 // truncated at |a|+|b| <= p, the cell-centre sums done as one periodic
 // convolution per (a, b) on the mesh.
+#include <utility>
+
 #include "ct2g_internal.cuh"
 
 namespace {
@@ -66,39 +68,87 @@ __global__ void __launch_bounds__(128) p2m_kernel(const uint32_t *__restrict__ x
 // MG2L: one thread per k-point, in place on the spectrum.
 // G_n is real for even |n| and i*g for odd |n| (parity of D^n phi).
 // ---------------------------------------------------------------------------
+// The (a, b) pairs with |a|+|b| <= P, grouped by a: since multi-indices are
+// ordered by degree, the b of one a are exactly the first ncomp(P-|a|).
+template <int P>
+struct Mg2lPairs {
+  static constexpr int NC = ct2g_ncomp(P);
+  static constexpr int count() {
+    int n = 0;
+    for (int d = 0; d <= P; d++) n += (ct2g_ncomp(d) - (d ? ct2g_ncomp(d - 1) : 0)) * ct2g_ncomp(P - d);
+    return n;
+  }
+  static constexpr int NP = count();
+  int a[NP], b[NP], ab[NP], odd[NP], first[NP], last[NP];
+  constexpr Mg2lPairs() : a(), b(), ab(), odd(), first(), last() {
+    MiTable<P> T{};
+    int i = 0;
+    for (int ia = 0; ia < NC; ia++) {
+      const int nb = ct2g_ncomp(P - T.deg[ia]);
+      for (int ib = 0; ib < nb; ib++) {
+        a[i] = ia;
+        b[i] = ib;
+        ab[i] = ct2g_mi_index(T.nx[ia] + T.nx[ib], T.ny[ia] + T.ny[ib], T.nz[ia] + T.nz[ib]);
+        odd[i] = (T.deg[ia] + T.deg[ib]) & 1;
+        first[i] = ib == 0;
+        last[i] = ib == nb - 1;
+        i++;
+      }
+    }
+  }
+};
+template <int P>
+struct Mg2lTab {
+  static constexpr Mg2lPairs<P> t{};
+};
+
+// one (a, b) term; every index is a compile-time constant, so m[] and acc
+// stay in registers
+template <int P, int I>
+__device__ __forceinline__ void mg2l_term(const float2 *m, const float *gcol, float2 &acc,
+                                          float2 *out, int64_t CK) {
+  constexpr int A = Mg2lTab<P>::t.a[I], B = Mg2lTab<P>::t.b[I], AB = Mg2lTab<P>::t.ab[I];
+  constexpr bool FIRST = Mg2lTab<P>::t.first[I] != 0, LAST = Mg2lTab<P>::t.last[I] != 0,
+                 ODD = Mg2lTab<P>::t.odd[I] != 0;
+  if constexpr (FIRST) acc = make_float2(0.f, 0.f);
+  const float gv = gcol[AB * 128];
+  const float2 mb = m[B];
+  if constexpr (!ODD) {
+    acc.x = fmaf(gv, mb.x, acc.x);
+    acc.y = fmaf(gv, mb.y, acc.y);
+  } else {  // i*g*(mx + i my) = (-g my, g mx)
+    acc.x = fmaf(-gv, mb.y, acc.x);
+    acc.y = fmaf(gv, mb.x, acc.y);
+  }
+  if constexpr (LAST) out[(int64_t)A * CK] = acc;
+}
+
+template <int P, int... I>
+__device__ __forceinline__ void mg2l_all(const float2 *m, const float *gcol, float2 *out,
+                                         int64_t CK, std::integer_sequence<int, I...>) {
+  float2 acc = make_float2(0.f, 0.f);
+  (mg2l_term<P, I>(m, gcol, acc, out, CK), ...);
+}
+
+// MG2L: one thread per k-point, in place on the spectrum.  G_n is real for
+// even |n| and i*g for odd |n| (parity of D^n phi).  The thread's Green's
+// values go to a private smem column (no sharing, so no barrier); the moments
+// stay in registers.
 template <int P>
 __global__ void __launch_bounds__(128) mg2l_kernel(float2 *__restrict__ spec,
                                                    const float *__restrict__ G, int64_t CK) {
-  constexpr MiTable<P> T{};
-  constexpr int NC = MiTable<P>::NC;
+  constexpr int NC = ct2g_ncomp(P);
+  __shared__ float gs[NC * 128];
   const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= CK) return;
   float2 m[NC];
-  float g[NC];
 #pragma unroll
   for (int k = 0; k < NC; k++) {
     m[k] = spec[(int64_t)k * CK + q];
-    g[k] = G[(int64_t)k * CK + q];
+    gs[k * 128 + threadIdx.x] = __ldg(G + (int64_t)k * CK + q);
   }
-#pragma unroll
-  for (int a = 0; a < NC; a++) {
-    float2 acc = make_float2(0.f, 0.f);
-#pragma unroll
-    for (int b = 0; b < NC; b++) {
-      if (T.deg[a] + T.deg[b] <= P) {
-        const int ab = ct2g_mi_index(T.nx[a] + T.nx[b], T.ny[a] + T.ny[b], T.nz[a] + T.nz[b]);
-        const float gv = g[ab];
-        if (((T.deg[a] + T.deg[b]) & 1) == 0) {
-          acc.x = fmaf(gv, m[b].x, acc.x);
-          acc.y = fmaf(gv, m[b].y, acc.y);
-        } else {  // i*g*(mx + i my) = (-g my, g mx)
-          acc.x = fmaf(-gv, m[b].y, acc.x);
-          acc.y = fmaf(gv, m[b].x, acc.y);
-        }
-      }
-    }
-    spec[(int64_t)a * CK + q] = acc;
-  }
+  mg2l_all<P>(m, gs + threadIdx.x, spec + q, CK,
+              std::make_integer_sequence<int, Mg2lPairs<P>::NP>{});
 }
 
 // ---------------------------------------------------------------------------

@@ -61,7 +61,8 @@ __global__ void __launch_bounds__(256) forces_kernel(
     const float *__restrict__ grid, int mbits, int nstencil, float soft, float GM,
     float *__restrict__ ofx, float *__restrict__ ofy, float *__restrict__ ofz,
     float *__restrict__ opot, unsigned long long *__restrict__ inter) {
-  const int lane = threadIdx.x & 31;
+  __shared__ float4 sbuf[8][32];  // one batch of 32 sources per warp
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const uint32_t ch = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (ch >= nchunks) return;
   const int M = 1 << mbits;
@@ -76,43 +77,63 @@ __global__ void __launch_bounds__(256) forces_kernel(
             cz = (int)ct2g_compact3(key);
   const int64_t cell = ((int64_t)cx * M + cy) * M + cz;  // row-major grid index
   float fx = 0.f, fy = 0.f, fz = 0.f, ph = 0.f;
-  if (P > 0) l2p<P>(grid, C, cell, si.x, si.y, si.z, fx, fy, fz, ph);
+  l2p<P>(grid, C, cell, si.x, si.y, si.z, fx, fy, fz, ph);
   const float hc = 1.0f / (float)M;
   const float h2 = soft * soft, hinv = 1.f / soft, hinv3 = hinv * hinv * hinv;
   float nx = 0.f, ny = 0.f, nz = 0.f, np = 0.f;
   uint32_t nsrc = 0;
-  for (int s = 0; s < nstencil; s++) {
-    const int ox = c_stencil[4 * s], oy = c_stencil[4 * s + 1], oz = c_stencil[4 * s + 2];
-    const uint32_t nb = ct2g_morton((uint32_t)((cx + ox) & (M - 1)),
-                                    (uint32_t)((cy + oy) & (M - 1)),
-                                    (uint32_t)((cz + oz) & (M - 1)));
-    const uint32_t j0 = cs[nb], j1 = cs[nb + 1];
-    nsrc += j1 - j0;
-    // sink position relative to the neighbour cell's centre
-    const float xs = si.x - (float)ox * hc, ys = si.y - (float)oy * hc,
-                zs = si.z - (float)oz * hc;
-    for (uint32_t j = j0; j < j1; j++) {
-      const float4 q = __ldg(src + j);
-      const float dx = xs - q.x, dy = ys - q.y, dz = zs - q.z;
-      const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-      float g;
-      if (KERNEL == CT2G_SOFT_PLUMMER) {
-        const float ri = rsqrtf(r2 + h2);
-        g = ri * ri * ri;
-        if (POT) np -= ri;
-      } else {
-        if (r2 < h2) {
-          g = hinv3;
-          if (POT) np -= 1.5f * hinv - 0.5f * r2 * hinv3;
-        } else {
-          const float ri = rsqrtf(r2);
-          g = ri * ri * ri;
-          if (POT) np -= ri;
+  float4 *sb = sbuf[wib];
+  for (int s0 = 0; s0 < nstencil; s0 += 32) {
+    // 32 neighbour ranges fetched at once, one per lane
+    uint32_t jb = 0, je = 0;
+    const int sl = s0 + lane;
+    if (sl < nstencil) {
+      const uint32_t nb = ct2g_morton((uint32_t)((cx + c_stencil[4 * sl]) & (M - 1)),
+                                      (uint32_t)((cy + c_stencil[4 * sl + 1]) & (M - 1)),
+                                      (uint32_t)((cz + c_stencil[4 * sl + 2]) & (M - 1)));
+      jb = cs[nb];
+      je = cs[nb + 1];
+    }
+    const int nt = min(32, nstencil - s0);
+    for (int t = 0; t < nt; t++) {
+      const uint32_t j0 = __shfl_sync(0xffffffffu, jb, t), j1 = __shfl_sync(0xffffffffu, je, t);
+      if (j0 == j1) continue;
+      nsrc += j1 - j0;
+      const int st = s0 + t;
+      // sink position relative to the neighbour cell's centre
+      const float xs = si.x - (float)c_stencil[4 * st] * hc;
+      const float ys = si.y - (float)c_stencil[4 * st + 1] * hc;
+      const float zs = si.z - (float)c_stencil[4 * st + 2] * hc;
+      for (uint32_t jj = j0; jj < j1; jj += 32) {
+        const int cnt = (int)min(32u, j1 - jj);
+        __syncwarp();
+        if (lane < cnt) sb[lane] = __ldg(src + jj + lane);
+        __syncwarp();
+#pragma unroll 8
+        for (int u = 0; u < cnt; u++) {
+          const float4 q = sb[u];
+          const float dx = xs - q.x, dy = ys - q.y, dz = zs - q.z;
+          const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+          float g;
+          if (KERNEL == CT2G_SOFT_PLUMMER) {
+            const float ri = rsqrtf(r2 + h2);
+            g = ri * ri * ri;
+            if (POT) np -= ri;
+          } else {
+            if (r2 < h2) {
+              g = hinv3;
+              if (POT) np -= 1.5f * hinv - 0.5f * r2 * hinv3;
+            } else {
+              const float ri = rsqrtf(r2);
+              g = ri * ri * ri;
+              if (POT) np -= ri;
+            }
+          }
+          nx = fmaf(-dx, g, nx);
+          ny = fmaf(-dy, g, ny);
+          nz = fmaf(-dz, g, nz);
         }
       }
-      nx = fmaf(-dx, g, nx);
-      ny = fmaf(-dy, g, ny);
-      nz = fmaf(-dz, g, nz);
     }
   }
   if (act) {
