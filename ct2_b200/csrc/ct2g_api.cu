@@ -75,7 +75,8 @@ void free_particles(ct2g_ctx *ctx) {
   void *ptrs[] = {ctx->x, ctx->y, ctx->z, ctx->id, ctx->vx, ctx->vy, ctx->vz, ctx->rung,
                   ctx->x2, ctx->y2, ctx->z2, ctx->id2, ctx->vx2, ctx->vy2, ctx->vz2, ctx->rung2,
                   ctx->keys, ctx->keys2, ctx->vals, ctx->vals2, ctx->hist, ctx->src,
-                  ctx->chunk_begin, ctx->flags, ctx->fx, ctx->fy, ctx->fz, ctx->pot};
+                  ctx->chunk_begin, ctx->sparse_list, ctx->flags, ctx->fx, ctx->fy, ctx->fz,
+                  ctx->pot};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   ctx->x = ctx->y = ctx->z = ctx->id = nullptr;
@@ -86,7 +87,7 @@ void free_particles(ct2g_ctx *ctx) {
   ctx->rung2 = nullptr;
   ctx->keys = ctx->keys2 = ctx->vals = ctx->vals2 = ctx->hist = nullptr;
   ctx->src = nullptr;
-  ctx->chunk_begin = ctx->flags = nullptr;
+  ctx->chunk_begin = ctx->sparse_list = ctx->flags = nullptr;
   ctx->fx = ctx->fy = ctx->fz = ctx->pot = nullptr;
   ctx->cap = 0;
 }
@@ -154,6 +155,7 @@ int ct2g_alloc_particles(ct2g_ctx *ctx, size_t n) {
   A(ctx->hist, ntiles * 256 * 4);
   A(ctx->src, cap * sizeof(float4));
   A(ctx->chunk_begin, cap * 4);
+  A(ctx->sparse_list, cap * 4);
   A(ctx->flags, cap * 4);
   A(ctx->fx, cap * 4);
   A(ctx->fy, cap * 4);
@@ -226,7 +228,8 @@ int ct2g_create(const ct2g_options *opt, ct2g_ctx **out) {
   ctx->M = opt->mesh;
   while ((1 << ctx->mbits) < ctx->M) ctx->mbits++;
   ctx->C = (int64_t)ctx->M * ctx->M * ctx->M;
-  ctx->CK = (int64_t)ctx->M * ctx->M * (ctx->M / 2 + 1);
+  ctx->ldk = ctx->M / 2 + 2;  // even, so spectrum rows start on 16-byte boundaries
+  ctx->CK = (int64_t)ctx->M * ctx->M * ctx->ldk;
   ctx->p = opt->order;
   ctx->nc = ct2g_ncomp(ctx->p);
   int rc = CT2G_OK;
@@ -427,17 +430,22 @@ int ct2g_download_greens(ct2g_ctx *ctx, float *out) {
   CT2G_TRY(check(ctx));
   if (!out) return ct2g_fail(ctx, CT2G_EINVAL, "null output");
   CT2G_TRY(ct2g_build_greens(ctx));
-  CT2G_CUDA(ctx, cudaMemcpyAsync(out, ctx->greens, sizeof(float) * ctx->nc * ctx->CK,
+  std::vector<float> h((size_t)ctx->nc * ctx->CK);
+  CT2G_CUDA(ctx, cudaMemcpyAsync(h.data(), ctx->greens, sizeof(float) * h.size(),
                                  cudaMemcpyDeviceToHost, ctx->stream));
   CT2G_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  const size_t NH = ctx->M / 2 + 1, rows = (size_t)ctx->nc * ctx->M * ctx->M;
+  for (size_t r = 0; r < rows; r++)
+    std::memcpy(out + r * NH, h.data() + r * ctx->ldk, sizeof(float) * NH);
   return CT2G_OK;
 }
 
 int ct2g_compute_forces(ct2g_ctx *ctx) {
   CT2G_TRY(check(ctx));
   CT2G_TRY(ensure_expansions(ctx));
-  CT2G_TRY(ct2g_forces(ctx));
+  CT2G_TRY(ct2g_forces(ctx, true));
   ctx->forces_valid = true;
+  ctx->pot_valid = true;
   return CT2G_OK;
 }
 
@@ -479,7 +487,8 @@ int ct2g_kick(ct2g_ctx *ctx, const ct2g_kick_params *p, int *max_rung) {
   if (!p) return ct2g_fail(ctx, CT2G_EINVAL, "null kick params");
   if (p->rung < 0 || p->rung > 30) return ct2g_fail(ctx, CT2G_EINVAL, "rung out of range");
   CT2G_TRY(ensure_expansions(ctx));
-  CT2G_TRY(ct2g_forces(ctx));
+  CT2G_TRY(ct2g_forces(ctx, false));
+  ctx->pot_valid = false;
   cudaEventRecord(ctx->ev[6], ctx->stream);
   ctx->forces_valid = true;
   CT2G_TRY(ct2g_update(ctx, p, max_rung, false, 0.f, 1.f));
@@ -673,7 +682,7 @@ int ct2g_fft_r2c_3d(ct2g_ctx *ctx, const double *xin, double *xout, int N, int b
   std::vector<double2> h(nk * batch);
   e = cudaMemcpyAsync(din, xin, sizeof(double) * n3 * batch, cudaMemcpyHostToDevice, ctx->stream);
   if (e == cudaSuccess) {
-    rc = ct2g_fft_r2c_f64(ctx, din, dout, N, batch);
+    rc = ct2g_fft_r2c_f64(ctx, din, dout, N, batch, N / 2 + 1);
     if (rc == CT2G_OK) {
       e = cudaMemcpyAsync(h.data(), dout, sizeof(double2) * nk * batch, cudaMemcpyDeviceToHost, ctx->stream);
       if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
@@ -715,7 +724,7 @@ int ct2g_fft_c2r_3d(ct2g_ctx *ctx, const double *xin, double *xout, int N, int b
   int rc = CT2G_OK;
   e = cudaMemcpyAsync(din, h.data(), sizeof(double2) * nk * batch, cudaMemcpyHostToDevice, ctx->stream);
   if (e == cudaSuccess) {
-    rc = ct2g_fft_c2r_f64(ctx, din, dout, N, batch);
+    rc = ct2g_fft_c2r_f64(ctx, din, dout, N, batch, N / 2 + 1);
     if (rc == CT2G_OK) {
       e = cudaMemcpyAsync(xout, dout, sizeof(double) * n3 * batch, cudaMemcpyDeviceToHost, ctx->stream);
       if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
@@ -732,8 +741,9 @@ int ct2g_fft3d_f32_dev(ct2g_ctx *ctx, int dir, void *d_real, void *d_complex, in
   CT2G_TRY(check(ctx));
   if (!d_real || !d_complex || batch < 1 || !is_pow2(N) || N < 4 || N > 512)
     return ct2g_fail(ctx, CT2G_EINVAL, "fft3d_f32_dev: bad arguments");
-  if (dir > 0) return ct2g_fft_r2c_f32(ctx, (const float *)d_real, (float2 *)d_complex, N, batch);
-  return ct2g_fft_c2r_f32(ctx, (float2 *)d_complex, (float *)d_real, N, batch);
+  if (dir > 0)
+    return ct2g_fft_r2c_f32(ctx, (const float *)d_real, (float2 *)d_complex, N, batch, N / 2 + 1);
+  return ct2g_fft_c2r_f32(ctx, (float2 *)d_complex, (float *)d_real, N, batch, N / 2 + 1);
 }
 
 void *ct2g_stream(ct2g_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }

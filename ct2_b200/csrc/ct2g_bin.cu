@@ -240,22 +240,29 @@ __global__ void gather_kernel(const uint32_t *__restrict__ perm, size_t begin, s
                        (float)((int32_t)(pz & mask) - half) * sc, 0.f);
 }
 
-// chunk starts: every 32nd particle of a cell (counted from the cell start)
+// Sink work lists.  Cells with at least kDenseCell particles are split into
+// warp chunks (every 32nd particle of the cell starts one); particles of
+// sparser cells are listed individually for the thread-per-sink path.
+constexpr uint32_t kDenseCell = 16;
+
 __global__ void chunk_flag_kernel(const uint32_t *__restrict__ skeys,
                                   const uint32_t *__restrict__ cs, size_t begin, size_t nr,
-                                  uint32_t *__restrict__ flags) {
+                                  uint32_t *__restrict__ flags, uint32_t *__restrict__ sflags) {
   size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nr) return;
-  uint32_t c0 = cs[skeys[i]];
-  flags[i] = (((uint32_t)(begin + i) - c0) & 31u) == 0 ? 1u : 0u;
+  const uint32_t k = skeys[i];
+  const uint32_t c0 = cs[k], n = cs[k + 1] - c0;
+  const bool dense = n >= kDenseCell;
+  flags[i] = (dense && ((((uint32_t)(begin + i) - c0) & 31u) == 0)) ? 1u : 0u;
+  sflags[i] = dense ? 0u : 1u;
 }
 
 __global__ void chunk_fill_kernel(const uint32_t *__restrict__ flags,
                                   const uint32_t *__restrict__ fscan, size_t begin, size_t nr,
-                                  uint32_t *__restrict__ chunk_begin) {
+                                  uint32_t *__restrict__ list) {
   size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nr) return;
-  if (flags[i]) chunk_begin[fscan[i]] = (uint32_t)(begin + i);
+  if (flags[i]) list[fscan[i]] = (uint32_t)(begin + i);
 }
 
 }  // namespace
@@ -357,16 +364,21 @@ int ct2g_bin_range(ct2g_ctx *ctx) {
     std::swap(ctx->vz, ctx->vz2);
     std::swap(ctx->rung, ctx->rung2);
     std::swap(ctx->id, ctx->id2);
-    // sink chunks
+    // sink work lists: warp chunks of dense cells, single sinks of sparse ones
     chunk_flag_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(ctx->keys, ctx->cell_start, begin, nr,
-                                                        ctx->flags);
+                                                        ctx->flags, ctx->vals);
     CT2G_LAUNCHED(ctx);
-    uint32_t total = 0;
+    uint32_t total = 0, nsparse = 0;
     CT2G_TRY(ct2g_scan_exclusive(ctx, ctx->flags, ctx->vals2, nr, &total, 0));
     chunk_fill_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(ctx->flags, ctx->vals2, begin, nr,
                                                         ctx->chunk_begin);
     CT2G_LAUNCHED(ctx);
+    CT2G_TRY(ct2g_scan_exclusive(ctx, ctx->vals, ctx->vals2, nr, &nsparse, 0));
+    chunk_fill_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(ctx->vals, ctx->vals2, begin, nr,
+                                                        ctx->sparse_list);
+    CT2G_LAUNCHED(ctx);
     ctx->nchunks = total;
+    ctx->nsparse = nsparse;
   } else {
     // empty range: every cell empty
     uint32_t v = (uint32_t)begin;
@@ -375,6 +387,7 @@ int ct2g_bin_range(ct2g_ctx *ctx) {
                                    cudaMemcpyHostToDevice, st));
     CT2G_CUDA(ctx, cudaStreamSynchronize(st));
     ctx->nchunks = 0;
+    ctx->nsparse = 0;
   }
   ctx->grid_valid = true;
   ctx->moments_valid = false;

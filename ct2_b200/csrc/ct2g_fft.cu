@@ -22,6 +22,8 @@
 // in-register DFTs are radix-2 decimation-in-frequency butterflies with
 // compile-time twiddles.  Row tiles pad one word pair every R1 points so both
 // exchange patterns are free of bank conflicts.
+#include <type_traits>
+
 #include "ct2g_internal.cuh"
 
 namespace {
@@ -178,97 +180,137 @@ __device__ __forceinline__ void load_twiddles(C2 *stw, const C2 *tw, int n) {
 }
 
 // ---- pass Z forward: pairs of real lines -> half spectra -------------------
-// LP complex (packed) lines per block; npairs = number of real-line pairs
-template <typename T, int N>
-__global__ void __launch_bounds__(256) fftz_r2c_kernel(const T *__restrict__ in,
-                                                       typename Cplx<T>::type *__restrict__ out,
-                                                       size_t npairs, int LP,
-                                                       const typename Cplx<T>::type *__restrict__ tw) {
+// LP complex (packed) lines per block; npairs = number of real-line pairs;
+// output rows hold ld >= N/2+1 complex (the rest is written as zero).  VEC:
+// ld*sizeof(complex) is a multiple of 16 bytes.
+template <typename T, int N, bool VEC>
+__global__ void __launch_bounds__(256, 3) fftz_r2c_kernel(const T *__restrict__ in,
+                                                          typename Cplx<T>::type *__restrict__ out,
+                                                          size_t npairs, int LP, int ld,
+                                                          const typename Cplx<T>::type *__restrict__ tw) {
   using C2 = typename Cplx<T>::type;
   using LL = LineLayout<N, true>;
   extern __shared__ __align__(16) unsigned char smraw[];
   constexpr int NH = N / 2 + 1;
+  constexpr int RC = 16 / sizeof(T);  // reals per 16-byte chunk
+  using RV = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
   C2 *stw = reinterpret_cast<C2 *>(smraw);
   C2 *s = stw + N;
+  T *sr = reinterpret_cast<T *>(s);
   load_twiddles(stw, tw, N);
   const size_t pair0 = (size_t)blockIdx.x * LP;
   const int np = (int)min((size_t)LP, npairs - pair0);
   const T *src = in + pair0 * 2 * N;
-  for (int e = threadIdx.x; e < np * N; e += blockDim.x) {
-    const int l = e / N, r = e % N;
-    C2 v;
-    v.x = src[(size_t)(2 * l) * N + r];
-    v.y = src[(size_t)(2 * l + 1) * N + r];
-    s[LL::at(l, r, 0)] = v;
+  // real line 2l -> .x of complex line l, real line 2l+1 -> .y
+  for (int c = threadIdx.x; c < np * 2 * N / RC; c += 256) {
+    const int e = c * RC, rl = e / N, r = e % N;
+    const RV v = *reinterpret_cast<const RV *>(src + e);
+    const T *vv = reinterpret_cast<const T *>(&v);
+#pragma unroll
+    for (int q = 0; q < RC; q++) sr[2 * LL::at(rl >> 1, r + q, 0) + (rl & 1)] = vv[q];
   }
   __syncthreads();
   tile_fft<N, true, C2, false>(s, np, 0, stw);
-  C2 *dst = out + pair0 * 2 * NH;
-  for (int e = threadIdx.x; e < np * NH; e += blockDim.x) {
-    const int l = e / NH, k = e % NH;
-    const C2 zk = s[LL::at(l, k & (N - 1), 0)];
-    const C2 zc = s[LL::at(l, (N - k) & (N - 1), 0)];
-    // A_k = (Z_k + conj Z_{N-k})/2, B_k = (Z_k - conj Z_{N-k})/(2i)
-    C2 a, b;
-    a.x = (T)0.5 * (zk.x + zc.x);
-    a.y = (T)0.5 * (zk.y - zc.y);
-    b.x = (T)0.5 * (zk.y + zc.y);
-    b.y = (T)0.5 * (zc.x - zk.x);
-    dst[(size_t)(2 * l) * NH + k] = a;
-    dst[(size_t)(2 * l + 1) * NH + k] = b;
+  C2 *dst = out + pair0 * 2 * (size_t)ld;
+  constexpr int CC = (VEC && sizeof(C2) == 8) ? 2 : 1;  // complex per store
+  const int nchunk = ld / CC;
+  for (int c = threadIdx.x; c < np * nchunk; c += 256) {
+    const int l = c / nchunk, k0 = (c % nchunk) * CC;
+    C2 a[CC], b[CC];
+#pragma unroll
+    for (int q = 0; q < CC; q++) {
+      const int k = k0 + q;
+      if (k < NH) {
+        const C2 zk = s[LL::at(l, k & (N - 1), 0)];
+        const C2 zc = s[LL::at(l, (N - k) & (N - 1), 0)];
+        // A_k = (Z_k + conj Z_{N-k})/2, B_k = (Z_k - conj Z_{N-k})/(2i)
+        a[q].x = (T)0.5 * (zk.x + zc.x);
+        a[q].y = (T)0.5 * (zk.y - zc.y);
+        b[q].x = (T)0.5 * (zk.y + zc.y);
+        b[q].y = (T)0.5 * (zc.x - zk.x);
+      } else {
+        a[q].x = a[q].y = b[q].x = b[q].y = (T)0;
+      }
+    }
+    if (CC == 2) {
+      *reinterpret_cast<float4 *>(dst + (size_t)(2 * l) * ld + k0) = *reinterpret_cast<float4 *>(a);
+      *reinterpret_cast<float4 *>(dst + (size_t)(2 * l + 1) * ld + k0) = *reinterpret_cast<float4 *>(b);
+    } else {
+      dst[(size_t)(2 * l) * ld + k0] = a[0];
+      dst[(size_t)(2 * l + 1) * ld + k0] = b[0];
+    }
   }
 }
 
 // ---- pass Z inverse: pairs of half spectra -> real lines --------------------
-template <typename T, int N>
-__global__ void __launch_bounds__(256) fftz_c2r_kernel(const typename Cplx<T>::type *__restrict__ in,
-                                                       T *__restrict__ out, size_t npairs, int LP,
-                                                       const typename Cplx<T>::type *__restrict__ tw) {
+template <typename T, int N, bool VEC>
+__global__ void __launch_bounds__(256, 3) fftz_c2r_kernel(const typename Cplx<T>::type *__restrict__ in,
+                                                          T *__restrict__ out, size_t npairs, int LP,
+                                                          int ld,
+                                                          const typename Cplx<T>::type *__restrict__ tw) {
   using C2 = typename Cplx<T>::type;
   using LL = LineLayout<N, true>;
   extern __shared__ __align__(16) unsigned char smraw[];
   constexpr int NH = N / 2 + 1;
+  constexpr int RC = 16 / sizeof(T);
+  using RV = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
   C2 *stw = reinterpret_cast<C2 *>(smraw);
   C2 *s = stw + N;
+  const T *sr = reinterpret_cast<const T *>(s);
   load_twiddles(stw, tw, N);
   const size_t pair0 = (size_t)blockIdx.x * LP;
   const int np = (int)min((size_t)LP, npairs - pair0);
-  const C2 *src = in + pair0 * 2 * NH;
-  for (int e = threadIdx.x; e < np * N; e += blockDim.x) {
-    const int l = e / N, k = e % N;
-    // Z_k = A_k + i B_k, with A_{N-k} = conj(A_k) for the upper half
-    C2 a, b, z;
-    if (k < NH) {
-      a = src[(size_t)(2 * l) * NH + k];
-      b = src[(size_t)(2 * l + 1) * NH + k];
+  const C2 *src = in + pair0 * 2 * (size_t)ld;
+  constexpr int CC = (VEC && sizeof(C2) == 8) ? 2 : 1;
+  constexpr int NCH = (NH + CC - 1) / CC;  // chunks covering k = 0..N/2
+  for (int c = threadIdx.x; c < np * NCH; c += 256) {
+    const int l = c / NCH, k0 = (c % NCH) * CC;
+    C2 a[CC], b[CC];
+    if (CC == 2) {
+      *reinterpret_cast<float4 *>(a) = *reinterpret_cast<const float4 *>(src + (size_t)(2 * l) * ld + k0);
+      *reinterpret_cast<float4 *>(b) = *reinterpret_cast<const float4 *>(src + (size_t)(2 * l + 1) * ld + k0);
     } else {
-      a = src[(size_t)(2 * l) * NH + (N - k)];
-      b = src[(size_t)(2 * l + 1) * NH + (N - k)];
-      a.y = -a.y;
-      b.y = -b.y;
+      a[0] = src[(size_t)(2 * l) * ld + k0];
+      b[0] = src[(size_t)(2 * l + 1) * ld + k0];
     }
-    z.x = a.x - b.y;
-    z.y = a.y + b.x;
-    s[LL::at(l, k, 0)] = z;
+#pragma unroll
+    for (int q = 0; q < CC; q++) {
+      const int k = k0 + q;
+      if (k >= NH) continue;
+      // Z_k = A_k + i B_k; Z_{N-k} = conj(A_k) + i conj(B_k)
+      C2 z;
+      z.x = a[q].x - b[q].y;
+      z.y = a[q].y + b[q].x;
+      s[LL::at(l, k, 0)] = z;
+      if (k > 0 && k < N / 2) {
+        C2 w;
+        w.x = a[q].x + b[q].y;
+        w.y = -a[q].y + b[q].x;
+        s[LL::at(l, N - k, 0)] = w;
+      }
+    }
   }
   __syncthreads();
   tile_fft<N, true, C2, true>(s, np, 0, stw);
   T *dst = out + pair0 * 2 * N;
-  for (int e = threadIdx.x; e < np * N; e += blockDim.x) {
-    const int l = e / N, r = e % N;
-    const C2 z = s[LL::at(l, r, 0)];
-    dst[(size_t)(2 * l) * N + r] = z.x;
-    dst[(size_t)(2 * l + 1) * N + r] = z.y;
+  for (int c = threadIdx.x; c < np * 2 * N / RC; c += 256) {
+    const int e = c * RC, rl = e / N, r = e % N;
+    RV v;
+    T *vv = reinterpret_cast<T *>(&v);
+#pragma unroll
+    for (int q = 0; q < RC; q++) vv[q] = sr[2 * LL::at(rl >> 1, r + q, 0) + (rl & 1)];
+    *reinterpret_cast<RV *>(dst + e) = v;
   }
 }
 
 // ---- strided passes: FFT along rows for tiles of W contiguous columns -------
 // array: outer blocks of `ostride` elements; inside, rows of `rstride`; ncols
-// valid columns per row.  grid.x = nouter * ntiles.
-template <typename C2, int N, bool INV>
-__global__ void __launch_bounds__(256) fft_cols_kernel(C2 *__restrict__ a, size_t ostride,
-                                                       size_t rstride, size_t ncols, int W,
-                                                       int ntiles, const C2 *__restrict__ tw) {
+// valid columns per row.  grid.x = nouter * ntiles.  VEC: rows start on
+// 16-byte boundaries, so the tile moves in 16-byte chunks.
+template <typename C2, int N, int W, bool INV, bool VEC>
+__global__ void __launch_bounds__(256, 3) fft_cols_kernel(C2 *__restrict__ a, size_t ostride,
+                                                          size_t rstride, size_t ncols,
+                                                          int ntiles, const C2 *__restrict__ tw) {
   extern __shared__ __align__(16) unsigned char smraw[];
   C2 *stw = reinterpret_cast<C2 *>(smraw);
   C2 *s = stw + N;
@@ -277,15 +319,21 @@ __global__ void __launch_bounds__(256) fft_cols_kernel(C2 *__restrict__ a, size_
   const size_t col0 = (size_t)(blockIdx.x % ntiles) * W;
   const int wv = (int)min((size_t)W, ncols - col0);
   C2 *base = a + outer * ostride + col0;
-  for (int e = threadIdx.x; e < N * W; e += blockDim.x) {
-    const int r = e / W, w = e % W;
-    if (w < wv) s[r * W + w] = base[(size_t)r * rstride + w];
+  // complex elements per 16-byte chunk
+  constexpr int CPC = (VEC && sizeof(C2) == 8) ? 2 : 1;
+  constexpr int CH = W / CPC;  // chunks per row
+  using V = typename std::conditional<CPC == 2, float4, C2>::type;
+#pragma unroll 4
+  for (int e = threadIdx.x; e < N * CH; e += 256) {
+    const int r = e / CH, c = (e % CH) * CPC;
+    if (c < wv) *reinterpret_cast<V *>(s + r * W + c) = *reinterpret_cast<const V *>(base + (size_t)r * rstride + c);
   }
   __syncthreads();
   tile_fft<N, false, C2, INV>(s, W, W, stw);
-  for (int e = threadIdx.x; e < N * W; e += blockDim.x) {
-    const int r = e / W, w = e % W;
-    if (w < wv) base[(size_t)r * rstride + w] = s[r * W + w];
+#pragma unroll 4
+  for (int e = threadIdx.x; e < N * CH; e += 256) {
+    const int r = e / CH, c = (e % CH) * CPC;
+    if (c < wv) *reinterpret_cast<V *>(base + (size_t)r * rstride + c) = *reinterpret_cast<const V *>(s + r * W + c);
   }
 }
 
@@ -296,97 +344,111 @@ const float2 *twiddle_ptr<float2>(ct2g_ctx *ctx) { return ctx->tw32; }
 template <>
 const double2 *twiddle_ptr<double2>(ct2g_ctx *ctx) { return ctx->tw64; }
 
+template <typename T, int N, bool INV, bool VEC>
+int launch_cols(ct2g_ctx *ctx, typename Cplx<T>::type *spec, size_t nouter, size_t ostride,
+                size_t rstride, size_t ncols) {
+  using C2 = typename Cplx<T>::type;
+  constexpr int W = N >= 256 ? 16 : 4096 / N;
+  const size_t smem = sizeof(C2) * ((size_t)N + (size_t)N * W);
+  auto k = fft_cols_kernel<C2, N, W, INV, VEC>;
+  CT2G_CUDA(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int ntiles = (int)((ncols + W - 1) / W);
+  k<<<(unsigned)(nouter * ntiles), 256, smem, ctx->stream>>>(spec, ostride, rstride, ncols, ntiles,
+                                                             twiddle_ptr<C2>(ctx));
+  CT2G_LAUNCHED(ctx);
+  return CT2G_OK;
+}
+
+// Y and X passes over a spectrum whose qk rows hold ld >= N/2+1 elements
 template <typename T, int N>
-int run_cols(ct2g_ctx *ctx, typename Cplx<T>::type *spec, int batch, bool inv) {
+int run_cols(ct2g_ctx *ctx, typename Cplx<T>::type *spec, int batch, bool inv, size_t ld) {
   using C2 = typename Cplx<T>::type;
   const size_t NH = N / 2 + 1;
-  const int W = std::max(16, 4096 / N);
-  const size_t smem = sizeof(C2) * ((size_t)N + (size_t)N * W);
-  auto kf = fft_cols_kernel<C2, N, false>;
-  auto ki = fft_cols_kernel<C2, N, true>;
-  CT2G_CUDA(ctx, cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  CT2G_CUDA(ctx, cudaFuncSetAttribute(ki, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const C2 *tw = twiddle_ptr<C2>(ctx);
+  const bool vec = (ld * sizeof(C2)) % 16 == 0;
   for (int pass = 0; pass < 2; pass++) {
     const bool ypass = (pass == 0) != inv;
     size_t nouter, ostride, rstride, ncols;
     if (ypass) {
       nouter = (size_t)batch * N;
-      ostride = (size_t)N * NH;
-      rstride = NH;
+      ostride = (size_t)N * ld;
+      rstride = ld;
       ncols = NH;
     } else {
       nouter = (size_t)batch;
-      ostride = (size_t)N * N * NH;
-      rstride = (size_t)N * NH;
-      ncols = (size_t)N * NH;
+      ostride = (size_t)N * N * ld;
+      rstride = (size_t)N * ld;
+      ncols = (size_t)N * ld;
     }
-    const int ntiles = (int)((ncols + W - 1) / W);
-    const size_t nblocks = nouter * ntiles;
-    (inv ? ki : kf)<<<(unsigned)nblocks, 256, smem, ctx->stream>>>(spec, ostride, rstride, ncols,
-                                                                     W, ntiles, tw);
-    CT2G_LAUNCHED(ctx);
+    if (inv) {
+      if (vec) CT2G_TRY((launch_cols<T, N, true, true>(ctx, spec, nouter, ostride, rstride, ncols)));
+      else CT2G_TRY((launch_cols<T, N, true, false>(ctx, spec, nouter, ostride, rstride, ncols)));
+    } else {
+      if (vec) CT2G_TRY((launch_cols<T, N, false, true>(ctx, spec, nouter, ostride, rstride, ncols)));
+      else CT2G_TRY((launch_cols<T, N, false, false>(ctx, spec, nouter, ostride, rstride, ncols)));
+    }
   }
   return CT2G_OK;
 }
 
 template <typename T, int N>
-int fft_r2c_n(ct2g_ctx *ctx, const T *in, typename Cplx<T>::type *out, int batch) {
+int fft_r2c_n(ct2g_ctx *ctx, const T *in, typename Cplx<T>::type *out, int batch, int ld) {
   using C2 = typename Cplx<T>::type;
   const size_t npairs = (size_t)batch * N * N / 2;
   const int LP = std::max(1, 4096 / N);
   const size_t smem = sizeof(C2) * ((size_t)N + (size_t)LP * LineLayout<N, true>::LS);
-  auto kern = fftz_r2c_kernel<T, N>;
+  const bool vec = ((size_t)ld * sizeof(C2)) % 16 == 0;
+  auto kern = vec ? fftz_r2c_kernel<T, N, true> : fftz_r2c_kernel<T, N, false>;
   CT2G_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  kern<<<ct2g_div_up(npairs, LP), 256, smem, ctx->stream>>>(in, out, npairs, LP,
+  kern<<<ct2g_div_up(npairs, LP), 256, smem, ctx->stream>>>(in, out, npairs, LP, ld,
                                                             twiddle_ptr<C2>(ctx));
   CT2G_LAUNCHED(ctx);
-  return run_cols<T, N>(ctx, out, batch, false);
+  return run_cols<T, N>(ctx, out, batch, false, ld);
 }
 
 template <typename T, int N>
-int fft_c2r_n(ct2g_ctx *ctx, typename Cplx<T>::type *in, T *out, int batch) {
+int fft_c2r_n(ct2g_ctx *ctx, typename Cplx<T>::type *in, T *out, int batch, int ld) {
   using C2 = typename Cplx<T>::type;
-  CT2G_TRY((run_cols<T, N>(ctx, in, batch, true)));
+  CT2G_TRY((run_cols<T, N>(ctx, in, batch, true, ld)));
   const size_t npairs = (size_t)batch * N * N / 2;
   const int LP = std::max(1, 4096 / N);
   const size_t smem = sizeof(C2) * ((size_t)N + (size_t)LP * LineLayout<N, true>::LS);
-  auto kern = fftz_c2r_kernel<T, N>;
+  const bool vec = ((size_t)ld * sizeof(C2)) % 16 == 0;
+  auto kern = vec ? fftz_c2r_kernel<T, N, true> : fftz_c2r_kernel<T, N, false>;
   CT2G_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  kern<<<ct2g_div_up(npairs, LP), 256, smem, ctx->stream>>>(in, out, npairs, LP,
+  kern<<<ct2g_div_up(npairs, LP), 256, smem, ctx->stream>>>(in, out, npairs, LP, ld,
                                                             twiddle_ptr<C2>(ctx));
   CT2G_LAUNCHED(ctx);
   return CT2G_OK;
 }
 
 template <typename T>
-int fft_r2c(ct2g_ctx *ctx, const T *in, typename Cplx<T>::type *out, int N, int batch) {
+int fft_r2c(ct2g_ctx *ctx, const T *in, typename Cplx<T>::type *out, int N, int batch, int ld) {
   CT2G_TRY(ct2g_twiddles(ctx, N));
   switch (N) {
-    case 4: return fft_r2c_n<T, 4>(ctx, in, out, batch);
-    case 8: return fft_r2c_n<T, 8>(ctx, in, out, batch);
-    case 16: return fft_r2c_n<T, 16>(ctx, in, out, batch);
-    case 32: return fft_r2c_n<T, 32>(ctx, in, out, batch);
-    case 64: return fft_r2c_n<T, 64>(ctx, in, out, batch);
-    case 128: return fft_r2c_n<T, 128>(ctx, in, out, batch);
-    case 256: return fft_r2c_n<T, 256>(ctx, in, out, batch);
-    case 512: return fft_r2c_n<T, 512>(ctx, in, out, batch);
+    case 4: return fft_r2c_n<T, 4>(ctx, in, out, batch, ld);
+    case 8: return fft_r2c_n<T, 8>(ctx, in, out, batch, ld);
+    case 16: return fft_r2c_n<T, 16>(ctx, in, out, batch, ld);
+    case 32: return fft_r2c_n<T, 32>(ctx, in, out, batch, ld);
+    case 64: return fft_r2c_n<T, 64>(ctx, in, out, batch, ld);
+    case 128: return fft_r2c_n<T, 128>(ctx, in, out, batch, ld);
+    case 256: return fft_r2c_n<T, 256>(ctx, in, out, batch, ld);
+    case 512: return fft_r2c_n<T, 512>(ctx, in, out, batch, ld);
   }
   return ct2g_fail(ctx, CT2G_EINVAL, "FFT size must be a power of two in [4, 512]");
 }
 
 template <typename T>
-int fft_c2r(ct2g_ctx *ctx, typename Cplx<T>::type *in, T *out, int N, int batch) {
+int fft_c2r(ct2g_ctx *ctx, typename Cplx<T>::type *in, T *out, int N, int batch, int ld) {
   CT2G_TRY(ct2g_twiddles(ctx, N));
   switch (N) {
-    case 4: return fft_c2r_n<T, 4>(ctx, in, out, batch);
-    case 8: return fft_c2r_n<T, 8>(ctx, in, out, batch);
-    case 16: return fft_c2r_n<T, 16>(ctx, in, out, batch);
-    case 32: return fft_c2r_n<T, 32>(ctx, in, out, batch);
-    case 64: return fft_c2r_n<T, 64>(ctx, in, out, batch);
-    case 128: return fft_c2r_n<T, 128>(ctx, in, out, batch);
-    case 256: return fft_c2r_n<T, 256>(ctx, in, out, batch);
-    case 512: return fft_c2r_n<T, 512>(ctx, in, out, batch);
+    case 4: return fft_c2r_n<T, 4>(ctx, in, out, batch, ld);
+    case 8: return fft_c2r_n<T, 8>(ctx, in, out, batch, ld);
+    case 16: return fft_c2r_n<T, 16>(ctx, in, out, batch, ld);
+    case 32: return fft_c2r_n<T, 32>(ctx, in, out, batch, ld);
+    case 64: return fft_c2r_n<T, 64>(ctx, in, out, batch, ld);
+    case 128: return fft_c2r_n<T, 128>(ctx, in, out, batch, ld);
+    case 256: return fft_c2r_n<T, 256>(ctx, in, out, batch, ld);
+    case 512: return fft_c2r_n<T, 512>(ctx, in, out, batch, ld);
   }
   return ct2g_fail(ctx, CT2G_EINVAL, "FFT size must be a power of two in [4, 512]");
 }
@@ -435,15 +497,15 @@ int ct2g_twiddles(ct2g_ctx *ctx, int N) {
   return CT2G_OK;
 }
 
-int ct2g_fft_r2c_f32(ct2g_ctx *ctx, const float *in, float2 *out, int N, int batch) {
-  return fft_r2c<float>(ctx, in, out, N, batch);
+int ct2g_fft_r2c_f32(ct2g_ctx *ctx, const float *in, float2 *out, int N, int batch, int ld) {
+  return fft_r2c<float>(ctx, in, out, N, batch, ld);
 }
-int ct2g_fft_c2r_f32(ct2g_ctx *ctx, float2 *in, float *out, int N, int batch) {
-  return fft_c2r<float>(ctx, in, out, N, batch);
+int ct2g_fft_c2r_f32(ct2g_ctx *ctx, float2 *in, float *out, int N, int batch, int ld) {
+  return fft_c2r<float>(ctx, in, out, N, batch, ld);
 }
-int ct2g_fft_r2c_f64(ct2g_ctx *ctx, const double *in, double2 *out, int N, int batch) {
-  return fft_r2c<double>(ctx, in, out, N, batch);
+int ct2g_fft_r2c_f64(ct2g_ctx *ctx, const double *in, double2 *out, int N, int batch, int ld) {
+  return fft_r2c<double>(ctx, in, out, N, batch, ld);
 }
-int ct2g_fft_c2r_f64(ct2g_ctx *ctx, double2 *in, double *out, int N, int batch) {
-  return fft_c2r<double>(ctx, in, out, N, batch);
+int ct2g_fft_c2r_f64(ct2g_ctx *ctx, double2 *in, double *out, int N, int batch, int ld) {
+  return fft_c2r<double>(ctx, in, out, N, batch, ld);
 }

@@ -80,7 +80,8 @@ struct ct2g_ctx {
   int mbits = 0;
   int M = 0;       // mesh cells per dim
   int64_t C = 0;   // mesh^3
-  int64_t CK = 0;  // mesh*mesh*(mesh/2+1)
+  int64_t CK = 0;  // mesh*mesh*ldk: spectrum entries per component
+  int ldk = 0;     // spectrum row pitch along the halved axis: mesh/2+2 (even)
   int p = 0;
   int nc = 0;      // ncomp(p)
   int device = 0;
@@ -107,9 +108,11 @@ struct ct2g_ctx {
   size_t scan_tmp_words = 0;
   uint32_t *cell_start = nullptr;  // [C+1] indexed by Morton key, absolute indices
   float4 *src = nullptr;           // per sorted particle: offset from own cell centre
-  uint32_t *chunk_begin = nullptr; // sink chunks (<=32 particles of one cell)
+  uint32_t *chunk_begin = nullptr; // sink chunks (<=32 particles of one dense cell)
+  uint32_t *sparse_list = nullptr; // sinks of sparse cells, one per thread
   uint32_t *flags = nullptr;
   uint32_t nchunks = 0;
+  uint32_t nsparse = 0;
   // forces
   float *fx = nullptr, *fy = nullptr, *fz = nullptr, *pot = nullptr;
   int *d_maxrung = nullptr;
@@ -134,6 +137,7 @@ struct ct2g_ctx {
   bool expansions_valid = false;
   bool greens_valid = false;
   bool forces_valid = false;
+  bool pot_valid = false;        // potential computed with the current forces
   bool has_particles = false;
 };
 
@@ -174,15 +178,17 @@ int ct2g_bin_range(ct2g_ctx *ctx);
 int ct2g_build_greens(ct2g_ctx *ctx);
 int ct2g_p2m(ct2g_ctx *ctx);
 int ct2g_mesh_solve(ct2g_ctx *ctx);
-int ct2g_forces(ct2g_ctx *ctx);
+// forces of the current range; pot: also the potential (diagnostics)
+int ct2g_forces(ct2g_ctx *ctx, bool pot);
 int ct2g_update(ct2g_ctx *ctx, const ct2g_kick_params *p, int *max_rung, bool fuse_drift,
                 float drift_dt, float drift_scale);
 int ct2g_drift_all(ct2g_ctx *ctx, float dt, float scale);
 int ct2g_twiddles(ct2g_ctx *ctx, int N);
-// batched 3D FFTs on device buffers, on ctx->stream
-int ct2g_fft_r2c_f32(ct2g_ctx *ctx, const float *in, float2 *out, int N, int batch);
-int ct2g_fft_c2r_f32(ct2g_ctx *ctx, float2 *in, float *out, int N, int batch);
-int ct2g_fft_r2c_f64(ct2g_ctx *ctx, const double *in, double2 *out, int N, int batch);
-int ct2g_fft_c2r_f64(ct2g_ctx *ctx, double2 *in, double *out, int N, int batch);
+// batched 3D FFTs on device buffers, on ctx->stream; spectrum rows (along the
+// halved axis) hold ld >= N/2+1 complex values
+int ct2g_fft_r2c_f32(ct2g_ctx *ctx, const float *in, float2 *out, int N, int batch, int ld);
+int ct2g_fft_c2r_f32(ct2g_ctx *ctx, float2 *in, float *out, int N, int batch, int ld);
+int ct2g_fft_r2c_f64(ct2g_ctx *ctx, const double *in, double2 *out, int N, int batch, int ld);
+int ct2g_fft_c2r_f64(ct2g_ctx *ctx, double2 *in, double *out, int N, int batch, int ld);
 
 static inline unsigned ct2g_div_up(size_t a, size_t b) { return (unsigned)((a + b - 1) / b); }

@@ -263,15 +263,20 @@ __global__ void greens_real_kernel(int mbits, int p, int kernel, double soft, do
 }
 
 // combine the FFT of the real-space part with the folded Ewald k-space sum
+// (spectrum rows hold ldk entries; those past M/2 are padding, set to zero)
 __global__ void greens_finish_kernel(int mbits, int p, double alpha, int kmax,
-                                     const int *__restrict__ mi, int k0, int K,
+                                     const int *__restrict__ mi, int k0, int K, int ldk,
                                      const double2 *__restrict__ spec64, float *__restrict__ G) {
   const int M = 1 << mbits;
   const int NH = M / 2 + 1;
-  const int64_t CK = (int64_t)M * M * NH;
+  const int64_t CK = (int64_t)M * M * ldk;
   const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= CK) return;
-  const int qx = (int)(q / ((int64_t)M * NH)), qy = (int)((q / NH) % M), qz = (int)(q % NH);
+  const int qx = (int)(q / ((int64_t)M * ldk)), qy = (int)((q / ldk) % M), qz = (int)(q % ldk);
+  if (qz >= NH) {
+    for (int kk = 0; kk < K; kk++) G[(int64_t)(k0 + kk) * CK + q] = 0.f;
+    return;
+  }
   const double norm = 1.0 / ((double)M * M * M);
   double acc[64];
   for (int kk = 0; kk < K; kk++) {
@@ -413,10 +418,10 @@ int ct2g_build_greens(ct2g_ctx *ctx) {
         rc = ct2g_cuda_fail(ctx, e, "greens_real_kernel");
         break;
       }
-      rc = ct2g_fft_r2c_f64(ctx, rs, sp, M, kk);
+      rc = ct2g_fft_r2c_f64(ctx, rs, sp, M, kk, ctx->ldk);
       if (rc != CT2G_OK) break;
       greens_finish_kernel<<<ct2g_div_up(ctx->CK, 128), 128, 0, ctx->stream>>>(
-          ctx->mbits, p, kGreensAlpha, kGreensKmax, d_mi, k0, kk, sp, ctx->greens);
+          ctx->mbits, p, kGreensAlpha, kGreensKmax, d_mi, k0, kk, ctx->ldk, sp, ctx->greens);
       ctx->launches++;
       if ((e = cudaGetLastError()) != cudaSuccess) {
         rc = ct2g_cuda_fail(ctx, e, "greens_finish_kernel");
@@ -450,7 +455,7 @@ int ct2g_p2m(ct2g_ctx *ctx) {
 int ct2g_mesh_solve(ct2g_ctx *ctx) {
   CT2G_TRY(ct2g_build_greens(ctx));
   cudaEventRecord(ctx->ev[2], ctx->stream);
-  CT2G_TRY(ct2g_fft_r2c_f32(ctx, ctx->grid, ctx->spec, ctx->M, ctx->nc));
+  CT2G_TRY(ct2g_fft_r2c_f32(ctx, ctx->grid, ctx->spec, ctx->M, ctx->nc, ctx->ldk));
   cudaEventRecord(ctx->ev[3], ctx->stream);
   switch (ctx->p) {
     case 1: CT2G_TRY(launch_mg2l<1>(ctx)); break;
@@ -462,7 +467,7 @@ int ct2g_mesh_solve(ct2g_ctx *ctx) {
     default: return ct2g_fail(ctx, CT2G_EINVAL, "unsupported order");
   }
   cudaEventRecord(ctx->ev[4], ctx->stream);
-  CT2G_TRY(ct2g_fft_c2r_f32(ctx, ctx->spec, ctx->grid, ctx->M, ctx->nc));
+  CT2G_TRY(ct2g_fft_c2r_f32(ctx, ctx->spec, ctx->grid, ctx->M, ctx->nc, ctx->ldk));
   cudaEventRecord(ctx->ev[5], ctx->stream);
   return CT2G_OK;
 }

@@ -145,6 +145,89 @@ __global__ void __launch_bounds__(256) forces_kernel(
   if (lane == 0 && inter) atomicAdd(inter, (unsigned long long)(cend - b) * nsrc);
 }
 
+// Thread-per-sink near field for sinks of sparse cells (fewer than 16
+// particles): each lane walks its own 123-ish stencil cells; neighbouring
+// lanes are neighbouring sinks (cell-sorted), so the source loads mostly hit
+// L1.  Neighbour ranges are fetched four at a time to overlap their latency.
+template <int P, int KERNEL, bool POT>
+__global__ void __launch_bounds__(128) forces_sparse_kernel(
+    const uint32_t *__restrict__ sinks, uint32_t nsinks, const uint32_t *__restrict__ cs,
+    const uint32_t *__restrict__ skeys, uint32_t rbegin, const float4 *__restrict__ src,
+    const float *__restrict__ grid, int mbits, int nstencil, float soft, float GM,
+    float *__restrict__ ofx, float *__restrict__ ofy, float *__restrict__ ofz,
+    float *__restrict__ opot, unsigned long long *__restrict__ inter) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t nsrc = 0;
+  if (t < nsinks) {
+    const int M = 1 << mbits;
+    const int64_t C = (int64_t)M * M * M;
+    const uint32_t i = sinks[t];
+    const uint32_t key = skeys[i - rbegin];
+    const float4 si = src[i];
+    const int cx = (int)ct2g_compact3(key >> 2), cy = (int)ct2g_compact3(key >> 1),
+              cz = (int)ct2g_compact3(key);
+    const int64_t cell = ((int64_t)cx * M + cy) * M + cz;
+    float fx = 0.f, fy = 0.f, fz = 0.f, ph = 0.f;
+    l2p<P>(grid, C, cell, si.x, si.y, si.z, fx, fy, fz, ph);
+    const float hc = 1.0f / (float)M;
+    const float h2 = soft * soft, hinv = 1.f / soft, hinv3 = hinv * hinv * hinv;
+    float nx = 0.f, ny = 0.f, nz = 0.f, np = 0.f;
+    for (int s0 = 0; s0 < nstencil; s0 += 4) {
+      uint32_t jb[4], je[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const int s = min(s0 + u, nstencil - 1);
+        const uint32_t nb = ct2g_morton((uint32_t)((cx + c_stencil[4 * s]) & (M - 1)),
+                                        (uint32_t)((cy + c_stencil[4 * s + 1]) & (M - 1)),
+                                        (uint32_t)((cz + c_stencil[4 * s + 2]) & (M - 1)));
+        jb[u] = cs[nb];
+        je[u] = s0 + u < nstencil ? cs[nb + 1] : jb[u];
+      }
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        if (jb[u] == je[u]) continue;
+        const int s = s0 + u;
+        nsrc += je[u] - jb[u];
+        const float xs = si.x - (float)c_stencil[4 * s] * hc;
+        const float ys = si.y - (float)c_stencil[4 * s + 1] * hc;
+        const float zs = si.z - (float)c_stencil[4 * s + 2] * hc;
+        for (uint32_t j = jb[u]; j < je[u]; j++) {
+          const float4 q = __ldg(src + j);
+          const float dx = xs - q.x, dy = ys - q.y, dz = zs - q.z;
+          const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+          float g;
+          if (KERNEL == CT2G_SOFT_PLUMMER) {
+            const float ri = rsqrtf(r2 + h2);
+            g = ri * ri * ri;
+            if (POT) np -= ri;
+          } else {
+            if (r2 < h2) {
+              g = hinv3;
+              if (POT) np -= 1.5f * hinv - 0.5f * r2 * hinv3;
+            } else {
+              const float ri = rsqrtf(r2);
+              g = ri * ri * ri;
+              if (POT) np -= ri;
+            }
+          }
+          nx = fmaf(-dx, g, nx);
+          ny = fmaf(-dy, g, ny);
+          nz = fmaf(-dz, g, nz);
+        }
+      }
+    }
+    ofx[i] = GM * (fx + nx);
+    ofy[i] = GM * (fy + ny);
+    ofz[i] = GM * (fz + nz);
+    if (POT) opot[i] = GM * (ph + np);
+  }
+  // warp-summed interaction count
+  unsigned long long c = nsrc;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0 && c && inter) atomicAdd(inter, c);
+}
+
 __device__ __forceinline__ int ceil_log2_exact(float v) {
   // exact ceil(log2(v)) for finite normal v > 0
   const uint32_t u = __float_as_uint(v);
@@ -208,20 +291,33 @@ __global__ void drift_kernel(size_t n, uint32_t *__restrict__ x, uint32_t *__res
 
 template <int P, int K, bool POT>
 int launch_forces_t(ct2g_ctx *ctx) {
-  const unsigned T = 256;
-  const size_t threads = (size_t)ctx->nchunks * 32;
-  forces_kernel<P, K, POT><<<ct2g_div_up(threads, T), T, 0, ctx->stream>>>(
-      ctx->chunk_begin, ctx->nchunks, ctx->cell_start, ctx->keys, (uint32_t)ctx->rung_begin,
-      ctx->src, ctx->grid, ctx->mbits, ctx->nstencil, ctx->opt.hsoft, ctx->opt.GM, ctx->fx,
-      ctx->fy, ctx->fz, ctx->pot, ctx->d_inter);
-  CT2G_LAUNCHED(ctx);
+  if (ctx->nchunks) {
+    const unsigned T = 256;
+    const size_t threads = (size_t)ctx->nchunks * 32;
+    forces_kernel<P, K, POT><<<ct2g_div_up(threads, T), T, 0, ctx->stream>>>(
+        ctx->chunk_begin, ctx->nchunks, ctx->cell_start, ctx->keys, (uint32_t)ctx->rung_begin,
+        ctx->src, ctx->grid, ctx->mbits, ctx->nstencil, ctx->opt.hsoft, ctx->opt.GM, ctx->fx,
+        ctx->fy, ctx->fz, ctx->pot, ctx->d_inter);
+    CT2G_LAUNCHED(ctx);
+  }
+  if (ctx->nsparse) {
+    const unsigned T = 128;
+    forces_sparse_kernel<P, K, POT><<<ct2g_div_up(ctx->nsparse, T), T, 0, ctx->stream>>>(
+        ctx->sparse_list, ctx->nsparse, ctx->cell_start, ctx->keys, (uint32_t)ctx->rung_begin,
+        ctx->src, ctx->grid, ctx->mbits, ctx->nstencil, ctx->opt.hsoft, ctx->opt.GM, ctx->fx,
+        ctx->fy, ctx->fz, ctx->pot, ctx->d_inter);
+    CT2G_LAUNCHED(ctx);
+  }
   return CT2G_OK;
 }
 
 template <int P>
-int launch_forces_p(ct2g_ctx *ctx) {
-  if (ctx->opt.kernel == CT2G_SOFT_SPHERE) return launch_forces_t<P, CT2G_SOFT_SPHERE, true>(ctx);
-  return launch_forces_t<P, CT2G_SOFT_PLUMMER, true>(ctx);
+int launch_forces_p(ct2g_ctx *ctx, bool pot) {
+  if (ctx->opt.kernel == CT2G_SOFT_SPHERE)
+    return pot ? launch_forces_t<P, CT2G_SOFT_SPHERE, true>(ctx)
+               : launch_forces_t<P, CT2G_SOFT_SPHERE, false>(ctx);
+  return pot ? launch_forces_t<P, CT2G_SOFT_PLUMMER, true>(ctx)
+             : launch_forces_t<P, CT2G_SOFT_PLUMMER, false>(ctx);
 }
 
 }  // namespace
@@ -232,22 +328,22 @@ int ct2g_upload_stencil(ct2g_ctx *ctx, const std::vector<int> &st4) {
   return CT2G_OK;
 }
 
-int ct2g_forces(ct2g_ctx *ctx) {
+int ct2g_forces(ct2g_ctx *ctx, bool pot) {
   const size_t n = ctx->n;
   // entries outside the range read as zero
   CT2G_CUDA(ctx, cudaMemsetAsync(ctx->fx, 0, n * 4, ctx->stream));
   CT2G_CUDA(ctx, cudaMemsetAsync(ctx->fy, 0, n * 4, ctx->stream));
   CT2G_CUDA(ctx, cudaMemsetAsync(ctx->fz, 0, n * 4, ctx->stream));
-  CT2G_CUDA(ctx, cudaMemsetAsync(ctx->pot, 0, n * 4, ctx->stream));
+  if (pot) CT2G_CUDA(ctx, cudaMemsetAsync(ctx->pot, 0, n * 4, ctx->stream));
   CT2G_CUDA(ctx, cudaMemsetAsync(ctx->d_inter, 0, sizeof(unsigned long long), ctx->stream));
-  if (ctx->nchunks == 0) return CT2G_OK;
+  if (ctx->nchunks == 0 && ctx->nsparse == 0) return CT2G_OK;
   switch (ctx->p) {
-    case 1: return launch_forces_p<1>(ctx);
-    case 2: return launch_forces_p<2>(ctx);
-    case 3: return launch_forces_p<3>(ctx);
-    case 4: return launch_forces_p<4>(ctx);
-    case 5: return launch_forces_p<5>(ctx);
-    case 6: return launch_forces_p<6>(ctx);
+    case 1: return launch_forces_p<1>(ctx, pot);
+    case 2: return launch_forces_p<2>(ctx, pot);
+    case 3: return launch_forces_p<3>(ctx, pot);
+    case 4: return launch_forces_p<4>(ctx, pot);
+    case 5: return launch_forces_p<5>(ctx, pot);
+    case 6: return launch_forces_p<6>(ctx, pot);
   }
   return ct2g_fail(ctx, CT2G_EINVAL, "unsupported order");
 }

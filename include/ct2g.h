@@ -135,7 +135,8 @@ int ct2g_download_greens(ct2g_ctx *ctx, float *out);
  * src/kick.cpp:19-74), without touching velocities. */
 int ct2g_compute_forces(ct2g_ctx *ctx);
 /* host float[n] each, current order; pot may be NULL.  Accelerations include
- * GM.  Entries outside the current range are zero. */
+ * GM.  Entries outside the current range are zero.  The potential is computed
+ * by ct2g_compute_forces only (ct2g_kick skips it; it then reads as zero). */
 int ct2g_download_forces(ct2g_ctx *ctx, float *fx, float *fy, float *fz, float *pot);
 /* host float[n] each: replaces the force buffer (for update-only tests) */
 int ct2g_upload_forces(ct2g_ctx *ctx, const float *fx, const float *fy, const float *fz);
