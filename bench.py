@@ -180,8 +180,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--ngrid", type=int, default=128)
     ap.add_argument("--mesh", type=int, default=256)
-    ap.add_argument("--order", type=int, default=5)
-    ap.add_argument("--bwidth", type=float, default=3.0)
+    ap.add_argument("--order", type=int, default=4)
+    ap.add_argument("--bwidth", type=float, default=4.0)
     ap.add_argument("--nspheres", type=int, default=512)
     ap.add_argument("--a", type=float, default=0.005)
     ap.add_argument("--dt", type=float, default=1e-3)
