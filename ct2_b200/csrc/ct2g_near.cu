@@ -145,6 +145,120 @@ __global__ void __launch_bounds__(256) forces_kernel(
   if (lane == 0 && inter) atomicAdd(inter, (unsigned long long)(cend - b) * nsrc);
 }
 
+// Source-parallel near field for a sparse cell (< 16 sinks) beside dense
+// cells: one warp per cell, the lanes hold 32 sources at a time and every
+// sink of the cell is a warp-uniform register value, so a dense neighbour is
+// consumed at full lane width; per-lane partial forces are reduced across the
+// warp once per sink at the end.
+template <int P, int KERNEL, bool POT>
+__global__ void __launch_bounds__(128) forces_heavy_kernel(
+    const uint32_t *__restrict__ cell_first, uint32_t ncells, const uint32_t *__restrict__ cs,
+    const uint32_t *__restrict__ skeys, uint32_t rbegin, const float4 *__restrict__ src,
+    const float *__restrict__ grid, int mbits, int nstencil, float soft, float GM,
+    float *__restrict__ ofx, float *__restrict__ ofy, float *__restrict__ ofz,
+    float *__restrict__ opot, unsigned long long *__restrict__ inter) {
+  constexpr int MS = 16;  // max sinks per cell on this path
+  const int lane = threadIdx.x & 31;
+  const uint32_t wc = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (wc >= ncells) return;
+  const int M = 1 << mbits;
+  const int64_t C = (int64_t)M * M * M;
+  const uint32_t b = cell_first[wc];
+  const uint32_t key = skeys[b - rbegin];
+  const int n = (int)min(cs[key + 1] - b, (uint32_t)MS);
+  const int cx = (int)ct2g_compact3(key >> 2), cy = (int)ct2g_compact3(key >> 1),
+            cz = (int)ct2g_compact3(key);
+  // sink positions (offsets from the cell centre), broadcast to all lanes
+  const float4 mine = src[b + min(lane, n - 1)];
+  float sx[MS], sy[MS], sz[MS], ax[MS], ay[MS], az[MS], ap[MS];
+#pragma unroll
+  for (int s = 0; s < MS; s++) {
+    sx[s] = __shfl_sync(0xffffffffu, mine.x, s);
+    sy[s] = __shfl_sync(0xffffffffu, mine.y, s);
+    sz[s] = __shfl_sync(0xffffffffu, mine.z, s);
+    ax[s] = ay[s] = az[s] = ap[s] = 0.f;
+  }
+  const float hc = 1.0f / (float)M;
+  const float h2 = soft * soft, hinv = 1.f / soft, hinv3 = hinv * hinv * hinv;
+  uint32_t nsrc = 0;
+  for (int s0 = 0; s0 < nstencil; s0 += 32) {
+    uint32_t jb = 0, je = 0;
+    const int sl = s0 + lane;
+    if (sl < nstencil) {
+      const uint32_t nb = ct2g_morton((uint32_t)((cx + c_stencil[4 * sl]) & (M - 1)),
+                                      (uint32_t)((cy + c_stencil[4 * sl + 1]) & (M - 1)),
+                                      (uint32_t)((cz + c_stencil[4 * sl + 2]) & (M - 1)));
+      jb = cs[nb];
+      je = cs[nb + 1];
+    }
+    const int nt = min(32, nstencil - s0);
+    for (int t = 0; t < nt; t++) {
+      const uint32_t j0 = __shfl_sync(0xffffffffu, jb, t), j1 = __shfl_sync(0xffffffffu, je, t);
+      if (j0 == j1) continue;
+      nsrc += j1 - j0;
+      const int st = s0 + t;
+      // source positions relative to the sink cell's centre
+      const float ox = (float)c_stencil[4 * st] * hc, oy = (float)c_stencil[4 * st + 1] * hc,
+                  oz = (float)c_stencil[4 * st + 2] * hc;
+      for (uint32_t jj = j0; jj < j1; jj += 32) {
+        const bool on = jj + lane < j1;
+        const float4 q = __ldg(src + (on ? jj + lane : j0));
+        const float qx = q.x + ox, qy = q.y + oy, qz = q.z + oz;
+#pragma unroll
+        for (int s = 0; s < MS; s++) {
+          if (s < n) {
+            const float dx = sx[s] - qx, dy = sy[s] - qy, dz = sz[s] - qz;
+            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            float g, pp = 0.f;
+            if (KERNEL == CT2G_SOFT_PLUMMER) {
+              const float ri = rsqrtf(r2 + h2);
+              g = ri * ri * ri;
+              pp = ri;
+            } else {
+              if (r2 < h2) {
+                g = hinv3;
+                pp = 1.5f * hinv - 0.5f * r2 * hinv3;
+              } else {
+                const float ri = rsqrtf(r2);
+                g = ri * ri * ri;
+                pp = ri;
+              }
+            }
+            g = on ? g : 0.f;
+            ax[s] = fmaf(-dx, g, ax[s]);
+            ay[s] = fmaf(-dy, g, ay[s]);
+            az[s] = fmaf(-dz, g, az[s]);
+            if (POT) ap[s] -= on ? pp : 0.f;
+          }
+        }
+      }
+    }
+  }
+  // far field for this lane's sink, then the warp reductions
+  float fx = 0.f, fy = 0.f, fz = 0.f, ph = 0.f;
+  l2p<P>(grid, C, ((int64_t)cx * M + cy) * M + cz, mine.x, mine.y, mine.z, fx, fy, fz, ph);
+#pragma unroll
+  for (int s = 0; s < MS; s++) {
+    if (s < n) {
+      float vx = ax[s], vy = ay[s], vz = az[s], vp = ap[s];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        vx += __shfl_xor_sync(0xffffffffu, vx, o);
+        vy += __shfl_xor_sync(0xffffffffu, vy, o);
+        vz += __shfl_xor_sync(0xffffffffu, vz, o);
+        if (POT) vp += __shfl_xor_sync(0xffffffffu, vp, o);
+      }
+      if (lane == s) {
+        ofx[b + s] = GM * (fx + vx);
+        ofy[b + s] = GM * (fy + vy);
+        ofz[b + s] = GM * (fz + vz);
+        if (POT) opot[b + s] = GM * (ph + vp);
+      }
+    }
+  }
+  if (lane == 0 && inter) atomicAdd(inter, (unsigned long long)n * nsrc);
+}
+
 // Thread-per-sink near field for sinks of sparse cells (fewer than 16
 // particles): each lane walks its own 123-ish stencil cells; neighbouring
 // lanes are neighbouring sinks (cell-sorted), so the source loads mostly hit
@@ -300,6 +414,15 @@ int launch_forces_t(ct2g_ctx *ctx) {
         ctx->fy, ctx->fz, ctx->pot, ctx->d_inter);
     CT2G_LAUNCHED(ctx);
   }
+  if (ctx->nheavy) {
+    const unsigned T = 128;
+    const size_t threads = (size_t)ctx->nheavy * 32;
+    forces_heavy_kernel<P, K, POT><<<ct2g_div_up(threads, T), T, 0, ctx->stream>>>(
+        ctx->heavy_list, ctx->nheavy, ctx->cell_start, ctx->keys, (uint32_t)ctx->rung_begin,
+        ctx->src, ctx->grid, ctx->mbits, ctx->nstencil, ctx->opt.hsoft, ctx->opt.GM, ctx->fx,
+        ctx->fy, ctx->fz, ctx->pot, ctx->d_inter);
+    CT2G_LAUNCHED(ctx);
+  }
   if (ctx->nsparse) {
     const unsigned T = 128;
     forces_sparse_kernel<P, K, POT><<<ct2g_div_up(ctx->nsparse, T), T, 0, ctx->stream>>>(
@@ -336,7 +459,7 @@ int ct2g_forces(ct2g_ctx *ctx, bool pot) {
   CT2G_CUDA(ctx, cudaMemsetAsync(ctx->fz, 0, n * 4, ctx->stream));
   if (pot) CT2G_CUDA(ctx, cudaMemsetAsync(ctx->pot, 0, n * 4, ctx->stream));
   CT2G_CUDA(ctx, cudaMemsetAsync(ctx->d_inter, 0, sizeof(unsigned long long), ctx->stream));
-  if (ctx->nchunks == 0 && ctx->nsparse == 0) return CT2G_OK;
+  if (ctx->nchunks == 0 && ctx->nsparse == 0 && ctx->nheavy == 0) return CT2G_OK;
   switch (ctx->p) {
     case 1: return launch_forces_p<1>(ctx, pot);
     case 2: return launch_forces_p<2>(ctx, pot);
