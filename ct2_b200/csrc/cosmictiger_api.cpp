@@ -74,11 +74,15 @@ void derive(options &o) {
   const double n3 = (double)o.Ngrid * o.Ngrid * o.Ngrid;
   o.GM = (float)(1.0 / n3);
   o.nparts = o.Ngrid * o.Ngrid * o.Ngrid;
-  o.code_to_g = (float)(M0 * o.mass_res);
+  // M0 * mass_res (~2e42 g by default) overflows the float field, as it does
+  // in the reference; the conversions that follow are carried in FP64 so
+  // code_to_cm and code_to_s (and the cosmology built on them) stay finite
+  const double code_to_g = M0 * (double)o.mass_res;
+  o.code_to_g = (float)code_to_g;
   const double Hh = H0 * o.hubble;
-  o.code_to_cm = (float)std::cbrt((double)o.code_to_g * 8.0 * pi * n3 * G /
-                                  (3.0 * o.omega_m * Hh * Hh));
-  o.code_to_s = (float)(o.code_to_cm / c);
+  const double code_to_cm = std::cbrt(code_to_g * 8.0 * pi * n3 * G / (3.0 * o.omega_m * Hh * Hh));
+  o.code_to_cm = (float)code_to_cm;
+  o.code_to_s = (float)(code_to_cm / c);
   // radiation: photons plus Neff = 3.086 neutrino species at (4/11)^(4/3)
   const double Neff = 3.086;
   const double Tcmb = 2.73 * o.Theta;

@@ -241,32 +241,20 @@ __global__ void gather_kernel(const uint32_t *__restrict__ perm, size_t begin, s
 }
 
 // Sink work lists.  Cells with at least kDenseCell particles are split into
-// warp chunks (every 32nd particle of the cell starts one).  Sparser cells
-// whose 4x4x4-cell parent block (a contiguous Morton range) holds at least
-// kHeavyBlock particles -- cells beside a cluster core -- are listed once per
-// cell for the source-parallel warp path; the remaining (isolated) sinks are
-// listed individually for the thread-per-sink path.
+// warp chunks (every 32nd particle of the cell starts one); particles of
+// sparser cells are listed individually for the thread-per-sink path.
 constexpr uint32_t kDenseCell = 16;
-constexpr uint32_t kHeavyBlock = 96;
 
 __global__ void chunk_flag_kernel(const uint32_t *__restrict__ skeys,
                                   const uint32_t *__restrict__ cs, size_t begin, size_t nr,
-                                  uint32_t C, uint32_t *__restrict__ flags,
-                                  uint32_t *__restrict__ cflags, uint32_t *__restrict__ sflags) {
+                                  uint32_t *__restrict__ flags, uint32_t *__restrict__ sflags) {
   size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nr) return;
   const uint32_t k = skeys[i];
   const uint32_t c0 = cs[k], n = cs[k + 1] - c0;
   const bool dense = n >= kDenseCell;
-  bool heavy = false;
-  if (!dense) {
-    const uint32_t kb = k & ~63u, ke = min(kb + 64u, C);
-    heavy = cs[ke] - cs[kb] >= kHeavyBlock;
-  }
-  const bool first = (uint32_t)(begin + i) == c0;
   flags[i] = (dense && ((((uint32_t)(begin + i) - c0) & 31u) == 0)) ? 1u : 0u;
-  cflags[i] = (!dense && heavy && first) ? 1u : 0u;
-  sflags[i] = (!dense && !heavy) ? 1u : 0u;
+  sflags[i] = dense ? 0u : 1u;
 }
 
 __global__ void chunk_fill_kernel(const uint32_t *__restrict__ flags,
@@ -376,27 +364,20 @@ int ct2g_bin_range(ct2g_ctx *ctx) {
     std::swap(ctx->vz, ctx->vz2);
     std::swap(ctx->rung, ctx->rung2);
     std::swap(ctx->id, ctx->id2);
-    // sink work lists: warp chunks of dense cells, warp cells beside dense
-    // regions, single isolated sinks
+    // sink work lists: warp chunks of dense cells, single sinks of sparse ones
     chunk_flag_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(ctx->keys, ctx->cell_start, begin, nr,
-                                                        (uint32_t)ctx->C, ctx->flags, ctx->x2,
-                                                        ctx->vals);
+                                                        ctx->flags, ctx->vals);
     CT2G_LAUNCHED(ctx);
-    uint32_t total = 0, nsparse = 0, nheavy = 0;
+    uint32_t total = 0, nsparse = 0;
     CT2G_TRY(ct2g_scan_exclusive(ctx, ctx->flags, ctx->vals2, nr, &total, 0));
     chunk_fill_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(ctx->flags, ctx->vals2, begin, nr,
                                                         ctx->chunk_begin);
-    CT2G_LAUNCHED(ctx);
-    CT2G_TRY(ct2g_scan_exclusive(ctx, ctx->x2, ctx->vals2, nr, &nheavy, 0));
-    chunk_fill_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(ctx->x2, ctx->vals2, begin, nr,
-                                                        ctx->heavy_list);
     CT2G_LAUNCHED(ctx);
     CT2G_TRY(ct2g_scan_exclusive(ctx, ctx->vals, ctx->vals2, nr, &nsparse, 0));
     chunk_fill_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(ctx->vals, ctx->vals2, begin, nr,
                                                         ctx->sparse_list);
     CT2G_LAUNCHED(ctx);
     ctx->nchunks = total;
-    ctx->nheavy = nheavy;
     ctx->nsparse = nsparse;
   } else {
     // empty range: every cell empty
@@ -406,7 +387,6 @@ int ct2g_bin_range(ct2g_ctx *ctx) {
                                    cudaMemcpyHostToDevice, st));
     CT2G_CUDA(ctx, cudaStreamSynchronize(st));
     ctx->nchunks = 0;
-    ctx->nheavy = 0;
     ctx->nsparse = 0;
   }
   ctx->grid_valid = true;

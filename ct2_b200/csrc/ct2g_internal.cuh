@@ -109,12 +109,10 @@ struct ct2g_ctx {
   uint32_t *cell_start = nullptr;  // [C+1] indexed by Morton key, absolute indices
   float4 *src = nullptr;           // per sorted particle: offset from own cell centre
   uint32_t *chunk_begin = nullptr; // sink chunks (<=32 particles of one dense cell)
-  uint32_t *heavy_list = nullptr;  // first particle of sparse cells beside dense regions
   uint32_t *sparse_list = nullptr; // isolated sinks, one per thread
   uint32_t *flags = nullptr;
   uint32_t nchunks = 0;
   uint32_t nsparse = 0;
-  uint32_t nheavy = 0;
   // forces
   float *fx = nullptr, *fy = nullptr, *fz = nullptr, *pot = nullptr;
   int *d_maxrung = nullptr;

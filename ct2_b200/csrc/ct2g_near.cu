@@ -145,124 +145,42 @@ __global__ void __launch_bounds__(256) forces_kernel(
   if (lane == 0 && inter) atomicAdd(inter, (unsigned long long)(cend - b) * nsrc);
 }
 
-// Source-parallel near field for a sparse cell (< 16 sinks) beside dense
-// cells: one warp per cell, the lanes hold 32 sources at a time and every
-// sink of the cell is a warp-uniform register value, so a dense neighbour is
-// consumed at full lane width; per-lane partial forces are reduced across the
-// warp once per sink at the end.
-template <int P, int KERNEL, bool POT>
-__global__ void __launch_bounds__(128) forces_heavy_kernel(
-    const uint32_t *__restrict__ cell_first, uint32_t ncells, const uint32_t *__restrict__ cs,
-    const uint32_t *__restrict__ skeys, uint32_t rbegin, const float4 *__restrict__ src,
-    const float *__restrict__ grid, int mbits, int nstencil, float soft, float GM,
-    float *__restrict__ ofx, float *__restrict__ ofy, float *__restrict__ ofz,
-    float *__restrict__ opot, unsigned long long *__restrict__ inter) {
-  constexpr int MS = 16;  // max sinks per cell on this path
-  const int lane = threadIdx.x & 31;
-  const uint32_t wc = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (wc >= ncells) return;
-  const int M = 1 << mbits;
-  const int64_t C = (int64_t)M * M * M;
-  const uint32_t b = cell_first[wc];
-  const uint32_t key = skeys[b - rbegin];
-  const int n = (int)min(cs[key + 1] - b, (uint32_t)MS);
-  const int cx = (int)ct2g_compact3(key >> 2), cy = (int)ct2g_compact3(key >> 1),
-            cz = (int)ct2g_compact3(key);
-  // sink positions (offsets from the cell centre), broadcast to all lanes
-  const float4 mine = src[b + min(lane, n - 1)];
-  float sx[MS], sy[MS], sz[MS], ax[MS], ay[MS], az[MS], ap[MS];
-#pragma unroll
-  for (int s = 0; s < MS; s++) {
-    sx[s] = __shfl_sync(0xffffffffu, mine.x, s);
-    sy[s] = __shfl_sync(0xffffffffu, mine.y, s);
-    sz[s] = __shfl_sync(0xffffffffu, mine.z, s);
-    ax[s] = ay[s] = az[s] = ap[s] = 0.f;
-  }
-  const float hc = 1.0f / (float)M;
-  const float h2 = soft * soft, hinv = 1.f / soft, hinv3 = hinv * hinv * hinv;
-  uint32_t nsrc = 0;
-  for (int s0 = 0; s0 < nstencil; s0 += 32) {
-    uint32_t jb = 0, je = 0;
-    const int sl = s0 + lane;
-    if (sl < nstencil) {
-      const uint32_t nb = ct2g_morton((uint32_t)((cx + c_stencil[4 * sl]) & (M - 1)),
-                                      (uint32_t)((cy + c_stencil[4 * sl + 1]) & (M - 1)),
-                                      (uint32_t)((cz + c_stencil[4 * sl + 2]) & (M - 1)));
-      jb = cs[nb];
-      je = cs[nb + 1];
-    }
-    const int nt = min(32, nstencil - s0);
-    for (int t = 0; t < nt; t++) {
-      const uint32_t j0 = __shfl_sync(0xffffffffu, jb, t), j1 = __shfl_sync(0xffffffffu, je, t);
-      if (j0 == j1) continue;
-      nsrc += j1 - j0;
-      const int st = s0 + t;
-      // source positions relative to the sink cell's centre
-      const float ox = (float)c_stencil[4 * st] * hc, oy = (float)c_stencil[4 * st + 1] * hc,
-                  oz = (float)c_stencil[4 * st + 2] * hc;
-      for (uint32_t jj = j0; jj < j1; jj += 32) {
-        const bool on = jj + lane < j1;
-        const float4 q = __ldg(src + (on ? jj + lane : j0));
-        const float qx = q.x + ox, qy = q.y + oy, qz = q.z + oz;
-#pragma unroll
-        for (int s = 0; s < MS; s++) {
-          if (s < n) {
-            const float dx = sx[s] - qx, dy = sy[s] - qy, dz = sz[s] - qz;
-            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-            float g, pp = 0.f;
-            if (KERNEL == CT2G_SOFT_PLUMMER) {
-              const float ri = rsqrtf(r2 + h2);
-              g = ri * ri * ri;
-              pp = ri;
-            } else {
-              if (r2 < h2) {
-                g = hinv3;
-                pp = 1.5f * hinv - 0.5f * r2 * hinv3;
-              } else {
-                const float ri = rsqrtf(r2);
-                g = ri * ri * ri;
-                pp = ri;
-              }
-            }
-            g = on ? g : 0.f;
-            ax[s] = fmaf(-dx, g, ax[s]);
-            ay[s] = fmaf(-dy, g, ay[s]);
-            az[s] = fmaf(-dz, g, az[s]);
-            if (POT) ap[s] -= on ? pp : 0.f;
-          }
-        }
-      }
+// Thread-per-sink near field for sinks of sparse cells (fewer than 16
+// particles).  Every lane walks its own stencil (neighbouring lanes are
+// neighbouring sinks, so source loads mostly hit L1).  A neighbour cell with
+// fewer than kLight sources is consumed by the lane alone; a heavier one (a
+// cluster core next to a halo sink) is consumed by the whole warp: lanes take
+// 32 sources at a time against the owning lane's sink, and a warp reduction
+// hands the sum to the owner, so no lane idles through a long private loop.
+constexpr uint32_t kLight = 24;
+
+template <int KERNEL, bool POT>
+__device__ __forceinline__ void pair_term(float dx, float dy, float dz, float h2, float hinv,
+                                          float hinv3, float &ax, float &ay, float &az,
+                                          float &ap, bool on) {
+  const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+  float g, pp;
+  if (KERNEL == CT2G_SOFT_PLUMMER) {
+    const float ri = rsqrtf(r2 + h2);
+    g = ri * ri * ri;
+    pp = ri;
+  } else {
+    if (r2 < h2) {
+      g = hinv3;
+      pp = 1.5f * hinv - 0.5f * r2 * hinv3;
+    } else {
+      const float ri = rsqrtf(r2);
+      g = ri * ri * ri;
+      pp = ri;
     }
   }
-  // far field for this lane's sink, then the warp reductions
-  float fx = 0.f, fy = 0.f, fz = 0.f, ph = 0.f;
-  l2p<P>(grid, C, ((int64_t)cx * M + cy) * M + cz, mine.x, mine.y, mine.z, fx, fy, fz, ph);
-#pragma unroll
-  for (int s = 0; s < MS; s++) {
-    if (s < n) {
-      float vx = ax[s], vy = ay[s], vz = az[s], vp = ap[s];
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        vx += __shfl_xor_sync(0xffffffffu, vx, o);
-        vy += __shfl_xor_sync(0xffffffffu, vy, o);
-        vz += __shfl_xor_sync(0xffffffffu, vz, o);
-        if (POT) vp += __shfl_xor_sync(0xffffffffu, vp, o);
-      }
-      if (lane == s) {
-        ofx[b + s] = GM * (fx + vx);
-        ofy[b + s] = GM * (fy + vy);
-        ofz[b + s] = GM * (fz + vz);
-        if (POT) opot[b + s] = GM * (ph + vp);
-      }
-    }
-  }
-  if (lane == 0 && inter) atomicAdd(inter, (unsigned long long)n * nsrc);
+  if (!on) g = pp = 0.f;
+  ax = fmaf(-dx, g, ax);
+  ay = fmaf(-dy, g, ay);
+  az = fmaf(-dz, g, az);
+  if (POT) ap -= pp;
 }
 
-// Thread-per-sink near field for sinks of sparse cells (fewer than 16
-// particles): each lane walks its own 123-ish stencil cells; neighbouring
-// lanes are neighbouring sinks (cell-sorted), so the source loads mostly hit
-// L1.  Neighbour ranges are fetched four at a time to overlap their latency.
 template <int P, int KERNEL, bool POT>
 __global__ void __launch_bounds__(128) forces_sparse_kernel(
     const uint32_t *__restrict__ sinks, uint32_t nsinks, const uint32_t *__restrict__ cs,
@@ -271,75 +189,90 @@ __global__ void __launch_bounds__(128) forces_sparse_kernel(
     float *__restrict__ ofx, float *__restrict__ ofy, float *__restrict__ ofz,
     float *__restrict__ opot, unsigned long long *__restrict__ inter) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  if ((t & ~31u) >= nsinks) return;  // whole warps only: the loop below shuffles
+  const bool act = t < nsinks;
+  const int M = 1 << mbits;
+  const int64_t C = (int64_t)M * M * M;
+  const uint32_t i = sinks[act ? t : nsinks - 1];
+  const uint32_t key = skeys[i - rbegin];
+  const float4 si = src[i];
+  const int cx = (int)ct2g_compact3(key >> 2), cy = (int)ct2g_compact3(key >> 1),
+            cz = (int)ct2g_compact3(key);
+  const float hc = 1.0f / (float)M;
+  const float h2 = soft * soft, hinv = 1.f / soft, hinv3 = hinv * hinv * hinv;
+  float nx = 0.f, ny = 0.f, nz = 0.f, np = 0.f;
   uint32_t nsrc = 0;
-  if (t < nsinks) {
-    const int M = 1 << mbits;
-    const int64_t C = (int64_t)M * M * M;
-    const uint32_t i = sinks[t];
-    const uint32_t key = skeys[i - rbegin];
-    const float4 si = src[i];
-    const int cx = (int)ct2g_compact3(key >> 2), cy = (int)ct2g_compact3(key >> 1),
-              cz = (int)ct2g_compact3(key);
-    const int64_t cell = ((int64_t)cx * M + cy) * M + cz;
-    float fx = 0.f, fy = 0.f, fz = 0.f, ph = 0.f;
-    l2p<P>(grid, C, cell, si.x, si.y, si.z, fx, fy, fz, ph);
-    const float hc = 1.0f / (float)M;
-    const float h2 = soft * soft, hinv = 1.f / soft, hinv3 = hinv * hinv * hinv;
-    float nx = 0.f, ny = 0.f, nz = 0.f, np = 0.f;
-    for (int s0 = 0; s0 < nstencil; s0 += 4) {
-      uint32_t jb[4], je[4];
+  for (int s0 = 0; s0 < nstencil; s0 += 4) {
+    uint32_t jb[4], je[4];
 #pragma unroll
-      for (int u = 0; u < 4; u++) {
-        const int s = min(s0 + u, nstencil - 1);
-        const uint32_t nb = ct2g_morton((uint32_t)((cx + c_stencil[4 * s]) & (M - 1)),
-                                        (uint32_t)((cy + c_stencil[4 * s + 1]) & (M - 1)),
-                                        (uint32_t)((cz + c_stencil[4 * s + 2]) & (M - 1)));
-        jb[u] = cs[nb];
-        je[u] = s0 + u < nstencil ? cs[nb + 1] : jb[u];
-      }
+    for (int u = 0; u < 4; u++) {
+      const int s = min(s0 + u, nstencil - 1);
+      const uint32_t nb = ct2g_morton((uint32_t)((cx + c_stencil[4 * s]) & (M - 1)),
+                                      (uint32_t)((cy + c_stencil[4 * s + 1]) & (M - 1)),
+                                      (uint32_t)((cz + c_stencil[4 * s + 2]) & (M - 1)));
+      jb[u] = cs[nb];
+      je[u] = (act && s0 + u < nstencil) ? cs[nb + 1] : jb[u];
+    }
 #pragma unroll
-      for (int u = 0; u < 4; u++) {
-        if (jb[u] == je[u]) continue;
-        const int s = s0 + u;
-        nsrc += je[u] - jb[u];
-        const float xs = si.x - (float)c_stencil[4 * s] * hc;
-        const float ys = si.y - (float)c_stencil[4 * s + 1] * hc;
-        const float zs = si.z - (float)c_stencil[4 * s + 2] * hc;
+    for (int u = 0; u < 4; u++) {
+      const int s = min(s0 + u, nstencil - 1);
+      const uint32_t k = je[u] - jb[u];
+      nsrc += k;
+      const float xs = si.x - (float)c_stencil[4 * s] * hc;
+      const float ys = si.y - (float)c_stencil[4 * s + 1] * hc;
+      const float zs = si.z - (float)c_stencil[4 * s + 2] * hc;
+      if (k < kLight) {
         for (uint32_t j = jb[u]; j < je[u]; j++) {
           const float4 q = __ldg(src + j);
-          const float dx = xs - q.x, dy = ys - q.y, dz = zs - q.z;
-          const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-          float g;
-          if (KERNEL == CT2G_SOFT_PLUMMER) {
-            const float ri = rsqrtf(r2 + h2);
-            g = ri * ri * ri;
-            if (POT) np -= ri;
-          } else {
-            if (r2 < h2) {
-              g = hinv3;
-              if (POT) np -= 1.5f * hinv - 0.5f * r2 * hinv3;
-            } else {
-              const float ri = rsqrtf(r2);
-              g = ri * ri * ri;
-              if (POT) np -= ri;
-            }
-          }
-          nx = fmaf(-dx, g, nx);
-          ny = fmaf(-dy, g, ny);
-          nz = fmaf(-dz, g, nz);
+          pair_term<KERNEL, POT>(xs - q.x, ys - q.y, zs - q.z, h2, hinv, hinv3, nx, ny, nz, np,
+                                 true);
+        }
+      }
+      unsigned heavy = __ballot_sync(0xffffffffu, k >= kLight);
+      while (heavy) {
+        const int L = __ffs(heavy) - 1;
+        heavy &= heavy - 1;
+        const float bx = __shfl_sync(0xffffffffu, xs, L), by = __shfl_sync(0xffffffffu, ys, L),
+                    bz = __shfl_sync(0xffffffffu, zs, L);
+        const uint32_t b0 = __shfl_sync(0xffffffffu, jb[u], L),
+                       b1 = __shfl_sync(0xffffffffu, je[u], L);
+        float ax = 0.f, ay = 0.f, az = 0.f, ap = 0.f;
+        for (uint32_t jj = b0; jj < b1; jj += 32) {
+          const bool on = jj + lane < b1;
+          const float4 q = __ldg(src + (on ? jj + lane : b0));
+          pair_term<KERNEL, POT>(bx - q.x, by - q.y, bz - q.z, h2, hinv, hinv3, ax, ay, az, ap,
+                                 on);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          ax += __shfl_xor_sync(0xffffffffu, ax, o);
+          ay += __shfl_xor_sync(0xffffffffu, ay, o);
+          az += __shfl_xor_sync(0xffffffffu, az, o);
+          if (POT) ap += __shfl_xor_sync(0xffffffffu, ap, o);
+        }
+        if (lane == L) {
+          nx += ax;
+          ny += ay;
+          nz += az;
+          np += ap;
         }
       }
     }
+  }
+  if (act) {
+    float fx = 0.f, fy = 0.f, fz = 0.f, ph = 0.f;
+    l2p<P>(grid, C, ((int64_t)cx * M + cy) * M + cz, si.x, si.y, si.z, fx, fy, fz, ph);
     ofx[i] = GM * (fx + nx);
     ofy[i] = GM * (fy + ny);
     ofz[i] = GM * (fz + nz);
     if (POT) opot[i] = GM * (ph + np);
   }
   // warp-summed interaction count
-  unsigned long long c = nsrc;
+  unsigned long long c = act ? nsrc : 0;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-  if ((threadIdx.x & 31) == 0 && c && inter) atomicAdd(inter, c);
+  if (lane == 0 && c && inter) atomicAdd(inter, c);
 }
 
 __device__ __forceinline__ int ceil_log2_exact(float v) {
@@ -414,15 +347,6 @@ int launch_forces_t(ct2g_ctx *ctx) {
         ctx->fy, ctx->fz, ctx->pot, ctx->d_inter);
     CT2G_LAUNCHED(ctx);
   }
-  if (ctx->nheavy) {
-    const unsigned T = 128;
-    const size_t threads = (size_t)ctx->nheavy * 32;
-    forces_heavy_kernel<P, K, POT><<<ct2g_div_up(threads, T), T, 0, ctx->stream>>>(
-        ctx->heavy_list, ctx->nheavy, ctx->cell_start, ctx->keys, (uint32_t)ctx->rung_begin,
-        ctx->src, ctx->grid, ctx->mbits, ctx->nstencil, ctx->opt.hsoft, ctx->opt.GM, ctx->fx,
-        ctx->fy, ctx->fz, ctx->pot, ctx->d_inter);
-    CT2G_LAUNCHED(ctx);
-  }
   if (ctx->nsparse) {
     const unsigned T = 128;
     forces_sparse_kernel<P, K, POT><<<ct2g_div_up(ctx->nsparse, T), T, 0, ctx->stream>>>(
@@ -459,7 +383,7 @@ int ct2g_forces(ct2g_ctx *ctx, bool pot) {
   CT2G_CUDA(ctx, cudaMemsetAsync(ctx->fz, 0, n * 4, ctx->stream));
   if (pot) CT2G_CUDA(ctx, cudaMemsetAsync(ctx->pot, 0, n * 4, ctx->stream));
   CT2G_CUDA(ctx, cudaMemsetAsync(ctx->d_inter, 0, sizeof(unsigned long long), ctx->stream));
-  if (ctx->nchunks == 0 && ctx->nsparse == 0 && ctx->nheavy == 0) return CT2G_OK;
+  if (ctx->nchunks == 0 && ctx->nsparse == 0) return CT2G_OK;
   switch (ctx->p) {
     case 1: return launch_forces_p<1>(ctx, pot);
     case 2: return launch_forces_p<2>(ctx, pot);
