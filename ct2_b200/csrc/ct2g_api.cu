@@ -169,6 +169,8 @@ int ct2g_alloc_particles(ct2g_ctx *ctx, size_t n) {
 
 int ct2g_alloc_mesh(ct2g_ctx *ctx) {
   CT2G_CUDA(ctx, cudaMalloc(&ctx->cell_start, sizeof(uint32_t) * (ctx->C + 1)));
+  CT2G_CUDA(ctx, cudaMalloc(&ctx->occ, sizeof(unsigned long long) * (ctx->C / 64)));
+  CT2G_CUDA(ctx, cudaMalloc(&ctx->stmask, sizeof(unsigned long long) * 64 * 27));
   CT2G_CUDA(ctx, cudaMalloc(&ctx->grid, sizeof(float) * ctx->nc * ctx->C));
   CT2G_CUDA(ctx, cudaMalloc(&ctx->spec, sizeof(float2) * ctx->nc * ctx->CK));
   CT2G_CUDA(ctx, cudaMalloc(&ctx->greens, sizeof(float) * ctx->nc * ctx->CK));
@@ -261,6 +263,31 @@ int ct2g_create(const ct2g_options *opt, ct2g_ctx **out) {
           }
     ctx->nstencil = (int)(st.size() / 4);
     if ((rc = ct2g_upload_stencil(ctx, st)) != CT2G_OK) break;
+    // stencil bits per (in-block Morton position p, block offset (dX,dY,dZ)):
+    // cells b of the neighbouring 4x4x4 block with |4 d + pos(b) - pos(p)|^2 <= bwidth^2
+    {
+      std::vector<unsigned long long> m(64 * 27, 0ull);
+      auto pos = [](int b, int &x, int &y, int &z) {
+        x = ((b >> 2) & 1) | ((b >> 4) & 2);
+        y = ((b >> 1) & 1) | ((b >> 3) & 2);
+        z = (b & 1) | ((b >> 2) & 2);
+      };
+      for (int p = 0; p < 64; p++) {
+        int px, py, pz;
+        pos(p, px, py, pz);
+        for (int o = 0; o < 27; o++) {
+          const int dX = o / 9 - 1, dY = (o / 3) % 3 - 1, dZ = o % 3 - 1;
+          for (int b = 0; b < 64; b++) {
+            int bx, by, bz;
+            pos(b, bx, by, bz);
+            const int ox = 4 * dX + bx - px, oy = 4 * dY + by - py, oz = 4 * dZ + bz - pz;
+            if ((double)(ox * ox + oy * oy + oz * oz) <= bw2) m[p * 27 + o] |= 1ull << b;
+          }
+        }
+      }
+      if (cudaMemcpy(ctx->stmask, m.data(), sizeof(unsigned long long) * m.size(),
+                     cudaMemcpyHostToDevice) != cudaSuccess) { rc = CT2G_ECUDA; break; }
+    }
     if (opt->max_particles && (rc = ct2g_alloc_particles(ctx, opt->max_particles)) != CT2G_OK) break;
     if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) { rc = CT2G_ECUDA; break; }
   } while (0);
@@ -278,7 +305,8 @@ int ct2g_destroy(ct2g_ctx *ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   free_particles(ctx);
-  void *ptrs[] = {ctx->cell_start, ctx->grid, ctx->spec, ctx->greens, ctx->tw32, ctx->tw64,
+  void *ptrs[] = {ctx->cell_start, ctx->occ, ctx->stmask, ctx->grid, ctx->spec, ctx->greens,
+                  ctx->tw32, ctx->tw64,
                   ctx->d_maxrung, ctx->d_inter, ctx->scan_tmp};
   for (void *p : ptrs)
     if (p) cudaFree(p);

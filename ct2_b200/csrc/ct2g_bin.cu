@@ -265,6 +265,24 @@ __global__ void chunk_fill_kernel(const uint32_t *__restrict__ flags,
   if (flags[i]) list[fscan[i]] = (uint32_t)(begin + i);
 }
 
+// occupancy of every 4x4x4 cell block: a block is 64 consecutive Morton keys,
+// bit b of word w set when cell 64w+b holds a particle of the range
+__global__ void occupancy_kernel(const uint32_t *__restrict__ cs, size_t nwords,
+                                 unsigned long long *__restrict__ occ) {
+  const size_t w = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= nwords) return;
+  const uint32_t *c = cs + 64 * w;
+  unsigned long long bits = 0;
+  uint32_t prev = c[0];
+#pragma unroll 8
+  for (int b = 0; b < 64; b++) {
+    const uint32_t next = c[b + 1];
+    if (next > prev) bits |= 1ull << b;
+    prev = next;
+  }
+  occ[w] = bits;
+}
+
 }  // namespace
 
 // exclusive scan of n uint32 values (in may equal out); optional host total
@@ -364,6 +382,9 @@ int ct2g_bin_range(ct2g_ctx *ctx) {
     std::swap(ctx->vz, ctx->vz2);
     std::swap(ctx->rung, ctx->rung2);
     std::swap(ctx->id, ctx->id2);
+    occupancy_kernel<<<ct2g_div_up(ctx->C / 64, T), T, 0, st>>>(ctx->cell_start, ctx->C / 64,
+                                                               ctx->occ);
+    CT2G_LAUNCHED(ctx);
     // sink work lists: warp chunks of dense cells, single sinks of sparse ones
     chunk_flag_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(ctx->keys, ctx->cell_start, begin, nr,
                                                         ctx->flags, ctx->vals);
@@ -385,6 +406,7 @@ int ct2g_bin_range(ct2g_ctx *ctx) {
     std::vector<uint32_t> h(ctx->C + 1, v);
     CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->cell_start, h.data(), sizeof(uint32_t) * h.size(),
                                    cudaMemcpyHostToDevice, st));
+    CT2G_CUDA(ctx, cudaMemsetAsync(ctx->occ, 0, sizeof(unsigned long long) * (ctx->C / 64), st));
     CT2G_CUDA(ctx, cudaStreamSynchronize(st));
     ctx->nchunks = 0;
     ctx->nsparse = 0;

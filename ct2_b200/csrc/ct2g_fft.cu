@@ -337,6 +337,67 @@ __global__ void __launch_bounds__(256, 3) fft_cols_kernel(C2 *__restrict__ a, si
   }
 }
 
+// Persistent, double-buffered form of the column pass for 16-byte aligned
+// rows: each block walks tiles blockIdx.x, blockIdx.x + gridDim.x, ...; the
+// next tile is copied into the second smem buffer with cp.async while the
+// current one is transformed and written back.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int NPEND>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(NPEND) : "memory");
+}
+
+template <typename C2, int N, int W, bool INV>
+__global__ void __launch_bounds__(256, 2) fft_cols_pipe_kernel(C2 *__restrict__ a, size_t ostride,
+                                                               size_t rstride, size_t ncols,
+                                                               int ntiles, size_t ntot,
+                                                               const C2 *__restrict__ tw) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C2 *stw = reinterpret_cast<C2 *>(smraw);
+  C2 *buf[2] = {stw + N, stw + N + N * W};
+  load_twiddles(stw, tw, N);
+  constexpr int CPC = 16 / sizeof(C2);  // complex per 16-byte chunk
+  constexpr int CH = W / CPC;           // chunks per row
+  auto issue = [&](size_t tile, C2 *s) {
+    const size_t outer = tile / ntiles;
+    const size_t col0 = (size_t)(tile % ntiles) * W;
+    const int wv = (int)min((size_t)W, ncols - col0);
+    const C2 *base = a + outer * ostride + col0;
+#pragma unroll 4
+    for (int e = threadIdx.x; e < N * CH; e += 256) {
+      const int r = e / CH, c = (e % CH) * CPC;
+      if (c < wv) cp_async16(s + r * W + c, base + (size_t)r * rstride + c);
+    }
+  };
+  size_t tile = blockIdx.x;
+  if (tile < ntot) issue(tile, buf[0]);
+  cp_async_commit();
+  for (int it = 0; tile < ntot; it++, tile += gridDim.x) {
+    C2 *s = buf[it & 1];
+    const size_t next = tile + gridDim.x;
+    if (next < ntot) issue(next, buf[(it + 1) & 1]);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    tile_fft<N, false, C2, INV>(s, W, W, stw);
+    const size_t outer = tile / ntiles;
+    const size_t col0 = (size_t)(tile % ntiles) * W;
+    const int wv = (int)min((size_t)W, ncols - col0);
+    C2 *base = a + outer * ostride + col0;
+#pragma unroll 4
+    for (int e = threadIdx.x; e < N * CH; e += 256) {
+      const int r = e / CH, c = (e % CH) * CPC;
+      if (c < wv) *reinterpret_cast<float4 *>(base + (size_t)r * rstride + c) = *reinterpret_cast<const float4 *>(s + r * W + c);
+    }
+    __syncthreads();  // this buffer is refilled two tiles later
+  }
+  cp_async_wait<0>();
+}
+
 template <typename C2>
 const C2 *twiddle_ptr(ct2g_ctx *ctx);
 template <>
@@ -349,6 +410,20 @@ int launch_cols(ct2g_ctx *ctx, typename Cplx<T>::type *spec, size_t nouter, size
                 size_t rstride, size_t ncols) {
   using C2 = typename Cplx<T>::type;
   constexpr int W = N >= 256 ? 16 : 4096 / N;
+  if (VEC && N >= 64) {
+    const size_t smem = sizeof(C2) * ((size_t)N + 2 * (size_t)N * W);
+    auto k = fft_cols_pipe_kernel<C2, N, W, INV>;
+    CT2G_CUDA(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    CT2G_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 256, smem));
+    const int ntiles = (int)((ncols + W - 1) / W);
+    const size_t ntot = nouter * ntiles;
+    const size_t grid = std::min(ntot, (size_t)std::max(1, per_sm) * ctx->num_sms);
+    k<<<(unsigned)grid, 256, smem, ctx->stream>>>(spec, ostride, rstride, ncols, ntiles, ntot,
+                                                  twiddle_ptr<C2>(ctx));
+    CT2G_LAUNCHED(ctx);
+    return CT2G_OK;
+  }
   const size_t smem = sizeof(C2) * ((size_t)N + (size_t)N * W);
   auto k = fft_cols_kernel<C2, N, W, INV, VEC>;
   CT2G_CUDA(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

@@ -107,6 +107,8 @@ struct ct2g_ctx {
   uint32_t *scan_tmp = nullptr;
   size_t scan_tmp_words = 0;
   uint32_t *cell_start = nullptr;  // [C+1] indexed by Morton key, absolute indices
+  unsigned long long *occ = nullptr;  // [C/64] occupancy bits of 4x4x4 cell blocks
+  unsigned long long *stmask = nullptr;  // [64][27] stencil bits per (in-block cell, block offset)
   float4 *src = nullptr;           // per sorted particle: offset from own cell centre
   uint32_t *chunk_begin = nullptr; // sink chunks (<=32 particles of one dense cell)
   uint32_t *sparse_list = nullptr; // isolated sinks, one per thread

@@ -54,105 +54,29 @@ __device__ __forceinline__ void l2p(const float *__restrict__ grid, int64_t C, i
   pot = ph;
 }
 
-template <int P, int KERNEL, bool POT>
-__global__ void __launch_bounds__(256) forces_kernel(
-    const uint32_t *__restrict__ chunk_begin, uint32_t nchunks, const uint32_t *__restrict__ cs,
-    const uint32_t *__restrict__ skeys, uint32_t rbegin, const float4 *__restrict__ src,
-    const float *__restrict__ grid, int mbits, int nstencil, float soft, float GM,
-    float *__restrict__ ofx, float *__restrict__ ofy, float *__restrict__ ofz,
-    float *__restrict__ opot, unsigned long long *__restrict__ inter) {
-  __shared__ float4 sbuf[8][32];  // one batch of 32 sources per warp
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const uint32_t ch = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (ch >= nchunks) return;
-  const int M = 1 << mbits;
-  const int64_t C = (int64_t)M * M * M;
-  const uint32_t b = chunk_begin[ch];
-  const uint32_t key = skeys[b - rbegin];  // Morton key of the sink cell
-  const uint32_t cend = min(cs[key + 1], b + 32u);
-  const uint32_t i = b + lane;
-  const bool act = i < cend;
-  const float4 si = src[act ? i : b];
-  const int cx = (int)ct2g_compact3(key >> 2), cy = (int)ct2g_compact3(key >> 1),
-            cz = (int)ct2g_compact3(key);
-  const int64_t cell = ((int64_t)cx * M + cy) * M + cz;  // row-major grid index
-  float fx = 0.f, fy = 0.f, fz = 0.f, ph = 0.f;
-  l2p<P>(grid, C, cell, si.x, si.y, si.z, fx, fy, fz, ph);
-  const float hc = 1.0f / (float)M;
-  const float h2 = soft * soft, hinv = 1.f / soft, hinv3 = hinv * hinv * hinv;
-  float nx = 0.f, ny = 0.f, nz = 0.f, np = 0.f;
-  uint32_t nsrc = 0;
-  float4 *sb = sbuf[wib];
-  for (int s0 = 0; s0 < nstencil; s0 += 32) {
-    // 32 neighbour ranges fetched at once, one per lane
-    uint32_t jb = 0, je = 0;
-    const int sl = s0 + lane;
-    if (sl < nstencil) {
-      const uint32_t nb = ct2g_morton((uint32_t)((cx + c_stencil[4 * sl]) & (M - 1)),
-                                      (uint32_t)((cy + c_stencil[4 * sl + 1]) & (M - 1)),
-                                      (uint32_t)((cz + c_stencil[4 * sl + 2]) & (M - 1)));
-      jb = cs[nb];
-      je = cs[nb + 1];
-    }
-    const int nt = min(32, nstencil - s0);
-    for (int t = 0; t < nt; t++) {
-      const uint32_t j0 = __shfl_sync(0xffffffffu, jb, t), j1 = __shfl_sync(0xffffffffu, je, t);
-      if (j0 == j1) continue;
-      nsrc += j1 - j0;
-      const int st = s0 + t;
-      // sink position relative to the neighbour cell's centre
-      const float xs = si.x - (float)c_stencil[4 * st] * hc;
-      const float ys = si.y - (float)c_stencil[4 * st + 1] * hc;
-      const float zs = si.z - (float)c_stencil[4 * st + 2] * hc;
-      for (uint32_t jj = j0; jj < j1; jj += 32) {
-        const int cnt = (int)min(32u, j1 - jj);
-        __syncwarp();
-        if (lane < cnt) sb[lane] = __ldg(src + jj + lane);
-        __syncwarp();
-#pragma unroll 8
-        for (int u = 0; u < cnt; u++) {
-          const float4 q = sb[u];
-          const float dx = xs - q.x, dy = ys - q.y, dz = zs - q.z;
-          const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-          float g;
-          if (KERNEL == CT2G_SOFT_PLUMMER) {
-            const float ri = rsqrtf(r2 + h2);
-            g = ri * ri * ri;
-            if (POT) np -= ri;
-          } else {
-            if (r2 < h2) {
-              g = hinv3;
-              if (POT) np -= 1.5f * hinv - 0.5f * r2 * hinv3;
-            } else {
-              const float ri = rsqrtf(r2);
-              g = ri * ri * ri;
-              if (POT) np -= ri;
-            }
-          }
-          nx = fmaf(-dx, g, nx);
-          ny = fmaf(-dy, g, ny);
-          nz = fmaf(-dz, g, nz);
-        }
-      }
-    }
-  }
-  if (act) {
-    ofx[i] = GM * (fx + nx);
-    ofy[i] = GM * (fy + ny);
-    ofz[i] = GM * (fz + nz);
-    if (POT) opot[i] = GM * (ph + np);
-  }
-  if (lane == 0 && inter) atomicAdd(inter, (unsigned long long)(cend - b) * nsrc);
-}
+// ---------------------------------------------------------------------------
+// Near-field neighbour walk.  The stencil (offsets |o|^2 <= bwidth^2, bwidth
+// <= 4) of a cell touches the 27 4x4x4 cell blocks around its own; a block
+// is 64 consecutive Morton keys, so its occupancy is one 64-bit word.  For
+// the cell at in-block position p and block offset o, stmask[p*27+o] holds
+// the stencil cells of that block; occ & stmask lists exactly the occupied
+// stencil cells.  Neighbour block keys come from dilated (bit-interleaved)
+// addition, which wraps periodically by itself.
+// ---------------------------------------------------------------------------
+__constant__ uint32_t c_doff[27 * 3];  // dilated block offsets, x/y/z lanes of the key
 
-// Thread-per-sink near field for sinks of sparse cells (fewer than 16
-// particles).  Every lane walks its own stencil (neighbouring lanes are
-// neighbouring sinks, so source loads mostly hit L1).  A neighbour cell with
-// fewer than kLight sources is consumed by the lane alone; a heavier one (a
-// cluster core next to a halo sink) is consumed by the whole warp: lanes take
-// 32 sources at a time against the owning lane's sink, and a warp reduction
-// hands the sum to the owner, so no lane idles through a long private loop.
-constexpr uint32_t kLight = 24;
+struct Walk {
+  uint32_t mx, my, mz;  // block-key masks of the x, y, z bits
+  __device__ __forceinline__ uint32_t add(uint32_t sb, int o) const {
+    const uint32_t x = ((sb | ~mx) + c_doff[3 * o]) & mx;
+    const uint32_t y = ((sb | ~my) + c_doff[3 * o + 1]) & my;
+    const uint32_t z = ((sb | ~mz) + c_doff[3 * o + 2]) & mz;
+    return x | y | z;
+  }
+};
+
+// minimum-image offset (in cells) from cell c to cell n along one axis
+__device__ __forceinline__ int wrap_off(int n, int c, int M) { return ((n - c + M / 2) & (M - 1)) - M / 2; }
 
 template <int KERNEL, bool POT>
 __device__ __forceinline__ void pair_term(float dx, float dy, float dz, float h2, float hinv,
@@ -181,16 +105,105 @@ __device__ __forceinline__ void pair_term(float dx, float dy, float dz, float h2
   if (POT) ap -= pp;
 }
 
+// Dense cells: one warp per chunk of <= 32 sinks of one cell; every occupied
+// stencil cell is a warp-uniform range whose sources are staged 32 at a time
+// in shared memory and read back as broadcasts.
+template <int P, int KERNEL, bool POT>
+__global__ void __launch_bounds__(256) forces_kernel(
+    const uint32_t *__restrict__ chunk_begin, uint32_t nchunks, const uint32_t *__restrict__ cs,
+    const unsigned long long *__restrict__ occ, const unsigned long long *__restrict__ stmask,
+    Walk walk, const uint32_t *__restrict__ skeys, uint32_t rbegin,
+    const float4 *__restrict__ src, const float *__restrict__ grid, int mbits, float soft,
+    float GM, float *__restrict__ ofx, float *__restrict__ ofy, float *__restrict__ ofz,
+    float *__restrict__ opot, unsigned long long *__restrict__ inter) {
+  __shared__ float4 sbuf[8][32];  // one batch of 32 sources per warp
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const uint32_t ch = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (ch >= nchunks) return;
+  const int M = 1 << mbits;
+  const int64_t C = (int64_t)M * M * M;
+  const uint32_t b = chunk_begin[ch];
+  const uint32_t key = skeys[b - rbegin];  // Morton key of the sink cell
+  const uint32_t cend = min(cs[key + 1], b + 32u);
+  const uint32_t i = b + lane;
+  const bool act = i < cend;
+  const float4 si = src[act ? i : b];
+  const int cx = (int)ct2g_compact3(key >> 2), cy = (int)ct2g_compact3(key >> 1),
+            cz = (int)ct2g_compact3(key);
+  const float hc = 1.0f / (float)M;
+  const float h2 = soft * soft, hinv = 1.f / soft, hinv3 = hinv * hinv * hinv;
+  float nx = 0.f, ny = 0.f, nz = 0.f, np = 0.f;
+  uint32_t nsrc = 0;
+  float4 *sb = sbuf[wib];
+  // the 27 neighbour-block words, one per lane, then broadcast
+  const uint32_t p = key & 63u, blk = key >> 6;
+  unsigned long long word = 0;
+  uint32_t nblk = 0;
+  if (lane < 27) {
+    nblk = walk.add(blk, lane);
+    word = occ[nblk] & __ldg(stmask + p * 27 + lane);
+  }
+  for (int o = 0; o < 27; o++) {
+    unsigned long long bits = __shfl_sync(0xffffffffu, word, o);
+    const uint32_t nb = __shfl_sync(0xffffffffu, nblk, o);
+    while (bits) {
+      const int bb = __ffsll((long long)bits) - 1;
+      bits &= bits - 1;
+      const uint32_t ck = (nb << 6) | (uint32_t)bb;
+      const uint32_t j0 = cs[ck], j1 = cs[ck + 1];
+      nsrc += j1 - j0;
+      const int ox = wrap_off((int)ct2g_compact3(ck >> 2), cx, M);
+      const int oy = wrap_off((int)ct2g_compact3(ck >> 1), cy, M);
+      const int oz = wrap_off((int)ct2g_compact3(ck), cz, M);
+      // sink position relative to the neighbour cell's centre
+      const float xs = si.x - (float)ox * hc, ys = si.y - (float)oy * hc, zs = si.z - (float)oz * hc;
+      for (uint32_t jj = j0; jj < j1; jj += 32) {
+        const int cnt = (int)min(32u, j1 - jj);
+        __syncwarp();
+        if (lane < cnt) sb[lane] = __ldg(src + jj + lane);
+        __syncwarp();
+#pragma unroll 8
+        for (int u = 0; u < cnt; u++) {
+          const float4 q = sb[u];
+          pair_term<KERNEL, POT>(xs - q.x, ys - q.y, zs - q.z, h2, hinv, hinv3, nx, ny, nz, np,
+                                 true);
+        }
+      }
+    }
+  }
+  float fx = 0.f, fy = 0.f, fz = 0.f, ph = 0.f;
+  l2p<P>(grid, C, ((int64_t)cx * M + cy) * M + cz, si.x, si.y, si.z, fx, fy, fz, ph);
+  if (act) {
+    ofx[i] = GM * (fx + nx);
+    ofy[i] = GM * (fy + ny);
+    ofz[i] = GM * (fz + nz);
+    if (POT) opot[i] = GM * (ph + np);
+  }
+  if (lane == 0 && inter) atomicAdd(inter, (unsigned long long)(cend - b) * nsrc);
+}
+
+// Sparse cells (fewer than 16 particles): one thread per sink, each walking
+// its own occupied stencil cells.  A neighbour with fewer than kLight
+// sources is consumed by the lane alone; heavier ones (a cluster core beside
+// a halo sink) are queued in shared memory and consumed afterwards by the
+// whole warp -- lanes take 32 sources at a time against the owning lane's
+// sink, and a warp reduction hands the sum back -- so no lane idles through
+// a long private loop.
+constexpr uint32_t kLight = 24;
+constexpr int kQueue = 16;
+
 template <int P, int KERNEL, bool POT>
 __global__ void __launch_bounds__(128) forces_sparse_kernel(
     const uint32_t *__restrict__ sinks, uint32_t nsinks, const uint32_t *__restrict__ cs,
-    const uint32_t *__restrict__ skeys, uint32_t rbegin, const float4 *__restrict__ src,
-    const float *__restrict__ grid, int mbits, int nstencil, float soft, float GM,
-    float *__restrict__ ofx, float *__restrict__ ofy, float *__restrict__ ofz,
+    const unsigned long long *__restrict__ occ, const unsigned long long *__restrict__ stmask,
+    Walk walk, const uint32_t *__restrict__ skeys, uint32_t rbegin,
+    const float4 *__restrict__ src, const float *__restrict__ grid, int mbits, float soft,
+    float GM, float *__restrict__ ofx, float *__restrict__ ofy, float *__restrict__ ofz,
     float *__restrict__ opot, unsigned long long *__restrict__ inter) {
+  __shared__ uint32_t queue[kQueue][128];
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
-  if ((t & ~31u) >= nsinks) return;  // whole warps only: the loop below shuffles
+  if ((t & ~31u) >= nsinks) return;  // whole warps only: the queue phase shuffles
   const bool act = t < nsinks;
   const int M = 1 << mbits;
   const int64_t C = (int64_t)M * M * M;
@@ -203,60 +216,71 @@ __global__ void __launch_bounds__(128) forces_sparse_kernel(
   const float h2 = soft * soft, hinv = 1.f / soft, hinv3 = hinv * hinv * hinv;
   float nx = 0.f, ny = 0.f, nz = 0.f, np = 0.f;
   uint32_t nsrc = 0;
-  for (int s0 = 0; s0 < nstencil; s0 += 4) {
-    uint32_t jb[4], je[4];
-#pragma unroll
-    for (int u = 0; u < 4; u++) {
-      const int s = min(s0 + u, nstencil - 1);
-      const uint32_t nb = ct2g_morton((uint32_t)((cx + c_stencil[4 * s]) & (M - 1)),
-                                      (uint32_t)((cy + c_stencil[4 * s + 1]) & (M - 1)),
-                                      (uint32_t)((cz + c_stencil[4 * s + 2]) & (M - 1)));
-      jb[u] = cs[nb];
-      je[u] = (act && s0 + u < nstencil) ? cs[nb + 1] : jb[u];
-    }
-#pragma unroll
-    for (int u = 0; u < 4; u++) {
-      const int s = min(s0 + u, nstencil - 1);
-      const uint32_t k = je[u] - jb[u];
-      nsrc += k;
-      const float xs = si.x - (float)c_stencil[4 * s] * hc;
-      const float ys = si.y - (float)c_stencil[4 * s + 1] * hc;
-      const float zs = si.z - (float)c_stencil[4 * s + 2] * hc;
-      if (k < kLight) {
-        for (uint32_t j = jb[u]; j < je[u]; j++) {
+  int nq = 0;
+  const uint32_t p = key & 63u, blk = key >> 6;
+  if (act) {
+    for (int o = 0; o < 27; o++) {
+      const uint32_t nb = walk.add(blk, o);
+      unsigned long long bits = occ[nb] & __ldg(stmask + p * 27 + o);
+      while (bits) {
+        const int bb = __ffsll((long long)bits) - 1;
+        bits &= bits - 1;
+        const uint32_t ck = (nb << 6) | (uint32_t)bb;
+        const uint32_t j0 = cs[ck], j1 = cs[ck + 1];
+        nsrc += j1 - j0;
+        if (j1 - j0 >= kLight && nq < kQueue) {
+          queue[nq++][threadIdx.x] = ck;
+          continue;
+        }
+        const float xs = si.x - (float)wrap_off((int)ct2g_compact3(ck >> 2), cx, M) * hc;
+        const float ys = si.y - (float)wrap_off((int)ct2g_compact3(ck >> 1), cy, M) * hc;
+        const float zs = si.z - (float)wrap_off((int)ct2g_compact3(ck), cz, M) * hc;
+        for (uint32_t j = j0; j < j1; j++) {
           const float4 q = __ldg(src + j);
           pair_term<KERNEL, POT>(xs - q.x, ys - q.y, zs - q.z, h2, hinv, hinv3, nx, ny, nz, np,
                                  true);
         }
       }
-      unsigned heavy = __ballot_sync(0xffffffffu, k >= kLight);
-      while (heavy) {
-        const int L = __ffs(heavy) - 1;
-        heavy &= heavy - 1;
-        const float bx = __shfl_sync(0xffffffffu, xs, L), by = __shfl_sync(0xffffffffu, ys, L),
-                    bz = __shfl_sync(0xffffffffu, zs, L);
-        const uint32_t b0 = __shfl_sync(0xffffffffu, jb[u], L),
-                       b1 = __shfl_sync(0xffffffffu, je[u], L);
-        float ax = 0.f, ay = 0.f, az = 0.f, ap = 0.f;
-        for (uint32_t jj = b0; jj < b1; jj += 32) {
-          const bool on = jj + lane < b1;
-          const float4 q = __ldg(src + (on ? jj + lane : b0));
-          pair_term<KERNEL, POT>(bx - q.x, by - q.y, bz - q.z, h2, hinv, hinv3, ax, ay, az, ap,
-                                 on);
-        }
+    }
+  }
+  // queued heavy cells, one per lane per round, each consumed by the warp
+  for (;;) {
+    const unsigned pending = __ballot_sync(0xffffffffu, nq > 0);
+    if (!pending) break;
+    uint32_t mine = 0;
+    float mx = 0.f, my = 0.f, mz = 0.f;
+    if (nq > 0) {
+      mine = queue[--nq][threadIdx.x];
+      mx = si.x - (float)wrap_off((int)ct2g_compact3(mine >> 2), cx, M) * hc;
+      my = si.y - (float)wrap_off((int)ct2g_compact3(mine >> 1), cy, M) * hc;
+      mz = si.z - (float)wrap_off((int)ct2g_compact3(mine), cz, M) * hc;
+    }
+    unsigned todo = pending;
+    while (todo) {
+      const int L = __ffs(todo) - 1;
+      todo &= todo - 1;
+      const uint32_t ck = __shfl_sync(0xffffffffu, mine, L);
+      const float bx = __shfl_sync(0xffffffffu, mx, L), by = __shfl_sync(0xffffffffu, my, L),
+                  bz = __shfl_sync(0xffffffffu, mz, L);
+      const uint32_t b0 = cs[ck], b1 = cs[ck + 1];
+      float ax = 0.f, ay = 0.f, az = 0.f, ap = 0.f;
+      for (uint32_t jj = b0; jj < b1; jj += 32) {
+        const bool on = jj + lane < b1;
+        const float4 q = __ldg(src + (on ? jj + lane : b0));
+        pair_term<KERNEL, POT>(bx - q.x, by - q.y, bz - q.z, h2, hinv, hinv3, ax, ay, az, ap, on);
+      }
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-          ax += __shfl_xor_sync(0xffffffffu, ax, o);
-          ay += __shfl_xor_sync(0xffffffffu, ay, o);
-          az += __shfl_xor_sync(0xffffffffu, az, o);
-          if (POT) ap += __shfl_xor_sync(0xffffffffu, ap, o);
-        }
-        if (lane == L) {
-          nx += ax;
-          ny += ay;
-          nz += az;
-          np += ap;
-        }
+      for (int o = 16; o > 0; o >>= 1) {
+        ax += __shfl_xor_sync(0xffffffffu, ax, o);
+        ay += __shfl_xor_sync(0xffffffffu, ay, o);
+        az += __shfl_xor_sync(0xffffffffu, az, o);
+        if (POT) ap += __shfl_xor_sync(0xffffffffu, ap, o);
+      }
+      if (lane == L) {
+        nx += ax;
+        ny += ay;
+        nz += az;
+        np += ap;
       }
     }
   }
@@ -268,7 +292,6 @@ __global__ void __launch_bounds__(128) forces_sparse_kernel(
     ofz[i] = GM * (fz + nz);
     if (POT) opot[i] = GM * (ph + np);
   }
-  // warp-summed interaction count
   unsigned long long c = act ? nsrc : 0;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
@@ -336,23 +359,34 @@ __global__ void drift_kernel(size_t n, uint32_t *__restrict__ x, uint32_t *__res
   z[i] += (uint32_t)__float2ll_rz(__fmul_rn(__fmul_rn(vz[i], lambda), two32));
 }
 
+Walk make_walk(int mbits) {
+  Walk w{0u, 0u, 0u};
+  for (int i = 0; i < mbits - 2; i++) {
+    w.mx |= 1u << (3 * i + 2);
+    w.my |= 1u << (3 * i + 1);
+    w.mz |= 1u << (3 * i);
+  }
+  return w;
+}
+
 template <int P, int K, bool POT>
 int launch_forces_t(ct2g_ctx *ctx) {
+  const Walk walk = make_walk(ctx->mbits);
   if (ctx->nchunks) {
     const unsigned T = 256;
     const size_t threads = (size_t)ctx->nchunks * 32;
     forces_kernel<P, K, POT><<<ct2g_div_up(threads, T), T, 0, ctx->stream>>>(
-        ctx->chunk_begin, ctx->nchunks, ctx->cell_start, ctx->keys, (uint32_t)ctx->rung_begin,
-        ctx->src, ctx->grid, ctx->mbits, ctx->nstencil, ctx->opt.hsoft, ctx->opt.GM, ctx->fx,
-        ctx->fy, ctx->fz, ctx->pot, ctx->d_inter);
+        ctx->chunk_begin, ctx->nchunks, ctx->cell_start, ctx->occ, ctx->stmask, walk, ctx->keys,
+        (uint32_t)ctx->rung_begin, ctx->src, ctx->grid, ctx->mbits, ctx->opt.hsoft, ctx->opt.GM,
+        ctx->fx, ctx->fy, ctx->fz, ctx->pot, ctx->d_inter);
     CT2G_LAUNCHED(ctx);
   }
   if (ctx->nsparse) {
     const unsigned T = 128;
     forces_sparse_kernel<P, K, POT><<<ct2g_div_up(ctx->nsparse, T), T, 0, ctx->stream>>>(
-        ctx->sparse_list, ctx->nsparse, ctx->cell_start, ctx->keys, (uint32_t)ctx->rung_begin,
-        ctx->src, ctx->grid, ctx->mbits, ctx->nstencil, ctx->opt.hsoft, ctx->opt.GM, ctx->fx,
-        ctx->fy, ctx->fz, ctx->pot, ctx->d_inter);
+        ctx->sparse_list, ctx->nsparse, ctx->cell_start, ctx->occ, ctx->stmask, walk, ctx->keys,
+        (uint32_t)ctx->rung_begin, ctx->src, ctx->grid, ctx->mbits, ctx->opt.hsoft, ctx->opt.GM,
+        ctx->fx, ctx->fy, ctx->fz, ctx->pot, ctx->d_inter);
     CT2G_LAUNCHED(ctx);
   }
   return CT2G_OK;
@@ -372,6 +406,18 @@ int launch_forces_p(ct2g_ctx *ctx, bool pot) {
 int ct2g_upload_stencil(ct2g_ctx *ctx, const std::vector<int> &st4) {
   CT2G_CUDA(ctx, cudaMemcpyToSymbolAsync(c_stencil, st4.data(), sizeof(int) * st4.size(), 0,
                                          cudaMemcpyHostToDevice, ctx->stream));
+  // dilated block offsets for the 27 neighbouring 4x4x4 blocks
+  const int nb = ctx->mbits - 2;
+  uint32_t d[27 * 3];
+  for (int o = 0; o < 27; o++) {
+    const int dd[3] = {o / 9 - 1, (o / 3) % 3 - 1, o % 3 - 1};
+    for (int a = 0; a < 3; a++) {
+      const uint32_t v = (uint32_t)dd[a] & ((1u << nb) - 1u);
+      d[3 * o + a] = ct2g_spread3(v) << (2 - a);
+    }
+  }
+  CT2G_CUDA(ctx, cudaMemcpyToSymbolAsync(c_doff, d, sizeof(d), 0, cudaMemcpyHostToDevice,
+                                         ctx->stream));
   return CT2G_OK;
 }
 
