@@ -106,23 +106,18 @@ int ensure_grid(ct2g_ctx *ctx) {
   return CT2G_OK;
 }
 
-int ensure_expansions(ct2g_ctx *ctx) {
+// far field of the current range into the force buffers: moments (if the
+// grid does not hold them), then the mesh solve whose inverse z pass
+// evaluates L2P for every particle (the moments stay in the grid)
+int far_field(ct2g_ctx *ctx, bool pot) {
   CT2G_TRY(ensure_grid(ctx));
-  if (!ctx->moments_valid && !ctx->expansions_valid) {
-    cudaEventRecord(ctx->ev[1], ctx->stream);
+  cudaEventRecord(ctx->ev[1], ctx->stream);
+  if (!ctx->moments_valid) {
     CT2G_TRY(ct2g_p2m(ctx));
     ctx->moments_valid = true;
-  } else {
-    cudaEventRecord(ctx->ev[1], ctx->stream);
+    ctx->expansions_valid = false;
   }
-  if (!ctx->expansions_valid) {
-    CT2G_TRY(ct2g_mesh_solve(ctx));
-    ctx->moments_valid = false;  // grid now holds expansions
-    ctx->expansions_valid = true;
-  } else {
-    for (int k = 2; k <= 5; k++) cudaEventRecord(ctx->ev[k], ctx->stream);
-  }
-  return CT2G_OK;
+  return ct2g_mesh_solve(ctx, true, pot);
 }
 
 }  // namespace
@@ -439,8 +434,8 @@ int ct2g_compute_expansions(ct2g_ctx *ctx) {
   CT2G_TRY(check(ctx));
   CT2G_TRY(ensure_grid(ctx));
   if (!ctx->moments_valid) CT2G_TRY(ct2g_compute_multipoles(ctx));
-  CT2G_TRY(ct2g_mesh_solve(ctx));
-  ctx->moments_valid = false;
+  CT2G_TRY(ct2g_mesh_solve(ctx, false, false));
+  ctx->moments_valid = false;  // the grid now holds the expansions
   ctx->expansions_valid = true;
   return CT2G_OK;
 }
@@ -471,7 +466,7 @@ int ct2g_download_greens(ct2g_ctx *ctx, float *out) {
 
 int ct2g_compute_forces(ct2g_ctx *ctx) {
   CT2G_TRY(check(ctx));
-  CT2G_TRY(ensure_expansions(ctx));
+  CT2G_TRY(far_field(ctx, true));
   CT2G_TRY(ct2g_forces(ctx, true));
   ctx->forces_valid = true;
   ctx->pot_valid = true;
@@ -515,7 +510,7 @@ int ct2g_kick(ct2g_ctx *ctx, const ct2g_kick_params *p, int *max_rung) {
   CT2G_TRY(check(ctx));
   if (!p) return ct2g_fail(ctx, CT2G_EINVAL, "null kick params");
   if (p->rung < 0 || p->rung > 30) return ct2g_fail(ctx, CT2G_EINVAL, "rung out of range");
-  CT2G_TRY(ensure_expansions(ctx));
+  CT2G_TRY(far_field(ctx, false));
   CT2G_TRY(ct2g_forces(ctx, false));
   ctx->pot_valid = false;
   cudaEventRecord(ctx->ev[6], ctx->stream);

@@ -528,6 +528,89 @@ int fft_c2r(ct2g_ctx *ctx, typename Cplx<T>::type *in, T *out, int N, int batch,
   return ct2g_fail(ctx, CT2G_EINVAL, "FFT size must be a power of two in [4, 512]");
 }
 
+// ---- inverse z pass fused with L2P ------------------------------------------
+// One block per (x, y) line of the mesh, all NC expansion components: pairs of
+// components are packed into complex lines (A + iB), transformed back along z
+// in shared memory, and the block then evaluates the far field of every
+// particle of the line's cells from the expansions in shared memory.  The
+// expansion grid itself is never written to HBM.
+template <int P, int N, bool POT>
+__global__ void __launch_bounds__(256) fftz_c2r_l2p_kernel(
+    const float2 *__restrict__ spec, int ld, int64_t CK, const uint32_t *__restrict__ cs,
+    const float4 *__restrict__ src, int mbits, float GM, float *__restrict__ ofx,
+    float *__restrict__ ofy, float *__restrict__ ofz, float *__restrict__ opot,
+    const float2 *__restrict__ tw) {
+  using LL = LineLayout<N, true>;
+  constexpr int NC = ct2g_ncomp(P), NL = (NC + 1) / 2, NH = N / 2 + 1;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  float2 *stw = reinterpret_cast<float2 *>(smraw);
+  float2 *s = stw + N;
+  load_twiddles(stw, tw, N);
+  const size_t line = blockIdx.x;
+  const float2 *base = spec + line * (size_t)ld;
+  for (int e = threadIdx.x; e < NL * N; e += 256) {
+    const int l = e / N, k = e % N;
+    const bool up = k >= NH;
+    const int kk = up ? N - k : k;
+    float2 a = base[(int64_t)(2 * l) * CK + kk];
+    float2 b = (2 * l + 1 < NC) ? base[(int64_t)(2 * l + 1) * CK + kk] : make_float2(0.f, 0.f);
+    if (up) {
+      a.y = -a.y;
+      b.y = -b.y;
+    }
+    s[LL::at(l, k, 0)] = make_float2(a.x - b.y, a.y + b.x);
+  }
+  __syncthreads();
+  tile_fft<N, true, float2, true>(s, NL, 0, stw);
+  const uint32_t x = (uint32_t)(line / N), y = (uint32_t)(line % N);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int z = w; z < N; z += 8) {
+    const uint32_t key = ct2g_morton(x, y, (uint32_t)z);
+    const uint32_t b0 = cs[key], b1 = cs[key + 1];
+    if (b0 == b1) continue;
+    const auto acc = [&](int k) {
+      const float2 v = s[LL::at(k >> 1, z, 0)];
+      return (k & 1) ? v.y : v.x;
+    };
+    for (uint32_t i = b0 + lane; i < b1; i += 32) {
+      const float4 t = src[i];
+      float fx, fy, fz, ph;
+      ct2g_l2p<P>(acc, t.x, t.y, t.z, fx, fy, fz, ph);
+      ofx[i] = GM * fx;
+      ofy[i] = GM * fy;
+      ofz[i] = GM * fz;
+      if (POT) opot[i] = GM * ph;
+    }
+  }
+}
+
+template <int P, int N>
+int launch_c2r_l2p(ct2g_ctx *ctx, bool pot) {
+  constexpr int NL = (ct2g_ncomp(P) + 1) / 2;
+  const size_t smem = sizeof(float2) * ((size_t)N + (size_t)NL * LineLayout<N, true>::LS);
+  auto k = pot ? fftz_c2r_l2p_kernel<P, N, true> : fftz_c2r_l2p_kernel<P, N, false>;
+  CT2G_CUDA(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k<<<(unsigned)((size_t)N * N), 256, smem, ctx->stream>>>(
+      ctx->spec, ctx->ldk, ctx->CK, ctx->cell_start, ctx->src, ctx->mbits, ctx->opt.GM, ctx->fx,
+      ctx->fy, ctx->fz, ctx->pot, twiddle_ptr<float2>(ctx));
+  CT2G_LAUNCHED(ctx);
+  return CT2G_OK;
+}
+
+template <int P>
+int c2r_l2p_p(ct2g_ctx *ctx, bool pot) {
+  switch (ctx->M) {
+    case 8: return launch_c2r_l2p<P, 8>(ctx, pot);
+    case 16: return launch_c2r_l2p<P, 16>(ctx, pot);
+    case 32: return launch_c2r_l2p<P, 32>(ctx, pot);
+    case 64: return launch_c2r_l2p<P, 64>(ctx, pot);
+    case 128: return launch_c2r_l2p<P, 128>(ctx, pot);
+    case 256: return launch_c2r_l2p<P, 256>(ctx, pot);
+    case 512: return launch_c2r_l2p<P, 512>(ctx, pot);
+  }
+  return ct2g_fail(ctx, CT2G_EINVAL, "mesh must be a power of two in [8, 512]");
+}
+
 }  // namespace
 
 // constant twiddles of the in-register DFTs, once per context (device)
@@ -583,4 +666,28 @@ int ct2g_fft_r2c_f64(ct2g_ctx *ctx, const double *in, double2 *out, int N, int b
 }
 int ct2g_fft_c2r_f64(ct2g_ctx *ctx, double2 *in, double *out, int N, int batch, int ld) {
   return fft_c2r<double>(ctx, in, out, N, batch, ld);
+}
+
+// inverse transform of the expansions (Y and X passes, then z fused with L2P)
+int ct2g_fft_c2r_l2p(ct2g_ctx *ctx, bool pot) {
+  CT2G_TRY(ct2g_twiddles(ctx, ctx->M));
+  switch (ctx->M) {
+    case 8: CT2G_TRY((run_cols<float, 8>(ctx, ctx->spec, ctx->nc, true, ctx->ldk))); break;
+    case 16: CT2G_TRY((run_cols<float, 16>(ctx, ctx->spec, ctx->nc, true, ctx->ldk))); break;
+    case 32: CT2G_TRY((run_cols<float, 32>(ctx, ctx->spec, ctx->nc, true, ctx->ldk))); break;
+    case 64: CT2G_TRY((run_cols<float, 64>(ctx, ctx->spec, ctx->nc, true, ctx->ldk))); break;
+    case 128: CT2G_TRY((run_cols<float, 128>(ctx, ctx->spec, ctx->nc, true, ctx->ldk))); break;
+    case 256: CT2G_TRY((run_cols<float, 256>(ctx, ctx->spec, ctx->nc, true, ctx->ldk))); break;
+    case 512: CT2G_TRY((run_cols<float, 512>(ctx, ctx->spec, ctx->nc, true, ctx->ldk))); break;
+    default: return ct2g_fail(ctx, CT2G_EINVAL, "mesh must be a power of two in [8, 512]");
+  }
+  switch (ctx->p) {
+    case 1: return c2r_l2p_p<1>(ctx, pot);
+    case 2: return c2r_l2p_p<2>(ctx, pot);
+    case 3: return c2r_l2p_p<3>(ctx, pot);
+    case 4: return c2r_l2p_p<4>(ctx, pot);
+    case 5: return c2r_l2p_p<5>(ctx, pot);
+    case 6: return c2r_l2p_p<6>(ctx, pot);
+  }
+  return ct2g_fail(ctx, CT2G_EINVAL, "unsupported order");
 }

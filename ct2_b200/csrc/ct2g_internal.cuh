@@ -70,6 +70,42 @@ struct MiTable {
   }
 };
 
+// L2P: evaluate the local expansion L (accessor L(k) -> coefficient k) at
+// offset t from the cell centre: F_i = sum_a L_{a+e_i} t^a/a! (without GM),
+// potential -sum_a L_a t^a/a!
+template <int P, typename LA>
+__device__ __forceinline__ void ct2g_l2p(const LA &Lacc, float tx, float ty, float tz, float &fx,
+                                         float &fy, float &fz, float &pot) {
+  constexpr MiTable<P> T{};
+  constexpr int NC = MiTable<P>::NC;
+  float L[NC];
+#pragma unroll
+  for (int k = 0; k < NC; k++) L[k] = Lacc(k);
+  float px[P + 1], py[P + 1], pz[P + 1];
+  px[0] = py[0] = pz[0] = 1.f;
+#pragma unroll
+  for (int q = 1; q <= P; q++) {
+    px[q] = px[q - 1] * tx * (1.f / q);
+    py[q] = py[q - 1] * ty * (1.f / q);
+    pz[q] = pz[q - 1] * tz * (1.f / q);
+  }
+  float ax = 0.f, ay = 0.f, az = 0.f, ph = 0.f;
+#pragma unroll
+  for (int k = 0; k < NC; k++) {
+    const float mono = px[T.nx[k]] * py[T.ny[k]] * pz[T.nz[k]];
+    ph = fmaf(-L[k], mono, ph);
+    if (T.deg[k] < P) {
+      ax = fmaf(L[ct2g_mi_index(T.nx[k] + 1, T.ny[k], T.nz[k])], mono, ax);
+      ay = fmaf(L[ct2g_mi_index(T.nx[k], T.ny[k] + 1, T.nz[k])], mono, ay);
+      az = fmaf(L[ct2g_mi_index(T.nx[k], T.ny[k], T.nz[k] + 1)], mono, az);
+    }
+  }
+  fx = ax;
+  fy = ay;
+  fz = az;
+  pot = ph;
+}
+
 // ---------------------------------------------------------------------------
 // Context
 // ---------------------------------------------------------------------------
@@ -179,7 +215,12 @@ int ct2g_scan_exclusive(ct2g_ctx *ctx, const uint32_t *in, uint32_t *out, size_t
 int ct2g_bin_range(ct2g_ctx *ctx);
 int ct2g_build_greens(ct2g_ctx *ctx);
 int ct2g_p2m(ct2g_ctx *ctx);
-int ct2g_mesh_solve(ct2g_ctx *ctx);
+// mesh solve; fused_l2p: the inverse z pass evaluates the far field of every
+// particle of the current range straight into the force buffers (the
+// expansion grid is not written)
+int ct2g_mesh_solve(ct2g_ctx *ctx, bool fused_l2p, bool pot);
+// inverse z pass fused with L2P (ct2g_fft.cu)
+int ct2g_fft_c2r_l2p(ct2g_ctx *ctx, bool pot);
 // forces of the current range; pot: also the potential (diagnostics)
 int ct2g_forces(ct2g_ctx *ctx, bool pot);
 int ct2g_update(ct2g_ctx *ctx, const ct2g_kick_params *p, int *max_rung, bool fuse_drift,

@@ -452,7 +452,7 @@ int ct2g_p2m(ct2g_ctx *ctx) {
 
 // forward FFT of the moment grids, MG2L, inverse FFT into the expansions
 // (which overwrite the moments in ctx->grid)
-int ct2g_mesh_solve(ct2g_ctx *ctx) {
+int ct2g_mesh_solve(ct2g_ctx *ctx, bool fused_l2p, bool pot) {
   CT2G_TRY(ct2g_build_greens(ctx));
   cudaEventRecord(ctx->ev[2], ctx->stream);
   CT2G_TRY(ct2g_fft_r2c_f32(ctx, ctx->grid, ctx->spec, ctx->M, ctx->nc, ctx->ldk));
@@ -467,7 +467,17 @@ int ct2g_mesh_solve(ct2g_ctx *ctx) {
     default: return ct2g_fail(ctx, CT2G_EINVAL, "unsupported order");
   }
   cudaEventRecord(ctx->ev[4], ctx->stream);
-  CT2G_TRY(ct2g_fft_c2r_f32(ctx, ctx->spec, ctx->grid, ctx->M, ctx->nc, ctx->ldk));
+  if (fused_l2p) {
+    // every particle of the range gets its far field; others read zero
+    const size_t n = ctx->n;
+    CT2G_CUDA(ctx, cudaMemsetAsync(ctx->fx, 0, n * 4, ctx->stream));
+    CT2G_CUDA(ctx, cudaMemsetAsync(ctx->fy, 0, n * 4, ctx->stream));
+    CT2G_CUDA(ctx, cudaMemsetAsync(ctx->fz, 0, n * 4, ctx->stream));
+    if (pot) CT2G_CUDA(ctx, cudaMemsetAsync(ctx->pot, 0, n * 4, ctx->stream));
+    CT2G_TRY(ct2g_fft_c2r_l2p(ctx, pot));
+  } else {
+    CT2G_TRY(ct2g_fft_c2r_f32(ctx, ctx->spec, ctx->grid, ctx->M, ctx->nc, ctx->ldk));
+  }
   cudaEventRecord(ctx->ev[5], ctx->stream);
   return CT2G_OK;
 }

@@ -20,40 +20,6 @@ namespace {
 
 __constant__ int c_stencil[4 * 729];  // (ox, oy, oz, unused) per offset
 
-template <int P>
-__device__ __forceinline__ void l2p(const float *__restrict__ grid, int64_t C, int64_t cell,
-                                    float tx, float ty, float tz, float &fx, float &fy,
-                                    float &fz, float &pot) {
-  constexpr MiTable<P> T{};
-  constexpr int NC = MiTable<P>::NC;
-  float L[NC];
-#pragma unroll
-  for (int k = 0; k < NC; k++) L[k] = __ldg(grid + (int64_t)k * C + cell);
-  float px[P + 1], py[P + 1], pz[P + 1];
-  px[0] = py[0] = pz[0] = 1.f;
-#pragma unroll
-  for (int q = 1; q <= P; q++) {
-    px[q] = px[q - 1] * tx * (1.f / q);
-    py[q] = py[q - 1] * ty * (1.f / q);
-    pz[q] = pz[q - 1] * tz * (1.f / q);
-  }
-  float ax = 0.f, ay = 0.f, az = 0.f, ph = 0.f;
-#pragma unroll
-  for (int k = 0; k < NC; k++) {
-    const float mono = px[T.nx[k]] * py[T.ny[k]] * pz[T.nz[k]];
-    ph = fmaf(-L[k], mono, ph);
-    if (T.deg[k] < P) {
-      ax = fmaf(L[ct2g_mi_index(T.nx[k] + 1, T.ny[k], T.nz[k])], mono, ax);
-      ay = fmaf(L[ct2g_mi_index(T.nx[k], T.ny[k] + 1, T.nz[k])], mono, ay);
-      az = fmaf(L[ct2g_mi_index(T.nx[k], T.ny[k], T.nz[k] + 1)], mono, az);
-    }
-  }
-  fx = ax;
-  fy = ay;
-  fz = az;
-  pot = ph;
-}
-
 // ---------------------------------------------------------------------------
 // Near-field neighbour walk.  The stencil (offsets |o|^2 <= bwidth^2, bwidth
 // <= 4) of a cell touches the 27 4x4x4 cell blocks around its own; a block
@@ -116,7 +82,8 @@ __global__ void __launch_bounds__(256) forces_kernel(
     const float4 *__restrict__ src, const float *__restrict__ grid, int mbits, float soft,
     float GM, float *__restrict__ ofx, float *__restrict__ ofy, float *__restrict__ ofz,
     float *__restrict__ opot, unsigned long long *__restrict__ inter) {
-  __shared__ float4 sbuf[8][32];  // one batch of 32 sources per warp
+  __shared__ float4 sbuf[8][32];    // one batch of 32 sources per warp
+  __shared__ uint32_t cells[8][736];  // occupied stencil cells per warp (<= 729)
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const uint32_t ch = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (ch >= nchunks) return;
@@ -135,7 +102,9 @@ __global__ void __launch_bounds__(256) forces_kernel(
   float nx = 0.f, ny = 0.f, nz = 0.f, np = 0.f;
   uint32_t nsrc = 0;
   float4 *sb = sbuf[wib];
-  // the 27 neighbour-block words, one per lane, then broadcast
+  // the 27 neighbour-block words, one per lane; their set bits are compacted
+  // into a list of occupied stencil cells (exclusive popc prefix over lanes)
+  uint32_t *list = cells[wib];
   const uint32_t p = key & 63u, blk = key >> 6;
   unsigned long long word = 0;
   uint32_t nblk = 0;
@@ -143,20 +112,44 @@ __global__ void __launch_bounds__(256) forces_kernel(
     nblk = walk.add(blk, lane);
     word = occ[nblk] & __ldg(stmask + p * 27 + lane);
   }
-  for (int o = 0; o < 27; o++) {
-    unsigned long long bits = __shfl_sync(0xffffffffu, word, o);
-    const uint32_t nb = __shfl_sync(0xffffffffu, nblk, o);
-    while (bits) {
-      const int bb = __ffsll((long long)bits) - 1;
-      bits &= bits - 1;
-      const uint32_t ck = (nb << 6) | (uint32_t)bb;
-      const uint32_t j0 = cs[ck], j1 = cs[ck + 1];
+  const int cnt_mine = __popcll(word);
+  int incl = cnt_mine;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  const int ncell = __shfl_sync(0xffffffffu, incl, 31);
+  {
+    int at = incl - cnt_mine;
+    unsigned long long w = word;
+    while (w) {
+      const int bb = __ffsll((long long)w) - 1;
+      w &= w - 1;
+      list[at++] = (nblk << 6) | (uint32_t)bb;
+    }
+  }
+  __syncwarp();
+  for (int s0 = 0; s0 < ncell; s0 += 32) {
+    // 32 occupied neighbours at a time: ranges and offsets fetched per lane
+    uint32_t jb = 0, je = 0;
+    int ox = 0, oy = 0, oz = 0;
+    if (s0 + lane < ncell) {
+      const uint32_t ck = list[s0 + lane];
+      jb = cs[ck];
+      je = cs[ck + 1];
+      ox = wrap_off((int)ct2g_compact3(ck >> 2), cx, M);
+      oy = wrap_off((int)ct2g_compact3(ck >> 1), cy, M);
+      oz = wrap_off((int)ct2g_compact3(ck), cz, M);
+    }
+    const int nt = min(32, ncell - s0);
+    for (int t = 0; t < nt; t++) {
+      const uint32_t j0 = __shfl_sync(0xffffffffu, jb, t), j1 = __shfl_sync(0xffffffffu, je, t);
       nsrc += j1 - j0;
-      const int ox = wrap_off((int)ct2g_compact3(ck >> 2), cx, M);
-      const int oy = wrap_off((int)ct2g_compact3(ck >> 1), cy, M);
-      const int oz = wrap_off((int)ct2g_compact3(ck), cz, M);
       // sink position relative to the neighbour cell's centre
-      const float xs = si.x - (float)ox * hc, ys = si.y - (float)oy * hc, zs = si.z - (float)oz * hc;
+      const float xs = si.x - (float)__shfl_sync(0xffffffffu, ox, t) * hc;
+      const float ys = si.y - (float)__shfl_sync(0xffffffffu, oy, t) * hc;
+      const float zs = si.z - (float)__shfl_sync(0xffffffffu, oz, t) * hc;
       for (uint32_t jj = j0; jj < j1; jj += 32) {
         const int cnt = (int)min(32u, j1 - jj);
         __syncwarp();
@@ -171,13 +164,12 @@ __global__ void __launch_bounds__(256) forces_kernel(
       }
     }
   }
-  float fx = 0.f, fy = 0.f, fz = 0.f, ph = 0.f;
-  l2p<P>(grid, C, ((int64_t)cx * M + cy) * M + cz, si.x, si.y, si.z, fx, fy, fz, ph);
+  // the far field (L2P, with GM) is already in the force buffers
   if (act) {
-    ofx[i] = GM * (fx + nx);
-    ofy[i] = GM * (fy + ny);
-    ofz[i] = GM * (fz + nz);
-    if (POT) opot[i] = GM * (ph + np);
+    ofx[i] += GM * nx;
+    ofy[i] += GM * ny;
+    ofz[i] += GM * nz;
+    if (POT) opot[i] += GM * np;
   }
   if (lane == 0 && inter) atomicAdd(inter, (unsigned long long)(cend - b) * nsrc);
 }
@@ -200,7 +192,8 @@ __global__ void __launch_bounds__(128) forces_sparse_kernel(
     const float4 *__restrict__ src, const float *__restrict__ grid, int mbits, float soft,
     float GM, float *__restrict__ ofx, float *__restrict__ ofy, float *__restrict__ ofz,
     float *__restrict__ opot, unsigned long long *__restrict__ inter) {
-  __shared__ uint32_t queue[kQueue][128];
+  __shared__ uint32_t queue[kQueue][128];  // queued heavy cells: key
+  __shared__ uint2 qrange[kQueue][128];    // and source range
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
   if ((t & ~31u) >= nsinks) return;  // whole warps only: the queue phase shuffles
@@ -229,7 +222,8 @@ __global__ void __launch_bounds__(128) forces_sparse_kernel(
         const uint32_t j0 = cs[ck], j1 = cs[ck + 1];
         nsrc += j1 - j0;
         if (j1 - j0 >= kLight && nq < kQueue) {
-          queue[nq++][threadIdx.x] = ck;
+          queue[nq][threadIdx.x] = ck;
+          qrange[nq++][threadIdx.x] = make_uint2(j0, j1);
           continue;
         }
         const float xs = si.x - (float)wrap_off((int)ct2g_compact3(ck >> 2), cx, M) * hc;
@@ -248,9 +242,12 @@ __global__ void __launch_bounds__(128) forces_sparse_kernel(
     const unsigned pending = __ballot_sync(0xffffffffu, nq > 0);
     if (!pending) break;
     uint32_t mine = 0;
+    uint2 mr = make_uint2(0u, 0u);
     float mx = 0.f, my = 0.f, mz = 0.f;
     if (nq > 0) {
-      mine = queue[--nq][threadIdx.x];
+      --nq;
+      mine = queue[nq][threadIdx.x];
+      mr = qrange[nq][threadIdx.x];
       mx = si.x - (float)wrap_off((int)ct2g_compact3(mine >> 2), cx, M) * hc;
       my = si.y - (float)wrap_off((int)ct2g_compact3(mine >> 1), cy, M) * hc;
       mz = si.z - (float)wrap_off((int)ct2g_compact3(mine), cz, M) * hc;
@@ -259,10 +256,9 @@ __global__ void __launch_bounds__(128) forces_sparse_kernel(
     while (todo) {
       const int L = __ffs(todo) - 1;
       todo &= todo - 1;
-      const uint32_t ck = __shfl_sync(0xffffffffu, mine, L);
       const float bx = __shfl_sync(0xffffffffu, mx, L), by = __shfl_sync(0xffffffffu, my, L),
                   bz = __shfl_sync(0xffffffffu, mz, L);
-      const uint32_t b0 = cs[ck], b1 = cs[ck + 1];
+      const uint32_t b0 = __shfl_sync(0xffffffffu, mr.x, L), b1 = __shfl_sync(0xffffffffu, mr.y, L);
       float ax = 0.f, ay = 0.f, az = 0.f, ap = 0.f;
       for (uint32_t jj = b0; jj < b1; jj += 32) {
         const bool on = jj + lane < b1;
@@ -284,13 +280,11 @@ __global__ void __launch_bounds__(128) forces_sparse_kernel(
       }
     }
   }
-  if (act) {
-    float fx = 0.f, fy = 0.f, fz = 0.f, ph = 0.f;
-    l2p<P>(grid, C, ((int64_t)cx * M + cy) * M + cz, si.x, si.y, si.z, fx, fy, fz, ph);
-    ofx[i] = GM * (fx + nx);
-    ofy[i] = GM * (fy + ny);
-    ofz[i] = GM * (fz + nz);
-    if (POT) opot[i] = GM * (ph + np);
+  if (act) {  // the far field (L2P, with GM) is already in the force buffers
+    ofx[i] += GM * nx;
+    ofy[i] += GM * ny;
+    ofz[i] += GM * nz;
+    if (POT) opot[i] += GM * np;
   }
   unsigned long long c = act ? nsrc : 0;
 #pragma unroll
@@ -423,11 +417,8 @@ int ct2g_upload_stencil(ct2g_ctx *ctx, const std::vector<int> &st4) {
 
 int ct2g_forces(ct2g_ctx *ctx, bool pot) {
   const size_t n = ctx->n;
-  // entries outside the range read as zero
-  CT2G_CUDA(ctx, cudaMemsetAsync(ctx->fx, 0, n * 4, ctx->stream));
-  CT2G_CUDA(ctx, cudaMemsetAsync(ctx->fy, 0, n * 4, ctx->stream));
-  CT2G_CUDA(ctx, cudaMemsetAsync(ctx->fz, 0, n * 4, ctx->stream));
-  if (pot) CT2G_CUDA(ctx, cudaMemsetAsync(ctx->pot, 0, n * 4, ctx->stream));
+  // the far-field pass (ct2g_fft_c2r_l2p) has written the range's entries
+  (void)n;
   CT2G_CUDA(ctx, cudaMemsetAsync(ctx->d_inter, 0, sizeof(unsigned long long), ctx->stream));
   if (ctx->nchunks == 0 && ctx->nsparse == 0) return CT2G_OK;
   switch (ctx->p) {
