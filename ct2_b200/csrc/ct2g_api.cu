@@ -75,7 +75,7 @@ void free_particles(ct2g_ctx *ctx) {
   void *ptrs[] = {ctx->x, ctx->y, ctx->z, ctx->id, ctx->vx, ctx->vy, ctx->vz, ctx->rung,
                   ctx->x2, ctx->y2, ctx->z2, ctx->id2, ctx->vx2, ctx->vy2, ctx->vz2, ctx->rung2,
                   ctx->keys, ctx->keys2, ctx->vals, ctx->vals2, ctx->hist, ctx->src,
-                  ctx->chunk_begin, ctx->sparse_list, ctx->flags, ctx->fx,
+                  ctx->chunks, ctx->sparse_list, ctx->flags, ctx->fx,
                   ctx->fy, ctx->fz,
                   ctx->pot};
   for (void *p : ptrs)
@@ -88,7 +88,8 @@ void free_particles(ct2g_ctx *ctx) {
   ctx->rung2 = nullptr;
   ctx->keys = ctx->keys2 = ctx->vals = ctx->vals2 = ctx->hist = nullptr;
   ctx->src = nullptr;
-  ctx->chunk_begin = ctx->sparse_list = ctx->flags = nullptr;
+  ctx->chunks = nullptr;
+  ctx->sparse_list = ctx->flags = nullptr;
   ctx->fx = ctx->fy = ctx->fz = ctx->pot = nullptr;
   ctx->cap = 0;
 }
@@ -150,7 +151,7 @@ int ct2g_alloc_particles(ct2g_ctx *ctx, size_t n) {
   A(ctx->vals2, cap * 4);
   A(ctx->hist, ntiles * 256 * 4);
   A(ctx->src, cap * sizeof(float4));
-  A(ctx->chunk_begin, cap * 4);
+  A(ctx->chunks, cap * sizeof(uint2));
   A(ctx->sparse_list, cap * 4);
   A(ctx->flags, cap * 4);
   A(ctx->fx, cap * 4);

@@ -240,9 +240,12 @@ __global__ void gather_kernel(const uint32_t *__restrict__ perm, size_t begin, s
                        (float)((int32_t)(pz & mask) - half) * sc, 0.f);
 }
 
-// Sink work lists.  Cells with at least kDenseCell particles are split into
-// warp chunks (every 32nd particle of the cell starts one); particles of
-// sparser cells are listed individually for the thread-per-sink path.
+// Sink work lists for the near field, all in warp chunks of <= 32 sinks:
+// cells with at least kDenseCell particles are split into chunks of one cell
+// (every 32nd particle of the cell starts one); the particles of sparser
+// cells are listed (sparse_list) and chunked per 4x4x4 cell block (a block is
+// 64 consecutive Morton keys), every 32nd sparse particle of a block starting
+// a chunk.
 constexpr uint32_t kDenseCell = 16;
 
 __global__ void chunk_flag_kernel(const uint32_t *__restrict__ skeys,
@@ -255,6 +258,48 @@ __global__ void chunk_flag_kernel(const uint32_t *__restrict__ skeys,
   const bool dense = n >= kDenseCell;
   flags[i] = (dense && ((((uint32_t)(begin + i) - c0) & 31u) == 0)) ? 1u : 0u;
   sflags[i] = dense ? 0u : 1u;
+}
+
+// sparse chunk starts, indexed by sparse rank r (rank = exclusive scan of sflags)
+__global__ void sparse_chunk_flag_kernel(const uint32_t *__restrict__ skeys,
+                                         const uint32_t *__restrict__ cs,
+                                         const uint32_t *__restrict__ sflags,
+                                         const uint32_t *__restrict__ rank, size_t begin, size_t nr,
+                                         uint32_t nsparse, uint32_t *__restrict__ scflag) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nr || !sflags[i]) return;
+  const uint32_t r = rank[i];
+  const uint32_t f = cs[skeys[i] & ~63u] - (uint32_t)begin;  // first particle of the block
+  const uint32_t rf = f < nr ? rank[f] : nsparse;
+  scflag[r] = ((r - rf) & 31u) == 0 ? 1u : 0u;
+}
+
+// (start, count) of dense chunks: particle index, sinks
+__global__ void dense_chunk_fill_kernel(const uint32_t *__restrict__ flags,
+                                        const uint32_t *__restrict__ fscan,
+                                        const uint32_t *__restrict__ skeys,
+                                        const uint32_t *__restrict__ cs, size_t begin, size_t nr,
+                                        uint2 *__restrict__ list) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nr || !flags[i]) return;
+  const uint32_t g = (uint32_t)(begin + i);
+  list[fscan[i]] = make_uint2(g, min(32u, cs[skeys[i] + 1] - g));
+}
+
+// (start, count) of sparse chunks: index into sparse_list, sinks
+__global__ void sparse_chunk_fill_kernel(const uint32_t *__restrict__ scflag,
+                                         const uint32_t *__restrict__ scscan,
+                                         const uint32_t *__restrict__ sparse_list,
+                                         const uint32_t *__restrict__ skeys,
+                                         const uint32_t *__restrict__ cs,
+                                         const uint32_t *__restrict__ rank, size_t begin, size_t nr,
+                                         uint32_t nsparse, uint2 *__restrict__ list) {
+  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nsparse || !scflag[r]) return;
+  const uint32_t i = sparse_list[r] - (uint32_t)begin;
+  const uint32_t e = cs[(skeys[i] | 63u) + 1] - (uint32_t)begin;  // past the block
+  const uint32_t re = e < nr ? rank[e] : nsparse;
+  list[scscan[r]] = make_uint2(r, min(32u, re - r));
 }
 
 __global__ void chunk_fill_kernel(const uint32_t *__restrict__ flags,
@@ -385,20 +430,32 @@ int ct2g_bin_range(ct2g_ctx *ctx) {
     occupancy_kernel<<<ct2g_div_up(ctx->C / 64, T), T, 0, st>>>(ctx->cell_start, ctx->C / 64,
                                                                ctx->occ);
     CT2G_LAUNCHED(ctx);
-    // sink work lists: warp chunks of dense cells, single sinks of sparse ones
+    // near-field work lists (scratch: flags, vals, vals2, x2, y2 are free here)
     chunk_flag_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(ctx->keys, ctx->cell_start, begin, nr,
                                                         ctx->flags, ctx->vals);
     CT2G_LAUNCHED(ctx);
-    uint32_t total = 0, nsparse = 0;
-    CT2G_TRY(ct2g_scan_exclusive(ctx, ctx->flags, ctx->vals2, nr, &total, 0));
-    chunk_fill_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(ctx->flags, ctx->vals2, begin, nr,
-                                                        ctx->chunk_begin);
+    uint32_t ndense = 0, nsparse = 0, nschunk = 0;
+    CT2G_TRY(ct2g_scan_exclusive(ctx, ctx->flags, ctx->vals2, nr, &ndense, 0));
+    dense_chunk_fill_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(
+        ctx->flags, ctx->vals2, ctx->keys, ctx->cell_start, begin, nr, ctx->chunks);
     CT2G_LAUNCHED(ctx);
-    CT2G_TRY(ct2g_scan_exclusive(ctx, ctx->vals, ctx->vals2, nr, &nsparse, 0));
-    chunk_fill_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(ctx->vals, ctx->vals2, begin, nr,
+    uint32_t *rank = ctx->x2, *scflag = ctx->y2;
+    CT2G_TRY(ct2g_scan_exclusive(ctx, ctx->vals, rank, nr, &nsparse, 0));
+    chunk_fill_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(ctx->vals, rank, begin, nr,
                                                         ctx->sparse_list);
     CT2G_LAUNCHED(ctx);
-    ctx->nchunks = total;
+    if (nsparse) {
+      sparse_chunk_flag_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(
+          ctx->keys, ctx->cell_start, ctx->vals, rank, begin, nr, nsparse, scflag);
+      CT2G_LAUNCHED(ctx);
+      CT2G_TRY(ct2g_scan_exclusive(ctx, scflag, ctx->vals2, nsparse, &nschunk, 0));
+      sparse_chunk_fill_kernel<<<ct2g_div_up(nsparse, T), T, 0, st>>>(
+          scflag, ctx->vals2, ctx->sparse_list, ctx->keys, ctx->cell_start, rank, begin, nr,
+          nsparse, ctx->chunks + ndense);
+      CT2G_LAUNCHED(ctx);
+    }
+    ctx->nchunks = ndense;
+    ctx->nschunks = nschunk;
     ctx->nsparse = nsparse;
   } else {
     // empty range: every cell empty
@@ -409,6 +466,7 @@ int ct2g_bin_range(ct2g_ctx *ctx) {
     CT2G_CUDA(ctx, cudaMemsetAsync(ctx->occ, 0, sizeof(unsigned long long) * (ctx->C / 64), st));
     CT2G_CUDA(ctx, cudaStreamSynchronize(st));
     ctx->nchunks = 0;
+    ctx->nschunks = 0;
     ctx->nsparse = 0;
   }
   ctx->grid_valid = true;

@@ -545,8 +545,16 @@ __global__ void __launch_bounds__(256) fftz_c2r_l2p_kernel(
   extern __shared__ __align__(16) unsigned char smraw[];
   float2 *stw = reinterpret_cast<float2 *>(smraw);
   float2 *s = stw + N;
+  __shared__ uint32_t cb[N + 1], ce[N];  // particle ranges of the line's cells
   load_twiddles(stw, tw, N);
   const size_t line = blockIdx.x;
+  const uint32_t x = (uint32_t)(line / N), y = (uint32_t)(line % N);
+  // issue the range loads first: their latency hides behind the transform
+  for (int z = threadIdx.x; z < N; z += 256) {
+    const uint32_t key = ct2g_morton(x, y, (uint32_t)z);
+    cb[z] = cs[key];
+    ce[z] = cs[key + 1];
+  }
   const float2 *base = spec + line * (size_t)ld;
   for (int e = threadIdx.x; e < NL * N; e += 256) {
     const int l = e / N, k = e % N;
@@ -562,11 +570,9 @@ __global__ void __launch_bounds__(256) fftz_c2r_l2p_kernel(
   }
   __syncthreads();
   tile_fft<N, true, float2, true>(s, NL, 0, stw);
-  const uint32_t x = (uint32_t)(line / N), y = (uint32_t)(line % N);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   for (int z = w; z < N; z += 8) {
-    const uint32_t key = ct2g_morton(x, y, (uint32_t)z);
-    const uint32_t b0 = cs[key], b1 = cs[key + 1];
+    const uint32_t b0 = cb[z], b1 = ce[z];
     if (b0 == b1) continue;
     const auto acc = [&](int k) {
       const float2 v = s[LL::at(k >> 1, z, 0)];

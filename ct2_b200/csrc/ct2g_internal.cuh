@@ -146,10 +146,12 @@ struct ct2g_ctx {
   unsigned long long *occ = nullptr;  // [C/64] occupancy bits of 4x4x4 cell blocks
   unsigned long long *stmask = nullptr;  // [64][27] stencil bits per (in-block cell, block offset)
   float4 *src = nullptr;           // per sorted particle: offset from own cell centre
-  uint32_t *chunk_begin = nullptr; // sink chunks (<=32 particles of one dense cell)
-  uint32_t *sparse_list = nullptr; // isolated sinks, one per thread
+  uint2 *chunks = nullptr;         // near-field warp chunks (start, count): dense ones
+                                   // (particle index) then sparse ones (sparse_list index)
+  uint32_t *sparse_list = nullptr; // particles of sparse cells, in order
   uint32_t *flags = nullptr;
-  uint32_t nchunks = 0;
+  uint32_t nchunks = 0;   // dense chunks
+  uint32_t nschunks = 0;  // sparse chunks
   uint32_t nsparse = 0;
   // forces
   float *fx = nullptr, *fy = nullptr, *fz = nullptr, *pot = nullptr;

@@ -71,95 +71,109 @@ __device__ __forceinline__ void pair_term(float dx, float dy, float dz, float h2
   if (POT) ap -= pp;
 }
 
-// Dense cells: one warp per chunk of <= 32 sinks of one cell; every occupied
-// stencil cell is a warp-uniform range whose sources are staged 32 at a time
-// in shared memory and read back as broadcasts.
-template <int P, int KERNEL, bool POT>
-__global__ void __launch_bounds__(256) forces_kernel(
-    const uint32_t *__restrict__ chunk_begin, uint32_t nchunks, const uint32_t *__restrict__ cs,
-    const unsigned long long *__restrict__ occ, const unsigned long long *__restrict__ stmask,
-    Walk walk, const uint32_t *__restrict__ skeys, uint32_t rbegin,
-    const float4 *__restrict__ src, const float *__restrict__ grid, int mbits, float soft,
-    float GM, float *__restrict__ ofx, float *__restrict__ ofy, float *__restrict__ ofz,
+// Near field, one warp per chunk of <= 32 sinks.  A dense chunk is 32 sinks
+// of one cell; a sparse chunk is up to 32 sinks of sparse cells of one 4x4x4
+// block.  The warp walks the union of its sinks' stencils (per neighbouring
+// block: occupancy & the OR of the sinks' stencil masks), fetching the ranges
+// of 32 candidate cells at a time; each source batch is staged in shared
+// memory and read back as broadcasts.  A lane takes part in a source cell only
+// if the cell lies in its own stencil (always true in a dense chunk), so every
+// sink sees exactly its own near zone.
+template <int KERNEL, bool POT, bool SPARSE>
+__global__ void __launch_bounds__(256) near_kernel(
+    const uint2 *__restrict__ chunks, uint32_t nchunks, const uint32_t *__restrict__ sparse_list,
+    const uint32_t *__restrict__ cs, const unsigned long long *__restrict__ occ,
+    const unsigned long long *__restrict__ stmask, Walk walk, const uint32_t *__restrict__ skeys,
+    uint32_t rbegin, const float4 *__restrict__ src, int mbits, float soft, float bw2, float GM,
+    float *__restrict__ ofx, float *__restrict__ ofy, float *__restrict__ ofz,
     float *__restrict__ opot, unsigned long long *__restrict__ inter) {
-  __shared__ float4 sbuf[8][32];    // one batch of 32 sources per warp
-  __shared__ uint32_t cells[8][736];  // occupied stencil cells per warp (<= 729)
+  __shared__ float4 sbuf[8][32];  // one batch of 32 sources per warp
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const uint32_t ch = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (ch >= nchunks) return;
   const int M = 1 << mbits;
-  const int64_t C = (int64_t)M * M * M;
-  const uint32_t b = chunk_begin[ch];
-  const uint32_t key = skeys[b - rbegin];  // Morton key of the sink cell
-  const uint32_t cend = min(cs[key + 1], b + 32u);
-  const uint32_t i = b + lane;
-  const bool act = i < cend;
-  const float4 si = src[act ? i : b];
+  const uint2 cd = chunks[ch];
+  const bool act = (uint32_t)lane < cd.y;
+  const uint32_t slot = cd.x + (act ? (uint32_t)lane : 0u);
+  const uint32_t i = SPARSE ? sparse_list[slot] : slot;
+  const uint32_t key = skeys[i - rbegin];
+  const float4 si = src[i];
   const int cx = (int)ct2g_compact3(key >> 2), cy = (int)ct2g_compact3(key >> 1),
             cz = (int)ct2g_compact3(key);
+  const uint32_t p = key & 63u, blk = key >> 6;  // blk is the same for the whole chunk
+  // cells of the block present in the chunk
+  unsigned long long pm = 1ull << p;
+  if (SPARSE) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) pm |= __shfl_xor_sync(0xffffffffu, pm, o);
+  }
+  unsigned long long word = 0;
+  uint32_t nblk = 0;
+  if (lane < 27) {
+    nblk = walk.add(blk, lane);
+    unsigned long long m = 0, q = pm;
+    while (q) {
+      const int pp = __ffsll((long long)q) - 1;
+      q &= q - 1;
+      m |= __ldg(stmask + pp * 27 + lane);
+    }
+    word = occ[nblk] & m;
+  }
   const float hc = 1.0f / (float)M;
   const float h2 = soft * soft, hinv = 1.f / soft, hinv3 = hinv * hinv * hinv;
   float nx = 0.f, ny = 0.f, nz = 0.f, np = 0.f;
   uint32_t nsrc = 0;
   float4 *sb = sbuf[wib];
-  // the 27 neighbour-block words, one per lane; their set bits are compacted
-  // into a list of occupied stencil cells (exclusive popc prefix over lanes)
-  uint32_t *list = cells[wib];
-  const uint32_t p = key & 63u, blk = key >> 6;
-  unsigned long long word = 0;
-  uint32_t nblk = 0;
-  if (lane < 27) {
-    nblk = walk.add(blk, lane);
-    word = occ[nblk] & __ldg(stmask + p * 27 + lane);
-  }
-  const int cnt_mine = __popcll(word);
-  int incl = cnt_mine;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int v = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= o) incl += v;
-  }
-  const int ncell = __shfl_sync(0xffffffffu, incl, 31);
-  {
-    int at = incl - cnt_mine;
-    unsigned long long w = word;
-    while (w) {
-      const int bb = __ffsll((long long)w) - 1;
-      w &= w - 1;
-      list[at++] = (nblk << 6) | (uint32_t)bb;
-    }
-  }
-  __syncwarp();
-  for (int s0 = 0; s0 < ncell; s0 += 32) {
-    // 32 occupied neighbours at a time: ranges and offsets fetched per lane
-    uint32_t jb = 0, je = 0;
-    int ox = 0, oy = 0, oz = 0;
-    if (s0 + lane < ncell) {
-      const uint32_t ck = list[s0 + lane];
-      jb = cs[ck];
-      je = cs[ck + 1];
-      ox = wrap_off((int)ct2g_compact3(ck >> 2), cx, M);
-      oy = wrap_off((int)ct2g_compact3(ck >> 1), cy, M);
-      oz = wrap_off((int)ct2g_compact3(ck), cz, M);
-    }
-    const int nt = min(32, ncell - s0);
-    for (int t = 0; t < nt; t++) {
-      const uint32_t j0 = __shfl_sync(0xffffffffu, jb, t), j1 = __shfl_sync(0xffffffffu, je, t);
-      nsrc += j1 - j0;
-      // sink position relative to the neighbour cell's centre
-      const float xs = si.x - (float)__shfl_sync(0xffffffffu, ox, t) * hc;
-      const float ys = si.y - (float)__shfl_sync(0xffffffffu, oy, t) * hc;
-      const float zs = si.z - (float)__shfl_sync(0xffffffffu, oz, t) * hc;
-      for (uint32_t jj = j0; jj < j1; jj += 32) {
-        const int cnt = (int)min(32u, j1 - jj);
-        __syncwarp();
-        if (lane < cnt) sb[lane] = __ldg(src + jj + lane);
-        __syncwarp();
-#pragma unroll 8
-        for (int u = 0; u < cnt; u++) {
-          const float4 q = sb[u];
-          pair_term<KERNEL, POT>(xs - q.x, ys - q.y, zs - q.z, h2, hinv, hinv3, nx, ny, nz, np,
-                                 true);
+  for (int o = 0; o < 27; o++) {
+    const unsigned long long bits = __shfl_sync(0xffffffffu, word, o);
+    if (!bits) continue;
+    const uint32_t nb = __shfl_sync(0xffffffffu, nblk, o);
+#pragma unroll 1
+    for (int half = 0; half < 2; half++) {
+      unsigned hb = (unsigned)(bits >> (32 * half));
+      if (!hb) continue;
+      // the ranges of up to 32 candidate cells, one per lane
+      uint32_t jb = 0, je = 0;
+      if ((hb >> lane) & 1u) {
+        const uint32_t ck = (nb << 6) | (uint32_t)(32 * half + lane);
+        jb = cs[ck];
+        je = cs[ck + 1];
+      }
+      while (hb) {
+        const int t = __ffs(hb) - 1;
+        hb &= hb - 1;
+        const uint32_t j0 = __shfl_sync(0xffffffffu, jb, t), j1 = __shfl_sync(0xffffffffu, je, t);
+        const uint32_t ck = (nb << 6) | (uint32_t)(32 * half + t);
+        const int ox = wrap_off((int)ct2g_compact3(ck >> 2), cx, M);
+        const int oy = wrap_off((int)ct2g_compact3(ck >> 1), cy, M);
+        const int oz = wrap_off((int)ct2g_compact3(ck), cz, M);
+        bool in = act;
+        if (SPARSE) in = in && (float)(ox * ox + oy * oy + oz * oz) <= bw2;
+        if (in) nsrc += j1 - j0;
+        // sink position relative to the neighbour cell's centre
+        const float xs = si.x - (float)ox * hc, ys = si.y - (float)oy * hc, zs = si.z - (float)oz * hc;
+        float4 nxt = __ldg(src + min(j0 + lane, j1 - 1));
+        for (uint32_t jj = j0; jj < j1; jj += 32) {
+          const int cnt = (int)min(32u, j1 - jj);
+          __syncwarp();
+          sb[lane] = nxt;
+          __syncwarp();
+          if (jj + 32 < j1) nxt = __ldg(src + min(jj + 32 + lane, j1 - 1));
+          if (cnt == 32) {
+#pragma unroll 16
+            for (int u = 0; u < 32; u++) {
+              const float4 q = sb[u];
+              pair_term<KERNEL, POT>(xs - q.x, ys - q.y, zs - q.z, h2, hinv, hinv3, nx, ny, nz,
+                                     np, !SPARSE || in);
+            }
+          } else {
+#pragma unroll 4
+            for (int u = 0; u < cnt; u++) {
+              const float4 q = sb[u];
+              pair_term<KERNEL, POT>(xs - q.x, ys - q.y, zs - q.z, h2, hinv, hinv3, nx, ny, nz,
+                                     np, !SPARSE || in);
+            }
+          }
         }
       }
     }
@@ -171,122 +185,7 @@ __global__ void __launch_bounds__(256) forces_kernel(
     ofz[i] += GM * nz;
     if (POT) opot[i] += GM * np;
   }
-  if (lane == 0 && inter) atomicAdd(inter, (unsigned long long)(cend - b) * nsrc);
-}
-
-// Sparse cells (fewer than 16 particles): one thread per sink, each walking
-// its own occupied stencil cells.  A neighbour with fewer than kLight
-// sources is consumed by the lane alone; heavier ones (a cluster core beside
-// a halo sink) are queued in shared memory and consumed afterwards by the
-// whole warp -- lanes take 32 sources at a time against the owning lane's
-// sink, and a warp reduction hands the sum back -- so no lane idles through
-// a long private loop.
-constexpr uint32_t kLight = 24;
-constexpr int kQueue = 16;
-
-template <int P, int KERNEL, bool POT>
-__global__ void __launch_bounds__(128) forces_sparse_kernel(
-    const uint32_t *__restrict__ sinks, uint32_t nsinks, const uint32_t *__restrict__ cs,
-    const unsigned long long *__restrict__ occ, const unsigned long long *__restrict__ stmask,
-    Walk walk, const uint32_t *__restrict__ skeys, uint32_t rbegin,
-    const float4 *__restrict__ src, const float *__restrict__ grid, int mbits, float soft,
-    float GM, float *__restrict__ ofx, float *__restrict__ ofy, float *__restrict__ ofz,
-    float *__restrict__ opot, unsigned long long *__restrict__ inter) {
-  __shared__ uint32_t queue[kQueue][128];  // queued heavy cells: key
-  __shared__ uint2 qrange[kQueue][128];    // and source range
-  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int lane = threadIdx.x & 31;
-  if ((t & ~31u) >= nsinks) return;  // whole warps only: the queue phase shuffles
-  const bool act = t < nsinks;
-  const int M = 1 << mbits;
-  const int64_t C = (int64_t)M * M * M;
-  const uint32_t i = sinks[act ? t : nsinks - 1];
-  const uint32_t key = skeys[i - rbegin];
-  const float4 si = src[i];
-  const int cx = (int)ct2g_compact3(key >> 2), cy = (int)ct2g_compact3(key >> 1),
-            cz = (int)ct2g_compact3(key);
-  const float hc = 1.0f / (float)M;
-  const float h2 = soft * soft, hinv = 1.f / soft, hinv3 = hinv * hinv * hinv;
-  float nx = 0.f, ny = 0.f, nz = 0.f, np = 0.f;
-  uint32_t nsrc = 0;
-  int nq = 0;
-  const uint32_t p = key & 63u, blk = key >> 6;
-  if (act) {
-    for (int o = 0; o < 27; o++) {
-      const uint32_t nb = walk.add(blk, o);
-      unsigned long long bits = occ[nb] & __ldg(stmask + p * 27 + o);
-      while (bits) {
-        const int bb = __ffsll((long long)bits) - 1;
-        bits &= bits - 1;
-        const uint32_t ck = (nb << 6) | (uint32_t)bb;
-        const uint32_t j0 = cs[ck], j1 = cs[ck + 1];
-        nsrc += j1 - j0;
-        if (j1 - j0 >= kLight && nq < kQueue) {
-          queue[nq][threadIdx.x] = ck;
-          qrange[nq++][threadIdx.x] = make_uint2(j0, j1);
-          continue;
-        }
-        const float xs = si.x - (float)wrap_off((int)ct2g_compact3(ck >> 2), cx, M) * hc;
-        const float ys = si.y - (float)wrap_off((int)ct2g_compact3(ck >> 1), cy, M) * hc;
-        const float zs = si.z - (float)wrap_off((int)ct2g_compact3(ck), cz, M) * hc;
-        for (uint32_t j = j0; j < j1; j++) {
-          const float4 q = __ldg(src + j);
-          pair_term<KERNEL, POT>(xs - q.x, ys - q.y, zs - q.z, h2, hinv, hinv3, nx, ny, nz, np,
-                                 true);
-        }
-      }
-    }
-  }
-  // queued heavy cells, one per lane per round, each consumed by the warp
-  for (;;) {
-    const unsigned pending = __ballot_sync(0xffffffffu, nq > 0);
-    if (!pending) break;
-    uint32_t mine = 0;
-    uint2 mr = make_uint2(0u, 0u);
-    float mx = 0.f, my = 0.f, mz = 0.f;
-    if (nq > 0) {
-      --nq;
-      mine = queue[nq][threadIdx.x];
-      mr = qrange[nq][threadIdx.x];
-      mx = si.x - (float)wrap_off((int)ct2g_compact3(mine >> 2), cx, M) * hc;
-      my = si.y - (float)wrap_off((int)ct2g_compact3(mine >> 1), cy, M) * hc;
-      mz = si.z - (float)wrap_off((int)ct2g_compact3(mine), cz, M) * hc;
-    }
-    unsigned todo = pending;
-    while (todo) {
-      const int L = __ffs(todo) - 1;
-      todo &= todo - 1;
-      const float bx = __shfl_sync(0xffffffffu, mx, L), by = __shfl_sync(0xffffffffu, my, L),
-                  bz = __shfl_sync(0xffffffffu, mz, L);
-      const uint32_t b0 = __shfl_sync(0xffffffffu, mr.x, L), b1 = __shfl_sync(0xffffffffu, mr.y, L);
-      float ax = 0.f, ay = 0.f, az = 0.f, ap = 0.f;
-      for (uint32_t jj = b0; jj < b1; jj += 32) {
-        const bool on = jj + lane < b1;
-        const float4 q = __ldg(src + (on ? jj + lane : b0));
-        pair_term<KERNEL, POT>(bx - q.x, by - q.y, bz - q.z, h2, hinv, hinv3, ax, ay, az, ap, on);
-      }
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        ax += __shfl_xor_sync(0xffffffffu, ax, o);
-        ay += __shfl_xor_sync(0xffffffffu, ay, o);
-        az += __shfl_xor_sync(0xffffffffu, az, o);
-        if (POT) ap += __shfl_xor_sync(0xffffffffu, ap, o);
-      }
-      if (lane == L) {
-        nx += ax;
-        ny += ay;
-        nz += az;
-        np += ap;
-      }
-    }
-  }
-  if (act) {  // the far field (L2P, with GM) is already in the force buffers
-    ofx[i] += GM * nx;
-    ofy[i] += GM * ny;
-    ofz[i] += GM * nz;
-    if (POT) opot[i] += GM * np;
-  }
-  unsigned long long c = act ? nsrc : 0;
+  unsigned long long c = nsrc;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
   if (lane == 0 && c && inter) atomicAdd(inter, c);
@@ -363,36 +262,26 @@ Walk make_walk(int mbits) {
   return w;
 }
 
-template <int P, int K, bool POT>
-int launch_forces_t(ct2g_ctx *ctx) {
+template <int K, bool POT>
+int launch_near(ct2g_ctx *ctx) {
   const Walk walk = make_walk(ctx->mbits);
+  const float bw2 = ctx->opt.bwidth * ctx->opt.bwidth;
+  const unsigned T = 256;
   if (ctx->nchunks) {
-    const unsigned T = 256;
-    const size_t threads = (size_t)ctx->nchunks * 32;
-    forces_kernel<P, K, POT><<<ct2g_div_up(threads, T), T, 0, ctx->stream>>>(
-        ctx->chunk_begin, ctx->nchunks, ctx->cell_start, ctx->occ, ctx->stmask, walk, ctx->keys,
-        (uint32_t)ctx->rung_begin, ctx->src, ctx->grid, ctx->mbits, ctx->opt.hsoft, ctx->opt.GM,
-        ctx->fx, ctx->fy, ctx->fz, ctx->pot, ctx->d_inter);
+    near_kernel<K, POT, false><<<ct2g_div_up((size_t)ctx->nchunks * 32, T), T, 0, ctx->stream>>>(
+        ctx->chunks, ctx->nchunks, ctx->sparse_list, ctx->cell_start, ctx->occ, ctx->stmask, walk,
+        ctx->keys, (uint32_t)ctx->rung_begin, ctx->src, ctx->mbits, ctx->opt.hsoft, bw2,
+        ctx->opt.GM, ctx->fx, ctx->fy, ctx->fz, ctx->pot, ctx->d_inter);
     CT2G_LAUNCHED(ctx);
   }
-  if (ctx->nsparse) {
-    const unsigned T = 128;
-    forces_sparse_kernel<P, K, POT><<<ct2g_div_up(ctx->nsparse, T), T, 0, ctx->stream>>>(
-        ctx->sparse_list, ctx->nsparse, ctx->cell_start, ctx->occ, ctx->stmask, walk, ctx->keys,
-        (uint32_t)ctx->rung_begin, ctx->src, ctx->grid, ctx->mbits, ctx->opt.hsoft, ctx->opt.GM,
-        ctx->fx, ctx->fy, ctx->fz, ctx->pot, ctx->d_inter);
+  if (ctx->nschunks) {
+    near_kernel<K, POT, true><<<ct2g_div_up((size_t)ctx->nschunks * 32, T), T, 0, ctx->stream>>>(
+        ctx->chunks + ctx->nchunks, ctx->nschunks, ctx->sparse_list, ctx->cell_start, ctx->occ,
+        ctx->stmask, walk, ctx->keys, (uint32_t)ctx->rung_begin, ctx->src, ctx->mbits,
+        ctx->opt.hsoft, bw2, ctx->opt.GM, ctx->fx, ctx->fy, ctx->fz, ctx->pot, ctx->d_inter);
     CT2G_LAUNCHED(ctx);
   }
   return CT2G_OK;
-}
-
-template <int P>
-int launch_forces_p(ct2g_ctx *ctx, bool pot) {
-  if (ctx->opt.kernel == CT2G_SOFT_SPHERE)
-    return pot ? launch_forces_t<P, CT2G_SOFT_SPHERE, true>(ctx)
-               : launch_forces_t<P, CT2G_SOFT_SPHERE, false>(ctx);
-  return pot ? launch_forces_t<P, CT2G_SOFT_PLUMMER, true>(ctx)
-             : launch_forces_t<P, CT2G_SOFT_PLUMMER, false>(ctx);
 }
 
 }  // namespace
@@ -420,16 +309,10 @@ int ct2g_forces(ct2g_ctx *ctx, bool pot) {
   // the far-field pass (ct2g_fft_c2r_l2p) has written the range's entries
   (void)n;
   CT2G_CUDA(ctx, cudaMemsetAsync(ctx->d_inter, 0, sizeof(unsigned long long), ctx->stream));
-  if (ctx->nchunks == 0 && ctx->nsparse == 0) return CT2G_OK;
-  switch (ctx->p) {
-    case 1: return launch_forces_p<1>(ctx, pot);
-    case 2: return launch_forces_p<2>(ctx, pot);
-    case 3: return launch_forces_p<3>(ctx, pot);
-    case 4: return launch_forces_p<4>(ctx, pot);
-    case 5: return launch_forces_p<5>(ctx, pot);
-    case 6: return launch_forces_p<6>(ctx, pot);
-  }
-  return ct2g_fail(ctx, CT2G_EINVAL, "unsupported order");
+  if (ctx->nchunks == 0 && ctx->nschunks == 0) return CT2G_OK;
+  if (ctx->opt.kernel == CT2G_SOFT_SPHERE)
+    return pot ? launch_near<CT2G_SOFT_SPHERE, true>(ctx) : launch_near<CT2G_SOFT_SPHERE, false>(ctx);
+  return pot ? launch_near<CT2G_SOFT_PLUMMER, true>(ctx) : launch_near<CT2G_SOFT_PLUMMER, false>(ctx);
 }
 
 int ct2g_update(ct2g_ctx *ctx, const ct2g_kick_params *p, int *max_rung, bool fuse_drift,
