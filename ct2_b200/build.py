@@ -49,11 +49,17 @@ def _stale(target, inputs):
     return any(os.path.getmtime(i) > t for i in inputs)
 
 
+# per-file extra flags: the near-field direct sum runs with flush-to-zero so
+# that rsqrtf is a single MUFU operation; the bit-exact update/drift kernels
+# live in their own file with IEEE single precision
+EXTRA_FLAGS = {"ct2g_near.cu": ["-ftz=true"]}
+
+
 def _compile(src, verbose):
     obj = os.path.join(BUILD, os.path.basename(src) + ".o")
-    if not _stale(obj, [src] + _deps()):
+    if not _stale(obj, [src] + _deps() + [os.path.abspath(__file__)]):
         return obj
-    cmd = [nvcc()] + NVCC_FLAGS + ["-c", src, "-o", obj]
+    cmd = [nvcc()] + NVCC_FLAGS + EXTRA_FLAGS.get(os.path.basename(src), []) + ["-c", src, "-o", obj]
     if verbose:
         cmd += ["-Xptxas", "-v"]
     r = subprocess.run(cmd, capture_output=True, text=True)

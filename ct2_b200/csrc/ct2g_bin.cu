@@ -247,6 +247,7 @@ __global__ void gather_kernel(const uint32_t *__restrict__ perm, size_t begin, s
 // 64 consecutive Morton keys), every 32nd sparse particle of a block starting
 // a chunk.
 constexpr uint32_t kDenseCell = 16;
+constexpr uint32_t kSparseChunk = 16;  // sinks per sparse chunk (near_kernel)
 
 __global__ void chunk_flag_kernel(const uint32_t *__restrict__ skeys,
                                   const uint32_t *__restrict__ cs, size_t begin, size_t nr,
@@ -271,7 +272,7 @@ __global__ void sparse_chunk_flag_kernel(const uint32_t *__restrict__ skeys,
   const uint32_t r = rank[i];
   const uint32_t f = cs[skeys[i] & ~63u] - (uint32_t)begin;  // first particle of the block
   const uint32_t rf = f < nr ? rank[f] : nsparse;
-  scflag[r] = ((r - rf) & 31u) == 0 ? 1u : 0u;
+  scflag[r] = ((r - rf) % kSparseChunk) == 0 ? 1u : 0u;
 }
 
 // (start, count) of dense chunks: particle index, sinks
@@ -299,7 +300,7 @@ __global__ void sparse_chunk_fill_kernel(const uint32_t *__restrict__ scflag,
   const uint32_t i = sparse_list[r] - (uint32_t)begin;
   const uint32_t e = cs[(skeys[i] | 63u) + 1] - (uint32_t)begin;  // past the block
   const uint32_t re = e < nr ? rank[e] : nsparse;
-  list[scscan[r]] = make_uint2(r, min(32u, re - r));
+  list[scscan[r]] = make_uint2(r, min(kSparseChunk, re - r));
 }
 
 __global__ void chunk_fill_kernel(const uint32_t *__restrict__ flags,

@@ -71,14 +71,27 @@ __device__ __forceinline__ void pair_term(float dx, float dy, float dz, float h2
   if (POT) ap -= pp;
 }
 
-// Near field, one warp per chunk of <= 32 sinks.  A dense chunk is 32 sinks
-// of one cell; a sparse chunk is up to 32 sinks of sparse cells of one 4x4x4
-// block.  The warp walks the union of its sinks' stencils (per neighbouring
-// block: occupancy & the OR of the sinks' stencil masks), fetching the ranges
-// of 32 candidate cells at a time; each source batch is staged in shared
-// memory and read back as broadcasts.  A lane takes part in a source cell only
-// if the cell lies in its own stencil (always true in a dense chunk), so every
-// sink sees exactly its own near zone.
+// Near field, one warp per chunk of sinks.  A dense chunk is <= 32 sinks of
+// one cell; a sparse chunk is <= kSparseChunk sinks of sparse cells of one
+// 4x4x4 block.  The warp walks the union of its sinks' stencils (per
+// neighbouring block: occupancy & the OR of the sinks' stencil masks).  A
+// lane takes part in a source cell only if the cell lies in its own stencil
+// (always true in a dense chunk), so every sink sees exactly its own near zone.
+// Source cells are consumed in one of two layouts:
+//  * lanes = sinks: each batch of 32 sources is staged in shared memory and
+//    read back as broadcasts (dense chunks, and small cells in sparse chunks);
+//  * lanes = sources (sparse chunks, cells with >= kWide sources): the chunk's
+//    few sinks are warp-uniform registers, each lane accumulates per sink, and
+//    the per-sink sums are reduced across the warp once at the end.
+constexpr int kSparseChunk = 16;
+constexpr uint32_t kWide = 16;
+
+__device__ __forceinline__ void inblock(int b, int &x, int &y, int &z) {
+  x = ((b >> 2) & 1) | ((b >> 4) & 2);
+  y = ((b >> 1) & 1) | ((b >> 3) & 2);
+  z = (b & 1) | ((b >> 2) & 2);
+}
+
 template <int KERNEL, bool POT, bool SPARSE>
 __global__ void __launch_bounds__(256) near_kernel(
     const uint2 *__restrict__ chunks, uint32_t nchunks, const uint32_t *__restrict__ sparse_list,
@@ -88,6 +101,7 @@ __global__ void __launch_bounds__(256) near_kernel(
     float *__restrict__ ofx, float *__restrict__ ofy, float *__restrict__ ofz,
     float *__restrict__ opot, unsigned long long *__restrict__ inter) {
   __shared__ float4 sbuf[8][32];  // one batch of 32 sources per warp
+  constexpr int NS = SPARSE ? kSparseChunk : 1;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const uint32_t ch = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (ch >= nchunks) return;
@@ -98,9 +112,9 @@ __global__ void __launch_bounds__(256) near_kernel(
   const uint32_t i = SPARSE ? sparse_list[slot] : slot;
   const uint32_t key = skeys[i - rbegin];
   const float4 si = src[i];
-  const int cx = (int)ct2g_compact3(key >> 2), cy = (int)ct2g_compact3(key >> 1),
-            cz = (int)ct2g_compact3(key);
   const uint32_t p = key & 63u, blk = key >> 6;  // blk is the same for the whole chunk
+  int px, py, pz;
+  inblock((int)p, px, py, pz);
   // cells of the block present in the chunk
   unsigned long long pm = 1ull << p;
   if (SPARSE) {
@@ -122,12 +136,16 @@ __global__ void __launch_bounds__(256) near_kernel(
   const float hc = 1.0f / (float)M;
   const float h2 = soft * soft, hinv = 1.f / soft, hinv3 = hinv * hinv * hinv;
   float nx = 0.f, ny = 0.f, nz = 0.f, np = 0.f;
+  float ax[NS], ay[NS], az[NS], ap[NS];  // lanes = sources: per-sink partial sums
+#pragma unroll
+  for (int k = 0; k < NS; k++) ax[k] = ay[k] = az[k] = ap[k] = 0.f;
   uint32_t nsrc = 0;
   float4 *sb = sbuf[wib];
   for (int o = 0; o < 27; o++) {
     const unsigned long long bits = __shfl_sync(0xffffffffu, word, o);
     if (!bits) continue;
     const uint32_t nb = __shfl_sync(0xffffffffu, nblk, o);
+    const int dX = 4 * (o / 9 - 1) - px, dY = 4 * ((o / 3) % 3 - 1) - py, dZ = 4 * (o % 3 - 1) - pz;
 #pragma unroll 1
     for (int half = 0; half < 2; half++) {
       unsigned hb = (unsigned)(bits >> (32 * half));
@@ -143,15 +161,32 @@ __global__ void __launch_bounds__(256) near_kernel(
         const int t = __ffs(hb) - 1;
         hb &= hb - 1;
         const uint32_t j0 = __shfl_sync(0xffffffffu, jb, t), j1 = __shfl_sync(0xffffffffu, je, t);
-        const uint32_t ck = (nb << 6) | (uint32_t)(32 * half + t);
-        const int ox = wrap_off((int)ct2g_compact3(ck >> 2), cx, M);
-        const int oy = wrap_off((int)ct2g_compact3(ck >> 1), cy, M);
-        const int oz = wrap_off((int)ct2g_compact3(ck), cz, M);
+        int bx, by, bz;
+        inblock(32 * half + t, bx, by, bz);
+        const int ox = dX + bx, oy = dY + by, oz = dZ + bz;  // cells, from this lane's cell
         bool in = act;
         if (SPARSE) in = in && (float)(ox * ox + oy * oy + oz * oz) <= bw2;
         if (in) nsrc += j1 - j0;
         // sink position relative to the neighbour cell's centre
         const float xs = si.x - (float)ox * hc, ys = si.y - (float)oy * hc, zs = si.z - (float)oz * hc;
+        if (SPARSE && j1 - j0 >= kWide) {
+          // lanes = sources; the chunk's sinks are broadcast one at a time
+          const unsigned inmask = __ballot_sync(0xffffffffu, in);
+          for (uint32_t jj = j0; jj < j1; jj += 32) {
+            const bool on = jj + lane < j1;
+            const float4 q = __ldg(src + (on ? jj + lane : j0));
+#pragma unroll
+            for (int k = 0; k < NS; k++) {
+              const float bxs = __shfl_sync(0xffffffffu, xs, k);
+              const float bys = __shfl_sync(0xffffffffu, ys, k);
+              const float bzs = __shfl_sync(0xffffffffu, zs, k);
+              if ((inmask >> k) & 1u)
+                pair_term<KERNEL, POT>(bxs - q.x, bys - q.y, bzs - q.z, h2, hinv, hinv3, ax[k],
+                                       ay[k], az[k], ap[k], on);
+            }
+          }
+          continue;
+        }
         float4 nxt = __ldg(src + min(j0 + lane, j1 - 1));
         for (uint32_t jj = j0; jj < j1; jj += 32) {
           const int cnt = (int)min(32u, j1 - jj);
@@ -178,6 +213,26 @@ __global__ void __launch_bounds__(256) near_kernel(
       }
     }
   }
+  if (SPARSE) {
+    // hand each sink its source-parallel partial sums
+#pragma unroll
+    for (int k = 0; k < NS; k++) {
+      float vx = ax[k], vy = ay[k], vz = az[k], vp = ap[k];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        vx += __shfl_xor_sync(0xffffffffu, vx, o);
+        vy += __shfl_xor_sync(0xffffffffu, vy, o);
+        vz += __shfl_xor_sync(0xffffffffu, vz, o);
+        if (POT) vp += __shfl_xor_sync(0xffffffffu, vp, o);
+      }
+      if (lane == k) {
+        nx += vx;
+        ny += vy;
+        nz += vz;
+        np += vp;
+      }
+    }
+  }
   // the far field (L2P, with GM) is already in the force buffers
   if (act) {
     ofx[i] += GM * nx;
@@ -189,67 +244,6 @@ __global__ void __launch_bounds__(256) near_kernel(
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
   if (lane == 0 && c && inter) atomicAdd(inter, c);
-}
-
-__device__ __forceinline__ int ceil_log2_exact(float v) {
-  // exact ceil(log2(v)) for finite normal v > 0
-  const uint32_t u = __float_as_uint(v);
-  const int e = (int)((u >> 23) & 255u) - 127;
-  return (u & 0x7fffffu) ? e + 1 : e;
-}
-
-__global__ void update_kernel(size_t begin, size_t end, const float *__restrict__ fx,
-                              const float *__restrict__ fy, const float *__restrict__ fz,
-                              float *__restrict__ vx, float *__restrict__ vy,
-                              float *__restrict__ vz, int8_t *__restrict__ rung,
-                              ct2g_kick_params p, float hsoft, int *__restrict__ maxrung) {
-  const size_t i = begin + (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  int mr = 0;
-  if (i < end) {
-    const float f[3] = {fx[i], fy[i], fz[i]};
-    double v[3] = {vx[i], vy[i], vz[i]};
-    const double sgn = p.top ? 1.0 : -1.0;
-    const float dth = __fdiv_rn(__fmul_rn(0.5f, p.t0), (float)(1 << p.rung));
-    if (p.ascending && !p.first) {
-#pragma unroll
-      for (int d = 0; d < 3; d++) v[d] = __dadd_rn(v[d], __dmul_rn(__dmul_rn(sgn, (double)f[d]), (double)dth));
-    }
-    if (p.descending) {
-      float g2 = __fmul_rn(f[0], f[0]);
-      g2 = __fadd_rn(g2, __fmul_rn(f[1], f[1]));
-      g2 = __fadd_rn(g2, __fmul_rn(f[2], f[2]));
-      float dt = fminf(__fmul_rn(p.eta, __fsqrt_rn(__fdiv_rn(__fmul_rn(p.scale, hsoft),
-                                                              __fsqrt_rn(g2)))),
-                       p.t0);
-      dt = fminf(p.max_dt, dt);
-      int r = rung[i];
-      int up = (ceil_log2_exact(__fdiv_rn(p.t0, dt)) > p.rung) ? 1 : 0;
-      int nr = max(p.rung + up, r - 1);
-      rung[i] = (int8_t)nr;
-      mr = nr;
-#pragma unroll
-      for (int d = 0; d < 3; d++) v[d] = __dadd_rn(v[d], __dmul_rn(__dmul_rn(sgn, (double)f[d]), (double)dth));
-    }
-    vx[i] = (float)v[0];
-    vy[i] = (float)v[1];
-    vz[i] = (float)v[2];
-  }
-  // block max -> global
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) mr = max(mr, __shfl_xor_sync(0xffffffffu, mr, o));
-  if ((threadIdx.x & 31) == 0 && mr > 0) atomicMax(maxrung, mr);
-}
-
-__global__ void drift_kernel(size_t n, uint32_t *__restrict__ x, uint32_t *__restrict__ y,
-                             uint32_t *__restrict__ z, const float *__restrict__ vx,
-                             const float *__restrict__ vy, const float *__restrict__ vz,
-                             float lambda) {
-  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const float two32 = 4294967296.0f;
-  x[i] += (uint32_t)__float2ll_rz(__fmul_rn(__fmul_rn(vx[i], lambda), two32));
-  y[i] += (uint32_t)__float2ll_rz(__fmul_rn(__fmul_rn(vy[i], lambda), two32));
-  z[i] += (uint32_t)__float2ll_rz(__fmul_rn(__fmul_rn(vz[i], lambda), two32));
 }
 
 Walk make_walk(int mbits) {
@@ -315,37 +309,3 @@ int ct2g_forces(ct2g_ctx *ctx, bool pot) {
   return pot ? launch_near<CT2G_SOFT_PLUMMER, true>(ctx) : launch_near<CT2G_SOFT_PLUMMER, false>(ctx);
 }
 
-int ct2g_update(ct2g_ctx *ctx, const ct2g_kick_params *p, int *max_rung, bool fuse_drift,
-                float drift_dt, float drift_scale) {
-  const size_t b = ctx->rung_begin, e = ctx->n;
-  CT2G_CUDA(ctx, cudaMemsetAsync(ctx->d_maxrung, 0, sizeof(int), ctx->stream));
-  if (e > b) {
-    update_kernel<<<ct2g_div_up(e - b, 256), 256, 0, ctx->stream>>>(
-        b, e, ctx->fx, ctx->fy, ctx->fz, ctx->vx, ctx->vy, ctx->vz, ctx->rung, *p,
-        ctx->opt.hsoft, ctx->d_maxrung);
-    CT2G_LAUNCHED(ctx);
-  }
-  if (fuse_drift) CT2G_TRY(ct2g_drift_all(ctx, drift_dt, drift_scale));
-  if (max_rung) {
-    CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->h_pinned, ctx->d_maxrung, sizeof(int),
-                                   cudaMemcpyDeviceToHost, ctx->stream));
-    CT2G_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    *max_rung = (int)ctx->h_pinned[0];
-  }
-  return CT2G_OK;
-}
-
-int ct2g_drift_all(ct2g_ctx *ctx, float dt, float scale) {
-  if (ctx->n == 0) return CT2G_OK;
-  const float lambda = dt / scale;
-  drift_kernel<<<ct2g_div_up(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->n, ctx->x, ctx->y, ctx->z,
-                                                                   ctx->vx, ctx->vy, ctx->vz,
-                                                                   lambda);
-  CT2G_LAUNCHED(ctx);
-  // positions changed: the cell structure is stale
-  ctx->grid_valid = false;
-  ctx->moments_valid = false;
-  ctx->expansions_valid = false;
-  ctx->forces_valid = false;
-  return CT2G_OK;
-}
