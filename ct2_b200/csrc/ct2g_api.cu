@@ -2,6 +2,7 @@
 // rung-hierarchical kick_step driver (src/main.cpp:8-92) and rung bookkeeping
 // (src/particle.cpp:31-57,320-347).
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 #include "ct2g_internal.cuh"

@@ -247,7 +247,7 @@ __global__ void gather_kernel(const uint32_t *__restrict__ perm, size_t begin, s
 // 64 consecutive Morton keys), every 32nd sparse particle of a block starting
 // a chunk.
 constexpr uint32_t kDenseCell = 16;
-constexpr uint32_t kSparseChunk = 16;  // sinks per sparse chunk (near_kernel)
+constexpr uint32_t kSparseChunk = 32;  // sinks per sparse chunk (near_kernel)
 
 __global__ void chunk_flag_kernel(const uint32_t *__restrict__ skeys,
                                   const uint32_t *__restrict__ cs, size_t begin, size_t nr,

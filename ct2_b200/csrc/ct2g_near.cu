@@ -71,20 +71,14 @@ __device__ __forceinline__ void pair_term(float dx, float dy, float dz, float h2
   if (POT) ap -= pp;
 }
 
-// Near field, one warp per chunk of sinks.  A dense chunk is <= 32 sinks of
-// one cell; a sparse chunk is <= kSparseChunk sinks of sparse cells of one
-// 4x4x4 block.  The warp walks the union of its sinks' stencils (per
-// neighbouring block: occupancy & the OR of the sinks' stencil masks).  A
-// lane takes part in a source cell only if the cell lies in its own stencil
-// (always true in a dense chunk), so every sink sees exactly its own near zone.
-// Source cells are consumed in one of two layouts:
-//  * lanes = sinks: each batch of 32 sources is staged in shared memory and
-//    read back as broadcasts (dense chunks, and small cells in sparse chunks);
-//  * lanes = sources (sparse chunks, cells with >= kWide sources): the chunk's
-//    few sinks are warp-uniform registers, each lane accumulates per sink, and
-//    the per-sink sums are reduced across the warp once at the end.
-constexpr int kSparseChunk = 16;
-constexpr uint32_t kWide = 16;
+// Near field, one warp per chunk of <= 32 sinks.  A dense chunk is sinks of
+// one cell; a sparse chunk is sinks of sparse cells of one 4x4x4 block.  The
+// warp walks the union of its sinks' stencils (per neighbouring block:
+// occupancy & the OR of the sinks' stencil masks), fetching the ranges of 32
+// candidate cells at a time; each source batch is staged in shared memory and
+// read back as broadcasts.  A lane takes part in a source cell only if the
+// cell lies in its own stencil (always true in a dense chunk), so every sink
+// sees exactly its own near zone.
 
 __device__ __forceinline__ void inblock(int b, int &x, int &y, int &z) {
   x = ((b >> 2) & 1) | ((b >> 4) & 2);
@@ -101,7 +95,6 @@ __global__ void __launch_bounds__(256) near_kernel(
     float *__restrict__ ofx, float *__restrict__ ofy, float *__restrict__ ofz,
     float *__restrict__ opot, unsigned long long *__restrict__ inter) {
   __shared__ float4 sbuf[8][32];  // one batch of 32 sources per warp
-  constexpr int NS = SPARSE ? kSparseChunk : 1;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const uint32_t ch = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (ch >= nchunks) return;
@@ -136,9 +129,6 @@ __global__ void __launch_bounds__(256) near_kernel(
   const float hc = 1.0f / (float)M;
   const float h2 = soft * soft, hinv = 1.f / soft, hinv3 = hinv * hinv * hinv;
   float nx = 0.f, ny = 0.f, nz = 0.f, np = 0.f;
-  float ax[NS], ay[NS], az[NS], ap[NS];  // lanes = sources: per-sink partial sums
-#pragma unroll
-  for (int k = 0; k < NS; k++) ax[k] = ay[k] = az[k] = ap[k] = 0.f;
   uint32_t nsrc = 0;
   float4 *sb = sbuf[wib];
   for (int o = 0; o < 27; o++) {
@@ -169,24 +159,6 @@ __global__ void __launch_bounds__(256) near_kernel(
         if (in) nsrc += j1 - j0;
         // sink position relative to the neighbour cell's centre
         const float xs = si.x - (float)ox * hc, ys = si.y - (float)oy * hc, zs = si.z - (float)oz * hc;
-        if (SPARSE && j1 - j0 >= kWide) {
-          // lanes = sources; the chunk's sinks are broadcast one at a time
-          const unsigned inmask = __ballot_sync(0xffffffffu, in);
-          for (uint32_t jj = j0; jj < j1; jj += 32) {
-            const bool on = jj + lane < j1;
-            const float4 q = __ldg(src + (on ? jj + lane : j0));
-#pragma unroll
-            for (int k = 0; k < NS; k++) {
-              const float bxs = __shfl_sync(0xffffffffu, xs, k);
-              const float bys = __shfl_sync(0xffffffffu, ys, k);
-              const float bzs = __shfl_sync(0xffffffffu, zs, k);
-              if ((inmask >> k) & 1u)
-                pair_term<KERNEL, POT>(bxs - q.x, bys - q.y, bzs - q.z, h2, hinv, hinv3, ax[k],
-                                       ay[k], az[k], ap[k], on);
-            }
-          }
-          continue;
-        }
         float4 nxt = __ldg(src + min(j0 + lane, j1 - 1));
         for (uint32_t jj = j0; jj < j1; jj += 32) {
           const int cnt = (int)min(32u, j1 - jj);
@@ -210,26 +182,6 @@ __global__ void __launch_bounds__(256) near_kernel(
             }
           }
         }
-      }
-    }
-  }
-  if (SPARSE) {
-    // hand each sink its source-parallel partial sums
-#pragma unroll
-    for (int k = 0; k < NS; k++) {
-      float vx = ax[k], vy = ay[k], vz = az[k], vp = ap[k];
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        vx += __shfl_xor_sync(0xffffffffu, vx, o);
-        vy += __shfl_xor_sync(0xffffffffu, vy, o);
-        vz += __shfl_xor_sync(0xffffffffu, vz, o);
-        if (POT) vp += __shfl_xor_sync(0xffffffffu, vp, o);
-      }
-      if (lane == k) {
-        nx += vx;
-        ny += vy;
-        nz += vz;
-        np += vp;
       }
     }
   }
