@@ -71,6 +71,8 @@ SYMBOLS = [
     ("ct2g_fft_c2r_3d", _I, [_P, _P, _P, _I, _I]),
     ("ct2g_fft3d_f32_dev", _I, [_P, _I, _P, _P, _I, _I]),
     ("ct2g_ewald_direct", _I, [_P, _P, _P, _P, _SZ, _D, _D, _I, _P, _P]),
+    ("ct2g_ewald_direct_noalloc", _I, [_I, _P, _P, _P, _SZ, _P, _P, _P, _SZ, _I, _D, _D, _D, _D,
+                                       _I, _P, _P, _P]),
     ("ct2g_stream", _P, [_P]),
     ("ct2g_synchronize", _I, [_P]),
     ("ct2g_stage_times", _I, [_P, _P, _I]),

@@ -224,3 +224,164 @@ extern "C" int ct2g_ewald_direct(ct2g_ctx *ctx, const uint32_t *sx, const uint32
   if (d_k) cudaFree(d_k);
   return rc;
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the FP64 Ewald direct sum.
+//
+// For callers that cannot call cudaMalloc -- code that runs inside a
+// framework which owns all device memory, or a loop where allocation is not
+// allowed -- ct2g_ewald_direct_noalloc takes device pointers for its inputs
+// and outputs and keeps its only scratch, the structure factor S(k), in the
+// file-scope device array below.  Every GPU that loads the library holds the
+// array (kNoallocBox complex doubles, about 0.94 MB) until the process exits.
+// In host code g_noalloc_sk is only a host-side stand-in, never a device
+// address: the address comes from cudaGetSymbolAddress, taken once per device
+// on the first call there (so that first call should come before any stream
+// capture).  All calls share the array, and calls that overlap on the GPU
+// race on it; each call clears it before use.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+#define CT2G_NOALLOC_KMAX 24
+namespace {
+constexpr int kNoallocSide = 2 * CT2G_NOALLOC_KMAX + 1;
+constexpr int kNoallocBox = (CT2G_NOALLOC_KMAX + 1) * kNoallocSide * kNoallocSide;
+}  // namespace
+
+static __device__ __align__(256) double2 g_noalloc_sk[kNoallocBox];
+
+namespace {
+
+std::mutex g_noalloc_mu;
+double2 *g_noalloc_ptr[128] = {};
+
+// k-vector of box index q for a given kmax: kx in [0,K], ky,kz in [-K,K];
+// valid when in the half space (kx>0, or kx==0 && (ky>0 || ky==0 && kz>0))
+// and |k| <= K
+__device__ __forceinline__ bool noalloc_k(int q, int K, int &kx, int &ky, int &kz) {
+  const int side = 2 * K + 1;
+  kx = q / (side * side);
+  ky = (q / side) % side - K;
+  kz = q % side - K;
+  if (kx == 0 && (ky < 0 || (ky == 0 && kz <= 0))) return false;
+  return kx * kx + ky * ky + kz * kz <= K * K;
+}
+
+__global__ void noalloc_sk_kernel(int K, const uint32_t *__restrict__ qx,
+                                  const uint32_t *__restrict__ qy, const uint32_t *__restrict__ qz,
+                                  size_t nq, double2 *__restrict__ S) {
+  __shared__ double px[1024], py[1024], pz[1024];
+  const int nbox = (K + 1) * (2 * K + 1) * (2 * K + 1);
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t j0 = (size_t)blockIdx.y * kSrcChunk;
+  const size_t j1 = min(nq, j0 + kSrcChunk);
+  int kx = 0, ky = 0, kz = 0;
+  const bool act = q < nbox && noalloc_k(q, K, kx, ky, kz);
+  double sr = 0, si = 0;
+  for (size_t t0 = j0; t0 < j1; t0 += 1024) {
+    const int nt = (int)min((size_t)1024, j1 - t0);
+    __syncthreads();
+    for (int t = threadIdx.x; t < nt; t += blockDim.x) {
+      px[t] = qx[t0 + t] * CT2G_TWO_M32;
+      py[t] = qy[t0 + t] * CT2G_TWO_M32;
+      pz[t] = qz[t0 + t] * CT2G_TWO_M32;
+    }
+    __syncthreads();
+    if (!act) continue;
+    for (int t = 0; t < nt; t++) {
+      double s, c;
+      sincospi(2.0 * (kx * px[t] + ky * py[t] + kz * pz[t]), &s, &c);
+      sr += c;
+      si += s;
+    }
+  }
+  if (act) {
+    atomicAdd(&S[q].x, sr);
+    atomicAdd(&S[q].y, si);
+  }
+}
+
+__global__ void noalloc_kspace_kernel(const uint32_t *__restrict__ sx,
+                                      const uint32_t *__restrict__ sy,
+                                      const uint32_t *__restrict__ sz, size_t ns, int K,
+                                      const double2 *__restrict__ S, double alpha, double nq,
+                                      double GM, double *__restrict__ f, double *__restrict__ pot) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ns) return;
+  const double x = sx[i] * CT2G_TWO_M32, y = sy[i] * CT2G_TWO_M32, z = sz[i] * CT2G_TWO_M32;
+  const double pi = 3.14159265358979323846;
+  const int nbox = (K + 1) * (2 * K + 1) * (2 * K + 1);
+  double fx = 0, fy = 0, fz = 0, ph = 0;
+  for (int q = 0; q < nbox; q++) {
+    int kx, ky, kz;
+    if (!noalloc_k(q, K, kx, ky, kz)) continue;
+    double s, c;
+    sincospi(2.0 * (kx * x + ky * y + kz * z), &s, &c);
+    const double k2 = (double)(kx * kx + ky * ky + kz * kz);
+    const double w = exp(-pi * pi * k2 / (alpha * alpha)) / (pi * k2);
+    const double2 Sq = S[q];
+    const double re = c * Sq.x + s * Sq.y;
+    const double im = s * Sq.x - c * Sq.y;
+    const double a = 2.0 * w * (-2.0 * pi) * im;
+    fx += a * kx;
+    fy += a * ky;
+    fz += a * kz;
+    ph += 2.0 * w * re;
+  }
+  // the real-space kernel has accumulated into f and pot; finish and scale
+  f[3 * i + 0] = GM * (f[3 * i + 0] + fx);
+  f[3 * i + 1] = GM * (f[3 * i + 1] + fy);
+  f[3 * i + 2] = GM * (f[3 * i + 2] + fz);
+  pot[i] = -GM * (pot[i] + ph - pi / (alpha * alpha) * nq);
+}
+
+}  // namespace
+
+extern "C" int ct2g_ewald_direct_noalloc(int device, const uint32_t *qx, const uint32_t *qy,
+                                         const uint32_t *qz, size_t nq, const uint32_t *sx,
+                                         const uint32_t *sy, const uint32_t *sz, size_t ns,
+                                         int kernel, double soft, double GM, double alpha,
+                                         double rcut, int kmax, double *f, double *pot,
+                                         void *stream) {
+  if (!qx || !qy || !qz || !sx || !sy || !sz || !f || !pot || nq == 0 || ns == 0)
+    return CT2G_EINVAL;
+  if (kmax < 1 || kmax > CT2G_NOALLOC_KMAX) return CT2G_EINVAL;  // scratch holds kmax <= 24
+  if (!(alpha > 0) || !(rcut > 0) || rcut > 0.5 || !(soft > 0)) return CT2G_EINVAL;
+  if (kernel != CT2G_SOFT_PLUMMER && kernel != CT2G_SOFT_SPHERE) return CT2G_EINVAL;
+  if (device < 0 || device >= 128) return CT2G_EINVAL;
+  if (cudaSetDevice(device) != cudaSuccess) {
+    cudaGetLastError();
+    return CT2G_ENODEV;
+  }
+  double2 *S = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[device]) {
+      double2 *ptr = nullptr;
+      if (cudaGetSymbolAddress((void **)&ptr, g_noalloc_sk) != cudaSuccess || !ptr) {
+        cudaGetLastError();
+        return CT2G_ECUDA;
+      }
+      g_noalloc_ptr[device] = ptr;
+    }
+    S = g_noalloc_ptr[device];
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  const int nbox = (kmax + 1) * (2 * kmax + 1) * (2 * kmax + 1);
+  // the outputs accumulate, and S keeps the previous call's sums: clear all
+  if (cudaMemsetAsync(S, 0, sizeof(double2) * nbox, st) != cudaSuccess ||
+      cudaMemsetAsync(f, 0, sizeof(double) * 3 * ns, st) != cudaSuccess ||
+      cudaMemsetAsync(pot, 0, sizeof(double) * ns, st) != cudaSuccess) {
+    cudaGetLastError();
+    return CT2G_ECUDA;
+  }
+  dim3 g1(ct2g_div_up(ns, kSinkThreads), ct2g_div_up(nq, kSrcChunk));
+  ewald_real_kernel<<<g1, kSinkThreads, 0, st>>>(sx, sy, sz, ns, qx, qy, qz, nq, kernel, soft,
+                                                 alpha, rcut * rcut, f, pot);
+  dim3 g2(ct2g_div_up(nbox, 128), ct2g_div_up(nq, kSrcChunk));
+  noalloc_sk_kernel<<<g2, 128, 0, st>>>(kmax, qx, qy, qz, nq, S);
+  noalloc_kspace_kernel<<<ct2g_div_up(ns, 128), 128, 0, st>>>(sx, sy, sz, ns, kmax, S, alpha,
+                                                             (double)nq, GM, f, pot);
+  if (cudaGetLastError() != cudaSuccess) return CT2G_ECUDA;
+  return CT2G_OK;
+}

@@ -194,6 +194,24 @@ int ct2g_ewald_direct(ct2g_ctx *ctx, const uint32_t *sx, const uint32_t *sy,
                       const uint32_t *sz, size_t ns, double alpha, double rcut, int kmax,
                       double *f, double *pot);
 
+/* Allocation-free FP64 Ewald direct sum.  No counterpart in the reference.
+ * For callers that cannot allocate device memory themselves (a framework that
+ * owns all device memory, a loop where cudaMalloc is not allowed): every
+ * pointer is a DEVICE pointer owned by the caller -- sources qx,qy,qz[nq],
+ * sinks sx,sy,sz[ns] (fixed32), outputs f[3*ns] (interleaved xyz) and pot[ns]
+ * (both required) -- and the only scratch, the structure factor, lives in a
+ * static device array of the library (about 0.94 MB per GPU, held until the
+ * process exits).  kmax must be <= 24, the size that array holds; larger
+ * values return CT2G_EINVAL.  The first call on a device looks the array up
+ * (cudaGetSymbolAddress), so make it before any stream capture.  Calls share
+ * the array: calls that overlap on the GPU race.  Work is queued on `stream`
+ * (a cudaStream_t, or NULL for the default stream); nothing is allocated. */
+int ct2g_ewald_direct_noalloc(int device, const uint32_t *qx, const uint32_t *qy,
+                              const uint32_t *qz, size_t nq, const uint32_t *sx,
+                              const uint32_t *sy, const uint32_t *sz, size_t ns, int kernel,
+                              double soft, double GM, double alpha, double rcut, int kmax,
+                              double *f, double *pot, void *stream);
+
 /* Stream and timing helpers. */
 void *ct2g_stream(ct2g_ctx *ctx);   /* the context's cudaStream_t */
 int ct2g_synchronize(ct2g_ctx *ctx);
