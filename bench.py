@@ -208,8 +208,8 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     torch.cuda.set_device(local)
 
+    from ct2_b200 import _lib, replicas
     from ct2_b200.gravity import Gravity
-    from ct2_b200 import _lib
 
     P, n = workload(args, rank)
     soft = 1.0 / (50 * args.ngrid)
@@ -268,13 +268,10 @@ def main():
     torch.cuda.synchronize()
     ck = clocks.stop()
     launches = g.launch_count() - l0
-    ms = e0.elapsed_time(e1) / args.steps
+    ms_local = e0.elapsed_time(e1) / args.steps
+    value, ms = replicas.job_throughput(n, ms_local, device="cuda")
     if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
-    value = n * world / (ms * 1e-3)
 
     # end to end through the public API: host state in, step, host state out
     e2e = None
@@ -312,12 +309,8 @@ def main():
             e2e_step()
         e1.record(stream)
         e1.synchronize()
-        ems = e0.elapsed_time(e1) / args.steps
-        if dist:
-            t = torch.tensor([ems], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
-        e2e = {"value": n * world / (ems * 1e-3), "unit": UNIT,
+        evalue, ems = replicas.job_throughput(n, e0.elapsed_time(e1) / args.steps, device="cuda")
+        e2e = {"value": evalue, "unit": UNIT,
                "h2d_bytes_per_step": int(n * 25), "d2h_bytes_per_step": int(n * 25)}
 
     # roofline of the dominant stage
