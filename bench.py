@@ -10,9 +10,18 @@ workload: 128^3 = 2,097,152 particles, 70% in 512 Plummer spheres (a = 0.005,
 log-uniform masses over 10x) plus 30% uniform, 256^3 mesh, Plummer softening
 eps = 1/(50*128), dt = 1e-3.
 
-`value` is whole-job particles/s (device time, CUDA events, max over ranks);
-`e2e` is the same metric through the public API with the particle state copied
-host->device before and device->host after every step.  `roofline` is for the
+Two forms of the same step are timed on the same particles:
+  plain   the eager calls particle_to_grid, kick, drift (one host call per
+          stage, the reference's call sequence);
+  graph   ct2g_kick_drift with CT2G_STEP_GRAPH after ct2g_autotune: the whole
+          step recorded once as a CUDA graph (device-held work-list sizes,
+          persistent near-field grid) with autotuned launch shapes, one graph
+          launch per step.
+`value` is the graph form's whole-job particles/s (device time, CUDA events,
+max over ranks); `forms` holds both.  `e2e` is the same metric through the
+public API (ct2g_upload_particles, ct2g_kick_drift, ct2g_download_particles)
+with the particle state copied host->device before and device->host after
+every step.  `roofline` is for the
 kernel with the largest share of the step; `cpu_baseline` is the CPU oracle
 timed on a bounded sample.  Under torchrun (N>1) every rank runs an
 independent box (replicas; the step has no exchange), value = all particles /
@@ -189,6 +198,8 @@ def main():
     ap.add_argument("--accuracy-sinks", type=int, default=4096)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--tune-cache", default=None,
+                    help="autotuner cache file (default: tune on every run)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -245,16 +256,14 @@ def main():
            "sinks": int(len(sel))}
     g.upload_dict(P)
 
+    # plain form: eager calls, per-stage events
     for _ in range(args.warmup):
         step()
     g.synchronize()
     stage_sum = np.zeros(7)
-    l0 = g.launch_count()
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    clocks = ClockSampler(local)
-    clocks.start()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
@@ -265,11 +274,33 @@ def main():
         inter += g.interaction_count()
     e1.record(stream)
     e1.synchronize()
+    plain_value, plain_ms = replicas.job_throughput(n, e0.elapsed_time(e1) / args.steps,
+                                                    device="cuda")
+
+    # graph form: autotuned launch shapes, one recorded graph per step
+    tune = g.autotune(kp, args.dt, 1.0, cache_path=args.tune_cache)
+    g.upload_dict(P)
+    for _ in range(args.warmup):
+        g.kick_drift(kp, args.dt, 1.0, graph=True, wait=False)
+    g.synchronize()
+    l0 = g.launch_count()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0.record(stream)
+    for _ in range(args.steps):
+        g.kick_drift(kp, args.dt, 1.0, graph=True, wait=False)
+    e1.record(stream)
+    e1.synchronize()
     torch.cuda.synchronize()
     ck = clocks.stop()
     launches = g.launch_count() - l0
     ms_local = e0.elapsed_time(e1) / args.steps
     value, ms = replicas.job_throughput(n, ms_local, device="cuda")
+    forms = {"plain": {"value": plain_value, "ms_per_step": plain_ms},
+             "graph_autotuned": {"value": value, "ms_per_step": ms, "tuning": tune}}
     if dist:
         dist.barrier()
 
@@ -293,7 +324,7 @@ def main():
 
         def e2e_step():
             g.upload(pin["x"], pin["y"], pin["z"], pin["vx"], pin["vy"], pin["vz"], pin["rung"])
-            step()
+            g.kick_drift(kp, args.dt, 1.0, graph=True, wait=True)
             vp = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
             rc = lib.ct2g_download_particles(g.handle, vp(outn["x"]), vp(outn["y"]), vp(outn["z"]),
                                              vp(outn["vx"]), vp(outn["vy"]), vp(outn["vz"]),
@@ -353,7 +384,7 @@ def main():
                 "data": "synthetic: seeded Plummer spheres + uniform background",
                 "config": _config(args, world), "e2e": e2e, "gpu_launches": int(launches),
                 "roofline": roof, "cpu_baseline": cb, "clocks": ck, "accuracy": acc,
-                "stage_ms": stages, "interactions_per_step": inter / args.steps}
+                "forms": forms, "stage_ms": stages, "interactions_per_step": inter / args.steps}
         print(json.dumps(line), flush=True)
     g.close()
     if dist:

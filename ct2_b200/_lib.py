@@ -24,6 +24,14 @@ class Options(ctypes.Structure):
                 ("max_particles", ctypes.c_size_t)]
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [("dense_cell", ctypes.c_int), ("near_blocks_per_sm", ctypes.c_int),
+                ("fft_tile", ctypes.c_int), ("reserved", ctypes.c_int * 5)]
+
+
+STEP_GRAPH = 1
+
+
 class KickParams(ctypes.Structure):
     _fields_ = [("ascending", ctypes.c_int), ("descending", ctypes.c_int), ("top", ctypes.c_int),
                 ("first", ctypes.c_int), ("rung", ctypes.c_int), ("t0", ctypes.c_float),
@@ -60,6 +68,17 @@ SYMBOLS = [
     ("ct2g_kick_update", _I, [_P, _P, _P]),
     ("ct2g_kick", _I, [_P, _P, _P]),
     ("ct2g_drift", _I, [_P, _F, _F]),
+    ("ct2g_kick_drift", _I, [_P, _P, _F, _F, _I, _P]),
+    ("ct2g_create_boxes", _I, [_P, _I, _P]),
+    ("ct2g_set_boxes", _I, [_P, _P, _P]),
+    ("ct2g_box_count", _I, [_P]),
+    ("ct2g_batch_create", _I, [_P, _I, _P]),
+    ("ct2g_batch_kick_drift", _I, [_P, _P, _F, _F, _P]),
+    ("ct2g_batch_last_ms", _I, [_P, _P]),
+    ("ct2g_batch_destroy", _I, [_P]),
+    ("ct2g_get_tuning", _I, [_P, _P]),
+    ("ct2g_set_tuning", _I, [_P, _P]),
+    ("ct2g_autotune", _I, [_P, _P, _F, _F, ctypes.c_char_p, _P]),
     ("ct2g_kick_step", _I, [_P, _P, _I, _D, _D, _D, _D, _I, _I, _P]),
     ("ct2g_sort_by_rung", _I, [_P, _I]),
     ("ct2g_push_rungs", _I, [_P]),

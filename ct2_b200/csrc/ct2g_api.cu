@@ -108,12 +108,20 @@ int ensure_grid(ct2g_ctx *ctx) {
   return CT2G_OK;
 }
 
+}  // namespace
+
+void ct2g_mark(ct2g_ctx *ctx, int k) {
+  if (!ctx->capturing) cudaEventRecord(ctx->ev[k], ctx->stream);
+}
+
+int ct2g_check(ct2g_ctx *ctx) { return check(ctx); }
+
 // far field of the current range into the force buffers: moments (if the
 // grid does not hold them), then the mesh solve whose inverse z pass
 // evaluates L2P for every particle (the moments stay in the grid)
-int far_field(ct2g_ctx *ctx, bool pot) {
+int ct2g_far_field(ct2g_ctx *ctx, bool pot) {
   CT2G_TRY(ensure_grid(ctx));
-  cudaEventRecord(ctx->ev[1], ctx->stream);
+  ct2g_mark(ctx, 1);
   if (!ctx->moments_valid) {
     CT2G_TRY(ct2g_p2m(ctx));
     ctx->moments_valid = true;
@@ -122,11 +130,24 @@ int far_field(ct2g_ctx *ctx, bool pot) {
   return ct2g_mesh_solve(ctx, true, pot);
 }
 
-}  // namespace
+// upload the box table (offsets and GM) of the context
+static int upload_boxes(ct2g_ctx *ctx) {
+  std::vector<uint32_t> off(ctx->nbox + 1);
+  for (int b = 0; b <= ctx->nbox; b++) off[b] = (uint32_t)ctx->h_box_off[b];
+  CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->box_off, off.data(), sizeof(uint32_t) * off.size(),
+                                 cudaMemcpyHostToDevice, ctx->stream));
+  CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->box_gm, ctx->h_box_gm.data(),
+                                 sizeof(float) * ctx->h_box_gm.size(), cudaMemcpyHostToDevice,
+                                 ctx->stream));
+  CT2G_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  // kernels read the table from device memory: a recorded graph stays valid
+  return CT2G_OK;
+}
 
 int ct2g_alloc_particles(ct2g_ctx *ctx, size_t n) {
   if (n <= ctx->cap) return CT2G_OK;
   free_particles(ctx);
+  ctx->epoch++;
   const size_t cap = n;
   const size_t ntiles = (cap + 4095) / 4096;
 #define A(ptr, bytes) CT2G_CUDA(ctx, cudaMalloc(&(ptr), (bytes)))
@@ -161,15 +182,30 @@ int ct2g_alloc_particles(ct2g_ctx *ctx, size_t n) {
   A(ctx->pot, cap * 4);
 #undef A
   ctx->cap = cap;
+  // scan scratch for the largest scan of a step (radix histograms, cell
+  // ranges, per-particle flags), so that no step allocates
+  const size_t words = ct2g_scan_scratch_words(
+      std::max<size_t>(std::max<size_t>(ntiles * 256, (size_t)ctx->CB + 1), cap));
+  if (ctx->scan_tmp_words < words) {
+    if (ctx->scan_tmp) cudaFree(ctx->scan_tmp);
+    ctx->scan_tmp = nullptr;
+    ctx->scan_tmp_words = 0;
+    CT2G_CUDA(ctx, cudaMalloc(&ctx->scan_tmp, sizeof(uint32_t) * words));
+    ctx->scan_tmp_words = words;
+  }
   return CT2G_OK;
 }
 
 int ct2g_alloc_mesh(ct2g_ctx *ctx) {
-  CT2G_CUDA(ctx, cudaMalloc(&ctx->cell_start, sizeof(uint32_t) * (ctx->C + 1)));
-  CT2G_CUDA(ctx, cudaMalloc(&ctx->occ, sizeof(unsigned long long) * (ctx->C / 64)));
+  const size_t nb = (size_t)ctx->nbox;
+  CT2G_CUDA(ctx, cudaMalloc(&ctx->cell_start, sizeof(uint32_t) * (ctx->CB + 1)));
+  CT2G_CUDA(ctx, cudaMalloc(&ctx->occ, sizeof(unsigned long long) * (ctx->CB / 64)));
   CT2G_CUDA(ctx, cudaMalloc(&ctx->stmask, sizeof(unsigned long long) * 64 * 27));
-  CT2G_CUDA(ctx, cudaMalloc(&ctx->grid, sizeof(float) * ctx->nc * ctx->C));
-  CT2G_CUDA(ctx, cudaMalloc(&ctx->spec, sizeof(float2) * ctx->nc * ctx->CK));
+  CT2G_CUDA(ctx, cudaMalloc(&ctx->grid, sizeof(float) * ctx->nc * nb * ctx->C));
+  CT2G_CUDA(ctx, cudaMalloc(&ctx->spec, sizeof(float2) * ctx->nc * nb * ctx->CK));
+  CT2G_CUDA(ctx, cudaMalloc(&ctx->d_counts, sizeof(uint32_t) * 8));
+  CT2G_CUDA(ctx, cudaMalloc(&ctx->box_off, sizeof(uint32_t) * (nb + 1)));
+  CT2G_CUDA(ctx, cudaMalloc(&ctx->box_gm, sizeof(float) * nb));
   CT2G_CUDA(ctx, cudaMalloc(&ctx->greens, sizeof(float) * ctx->nc * ctx->CK));
   return CT2G_OK;
 }
@@ -205,9 +241,12 @@ const char *ct2g_status_string(int s) {
 
 const char *ct2g_last_error(const ct2g_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 
-int ct2g_create(const ct2g_options *opt, ct2g_ctx **out) {
+int ct2g_create(const ct2g_options *opt, ct2g_ctx **out) { return ct2g_create_boxes(opt, 1, out); }
+
+int ct2g_create_boxes(const ct2g_options *opt, int nbox, ct2g_ctx **out) {
   if (!opt || !out) return CT2G_EINVAL;
   *out = nullptr;
+  if (nbox < 1) return CT2G_EINVAL;
   if (!is_pow2(opt->mesh) || opt->mesh < 8 || opt->mesh > 512) return CT2G_EINVAL;
   if (opt->order < 1 || opt->order > CT2G_MAX_ORDER) return CT2G_EINVAL;
   if (!(opt->bwidth >= 0.f) || 2.0f * opt->bwidth + 1.0f > (float)opt->mesh || opt->bwidth > 4.0f)
@@ -232,6 +271,16 @@ int ct2g_create(const ct2g_options *opt, ct2g_ctx **out) {
   ctx->CK = (int64_t)ctx->M * ctx->M * ctx->ldk;
   ctx->p = opt->order;
   ctx->nc = ct2g_ncomp(ctx->p);
+  ctx->nbox = nbox;
+  while ((1 << ctx->boxbits) < nbox) ctx->boxbits++;
+  ctx->CB = ctx->C * nbox;
+  if (3 * ctx->mbits + ctx->boxbits > 32) {
+    delete ctx;
+    return CT2G_EINVAL;  // cell keys are 32 bits: box index above the Morton key
+  }
+  ctx->h_box_off.assign(nbox + 1, 0);
+  ctx->h_box_gm.assign(nbox, opt->GM);
+  ctx->boxes_set = nbox == 1;
   int rc = CT2G_OK;
   do {
     if (cudaSetDevice(ctx->device) != cudaSuccess) { rc = CT2G_ENODEV; break; }
@@ -302,8 +351,9 @@ int ct2g_destroy(ct2g_ctx *ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   free_particles(ctx);
+  if (ctx->self_batch) ct2g_batch_destroy(ctx->self_batch);
   void *ptrs[] = {ctx->cell_start, ctx->occ, ctx->stmask, ctx->grid, ctx->spec, ctx->greens,
-                  ctx->tw32, ctx->tw64,
+                  ctx->tw32, ctx->tw64, ctx->d_counts, ctx->box_off, ctx->box_gm,
                   ctx->d_maxrung, ctx->d_inter, ctx->scan_tmp};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -321,6 +371,27 @@ int ct2g_get_options(const ct2g_ctx *ctx, ct2g_options *out) {
   return CT2G_OK;
 }
 
+int ct2g_set_boxes(ct2g_ctx *ctx, const uint64_t *counts, const float *GM) {
+  CT2G_TRY(check(ctx));
+  if (!counts || !GM) return ct2g_fail(ctx, CT2G_EINVAL, "null box table");
+  if (!ctx->has_particles) return ct2g_fail(ctx, CT2G_ESTATE, "upload the particles first");
+  uint64_t sum = 0;
+  for (int b = 0; b < ctx->nbox; b++) {
+    if (!(GM[b] > 0.f)) return ct2g_fail(ctx, CT2G_EINVAL, "box GM must be > 0");
+    ctx->h_box_off[b] = sum;
+    sum += counts[b];
+  }
+  if (sum != ctx->n) return ct2g_fail(ctx, CT2G_EINVAL, "box counts do not add up to the upload");
+  ctx->h_box_off[ctx->nbox] = sum;
+  ctx->h_box_gm.assign(GM, GM + ctx->nbox);
+  CT2G_TRY(upload_boxes(ctx));
+  ctx->boxes_set = true;
+  ctx->grid_valid = ctx->moments_valid = ctx->expansions_valid = ctx->forces_valid = false;
+  return CT2G_OK;
+}
+
+int ct2g_box_count(const ct2g_ctx *ctx) { return ctx ? ctx->nbox : 0; }
+
 int ct2g_set_params(ct2g_ctx *ctx, float hsoft, float eta, float GM) {
   if (!ctx) return CT2G_EINVAL;
   if (!(hsoft > 0.f) || !(eta > 0.f)) return ct2g_fail(ctx, CT2G_EINVAL, "hsoft and eta must be > 0");
@@ -330,8 +401,16 @@ int ct2g_set_params(ct2g_ctx *ctx, float hsoft, float eta, float GM) {
   }
   ctx->opt.hsoft = hsoft;
   ctx->opt.eta = eta;
-  if (GM > 0.f) ctx->opt.GM = GM;
   ctx->forces_valid = false;
+  ctx->epoch++;
+  if (GM > 0.f) {
+    ctx->opt.GM = GM;
+    if (ctx->nbox == 1) {
+      ctx->h_box_gm[0] = GM;
+      CT2G_TRY(check(ctx));
+      CT2G_TRY(upload_boxes(ctx));
+    }
+  }
   return CT2G_OK;
 }
 
@@ -360,6 +439,14 @@ int ct2g_upload_particles(ct2g_ctx *ctx, const uint32_t *x, const uint32_t *y, c
   CT2G_CUDA(ctx, cudaStreamSynchronize(st));
   ctx->n = n;
   if (!(ctx->opt.GM > 0.f)) ctx->opt.GM = n ? 1.0f / (float)n : 0.f;
+  if (ctx->nbox == 1) {
+    ctx->h_box_off[0] = 0;
+    ctx->h_box_off[1] = n;
+    ctx->h_box_gm[0] = ctx->opt.GM;
+    CT2G_TRY(upload_boxes(ctx));
+  } else {
+    ctx->boxes_set = false;  // ct2g_set_boxes must describe this upload
+  }
   ctx->rung_begin = 0;
   ctx->rung_stack.clear();
   ctx->has_particles = true;
@@ -389,7 +476,7 @@ size_t ct2g_particle_count(const ct2g_ctx *ctx) { return ctx ? ctx->n : 0; }
 int ct2g_particle_to_grid(ct2g_ctx *ctx) {
   CT2G_TRY(check(ctx));
   if (!ctx->has_particles) return ct2g_fail(ctx, CT2G_ESTATE, "no particles uploaded");
-  cudaEventRecord(ctx->ev[0], ctx->stream);
+  ct2g_mark(ctx, 0);
   return ct2g_bin_range(ctx);
 }
 
@@ -397,19 +484,20 @@ int ct2g_download_cells(ct2g_ctx *ctx, int64_t *cell_begin, int64_t *cell_end) {
   CT2G_TRY(check(ctx));
   if (!cell_begin || !cell_end) return ct2g_fail(ctx, CT2G_EINVAL, "null output");
   CT2G_TRY(ensure_grid(ctx));
-  std::vector<uint32_t> h(ctx->C + 1);
+  std::vector<uint32_t> h(ctx->CB + 1);
   CT2G_CUDA(ctx, cudaMemcpyAsync(h.data(), ctx->cell_start, sizeof(uint32_t) * h.size(),
                                  cudaMemcpyDeviceToHost, ctx->stream));
   CT2G_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   const uint32_t M = (uint32_t)ctx->M;
-  for (uint32_t i = 0; i < M; i++)
-    for (uint32_t j = 0; j < M; j++)
-      for (uint32_t k = 0; k < M; k++) {
-        const uint32_t key = ct2g_morton(i, j, k);
-        const size_t c = ((size_t)i * M + j) * M + k;
-        cell_begin[c] = h[key];
-        cell_end[c] = h[key + 1];
-      }
+  for (int b = 0; b < ctx->nbox; b++)
+    for (uint32_t i = 0; i < M; i++)
+      for (uint32_t j = 0; j < M; j++)
+        for (uint32_t k = 0; k < M; k++) {
+          const uint32_t key = ((uint32_t)b << (3 * ctx->mbits)) | ct2g_morton(i, j, k);
+          const size_t c = (size_t)b * ctx->C + ((size_t)i * M + j) * M + k;
+          cell_begin[c] = h[key];
+          cell_end[c] = h[key + 1];
+        }
   return CT2G_OK;
 }
 
@@ -426,7 +514,7 @@ int ct2g_download_multipoles(ct2g_ctx *ctx, float *out) {
   CT2G_TRY(check(ctx));
   if (!out) return ct2g_fail(ctx, CT2G_EINVAL, "null output");
   if (!ctx->moments_valid) return ct2g_fail(ctx, CT2G_ESTATE, "moments not computed (or already transformed)");
-  CT2G_CUDA(ctx, cudaMemcpyAsync(out, ctx->grid, sizeof(float) * ctx->nc * ctx->C,
+  CT2G_CUDA(ctx, cudaMemcpyAsync(out, ctx->grid, sizeof(float) * ctx->nc * ctx->CB,
                                  cudaMemcpyDeviceToHost, ctx->stream));
   CT2G_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return CT2G_OK;
@@ -446,7 +534,7 @@ int ct2g_download_expansions(ct2g_ctx *ctx, float *out) {
   CT2G_TRY(check(ctx));
   if (!out) return ct2g_fail(ctx, CT2G_EINVAL, "null output");
   if (!ctx->expansions_valid) return ct2g_fail(ctx, CT2G_ESTATE, "expansions not computed");
-  CT2G_CUDA(ctx, cudaMemcpyAsync(out, ctx->grid, sizeof(float) * ctx->nc * ctx->C,
+  CT2G_CUDA(ctx, cudaMemcpyAsync(out, ctx->grid, sizeof(float) * ctx->nc * ctx->CB,
                                  cudaMemcpyDeviceToHost, ctx->stream));
   CT2G_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return CT2G_OK;
@@ -468,7 +556,7 @@ int ct2g_download_greens(ct2g_ctx *ctx, float *out) {
 
 int ct2g_compute_forces(ct2g_ctx *ctx) {
   CT2G_TRY(check(ctx));
-  CT2G_TRY(far_field(ctx, true));
+  CT2G_TRY(ct2g_far_field(ctx, true));
   CT2G_TRY(ct2g_forces(ctx, true));
   ctx->forces_valid = true;
   ctx->pot_valid = true;
@@ -512,13 +600,13 @@ int ct2g_kick(ct2g_ctx *ctx, const ct2g_kick_params *p, int *max_rung) {
   CT2G_TRY(check(ctx));
   if (!p) return ct2g_fail(ctx, CT2G_EINVAL, "null kick params");
   if (p->rung < 0 || p->rung > 30) return ct2g_fail(ctx, CT2G_EINVAL, "rung out of range");
-  CT2G_TRY(far_field(ctx, false));
+  CT2G_TRY(ct2g_far_field(ctx, false));
   CT2G_TRY(ct2g_forces(ctx, false));
   ctx->pot_valid = false;
-  cudaEventRecord(ctx->ev[6], ctx->stream);
+  ct2g_mark(ctx, 6);
   ctx->forces_valid = true;
   CT2G_TRY(ct2g_update(ctx, p, max_rung, false, 0.f, 1.f));
-  cudaEventRecord(ctx->ev[7], ctx->stream);
+  ct2g_mark(ctx, 7);
   return CT2G_OK;
 }
 
@@ -530,6 +618,7 @@ int ct2g_drift(ct2g_ctx *ctx, float dt, float scale) {
 
 int ct2g_sort_by_rung(ct2g_ctx *ctx, int minrung) {
   CT2G_TRY(check(ctx));
+  if (ctx->nbox > 1) return ct2g_fail(ctx, CT2G_EINVAL, "rung levels need a single-box context");
   if (minrung == 0) {
     ctx->rung_begin = 0;
     return CT2G_OK;
@@ -541,8 +630,11 @@ int ct2g_sort_by_rung(ct2g_ctx *ctx, int minrung) {
   const unsigned T = 256, G = ct2g_div_up(nr, T);
   rung_flag_kernel<<<G, T, 0, st>>>(ctx->rung, b, nr, minrung, ctx->flags);
   CT2G_LAUNCHED(ctx);
-  uint32_t nlow = 0;
-  CT2G_TRY(ct2g_scan_exclusive(ctx, ctx->flags, ctx->vals2, nr, &nlow, 0));
+  CT2G_TRY(ct2g_scan_exclusive(ctx, ctx->flags, ctx->vals2, nr, ctx->d_counts + 5, 0));
+  CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->h_pinned, ctx->d_counts + 5, sizeof(uint32_t),
+                                 cudaMemcpyDeviceToHost, st));
+  CT2G_CUDA(ctx, cudaStreamSynchronize(st));
+  const uint32_t nlow = ctx->h_pinned[0];
   rung_scatter_kernel<<<G, T, 0, st>>>(ctx->flags, ctx->vals2, b, nr, nlow, ctx->vals);
   CT2G_LAUNCHED(ctx);
   permute_kernel<uint32_t><<<G, T, 0, st>>>(ctx->vals, b, nr, ctx->x, ctx->x2);
@@ -573,6 +665,7 @@ int ct2g_sort_by_rung(ct2g_ctx *ctx, int minrung) {
   std::swap(ctx->vy, ctx->vy2);
   std::swap(ctx->vz, ctx->vz2);
   std::swap(ctx->rung, ctx->rung2);
+  ctx->epoch++;  // the store moved to the other buffers
   ctx->rung_begin = b + nlow;
   ctx->grid_valid = ctx->moments_valid = ctx->expansions_valid = ctx->forces_valid = false;
   return CT2G_OK;

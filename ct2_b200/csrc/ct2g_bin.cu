@@ -180,14 +180,26 @@ __global__ void radix_scatter_kernel(const uint32_t *__restrict__ keys,
 }
 
 // ---------------------------------------------------------------------------
+// key = (box << 3*mbits) | Morton index of the cell; the box of a particle
+// is found by bisection of the box offsets (boxes never exchange particles)
 __global__ void keys_kernel(const uint32_t *__restrict__ x, const uint32_t *__restrict__ y,
                             const uint32_t *__restrict__ z, size_t begin, size_t nr, int mbits,
+                            const uint32_t *__restrict__ box_off, int nbox,
                             uint32_t *__restrict__ keys, uint32_t *__restrict__ vals) {
   size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nr) return;
   const int sh = 32 - mbits;
   size_t g = begin + i;
-  keys[i] = ct2g_morton(x[g] >> sh, y[g] >> sh, z[g] >> sh);
+  uint32_t box = 0;
+  if (nbox > 1) {
+    uint32_t lo = 0, hi = (uint32_t)nbox;  // box_off[lo] <= g < box_off[hi]
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (__ldg(box_off + mid) <= (uint32_t)g) lo = mid; else hi = mid;
+    }
+    box = lo << (3 * mbits);
+  }
+  keys[i] = box | ct2g_morton(x[g] >> sh, y[g] >> sh, z[g] >> sh);
   vals[i] = (uint32_t)i;
 }
 
@@ -246,17 +258,17 @@ __global__ void gather_kernel(const uint32_t *__restrict__ perm, size_t begin, s
 // cells are listed (sparse_list) and chunked per 4x4x4 cell block (a block is
 // 64 consecutive Morton keys), every 32nd sparse particle of a block starting
 // a chunk.
-constexpr uint32_t kDenseCell = 16;
 constexpr uint32_t kSparseChunk = 32;  // sinks per sparse chunk (near_kernel)
 
 __global__ void chunk_flag_kernel(const uint32_t *__restrict__ skeys,
                                   const uint32_t *__restrict__ cs, size_t begin, size_t nr,
-                                  uint32_t *__restrict__ flags, uint32_t *__restrict__ sflags) {
+                                  uint32_t dense_cell, uint32_t *__restrict__ flags,
+                                  uint32_t *__restrict__ sflags) {
   size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nr) return;
   const uint32_t k = skeys[i];
   const uint32_t c0 = cs[k], n = cs[k + 1] - c0;
-  const bool dense = n >= kDenseCell;
+  const bool dense = n >= dense_cell;
   flags[i] = (dense && ((((uint32_t)(begin + i) - c0) & 31u) == 0)) ? 1u : 0u;
   sflags[i] = dense ? 0u : 1u;
 }
@@ -266,9 +278,11 @@ __global__ void sparse_chunk_flag_kernel(const uint32_t *__restrict__ skeys,
                                          const uint32_t *__restrict__ cs,
                                          const uint32_t *__restrict__ sflags,
                                          const uint32_t *__restrict__ rank, size_t begin, size_t nr,
-                                         uint32_t nsparse, uint32_t *__restrict__ scflag) {
+                                         const uint32_t *__restrict__ nsparse_dev,
+                                         uint32_t *__restrict__ scflag) {
   size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nr || !sflags[i]) return;
+  const uint32_t nsparse = *nsparse_dev;
   const uint32_t r = rank[i];
   const uint32_t f = cs[skeys[i] & ~63u] - (uint32_t)begin;  // first particle of the block
   const uint32_t rf = f < nr ? rank[f] : nsparse;
@@ -294,13 +308,15 @@ __global__ void sparse_chunk_fill_kernel(const uint32_t *__restrict__ scflag,
                                          const uint32_t *__restrict__ skeys,
                                          const uint32_t *__restrict__ cs,
                                          const uint32_t *__restrict__ rank, size_t begin, size_t nr,
-                                         uint32_t nsparse, uint2 *__restrict__ list) {
+                                         const uint32_t *__restrict__ counts,
+                                         uint2 *__restrict__ list) {
   const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t nsparse = counts[1];
   if (r >= nsparse || !scflag[r]) return;
   const uint32_t i = sparse_list[r] - (uint32_t)begin;
   const uint32_t e = cs[(skeys[i] | 63u) + 1] - (uint32_t)begin;  // past the block
   const uint32_t re = e < nr ? rank[e] : nsparse;
-  list[scscan[r]] = make_uint2(r, min(kSparseChunk, re - r));
+  list[counts[0] + scscan[r]] = make_uint2(r, min(kSparseChunk, re - r));
 }
 
 __global__ void chunk_fill_kernel(const uint32_t *__restrict__ flags,
@@ -329,17 +345,51 @@ __global__ void occupancy_kernel(const uint32_t *__restrict__ cs, size_t nwords,
   occ[w] = bits;
 }
 
+// the gathered (cell-ordered) store goes back into the primary buffers, so
+// that every step reads and writes the same addresses (a recorded graph
+// replays with fixed pointers)
+__global__ void copy_back_kernel(size_t begin, size_t nr, const uint32_t *__restrict__ x2,
+                                 const uint32_t *__restrict__ y2, const uint32_t *__restrict__ z2,
+                                 const float *__restrict__ vx2, const float *__restrict__ vy2,
+                                 const float *__restrict__ vz2, const int8_t *__restrict__ rung2,
+                                 const uint32_t *__restrict__ id2, uint32_t *__restrict__ x,
+                                 uint32_t *__restrict__ y, uint32_t *__restrict__ z,
+                                 float *__restrict__ vx, float *__restrict__ vy,
+                                 float *__restrict__ vz, int8_t *__restrict__ rung,
+                                 uint32_t *__restrict__ id) {
+  const size_t i = begin + (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= begin + nr) return;
+  x[i] = x2[i];
+  y[i] = y2[i];
+  z[i] = z2[i];
+  vx[i] = vx2[i];
+  vy[i] = vy2[i];
+  vz[i] = vz2[i];
+  rung[i] = rung2[i];
+  id[i] = id2[i];
+}
+
+__global__ void fill_kernel(uint32_t *__restrict__ a, size_t n, uint32_t v) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) a[i] = v;
+}
+
 }  // namespace
 
-// exclusive scan of n uint32 values (in may equal out); optional host total
+size_t ct2g_scan_scratch_words(size_t n) { return (n + kScanTile - 1) / kScanTile + 1; }
+
+// exclusive scan of n uint32 values (in may equal out); the sum optionally
+// goes to the device word total_dev
 int ct2g_scan_exclusive(ct2g_ctx *ctx, const uint32_t *in, uint32_t *out, size_t n,
-                        uint32_t *total_host, uint32_t offset) {
+                        uint32_t *total_dev, uint32_t offset) {
   if (n == 0) {
-    if (total_host) *total_host = 0;
+    if (total_dev) CT2G_CUDA(ctx, cudaMemsetAsync(total_dev, 0, sizeof(uint32_t), ctx->stream));
     return CT2G_OK;
   }
   unsigned nb = ct2g_div_up(n, kScanTile);
   if (ctx->scan_tmp_words < (size_t)nb + 1) {
+    if (ctx->capturing) return ct2g_fail(ctx, CT2G_ESTATE, "scan scratch too small while recording");
+    ctx->epoch++;
     if (ctx->scan_tmp) cudaFree(ctx->scan_tmp);
     ctx->scan_tmp = nullptr;
     ctx->scan_tmp_words = 0;
@@ -349,31 +399,29 @@ int ct2g_scan_exclusive(ct2g_ctx *ctx, const uint32_t *in, uint32_t *out, size_t
   uint32_t *bsum = ctx->scan_tmp;
   scan_reduce_kernel<<<nb, kScanThreads, 0, ctx->stream>>>(in, n, bsum);
   CT2G_LAUNCHED(ctx);
-  scan_single_kernel<<<1, 1024, 0, ctx->stream>>>(bsum, nb, bsum + nb);
+  scan_single_kernel<<<1, 1024, 0, ctx->stream>>>(bsum, nb, total_dev ? total_dev : bsum + nb);
   CT2G_LAUNCHED(ctx);
   scan_apply_kernel<<<nb, kScanThreads, 0, ctx->stream>>>(in, n, bsum, offset, out);
   CT2G_LAUNCHED(ctx);
-  if (total_host) {
-    CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->h_pinned, bsum + nb, sizeof(uint32_t),
-                                   cudaMemcpyDeviceToHost, ctx->stream));
-    CT2G_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    *total_host = ctx->h_pinned[0];
-  }
   return CT2G_OK;
 }
 
 // Sort the current range [rung_begin, n) by cell; build cell ranges, source
-// records and sink chunks.
+// records and sink chunks.  Every size a later kernel needs stays on the
+// device (ctx->d_counts), so the sequence can be recorded into a graph.
 int ct2g_bin_range(ct2g_ctx *ctx) {
   const size_t begin = ctx->rung_begin, nr = ctx->n - ctx->rung_begin;
   const int mbits = ctx->mbits;
   cudaStream_t st = ctx->stream;
   const unsigned T = 256;
+  if (!ctx->boxes_set) return ct2g_fail(ctx, CT2G_ESTATE, "box sizes not set since the upload");
+  uint32_t *counts = ctx->d_counts;
+  CT2G_CUDA(ctx, cudaMemsetAsync(counts, 0, sizeof(uint32_t) * 8, st));
   if (nr > 0) {
     keys_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(ctx->x, ctx->y, ctx->z, begin, nr, mbits,
-                                                    ctx->keys, ctx->vals);
+                                                    ctx->box_off, ctx->nbox, ctx->keys, ctx->vals);
     CT2G_LAUNCHED(ctx);
-    const int bits = 3 * mbits;
+    const int bits = 3 * mbits + ctx->boxbits;
     const uint32_t ntiles = ct2g_div_up(nr, kRadixTile);
     uint32_t *ka = ctx->keys, *va = ctx->vals, *kb = ctx->keys2, *vb = ctx->vals2;
     for (int shift = 0; shift < bits; shift += 8) {
@@ -391,6 +439,8 @@ int ct2g_bin_range(ct2g_ctx *ctx) {
       vb = t;
     }
     // sorted keys/perm now in (ka, va); keep them addressable as keys/vals
+    // (the number of passes is fixed per context, so a replay ends in the
+    // same buffers)
     if (ka != ctx->keys) {
       uint32_t *t = ctx->keys;
       ctx->keys = ka;
@@ -399,76 +449,53 @@ int ct2g_bin_range(ct2g_ctx *ctx) {
       ctx->vals = va;
       ctx->vals2 = t;
     }
-    CT2G_CUDA(ctx, cudaMemsetAsync(ctx->cell_start, 0, sizeof(uint32_t) * (ctx->C + 1), st));
+    CT2G_CUDA(ctx, cudaMemsetAsync(ctx->cell_start, 0, sizeof(uint32_t) * (ctx->CB + 1), st));
     cell_count_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(ctx->keys, nr, ctx->cell_start);
     CT2G_LAUNCHED(ctx);
-    CT2G_TRY(ct2g_scan_exclusive(ctx, ctx->cell_start, ctx->cell_start, (size_t)ctx->C + 1,
+    CT2G_TRY(ct2g_scan_exclusive(ctx, ctx->cell_start, ctx->cell_start, (size_t)ctx->CB + 1,
                                  nullptr, (uint32_t)begin));
     gather_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(
         ctx->vals, begin, nr, mbits, ctx->x, ctx->y, ctx->z, ctx->vx, ctx->vy, ctx->vz,
         ctx->rung, ctx->id, ctx->x2, ctx->y2, ctx->z2, ctx->vx2, ctx->vy2, ctx->vz2, ctx->rung2,
         ctx->id2, ctx->src);
     CT2G_LAUNCHED(ctx);
-    // particles outside the range keep their place
-    if (begin > 0) {
-      CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->x2, ctx->x, begin * 4, cudaMemcpyDeviceToDevice, st));
-      CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->y2, ctx->y, begin * 4, cudaMemcpyDeviceToDevice, st));
-      CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->z2, ctx->z, begin * 4, cudaMemcpyDeviceToDevice, st));
-      CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->vx2, ctx->vx, begin * 4, cudaMemcpyDeviceToDevice, st));
-      CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->vy2, ctx->vy, begin * 4, cudaMemcpyDeviceToDevice, st));
-      CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->vz2, ctx->vz, begin * 4, cudaMemcpyDeviceToDevice, st));
-      CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->rung2, ctx->rung, begin, cudaMemcpyDeviceToDevice, st));
-      CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->id2, ctx->id, begin * 4, cudaMemcpyDeviceToDevice, st));
-    }
-    std::swap(ctx->x, ctx->x2);
-    std::swap(ctx->y, ctx->y2);
-    std::swap(ctx->z, ctx->z2);
-    std::swap(ctx->vx, ctx->vx2);
-    std::swap(ctx->vy, ctx->vy2);
-    std::swap(ctx->vz, ctx->vz2);
-    std::swap(ctx->rung, ctx->rung2);
-    std::swap(ctx->id, ctx->id2);
-    occupancy_kernel<<<ct2g_div_up(ctx->C / 64, T), T, 0, st>>>(ctx->cell_start, ctx->C / 64,
-                                                               ctx->occ);
+    copy_back_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(
+        begin, nr, ctx->x2, ctx->y2, ctx->z2, ctx->vx2, ctx->vy2, ctx->vz2, ctx->rung2, ctx->id2,
+        ctx->x, ctx->y, ctx->z, ctx->vx, ctx->vy, ctx->vz, ctx->rung, ctx->id);
+    CT2G_LAUNCHED(ctx);
+    occupancy_kernel<<<ct2g_div_up(ctx->CB / 64, T), T, 0, st>>>(ctx->cell_start, ctx->CB / 64,
+                                                                ctx->occ);
     CT2G_LAUNCHED(ctx);
     // near-field work lists (scratch: flags, vals, vals2, x2, y2 are free here)
     chunk_flag_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(ctx->keys, ctx->cell_start, begin, nr,
-                                                        ctx->flags, ctx->vals);
+                                                        ctx->dense_cell, ctx->flags, ctx->vals);
     CT2G_LAUNCHED(ctx);
-    uint32_t ndense = 0, nsparse = 0, nschunk = 0;
-    CT2G_TRY(ct2g_scan_exclusive(ctx, ctx->flags, ctx->vals2, nr, &ndense, 0));
+    CT2G_TRY(ct2g_scan_exclusive(ctx, ctx->flags, ctx->vals2, nr, counts + 0, 0));
     dense_chunk_fill_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(
         ctx->flags, ctx->vals2, ctx->keys, ctx->cell_start, begin, nr, ctx->chunks);
     CT2G_LAUNCHED(ctx);
     uint32_t *rank = ctx->x2, *scflag = ctx->y2;
-    CT2G_TRY(ct2g_scan_exclusive(ctx, ctx->vals, rank, nr, &nsparse, 0));
+    CT2G_TRY(ct2g_scan_exclusive(ctx, ctx->vals, rank, nr, counts + 1, 0));
     chunk_fill_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(ctx->vals, rank, begin, nr,
                                                         ctx->sparse_list);
     CT2G_LAUNCHED(ctx);
-    if (nsparse) {
-      sparse_chunk_flag_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(
-          ctx->keys, ctx->cell_start, ctx->vals, rank, begin, nr, nsparse, scflag);
-      CT2G_LAUNCHED(ctx);
-      CT2G_TRY(ct2g_scan_exclusive(ctx, scflag, ctx->vals2, nsparse, &nschunk, 0));
-      sparse_chunk_fill_kernel<<<ct2g_div_up(nsparse, T), T, 0, st>>>(
-          scflag, ctx->vals2, ctx->sparse_list, ctx->keys, ctx->cell_start, rank, begin, nr,
-          nsparse, ctx->chunks + ndense);
-      CT2G_LAUNCHED(ctx);
-    }
-    ctx->nchunks = ndense;
-    ctx->nschunks = nschunk;
-    ctx->nsparse = nsparse;
+    // sparse chunk starts, indexed by sparse rank (entries past the sparse
+    // count stay zero)
+    CT2G_CUDA(ctx, cudaMemsetAsync(scflag, 0, sizeof(uint32_t) * nr, st));
+    sparse_chunk_flag_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(
+        ctx->keys, ctx->cell_start, ctx->vals, rank, begin, nr, counts + 1, scflag);
+    CT2G_LAUNCHED(ctx);
+    CT2G_TRY(ct2g_scan_exclusive(ctx, scflag, ctx->vals2, nr, counts + 2, 0));
+    sparse_chunk_fill_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(
+        scflag, ctx->vals2, ctx->sparse_list, ctx->keys, ctx->cell_start, rank, begin, nr, counts,
+        ctx->chunks);
+    CT2G_LAUNCHED(ctx);
   } else {
     // empty range: every cell empty
-    uint32_t v = (uint32_t)begin;
-    std::vector<uint32_t> h(ctx->C + 1, v);
-    CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->cell_start, h.data(), sizeof(uint32_t) * h.size(),
-                                   cudaMemcpyHostToDevice, st));
-    CT2G_CUDA(ctx, cudaMemsetAsync(ctx->occ, 0, sizeof(unsigned long long) * (ctx->C / 64), st));
-    CT2G_CUDA(ctx, cudaStreamSynchronize(st));
-    ctx->nchunks = 0;
-    ctx->nschunks = 0;
-    ctx->nsparse = 0;
+    fill_kernel<<<ct2g_div_up(ctx->CB + 1, T), T, 0, st>>>(ctx->cell_start, ctx->CB + 1,
+                                                          (uint32_t)begin);
+    CT2G_LAUNCHED(ctx);
+    CT2G_CUDA(ctx, cudaMemsetAsync(ctx->occ, 0, sizeof(unsigned long long) * (ctx->CB / 64), st));
   }
   ctx->grid_valid = true;
   ctx->moments_valid = false;

@@ -405,24 +405,39 @@ const float2 *twiddle_ptr<float2>(ct2g_ctx *ctx) { return ctx->tw32; }
 template <>
 const double2 *twiddle_ptr<double2>(ct2g_ctx *ctx) { return ctx->tw64; }
 
+template <typename C2, int N, int W, bool INV>
+int launch_pipe(ct2g_ctx *ctx, C2 *spec, size_t nouter, size_t ostride, size_t rstride,
+                size_t ncols) {
+  const size_t smem = sizeof(C2) * ((size_t)N + 2 * (size_t)N * W);
+  auto k = fft_cols_pipe_kernel<C2, N, W, INV>;
+  CT2G_CUDA(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  CT2G_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 256, smem));
+  const int ntiles = (int)((ncols + W - 1) / W);
+  const size_t ntot = nouter * ntiles;
+  const size_t grid = std::min(ntot, (size_t)std::max(1, per_sm) * ctx->num_sms);
+  k<<<(unsigned)grid, 256, smem, ctx->stream>>>(spec, ostride, rstride, ncols, ntiles, ntot,
+                                                twiddle_ptr<C2>(ctx));
+  CT2G_LAUNCHED(ctx);
+  return CT2G_OK;
+}
+
+// column tile widths: the default W, and W/2 or 2W (FP32 only) when the
+// context's tuning asks for them and the double buffer fits in shared memory
 template <typename T, int N, bool INV, bool VEC>
 int launch_cols(ct2g_ctx *ctx, typename Cplx<T>::type *spec, size_t nouter, size_t ostride,
                 size_t rstride, size_t ncols) {
   using C2 = typename Cplx<T>::type;
   constexpr int W = N >= 256 ? 16 : 4096 / N;
   if (VEC && N >= 64) {
-    const size_t smem = sizeof(C2) * ((size_t)N + 2 * (size_t)N * W);
-    auto k = fft_cols_pipe_kernel<C2, N, W, INV>;
-    CT2G_CUDA(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int per_sm = 0;
-    CT2G_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 256, smem));
-    const int ntiles = (int)((ncols + W - 1) / W);
-    const size_t ntot = nouter * ntiles;
-    const size_t grid = std::min(ntot, (size_t)std::max(1, per_sm) * ctx->num_sms);
-    k<<<(unsigned)grid, 256, smem, ctx->stream>>>(spec, ostride, rstride, ncols, ntiles, ntot,
-                                                  twiddle_ptr<C2>(ctx));
-    CT2G_LAUNCHED(ctx);
-    return CT2G_OK;
+    if constexpr (sizeof(C2) == 8) {
+      if (ctx->fft_tile == W / 2)
+        return launch_pipe<C2, N, W / 2, INV>(ctx, spec, nouter, ostride, rstride, ncols);
+      if constexpr (sizeof(C2) * ((size_t)N + 4 * (size_t)N * W) <= 200 * 1024)
+        if (ctx->fft_tile == 2 * W)
+          return launch_pipe<C2, N, 2 * W, INV>(ctx, spec, nouter, ostride, rstride, ncols);
+    }
+    return launch_pipe<C2, N, W, INV>(ctx, spec, nouter, ostride, rstride, ncols);
   }
   const size_t smem = sizeof(C2) * ((size_t)N + (size_t)N * W);
   auto k = fft_cols_kernel<C2, N, W, INV, VEC>;
@@ -533,13 +548,14 @@ int fft_c2r(ct2g_ctx *ctx, typename Cplx<T>::type *in, T *out, int N, int batch,
 // components are packed into complex lines (A + iB), transformed back along z
 // in shared memory, and the block then evaluates the far field of every
 // particle of the line's cells from the expansions in shared memory.  The
-// expansion grid itself is never written to HBM.
+// expansion grid itself is never written to HBM.  Block b is line b % N^2
+// of box b / N^2; component k of box q starts at spec + (k * nbox + q) * CK.
 template <int P, int N, bool POT>
 __global__ void __launch_bounds__(256) fftz_c2r_l2p_kernel(
-    const float2 *__restrict__ spec, int ld, int64_t CK, const uint32_t *__restrict__ cs,
-    const float4 *__restrict__ src, int mbits, float GM, float *__restrict__ ofx,
-    float *__restrict__ ofy, float *__restrict__ ofz, float *__restrict__ opot,
-    const float2 *__restrict__ tw) {
+    const float2 *__restrict__ spec, int ld, int64_t CK, int64_t SK,
+    const uint32_t *__restrict__ cs, const float4 *__restrict__ src, int mbits,
+    const float *__restrict__ box_gm, float *__restrict__ ofx, float *__restrict__ ofy,
+    float *__restrict__ ofz, float *__restrict__ opot, const float2 *__restrict__ tw) {
   using LL = LineLayout<N, true>;
   constexpr int NC = ct2g_ncomp(P), NL = (NC + 1) / 2, NH = N / 2 + 1;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -547,21 +563,23 @@ __global__ void __launch_bounds__(256) fftz_c2r_l2p_kernel(
   float2 *s = stw + N;
   __shared__ uint32_t cb[N + 1], ce[N];  // particle ranges of the line's cells
   load_twiddles(stw, tw, N);
-  const size_t line = blockIdx.x;
+  const size_t line = blockIdx.x % ((size_t)N * N);
+  const uint32_t box = (uint32_t)(blockIdx.x / ((size_t)N * N));
   const uint32_t x = (uint32_t)(line / N), y = (uint32_t)(line % N);
   // issue the range loads first: their latency hides behind the transform
   for (int z = threadIdx.x; z < N; z += 256) {
-    const uint32_t key = ct2g_morton(x, y, (uint32_t)z);
+    const uint32_t key = (box << (3 * mbits)) | ct2g_morton(x, y, (uint32_t)z);
     cb[z] = cs[key];
     ce[z] = cs[key + 1];
   }
-  const float2 *base = spec + line * (size_t)ld;
+  const float GM = __ldg(box_gm + box);
+  const float2 *base = spec + (int64_t)box * CK + line * (size_t)ld;
   for (int e = threadIdx.x; e < NL * N; e += 256) {
     const int l = e / N, k = e % N;
     const bool up = k >= NH;
     const int kk = up ? N - k : k;
-    float2 a = base[(int64_t)(2 * l) * CK + kk];
-    float2 b = (2 * l + 1 < NC) ? base[(int64_t)(2 * l + 1) * CK + kk] : make_float2(0.f, 0.f);
+    float2 a = base[(int64_t)(2 * l) * SK + kk];
+    float2 b = (2 * l + 1 < NC) ? base[(int64_t)(2 * l + 1) * SK + kk] : make_float2(0.f, 0.f);
     if (up) {
       a.y = -a.y;
       b.y = -b.y;
@@ -596,9 +614,9 @@ int launch_c2r_l2p(ct2g_ctx *ctx, bool pot) {
   const size_t smem = sizeof(float2) * ((size_t)N + (size_t)NL * LineLayout<N, true>::LS);
   auto k = pot ? fftz_c2r_l2p_kernel<P, N, true> : fftz_c2r_l2p_kernel<P, N, false>;
   CT2G_CUDA(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k<<<(unsigned)((size_t)N * N), 256, smem, ctx->stream>>>(
-      ctx->spec, ctx->ldk, ctx->CK, ctx->cell_start, ctx->src, ctx->mbits, ctx->opt.GM, ctx->fx,
-      ctx->fy, ctx->fz, ctx->pot, twiddle_ptr<float2>(ctx));
+  k<<<(unsigned)((size_t)N * N * ctx->nbox), 256, smem, ctx->stream>>>(
+      ctx->spec, ctx->ldk, ctx->CK, ctx->CK * ctx->nbox, ctx->cell_start, ctx->src, ctx->mbits,
+      ctx->box_gm, ctx->fx, ctx->fy, ctx->fz, ctx->pot, twiddle_ptr<float2>(ctx));
   CT2G_LAUNCHED(ctx);
   return CT2G_OK;
 }
@@ -637,6 +655,8 @@ int ct2g_fft_init(ct2g_ctx *ctx) {
 // twiddles exp(-2 pi i k/N), k < N, computed on the host in FP64
 int ct2g_twiddles(ct2g_ctx *ctx, int N) {
   if (ctx->tw_n == N) return CT2G_OK;
+  if (ctx->capturing) return ct2g_fail(ctx, CT2G_ESTATE, "FFT twiddles not set up before recording");
+  ctx->epoch++;  // twiddle pointers are part of a recorded graph
   if (ctx->tw32) cudaFree(ctx->tw32);
   if (ctx->tw64) cudaFree(ctx->tw64);
   ctx->tw32 = nullptr;
@@ -678,13 +698,13 @@ int ct2g_fft_c2r_f64(ct2g_ctx *ctx, double2 *in, double *out, int N, int batch, 
 int ct2g_fft_c2r_l2p(ct2g_ctx *ctx, bool pot) {
   CT2G_TRY(ct2g_twiddles(ctx, ctx->M));
   switch (ctx->M) {
-    case 8: CT2G_TRY((run_cols<float, 8>(ctx, ctx->spec, ctx->nc, true, ctx->ldk))); break;
-    case 16: CT2G_TRY((run_cols<float, 16>(ctx, ctx->spec, ctx->nc, true, ctx->ldk))); break;
-    case 32: CT2G_TRY((run_cols<float, 32>(ctx, ctx->spec, ctx->nc, true, ctx->ldk))); break;
-    case 64: CT2G_TRY((run_cols<float, 64>(ctx, ctx->spec, ctx->nc, true, ctx->ldk))); break;
-    case 128: CT2G_TRY((run_cols<float, 128>(ctx, ctx->spec, ctx->nc, true, ctx->ldk))); break;
-    case 256: CT2G_TRY((run_cols<float, 256>(ctx, ctx->spec, ctx->nc, true, ctx->ldk))); break;
-    case 512: CT2G_TRY((run_cols<float, 512>(ctx, ctx->spec, ctx->nc, true, ctx->ldk))); break;
+    case 8: CT2G_TRY((run_cols<float, 8>(ctx, ctx->spec, ctx->nc * ctx->nbox, true, ctx->ldk))); break;
+    case 16: CT2G_TRY((run_cols<float, 16>(ctx, ctx->spec, ctx->nc * ctx->nbox, true, ctx->ldk))); break;
+    case 32: CT2G_TRY((run_cols<float, 32>(ctx, ctx->spec, ctx->nc * ctx->nbox, true, ctx->ldk))); break;
+    case 64: CT2G_TRY((run_cols<float, 64>(ctx, ctx->spec, ctx->nc * ctx->nbox, true, ctx->ldk))); break;
+    case 128: CT2G_TRY((run_cols<float, 128>(ctx, ctx->spec, ctx->nc * ctx->nbox, true, ctx->ldk))); break;
+    case 256: CT2G_TRY((run_cols<float, 256>(ctx, ctx->spec, ctx->nc * ctx->nbox, true, ctx->ldk))); break;
+    case 512: CT2G_TRY((run_cols<float, 512>(ctx, ctx->spec, ctx->nc * ctx->nbox, true, ctx->ldk))); break;
     default: return ct2g_fail(ctx, CT2G_EINVAL, "mesh must be a power of two in [8, 512]");
   }
   switch (ctx->p) {

@@ -1,0 +1,439 @@
+// One kick + drift as a recorded CUDA graph, batches of contexts stepped by
+// one graph launch, and the launch-shape autotuner.
+//
+// The step is the single-level body of the reference's kick_step
+// (src/main.cpp:49 particle_to_grid, :68 kick, :81 drift).  Every stage keeps
+// its sizes on the device (work-list counts, persistent near-field grid), so
+// the whole sequence records into one graph; replays need no host round trip.
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+
+#include "ct2g_internal.cuh"
+
+struct ct2g_batch {
+  std::vector<ct2g_ctx *> ctx;
+  int device = 0;
+  cudaStream_t s0 = nullptr;  // launch stream: the first context's
+  cudaGraphExec_t exec = nullptr;
+  cudaEvent_t fork = nullptr, t0 = nullptr, t1 = nullptr;
+  std::vector<cudaEvent_t> join;
+  int *h_maxrung = nullptr;  // pinned [nctx], written by the graph
+  // what the recorded graph was made for
+  bool recorded = false;
+  ct2g_kick_params p{};
+  float dt = 0.f, scale = 0.f;
+  std::vector<uint64_t> epochs;
+  std::vector<size_t> ns, begins;
+  std::vector<uint64_t> launches;  // kernels per replay, per context
+  bool launched = false;
+};
+
+namespace {
+
+int check_params(ct2g_ctx *ctx, const ct2g_kick_params *p, float scale) {
+  if (!p) return ct2g_fail(ctx, CT2G_EINVAL, "null kick params");
+  if (p->rung < 0 || p->rung > 30) return ct2g_fail(ctx, CT2G_EINVAL, "rung out of range");
+  if (!(scale != 0.f)) return ct2g_fail(ctx, CT2G_EINVAL, "scale must be nonzero");
+  return CT2G_OK;
+}
+
+// particle_to_grid, kick, drift on ctx->stream
+int step_body(ct2g_ctx *ctx, const ct2g_kick_params *p, float dt, float scale) {
+  if (!ctx->has_particles) return ct2g_fail(ctx, CT2G_ESTATE, "no particles uploaded");
+  ct2g_mark(ctx, 0);
+  CT2G_TRY(ct2g_bin_range(ctx));
+  CT2G_TRY(ct2g_far_field(ctx, false));
+  CT2G_TRY(ct2g_forces(ctx, false));
+  ctx->pot_valid = false;
+  ctx->forces_valid = true;
+  ct2g_mark(ctx, 6);
+  CT2G_TRY(ct2g_update(ctx, p, nullptr, false, 0.f, 1.f));
+  CT2G_TRY(ct2g_drift_all(ctx, dt, scale));
+  ct2g_mark(ctx, 7);
+  return CT2G_OK;
+}
+
+// one-time work a recording cannot contain (allocation, host uploads)
+int prepare(ct2g_ctx *ctx) {
+  CT2G_TRY(ct2g_check(ctx));
+  if (!ctx->has_particles) return ct2g_fail(ctx, CT2G_ESTATE, "no particles uploaded");
+  if (!ctx->boxes_set) return ct2g_fail(ctx, CT2G_ESTATE, "box sizes not set since the upload");
+  CT2G_TRY(ct2g_build_greens(ctx));
+  CT2G_TRY(ct2g_twiddles(ctx, ctx->M));
+  return CT2G_OK;
+}
+
+bool same_recording(const ct2g_batch *b, const ct2g_kick_params *p, float dt, float scale) {
+  if (!b->recorded || std::memcmp(&b->p, p, sizeof(*p)) != 0 || b->dt != dt || b->scale != scale)
+    return false;
+  for (size_t i = 0; i < b->ctx.size(); i++) {
+    const ct2g_ctx *c = b->ctx[i];
+    if (b->epochs[i] != c->epoch || b->ns[i] != c->n || b->begins[i] != c->rung_begin) return false;
+  }
+  return true;
+}
+
+int record(ct2g_batch *b, const ct2g_kick_params *p, float dt, float scale) {
+  ct2g_ctx *c0 = b->ctx[0];
+  const size_t nctx = b->ctx.size();
+  for (ct2g_ctx *c : b->ctx) CT2G_TRY(prepare(c));
+  CT2G_TRY(ct2g_check(c0));
+  std::vector<uint64_t> l0(nctx);
+  for (size_t i = 0; i < nctx; i++) l0[i] = b->ctx[i]->launches;
+  b->recorded = false;
+  cudaError_t e = cudaStreamBeginCapture(b->s0, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return ct2g_cuda_fail(c0, e, "cudaStreamBeginCapture");
+  int rc = CT2G_OK;
+  ct2g_ctx *failed = nullptr;
+  std::vector<bool> forked(nctx, false);
+  e = cudaEventRecord(b->fork, b->s0);
+  for (size_t i = 0; i < nctx && rc == CT2G_OK && e == cudaSuccess; i++) {
+    ct2g_ctx *c = b->ctx[i];
+    if (c->stream != b->s0) {
+      e = cudaStreamWaitEvent(c->stream, b->fork, 0);
+      if (e != cudaSuccess) break;
+      forked[i] = true;
+    }
+    c->capturing = true;
+    rc = step_body(c, p, dt, scale);
+    c->capturing = false;
+    if (rc != CT2G_OK) {
+      failed = c;
+      break;
+    }
+    e = cudaMemcpyAsync(b->h_maxrung + i, c->d_maxrung, sizeof(int), cudaMemcpyDeviceToHost,
+                        c->stream);
+  }
+  // join every forked stream back, also on failure, so the capture can end
+  for (size_t i = 0; i < nctx; i++)
+    if (forked[i]) {
+      cudaEventRecord(b->join[i], b->ctx[i]->stream);
+      cudaStreamWaitEvent(b->s0, b->join[i], 0);
+    }
+  cudaGraph_t g = nullptr;
+  const cudaError_t ee = cudaStreamEndCapture(b->s0, &g);
+  for (size_t i = 0; i < nctx; i++) b->ctx[i]->capturing = false;
+  if (rc != CT2G_OK || e != cudaSuccess || ee != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    // nothing ran: the host-side stage flags say "stale", which is safe
+    for (size_t i = 0; i < nctx; i++) {
+      ct2g_ctx *c = b->ctx[i];
+      c->launches = l0[i];
+      c->grid_valid = c->moments_valid = c->expansions_valid = c->forces_valid = false;
+    }
+    if (rc != CT2G_OK) {
+      if (failed && failed != c0) ct2g_fail(c0, rc, std::string("batch member: ") + ct2g_last_error(failed));
+      return rc;
+    }
+    return ct2g_cuda_fail(c0, e != cudaSuccess ? e : ee, "graph capture");
+  }
+  if (b->exec) {
+    cudaGraphExecUpdateResultInfo info;
+    if (cudaGraphExecUpdate(b->exec, g, &info) != cudaSuccess) {
+      cudaGetLastError();
+      cudaGraphExecDestroy(b->exec);
+      b->exec = nullptr;
+    }
+  }
+  if (!b->exec) {
+    e = cudaGraphInstantiate(&b->exec, g, 0);
+    if (e != cudaSuccess) {
+      cudaGraphDestroy(g);
+      b->exec = nullptr;
+      return ct2g_cuda_fail(c0, e, "cudaGraphInstantiate");
+    }
+  }
+  cudaGraphDestroy(g);
+  b->launches.assign(nctx, 0);
+  b->epochs.assign(nctx, 0);
+  b->ns.assign(nctx, 0);
+  b->begins.assign(nctx, 0);
+  for (size_t i = 0; i < nctx; i++) {
+    ct2g_ctx *c = b->ctx[i];
+    b->launches[i] = c->launches - l0[i];
+    c->launches = l0[i];  // recording launches nothing
+    b->epochs[i] = c->epoch;
+    b->ns[i] = c->n;
+    b->begins[i] = c->rung_begin;
+  }
+  b->p = *p;
+  b->dt = dt;
+  b->scale = scale;
+  b->recorded = true;
+  return CT2G_OK;
+}
+
+int replay(ct2g_batch *b, int *max_rung) {
+  ct2g_ctx *c0 = b->ctx[0];
+  // the graph runs after the work already queued on every member's stream,
+  // and every member's stream waits for the graph
+  for (size_t i = 0; i < b->ctx.size(); i++) {
+    ct2g_ctx *c = b->ctx[i];
+    if (c->stream == b->s0) continue;
+    CT2G_CUDA(c0, cudaEventRecord(b->join[i], c->stream));
+    CT2G_CUDA(c0, cudaStreamWaitEvent(b->s0, b->join[i], 0));
+  }
+  CT2G_CUDA(c0, cudaEventRecord(b->t0, b->s0));
+  CT2G_CUDA(c0, cudaGraphLaunch(b->exec, b->s0));
+  CT2G_CUDA(c0, cudaEventRecord(b->t1, b->s0));
+  for (size_t i = 0; i < b->ctx.size(); i++) {
+    ct2g_ctx *c = b->ctx[i];
+    c->launches += b->launches[i];
+    if (c->stream != b->s0) CT2G_CUDA(c0, cudaStreamWaitEvent(c->stream, b->t1, 0));
+  }
+  b->launched = true;
+  if (max_rung) {
+    CT2G_CUDA(c0, cudaStreamSynchronize(b->s0));
+    int m = 0;
+    for (size_t i = 0; i < b->ctx.size(); i++) m = std::max(m, b->h_maxrung[i]);
+    *max_rung = m;
+  }
+  return CT2G_OK;
+}
+
+int batch_step(ct2g_batch *b, const ct2g_kick_params *p, float dt, float scale, int *max_rung) {
+  ct2g_ctx *c0 = b->ctx[0];
+  CT2G_TRY(check_params(c0, p, scale));
+  if (!same_recording(b, p, dt, scale)) CT2G_TRY(record(b, p, dt, scale));
+  return replay(b, max_rung);
+}
+
+int batch_new(ct2g_ctx *const *ctxs, int nctx, ct2g_batch **out) {
+  ct2g_batch *b = new ct2g_batch();
+  b->ctx.assign(ctxs, ctxs + nctx);
+  b->device = ctxs[0]->device;
+  b->s0 = ctxs[0]->stream;
+  b->join.assign(nctx, nullptr);
+  cudaError_t e = cudaSetDevice(b->device);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreate(&b->t0);
+  if (e == cudaSuccess) e = cudaEventCreate(&b->t1);
+  for (int i = 0; i < nctx && e == cudaSuccess; i++)
+    e = cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaMallocHost(&b->h_maxrung, sizeof(int) * nctx);
+  if (e != cudaSuccess) {
+    ct2g_cuda_fail(ctxs[0], e, "batch setup");
+    ct2g_batch_destroy(b);
+    return CT2G_ECUDA;
+  }
+  std::memset(b->h_maxrung, 0, sizeof(int) * nctx);
+  *out = b;
+  return CT2G_OK;
+}
+
+// ---------------------------------------------------------------------------
+// autotuner
+// ---------------------------------------------------------------------------
+std::string tune_key(const ct2g_ctx *c) {
+  int oct = 0;
+  while (((size_t)2 << oct) <= c->n) oct++;
+  char buf[160];
+  std::snprintf(buf, sizeof(buf), "m%d_p%d_bw%.3f_k%d_box%d_n2^%d", c->M, c->p, c->opt.bwidth,
+                c->opt.kernel, c->nbox, oct);
+  return buf;
+}
+
+struct Saved {
+  void *p[8] = {};
+  size_t bytes[8] = {};
+};
+
+int save_store(ct2g_ctx *c, Saved &s) {
+  void *src[8] = {c->x, c->y, c->z, c->vx, c->vy, c->vz, c->rung, c->id};
+  const size_t n = c->n;
+  const size_t bytes[8] = {n * 4, n * 4, n * 4, n * 4, n * 4, n * 4, n, n * 4};
+  for (int k = 0; k < 8; k++) {
+    s.bytes[k] = bytes[k];
+    CT2G_CUDA(c, cudaMalloc(&s.p[k], std::max<size_t>(bytes[k], 16)));
+    CT2G_CUDA(c, cudaMemcpyAsync(s.p[k], src[k], bytes[k], cudaMemcpyDeviceToDevice, c->stream));
+  }
+  return CT2G_OK;
+}
+
+int restore_store(ct2g_ctx *c, const Saved &s) {
+  void *dst[8] = {c->x, c->y, c->z, c->vx, c->vy, c->vz, c->rung, c->id};
+  for (int k = 0; k < 8; k++)
+    CT2G_CUDA(c, cudaMemcpyAsync(dst[k], s.p[k], s.bytes[k], cudaMemcpyDeviceToDevice, c->stream));
+  c->grid_valid = c->moments_valid = c->expansions_valid = c->forces_valid = false;
+  return CT2G_OK;
+}
+
+void free_store(Saved &s) {
+  for (void *p : s.p)
+    if (p) cudaFree(p);
+}
+
+}  // namespace
+
+extern "C" {
+
+int ct2g_kick_drift(ct2g_ctx *ctx, const ct2g_kick_params *p, float dt, float scale, int flags,
+                    int *max_rung) {
+  CT2G_TRY(ct2g_check(ctx));
+  CT2G_TRY(check_params(ctx, p, scale));
+  if (flags & CT2G_STEP_GRAPH) {
+    if (!ctx->self_batch) CT2G_TRY(batch_new(&ctx, 1, &ctx->self_batch));
+    return batch_step(ctx->self_batch, p, dt, scale, max_rung);
+  }
+  CT2G_TRY(step_body(ctx, p, dt, scale));
+  if (max_rung) {
+    CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->h_pinned, ctx->d_maxrung, sizeof(int),
+                                   cudaMemcpyDeviceToHost, ctx->stream));
+    CT2G_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    *max_rung = (int)ctx->h_pinned[0];
+  }
+  return CT2G_OK;
+}
+
+int ct2g_batch_create(ct2g_ctx *const *ctxs, int nctx, ct2g_batch **out) {
+  if (!ctxs || nctx < 1 || !out) return CT2G_EINVAL;
+  *out = nullptr;
+  for (int i = 0; i < nctx; i++) {
+    if (!ctxs[i]) return CT2G_EINVAL;
+    if (ctxs[i]->device != ctxs[0]->device)
+      return ct2g_fail(ctxs[0], CT2G_EINVAL, "batch contexts must share one device");
+    for (int j = 0; j < i; j++)
+      if (ctxs[j] == ctxs[i]) return ct2g_fail(ctxs[0], CT2G_EINVAL, "context listed twice");
+  }
+  return batch_new(ctxs, nctx, out);
+}
+
+int ct2g_batch_kick_drift(ct2g_batch *b, const ct2g_kick_params *p, float dt, float scale,
+                          int *max_rung) {
+  if (!b) return CT2G_EINVAL;
+  return batch_step(b, p, dt, scale, max_rung);
+}
+
+int ct2g_batch_last_ms(ct2g_batch *b, float *ms) {
+  if (!b || !ms) return CT2G_EINVAL;
+  ct2g_ctx *c0 = b->ctx[0];
+  if (!b->launched) return ct2g_fail(c0, CT2G_ESTATE, "batch not launched yet");
+  CT2G_TRY(ct2g_check(c0));
+  CT2G_CUDA(c0, cudaEventSynchronize(b->t1));
+  CT2G_CUDA(c0, cudaEventElapsedTime(ms, b->t0, b->t1));
+  return CT2G_OK;
+}
+
+int ct2g_batch_destroy(ct2g_batch *b) {
+  if (!b) return CT2G_OK;
+  cudaSetDevice(b->device);
+  // wait through the batch's own event: the member streams may be gone
+  if (b->launched) cudaEventSynchronize(b->t1);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->fork) cudaEventDestroy(b->fork);
+  if (b->t0) cudaEventDestroy(b->t0);
+  if (b->t1) cudaEventDestroy(b->t1);
+  for (cudaEvent_t e : b->join)
+    if (e) cudaEventDestroy(e);
+  if (b->h_maxrung) cudaFreeHost(b->h_maxrung);
+  delete b;
+  return CT2G_OK;
+}
+
+int ct2g_get_tuning(const ct2g_ctx *ctx, ct2g_tuning *t) {
+  if (!ctx || !t) return CT2G_EINVAL;
+  std::memset(t, 0, sizeof(*t));
+  t->dense_cell = (int)ctx->dense_cell;
+  t->near_blocks_per_sm = ctx->near_blocks_per_sm;
+  t->fft_tile = ctx->fft_tile;
+  return CT2G_OK;
+}
+
+int ct2g_set_tuning(ct2g_ctx *ctx, const ct2g_tuning *t) {
+  if (!ctx || !t) return CT2G_EINVAL;
+  if (t->dense_cell < 1 || t->dense_cell > 4096 || t->near_blocks_per_sm < 0 ||
+      t->near_blocks_per_sm > 32 || t->fft_tile < 0 || t->fft_tile > 512)
+    return ct2g_fail(ctx, CT2G_EINVAL, "tuning out of range");
+  ctx->dense_cell = (uint32_t)t->dense_cell;
+  ctx->near_blocks_per_sm = t->near_blocks_per_sm;
+  ctx->fft_tile = t->fft_tile;
+  ctx->epoch++;  // launch shapes are part of a recorded graph
+  ctx->grid_valid = false;  // the chunk lists depend on dense_cell
+  return CT2G_OK;
+}
+
+int ct2g_autotune(ct2g_ctx *ctx, const ct2g_kick_params *p, float dt, float scale,
+                  const char *cache_path, ct2g_tuning *out) {
+  CT2G_TRY(ct2g_check(ctx));
+  CT2G_TRY(check_params(ctx, p, scale));
+  if (!ctx->has_particles || ctx->n == 0) return ct2g_fail(ctx, CT2G_ESTATE, "no particles uploaded");
+  const std::string key = tune_key(ctx);
+  ct2g_tuning best;
+  CT2G_TRY(ct2g_get_tuning(ctx, &best));
+  if (cache_path) {
+    std::ifstream f(cache_path);
+    std::string line;
+    while (std::getline(f, line)) {
+      std::istringstream ls(line);
+      std::string k;
+      ct2g_tuning t;
+      std::memset(&t, 0, sizeof(t));
+      double ms = 0;
+      if (ls >> k >> t.dense_cell >> t.near_blocks_per_sm >> t.fft_tile >> ms && k == key &&
+          ct2g_set_tuning(ctx, &t) == CT2G_OK) {
+        if (out) *out = t;
+        return CT2G_OK;
+      }
+    }
+  }
+  Saved saved;
+  int rc = save_store(ctx, saved);
+  float best_ms = 0.f;
+  // time one tuning: a recorded step (warm), then the fastest of three
+  // replays, each from the saved particles
+  auto time_one = [&](const ct2g_tuning &t, float &ms) -> int {
+    CT2G_TRY(ct2g_set_tuning(ctx, &t));
+    CT2G_TRY(restore_store(ctx, saved));
+    CT2G_TRY(ct2g_kick_drift(ctx, p, dt, scale, CT2G_STEP_GRAPH, nullptr));
+    ms = 1e30f;
+    for (int r = 0; r < 3; r++) {
+      CT2G_TRY(restore_store(ctx, saved));
+      CT2G_TRY(ct2g_kick_drift(ctx, p, dt, scale, CT2G_STEP_GRAPH, nullptr));
+      float m = 0.f;
+      CT2G_TRY(ct2g_batch_last_ms(ctx->self_batch, &m));
+      ms = std::min(ms, m);
+    }
+    return CT2G_OK;
+  };
+  if (rc == CT2G_OK) rc = time_one(best, best_ms);
+  // coordinate descent over the three shapes
+  const int W = ctx->M >= 256 ? 16 : 4096 / ctx->M;
+  std::vector<std::vector<int>> cand = {
+      {8, 12, 16, 24, 32, 48},  // dense_cell
+      {0, 1, 2},                // near_blocks_per_sm
+      ctx->M >= 64 ? std::vector<int>{0, W / 2, 2 * W} : std::vector<int>{0}};
+  for (int dim = 0; dim < 3 && rc == CT2G_OK; dim++) {
+    for (int v : cand[dim]) {
+      ct2g_tuning t = best;
+      int *field = dim == 0 ? &t.dense_cell : dim == 1 ? &t.near_blocks_per_sm : &t.fft_tile;
+      if (*field == v) continue;
+      *field = v;
+      float ms = 0.f;
+      if ((rc = time_one(t, ms)) != CT2G_OK) break;
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = t;
+      }
+    }
+  }
+  // keep the best, and leave the particles as they were
+  if (rc == CT2G_OK) rc = ct2g_set_tuning(ctx, &best);
+  if (saved.p[0]) {
+    const int r2 = restore_store(ctx, saved);
+    if (rc == CT2G_OK) rc = r2;
+    cudaStreamSynchronize(ctx->stream);
+  }
+  free_store(saved);
+  if (rc != CT2G_OK) return rc;
+  if (cache_path) {
+    std::ofstream f(cache_path, std::ios::app);
+    if (f) f << key << ' ' << best.dense_cell << ' ' << best.near_blocks_per_sm << ' ' << best.fft_tile << ' ' << best_ms << '\n';
+  }
+  if (out) *out = best;
+  return CT2G_OK;
+}
+
+}  // extern "C"

@@ -150,18 +150,36 @@ struct ct2g_ctx {
                                    // (particle index) then sparse ones (sparse_list index)
   uint32_t *sparse_list = nullptr; // particles of sparse cells, in order
   uint32_t *flags = nullptr;
-  uint32_t nchunks = 0;   // dense chunks
-  uint32_t nschunks = 0;  // sparse chunks
-  uint32_t nsparse = 0;
+  // work-list sizes stay on the device, so a step needs no host readback:
+  // [0] dense chunks, [1] sparse sinks, [2] sparse chunks, [3] and [4] the
+  // dense and sparse near-field work counters
+  uint32_t *d_counts = nullptr;
+  uint32_t dense_cell = 16;  // cells with at least this many particles get their own chunks
+  int near_blocks_per_sm = 0;  // persistent near-field grid: blocks per SM (0: occupancy)
+  int fft_tile = 0;            // y/x FFT pass tile width (0: default)
+  struct ct2g_batch *self_batch = nullptr;  // graph of ct2g_kick_drift
+
+  // independent periodic boxes sharing the mesh: box b holds particles
+  // [box_off[b], box_off[b+1]); its cells are keys (b << 3*mbits) | morton
+  int nbox = 1;
+  int boxbits = 0;
+  int64_t CB = 0;                    // nbox * C
+  std::vector<uint64_t> h_box_off;   // [nbox+1]
+  std::vector<float> h_box_gm;       // [nbox]: G x particle mass
+  bool boxes_set = true;
+  uint32_t *box_off = nullptr;       // device [nbox+1]
+  float *box_gm = nullptr;           // device [nbox]
+  uint64_t epoch = 0;                // bumped when buffers or parameters change
+  bool capturing = false;            // recording a CUDA graph: no events, no host reads
   // forces
   float *fx = nullptr, *fy = nullptr, *fz = nullptr, *pot = nullptr;
   int *d_maxrung = nullptr;
   unsigned long long *d_inter = nullptr;
   uint32_t *h_pinned = nullptr;  // small pinned host scratch
   // mesh
-  float *grid = nullptr;    // [nc][C] real: moments, then expansions
-  float2 *spec = nullptr;   // [nc][CK] complex
-  float *greens = nullptr;  // [nc][CK] real-or-imag
+  float *grid = nullptr;    // [nc][nbox][C] real: moments, then expansions
+  float2 *spec = nullptr;   // [nc][nbox][CK] complex
+  float *greens = nullptr;  // [nc][CK] real-or-imag, shared by the boxes
   float2 *tw32 = nullptr;   // twiddles exp(-2 pi i k/M), k < M/2
   double2 *tw64 = nullptr;
   int tw_n = 0;
@@ -212,9 +230,18 @@ int ct2g_cuda_fail(ct2g_ctx *ctx, cudaError_t e, const char *what);
 int ct2g_alloc_particles(ct2g_ctx *ctx, size_t n);
 int ct2g_alloc_mesh(ct2g_ctx *ctx);
 // exclusive scan (+ offset) of n uint32 values; in may equal out
+// (total_dev: optional device word that receives the sum)
 int ct2g_scan_exclusive(ct2g_ctx *ctx, const uint32_t *in, uint32_t *out, size_t n,
-                        uint32_t *total_host, uint32_t offset);
+                        uint32_t *total_dev, uint32_t offset);
+// words of scan scratch for n inputs
+size_t ct2g_scan_scratch_words(size_t n);
+// stage-time event k, skipped while a graph is recorded
+void ct2g_mark(ct2g_ctx *ctx, int k);
 int ct2g_bin_range(ct2g_ctx *ctx);
+int ct2g_check(ct2g_ctx *ctx);  // valid context; selects its device
+// far field of the current range into the force buffers (P2M if needed, mesh
+// solve with the fused inverse z pass + L2P)
+int ct2g_far_field(ct2g_ctx *ctx, bool pot);
 int ct2g_build_greens(ct2g_ctx *ctx);
 int ct2g_p2m(ct2g_ctx *ctx);
 // mesh solve; fused_l2p: the inverse z pass evaluates the far field of every

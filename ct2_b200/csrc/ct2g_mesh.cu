@@ -21,22 +21,25 @@
 namespace {
 
 // ---------------------------------------------------------------------------
-// P2M: one thread per cell (particles are cell-sorted, so no atomics)
+// P2M: one thread per cell (particles are cell-sorted, so no atomics).
+// Thread t is row-major cell t % C of box t / C; moments are per unit mass
+// (the box's GM is applied to the forces).
 // ---------------------------------------------------------------------------
 template <int P>
 __global__ void __launch_bounds__(128) p2m_kernel(const uint32_t *__restrict__ x,
                                                   const uint32_t *__restrict__ y,
                                                   const uint32_t *__restrict__ z,
                                                   const uint32_t *__restrict__ cs, int mbits,
-                                                  int64_t C, float *__restrict__ grid) {
+                                                  int64_t CB, float *__restrict__ grid) {
   constexpr MiTable<P> T{};
   constexpr int NC = MiTable<P>::NC;
-  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;  // row-major cell
-  if (c >= C) return;
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;  // box * C + row-major cell
+  if (c >= CB) return;
   const uint32_t M1 = (1u << mbits) - 1u;
-  const uint32_t cx = (uint32_t)(c >> (2 * mbits)), cy = (uint32_t)(c >> mbits) & M1,
+  const uint32_t cx = (uint32_t)(c >> (2 * mbits)) & M1, cy = (uint32_t)(c >> mbits) & M1,
                  cz = (uint32_t)c & M1;
-  const uint32_t key = ct2g_morton(cx, cy, cz);
+  const uint32_t box = (uint32_t)(c >> (3 * mbits));
+  const uint32_t key = (box << (3 * mbits)) | ct2g_morton(cx, cy, cz);
   const uint32_t b = cs[key], e = cs[key + 1];
   double acc[NC];
 #pragma unroll
@@ -61,7 +64,7 @@ __global__ void __launch_bounds__(128) p2m_kernel(const uint32_t *__restrict__ x
     for (int k = 0; k < NC; k++) acc[k] += px[T.nx[k]] * py[T.ny[k]] * pz[T.nz[k]];
   }
 #pragma unroll
-  for (int k = 0; k < NC; k++) grid[(int64_t)k * C + c] = (float)acc[k];
+  for (int k = 0; k < NC; k++) grid[(int64_t)k * CB + c] = (float)acc[k];
 }
 
 // ---------------------------------------------------------------------------
@@ -106,7 +109,7 @@ struct Mg2lTab {
 // stay in registers
 template <int P, int I>
 __device__ __forceinline__ void mg2l_term(const float2 *m, const float *gcol, float2 &acc,
-                                          float2 *out, int64_t CK) {
+                                          float2 *out, int64_t SK) {
   constexpr int A = Mg2lTab<P>::t.a[I], B = Mg2lTab<P>::t.b[I], AB = Mg2lTab<P>::t.ab[I];
   constexpr bool FIRST = Mg2lTab<P>::t.first[I] != 0, LAST = Mg2lTab<P>::t.last[I] != 0,
                  ODD = Mg2lTab<P>::t.odd[I] != 0;
@@ -120,35 +123,37 @@ __device__ __forceinline__ void mg2l_term(const float2 *m, const float *gcol, fl
     acc.x = fmaf(-gv, mb.y, acc.x);
     acc.y = fmaf(gv, mb.x, acc.y);
   }
-  if constexpr (LAST) out[(int64_t)A * CK] = acc;
+  if constexpr (LAST) out[(int64_t)A * SK] = acc;
 }
 
 template <int P, int... I>
 __device__ __forceinline__ void mg2l_all(const float2 *m, const float *gcol, float2 *out,
-                                         int64_t CK, std::integer_sequence<int, I...>) {
+                                         int64_t SK, std::integer_sequence<int, I...>) {
   float2 acc = make_float2(0.f, 0.f);
-  (mg2l_term<P, I>(m, gcol, acc, out, CK), ...);
+  (mg2l_term<P, I>(m, gcol, acc, out, SK), ...);
 }
 
 // MG2L: one thread per k-point, in place on the spectrum.  G_n is real for
 // even |n| and i*g for odd |n| (parity of D^n phi).  The thread's Green's
 // values go to a private smem column (no sharing, so no barrier); the moments
-// stay in registers.
+// stay in registers.  blockIdx.y is the box: the spectrum holds component k
+// of box b at (k * nbox + b) * CK, and the boxes share G.
 template <int P>
 __global__ void __launch_bounds__(128) mg2l_kernel(float2 *__restrict__ spec,
-                                                   const float *__restrict__ G, int64_t CK) {
+                                                   const float *__restrict__ G, int64_t CK,
+                                                   int64_t SK) {
   constexpr int NC = ct2g_ncomp(P);
   __shared__ float gs[NC * 128];
   const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= CK) return;
+  float2 *sp = spec + (int64_t)blockIdx.y * CK + q;
   float2 m[NC];
 #pragma unroll
   for (int k = 0; k < NC; k++) {
-    m[k] = spec[(int64_t)k * CK + q];
+    m[k] = sp[(int64_t)k * SK];
     gs[k * 128 + threadIdx.x] = __ldg(G + (int64_t)k * CK + q);
   }
-  mg2l_all<P>(m, gs + threadIdx.x, spec + q, CK,
-              std::make_integer_sequence<int, Mg2lPairs<P>::NP>{});
+  mg2l_all<P>(m, gs + threadIdx.x, sp, SK, std::make_integer_sequence<int, Mg2lPairs<P>::NP>{});
 }
 
 // ---------------------------------------------------------------------------
@@ -320,8 +325,8 @@ double factd(int n) {
 template <int P>
 int launch_p2m(ct2g_ctx *ctx) {
   const unsigned T = 128;
-  p2m_kernel<P><<<ct2g_div_up(ctx->C, T), T, 0, ctx->stream>>>(
-      ctx->x, ctx->y, ctx->z, ctx->cell_start, ctx->mbits, ctx->C, ctx->grid);
+  p2m_kernel<P><<<ct2g_div_up(ctx->CB, T), T, 0, ctx->stream>>>(
+      ctx->x, ctx->y, ctx->z, ctx->cell_start, ctx->mbits, ctx->CB, ctx->grid);
   CT2G_LAUNCHED(ctx);
   return CT2G_OK;
 }
@@ -329,8 +334,9 @@ int launch_p2m(ct2g_ctx *ctx) {
 template <int P>
 int launch_mg2l(ct2g_ctx *ctx) {
   const unsigned T = 128;
-  mg2l_kernel<P><<<ct2g_div_up(ctx->CK, T), T, 0, ctx->stream>>>(ctx->spec, ctx->greens,
-                                                                  ctx->CK);
+  const dim3 grid(ct2g_div_up(ctx->CK, T), (unsigned)ctx->nbox);
+  mg2l_kernel<P><<<grid, T, 0, ctx->stream>>>(ctx->spec, ctx->greens, ctx->CK,
+                                               ctx->CK * ctx->nbox);
   CT2G_LAUNCHED(ctx);
   return CT2G_OK;
 }
@@ -343,6 +349,7 @@ static const int kGreensKmax = 36;
 
 int ct2g_build_greens(ct2g_ctx *ctx) {
   if (ctx->greens_valid) return CT2G_OK;
+  if (ctx->capturing) return ct2g_fail(ctx, CT2G_ESTATE, "Green's table not built before recording");
   const int p = ctx->p, nc = ctx->nc, M = ctx->M;
   // D^n term tables and multi-indices
   std::vector<DTerm> terms((size_t)nc * kMaxTerms);
@@ -454,9 +461,9 @@ int ct2g_p2m(ct2g_ctx *ctx) {
 // (which overwrite the moments in ctx->grid)
 int ct2g_mesh_solve(ct2g_ctx *ctx, bool fused_l2p, bool pot) {
   CT2G_TRY(ct2g_build_greens(ctx));
-  cudaEventRecord(ctx->ev[2], ctx->stream);
-  CT2G_TRY(ct2g_fft_r2c_f32(ctx, ctx->grid, ctx->spec, ctx->M, ctx->nc, ctx->ldk));
-  cudaEventRecord(ctx->ev[3], ctx->stream);
+  ct2g_mark(ctx, 2);
+  CT2G_TRY(ct2g_fft_r2c_f32(ctx, ctx->grid, ctx->spec, ctx->M, ctx->nc * ctx->nbox, ctx->ldk));
+  ct2g_mark(ctx, 3);
   switch (ctx->p) {
     case 1: CT2G_TRY(launch_mg2l<1>(ctx)); break;
     case 2: CT2G_TRY(launch_mg2l<2>(ctx)); break;
@@ -466,7 +473,7 @@ int ct2g_mesh_solve(ct2g_ctx *ctx, bool fused_l2p, bool pot) {
     case 6: CT2G_TRY(launch_mg2l<6>(ctx)); break;
     default: return ct2g_fail(ctx, CT2G_EINVAL, "unsupported order");
   }
-  cudaEventRecord(ctx->ev[4], ctx->stream);
+  ct2g_mark(ctx, 4);
   if (fused_l2p) {
     // every particle of the range gets its far field; others read zero
     const size_t n = ctx->n;
@@ -476,8 +483,8 @@ int ct2g_mesh_solve(ct2g_ctx *ctx, bool fused_l2p, bool pot) {
     if (pot) CT2G_CUDA(ctx, cudaMemsetAsync(ctx->pot, 0, n * 4, ctx->stream));
     CT2G_TRY(ct2g_fft_c2r_l2p(ctx, pot));
   } else {
-    CT2G_TRY(ct2g_fft_c2r_f32(ctx, ctx->spec, ctx->grid, ctx->M, ctx->nc, ctx->ldk));
+    CT2G_TRY(ct2g_fft_c2r_f32(ctx, ctx->spec, ctx->grid, ctx->M, ctx->nc * ctx->nbox, ctx->ldk));
   }
-  cudaEventRecord(ctx->ev[5], ctx->stream);
+  ct2g_mark(ctx, 5);
   return CT2G_OK;
 }

@@ -32,12 +32,13 @@ __constant__ int c_stencil[4 * 729];  // (ox, oy, oz, unused) per offset
 __constant__ uint32_t c_doff[27 * 3];  // dilated block offsets, x/y/z lanes of the key
 
 struct Walk {
-  uint32_t mx, my, mz;  // block-key masks of the x, y, z bits
+  uint32_t mx, my, mz;  // block-key masks of the x, y, z bits; the bits above
+                        // them are the box index, which the walk keeps
   __device__ __forceinline__ uint32_t add(uint32_t sb, int o) const {
     const uint32_t x = ((sb | ~mx) + c_doff[3 * o]) & mx;
     const uint32_t y = ((sb | ~my) + c_doff[3 * o + 1]) & my;
     const uint32_t z = ((sb | ~mz) + c_doff[3 * o + 2]) & mz;
-    return x | y | z;
+    return x | y | z | (sb & ~(mx | my | mz));
   }
 };
 
@@ -71,7 +72,9 @@ __device__ __forceinline__ void pair_term(float dx, float dy, float dz, float h2
   if (POT) ap -= pp;
 }
 
-// Near field, one warp per chunk of <= 32 sinks.  A dense chunk is sinks of
+// Near field, one warp per chunk of <= 32 sinks; the grid is persistent and
+// warps take chunks from a device work counter until the device-held chunk
+// count is reached.  A dense chunk is sinks of
 // one cell; a sparse chunk is sinks of sparse cells of one 4x4x4 block.  The
 // warp walks the union of its sinks' stencils (per neighbouring block:
 // occupancy & the OR of the sinks' stencil masks), fetching the ranges of 32
@@ -87,25 +90,22 @@ __device__ __forceinline__ void inblock(int b, int &x, int &y, int &z) {
 }
 
 template <int KERNEL, bool POT, bool SPARSE>
-__global__ void __launch_bounds__(256) near_kernel(
-    const uint2 *__restrict__ chunks, uint32_t nchunks, const uint32_t *__restrict__ sparse_list,
+__device__ __forceinline__ void near_chunk(
+    const uint2 cd, const uint32_t *__restrict__ sparse_list,
     const uint32_t *__restrict__ cs, const unsigned long long *__restrict__ occ,
-    const unsigned long long *__restrict__ stmask, Walk walk, const uint32_t *__restrict__ skeys,
-    uint32_t rbegin, const float4 *__restrict__ src, int mbits, float soft, float bw2, float GM,
+    const unsigned long long *__restrict__ stmask, const Walk &walk,
+    const uint32_t *__restrict__ skeys, uint32_t rbegin, const float4 *__restrict__ src,
+    int mbits, float soft, float bw2, const float *__restrict__ box_gm,
     float *__restrict__ ofx, float *__restrict__ ofy, float *__restrict__ ofz,
-    float *__restrict__ opot, unsigned long long *__restrict__ inter) {
-  __shared__ float4 sbuf[8][32];  // one batch of 32 sources per warp
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const uint32_t ch = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (ch >= nchunks) return;
+    float *__restrict__ opot, unsigned long long *__restrict__ inter, float4 *sb, int lane) {
   const int M = 1 << mbits;
-  const uint2 cd = chunks[ch];
   const bool act = (uint32_t)lane < cd.y;
   const uint32_t slot = cd.x + (act ? (uint32_t)lane : 0u);
   const uint32_t i = SPARSE ? sparse_list[slot] : slot;
   const uint32_t key = skeys[i - rbegin];
   const float4 si = src[i];
   const uint32_t p = key & 63u, blk = key >> 6;  // blk is the same for the whole chunk
+  const float GM = __ldg(box_gm + (key >> (3 * mbits)));
   int px, py, pz;
   inblock((int)p, px, py, pz);
   // cells of the block present in the chunk
@@ -130,7 +130,6 @@ __global__ void __launch_bounds__(256) near_kernel(
   const float h2 = soft * soft, hinv = 1.f / soft, hinv3 = hinv * hinv * hinv;
   float nx = 0.f, ny = 0.f, nz = 0.f, np = 0.f;
   uint32_t nsrc = 0;
-  float4 *sb = sbuf[wib];
   for (int o = 0; o < 27; o++) {
     const unsigned long long bits = __shfl_sync(0xffffffffu, word, o);
     if (!bits) continue;
@@ -198,6 +197,33 @@ __global__ void __launch_bounds__(256) near_kernel(
   if (lane == 0 && c && inter) atomicAdd(inter, c);
 }
 
+// counts[0] dense chunks, counts[2] sparse chunks (stored after the dense
+// ones), counts[3] / counts[4] the work counters (zero at launch)
+template <int KERNEL, bool POT, bool SPARSE>
+__global__ void __launch_bounds__(256) near_kernel(
+    const uint2 *__restrict__ chunks, uint32_t *__restrict__ counts,
+    const uint32_t *__restrict__ sparse_list, const uint32_t *__restrict__ cs,
+    const unsigned long long *__restrict__ occ, const unsigned long long *__restrict__ stmask,
+    Walk walk, const uint32_t *__restrict__ skeys, uint32_t rbegin,
+    const float4 *__restrict__ src, int mbits, float soft, float bw2,
+    const float *__restrict__ box_gm, float *__restrict__ ofx, float *__restrict__ ofy,
+    float *__restrict__ ofz, float *__restrict__ opot, unsigned long long *__restrict__ inter) {
+  __shared__ float4 sbuf[8][32];  // one batch of 32 sources per warp
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const uint32_t nch = SPARSE ? counts[2] : counts[0];
+  const uint2 *list = SPARSE ? chunks + counts[0] : chunks;
+  uint32_t *work = counts + (SPARSE ? 4 : 3);
+  for (;;) {
+    uint32_t ch = 0;
+    if (lane == 0) ch = atomicAdd(work, 1u);
+    ch = __shfl_sync(0xffffffffu, ch, 0);
+    if (ch >= nch) break;
+    near_chunk<KERNEL, POT, SPARSE>(list[ch], sparse_list, cs, occ, stmask, walk, skeys, rbegin,
+                                    src, mbits, soft, bw2, box_gm, ofx, ofy, ofz, opot, inter,
+                                    sbuf[wib], lane);
+  }
+}
+
 Walk make_walk(int mbits) {
   Walk w{0u, 0u, 0u};
   for (int i = 0; i < mbits - 2; i++) {
@@ -208,26 +234,31 @@ Walk make_walk(int mbits) {
   return w;
 }
 
+// persistent grid: the resident blocks of every SM (or the tuned count), and
+// no more than one block per 256 sinks of the range
+template <int K, bool POT, bool SPARSE>
+int launch_near1(ct2g_ctx *ctx, const Walk &walk, float bw2) {
+  auto k = near_kernel<K, POT, SPARSE>;
+  int per_sm = 0;
+  CT2G_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 256, 0));
+  const size_t nr = ctx->n - ctx->rung_begin;
+  if (ctx->near_blocks_per_sm > 0) per_sm = std::min(per_sm, ctx->near_blocks_per_sm);
+  size_t blocks = (size_t)std::max(1, per_sm) * ctx->num_sms;
+  blocks = std::max<size_t>(1, std::min(blocks, (nr + 255) / 256));
+  k<<<(unsigned)blocks, 256, 0, ctx->stream>>>(
+      ctx->chunks, ctx->d_counts, ctx->sparse_list, ctx->cell_start, ctx->occ, ctx->stmask, walk,
+      ctx->keys, (uint32_t)ctx->rung_begin, ctx->src, ctx->mbits, ctx->opt.hsoft, bw2,
+      ctx->box_gm, ctx->fx, ctx->fy, ctx->fz, ctx->pot, ctx->d_inter);
+  CT2G_LAUNCHED(ctx);
+  return CT2G_OK;
+}
+
 template <int K, bool POT>
 int launch_near(ct2g_ctx *ctx) {
   const Walk walk = make_walk(ctx->mbits);
   const float bw2 = ctx->opt.bwidth * ctx->opt.bwidth;
-  const unsigned T = 256;
-  if (ctx->nchunks) {
-    near_kernel<K, POT, false><<<ct2g_div_up((size_t)ctx->nchunks * 32, T), T, 0, ctx->stream>>>(
-        ctx->chunks, ctx->nchunks, ctx->sparse_list, ctx->cell_start, ctx->occ, ctx->stmask, walk,
-        ctx->keys, (uint32_t)ctx->rung_begin, ctx->src, ctx->mbits, ctx->opt.hsoft, bw2,
-        ctx->opt.GM, ctx->fx, ctx->fy, ctx->fz, ctx->pot, ctx->d_inter);
-    CT2G_LAUNCHED(ctx);
-  }
-  if (ctx->nschunks) {
-    near_kernel<K, POT, true><<<ct2g_div_up((size_t)ctx->nschunks * 32, T), T, 0, ctx->stream>>>(
-        ctx->chunks + ctx->nchunks, ctx->nschunks, ctx->sparse_list, ctx->cell_start, ctx->occ,
-        ctx->stmask, walk, ctx->keys, (uint32_t)ctx->rung_begin, ctx->src, ctx->mbits,
-        ctx->opt.hsoft, bw2, ctx->opt.GM, ctx->fx, ctx->fy, ctx->fz, ctx->pot, ctx->d_inter);
-    CT2G_LAUNCHED(ctx);
-  }
-  return CT2G_OK;
+  CT2G_TRY((launch_near1<K, POT, false>(ctx, walk, bw2)));
+  return launch_near1<K, POT, true>(ctx, walk, bw2);
 }
 
 }  // namespace
@@ -255,7 +286,8 @@ int ct2g_forces(ct2g_ctx *ctx, bool pot) {
   // the far-field pass (ct2g_fft_c2r_l2p) has written the range's entries
   (void)n;
   CT2G_CUDA(ctx, cudaMemsetAsync(ctx->d_inter, 0, sizeof(unsigned long long), ctx->stream));
-  if (ctx->nchunks == 0 && ctx->nschunks == 0) return CT2G_OK;
+  CT2G_CUDA(ctx, cudaMemsetAsync(ctx->d_counts + 3, 0, 2 * sizeof(uint32_t), ctx->stream));
+  if (ctx->n == ctx->rung_begin) return CT2G_OK;
   if (ctx->opt.kernel == CT2G_SOFT_SPHERE)
     return pot ? launch_near<CT2G_SOFT_SPHERE, true>(ctx) : launch_near<CT2G_SOFT_SPHERE, false>(ctx);
   return pot ? launch_near<CT2G_SOFT_PLUMMER, true>(ctx) : launch_near<CT2G_SOFT_PLUMMER, false>(ctx);

@@ -11,6 +11,11 @@ operator interface for the gravity step (dmarce1/ct2):
   kick_step(...) (src/main.cpp:8-92)                -> Gravity.kick_step
   fft_r2c_3d / fft_c2r_3d (cosmictiger/fft.hpp:28-29) -> fft_r2c_3d / fft_c2r_3d
 
+Beyond the reference: Gravity.kick_drift (one kick + drift, optionally as a
+replayed CUDA graph), box contexts (nbox independent periodic boxes sharing
+one mesh), Batch (several contexts stepped by one graph launch) and the
+launch-shape tuning / autotuner.
+
 Arrays are numpy; every call goes to libct2g.so on the GPU.  Errors raise
 CT2GError with the library's message (the reference aborts or has none).
 """
@@ -22,7 +27,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _lib
-from ._lib import CT2GError, KickParams, Options
+from ._lib import CT2GError, KickParams, Options, Tuning
 
 
 def ncomp(p: int) -> int:
@@ -56,18 +61,20 @@ class Gravity:
     """One GPU context: particle store, mesh, Green's tensor, stream."""
 
     def __init__(self, mesh=64, order=4, bwidth=3.0, hsoft=1.0 / 50.0, eta=0.15, GM=0.0,
-                 kernel=_lib.SOFT_PLUMMER, device=0, max_particles=0):
+                 kernel=_lib.SOFT_PLUMMER, device=0, max_particles=0, nbox=1):
         self._l = _lib.load()
         o = Options()
         self._l.ct2g_default_options(ctypes.byref(o))
         o.mesh, o.order, o.bwidth, o.hsoft, o.eta, o.GM = mesh, order, bwidth, hsoft, eta, GM
         o.kernel, o.device, o.max_particles = kernel, device, max_particles
         h = ctypes.c_void_p()
-        rc = self._l.ct2g_create(ctypes.byref(o), ctypes.byref(h))
+        rc = self._l.ct2g_create_boxes(ctypes.byref(o), int(nbox), ctypes.byref(h))
         if rc != 0:
-            raise CT2GError(rc, "ct2g_create(mesh=%d, order=%d, bwidth=%g)" % (mesh, order, bwidth))
+            raise CT2GError(rc, "ct2g_create_boxes(mesh=%d, order=%d, bwidth=%g, nbox=%d)"
+                            % (mesh, order, bwidth, nbox))
         self._h = h
         self.mesh, self.order, self.bwidth, self.kernel = mesh, order, bwidth, kernel
+        self.nbox = int(nbox)
         self.nc = ncomp(order)
 
     # -- plumbing -----------------------------------------------------------
@@ -116,6 +123,14 @@ class Gravity:
     def upload_dict(self, d):
         self.upload(d["x"], d["y"], d["z"], d["vx"], d["vy"], d["vz"], d.get("rung"))
 
+    def set_boxes(self, counts, GM):
+        """Box b holds the next counts[b] uploaded particles; GM[b] = G x mass."""
+        c = np.ascontiguousarray(counts, np.uint64)
+        g = np.ascontiguousarray(GM, np.float32)
+        if len(c) != self.nbox or len(g) != self.nbox:
+            raise ValueError("need %d box counts and GM values" % self.nbox)
+        self._chk(self._l.ct2g_set_boxes(self._h, _ptr(c), _ptr(g)))
+
     def count(self):
         return int(self._l.ct2g_particle_count(self._h))
 
@@ -134,17 +149,21 @@ class Gravity:
         self._chk(self._l.ct2g_particle_to_grid(self._h))
 
     def cells(self):
-        """(begin, end) per row-major cell (i*mesh+j)*mesh+k."""
-        b = np.empty(self.mesh ** 3, np.int64)
-        e = np.empty(self.mesh ** 3, np.int64)
+        """(begin, end) per row-major cell box*mesh^3 + (i*mesh+j)*mesh+k."""
+        b = np.empty(self.nbox * self.mesh ** 3, np.int64)
+        e = np.empty(self.nbox * self.mesh ** 3, np.int64)
         self._chk(self._l.ct2g_download_cells(self._h, _ptr(b), _ptr(e)))
         return b, e
 
     def compute_multipoles(self):
         self._chk(self._l.ct2g_compute_multipoles(self._h))
 
+    def _grid_shape(self):
+        m = self.mesh
+        return (self.nc, m, m, m) if self.nbox == 1 else (self.nc, self.nbox, m, m, m)
+
     def multipoles(self):
-        out = np.empty((self.nc, self.mesh, self.mesh, self.mesh), np.float32)
+        out = np.empty(self._grid_shape(), np.float32)
         self._chk(self._l.ct2g_download_multipoles(self._h, _ptr(out)))
         return out
 
@@ -152,7 +171,7 @@ class Gravity:
         self._chk(self._l.ct2g_compute_expansions(self._h))
 
     def expansions(self):
-        out = np.empty((self.nc, self.mesh, self.mesh, self.mesh), np.float32)
+        out = np.empty(self._grid_shape(), np.float32)
         self._chk(self._l.ct2g_download_expansions(self._h, _ptr(out)))
         return out
 
@@ -189,6 +208,36 @@ class Gravity:
 
     def drift(self, dt: float, scale: float):
         self._chk(self._l.ct2g_drift(self._h, dt, scale))
+
+    def kick_drift(self, params: kick_params, dt: float, scale: float = 1.0, graph=True,
+                   wait=True):
+        """particle_to_grid + kick + drift; graph=True records the sequence
+        once into a CUDA graph and replays it.  Returns the max rung (None
+        with wait=False: the call only queues the work)."""
+        mr = ctypes.c_int(0)
+        self._chk(self._l.ct2g_kick_drift(self._h, ctypes.byref(params._c()), dt, scale,
+                                          _lib.STEP_GRAPH if graph else 0,
+                                          ctypes.byref(mr) if wait else None))
+        return mr.value if wait else None
+
+    # -- launch shapes ------------------------------------------------------
+    def tuning(self):
+        t = Tuning()
+        self._chk(self._l.ct2g_get_tuning(self._h, ctypes.byref(t)))
+        return dict(dense_cell=t.dense_cell, near_blocks_per_sm=t.near_blocks_per_sm,
+                    fft_tile=t.fft_tile)
+
+    def set_tuning(self, dense_cell=16, near_blocks_per_sm=0, fft_tile=0):
+        t = Tuning(dense_cell, near_blocks_per_sm, fft_tile)
+        self._chk(self._l.ct2g_set_tuning(self._h, ctypes.byref(t)))
+
+    def autotune(self, params: kick_params, dt: float, scale: float = 1.0, cache_path=None):
+        t = Tuning()
+        cp = None if cache_path is None else str(cache_path).encode()
+        self._chk(self._l.ct2g_autotune(self._h, ctypes.byref(params._c()), dt, scale, cp,
+                                        ctypes.byref(t)))
+        return dict(dense_cell=t.dense_cell, near_blocks_per_sm=t.near_blocks_per_sm,
+                    fft_tile=t.fft_tile)
 
     def kick_step(self, minrung, max_rung, scale, adot, tau, t0, minrung0, nocrop=False):
         """Returns (max_rung, minrung) -- the reference returns max_rung and
@@ -266,3 +315,44 @@ class Gravity:
 
     def interaction_count(self):
         return int(self._l.ct2g_interaction_count(self._h))
+
+
+class Batch:
+    """Several contexts on one device stepped by one CUDA graph launch (on the
+    first context's stream); each context runs on its own stream inside it."""
+
+    def __init__(self, contexts):
+        self._l = _lib.load()
+        self.contexts = list(contexts)
+        arr = (ctypes.c_void_p * len(self.contexts))(*[g.handle for g in self.contexts])
+        h = ctypes.c_void_p()
+        rc = self._l.ct2g_batch_create(arr, len(self.contexts), ctypes.byref(h))
+        if rc != 0:
+            raise CT2GError(rc, self._l.ct2g_last_error(self.contexts[0].handle).decode())
+        self._h = h
+
+    def _chk(self, rc):
+        if rc != 0:
+            raise CT2GError(rc, self._l.ct2g_last_error(self.contexts[0].handle).decode())
+
+    def kick_drift(self, params: kick_params, dt: float, scale: float = 1.0, wait=True):
+        mr = ctypes.c_int(0)
+        self._chk(self._l.ct2g_batch_kick_drift(self._h, ctypes.byref(params._c()), dt, scale,
+                                                ctypes.byref(mr) if wait else None))
+        return mr.value if wait else None
+
+    def last_ms(self):
+        ms = ctypes.c_float(0)
+        self._chk(self._l.ct2g_batch_last_ms(self._h, ctypes.byref(ms)))
+        return ms.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._l.ct2g_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -162,6 +162,69 @@ int ct2g_drift(ct2g_ctx *ctx, float dt, float scale);
 int ct2g_kick_step(ct2g_ctx *ctx, int *minrung, int max_rung, double scale, double adot,
                    double tau, double t0, int minrung0, int nocrop, int *out_max_rung);
 
+/* One kick + drift of every particle: particle_to_grid, kick (far field, near
+ * field, velocity and rung update) and drift -- the body of the reference's
+ * single-level step (src/main.cpp:49,68,81 at one rung level:
+ * particle_to_grid(), kick(kparams), drift(dt, scale)).  flags & CT2G_STEP_GRAPH: the sequence is recorded once
+ * into a CUDA graph and replayed while the parameters, the particle count and
+ * the buffers stay the same (any change records it again); the step then needs
+ * no host round trip.  *max_rung (may be NULL: no wait) gets kick()'s return
+ * value; with NULL the call returns as soon as the work is queued. */
+#define CT2G_STEP_GRAPH 1
+int ct2g_kick_drift(ct2g_ctx *ctx, const ct2g_kick_params *p, float dt, float scale, int flags,
+                    int *max_rung);
+
+/* Many independent periodic boxes.  No counterpart in the reference (one box
+ * per process there).  A box context holds nbox unit boxes that share the
+ * mesh, order, stencil and softening of *opt (so they share one Green's
+ * table); each box has its own particles and its own GM.  Upload the boxes'
+ * particles concatenated box after box with ct2g_upload_particles, then call
+ * ct2g_set_boxes with the per-box counts (summing to the upload) and GM
+ * (G x particle mass) before particle_to_grid.  Particles stay inside their
+ * box's range of the store.  Requires 3*log2(mesh) + ceil(log2(nbox)) <= 32.
+ * Grid downloads hold [component][box][cell]; ct2g_download_cells gives
+ * nbox*mesh^3 ranges, box-major.  Rung levels (ct2g_sort_by_rung,
+ * ct2g_kick_step) need nbox == 1. */
+int ct2g_create_boxes(const ct2g_options *opt, int nbox, ct2g_ctx **ctx);
+int ct2g_set_boxes(ct2g_ctx *ctx, const uint64_t *counts, const float *GM);
+int ct2g_box_count(const ct2g_ctx *ctx);
+
+/* A batch: several contexts on one device (e.g. box contexts of different
+ * meshes) stepped together by ONE graph launch on the first context's stream;
+ * each context's stages run on its own stream inside the graph, so the
+ * contexts overlap on the GPU.  No counterpart in the reference. */
+typedef struct ct2g_batch ct2g_batch;
+int ct2g_batch_create(ct2g_ctx *const *ctxs, int nctx, ct2g_batch **out);
+/* kick + drift of every context, as ct2g_kick_drift with CT2G_STEP_GRAPH;
+ * *max_rung (may be NULL: no wait) = the largest over the contexts */
+int ct2g_batch_kick_drift(ct2g_batch *b, const ct2g_kick_params *p, float dt, float scale,
+                          int *max_rung);
+/* device time (ms) of the last batch launch; waits for it */
+int ct2g_batch_last_ms(ct2g_batch *b, float *ms);
+int ct2g_batch_destroy(ct2g_batch *b);
+
+/* Tunable launch shapes of a context (no counterpart in the reference):
+ * dense_cell -- cells with at least this many particles get their own sink
+ * chunks, the rest are chunked per 4x4x4 block; near_blocks_per_sm -- blocks
+ * per SM of the persistent near-field grid (0: occupancy limit); fft_tile --
+ * columns per tile of the y/x FFT passes (0: default). */
+typedef struct {
+  int dense_cell;
+  int near_blocks_per_sm;
+  int fft_tile;
+  int reserved[5];
+} ct2g_tuning;
+int ct2g_get_tuning(const ct2g_ctx *ctx, ct2g_tuning *t);
+int ct2g_set_tuning(ct2g_ctx *ctx, const ct2g_tuning *t);
+/* Autotuner: times ct2g_kick_drift (graph replays) on the context's current
+ * particles for candidate tunings, keeps the fastest and restores the
+ * particles afterwards.  cache_path (may be NULL): a text file of
+ * "key dense_cell near_blocks_per_sm fft_tile ms" lines; a hit for this
+ * context's key (mesh, order, bwidth, boxes, particle-count octave) is used
+ * without timing, a miss is appended.  *out (may be NULL) gets the choice. */
+int ct2g_autotune(ct2g_ctx *ctx, const ct2g_kick_params *p, float dt, float scale,
+                  const char *cache_path, ct2g_tuning *out);
+
 /* Rung bookkeeping (src/particle.cpp:31-57,320-347). */
 int ct2g_sort_by_rung(ct2g_ctx *ctx, int minrung);        /* particle_sort_by_rung   */
 int ct2g_push_rungs(ct2g_ctx *ctx);                       /* particle_push_rungs     */
