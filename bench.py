@@ -181,6 +181,159 @@ def _config(args, world):
             "l2": "inputs larger than L2 (particle store + mesh grids >> 126 MB)"}
 
 
+BOX_METRIC = ("particles/s per kick+drift over 96 independent periodic boxes "
+              "(16^3..128^3 particles, meshes 32^3..256^3)")
+
+
+def run_boxes(args, rank, world, local):
+    """--workload boxes96: 96 independent boxes (particle counts 2^U[12,21],
+    mesh = nearest power of two to 2 N^(1/3) clipped to [32, 256], Plummer +
+    background generator seeded per box, softening = cell/25, GM = 1/N per
+    box).  plain: the boxes one after another, each through the eager calls
+    on a context of its mesh (data resident, uploads untimed).  batched: one
+    box context per mesh holding all of that mesh's boxes, autotuned, and one
+    Batch graph launch per step for all 96 boxes."""
+    import torch
+
+    from ct2_b200 import ics, replicas
+    from ct2_b200.gravity import Batch, Gravity, kick_params
+    boxes = ics.batch_boxes(96, seed=args.seed + 1000 * rank)
+    meshes = sorted({b["mesh"] for b in boxes})
+    groups = {m: [b for b in boxes if b["mesh"] == m] for m in meshes}
+    ntot = sum(len(b["x"]) for b in boxes)
+    kp = kick_params(ascending=True, descending=True, top=True, first=False, rung=0,
+                     t0=args.dt, eta=0.15, max_dt=0.01, scale=1.0)
+    keys = ("x", "y", "z", "vx", "vy", "vz")
+
+    def order_for(mesh):
+        # the sparse boxes of the small meshes need one more order for rms
+        # 1e-4 (measured 1.0e-4 and 1.1e-4 at order 4); they hold ~3% of the
+        # particles
+        return args.order + 1 if mesh <= 64 else args.order
+
+    def mk(mesh, nbox=1, nmax=0):
+        return Gravity(mesh=mesh, order=order_for(mesh), bwidth=args.bwidth,
+                       hsoft=1.0 / (25 * mesh), device=local, nbox=nbox, max_particles=nmax)
+
+    # plain: box after box, eager calls, device time per box
+    plain_ms = 0.0
+    acc = []
+    rng = np.random.Generator(np.random.PCG64(7))
+    for m in meshes:
+        g = mk(m, nmax=max(len(b["x"]) for b in groups[m]))
+        st = torch.cuda.ExternalStream(g.stream(), device=local)
+        for bi, b in enumerate(groups[m]):
+            n = len(b["x"])
+            g.upload_dict(b)
+            g.set_params(1.0 / (25 * m), 0.15, 1.0 / n)
+            if bi == 0:  # accuracy on the first box of each mesh
+                g.particle_to_grid()
+                g.compute_forces()
+                f, _ = g.forces()
+                d = g.download()
+                sel = np.sort(rng.choice(n, size=min(1024, n), replace=False))
+                t = g.ewald_direct(d["x"][sel], d["y"][sel], d["z"][sel])
+                diff = np.linalg.norm(f[sel] - t, axis=1) / np.linalg.norm(t, axis=1)
+                acc.append({"mesh": m, "particles": n, "rms_rel": float(np.sqrt(np.mean(diff ** 2))),
+                            "max_rel": float(diff.max())})
+                g.upload_dict(b)
+            for _ in range(args.warmup):
+                g.particle_to_grid()
+                g.kick(kp)
+                g.drift(args.dt, 1.0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            for _ in range(args.steps):
+                g.particle_to_grid()
+                g.kick(kp)
+                g.drift(args.dt, 1.0)
+            e1.record(st)
+            e1.synchronize()
+            plain_ms += e0.elapsed_time(e1) / args.steps
+        g.close()
+        del g
+    plain_value = ntot / (plain_ms * 1e-3)
+
+    # batched: a box context per mesh, autotuned, one graph launch per step
+    ctxs = []
+    tunings = {}
+    for m in meshes:
+        bs = groups[m]
+        g = mk(m, nbox=len(bs), nmax=sum(len(b["x"]) for b in bs))
+        cat = {k: np.concatenate([b[k] for b in bs]) for k in keys}
+        g.upload_dict(cat)
+        counts = [len(b["x"]) for b in bs]
+        g.set_boxes(counts, [1.0 / c for c in counts])
+        tunings[m] = g.autotune(kp, args.dt, 1.0, cache_path=args.tune_cache)
+        g.upload_dict(cat)
+        g.set_boxes(counts, [1.0 / c for c in counts])
+        ctxs.append((g, cat, counts))
+    batch = Batch([c[0] for c in ctxs])
+    st = torch.cuda.ExternalStream(ctxs[0][0].stream(), device=local)
+    for _ in range(args.warmup):
+        batch.kick_drift(kp, args.dt, 1.0, wait=False)
+    torch.cuda.synchronize()
+    l0 = sum(c[0].launch_count() for c in ctxs)
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(args.steps):
+        batch.kick_drift(kp, args.dt, 1.0, wait=False)
+    e1.record(st)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    ck = clocks.stop()
+    launches = sum(c[0].launch_count() for c in ctxs) - l0
+    value, ms = replicas.job_throughput(ntot, e0.elapsed_time(e1) / args.steps, device="cuda")
+
+    # end to end: every box's state host->device, one batch step, device->host
+    e2e = None
+    if not args.no_e2e:
+        def e2e_step():
+            for g, cat, counts in ctxs:
+                g.upload_dict(cat)
+                g.set_boxes(counts, [1.0 / c for c in counts])
+            batch.kick_drift(kp, args.dt, 1.0, wait=True)
+            for g, _, _ in ctxs:
+                g.download()
+        e2e_step()
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        for _ in range(max(1, args.steps // 2)):
+            e2e_step()
+        torch.cuda.synchronize()
+        ems = (time.perf_counter() - t) * 1e3 / max(1, args.steps // 2)
+        ev, _ = replicas.job_throughput(ntot, ems, device="cuda")
+        e2e = {"value": ev, "unit": UNIT, "h2d_bytes_per_step": int(ntot * 25),
+               "d2h_bytes_per_step": int(ntot * 29), "timing": "host wall clock (pageable copies)"}
+    batch.close()
+    if rank == 0:
+        line = {"metric": BOX_METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic: 96 seeded Plummer+background boxes",
+                "config": {"workload": "boxes96", "particles_per_gpu": ntot,
+                           "boxes_per_mesh": {str(m): len(groups[m]) for m in meshes},
+                           "particles_per_mesh": {str(m): int(sum(len(b["x"]) for b in groups[m]))
+                                                  for m in meshes},
+                           "order": {str(m): order_for(m) for m in meshes},
+                           "bwidth": args.bwidth,
+                           "softening": "plummer eps = cell/25", "dt": args.dt,
+                           "parallelism": "replicas" if world > 1 else "single",
+                           "l2": "inputs larger than L2"},
+                "e2e": e2e, "gpu_launches": int(launches), "roofline": None,
+                "cpu_baseline": None, "clocks": ck, "accuracy": acc,
+                "forms": {"plain_box_by_box": {"value": plain_value, "ms_per_step": plain_ms},
+                          "batched_graph": {"value": value, "ms_per_step": ms,
+                                            "tuning": {str(k): v for k, v in tunings.items()}}}}
+        print(json.dumps(line), flush=True)
+    for g, _, _ in ctxs:
+        g.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -198,6 +351,7 @@ def main():
     ap.add_argument("--accuracy-sinks", type=int, default=4096)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", default="plummer128", choices=["plummer128", "boxes96"])
     ap.add_argument("--tune-cache", default=None,
                     help="autotuner cache file (default: tune on every run)")
     args = ap.parse_args()
@@ -218,6 +372,12 @@ def main():
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     torch.cuda.set_device(local)
+
+    if args.workload == "boxes96":
+        run_boxes(args, rank, world, local)
+        if dist:
+            dist.destroy_process_group()
+        return
 
     from ct2_b200 import _lib, replicas
     from ct2_b200.gravity import Gravity
