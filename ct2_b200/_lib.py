@@ -30,6 +30,8 @@ class Tuning(ctypes.Structure):
 
 
 STEP_GRAPH = 1
+SELECT_NONE, SELECT_FIXED, SELECT_MLP, SELECT_ALL = 0, 1, 2, 3
+MLP_NIN, MLP_NHID, MLP_NPARAM = 24, 64, 5825
 
 
 class KickParams(ctypes.Structure):
@@ -79,6 +81,17 @@ SYMBOLS = [
     ("ct2g_get_tuning", _I, [_P, _P]),
     ("ct2g_set_tuning", _I, [_P, _P]),
     ("ct2g_autotune", _I, [_P, _P, _F, _F, ctypes.c_char_p, _P]),
+    ("ct2g_learned_enable", _I, [_P, _F]),
+    ("ct2g_learned_select", _I, [_P, _I, _F]),
+    ("ct2g_learned_collect", _I, [_P, _P]),
+    ("ct2g_learned_dataset", _I, [_P, _P, _P, _SZ, _P]),
+    ("ct2g_learned_clear", _I, [_P]),
+    ("ct2g_learned_cells", _I, [_P, _P, _P, _P, _P, _P, _SZ, _P, _P]),
+    ("ct2g_mlp_init", _I, [_P, ctypes.c_uint64]),
+    ("ct2g_mlp_set", _I, [_P, _P, _P, _P]),
+    ("ct2g_mlp_get", _I, [_P, _P, _P, _P]),
+    ("ct2g_mlp_train", _I, [_P, _I, _I, _F, ctypes.c_uint64, _I, _P]),
+    ("ct2g_mlp_gradients", _I, [_P, _P, _P, _SZ, _P, _P]),
     ("ct2g_kick_step", _I, [_P, _P, _I, _D, _D, _D, _D, _I, _I, _P]),
     ("ct2g_sort_by_rung", _I, [_P, _I]),
     ("ct2g_push_rungs", _I, [_P]),

@@ -49,10 +49,10 @@ def _stale(target, inputs):
     return any(os.path.getmtime(i) > t for i in inputs)
 
 
-# per-file extra flags: the near-field direct sum runs with flush-to-zero so
-# that rsqrtf is a single MUFU operation; the bit-exact update/drift kernels
+# per-file extra flags: the near-field direct sums (plain and learned shell
+# correction) run with flush-to-zero so that rsqrtf is a single MUFU operation; the bit-exact update/drift kernels
 # live in their own file with IEEE single precision
-EXTRA_FLAGS = {"ct2g_near.cu": ["-ftz=true"]}
+EXTRA_FLAGS = {"ct2g_near.cu": ["-ftz=true"], "ct2g_learned.cu": ["-ftz=true"]}
 
 
 def _compile(src, verbose):

@@ -193,7 +193,7 @@ int ct2g_alloc_particles(ct2g_ctx *ctx, size_t n) {
     CT2G_CUDA(ctx, cudaMalloc(&ctx->scan_tmp, sizeof(uint32_t) * words));
     ctx->scan_tmp_words = words;
   }
-  return CT2G_OK;
+  return ct2g_learned_resize(ctx);
 }
 
 int ct2g_alloc_mesh(ct2g_ctx *ctx) {
@@ -352,6 +352,7 @@ int ct2g_destroy(ct2g_ctx *ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   free_particles(ctx);
   if (ctx->self_batch) ct2g_batch_destroy(ctx->self_batch);
+  ct2g_learned_free(ctx);
   void *ptrs[] = {ctx->cell_start, ctx->occ, ctx->stmask, ctx->grid, ctx->spec, ctx->greens,
                   ctx->tw32, ctx->tw64, ctx->d_counts, ctx->box_off, ctx->box_gm,
                   ctx->d_maxrung, ctx->d_inter, ctx->scan_tmp};

@@ -106,6 +106,70 @@ __device__ __forceinline__ void ct2g_l2p(const LA &Lacc, float tx, float ty, flo
   pot = ph;
 }
 
+// Softened pair acceleration (src/kick.cpp:44-60) of a sink at offset d from
+// a source, accumulated into (ax, ay, az) and the potential ap; `on` false
+// adds exact zeros (masked lanes keep their summation order).
+template <int KERNEL, bool POT>
+__device__ __forceinline__ void ct2g_pair_term(float dx, float dy, float dz, float h2, float hinv,
+                                          float hinv3, float &ax, float &ay, float &az,
+                                          float &ap, bool on) {
+  const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+  float g, pp;
+  if (KERNEL == CT2G_SOFT_PLUMMER) {
+    const float ri = rsqrtf(r2 + h2);
+    g = ri * ri * ri;
+    pp = ri;
+  } else {
+    if (r2 < h2) {
+      g = hinv3;
+      pp = 1.5f * hinv - 0.5f * r2 * hinv3;
+    } else {
+      const float ri = rsqrtf(r2);
+      g = ri * ri * ri;
+      pp = ri;
+    }
+  }
+  if (!on) g = pp = 0.f;
+  ax = fmaf(-dx, g, ax);
+  ay = fmaf(-dy, g, ay);
+  az = fmaf(-dz, g, az);
+  if (POT) ap -= pp;
+}
+
+// The (a, b) pairs with |a|+|b| <= P, grouped by a: since multi-indices are
+// ordered by degree, the b of one a are exactly the first ncomp(P-|a|).
+template <int P>
+struct Mg2lPairs {
+  static constexpr int NC = ct2g_ncomp(P);
+  static constexpr int count() {
+    int n = 0;
+    for (int d = 0; d <= P; d++) n += (ct2g_ncomp(d) - (d ? ct2g_ncomp(d - 1) : 0)) * ct2g_ncomp(P - d);
+    return n;
+  }
+  static constexpr int NP = count();
+  int a[NP], b[NP], ab[NP], odd[NP], first[NP], last[NP];
+  constexpr Mg2lPairs() : a(), b(), ab(), odd(), first(), last() {
+    MiTable<P> T{};
+    int i = 0;
+    for (int ia = 0; ia < NC; ia++) {
+      const int nb = ct2g_ncomp(P - T.deg[ia]);
+      for (int ib = 0; ib < nb; ib++) {
+        a[i] = ia;
+        b[i] = ib;
+        ab[i] = ct2g_mi_index(T.nx[ia] + T.nx[ib], T.ny[ia] + T.ny[ib], T.nz[ia] + T.nz[ib]);
+        odd[i] = (T.deg[ia] + T.deg[ib]) & 1;
+        first[i] = ib == 0;
+        last[i] = ib == nb - 1;
+        i++;
+      }
+    }
+  }
+};
+template <int P>
+struct Mg2lTab {
+  static constexpr Mg2lPairs<P> t{};
+};
+
 // ---------------------------------------------------------------------------
 // Context
 // ---------------------------------------------------------------------------
@@ -158,6 +222,7 @@ struct ct2g_ctx {
   int near_blocks_per_sm = 0;  // persistent near-field grid: blocks per SM (0: occupancy)
   int fft_tile = 0;            // y/x FFT pass tile width (0: default)
   struct ct2g_batch *self_batch = nullptr;  // graph of ct2g_kick_drift
+  struct ct2g_learn *learn = nullptr;       // learned near-field correction
 
   // independent periodic boxes sharing the mesh: box b holds particles
   // [box_off[b], box_off[b+1]); its cells are keys (b << 3*mbits) | morton
@@ -239,6 +304,12 @@ size_t ct2g_scan_scratch_words(size_t n);
 void ct2g_mark(ct2g_ctx *ctx, int k);
 int ct2g_bin_range(ct2g_ctx *ctx);
 int ct2g_check(ct2g_ctx *ctx);  // valid context; selects its device
+// learned correction (ct2g_learned.cu): applied after the plain forces
+int ct2g_learned_apply(ct2g_ctx *ctx, bool pot);
+int ct2g_learned_resize(ct2g_ctx *ctx);  // per-cell arrays follow the particle capacity
+void ct2g_learned_free(ct2g_ctx *ctx);
+// D^n phi_eps(-o h) for the offsets o (x,y,z triples) -> d_out[nshell][nc]
+int ct2g_shell_greens(ct2g_ctx *ctx, const std::vector<int> &offs3, float *d_out);
 // far field of the current range into the force buffers (P2M if needed, mesh
 // solve with the fused inverse z pass + L2P)
 int ct2g_far_field(ct2g_ctx *ctx, bool pot);

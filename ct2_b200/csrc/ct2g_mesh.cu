@@ -71,40 +71,6 @@ __global__ void __launch_bounds__(128) p2m_kernel(const uint32_t *__restrict__ x
 // MG2L: one thread per k-point, in place on the spectrum.
 // G_n is real for even |n| and i*g for odd |n| (parity of D^n phi).
 // ---------------------------------------------------------------------------
-// The (a, b) pairs with |a|+|b| <= P, grouped by a: since multi-indices are
-// ordered by degree, the b of one a are exactly the first ncomp(P-|a|).
-template <int P>
-struct Mg2lPairs {
-  static constexpr int NC = ct2g_ncomp(P);
-  static constexpr int count() {
-    int n = 0;
-    for (int d = 0; d <= P; d++) n += (ct2g_ncomp(d) - (d ? ct2g_ncomp(d - 1) : 0)) * ct2g_ncomp(P - d);
-    return n;
-  }
-  static constexpr int NP = count();
-  int a[NP], b[NP], ab[NP], odd[NP], first[NP], last[NP];
-  constexpr Mg2lPairs() : a(), b(), ab(), odd(), first(), last() {
-    MiTable<P> T{};
-    int i = 0;
-    for (int ia = 0; ia < NC; ia++) {
-      const int nb = ct2g_ncomp(P - T.deg[ia]);
-      for (int ib = 0; ib < nb; ib++) {
-        a[i] = ia;
-        b[i] = ib;
-        ab[i] = ct2g_mi_index(T.nx[ia] + T.nx[ib], T.ny[ia] + T.ny[ib], T.nz[ia] + T.nz[ib]);
-        odd[i] = (T.deg[ia] + T.deg[ib]) & 1;
-        first[i] = ib == 0;
-        last[i] = ib == nb - 1;
-        i++;
-      }
-    }
-  }
-};
-template <int P>
-struct Mg2lTab {
-  static constexpr Mg2lPairs<P> t{};
-};
-
 // one (a, b) term; every index is a compile-time constant, so m[] and acc
 // stay in registers
 template <int P, int I>
@@ -267,6 +233,33 @@ __global__ void greens_real_kernel(int mbits, int p, int kernel, double soft, do
   }
 }
 
+// D^n phi_eps(R) of the softened kernel alone (no near-zone exclusion, no
+// Ewald split) at R = -o h for a list of lattice offsets o: the primary-image
+// term the mesh holds for a source cell at offset o from the sink cell
+__global__ void shell_greens_kernel(int nshell, const int *__restrict__ offs, int mbits, int p,
+                                    int nc, int kernel, double soft,
+                                    const DTerm *__restrict__ terms,
+                                    const int *__restrict__ nterms, float *__restrict__ out) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nshell) return;
+  const double h = 1.0 / (double)(1 << mbits);
+  const double R[3] = {-offs[3 * s] * h, -offs[3 * s + 1] * h, -offs[3 * s + 2] * h};
+  const double r2 = R[0] * R[0] + R[1] * R[1] + R[2] * R[2];
+  double f[CT2G_MAX_ORDER + 1];
+  if (kernel == CT2G_SOFT_SPHERE)
+    radial_sphere(r2, soft, p, f);
+  else
+    radial_plummer(r2, soft, p, f);
+  for (int k = 0; k < nc; k++) {
+    double g = 0.0;
+    for (int t = 0; t < nterms[k]; t++) {
+      const DTerm d = terms[k * kMaxTerms + t];
+      g += d.coef * ipow(R[0], d.mx) * ipow(R[1], d.my) * ipow(R[2], d.mz) * f[d.j];
+    }
+    out[(size_t)s * nc + k] = (float)g;
+  }
+}
+
 // combine the FFT of the real-space part with the folded Ewald k-space sum
 // (spectrum rows hold ldk entries; those past M/2 are padding, set to zero)
 __global__ void greens_finish_kernel(int mbits, int p, double alpha, int kmax,
@@ -347,13 +340,14 @@ int launch_mg2l(ct2g_ctx *ctx) {
 static const double kGreensAlpha = 12.0;
 static const int kGreensKmax = 36;
 
-int ct2g_build_greens(ct2g_ctx *ctx) {
-  if (ctx->greens_valid) return CT2G_OK;
-  if (ctx->capturing) return ct2g_fail(ctx, CT2G_ESTATE, "Green's table not built before recording");
-  const int p = ctx->p, nc = ctx->nc, M = ctx->M;
-  // D^n term tables and multi-indices
-  std::vector<DTerm> terms((size_t)nc * kMaxTerms);
-  std::vector<int> nterms(nc), mi(3 * nc);
+// D^n f = sum_m n!/(m!(n-2m)! 2^|m|) R^(n-2m) f^[|n|-|m|]: one DTerm per m,
+// per multi-index of degree <= p; mi holds the multi-indices
+static void build_dterms(int p, std::vector<DTerm> &terms, std::vector<int> &nterms,
+                         std::vector<int> &mi) {
+  const int nc = ct2g_ncomp(p);
+  terms.assign((size_t)nc * kMaxTerms, DTerm{});
+  nterms.assign(nc, 0);
+  mi.assign(3 * nc, 0);
   {
     int k = 0;
     for (int d = 0; d <= p; d++)
@@ -384,6 +378,47 @@ int ct2g_build_greens(ct2g_ctx *ctx) {
           k++;
         }
   }
+}
+
+int ct2g_shell_greens(ct2g_ctx *ctx, const std::vector<int> &offs3, float *d_out) {
+  const int nshell = (int)(offs3.size() / 3);
+  if (nshell == 0) return CT2G_OK;
+  std::vector<DTerm> terms;
+  std::vector<int> nterms, mi;
+  build_dterms(ctx->p, terms, nterms, mi);
+  DTerm *d_terms = nullptr;
+  int *d_nterms = nullptr, *d_offs = nullptr;
+  cudaError_t e = cudaMalloc(&d_terms, sizeof(DTerm) * terms.size());
+  if (e == cudaSuccess) e = cudaMalloc(&d_nterms, sizeof(int) * nterms.size());
+  if (e == cudaSuccess) e = cudaMalloc(&d_offs, sizeof(int) * offs3.size());
+  if (e == cudaSuccess)
+    e = cudaMemcpy(d_terms, terms.data(), sizeof(DTerm) * terms.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(d_nterms, nterms.data(), sizeof(int) * nterms.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(d_offs, offs3.data(), sizeof(int) * offs3.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    shell_greens_kernel<<<ct2g_div_up(nshell, 64), 64, 0, ctx->stream>>>(
+        nshell, d_offs, ctx->mbits, ctx->p, ctx->nc, ctx->opt.kernel, ctx->opt.hsoft, d_terms,
+        d_nterms, d_out);
+    ctx->launches++;
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (d_terms) cudaFree(d_terms);
+  if (d_nterms) cudaFree(d_nterms);
+  if (d_offs) cudaFree(d_offs);
+  if (e != cudaSuccess) return ct2g_cuda_fail(ctx, e, "shell Green's table");
+  return CT2G_OK;
+}
+
+int ct2g_build_greens(ct2g_ctx *ctx) {
+  if (ctx->greens_valid) return CT2G_OK;
+  if (ctx->capturing) return ct2g_fail(ctx, CT2G_ESTATE, "Green's table not built before recording");
+  const int p = ctx->p, nc = ctx->nc, M = ctx->M;
+  std::vector<DTerm> terms;
+  std::vector<int> nterms, mi;
+  build_dterms(p, terms, nterms, mi);
   DTerm *d_terms = nullptr;
   int *d_nterms = nullptr, *d_mi = nullptr;
   double *rs = nullptr;

@@ -45,33 +45,6 @@ struct Walk {
 // minimum-image offset (in cells) from cell c to cell n along one axis
 __device__ __forceinline__ int wrap_off(int n, int c, int M) { return ((n - c + M / 2) & (M - 1)) - M / 2; }
 
-template <int KERNEL, bool POT>
-__device__ __forceinline__ void pair_term(float dx, float dy, float dz, float h2, float hinv,
-                                          float hinv3, float &ax, float &ay, float &az,
-                                          float &ap, bool on) {
-  const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-  float g, pp;
-  if (KERNEL == CT2G_SOFT_PLUMMER) {
-    const float ri = rsqrtf(r2 + h2);
-    g = ri * ri * ri;
-    pp = ri;
-  } else {
-    if (r2 < h2) {
-      g = hinv3;
-      pp = 1.5f * hinv - 0.5f * r2 * hinv3;
-    } else {
-      const float ri = rsqrtf(r2);
-      g = ri * ri * ri;
-      pp = ri;
-    }
-  }
-  if (!on) g = pp = 0.f;
-  ax = fmaf(-dx, g, ax);
-  ay = fmaf(-dy, g, ay);
-  az = fmaf(-dz, g, az);
-  if (POT) ap -= pp;
-}
-
 // Near field, one warp per chunk of <= 32 sinks; the grid is persistent and
 // warps take chunks from a device work counter until the device-held chunk
 // count is reached.  A dense chunk is sinks of
@@ -169,14 +142,14 @@ __device__ __forceinline__ void near_chunk(
 #pragma unroll 16
             for (int u = 0; u < 32; u++) {
               const float4 q = sb[u];
-              pair_term<KERNEL, POT>(xs - q.x, ys - q.y, zs - q.z, h2, hinv, hinv3, nx, ny, nz,
+              ct2g_pair_term<KERNEL, POT>(xs - q.x, ys - q.y, zs - q.z, h2, hinv, hinv3, nx, ny, nz,
                                      np, !SPARSE || in);
             }
           } else {
 #pragma unroll 4
             for (int u = 0; u < cnt; u++) {
               const float4 q = sb[u];
-              pair_term<KERNEL, POT>(xs - q.x, ys - q.y, zs - q.z, h2, hinv, hinv3, nx, ny, nz,
+              ct2g_pair_term<KERNEL, POT>(xs - q.x, ys - q.y, zs - q.z, h2, hinv, hinv3, nx, ny, nz,
                                      np, !SPARSE || in);
             }
           }
@@ -288,8 +261,12 @@ int ct2g_forces(ct2g_ctx *ctx, bool pot) {
   CT2G_CUDA(ctx, cudaMemsetAsync(ctx->d_inter, 0, sizeof(unsigned long long), ctx->stream));
   CT2G_CUDA(ctx, cudaMemsetAsync(ctx->d_counts + 3, 0, 2 * sizeof(uint32_t), ctx->stream));
   if (ctx->n == ctx->rung_begin) return CT2G_OK;
+  int rc;
   if (ctx->opt.kernel == CT2G_SOFT_SPHERE)
-    return pot ? launch_near<CT2G_SOFT_SPHERE, true>(ctx) : launch_near<CT2G_SOFT_SPHERE, false>(ctx);
-  return pot ? launch_near<CT2G_SOFT_PLUMMER, true>(ctx) : launch_near<CT2G_SOFT_PLUMMER, false>(ctx);
+    rc = pot ? launch_near<CT2G_SOFT_SPHERE, true>(ctx) : launch_near<CT2G_SOFT_SPHERE, false>(ctx);
+  else
+    rc = pot ? launch_near<CT2G_SOFT_PLUMMER, true>(ctx) : launch_near<CT2G_SOFT_PLUMMER, false>(ctx);
+  CT2G_TRY(rc);
+  return ct2g_learned_apply(ctx, pot);
 }
 

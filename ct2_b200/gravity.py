@@ -220,6 +220,77 @@ class Gravity:
                                           ctypes.byref(mr) if wait else None))
         return mr.value if wait else None
 
+    # -- learned near-field correction ---------------------------------------
+    def learned_enable(self, bwidth_ext):
+        self._chk(self._l.ct2g_learned_enable(self._h, float(bwidth_ext)))
+
+    def learned_select(self, mode, threshold=0.0):
+        """mode: 'none', 'fixed', 'mlp' or 'all' (or the CT2G_SELECT_* value)."""
+        m = {"none": 0, "fixed": 1, "mlp": 2, "all": 3}.get(mode, mode)
+        self._chk(self._l.ct2g_learned_select(self._h, int(m), float(threshold)))
+
+    def learned_collect(self):
+        n = ctypes.c_size_t(0)
+        self._chk(self._l.ct2g_learned_collect(self._h, ctypes.byref(n)))
+        return n.value
+
+    def learned_dataset(self):
+        n = ctypes.c_size_t(0)
+        self._chk(self._l.ct2g_learned_dataset(self._h, None, None, 0, ctypes.byref(n)))
+        X = np.empty((n.value, _lib.MLP_NIN), np.float32)
+        T = np.empty(n.value, np.float32)
+        self._chk(self._l.ct2g_learned_dataset(self._h, _ptr(X), _ptr(T), n.value, None))
+        return X, T
+
+    def learned_clear(self):
+        self._chk(self._l.ct2g_learned_clear(self._h))
+
+    def learned_cells(self):
+        """Cells of the last selection pass: dict of keys, X, score, pred, selected."""
+        n, s = ctypes.c_size_t(0), ctypes.c_size_t(0)
+        self._chk(self._l.ct2g_learned_cells(self._h, None, None, None, None, None, 0,
+                                             ctypes.byref(n), ctypes.byref(s)))
+        m = n.value
+        out = dict(keys=np.empty(m, np.uint32), X=np.empty((m, _lib.MLP_NIN), np.float32),
+                   score=np.empty(m, np.float32), pred=np.empty(m, np.float32),
+                   selected=np.empty(m, np.uint8))
+        self._chk(self._l.ct2g_learned_cells(self._h, _ptr(out["keys"]), _ptr(out["X"]),
+                                             _ptr(out["score"]), _ptr(out["pred"]),
+                                             _ptr(out["selected"]), m, None, None))
+        out["nselected"] = s.value
+        return out
+
+    def mlp_init(self, seed=0):
+        self._chk(self._l.ct2g_mlp_init(self._h, int(seed)))
+
+    def mlp_set(self, params, fmean, fstd):
+        p = np.ascontiguousarray(params, np.float32)
+        m = np.ascontiguousarray(fmean, np.float32)
+        sd = np.ascontiguousarray(fstd, np.float32)
+        self._chk(self._l.ct2g_mlp_set(self._h, _ptr(p), _ptr(m), _ptr(sd)))
+
+    def mlp_get(self):
+        p = np.empty(_lib.MLP_NPARAM, np.float32)
+        m = np.empty(_lib.MLP_NIN, np.float32)
+        sd = np.empty(_lib.MLP_NIN, np.float32)
+        self._chk(self._l.ct2g_mlp_get(self._h, _ptr(p), _ptr(m), _ptr(sd)))
+        return p, m, sd
+
+    def mlp_train(self, epochs=20, batch=4096, lr=1e-3, seed=0, normalize=True):
+        loss = ctypes.c_float(0)
+        self._chk(self._l.ct2g_mlp_train(self._h, int(epochs), int(batch), float(lr), int(seed),
+                                         int(bool(normalize)), ctypes.byref(loss)))
+        return loss.value
+
+    def mlp_gradients(self, X, T):
+        X = np.ascontiguousarray(X, np.float32)
+        T = np.ascontiguousarray(T, np.float32)
+        g = np.empty(_lib.MLP_NPARAM, np.float32)
+        loss = ctypes.c_float(0)
+        self._chk(self._l.ct2g_mlp_gradients(self._h, _ptr(X), _ptr(T), len(T), _ptr(g),
+                                             ctypes.byref(loss)))
+        return g, loss.value
+
     # -- launch shapes ------------------------------------------------------
     def tuning(self):
         t = Tuning()

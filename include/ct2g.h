@@ -225,6 +225,57 @@ int ct2g_set_tuning(ct2g_ctx *ctx, const ct2g_tuning *t);
 int ct2g_autotune(ct2g_ctx *ctx, const ct2g_kick_params *p, float dt, float scale,
                   const char *cache_path, ct2g_tuning *out);
 
+/* Learned near-field correction.  No counterpart in the reference.
+ *
+ * For selected sink cells the direct sum is widened from the stencil
+ * |o|^2 <= bwidth^2 to |o|^2 <= bwidth_ext^2: the shell's particles are summed
+ * exactly and the mesh's Taylor term for those cells is subtracted, so a
+ * selected cell gets the forces of the method run with bwidth_ext.  Cells are
+ * selected by CT2G_SELECT_FIXED (score = the shell's monopole pull relative to
+ * the sink's force, above `threshold`), CT2G_SELECT_MLP (an MLP of 24 per-cell
+ * moment and density features -> 64 -> 64 -> 1, BF16 weights, FP32
+ * accumulation, predicts log10 of the cell's rms relative force residual;
+ * selected above `threshold`) or CT2G_SELECT_ALL.  Once a mode is set, every
+ * force computation (ct2g_compute_forces, ct2g_kick, ct2g_kick_drift) applies
+ * it.  Training: ct2g_learned_collect computes, for the current state, the
+ * plain forces, the widened forces with every cell corrected, and appends
+ * one (features, log10 residual) sample per occupied cell to the device
+ * training set; ct2g_mlp_train runs Adam on it with the library's own
+ * forward and backward kernels.  Parameters: W1[64][24], b1[64], W2[64][64],
+ * b2[64], W3[64], b3 (CT2G_MLP_NPARAM floats); features are normalised by
+ * (x - fmean) / fstd. */
+#define CT2G_SELECT_NONE 0
+#define CT2G_SELECT_FIXED 1
+#define CT2G_SELECT_MLP 2
+#define CT2G_SELECT_ALL 3
+#define CT2G_MLP_NIN 24
+#define CT2G_MLP_NHID 64
+#define CT2G_MLP_NPARAM 5825
+/* shell tables for bwidth < bwidth_ext <= 8 (2*bwidth_ext+1 <= mesh); order >= 2 */
+int ct2g_learned_enable(ct2g_ctx *ctx, float bwidth_ext);
+int ct2g_learned_select(ct2g_ctx *ctx, int mode, float threshold);
+/* after particle_to_grid; *ncells = samples added */
+int ct2g_learned_collect(ct2g_ctx *ctx, size_t *ncells);
+/* training set: *n samples; copies min(cap, n) rows of X [n][24] and T [n] */
+int ct2g_learned_dataset(ct2g_ctx *ctx, float *X, float *T, size_t cap, size_t *n);
+int ct2g_learned_clear(ct2g_ctx *ctx);
+/* cells of the last selection pass: keys, features, fixed-criterion scores,
+ * MLP predictions, selected flags (each may be NULL; min(cap, ncells) rows) */
+int ct2g_learned_cells(ct2g_ctx *ctx, uint32_t *keys, float *X, float *score, float *pred,
+                       uint8_t *selected, size_t cap, size_t *ncells, size_t *nselected);
+int ct2g_mlp_init(ct2g_ctx *ctx, uint64_t seed);
+int ct2g_mlp_set(ct2g_ctx *ctx, const float *params, const float *fmean, const float *fstd);
+int ct2g_mlp_get(ct2g_ctx *ctx, float *params, float *fmean, float *fstd);
+/* epochs of Adam over the training set in shuffled batches; normalize != 0
+ * first sets fmean/fstd from the set; *loss = final mean squared error */
+int ct2g_mlp_train(ct2g_ctx *ctx, int epochs, int batch, float lr, uint64_t seed, int normalize,
+                   float *loss);
+/* gradient of the mean squared error over n host samples (raw features X
+ * [n][24], targets T[n]) at the current weights, as the training step
+ * computes it: grad[CT2G_MLP_NPARAM], *loss */
+int ct2g_mlp_gradients(ct2g_ctx *ctx, const float *X, const float *T, size_t n, float *grad,
+                       float *loss);
+
 /* Rung bookkeeping (src/particle.cpp:31-57,320-347). */
 int ct2g_sort_by_rung(ct2g_ctx *ctx, int minrung);        /* particle_sort_by_rung   */
 int ct2g_push_rungs(ct2g_ctx *ctx);                       /* particle_push_rungs     */

@@ -1,0 +1,209 @@
+"""Learned near-field correction on the GPU against the CPU restatements.
+
+  * widening the direct sum of a cell reproduces the method run with the
+    wider stencil (oracle.method_forces at bwidth_ext), cell by cell;
+  * the 24 features and the fixed criterion's score match oracle.learned;
+  * the MLP gradients of the training kernels match the FP64 restatement;
+  * a network trained on the method's own residuals (one seed) selects cells
+    on another seed; judged by the FP64 Ewald sum, it cuts the plain error
+    and does at least as well as the fixed criterion at the same number of
+    corrected cells.
+"""
+import numpy as np
+import pytest
+
+from ct2_b200 import ics
+from ct2_b200.gravity import Gravity, kick_params
+from oracle import learned as OL
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(n=6000, mbits=5, p=3, bw=2.0, bwx=3.0, seed=3, nspheres=6):
+    P = ics.plummer_spheres(n, seed=seed, nspheres=nspheres, a=2.0 / (1 << mbits))
+    soft = 0.02 / (1 << mbits)
+    GM = 1.0 / n
+    g = Gravity(mesh=1 << mbits, order=p, bwidth=bw, hsoft=soft, GM=GM)
+    g.upload_dict(P)
+    g.learned_enable(bwx)
+    return P, g, soft, GM
+
+
+def _rel(f, fref):
+    return np.linalg.norm(f - fref, axis=1) / np.maximum(np.linalg.norm(fref, axis=1), 1e-30)
+
+
+def _cell_keys(d, mbits):
+    sh = 32 - mbits
+    return O.morton(d["x"] >> sh, d["y"] >> sh, d["z"] >> sh).astype(np.int64)
+
+
+def test_widened_cells_match_wider_method(gpu):
+    mbits, p, bw, bwx = 5, 3, 2.0, 3.0
+    P, g, soft, GM = _setup(mbits=mbits, p=p, bw=bw, bwx=bwx)
+    base = O.method_forces(P["x"], P["y"], P["z"], mbits, p, 0, soft, bw, GM)
+    wide = O.method_forces(P["x"], P["y"], P["z"], mbits, p, 0, soft, bwx, GM)
+    fb = base["ffar"] + base["fnear"]
+    fw = wide["ffar"] + wide["fnear"]
+    # every cell widened == the method with the wider stencil (same FP32
+    # tolerances as the plain force parity test)
+    g.learned_select("all")
+    g.particle_to_grid()
+    g.compute_forces()
+    f, pot = g.forces()
+    e = _rel(f, fw)
+    assert np.sqrt(np.mean(e ** 2)) < 1e-5 and e.max() < 1e-3
+    prel = np.abs(pot - wide["pot"]) / np.abs(wide["pot"])
+    assert np.sqrt(np.mean(prel ** 2)) < 1e-3
+    # no cell widened == the plain method
+    g.learned_select("none")
+    g.compute_forces()
+    f0, _ = g.forces()
+    e = _rel(f0, fb)
+    assert np.sqrt(np.mean(e ** 2)) < 1e-5 and e.max() < 1e-3
+    # fixed criterion: selected cells get the wide forces, the rest the plain
+    g.learned_select("fixed", 0.0)
+    g.compute_forces()
+    sc = g.learned_cells()["score"]
+    thr = float(np.median(sc))
+    g.learned_select("fixed", thr)
+    g.compute_forces()
+    f1, _ = g.forces()
+    c = g.learned_cells()
+    assert 0 < c["nselected"] < len(c["keys"])
+    assert c["nselected"] == int((c["score"] > thr).sum())
+    keys = _cell_keys(g.download(), mbits)
+    on = np.isin(keys, c["keys"][c["selected"] == 1])
+    assert on.any() and (~on).any()
+    e = np.where(on, _rel(f1, fw), _rel(f1, fb))
+    assert np.sqrt(np.mean(e ** 2)) < 1e-5 and e.max() < 1e-3
+
+
+def test_features_match_oracle(gpu):
+    mbits, p, bw, bwx = 5, 3, 2.0, 3.0
+    P, g, soft, GM = _setup(n=8000, mbits=mbits, p=p, bw=bw, bwx=bwx, seed=9)
+    g.particle_to_grid()
+    g.learned_select("none")
+    g.compute_forces()
+    f0, _ = g.forces()  # the plain forces the features are computed from
+    g.learned_select("fixed", 1e30)  # features and scores, nothing selected
+    g.compute_forces()
+    f1, _ = g.forces()
+    assert np.array_equal(f0, f1)
+    c = g.learned_cells()
+    assert c["nselected"] == 0
+    M = 1 << mbits
+    b, e = g.cells()
+    cs = np.zeros(M ** 3 + 1, np.int64)
+    ii, jj, kk = np.meshgrid(np.arange(M), np.arange(M), np.arange(M), indexing="ij")
+    cs[O.morton(ii.ravel(), jj.ravel(), kk.ravel()).astype(np.int64)] = b
+    cs[M ** 3] = len(f0)
+    mom = g.multipoles().reshape(g.nc, -1)
+    X, score = OL.features(c["keys"], cs, mom, f0, [0, len(f0)], [GM], mbits, p, bw, bwx)
+    # the cell list is every occupied cell, in key order
+    occ = np.nonzero(cs[1:] - cs[:-1])[0]
+    assert np.array_equal(np.sort(c["keys"].astype(np.int64)), occ)
+    # FP32 sums and logs against FP64
+    np.testing.assert_allclose(c["X"], X, rtol=1e-3, atol=2e-3)
+    np.testing.assert_allclose(c["score"], score, rtol=1e-3, atol=1e-9)
+
+
+def test_mlp_gradients_match_oracle(gpu):
+    _, g, _, _ = _setup(n=2000)
+    g.mlp_init(seed=7)
+    params, _, _ = g.mlp_get()
+    rng = np.random.Generator(np.random.PCG64(11))
+    fmean = rng.normal(0, 1, 24).astype(np.float32)
+    fstd = rng.uniform(0.5, 2.0, 24).astype(np.float32)
+    g.mlp_set(params, fmean, fstd)
+    X = (fmean + fstd * rng.normal(0, 1, (512, 24))).astype(np.float32)
+    T = rng.normal(-5, 1, 512).astype(np.float32)
+    grad, loss = g.mlp_gradients(X, T)
+    loss_ref, grad_ref = OL.mlp_loss_grad(params, fmean, fstd, X, T)
+    assert abs(loss - loss_ref) <= 1e-5 * loss_ref
+    # FP32 accumulation against FP64; a ReLU sign flip at |z| ~ 1e-7 would
+    # move one sample's share, far below this bound
+    assert np.abs(grad - grad_ref).max() <= 1e-3 * np.abs(grad_ref).max()
+    for lo, hi in ((OL.OW1, OL.OB1), (OL.OW2, OL.OB2), (OL.OW3, OL.OB3)):
+        gr = grad_ref[lo:hi]
+        assert np.abs(grad[lo:hi] - gr).max() <= 2e-3 * np.abs(gr).max()
+    # the parameters round trip and the forward matches too
+    p2, m2, s2 = g.mlp_get()
+    assert np.array_equal(p2, params) and np.array_equal(m2, fmean) and np.array_equal(s2, fstd)
+
+
+def _errors(g, P, truth, sel):
+    g.compute_forces()
+    f, _ = g.forces()
+    d = g.download()
+    inv = np.empty_like(d["id"])
+    inv[d["id"]] = np.arange(len(inv), dtype=inv.dtype)
+    e = _rel(f[inv[sel]], truth)
+    return float(np.sqrt(np.mean(e ** 2))), g.learned_cells()["nselected"]
+
+
+def test_trained_selection_beats_plain_and_fixed(gpu):
+    mbits, p, bw, bwx = 6, 4, 3.0, 4.0
+    n = 32 ** 3
+    # training state: seed 1; evaluation state: seed 2
+    Ptr, g, soft, GM = _setup(n=n, mbits=mbits, p=p, bw=bw, bwx=bwx, seed=1, nspheres=8)
+    g.particle_to_grid()
+    ncell = g.learned_collect()
+    X, T = g.learned_dataset()
+    assert len(T) == ncell > 0 and np.isfinite(X).all() and np.isfinite(T).all()
+    g.mlp_init(seed=3)
+    loss0 = float(np.var(T))
+    loss = g.mlp_train(epochs=60, batch=1024, lr=2e-3, seed=5)
+    print("targets var %.3f -> training mse %.3f over %d cells" % (loss0, loss, ncell))
+    assert loss < 0.5 * loss0
+    params, fm, fs = g.mlp_get()
+    pred = OL.mlp_forward(params, fm, fs, X)
+    assert np.sqrt(np.mean((pred - T) ** 2)) < 1.2 * np.sqrt(loss) + 1e-3
+
+    Pev = ics.plummer_spheres(n, seed=2, nspheres=8, a=2.0 / (1 << mbits))
+    h = Gravity(mesh=1 << mbits, order=p, bwidth=bw, hsoft=soft, GM=GM)
+    h.upload_dict(Pev)
+    h.learned_enable(bwx)
+    h.mlp_set(params, fm, fs)
+    rng = np.random.Generator(np.random.PCG64(4))
+    sel = np.sort(rng.choice(n, 4096, replace=False))
+    truth = h.ewald_direct(Pev["x"][sel], Pev["y"][sel], Pev["z"][sel])
+    h.particle_to_grid()
+    h.learned_select("none")
+    e_plain, _ = _errors(h, Pev, truth, sel)
+    h.learned_select("all")
+    e_all, n_all = _errors(h, Pev, truth, sel)
+    # MLP: cells predicted above 10^-3.9; the fixed criterion at the same count
+    h.learned_select("mlp", -3.9)
+    e_mlp, k = _errors(h, Pev, truth, sel)
+    sc = np.sort(h.learned_cells()["score"])[::-1]
+    h.learned_select("fixed", float(sc[k]) if k < len(sc) else -1.0)
+    e_fix, kf = _errors(h, Pev, truth, sel)
+    print("rms rel err: plain %.3e  all (%d cells) %.3e  mlp (%d) %.3e  fixed (%d) %.3e"
+          % (e_plain, n_all, e_all, k, e_mlp, kf, e_fix))
+    assert 0 < k < n_all and abs(kf - k) <= max(2, k // 100)
+    assert e_all < e_plain
+    assert e_mlp < 0.8 * e_plain
+    assert e_mlp <= 1.05 * e_fix
+
+
+def test_learned_step_records_into_graph(gpu):
+    mbits, p, bw, bwx = 5, 3, 2.0, 3.0
+    P, a, soft, GM = _setup(n=6000, mbits=mbits, p=p, bw=bw, bwx=bwx)
+    b = Gravity(mesh=1 << mbits, order=p, bwidth=bw, hsoft=soft, GM=GM)
+    b.upload_dict(P)
+    b.learned_enable(bwx)
+    a.mlp_init(seed=2)
+    b.mlp_set(*a.mlp_get())
+    for g in (a, b):
+        g.learned_select("mlp", -6.0)
+    kp = kick_params(t0=1e-3)
+    for _ in range(2):
+        ra = a.kick_drift(kp, 1e-3, graph=False)
+        rb = b.kick_drift(kp, 1e-3, graph=True)
+        assert ra == rb
+    da, db = a.download(), b.download()
+    for k in ("x", "y", "z", "vx", "vy", "vz", "rung", "id"):
+        assert np.array_equal(da[k], db[k]), k
+    assert a.learned_cells()["nselected"] == b.learned_cells()["nselected"]
