@@ -181,6 +181,54 @@ def _config(args, world):
             "l2": "inputs larger than L2 (particle store + mesh grids >> 126 MB)"}
 
 
+def learned_form(args, P, n, soft, local, kp, accuracy):
+    """Learned form: the plain stencil narrowed to --learned-base, and the
+    cells an MLP selects widened back to --bwidth.  The MLP is trained first
+    on a state of the same generator with another seed (time reported, not
+    part of the step); the step is then timed as graph replays."""
+    import torch
+
+    from ct2_b200 import ics, replicas
+    from ct2_b200.gravity import Gravity
+    gl = Gravity(mesh=args.mesh, order=args.order, bwidth=args.learned_base, hsoft=soft,
+                 GM=1.0 / n, device=local, max_particles=n)
+    gl.learned_enable(args.bwidth)
+    Pt = ics.plummer_spheres(n, seed=args.seed + 100, nspheres=args.nspheres, a=args.a)
+    t = time.perf_counter()
+    gl.upload_dict(Pt)
+    gl.particle_to_grid()
+    ncell = gl.learned_collect()
+    gl.mlp_init(seed=1)
+    loss = gl.mlp_train(epochs=args.learned_epochs, batch=4096, lr=2e-3, seed=2)
+    gl.synchronize()
+    train_s = time.perf_counter() - t
+    gl.upload_dict(P)
+    gl.learned_select("mlp", args.learned_threshold)
+    acc = accuracy(gl)
+    nsel = gl.learned_cells()["nselected"]
+    tune = gl.autotune(kp, args.dt, 1.0, cache_path=args.tune_cache)
+    gl.upload_dict(P)
+    stream = torch.cuda.ExternalStream(gl.stream(), device=local)
+    for _ in range(args.warmup):
+        gl.kick_drift(kp, args.dt, 1.0, graph=True, wait=False)
+    gl.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        gl.kick_drift(kp, args.dt, 1.0, graph=True, wait=False)
+    e1.record(stream)
+    e1.synchronize()
+    value, ms = replicas.job_throughput(n, e0.elapsed_time(e1) / args.steps, device="cuda")
+    out = {"value": value, "ms_per_step": ms, "accuracy": acc, "tuning": tune,
+           "base_bwidth": args.learned_base, "widened_to": args.bwidth,
+           "threshold_log10": args.learned_threshold, "cells_selected": int(nsel),
+           "training": {"cells": int(ncell), "epochs": args.learned_epochs, "mse": loss,
+                        "seconds": train_s, "state": "same generator, seed + 100"}}
+    gl.close()
+    return out
+
+
 BOX_METRIC = ("particles/s per kick+drift over 96 independent periodic boxes "
               "(16^3..128^3 particles, meshes 32^3..256^3)")
 
@@ -352,6 +400,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", default="plummer128", choices=["plummer128", "boxes96"])
+    ap.add_argument("--learned-base", type=float, default=3.0,
+                    help="learned form: plain stencil of the base step (0: skip the form)")
+    ap.add_argument("--learned-threshold", type=float, default=-4.0,
+                    help="learned form: widen cells whose predicted log10 residual exceeds this")
+    ap.add_argument("--learned-epochs", type=int, default=30)
     ap.add_argument("--tune-cache", default=None,
                     help="autotuner cache file (default: tune on every run)")
     args = ap.parse_args()
@@ -400,20 +453,27 @@ def main():
         g.kick(kp)
         g.drift(args.dt, 1.0)
 
-    # accuracy on the initial state: forces vs the FP64 Ewald direct sum
-    g.particle_to_grid()
-    g.compute_forces()
-    f, _ = g.forces()
-    d = g.download()
+    # accuracy on the initial state: forces vs the FP64 Ewald direct sum at
+    # a seeded sample of particles (by upload index)
     rng = np.random.Generator(np.random.PCG64(123))
     sel = np.sort(rng.choice(n, size=min(args.accuracy_sinks, n), replace=False))
-    truth = g.ewald_direct(d["x"][sel], d["y"][sel], d["z"][sel])
-    diff = np.linalg.norm(f[sel] - truth, axis=1)
-    tn = np.linalg.norm(truth, axis=1)
-    acc = {"rms_rel": float(np.sqrt(np.mean((diff / tn) ** 2))),
-           "max_rel": float((diff / tn).max()),
-           "rms_norm": float(np.sqrt(np.mean(diff ** 2) / np.mean(tn ** 2))),
-           "sinks": int(len(sel))}
+    truth = g.ewald_direct(P["x"][sel], P["y"][sel], P["z"][sel])
+
+    def accuracy(ctx):
+        ctx.particle_to_grid()
+        ctx.compute_forces()
+        f, _ = ctx.forces()
+        ids = ctx.download()["id"]
+        inv = np.empty_like(ids)
+        inv[ids] = np.arange(len(ids), dtype=ids.dtype)
+        diff = np.linalg.norm(f[inv[sel]] - truth, axis=1)
+        tn = np.linalg.norm(truth, axis=1)
+        return {"rms_rel": float(np.sqrt(np.mean((diff / tn) ** 2))),
+                "max_rel": float((diff / tn).max()),
+                "rms_norm": float(np.sqrt(np.mean(diff ** 2) / np.mean(tn ** 2))),
+                "sinks": int(len(sel))}
+
+    acc = accuracy(g)
     g.upload_dict(P)
 
     # plain form: eager calls, per-stage events
@@ -459,8 +519,11 @@ def main():
     launches = g.launch_count() - l0
     ms_local = e0.elapsed_time(e1) / args.steps
     value, ms = replicas.job_throughput(n, ms_local, device="cuda")
-    forms = {"plain": {"value": plain_value, "ms_per_step": plain_ms},
-             "graph_autotuned": {"value": value, "ms_per_step": ms, "tuning": tune}}
+    forms = {"plain": {"value": plain_value, "ms_per_step": plain_ms, "accuracy": acc},
+             "graph_autotuned": {"value": value, "ms_per_step": ms, "tuning": tune,
+                                 "accuracy": acc}}
+    if args.learned_base > 0:
+        forms["learned"] = learned_form(args, P, n, soft, local, kp, accuracy)
     if dist:
         dist.barrier()
 
