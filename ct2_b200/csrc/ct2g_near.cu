@@ -56,6 +56,61 @@ __device__ __forceinline__ int wrap_off(int n, int c, int M) { return ((n - c + 
 // cell lies in its own stencil (always true in a dense chunk), so every sink
 // sees exactly its own near zone.
 
+// ---------------------------------------------------------------------------
+// Packed pairs: Blackwell's f32x2 add/mul/fma do two FP32 operations per
+// issued instruction.  For the Plummer kernel the warp's source batch is
+// staged as pair records -- (x0, x1, y0, y1) in one 16-byte slot and (z0, z1)
+// in an 8-byte slot -- so one broadcast load of each feeds two interactions.
+// ---------------------------------------------------------------------------
+typedef unsigned long long f32x2;
+__device__ __forceinline__ f32x2 f2_pack(float a, float b) {
+  f32x2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ void f2_unpack(f32x2 v, float &a, float &b) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+}
+__device__ __forceinline__ f32x2 f2_sub(f32x2 a, f32x2 b) {
+  f32x2 r;
+  asm("sub.rn.ftz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f32x2 f2_mul(f32x2 a, f32x2 b) {
+  f32x2 r;
+  asm("mul.rn.ftz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f32x2 f2_fma(f32x2 a, f32x2 b, f32x2 c) {
+  f32x2 r;
+  asm("fma.rn.ftz.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+
+// two Plummer interactions of a sink at (X, Y, Z) (both halves equal) with
+// the sources of pair record pr; accumulates +d g (the caller negates) and
+// the potential +1/r; MASK (sparse chunks) is 1 or 0 per lane
+template <bool POT, bool MASKED>
+__device__ __forceinline__ void plummer_pair(const float *sbf, int pr, f32x2 X, f32x2 Y, f32x2 Z,
+                                             f32x2 H2, f32x2 MASK, f32x2 &ax, f32x2 &ay,
+                                             f32x2 &az, f32x2 &ap) {
+  const float4 a = reinterpret_cast<const float4 *>(sbf)[pr];       // x0 x1 y0 y1
+  const float2 b = reinterpret_cast<const float2 *>(sbf + 64)[pr];  // z0 z1
+  const f32x2 dx = f2_sub(X, f2_pack(a.x, a.y));
+  const f32x2 dy = f2_sub(Y, f2_pack(a.z, a.w));
+  const f32x2 dz = f2_sub(Z, f2_pack(b.x, b.y));
+  const f32x2 r2 = f2_fma(dz, dz, f2_fma(dy, dy, f2_fma(dx, dx, H2)));
+  float r0, r1;
+  f2_unpack(r2, r0, r1);
+  f32x2 ri = f2_pack(rsqrtf(r0), rsqrtf(r1));
+  if (MASKED) ri = f2_mul(ri, MASK);
+  const f32x2 g = f2_mul(f2_mul(ri, ri), ri);
+  ax = f2_fma(dx, g, ax);
+  ay = f2_fma(dy, g, ay);
+  az = f2_fma(dz, g, az);
+  if (POT) ap = f2_sub(ap, ri);
+}
+
 __device__ __forceinline__ void inblock(int b, int &x, int &y, int &z) {
   x = ((b >> 2) & 1) | ((b >> 4) & 2);
   y = ((b >> 1) & 1) | ((b >> 3) & 2);
@@ -102,6 +157,9 @@ __device__ __forceinline__ void near_chunk(
   const float hc = 1.0f / (float)M;
   const float h2 = soft * soft, hinv = 1.f / soft, hinv3 = hinv * hinv * hinv;
   float nx = 0.f, ny = 0.f, nz = 0.f, np = 0.f;
+  // packed accumulators of the Plummer path (+d g and +1/r per pair half)
+  f32x2 pax = 0ull, pay = 0ull, paz = 0ull, pap = 0ull;
+  const f32x2 H2 = f2_pack(h2, h2);
   uint32_t nsrc = 0;
   for (int o = 0; o < 27; o++) {
     const unsigned long long bits = __shfl_sync(0xffffffffu, word, o);
@@ -132,6 +190,38 @@ __device__ __forceinline__ void near_chunk(
         // sink position relative to the neighbour cell's centre
         const float xs = si.x - (float)ox * hc, ys = si.y - (float)oy * hc, zs = si.z - (float)oz * hc;
         float4 nxt = __ldg(src + min(j0 + lane, j1 - 1));
+        if constexpr (KERNEL == CT2G_SOFT_PLUMMER) {
+          const f32x2 X = f2_pack(xs, xs), Y = f2_pack(ys, ys), Z = f2_pack(zs, zs);
+          const float mk = (!SPARSE || in) ? 1.f : 0.f;
+          const f32x2 MASK = f2_pack(mk, mk);
+          float *sbf = reinterpret_cast<float *>(sb);
+          const int rec = 4 * (lane >> 1) + (lane & 1);
+          for (uint32_t jj = j0; jj < j1; jj += 32) {
+            const int cnt = (int)min(32u, j1 - jj);
+            __syncwarp();
+            sbf[rec] = nxt.x;
+            sbf[rec + 2] = nxt.y;
+            sbf[64 + 2 * (lane >> 1) + (lane & 1)] = nxt.z;
+            __syncwarp();
+            if (jj + 32 < j1) nxt = __ldg(src + min(jj + 32 + lane, j1 - 1));
+            if (cnt == 32) {
+#pragma unroll 8
+              for (int pr = 0; pr < 16; pr++)
+                plummer_pair<POT, SPARSE>(sbf, pr, X, Y, Z, H2, MASK, pax, pay, paz, pap);
+            } else {
+#pragma unroll 2
+              for (int pr = 0; pr < (cnt >> 1); pr++)
+                plummer_pair<POT, SPARSE>(sbf, pr, X, Y, Z, H2, MASK, pax, pay, paz, pap);
+              if (cnt & 1) {  // the odd last source
+                const int pr = cnt >> 1;
+                const float qx = sbf[4 * pr], qy = sbf[4 * pr + 2], qz = sbf[64 + 2 * pr];
+                ct2g_pair_term<KERNEL, POT>(xs - qx, ys - qy, zs - qz, h2, hinv, hinv3, nx, ny,
+                                            nz, np, !SPARSE || in);
+              }
+            }
+          }
+          continue;
+        }
         for (uint32_t jj = j0; jj < j1; jj += 32) {
           const int cnt = (int)min(32u, j1 - jj);
           __syncwarp();
@@ -157,6 +247,19 @@ __device__ __forceinline__ void near_chunk(
       }
     }
   }
+  if constexpr (KERNEL == CT2G_SOFT_PLUMMER) {
+    float a0, a1;
+    f2_unpack(pax, a0, a1);
+    nx -= a0 + a1;
+    f2_unpack(pay, a0, a1);
+    ny -= a0 + a1;
+    f2_unpack(paz, a0, a1);
+    nz -= a0 + a1;
+    if (POT) {
+      f2_unpack(pap, a0, a1);
+      np += a0 + a1;
+    }
+  }
   // the far field (L2P, with GM) is already in the force buffers
   if (act) {
     ofx[i] += GM * nx;
@@ -173,7 +276,7 @@ __device__ __forceinline__ void near_chunk(
 // counts[0] dense chunks, counts[2] sparse chunks (stored after the dense
 // ones), counts[3] / counts[4] the work counters (zero at launch)
 template <int KERNEL, bool POT, bool SPARSE>
-__global__ void __launch_bounds__(256) near_kernel(
+__global__ void __launch_bounds__(256, 4) near_kernel(
     const uint2 *__restrict__ chunks, uint32_t *__restrict__ counts,
     const uint32_t *__restrict__ sparse_list, const uint32_t *__restrict__ cs,
     const unsigned long long *__restrict__ occ, const unsigned long long *__restrict__ stmask,
