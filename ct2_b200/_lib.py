@@ -105,6 +105,7 @@ SYMBOLS = [
     ("ct2g_ewald_direct", _I, [_P, _P, _P, _P, _SZ, _D, _D, _I, _P, _P]),
     ("ct2g_ewald_direct_noalloc", _I, [_I, _P, _P, _P, _SZ, _P, _P, _P, _SZ, _I, _D, _D, _D, _D,
                                        _I, _P, _P, _P]),
+    ("ct2g_tc_selftest", _I, [_I, _P, _P, _I, _I, _P]),
     ("ct2g_stream", _P, [_P]),
     ("ct2g_synchronize", _I, [_P]),
     ("ct2g_stage_times", _I, [_P, _P, _I]),

@@ -326,6 +326,14 @@ int ct2g_ewald_direct_noalloc(int device, const uint32_t *qx, const uint32_t *qy
                               double soft, double GM, double alpha, double rcut, int kmax,
                               double *f, double *pot, void *stream);
 
+/* Self-test of the tcgen05 building blocks (tensor memory, UMMA descriptors,
+ * MMA completion) the tensor-core passes use.  No counterpart in the
+ * reference.  One CTA computes D[128][N] = A[128][K] * B[N][K]^T with the
+ * operands rounded to BF16 and FP32 accumulation; host arrays, row-major;
+ * N in {32, 64}, K in {16, 32, 64, 96}.  CT2G_ETIMEOUT if the MMA did not
+ * complete within the kernel's bounded wait. */
+int ct2g_tc_selftest(int device, const float *A, const float *B, int N, int K, float *D);
+
 /* Stream and timing helpers. */
 void *ct2g_stream(ct2g_ctx *ctx);   /* the context's cudaStream_t */
 int ct2g_synchronize(ct2g_ctx *ctx);
