@@ -30,6 +30,7 @@ class Tuning(ctypes.Structure):
 
 
 STEP_GRAPH = 1
+FFT_FP32, FFT_TC_BF16X3 = 0, 1
 SELECT_NONE, SELECT_FIXED, SELECT_MLP, SELECT_ALL = 0, 1, 2, 3
 MLP_NIN, MLP_NHID, MLP_NPARAM = 24, 64, 5825
 
@@ -106,6 +107,7 @@ SYMBOLS = [
     ("ct2g_ewald_direct_noalloc", _I, [_I, _P, _P, _P, _SZ, _P, _P, _P, _SZ, _I, _D, _D, _D, _D,
                                        _I, _P, _P, _P]),
     ("ct2g_tc_selftest", _I, [_I, _P, _P, _I, _I, _P]),
+    ("ct2g_set_fft_mode", _I, [_P, _I]),
     ("ct2g_stream", _P, [_P]),
     ("ct2g_synchronize", _I, [_P]),
     ("ct2g_stage_times", _I, [_P, _P, _I]),

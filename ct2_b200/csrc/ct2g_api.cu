@@ -116,6 +116,17 @@ void ct2g_mark(ct2g_ctx *ctx, int k) {
 
 int ct2g_check(ct2g_ctx *ctx) { return check(ctx); }
 
+int ct2g_device_error(ct2g_ctx *ctx) {
+  uint32_t e = 0;
+  CT2G_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  CT2G_CUDA(ctx, cudaMemcpy(&e, ctx->d_counts + 6, sizeof(e), cudaMemcpyDeviceToHost));
+  if (e) {
+    cudaMemset(ctx->d_counts + 6, 0, sizeof(uint32_t));
+    return ct2g_fail(ctx, (int)e, "a device-side wait gave up (tensor-core pass)");
+  }
+  return CT2G_OK;
+}
+
 // far field of the current range into the force buffers: moments (if the
 // grid does not hold them), then the mesh solve whose inverse z pass
 // evaluates L2P for every particle (the moments stay in the grid)
@@ -204,6 +215,7 @@ int ct2g_alloc_mesh(ct2g_ctx *ctx) {
   CT2G_CUDA(ctx, cudaMalloc(&ctx->grid, sizeof(float) * ctx->nc * nb * ctx->C));
   CT2G_CUDA(ctx, cudaMalloc(&ctx->spec, sizeof(float2) * ctx->nc * nb * ctx->CK));
   CT2G_CUDA(ctx, cudaMalloc(&ctx->d_counts, sizeof(uint32_t) * 8));
+  CT2G_CUDA(ctx, cudaMemset(ctx->d_counts, 0, sizeof(uint32_t) * 8));
   CT2G_CUDA(ctx, cudaMalloc(&ctx->box_off, sizeof(uint32_t) * (nb + 1)));
   CT2G_CUDA(ctx, cudaMalloc(&ctx->box_gm, sizeof(float) * nb));
   CT2G_CUDA(ctx, cudaMalloc(&ctx->greens, sizeof(float) * ctx->nc * ctx->CK));
@@ -354,7 +366,7 @@ int ct2g_destroy(ct2g_ctx *ctx) {
   if (ctx->self_batch) ct2g_batch_destroy(ctx->self_batch);
   ct2g_learned_free(ctx);
   void *ptrs[] = {ctx->cell_start, ctx->occ, ctx->stmask, ctx->grid, ctx->spec, ctx->greens,
-                  ctx->tw32, ctx->tw64, ctx->d_counts, ctx->box_off, ctx->box_gm,
+                  ctx->tw32, ctx->tw64, ctx->d_counts, ctx->box_off, ctx->box_gm, ctx->tc_tables,
                   ctx->d_maxrung, ctx->d_inter, ctx->scan_tmp};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -870,7 +882,22 @@ void *ct2g_stream(ct2g_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
 
 int ct2g_synchronize(ct2g_ctx *ctx) {
   CT2G_TRY(check(ctx));
-  CT2G_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return ct2g_device_error(ctx);
+}
+
+int ct2g_set_fft_mode(ct2g_ctx *ctx, int mode) {
+  CT2G_TRY(check(ctx));
+  if (mode == CT2G_FFT_FP32) {
+    ctx->fft_tc = false;
+  } else if (mode == CT2G_FFT_TC_BF16X3) {
+    if (!ct2g_fft_tc_supported(ctx->M)) return ct2g_fail(ctx, CT2G_EINVAL, "the tensor-core FFT supports meshes 256 and 512");
+    CT2G_TRY(ct2g_fft_tc_prepare(ctx));
+    ctx->fft_tc = true;
+  } else {
+    return ct2g_fail(ctx, CT2G_EINVAL, "unknown FFT mode");
+  }
+  ctx->epoch++;
+  ctx->expansions_valid = ctx->forces_valid = false;
   return CT2G_OK;
 }
 

@@ -416,7 +416,7 @@ int ct2g_bin_range(ct2g_ctx *ctx) {
   const unsigned T = 256;
   if (!ctx->boxes_set) return ct2g_fail(ctx, CT2G_ESTATE, "box sizes not set since the upload");
   uint32_t *counts = ctx->d_counts;
-  CT2G_CUDA(ctx, cudaMemsetAsync(counts, 0, sizeof(uint32_t) * 8, st));
+  CT2G_CUDA(ctx, cudaMemsetAsync(counts, 0, sizeof(uint32_t) * 6, st));
   if (nr > 0) {
     keys_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(ctx->x, ctx->y, ctx->z, begin, nr, mbits,
                                                     ctx->box_off, ctx->nbox, ctx->keys, ctx->vals);

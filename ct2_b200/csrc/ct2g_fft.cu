@@ -469,6 +469,12 @@ int run_cols(ct2g_ctx *ctx, typename Cplx<T>::type *spec, int batch, bool inv, s
       rstride = (size_t)N * ld;
       ncols = (size_t)N * ld;
     }
+    if constexpr (sizeof(C2) == 8 && (N == 256 || N == 512)) {
+      if (ctx->fft_tc) {
+        CT2G_TRY(ct2g_fft_cols_tc(ctx, spec, N, nouter, ostride, rstride, ncols, inv));
+        continue;
+      }
+    }
     if (inv) {
       if (vec) CT2G_TRY((launch_cols<T, N, true, true>(ctx, spec, nouter, ostride, rstride, ncols)));
       else CT2G_TRY((launch_cols<T, N, true, false>(ctx, spec, nouter, ostride, rstride, ncols)));

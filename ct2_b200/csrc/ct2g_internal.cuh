@@ -216,13 +216,16 @@ struct ct2g_ctx {
   uint32_t *flags = nullptr;
   // work-list sizes stay on the device, so a step needs no host readback:
   // [0] dense chunks, [1] sparse sinks, [2] sparse chunks, [3] and [4] the
-  // dense and sparse near-field work counters
+  // dense and sparse near-field work counters, [5] scan total scratch,
+  // [6] sticky device error (a status code a kernel left)
   uint32_t *d_counts = nullptr;
   uint32_t dense_cell = 16;  // cells with at least this many particles get their own chunks
   int near_blocks_per_sm = 0;  // persistent near-field grid: blocks per SM (0: occupancy)
   int fft_tile = 0;            // y/x FFT pass tile width (0: default)
   struct ct2g_batch *self_batch = nullptr;  // graph of ct2g_kick_drift
   struct ct2g_learn *learn = nullptr;       // learned near-field correction
+  bool fft_tc = false;                      // y/x FFT passes on the tensor cores
+  unsigned char *tc_tables = nullptr;       // their DFT matrices and twiddles
 
   // independent periodic boxes sharing the mesh: box b holds particles
   // [box_off[b], box_off[b+1]); its cells are keys (b << 3*mbits) | morton
@@ -304,6 +307,13 @@ size_t ct2g_scan_scratch_words(size_t n);
 void ct2g_mark(ct2g_ctx *ctx, int k);
 int ct2g_bin_range(ct2g_ctx *ctx);
 int ct2g_check(ct2g_ctx *ctx);  // valid context; selects its device
+// waits for the stream, then reports a status a kernel left in d_counts[6]
+int ct2g_device_error(ct2g_ctx *ctx);
+// tensor-core FFT passes (ct2g_fft_tc.cu)
+bool ct2g_fft_tc_supported(int N);
+int ct2g_fft_tc_prepare(ct2g_ctx *ctx);
+int ct2g_fft_cols_tc(ct2g_ctx *ctx, float2 *spec, int N, size_t nouter, size_t ostride,
+                     size_t rstride, size_t ncols, bool inv);
 // learned correction (ct2g_learned.cu): applied after the plain forces
 int ct2g_learned_apply(ct2g_ctx *ctx, bool pot);
 int ct2g_learned_resize(ct2g_ctx *ctx);  // per-cell arrays follow the particle capacity

@@ -291,6 +291,11 @@ class Gravity:
                                              ctypes.byref(loss)))
         return g, loss.value
 
+    def set_fft_mode(self, mode):
+        """'fp32' (CUDA cores) or 'tc' (tensor-core DFT passes, BF16 hi+lo)."""
+        m = {"fp32": _lib.FFT_FP32, "tc": _lib.FFT_TC_BF16X3}.get(mode, mode)
+        self._chk(self._l.ct2g_set_fft_mode(self._h, int(m)))
+
     # -- launch shapes ------------------------------------------------------
     def tuning(self):
         t = Tuning()

@@ -334,7 +334,18 @@ int ct2g_ewald_direct_noalloc(int device, const uint32_t *qx, const uint32_t *qy
  * complete within the kernel's bounded wait. */
 int ct2g_tc_selftest(int device, const float *A, const float *B, int N, int K, float *D);
 
-/* Stream and timing helpers. */
+/* FFT arithmetic of the mesh solve (precision form).  No counterpart in the
+ * reference.  CT2G_FFT_FP32 (default): every pass on the CUDA cores in FP32.
+ * CT2G_FFT_TC_BF16X3: the y and x passes as radix-R2 x radix-16 DFT matrix
+ * products on the tensor cores (tcgen05), operands split into BF16 hi + lo
+ * parts (three products per term, FP32 accumulation); meshes 256 and 512.
+ * Applies to every later mesh solve of the context and to ct2g_fft3d_f32_dev. */
+#define CT2G_FFT_FP32 0
+#define CT2G_FFT_TC_BF16X3 1
+int ct2g_set_fft_mode(ct2g_ctx *ctx, int mode);
+
+/* Stream and timing helpers.  ct2g_synchronize also reports a status a
+ * kernel left behind (CT2G_ETIMEOUT: a bounded device-side wait gave up). */
 void *ct2g_stream(ct2g_ctx *ctx);   /* the context's cudaStream_t */
 int ct2g_synchronize(ct2g_ctx *ctx);
 /* Per-stage device times (ms) of the last ct2g_kick / ct2g_kick_step call:
