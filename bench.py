@@ -181,6 +181,41 @@ def _config(args, world):
             "l2": "inputs larger than L2 (particle store + mesh grids >> 126 MB)"}
 
 
+def precision_form(args, g, P, n, local, kp, accuracy, stream):
+    """Precision form: the same context with its y/x FFT passes on the tensor
+    cores (BF16 hi+lo DFT matrix products), graph replays, own accuracy; the
+    forward / inverse FFT stage times of both modes from one eager step."""
+    import torch
+
+    from ct2_b200 import replicas
+    stages = {}
+    for mode in ("fp32", "tc"):
+        g.set_fft_mode(mode)
+        g.upload_dict(P)
+        g.particle_to_grid()
+        g.kick(kp)
+        st = g.stage_times()
+        stages[mode] = {"fft_fwd_ms": float(st[2]), "mg2l_ms": float(st[3]),
+                        "fft_inv_l2p_ms": float(st[4])}
+    acc = accuracy(g)
+    g.upload_dict(P)
+    for _ in range(args.warmup):
+        g.kick_drift(kp, args.dt, 1.0, graph=True, wait=False)
+    g.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        g.kick_drift(kp, args.dt, 1.0, graph=True, wait=False)
+    e1.record(stream)
+    e1.synchronize()
+    g.synchronize()
+    value, ms = replicas.job_throughput(n, e0.elapsed_time(e1) / args.steps, device="cuda")
+    g.set_fft_mode("fp32")
+    return {"value": value, "ms_per_step": ms, "accuracy": acc, "stages": stages,
+            "fft": "y/x passes: tcgen05 DFT products, BF16 hi+lo operands, FP32 accumulation"}
+
+
 def learned_form(args, P, n, soft, local, kp, accuracy):
     """Learned form: the plain stencil narrowed to --learned-base, and the
     cells an MLP selects widened back to --bwidth.  The MLP is trained first
@@ -227,6 +262,77 @@ def learned_form(args, P, n, soft, local, kp, accuracy):
                         "seconds": train_s, "state": "same generator, seed + 100"}}
     gl.close()
     return out
+
+
+FFT_METRIC = "3D FFT of 4 x 512^3 moment grids (grid points/s, forward + inverse)"
+
+
+def run_fft512(args, rank, world, local):
+    """--workload fft512: the precision form's configuration.  The 128^3
+    Plummer particles deposited on a 512^3 mesh as their four order-1 moment
+    grids (monopole and dipole about the cell centres: the method's own
+    deposit); the mesh solve's forward r2c and inverse c2r 3D FFTs of the four
+    grids timed with CUDA events, FP32 CUDA-core passes against tensor-core
+    y/x passes (BF16 hi+lo); the spectrum of the monopole grid checked against
+    the FP64 transform in both modes."""
+    import ctypes
+
+    import torch
+
+    from ct2_b200 import _lib
+    from ct2_b200.gravity import Gravity
+    P, n = workload(args, rank)
+    M = 512
+    g = Gravity(mesh=M, order=1, bwidth=args.bwidth, hsoft=1.0 / (50 * args.ngrid),
+                GM=1.0 / n, device=local, max_particles=n)
+    g.upload_dict(P)
+    g.particle_to_grid()
+    res = {}
+    for mode in ("fp32", "tc"):
+        g.set_fft_mode(mode)
+        fw, iv = [], []
+        for it in range(args.warmup + args.steps):
+            g.compute_multipoles()
+            g.compute_expansions()  # r2c, MG2L, c2r of the 4 grids
+            st = g.stage_times()
+            if it >= args.warmup:
+                fw.append(float(st[2]))
+                iv.append(float(st[4]))
+        res[mode] = {"fft_fwd_ms": float(np.median(fw)), "fft_inv_ms": float(np.median(iv))}
+    # spectrum accuracy on the monopole grid against FP64
+    g.compute_multipoles()
+    m0 = np.ascontiguousarray(g.multipoles()[0])
+    ref = g.fft_r2c_3d(m0.astype(np.float64))  # FP64 on the GPU, split planes
+    dim = M * M * (M // 2 + 1)
+    ref = (ref[:dim] + 1j * ref[dim:]).reshape(M, M, M // 2 + 1)
+    scale = np.sqrt(np.mean(np.abs(ref) ** 2))
+    lib = _lib.load()
+    xin = torch.from_numpy(m0).cuda()
+    out = torch.empty((M, M, M // 2 + 1), dtype=torch.complex64, device="cuda")
+    for mode in ("fp32", "tc"):
+        g.set_fft_mode(mode)
+        torch.cuda.synchronize()
+        rc = lib.ct2g_fft3d_f32_dev(g.handle, 1, ctypes.c_void_p(xin.data_ptr()),
+                                    ctypes.c_void_p(out.data_ptr()), M, 1)
+        assert rc == 0
+        g.synchronize()
+        y = out.cpu().numpy()
+        res[mode]["spectrum_rms_rel_err"] = float(np.sqrt(np.mean(np.abs(y - ref) ** 2)) / scale)
+    points = 4.0 * M ** 3
+    best = res["tc"]
+    ms = best["fft_fwd_ms"] + best["fft_inv_ms"]
+    if rank == 0:
+        line = {"metric": FFT_METRIC, "value": points / (ms * 1e-3), "unit": "grid points/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "bf16x3 (tensor cores) / f32",
+                "data": "synthetic: moments of the seeded 128^3 Plummer workload",
+                "config": {"workload": "fft512x4", "mesh": M, "grids": 4,
+                           "particles": n, "l2": "inputs larger than L2 (4.3 GB)"},
+                "forms": res, "gpu_launches": None, "roofline": None, "cpu_baseline": None,
+                "e2e": None}
+        print(json.dumps(line), flush=True)
+    g.close()
 
 
 BOX_METRIC = ("particles/s per kick+drift over 96 independent periodic boxes "
@@ -399,12 +505,15 @@ def main():
     ap.add_argument("--accuracy-sinks", type=int, default=4096)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="plummer128", choices=["plummer128", "boxes96"])
+    ap.add_argument("--workload", default="plummer128",
+                    choices=["plummer128", "boxes96", "fft512"])
     ap.add_argument("--learned-base", type=float, default=3.0,
                     help="learned form: plain stencil of the base step (0: skip the form)")
     ap.add_argument("--learned-threshold", type=float, default=-4.0,
                     help="learned form: widen cells whose predicted log10 residual exceeds this")
     ap.add_argument("--learned-epochs", type=int, default=30)
+    ap.add_argument("--no-precision-form", dest="precision_form", action="store_false",
+                    help="skip the tensor-core FFT form")
     ap.add_argument("--tune-cache", default=None,
                     help="autotuner cache file (default: tune on every run)")
     args = ap.parse_args()
@@ -426,8 +535,8 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     torch.cuda.set_device(local)
 
-    if args.workload == "boxes96":
-        run_boxes(args, rank, world, local)
+    if args.workload in ("boxes96", "fft512"):
+        (run_boxes if args.workload == "boxes96" else run_fft512)(args, rank, world, local)
         if dist:
             dist.destroy_process_group()
         return
@@ -522,6 +631,9 @@ def main():
     forms = {"plain": {"value": plain_value, "ms_per_step": plain_ms, "accuracy": acc},
              "graph_autotuned": {"value": value, "ms_per_step": ms, "tuning": tune,
                                  "accuracy": acc}}
+    if args.precision_form and args.mesh in (256, 512):
+        forms["precision"] = precision_form(args, g, P, n, local, kp, accuracy, stream)
+        g.upload_dict(P)
     if args.learned_base > 0:
         forms["learned"] = learned_form(args, P, n, soft, local, kp, accuracy)
     if dist:

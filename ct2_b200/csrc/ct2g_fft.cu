@@ -428,7 +428,9 @@ template <typename T, int N, bool INV, bool VEC>
 int launch_cols(ct2g_ctx *ctx, typename Cplx<T>::type *spec, size_t nouter, size_t ostride,
                 size_t rstride, size_t ncols) {
   using C2 = typename Cplx<T>::type;
-  constexpr int W = N >= 256 ? 16 : 4096 / N;
+  // 16-column tiles from N = 256 on; FP64 at N = 512 takes 8 so that the
+  // double-buffered tile fits in shared memory
+  constexpr int W = N >= 256 ? (sizeof(C2) == 16 && N >= 512 ? 8 : 16) : 4096 / N;
   if (VEC && N >= 64) {
     if constexpr (sizeof(C2) == 8) {
       if (ctx->fft_tile == W / 2)

@@ -11,8 +11,10 @@
 // A are (line, n1) for stage 1 and (line, k2) for stage 2; a complex radix-R
 // DFT is the real 2R x 2R matrix [[Re F, -Im F], [Im F, Re F]] acting on
 // (Re, Im), and the split products x_hi F_hi + x_lo F_hi + x_hi F_lo are one
-// GEMM over K = 3 * 2R with A = [x_hi | x_lo | x_hi] and B = [F_hi | F_hi |
-// F_lo].  The DFT matrices are split on the host from FP64 values.
+// accumulation over K = 3 * 2R: B = [F_hi | F_hi | F_lo] in shared memory,
+// A = [x_hi | x_lo] with the third K block read from x_hi again (its
+// descriptor points back at the first block).  The DFT matrices are split on
+// the host from FP64 values.
 #include <cstring>
 
 #include "ct2g_internal.cuh"
@@ -21,26 +23,29 @@
 namespace {
 
 constexpr int TW = 8;   // lines per tile
+constexpr int TP = 9;   // tile row pitch (complex): odd, so strided reads spread over the banks
 constexpr int R1 = 16;  // radix of stage 2
 constexpr uint32_t kWaitLimit = 1u << 22;
 
 template <int N>
 struct TcShape {
   static constexpr int R2 = N / R1;
-  static constexpr int K1 = 6 * R2, N1 = 2 * R2;  // stage 1 GEMM
+  static constexpr int K1 = 6 * R2, N1 = 2 * R2;  // stage 1 GEMM (B's K extent)
   static constexpr int K2 = 6 * R1, N2 = 2 * R1;  // stage 2 GEMM
+  static constexpr int KA1 = 4 * R2, KA2 = 4 * R1; // A's stored K extent: [hi | lo]
   static constexpr int MT2 = TW * R2 / 128;        // 128-row tiles in stage 2
   static constexpr uint32_t KA = 16 * 128;         // K step of a 128-row A tile
   static constexpr uint32_t KB1 = (N1 / 8) * 128, KB2 = (N2 / 8) * 128;
-  static constexpr uint32_t SZ_A1 = (K1 / 8) * KA, SZ_A2 = MT2 * (K2 / 8) * KA;
+  static constexpr uint32_t SZ_A1 = (KA1 / 8) * KA, SZ_A2 = MT2 * (KA2 / 8) * KA;
   static constexpr uint32_t SZ_A = SZ_A1 > SZ_A2 ? SZ_A1 : SZ_A2;
   static constexpr uint32_t SZ_B1 = (K1 / 8) * KB1, SZ_B2 = (K2 / 8) * KB2;
-  static constexpr uint32_t SZ_TW = N * 8, SZ_T = N * TW * 8;
+  static constexpr uint32_t SZ_TW = N * 8, SZ_T = N * TP * 8;
   static constexpr uint32_t OFF_B1 = SZ_A, OFF_B2 = OFF_B1 + SZ_B1, OFF_TW = OFF_B2 + SZ_B2,
                             OFF_T = OFF_TW + SZ_TW, SMEM = OFF_T + SZ_T;
   static constexpr uint32_t TABLE = SZ_B1 + SZ_B2 + SZ_TW;  // bytes of one direction's tables
   static constexpr uint32_t TCOLS = (N1 + MT2 * N2) <= 64 ? 64 : 128;
   static_assert(TW * R1 == 128, "stage 1 rows");
+  static_assert(TW * R2 * 17 * 8 <= SZ_T, "transposed stage-1 results fit the tile buffer");
   static_assert(SMEM <= 200 * 1024, "shared memory");
 };
 
@@ -80,36 +85,54 @@ __global__ void __launch_bounds__(128) fft_cols_tc_kernel(float2 *__restrict__ a
   const uint32_t lane_base = (uint32_t)(32 * warp) << 16;
   unsigned char *A = sm;
   const float2 *tw = reinterpret_cast<const float2 *>(sm + S::OFF_TW);
-  float2 *T = reinterpret_cast<float2 *>(sm + S::OFF_T);  // [N][TW]
+  float2 *T = reinterpret_cast<float2 *>(sm + S::OFF_T);  // [N][TP], TW used
   const uint32_t sA = tc::smem_addr(A), sB1 = tc::smem_addr(sm + S::OFF_B1),
                  sB2 = tc::smem_addr(sm + S::OFF_B2);
   uint32_t phase = 0;
   bool ok = true;
+  // a tile is N rows of TW complex, 4 chunks of 16 bytes per row; every
+  // thread holds its chunks of the next tile in registers while the current
+  // one is transformed
+  constexpr int CH = N * 4 / 128;
+  float4 pre[CH];
+  auto fetch = [&](size_t t) {
+    const size_t outer = t / ntiles, c0 = (size_t)(t % ntiles) * TW;
+    const int nv = (int)min((size_t)TW, ncols - c0);
+    const float2 *b = a + outer * ostride + c0;
+#pragma unroll
+    for (int j = 0; j < CH; j++) {
+      const int e = tid + 128 * j, r = e >> 2, c = (e & 3) * 2;
+      float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (VEC && c + 1 < nv) {
+        v = __ldg(reinterpret_cast<const float4 *>(b + (size_t)r * rstride + c));
+      } else {
+        if (c < nv) {
+          const float2 u = b[(size_t)r * rstride + c];
+          v.x = u.x;
+          v.y = u.y;
+        }
+        if (c + 1 < nv) {
+          const float2 u = b[(size_t)r * rstride + c + 1];
+          v.z = u.x;
+          v.w = u.y;
+        }
+      }
+      pre[j] = v;
+    }
+  };
+  if ((size_t)blockIdx.x < ntot) fetch(blockIdx.x);
   for (size_t tile = blockIdx.x; tile < ntot; tile += gridDim.x) {
     const size_t outer = tile / ntiles;
     const size_t col0 = (size_t)(tile % ntiles) * TW;
     const int wv = (int)min((size_t)TW, ncols - col0);
     float2 *base = a + outer * ostride + col0;
-    // load the tile: row n holds TW complex, 4 chunks of 16 bytes
-    for (int e = tid; e < N * 4; e += 128) {
-      const int r = e >> 2, c = (e & 3) * 2;
-      float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (VEC && c + 1 < wv) {
-        v = *reinterpret_cast<const float4 *>(base + (size_t)r * rstride + c);
-      } else {
-        if (c < wv) {
-          const float2 u = base[(size_t)r * rstride + c];
-          v.x = u.x;
-          v.y = u.y;
-        }
-        if (c + 1 < wv) {
-          const float2 u = base[(size_t)r * rstride + c + 1];
-          v.z = u.x;
-          v.w = u.y;
-        }
-      }
-      reinterpret_cast<float4 *>(T)[e] = v;
+#pragma unroll
+    for (int j = 0; j < CH; j++) {
+      const int e = tid + 128 * j, r = e >> 2, c = (e & 3) * 2;
+      T[r * TP + c] = make_float2(pre[j].x, pre[j].y);
+      T[r * TP + c + 1] = make_float2(pre[j].z, pre[j].w);
     }
+    if (tile + gridDim.x < ntot) fetch(tile + gridDim.x);
     __syncthreads();
     // stage 1 operand: row tid = (w, n1); K = [hi | lo | hi] x (Re, Im) x n2
     {
@@ -117,12 +140,12 @@ __global__ void __launch_bounds__(128) fft_cols_tc_kernel(float2 *__restrict__ a
       float hr[R2], lr[R2], hi_[R2], li[R2];
 #pragma unroll
       for (int n2 = 0; n2 < R2; n2++) {
-        const float2 x = T[(n1 + R1 * n2) * TW + w];
+        const float2 x = T[(n1 + R1 * n2) * TP + w];
         split_bf16(x.x, hr[n2], lr[n2]);
         split_bf16(x.y, hi_[n2], li[n2]);
       }
 #pragma unroll
-      for (int kg = 0; kg < S::K1 / 8; kg++) {
+      for (int kg = 0; kg < S::KA1 / 8; kg++) {
         const int blk = (8 * kg) / (2 * R2), kk = (8 * kg) % (2 * R2);
         const bool im = kk >= R2;
         const int m0 = im ? kk - R2 : kk;
@@ -140,9 +163,11 @@ __global__ void __launch_bounds__(128) fft_cols_tc_kernel(float2 *__restrict__ a
     if (tid == 0) {
       constexpr uint32_t idesc = tc::idesc_bf16_f32(128, S::N1);
 #pragma unroll
-      for (int kk = 0; kk < S::K1 / 16; kk++)
-        tc::mma_bf16(tmem, tc::sdesc(sA + kk * 2 * S::KA, S::KA, 128),
+      for (int kk = 0; kk < S::K1 / 16; kk++) {
+        const int ka = kk < S::KA1 / 16 ? kk : kk - S::KA1 / 16;  // third block: x_hi again
+        tc::mma_bf16(tmem, tc::sdesc(sA + ka * 2 * S::KA, S::KA, 128),
                      tc::sdesc(sB1 + kk * 2 * S::KB1, S::KB1, 128), idesc, kk > 0);
+      }
       tc::mma_commit(&bar);
     }
     ok = __syncthreads_and(tc::mbar_wait(&bar, phase, kWaitLimit));
@@ -155,25 +180,41 @@ __global__ void __launch_bounds__(128) fft_cols_tc_kernel(float2 *__restrict__ a
       float y[S::N1];
 #pragma unroll
       for (int c = 0; c < S::N1; c += 32) tc::tmem_ld32(tmem + lane_base + (uint32_t)c, y + c);
-      // twiddle, split, and write stage 2's operand: row (w, k2), K = n1
+      // twiddle; the results go through the tile buffer (free now) transposed
+      // to rows (w, k2) of 16 complex n1 values (pitch 17)
 #pragma unroll
       for (int k2 = 0; k2 < R2; k2++) {
         const float2 t = tw[n1 * k2];
         const float re = y[k2] * t.x - y[R2 + k2] * t.y;
         const float im = y[k2] * t.y + y[R2 + k2] * t.x;
-        float rh, rl, ih, il;
-        split_bf16(re, rh, rl);
-        split_bf16(im, ih, il);
-        const int r2 = w * R2 + k2;
-        unsigned char *At = A + (r2 >> 7) * (S::K2 / 8) * S::KA;
-        const uint32_t row = (uint32_t)(r2 & 127);
-        const __nv_bfloat16 vals[6] = {__float2bfloat16_rn(rh), __float2bfloat16_rn(ih),
-                                       __float2bfloat16_rn(rl), __float2bfloat16_rn(il),
-                                       __float2bfloat16_rn(rh), __float2bfloat16_rn(ih)};
+        T[(w * R2 + k2) * 17 + n1] = make_float2(re, im);
+      }
+    }
+    __syncthreads();
+    // stage 2 operand: row r2 = (w, k2); K = [hi | lo | hi] x (Re, Im) x n1
 #pragma unroll
-        for (int b = 0; b < 6; b++)
-          *reinterpret_cast<__nv_bfloat16 *>(At + tc::kmajor_offset(row, R1 * b + n1, S::KA, 128)) =
-              vals[b];
+    for (int mt = 0; mt < S::MT2; mt++) {
+      const int r2 = mt * 128 + tid;
+      float hr[R1], lr[R1], hi_[R1], li[R1];
+#pragma unroll
+      for (int n1 = 0; n1 < R1; n1++) {
+        const float2 x = T[r2 * 17 + n1];
+        split_bf16(x.x, hr[n1], lr[n1]);
+        split_bf16(x.y, hi_[n1], li[n1]);
+      }
+      unsigned char *At = A + mt * (S::KA2 / 8) * S::KA;
+#pragma unroll
+      for (int kg = 0; kg < S::KA2 / 8; kg++) {
+        const int blk = (8 * kg) / (2 * R1), kk = (8 * kg) % (2 * R1);
+        const bool im = kk >= R1;
+        const int m0 = im ? kk - R1 : kk;
+        const float *src = blk == 1 ? (im ? li : lr) : (im ? hi_ : hr);
+        uint4 q;
+        q.x = pack_bf16(src[m0 + 0], src[m0 + 1]);
+        q.y = pack_bf16(src[m0 + 2], src[m0 + 3]);
+        q.z = pack_bf16(src[m0 + 4], src[m0 + 5]);
+        q.w = pack_bf16(src[m0 + 6], src[m0 + 7]);
+        *reinterpret_cast<uint4 *>(At + tc::kmajor_offset(tid, 8 * kg, S::KA, 128)) = q;
       }
     }
     tc::fence_before_sync();
@@ -185,10 +226,12 @@ __global__ void __launch_bounds__(128) fft_cols_tc_kernel(float2 *__restrict__ a
 #pragma unroll
       for (int mt = 0; mt < S::MT2; mt++)
 #pragma unroll
-        for (int kk = 0; kk < S::K2 / 16; kk++)
+        for (int kk = 0; kk < S::K2 / 16; kk++) {
+          const int ka = kk < S::KA2 / 16 ? kk : kk - S::KA2 / 16;
           tc::mma_bf16(tmem + (uint32_t)(S::N1 + mt * S::N2),
-                       tc::sdesc(sA + mt * (S::K2 / 8) * S::KA + kk * 2 * S::KA, S::KA, 128),
+                       tc::sdesc(sA + mt * (S::KA2 / 8) * S::KA + ka * 2 * S::KA, S::KA, 128),
                        tc::sdesc(sB2 + kk * 2 * S::KB2, S::KB2, 128), idesc, kk > 0);
+        }
       tc::mma_commit(&bar);
     }
     ok = __syncthreads_and(tc::mbar_wait(&bar, phase, kWaitLimit));
@@ -202,12 +245,13 @@ __global__ void __launch_bounds__(128) fft_cols_tc_kernel(float2 *__restrict__ a
       float v[32];
       tc::tmem_ld32(tmem + lane_base + (uint32_t)(S::N1 + mt * S::N2), v);
 #pragma unroll
-      for (int k1 = 0; k1 < R1; k1++) T[(k2 + R2 * k1) * TW + w] = make_float2(v[k1], v[R1 + k1]);
+      for (int k1 = 0; k1 < R1; k1++) T[(k2 + R2 * k1) * TP + w] = make_float2(v[k1], v[R1 + k1]);
     }
     __syncthreads();
     for (int e = tid; e < N * 4; e += 128) {
       const int r = e >> 2, c = (e & 3) * 2;
-      const float4 v = reinterpret_cast<const float4 *>(T)[e];
+      const float2 u0 = T[r * TP + c], u1 = T[r * TP + c + 1];
+      const float4 v = make_float4(u0.x, u0.y, u1.x, u1.y);
       if (VEC && c + 1 < wv) {
         *reinterpret_cast<float4 *>(base + (size_t)r * rstride + c) = v;
       } else {
@@ -289,6 +333,9 @@ int launch_tc(ct2g_ctx *ctx, float2 *spec, size_t nouter, size_t ostride, size_t
                    (reinterpret_cast<uintptr_t>(spec) % 16 == 0);
   auto k = vec ? fft_cols_tc_kernel<N, true> : fft_cols_tc_kernel<N, false>;
   CT2G_CUDA(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM));
+  // all of the unified L1 as shared memory, so that several CTAs fit per SM
+  CT2G_CUDA(ctx, cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                      (int)cudaSharedmemCarveoutMaxShared));
   int per_sm = 0;
   CT2G_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 128, S::SMEM));
   per_sm = std::max(1, std::min(per_sm, (int)(512 / S::TCOLS)));  // tensor memory columns
