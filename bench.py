@@ -265,6 +265,120 @@ def learned_form(args, P, n, soft, local, kp, accuracy):
 
 
 FFT_METRIC = "3D FFT of 4 x 512^3 moment grids (grid points/s, forward + inverse)"
+NFW_METRIC = "particles/s per kick+drift, 256^3 NFW halos on a 512^3 mesh"
+
+
+def run_nfw(args, rank, world, local):
+    """--workload nfw256: the learned form's configuration.  256^3 particles in
+    2000 NFW halos (c ~ U[5,15], dN/dM ~ M^-1.9 over two decades, r_vir ~
+    M^(1/3)), 512^3 mesh, Plummer eps = cell/25, order --order.  plain: the
+    graph step at bwidth --bwidth.  learned: bwidth --learned-base, the cells
+    an MLP (trained first on the same generator with another seed) selects
+    widened to --bwidth.  Both judged on a seeded 1% particle sample against
+    the FP64 Ewald direct sum."""
+    import torch
+
+    from ct2_b200 import ics, replicas
+    from ct2_b200.gravity import Gravity, kick_params
+    ng = 256
+    n = ng ** 3
+    M = 512
+    soft = 1.0 / (25 * M)
+    t = time.perf_counter()
+    P = ics.nfw_halos(n, seed=args.seed + rank)
+    gen_s = time.perf_counter() - t
+    kp = kick_params(ascending=True, descending=True, top=True, first=False, rung=0,
+                     t0=args.dt, eta=0.15, max_dt=0.01, scale=1.0)
+    rng = np.random.Generator(np.random.PCG64(321))
+    sel = np.sort(rng.choice(n, size=max(1, int(round(args.nfw_sample * n))), replace=False))
+
+    def timed(g):
+        st = torch.cuda.ExternalStream(g.stream(), device=local)
+        g.upload_dict(P)
+        for _ in range(args.warmup):
+            g.kick_drift(kp, args.dt, 1.0, graph=True, wait=False)
+        g.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(args.steps):
+            g.kick_drift(kp, args.dt, 1.0, graph=True, wait=False)
+        e1.record(st)
+        e1.synchronize()
+        g.synchronize()
+        return e0.elapsed_time(e1) / args.steps
+
+    def errors(g, truth):
+        g.upload_dict(P)
+        g.particle_to_grid()
+        g.compute_forces()
+        f, _ = g.forces()
+        ids = g.download()["id"]
+        inv = np.empty_like(ids)
+        inv[ids] = np.arange(n, dtype=ids.dtype)
+        d = np.linalg.norm(f[inv[sel]] - truth, axis=1)
+        tn = np.linalg.norm(truth, axis=1)
+        return {"rms_rel": float(np.sqrt(np.mean((d / tn) ** 2))), "max_rel": float((d / tn).max()),
+                "sinks": int(len(sel))}
+
+    g = Gravity(mesh=M, order=args.order, bwidth=args.bwidth, hsoft=soft, GM=1.0 / n,
+                device=local, max_particles=n)
+    g.upload_dict(P)
+    t = time.perf_counter()
+    truth = g.ewald_direct(P["x"][sel], P["y"][sel], P["z"][sel])
+    truth_s = time.perf_counter() - t
+    plain_acc = errors(g, truth)
+    inter = g.interaction_count()
+    plain_ms = timed(g)
+    g.close()
+    del g
+    gl = Gravity(mesh=M, order=args.order, bwidth=args.learned_base, hsoft=soft, GM=1.0 / n,
+                 device=local, max_particles=n)
+    gl.learned_enable(args.bwidth)
+    t = time.perf_counter()
+    Pt = ics.nfw_halos(n, seed=args.seed + 100 + rank)
+    gl.upload_dict(Pt)
+    del Pt
+    gl.particle_to_grid()
+    ncell = gl.learned_collect()
+    gl.mlp_init(seed=1)
+    loss = gl.mlp_train(epochs=args.learned_epochs, batch=4096, lr=2e-3, seed=2)
+    gl.synchronize()
+    train_s = time.perf_counter() - t
+    gl.learned_select("none")
+    base_acc = errors(gl, truth)
+    base_ms = timed(gl)
+    gl.learned_select("mlp", args.learned_threshold)
+    learned_acc = errors(gl, truth)
+    nsel = gl.learned_cells()["nselected"]
+    learned_ms = timed(gl)
+    gl.close()
+    value, ms = replicas.job_throughput(n, plain_ms, device="cuda")
+    if rank == 0:
+        line = {"metric": NFW_METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic: seeded NFW halos",
+                "config": {"workload": "nfw256_mesh512", "particles_per_gpu": n, "mesh": M,
+                           "order": args.order, "bwidth": args.bwidth,
+                           "softening": "plummer eps=cell/25", "halos": 2000,
+                           "l2": "inputs larger than L2"},
+                "accuracy": plain_acc, "interactions_per_step": inter,
+                "forms": {"plain": {"value": n / (plain_ms * 1e-3), "ms_per_step": plain_ms,
+                                    "accuracy": plain_acc},
+                          "base_narrow": {"bwidth": args.learned_base,
+                                          "value": n / (base_ms * 1e-3), "ms_per_step": base_ms,
+                                          "accuracy": base_acc},
+                          "learned": {"value": n / (learned_ms * 1e-3), "ms_per_step": learned_ms,
+                                      "accuracy": learned_acc, "cells_selected": int(nsel),
+                                      "threshold_log10": args.learned_threshold,
+                                      "training": {"cells": int(ncell), "mse": loss,
+                                                   "seconds": train_s,
+                                                   "state": "same generator, seed + 100"}}},
+                "timings_s": {"generate": gen_s, "ewald_truth": truth_s},
+                "e2e": None, "gpu_launches": None, "roofline": None, "cpu_baseline": None}
+        print(json.dumps(line), flush=True)
+
 
 
 def run_fft512(args, rank, world, local):
@@ -506,7 +620,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", default="plummer128",
-                    choices=["plummer128", "boxes96", "fft512"])
+                    choices=["plummer128", "boxes96", "fft512", "nfw256"])
+    ap.add_argument("--nfw-sample", type=float, default=0.01,
+                    help="nfw256: fraction of particles judged against FP64 Ewald")
     ap.add_argument("--learned-base", type=float, default=3.0,
                     help="learned form: plain stencil of the base step (0: skip the form)")
     ap.add_argument("--learned-threshold", type=float, default=-4.0,
@@ -535,8 +651,9 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     torch.cuda.set_device(local)
 
-    if args.workload in ("boxes96", "fft512"):
-        (run_boxes if args.workload == "boxes96" else run_fft512)(args, rank, world, local)
+    if args.workload in ("boxes96", "fft512", "nfw256"):
+        {"boxes96": run_boxes, "fft512": run_fft512, "nfw256": run_nfw}[args.workload](
+            args, rank, world, local)
         if dist:
             dist.destroy_process_group()
         return
