@@ -318,6 +318,11 @@ int ct2g_fft_cols_tc(ct2g_ctx *ctx, float2 *spec, int N, size_t nouter, size_t o
 int ct2g_learned_apply(ct2g_ctx *ctx, bool pot);
 int ct2g_learned_resize(ct2g_ctx *ctx);  // per-cell arrays follow the particle capacity
 void ct2g_learned_free(ct2g_ctx *ctx);
+// near-field direct sum of listed sinks over the cell window lo2 < |o|^2 <=
+// hi2 (ct2g_near.cu); sparse-style chunks, persistent over *nch / *work
+int ct2g_near_window(ct2g_ctx *ctx, const uint2 *chunks, const uint32_t *nch, uint32_t *work,
+                     const uint32_t *slist, const unsigned long long *stm, float lo2, float hi2,
+                     bool pot, float *fx, float *fy, float *fz, float *po);
 // D^n phi_eps(-o h) for the offsets o (x,y,z triples) -> d_out[nshell][nc]
 int ct2g_shell_greens(ct2g_ctx *ctx, const std::vector<int> &offs3, float *d_out);
 // far field of the current range into the force buffers (P2M if needed, mesh

@@ -53,7 +53,21 @@ struct ct2g_learn {
   uint32_t *cells = nullptr;   // occupied cell keys
   uint32_t *flags = nullptr;   // scratch
   uint32_t *scan = nullptr;    // scratch
-  uint32_t *d_cnt = nullptr;   // [0] cells [1] selected [2] chunks [3] work counter
+  uint32_t *d_cnt = nullptr;   // [0] cells [1] selected cells [2] chunks [3] work counter
+                               // [4] selected sinks [5] scan total scratch
+  // block-walk form of the widening (bwidth_ext <= 4): stencil masks of the
+  // shell per (in-block cell, neighbouring block), selected cells and sinks
+  unsigned long long *d_stm = nullptr;  // [64][27]
+  uint32_t *sel_cells = nullptr;        // [nsel] index into cells
+  uint32_t *pflag = nullptr, *pscan = nullptr;  // per particle of the range
+  uint32_t *ssink = nullptr, *scell = nullptr;  // [nsink] particle, selected-cell rank
+  uint32_t *cflag = nullptr, *cscan = nullptr;  // chunk starts over the sink list
+  float *lsub = nullptr;                        // [nsel][nc] mesh terms of the shell
+  // compact moments of the occupied cells ([ncell][nc], components
+  // contiguous) and the cell key -> record index (~0u: empty cell)
+  float *mc = nullptr;
+  uint32_t *idx = nullptr;
+  size_t idx_cap = 0;
   float *X = nullptr;          // [cap][NIN] features
   float *score = nullptr;      // fixed criterion
   float *pred = nullptr;       // MLP output
@@ -93,6 +107,12 @@ __global__ void run_list_kernel(const uint32_t *__restrict__ keys, size_t nr,
   if (i < nr && flag[i]) cells[scan[i]] = keys[i];
 }
 
+__global__ void cell_index_kernel(const uint32_t *__restrict__ cells,
+                                  const uint32_t *__restrict__ cnt, uint32_t *__restrict__ idx) {
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < cnt[0]) idx[cells[c]] = c;
+}
+
 struct CellGeo {
   int mbits;
   uint32_t cmask;  // C - 1
@@ -114,6 +134,20 @@ struct CellGeo {
   }
 };
 
+// all components of an occupied cell's moments, contiguous
+__global__ void compact_moments_kernel(const uint32_t *__restrict__ cells,
+                                       const uint32_t *__restrict__ cnt,
+                                       const float *__restrict__ grid, int64_t CB, CellGeo geo,
+                                       int nc, float *__restrict__ mc) {
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= cnt[0]) return;
+  uint32_t box;
+  int i, j, k;
+  geo.decode(cells[c], box, i, j, k);
+  const int64_t r = geo.rowmajor(box, i, j, k);
+  for (int q = 0; q < nc; q++) mc[(size_t)c * nc + q] = grid[(int64_t)q * CB + r];
+}
+
 __device__ __forceinline__ float warp_sum(float v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -126,11 +160,12 @@ __device__ __forceinline__ float warp_sum(float v) {
 template <int P>
 __global__ void __launch_bounds__(256) features_kernel(
     const uint32_t *__restrict__ cells, const uint32_t *__restrict__ cnt,
-    const uint32_t *__restrict__ cs, const float *__restrict__ grid, int64_t CB, CellGeo geo,
-    const int *__restrict__ shell, int nshell, const float *__restrict__ fx,
-    const float *__restrict__ fy, const float *__restrict__ fz,
+    const uint32_t *__restrict__ cs, const float *__restrict__ mc,
+    const uint32_t *__restrict__ idx, CellGeo geo, const int *__restrict__ shell, int nshell,
+    const float *__restrict__ fx, const float *__restrict__ fy, const float *__restrict__ fz,
     const uint32_t *__restrict__ box_off, const float *__restrict__ box_gm,
     float *__restrict__ X, float *__restrict__ score) {
+  constexpr int NC = ct2g_ncomp(P);
   const int lane = threadIdx.x & 31;
   const uint32_t ncell = cnt[0];
   const int M = 1 << geo.mbits;
@@ -160,12 +195,9 @@ __global__ void __launch_bounds__(256) features_kernel(
     s2 = warp_sum(s2);
     const float fmean = fmaxf(s1 / nc, 1e-30f);
     const float fstdv = sqrtf(fmaxf(s2 / nc - fmean * fmean, 0.f));
-    const int64_t rc = geo.rowmajor(box, ix, iy, iz);
-    const float sig_c = sqrtf(fmaxf(2.f * (grid[i200 * CB + rc] + grid[i020 * CB + rc] +
-                                           grid[i002 * CB + rc]) / nc, 0.f));
-    const float dip = sqrtf(grid[i100 * CB + rc] * grid[i100 * CB + rc] +
-                            grid[i010 * CB + rc] * grid[i010 * CB + rc] +
-                            grid[i001 * CB + rc] * grid[i001 * CB + rc]) / nc;
+    const float *mo = mc + (size_t)ci * NC;
+    const float sig_c = sqrtf(fmaxf(2.f * (mo[i200] + mo[i020] + mo[i002]) / nc, 0.f));
+    const float dip = sqrtf(mo[i100] * mo[i100] + mo[i010] * mo[i010] + mo[i001] * mo[i001]) / nc;
     // shell sums per distance bin
     float cntb[3] = {0.f, 0.f, 0.f}, mono[3] = {0.f, 0.f, 0.f}, quad[3] = {0.f, 0.f, 0.f},
           trunc[3] = {0.f, 0.f, 0.f};
@@ -173,12 +205,11 @@ __global__ void __launch_bounds__(256) features_kernel(
     for (int s = lane; s < nshell; s += 32) {
       const int4 o = reinterpret_cast<const int4 *>(shell)[s];
       const uint32_t k2 = geo.key(box, ix + o.x, iy + o.y, iz + o.z);
-      const uint32_t n2 = cs[k2 + 1] - cs[k2];
-      if (!n2) continue;
-      const float ns = (float)n2;
-      const int64_t r2c = geo.rowmajor(box, ix + o.x, iy + o.y, iz + o.z);
-      const float sig2 = fmaxf(2.f * (grid[i200 * CB + r2c] + grid[i020 * CB + r2c] +
-                                      grid[i002 * CB + r2c]) / ns, 0.f);
+      const uint32_t c2 = idx[k2];
+      if (c2 == ~0u) continue;
+      const float ns = (float)(cs[k2 + 1] - cs[k2]);
+      const float *m2 = mc + (size_t)c2 * NC;
+      const float sig2 = fmaxf(2.f * (m2[i200] + m2[i020] + m2[i002]) / ns, 0.f);
       const float R2 = (float)(o.x * o.x + o.y * o.y + o.z * o.z) * h * h;
       const float R = sqrtf(R2);
       const float m = ns / R2;
@@ -425,6 +456,140 @@ __global__ void chunk_list_kernel(const uint32_t *__restrict__ cells,
     chunks[first[c] + j] = make_uint2(c, ((32u * j) << 8) | min(32u, n - 32u * j));
 }
 
+// ---- block-walk widening (bwidth_ext <= 4) ---------------------------------
+// selected cells -> 0/1 flags over the range's upper bound (scan: rank)
+__global__ void sel_flag_kernel(const uint32_t *__restrict__ cnt, const uint8_t *__restrict__ sel,
+                                size_t nr, uint32_t *__restrict__ flag) {
+  const size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < nr) flag[c] = (c < cnt[0] && sel[c]) ? 1u : 0u;
+}
+
+__global__ void sel_list_kernel(const uint32_t *__restrict__ cnt, const uint8_t *__restrict__ sel,
+                                const uint32_t *__restrict__ rank, uint32_t *__restrict__ sel_cells) {
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < cnt[0] && sel[c]) sel_cells[rank[c]] = c;
+}
+
+// particles of the selected cells (one thread per selected cell)
+__global__ void sink_flag_kernel(const uint32_t *__restrict__ cnt,
+                                 const uint32_t *__restrict__ sel_cells,
+                                 const uint32_t *__restrict__ cells, const uint32_t *__restrict__ cs,
+                                 uint32_t begin, uint32_t *__restrict__ pflag) {
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= cnt[1]) return;
+  const uint32_t key = cells[sel_cells[j]];
+  for (uint32_t i = cs[key]; i < cs[key + 1]; i++) pflag[i - begin] = 1u;
+}
+
+__global__ void sink_list_kernel(const uint32_t *__restrict__ cnt,
+                                 const uint32_t *__restrict__ sel_cells,
+                                 const uint32_t *__restrict__ cells, const uint32_t *__restrict__ cs,
+                                 uint32_t begin, const uint32_t *__restrict__ pscan,
+                                 uint32_t *__restrict__ ssink, uint32_t *__restrict__ scell) {
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= cnt[1]) return;
+  const uint32_t key = cells[sel_cells[j]];
+  for (uint32_t i = cs[key]; i < cs[key + 1]; i++) {
+    const uint32_t q = pscan[i - begin];
+    ssink[q] = i;
+    scell[q] = j;
+  }
+}
+
+// chunk starts over the sink list: the first selected sink of every 4x4x4
+// cell block and every 32nd one after it
+__global__ void sink_chunk_flag_kernel(const uint32_t *__restrict__ keys,
+                                       const uint32_t *__restrict__ cs,
+                                       const uint32_t *__restrict__ pflag,
+                                       const uint32_t *__restrict__ pscan, uint32_t begin,
+                                       size_t nr, uint32_t *__restrict__ cflag) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nr || !pflag[i]) return;
+  const uint32_t q = pscan[i];
+  const uint32_t f = cs[keys[i] & ~63u] - begin;  // first particle of the block (<= i)
+  cflag[q] = ((q - pscan[f]) % 32u) == 0u ? 1u : 0u;
+}
+
+__global__ void sink_chunk_fill_kernel(const uint32_t *__restrict__ cnt,
+                                       const uint32_t *__restrict__ cflag,
+                                       const uint32_t *__restrict__ cscan,
+                                       const uint32_t *__restrict__ ssink,
+                                       const uint32_t *__restrict__ keys,
+                                       const uint32_t *__restrict__ cs,
+                                       const uint32_t *__restrict__ pscan, uint32_t begin,
+                                       size_t nr, uint2 *__restrict__ chunks) {
+  const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t nsink = cnt[4];
+  if (q >= nsink || !cflag[q]) return;
+  const uint32_t i = ssink[q] - begin;
+  const uint32_t e = cs[(keys[i] | 63u) + 1] - begin;  // past the block
+  const uint32_t qe = e < nr ? pscan[e] : nsink;
+  chunks[cscan[q]] = make_uint2(q, min(32u, qe - q));
+}
+
+// the mesh's Taylor term of the shell, once per selected cell: warp per
+// cell, lanes over the shell offsets
+template <int P>
+__global__ void __launch_bounds__(256) shell_m2l_kernel(
+    const uint32_t *__restrict__ cnt, const uint32_t *__restrict__ sel_cells,
+    const uint32_t *__restrict__ cells, const float *__restrict__ mc,
+    const uint32_t *__restrict__ idx, CellGeo geo, const int *__restrict__ shell,
+    const float *__restrict__ shellG, int nshell, float *__restrict__ lsub) {
+  constexpr int NC = ct2g_ncomp(P);
+  constexpr Mg2lPairs<P> T{};
+  const int lane = threadIdx.x & 31;
+  const uint32_t nsel = cnt[1];
+  for (uint32_t j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; j < nsel;
+       j += (gridDim.x * blockDim.x) >> 5) {
+    const uint32_t key = cells[sel_cells[j]];
+    uint32_t box;
+    int ix, iy, iz;
+    geo.decode(key, box, ix, iy, iz);
+    float L[NC];
+#pragma unroll
+    for (int k = 0; k < NC; k++) L[k] = 0.f;
+    for (int s = lane; s < nshell; s += 32) {
+      const int4 o = reinterpret_cast<const int4 *>(shell)[s];
+      const uint32_t c2 = idx[geo.key(box, ix + o.x, iy + o.y, iz + o.z)];
+      if (c2 == ~0u) continue;
+      float Mv[NC];
+#pragma unroll
+      for (int k = 0; k < NC; k++) Mv[k] = mc[(size_t)c2 * NC + k];
+      const float *G = shellG + (size_t)s * NC;
+#pragma unroll
+      for (int q = 0; q < Mg2lPairs<P>::NP; q++) L[T.a[q]] = fmaf(__ldg(G + T.ab[q]), Mv[T.b[q]], L[T.a[q]]);
+    }
+#pragma unroll
+    for (int k = 0; k < NC; k++) L[k] = warp_sum(L[k]);
+    if (lane == 0)
+#pragma unroll
+      for (int k = 0; k < NC; k++) lsub[(size_t)j * NC + k] = L[k];
+  }
+}
+
+// removes the shell's mesh term from every selected sink
+template <int P, bool POT>
+__global__ void shell_l2p_kernel(const uint32_t *__restrict__ cnt, const uint32_t *__restrict__ ssink,
+                                 const uint32_t *__restrict__ scell, const uint32_t *__restrict__ keys,
+                                 uint32_t begin, int mbits, const float4 *__restrict__ src,
+                                 const float *__restrict__ lsub, const float *__restrict__ box_gm,
+                                 float *__restrict__ ofx, float *__restrict__ ofy,
+                                 float *__restrict__ ofz, float *__restrict__ opot) {
+  constexpr int NC = ct2g_ncomp(P);
+  const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= cnt[4]) return;
+  const uint32_t i = ssink[q];
+  const float *Lc = lsub + (size_t)scell[q] * NC;
+  const float4 t = src[i];
+  const float GM = box_gm[keys[i - begin] >> (3 * mbits)];
+  float fx, fy, fz, ph;
+  ct2g_l2p<P>([&](int k) { return __ldg(Lc + k); }, t.x, t.y, t.z, fx, fy, fz, ph);
+  ofx[i] -= GM * fx;
+  ofy[i] -= GM * fy;
+  ofz[i] -= GM * fz;
+  if (POT) opot[i] -= GM * ph;
+}
+
 // Shell correction, one warp per chunk of <= 32 sinks of a selected cell,
 // persistent over the device-held chunk count (cnt[2], work counter cnt[3]).
 // Lanes walk the shell offsets 32 at a time: each lane adds its source
@@ -612,9 +777,14 @@ __global__ void loss_sum_kernel(const float *__restrict__ l, int n, float *__res
 // ---------------------------------------------------------------------------
 int free_learn_cells(ct2g_learn *L) {
   void *ptrs[] = {L->cells, L->flags, L->scan, L->X, L->score, L->pred, L->sel, L->chunks,
-                  L->ex, L->ey, L->ez};
+                  L->ex, L->ey, L->ez, L->sel_cells, L->pflag, L->pscan, L->ssink, L->scell,
+                  L->cflag, L->cscan, L->lsub};
   for (void *p : ptrs)
     if (p) cudaFree(p);
+  L->sel_cells = L->pflag = L->pscan = L->ssink = L->scell = L->cflag = L->cscan = nullptr;
+  L->lsub = nullptr;
+  if (L->mc) cudaFree(L->mc);
+  L->mc = nullptr;
   L->cells = L->flags = L->scan = nullptr;
   L->X = L->score = L->pred = L->ex = L->ey = L->ez = nullptr;
   L->sel = nullptr;
@@ -640,6 +810,22 @@ int learn_cells_alloc(ct2g_ctx *ctx) {
   A(L->ex, cap * 4);
   A(L->ey, cap * 4);
   A(L->ez, cap * 4);
+  A(L->sel_cells, cap * 4);
+  A(L->pflag, cap * 4);
+  A(L->pscan, cap * 4);
+  A(L->ssink, cap * 4);
+  A(L->scell, cap * 4);
+  A(L->cflag, cap * 4);
+  A(L->cscan, cap * 4);
+  A(L->lsub, cap * sizeof(float) * ctx->nc);
+  A(L->mc, cap * sizeof(float) * ctx->nc);
+  if (L->idx_cap < (size_t)ctx->CB) {
+    if (L->idx) cudaFree(L->idx);
+    L->idx = nullptr;
+    L->idx_cap = 0;
+    A(L->idx, sizeof(uint32_t) * (size_t)ctx->CB);
+    L->idx_cap = (size_t)ctx->CB;
+  }
 #undef A
   L->cap = cap;
   ctx->epoch++;
@@ -662,6 +848,14 @@ int occupied_cells(ct2g_ctx *ctx) {
   CT2G_TRY(ct2g_scan_exclusive(ctx, L->flags, L->scan, nr, L->d_cnt, 0));
   run_list_kernel<<<ct2g_div_up(nr, 256), 256, 0, st>>>(ctx->keys, nr, L->flags, L->scan, L->cells);
   CT2G_LAUNCHED(ctx);
+  // key -> record index and the compact moment records
+  CT2G_CUDA(ctx, cudaMemsetAsync(L->idx, 0xFF, sizeof(uint32_t) * (size_t)ctx->CB, st));
+  cell_index_kernel<<<ct2g_div_up(nr, 256), 256, 0, st>>>(L->cells, L->d_cnt, L->idx);
+  CT2G_LAUNCHED(ctx);
+  compact_moments_kernel<<<ct2g_div_up(nr, 256), 256, 0, st>>>(L->cells, L->d_cnt, ctx->grid,
+                                                               ctx->CB, geo_of(ctx), ctx->nc,
+                                                               L->mc);
+  CT2G_LAUNCHED(ctx);
   return CT2G_OK;
 }
 
@@ -676,7 +870,7 @@ int launch_features(ct2g_ctx *ctx, const float *fx, const float *fy, const float
   ct2g_learn *L = ctx->learn;
   const size_t nr = ctx->n - ctx->rung_begin;
   features_kernel<P><<<warp_grid(ctx, nr), 256, 0, ctx->stream>>>(
-      L->cells, L->d_cnt, ctx->cell_start, ctx->grid, ctx->CB, geo_of(ctx), L->d_shell, L->nshell,
+      L->cells, L->d_cnt, ctx->cell_start, L->mc, L->idx, geo_of(ctx), L->d_shell, L->nshell,
       fx, fy, fz, ctx->box_off, ctx->box_gm, L->X, L->score);
   CT2G_LAUNCHED(ctx);
   return CT2G_OK;
@@ -708,8 +902,9 @@ int infer(ct2g_ctx *ctx) {
   return CT2G_OK;
 }
 
-// selection -> chunk list (count in d_cnt[2]); work counter d_cnt[3] reset
-int build_chunks(ct2g_ctx *ctx, int mode, float thr) {
+// selection (count in d_cnt[1]); with `lists`, the per-cell chunk list of
+// the cell-walk form too (count in d_cnt[2]); work counter d_cnt[3] reset
+int build_chunks(ct2g_ctx *ctx, int mode, float thr, bool lists) {
   ct2g_learn *L = ctx->learn;
   const size_t nr = ctx->n - ctx->rung_begin;
   cudaStream_t st = ctx->stream;
@@ -720,6 +915,7 @@ int build_chunks(ct2g_ctx *ctx, int mode, float thr) {
                                                       L->score, L->pred, mode, thr, L->flags,
                                                       L->sel, L->d_cnt + 1);
   CT2G_LAUNCHED(ctx);
+  if (!lists) return CT2G_OK;
   CT2G_TRY(ct2g_scan_exclusive(ctx, L->flags, L->scan, nr, L->d_cnt + 2, 0));
   chunk_list_kernel<<<ct2g_div_up(nr, 256), 256, 0, st>>>(L->cells, L->d_cnt, ctx->cell_start,
                                                           L->flags, L->scan, L->chunks);
@@ -760,6 +956,70 @@ int shell_correct(ct2g_ctx *ctx, bool pot, float *fx, float *fy, float *fz, floa
     case 4: return launch_shell_p<4>(ctx, pot, fx, fy, fz, po);
     case 5: return launch_shell_p<5>(ctx, pot, fx, fy, fz, po);
     case 6: return launch_shell_p<6>(ctx, pot, fx, fy, fz, po);
+  }
+  return ct2g_fail(ctx, CT2G_EINVAL, "unsupported order");
+}
+
+template <int P>
+int widen_block_p(ct2g_ctx *ctx, bool pot, float *fx, float *fy, float *fz, float *po) {
+  ct2g_learn *L = ctx->learn;
+  const size_t nr = ctx->n - ctx->rung_begin;
+  const uint32_t begin = (uint32_t)ctx->rung_begin;
+  cudaStream_t st = ctx->stream;
+  const unsigned T = 256, G = ct2g_div_up(nr, T);
+  sel_flag_kernel<<<G, T, 0, st>>>(L->d_cnt, L->sel, nr, L->flags);
+  CT2G_LAUNCHED(ctx);
+  CT2G_TRY(ct2g_scan_exclusive(ctx, L->flags, L->scan, nr, L->d_cnt + 1, 0));
+  sel_list_kernel<<<G, T, 0, st>>>(L->d_cnt, L->sel, L->scan, L->sel_cells);
+  CT2G_LAUNCHED(ctx);
+  CT2G_CUDA(ctx, cudaMemsetAsync(L->pflag, 0, sizeof(uint32_t) * nr, st));
+  sink_flag_kernel<<<G, T, 0, st>>>(L->d_cnt, L->sel_cells, L->cells, ctx->cell_start, begin,
+                                    L->pflag);
+  CT2G_LAUNCHED(ctx);
+  CT2G_TRY(ct2g_scan_exclusive(ctx, L->pflag, L->pscan, nr, L->d_cnt + 4, 0));
+  sink_list_kernel<<<G, T, 0, st>>>(L->d_cnt, L->sel_cells, L->cells, ctx->cell_start, begin,
+                                    L->pscan, L->ssink, L->scell);
+  CT2G_LAUNCHED(ctx);
+  CT2G_CUDA(ctx, cudaMemsetAsync(L->cflag, 0, sizeof(uint32_t) * nr, st));
+  sink_chunk_flag_kernel<<<G, T, 0, st>>>(ctx->keys, ctx->cell_start, L->pflag, L->pscan, begin,
+                                          nr, L->cflag);
+  CT2G_LAUNCHED(ctx);
+  CT2G_TRY(ct2g_scan_exclusive(ctx, L->cflag, L->cscan, nr, L->d_cnt + 2, 0));
+  sink_chunk_fill_kernel<<<G, T, 0, st>>>(L->d_cnt, L->cflag, L->cscan, L->ssink, ctx->keys,
+                                          ctx->cell_start, L->pscan, begin, nr, L->chunks);
+  CT2G_LAUNCHED(ctx);
+  CT2G_CUDA(ctx, cudaMemsetAsync(L->d_cnt + 3, 0, sizeof(uint32_t), st));
+  shell_m2l_kernel<P><<<warp_grid(ctx, nr), 256, 0, st>>>(
+      L->d_cnt, L->sel_cells, L->cells, L->mc, L->idx, geo_of(ctx), L->d_shell, L->d_shellG,
+      L->nshell, L->lsub);
+  CT2G_LAUNCHED(ctx);
+  const float bw = ctx->opt.bwidth, bx = L->bw_ext;
+  CT2G_TRY(ct2g_near_window(ctx, L->chunks, L->d_cnt + 2, L->d_cnt + 3, L->ssink, L->d_stm,
+                            bw * bw, bx * bx, pot, fx, fy, fz, po));
+  if (pot)
+    shell_l2p_kernel<P, true><<<G, T, 0, st>>>(L->d_cnt, L->ssink, L->scell, ctx->keys, begin,
+                                                ctx->mbits, ctx->src, L->lsub, ctx->box_gm, fx, fy,
+                                                fz, po);
+  else
+    shell_l2p_kernel<P, false><<<G, T, 0, st>>>(L->d_cnt, L->ssink, L->scell, ctx->keys, begin,
+                                                 ctx->mbits, ctx->src, L->lsub, ctx->box_gm, fx, fy,
+                                                 fz, po);
+  CT2G_LAUNCHED(ctx);
+  return CT2G_OK;
+}
+
+// widen the direct sum of the selected cells (selection already made)
+int widen(ct2g_ctx *ctx, int mode, float thr, bool pot, float *fx, float *fy, float *fz,
+          float *po) {
+  ct2g_learn *L = ctx->learn;
+  CT2G_TRY(build_chunks(ctx, mode, thr, !L->d_stm));
+  if (!L->d_stm) return shell_correct(ctx, pot, fx, fy, fz, po);
+  switch (ctx->p) {
+    case 2: return widen_block_p<2>(ctx, pot, fx, fy, fz, po);
+    case 3: return widen_block_p<3>(ctx, pot, fx, fy, fz, po);
+    case 4: return widen_block_p<4>(ctx, pot, fx, fy, fz, po);
+    case 5: return widen_block_p<5>(ctx, pot, fx, fy, fz, po);
+    case 6: return widen_block_p<6>(ctx, pot, fx, fy, fz, po);
   }
   return ct2g_fail(ctx, CT2G_EINVAL, "unsupported order");
 }
@@ -830,7 +1090,7 @@ void ct2g_learned_free(ct2g_ctx *ctx) {
   ct2g_learn *L = ctx->learn;
   if (!L) return;
   free_learn_cells(L);
-  void *ptrs[] = {L->d_shell, L->d_shellG, L->d_cnt, L->params, L->grad, L->am, L->av, L->wbf,
+  void *ptrs[] = {L->d_shell, L->d_shellG, L->d_stm, L->idx, L->d_cnt, L->params, L->grad, L->am, L->av, L->wbf,
                   L->fmean, L->fstd, L->tX, L->tT, L->stash, L->sloss, L->tidx};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -848,8 +1108,7 @@ int ct2g_learned_apply(ct2g_ctx *ctx, bool pot) {
   if (L->mode == CT2G_SELECT_FIXED || L->mode == CT2G_SELECT_MLP)
     CT2G_TRY(features(ctx, ctx->fx, ctx->fy, ctx->fz));
   if (L->mode == CT2G_SELECT_MLP) CT2G_TRY(infer(ctx));
-  CT2G_TRY(build_chunks(ctx, L->mode, L->threshold));
-  return shell_correct(ctx, pot, ctx->fx, ctx->fy, ctx->fz, ctx->pot);
+  return widen(ctx, L->mode, L->threshold, pot, ctx->fx, ctx->fy, ctx->fz, ctx->pot);
 }
 
 extern "C" {
@@ -863,7 +1122,8 @@ int ct2g_learned_enable(ct2g_ctx *ctx, float bwidth_ext) {
   if (!ctx->learn) {
     ctx->learn = new ct2g_learn();
     ct2g_learn *L = ctx->learn;
-    CT2G_CUDA(ctx, cudaMalloc(&L->d_cnt, sizeof(uint32_t) * 4));
+    CT2G_CUDA(ctx, cudaMalloc(&L->d_cnt, sizeof(uint32_t) * 8));
+    CT2G_CUDA(ctx, cudaMemset(L->d_cnt, 0, sizeof(uint32_t) * 8));
     CT2G_CUDA(ctx, cudaMalloc(&L->params, sizeof(float) * NP));
     CT2G_CUDA(ctx, cudaMalloc(&L->grad, sizeof(float) * NP));
     CT2G_CUDA(ctx, cudaMalloc(&L->am, sizeof(float) * NP));
@@ -905,6 +1165,34 @@ int ct2g_learned_enable(ct2g_ctx *ctx, float bwidth_ext) {
   if (!offs.empty())
     CT2G_CUDA(ctx, cudaMemcpy(L->d_shell, o4.data(), sizeof(int) * o4.size(), cudaMemcpyHostToDevice));
   CT2G_TRY(ct2g_shell_greens(ctx, o3, L->d_shellG));
+  // shell cells of each neighbouring 4x4x4 block per in-block position (the
+  // block walk reaches 4 cells in every direction)
+  if (L->d_stm) cudaFree(L->d_stm);
+  L->d_stm = nullptr;
+  if (bwidth_ext <= 4.f) {
+    std::vector<unsigned long long> m(64 * 27, 0ull);
+    auto pos = [](int b, int &x, int &y, int &z) {
+      x = ((b >> 2) & 1) | ((b >> 4) & 2);
+      y = ((b >> 1) & 1) | ((b >> 3) & 2);
+      z = (b & 1) | ((b >> 2) & 2);
+    };
+    for (int p = 0; p < 64; p++) {
+      int px, py, pz;
+      pos(p, px, py, pz);
+      for (int o = 0; o < 27; o++)
+        for (int b = 0; b < 64; b++) {
+          int bx, by, bz;
+          pos(b, bx, by, bz);
+          const int ox = 4 * (o / 9 - 1) + bx - px, oy = 4 * ((o / 3) % 3 - 1) + by - py,
+                    oz = 4 * (o % 3 - 1) + bz - pz;
+          const double d2 = (double)(ox * ox + oy * oy + oz * oz);
+          if (d2 > b2 && d2 <= x2) m[p * 27 + o] |= 1ull << b;
+        }
+    }
+    CT2G_CUDA(ctx, cudaMalloc(&L->d_stm, sizeof(unsigned long long) * m.size()));
+    CT2G_CUDA(ctx, cudaMemcpy(L->d_stm, m.data(), sizeof(unsigned long long) * m.size(),
+                              cudaMemcpyHostToDevice));
+  }
   L->bw_ext = bwidth_ext;
   CT2G_TRY(learn_cells_alloc(ctx));
   ctx->epoch++;
@@ -948,8 +1236,7 @@ int ct2g_learned_collect(ct2g_ctx *ctx, size_t *ncells) {
   CT2G_CUDA(ctx, cudaMemcpyAsync(L->ex, ctx->fx, ctx->n * 4, cudaMemcpyDeviceToDevice, st));
   CT2G_CUDA(ctx, cudaMemcpyAsync(L->ey, ctx->fy, ctx->n * 4, cudaMemcpyDeviceToDevice, st));
   CT2G_CUDA(ctx, cudaMemcpyAsync(L->ez, ctx->fz, ctx->n * 4, cudaMemcpyDeviceToDevice, st));
-  CT2G_TRY(build_chunks(ctx, CT2G_SELECT_ALL, 0.f));
-  CT2G_TRY(shell_correct(ctx, false, L->ex, L->ey, L->ez, nullptr));
+  CT2G_TRY(widen(ctx, CT2G_SELECT_ALL, 0.f, false, L->ex, L->ey, L->ez, nullptr));
   // append (features, target) to the training set
   uint32_t nc = 0;
   CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->h_pinned, L->d_cnt, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));

@@ -123,7 +123,7 @@ __device__ __forceinline__ void near_chunk(
     const uint32_t *__restrict__ cs, const unsigned long long *__restrict__ occ,
     const unsigned long long *__restrict__ stmask, const Walk &walk,
     const uint32_t *__restrict__ skeys, uint32_t rbegin, const float4 *__restrict__ src,
-    int mbits, float soft, float bw2, const float *__restrict__ box_gm,
+    int mbits, float soft, float lo2, float bw2, const float *__restrict__ box_gm,
     float *__restrict__ ofx, float *__restrict__ ofy, float *__restrict__ ofz,
     float *__restrict__ opot, unsigned long long *__restrict__ inter, float4 *sb, int lane) {
   const int M = 1 << mbits;
@@ -185,7 +185,10 @@ __device__ __forceinline__ void near_chunk(
         inblock(32 * half + t, bx, by, bz);
         const int ox = dX + bx, oy = dY + by, oz = dZ + bz;  // cells, from this lane's cell
         bool in = act;
-        if (SPARSE) in = in && (float)(ox * ox + oy * oy + oz * oz) <= bw2;
+        if (SPARSE) {
+          const float d2 = (float)(ox * ox + oy * oy + oz * oz);
+          in = in && d2 > lo2 && d2 <= bw2;
+        }
         if (in) nsrc += j1 - j0;
         // sink position relative to the neighbour cell's centre
         const float xs = si.x - (float)ox * hc, ys = si.y - (float)oy * hc, zs = si.z - (float)oz * hc;
@@ -273,30 +276,33 @@ __device__ __forceinline__ void near_chunk(
   if (lane == 0 && c && inter) atomicAdd(inter, c);
 }
 
-// counts[0] dense chunks, counts[2] sparse chunks (stored after the dense
-// ones), counts[3] / counts[4] the work counters (zero at launch)
+// The chunk count is *nch_ptr, the chunks start at chunks + *off_ptr (none:
+// at chunks), warps take them from the work counter *work (zero at launch).
+// Sparse-style chunks (SPARSE) list sinks through slist and take only the
+// source cells with lo2 < |o|^2 <= bw2 of each lane's own cell; the stencil
+// masks stm must cover that window.
 template <int KERNEL, bool POT, bool SPARSE>
 __global__ void __launch_bounds__(256, 4) near_kernel(
-    const uint2 *__restrict__ chunks, uint32_t *__restrict__ counts,
+    const uint2 *__restrict__ chunks, const uint32_t *__restrict__ nch_ptr,
+    const uint32_t *__restrict__ off_ptr, uint32_t *__restrict__ work,
     const uint32_t *__restrict__ sparse_list, const uint32_t *__restrict__ cs,
     const unsigned long long *__restrict__ occ, const unsigned long long *__restrict__ stmask,
     Walk walk, const uint32_t *__restrict__ skeys, uint32_t rbegin,
-    const float4 *__restrict__ src, int mbits, float soft, float bw2,
+    const float4 *__restrict__ src, int mbits, float soft, float lo2, float bw2,
     const float *__restrict__ box_gm, float *__restrict__ ofx, float *__restrict__ ofy,
     float *__restrict__ ofz, float *__restrict__ opot, unsigned long long *__restrict__ inter) {
   __shared__ float4 sbuf[8][32];  // one batch of 32 sources per warp
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const uint32_t nch = SPARSE ? counts[2] : counts[0];
-  const uint2 *list = SPARSE ? chunks + counts[0] : chunks;
-  uint32_t *work = counts + (SPARSE ? 4 : 3);
+  const uint32_t nch = *nch_ptr;
+  const uint2 *list = off_ptr ? chunks + *off_ptr : chunks;
   for (;;) {
     uint32_t ch = 0;
     if (lane == 0) ch = atomicAdd(work, 1u);
     ch = __shfl_sync(0xffffffffu, ch, 0);
     if (ch >= nch) break;
     near_chunk<KERNEL, POT, SPARSE>(list[ch], sparse_list, cs, occ, stmask, walk, skeys, rbegin,
-                                    src, mbits, soft, bw2, box_gm, ofx, ofy, ofz, opot, inter,
-                                    sbuf[wib], lane);
+                                    src, mbits, soft, lo2, bw2, box_gm, ofx, ofy, ofz, opot,
+                                    inter, sbuf[wib], lane);
   }
 }
 
@@ -313,7 +319,10 @@ Walk make_walk(int mbits) {
 // persistent grid: the resident blocks of every SM (or the tuned count), and
 // no more than one block per 256 sinks of the range
 template <int K, bool POT, bool SPARSE>
-int launch_near1(ct2g_ctx *ctx, const Walk &walk, float bw2) {
+int launch_near1(ct2g_ctx *ctx, const Walk &walk, const uint2 *chunks, const uint32_t *nch,
+                 const uint32_t *off, uint32_t *work, const uint32_t *slist,
+                 const unsigned long long *stm, float lo2, float bw2, float *fx, float *fy,
+                 float *fz, float *pot, unsigned long long *inter) {
   auto k = near_kernel<K, POT, SPARSE>;
   int per_sm = 0;
   CT2G_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 256, 0));
@@ -322,22 +331,50 @@ int launch_near1(ct2g_ctx *ctx, const Walk &walk, float bw2) {
   size_t blocks = (size_t)std::max(1, per_sm) * ctx->num_sms;
   blocks = std::max<size_t>(1, std::min(blocks, (nr + 255) / 256));
   k<<<(unsigned)blocks, 256, 0, ctx->stream>>>(
-      ctx->chunks, ctx->d_counts, ctx->sparse_list, ctx->cell_start, ctx->occ, ctx->stmask, walk,
-      ctx->keys, (uint32_t)ctx->rung_begin, ctx->src, ctx->mbits, ctx->opt.hsoft, bw2,
-      ctx->box_gm, ctx->fx, ctx->fy, ctx->fz, ctx->pot, ctx->d_inter);
+      chunks, nch, off, work, slist, ctx->cell_start, ctx->occ, stm, walk, ctx->keys,
+      (uint32_t)ctx->rung_begin, ctx->src, ctx->mbits, ctx->opt.hsoft, lo2, bw2, ctx->box_gm, fx,
+      fy, fz, pot, inter);
   CT2G_LAUNCHED(ctx);
   return CT2G_OK;
 }
 
+// dense chunks (counts[0], work counter counts[3]), then sparse chunks
+// (counts[2], stored after the dense ones, work counter counts[4])
 template <int K, bool POT>
 int launch_near(ct2g_ctx *ctx) {
   const Walk walk = make_walk(ctx->mbits);
   const float bw2 = ctx->opt.bwidth * ctx->opt.bwidth;
-  CT2G_TRY((launch_near1<K, POT, false>(ctx, walk, bw2)));
-  return launch_near1<K, POT, true>(ctx, walk, bw2);
+  uint32_t *c = ctx->d_counts;
+  CT2G_TRY((launch_near1<K, POT, false>(ctx, walk, ctx->chunks, c + 0, nullptr, c + 3,
+                                        ctx->sparse_list, ctx->stmask, -1.f, bw2, ctx->fx,
+                                        ctx->fy, ctx->fz, ctx->pot, ctx->d_inter)));
+  return launch_near1<K, POT, true>(ctx, walk, ctx->chunks, c + 2, c + 0, c + 4,
+                                    ctx->sparse_list, ctx->stmask, -1.f, bw2, ctx->fx, ctx->fy,
+                                    ctx->fz, ctx->pot, ctx->d_inter);
 }
 
 }  // namespace
+
+// direct sum over a window lo2 < |o|^2 <= hi2 of cells for listed sinks
+// (sparse-style chunks), added into the given force buffers
+int ct2g_near_window(ct2g_ctx *ctx, const uint2 *chunks, const uint32_t *nch, uint32_t *work,
+                     const uint32_t *slist, const unsigned long long *stm, float lo2, float hi2,
+                     bool pot, float *fx, float *fy, float *fz, float *po) {
+  const Walk walk = make_walk(ctx->mbits);
+  if (ctx->opt.kernel == CT2G_SOFT_SPHERE)
+    return pot ? launch_near1<CT2G_SOFT_SPHERE, true, true>(ctx, walk, chunks, nch, nullptr, work,
+                                                            slist, stm, lo2, hi2, fx, fy, fz, po,
+                                                            nullptr)
+               : launch_near1<CT2G_SOFT_SPHERE, false, true>(ctx, walk, chunks, nch, nullptr,
+                                                             work, slist, stm, lo2, hi2, fx, fy,
+                                                             fz, po, nullptr);
+  return pot ? launch_near1<CT2G_SOFT_PLUMMER, true, true>(ctx, walk, chunks, nch, nullptr, work,
+                                                           slist, stm, lo2, hi2, fx, fy, fz, po,
+                                                           nullptr)
+             : launch_near1<CT2G_SOFT_PLUMMER, false, true>(ctx, walk, chunks, nch, nullptr, work,
+                                                            slist, stm, lo2, hi2, fx, fy, fz, po,
+                                                            nullptr);
+}
 
 int ct2g_upload_stencil(ct2g_ctx *ctx, const std::vector<int> &st4) {
   CT2G_CUDA(ctx, cudaMemcpyToSymbolAsync(c_stencil, st4.data(), sizeof(int) * st4.size(), 0,

@@ -39,8 +39,10 @@ def _cell_keys(d, mbits):
     return O.morton(d["x"] >> sh, d["y"] >> sh, d["z"] >> sh).astype(np.int64)
 
 
-def test_widened_cells_match_wider_method(gpu):
-    mbits, p, bw, bwx = 5, 3, 2.0, 3.0
+@pytest.mark.parametrize("bw,bwx", [(2.0, 3.0), (2.0, 5.0)])
+def test_widened_cells_match_wider_method(gpu, bw, bwx):
+    # bwidth_ext <= 4: block walk with shell stencil masks; beyond: cell walk
+    mbits, p = 5, 3
     P, g, soft, GM = _setup(mbits=mbits, p=p, bw=bw, bwx=bwx)
     base = O.method_forces(P["x"], P["y"], P["z"], mbits, p, 0, soft, bw, GM)
     wide = O.method_forces(P["x"], P["y"], P["z"], mbits, p, 0, soft, bwx, GM)
