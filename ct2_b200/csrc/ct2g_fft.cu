@@ -410,7 +410,7 @@ int launch_pipe(ct2g_ctx *ctx, C2 *spec, size_t nouter, size_t ostride, size_t r
                 size_t ncols) {
   const size_t smem = sizeof(C2) * ((size_t)N + 2 * (size_t)N * W);
   auto k = fft_cols_pipe_kernel<C2, N, W, INV>;
-  CT2G_CUDA(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CT2G_TRY(ct2g_smem_attrs(ctx, k, smem));
   int per_sm = 0;
   CT2G_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 256, smem));
   const int ntiles = (int)((ncols + W - 1) / W);
@@ -443,7 +443,7 @@ int launch_cols(ct2g_ctx *ctx, typename Cplx<T>::type *spec, size_t nouter, size
   }
   const size_t smem = sizeof(C2) * ((size_t)N + (size_t)N * W);
   auto k = fft_cols_kernel<C2, N, W, INV, VEC>;
-  CT2G_CUDA(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CT2G_TRY(ct2g_smem_attrs(ctx, k, smem));
   const int ntiles = (int)((ncols + W - 1) / W);
   k<<<(unsigned)(nouter * ntiles), 256, smem, ctx->stream>>>(spec, ostride, rstride, ncols, ntiles,
                                                              twiddle_ptr<C2>(ctx));
@@ -496,7 +496,7 @@ int fft_r2c_n(ct2g_ctx *ctx, const T *in, typename Cplx<T>::type *out, int batch
   const size_t smem = sizeof(C2) * ((size_t)N + (size_t)LP * LineLayout<N, true>::LS);
   const bool vec = ((size_t)ld * sizeof(C2)) % 16 == 0;
   auto kern = vec ? fftz_r2c_kernel<T, N, true> : fftz_r2c_kernel<T, N, false>;
-  CT2G_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CT2G_TRY(ct2g_smem_attrs(ctx, kern, smem));
   kern<<<ct2g_div_up(npairs, LP), 256, smem, ctx->stream>>>(in, out, npairs, LP, ld,
                                                             twiddle_ptr<C2>(ctx));
   CT2G_LAUNCHED(ctx);
@@ -512,7 +512,7 @@ int fft_c2r_n(ct2g_ctx *ctx, typename Cplx<T>::type *in, T *out, int batch, int 
   const size_t smem = sizeof(C2) * ((size_t)N + (size_t)LP * LineLayout<N, true>::LS);
   const bool vec = ((size_t)ld * sizeof(C2)) % 16 == 0;
   auto kern = vec ? fftz_c2r_kernel<T, N, true> : fftz_c2r_kernel<T, N, false>;
-  CT2G_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CT2G_TRY(ct2g_smem_attrs(ctx, kern, smem));
   kern<<<ct2g_div_up(npairs, LP), 256, smem, ctx->stream>>>(in, out, npairs, LP, ld,
                                                             twiddle_ptr<C2>(ctx));
   CT2G_LAUNCHED(ctx);
@@ -549,6 +549,148 @@ int fft_c2r(ct2g_ctx *ctx, typename Cplx<T>::type *in, T *out, int N, int batch,
     case 512: return fft_c2r_n<T, 512>(ctx, in, out, batch, ld);
   }
   return ct2g_fail(ctx, CT2G_EINVAL, "FFT size must be a power of two in [4, 512]");
+}
+
+// ---- forward z pass fused with P2M -----------------------------------------
+// One block per (x, y) line of one box: the moments of the line's N cells
+// (FP64 sums about the cell centres, as p2m_kernel) go straight into shared
+// memory as FP32, components paired into complex lines (2l -> .x, 2l+1 ->
+// .y), are transformed along z and split into the half spectra of the two
+// components.  The moment grid is never written to HBM.  A thread sums a
+// cell of up to kWarpCell particles; bigger cells are summed by a warp
+// (lanes stride over the particles, partial moments reduced by shuffles), so
+// no block waits on one thread's long loop.
+constexpr uint32_t kWarpCell = 32;
+
+template <int P>
+__device__ __forceinline__ void p2m_accumulate(const uint32_t *__restrict__ px,
+                                               const uint32_t *__restrict__ py,
+                                               const uint32_t *__restrict__ pz, uint32_t i,
+                                               uint32_t ux, uint32_t uy, uint32_t uz,
+                                               double *acc) {
+  constexpr MiTable<P> T{};
+  constexpr int NC = ct2g_ncomp(P);
+  const double sx = -(double)(int32_t)(px[i] - ux) * CT2G_TWO_M32;
+  const double sy = -(double)(int32_t)(py[i] - uy) * CT2G_TWO_M32;
+  const double sz = -(double)(int32_t)(pz[i] - uz) * CT2G_TWO_M32;
+  double qx[P + 1], qy[P + 1], qz[P + 1];
+  qx[0] = qy[0] = qz[0] = 1.0;
+#pragma unroll
+  for (int q = 1; q <= P; q++) {
+    qx[q] = qx[q - 1] * sx * (1.0 / q);
+    qy[q] = qy[q - 1] * sy * (1.0 / q);
+    qz[q] = qz[q - 1] * sz * (1.0 / q);
+  }
+#pragma unroll
+  for (int k = 0; k < NC; k++) acc[k] += qx[T.nx[k]] * qy[T.ny[k]] * qz[T.nz[k]];
+}
+
+template <int P, int N>
+__global__ void __launch_bounds__(256, 2) fftz_p2m_r2c_kernel(
+    const uint32_t *__restrict__ px, const uint32_t *__restrict__ py,
+    const uint32_t *__restrict__ pz, const uint32_t *__restrict__ cs, int mbits,
+    float2 *__restrict__ spec, int ld, int64_t CK, int64_t SK, const float2 *__restrict__ tw) {
+  using LL = LineLayout<N, true>;
+  constexpr int NC = ct2g_ncomp(P), NL = (NC + 1) / 2, NH = N / 2 + 1;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  float2 *stw = reinterpret_cast<float2 *>(smraw);
+  float2 *s = stw + N;
+  float *sr = reinterpret_cast<float *>(s);
+  __shared__ uint32_t big[N], nbig;
+  if (threadIdx.x == 0) nbig = 0;
+  load_twiddles(stw, tw, N);
+  __syncthreads();
+  const size_t line = blockIdx.x % ((size_t)N * N);
+  const uint32_t box = (uint32_t)(blockIdx.x / ((size_t)N * N));
+  const uint32_t cx = (uint32_t)(line / N), cy = (uint32_t)(line % N);
+  const int sh = 32 - mbits;
+  const uint32_t halfc = 1u << (sh - 1);
+  const uint32_t ux = (cx << sh) + halfc, uy = (cy << sh) + halfc;
+  for (int zc = threadIdx.x; zc < N; zc += 256) {
+    const uint32_t key = (box << (3 * mbits)) | ct2g_morton(cx, cy, (uint32_t)zc);
+    const uint32_t b = cs[key], e = cs[key + 1];
+    if (e - b > kWarpCell) {
+      big[atomicAdd(&nbig, 1u)] = (uint32_t)zc;
+      continue;
+    }
+    const uint32_t uz = ((uint32_t)zc << sh) + halfc;
+    double acc[NC];
+#pragma unroll
+    for (int k = 0; k < NC; k++) acc[k] = 0.0;
+    for (uint32_t i = b; i < e; i++) p2m_accumulate<P>(px, py, pz, i, ux, uy, uz, acc);
+#pragma unroll
+    for (int k = 0; k < NC; k++) sr[2 * LL::at(k >> 1, zc, 0) + (k & 1)] = (float)acc[k];
+    if (NC & 1) sr[2 * LL::at(NL - 1, zc, 0) + 1] = 0.f;
+  }
+  __syncthreads();
+  {  // the big cells, a warp each
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (uint32_t q = warp; q < nbig; q += 8) {
+      const uint32_t zc = big[q];
+      const uint32_t key = (box << (3 * mbits)) | ct2g_morton(cx, cy, zc);
+      const uint32_t b = cs[key], e = cs[key + 1];
+      const uint32_t uz = (zc << sh) + halfc;
+      double acc[NC];
+#pragma unroll
+      for (int k = 0; k < NC; k++) acc[k] = 0.0;
+      for (uint32_t i = b + lane; i < e; i += 32) p2m_accumulate<P>(px, py, pz, i, ux, uy, uz, acc);
+#pragma unroll
+      for (int k = 0; k < NC; k++) {
+        double v = acc[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        acc[k] = v;
+      }
+      if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < NC; k++) sr[2 * LL::at(k >> 1, (int)zc, 0) + (k & 1)] = (float)acc[k];
+        if (NC & 1) sr[2 * LL::at(NL - 1, (int)zc, 0) + 1] = 0.f;
+      }
+    }
+  }
+  __syncthreads();
+  tile_fft<N, true, float2, false>(s, NL, 0, stw);
+  float2 *base = spec + (int64_t)box * CK + line * (size_t)ld;
+  for (int c = threadIdx.x; c < NL * ld; c += 256) {
+    const int l = c / ld, k = c % ld;
+    float2 a = make_float2(0.f, 0.f), bb = make_float2(0.f, 0.f);
+    if (k < NH) {
+      const float2 zk = s[LL::at(l, k & (N - 1), 0)];
+      const float2 zn = s[LL::at(l, (N - k) & (N - 1), 0)];
+      // A_k = (Z_k + conj Z_{N-k})/2, B_k = (Z_k - conj Z_{N-k})/(2i)
+      a = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
+      bb = make_float2(0.5f * (zk.y + zn.y), 0.5f * (zn.x - zk.x));
+    }
+    base[(int64_t)(2 * l) * SK + k] = a;
+    if (2 * l + 1 < NC) base[(int64_t)(2 * l + 1) * SK + k] = bb;
+  }
+}
+
+template <int P, int N>
+int launch_p2m_r2c(ct2g_ctx *ctx) {
+  constexpr int NL = (ct2g_ncomp(P) + 1) / 2;
+  const size_t smem = sizeof(float2) * ((size_t)N + (size_t)NL * LineLayout<N, true>::LS);
+  auto k = fftz_p2m_r2c_kernel<P, N>;
+  CT2G_TRY(ct2g_smem_attrs(ctx, k, smem));
+  k<<<(unsigned)((size_t)N * N * ctx->nbox), 256, smem, ctx->stream>>>(
+      ctx->x, ctx->y, ctx->z, ctx->cell_start, ctx->mbits, ctx->spec, ctx->ldk, ctx->CK,
+      ctx->CK * ctx->nbox, twiddle_ptr<float2>(ctx));
+  CT2G_LAUNCHED(ctx);
+  return run_cols<float, N>(ctx, ctx->spec, ctx->nc * ctx->nbox, false, ctx->ldk);
+}
+
+template <int P>
+int p2m_r2c_p(ct2g_ctx *ctx) {
+  switch (ctx->M) {
+    case 8: return launch_p2m_r2c<P, 8>(ctx);
+    case 16: return launch_p2m_r2c<P, 16>(ctx);
+    case 32: return launch_p2m_r2c<P, 32>(ctx);
+    case 64: return launch_p2m_r2c<P, 64>(ctx);
+    case 128: return launch_p2m_r2c<P, 128>(ctx);
+    case 256: return launch_p2m_r2c<P, 256>(ctx);
+    case 512: return launch_p2m_r2c<P, 512>(ctx);
+  }
+  return ct2g_fail(ctx, CT2G_EINVAL, "mesh must be a power of two in [8, 512]");
 }
 
 // ---- inverse z pass fused with L2P ------------------------------------------
@@ -621,7 +763,7 @@ int launch_c2r_l2p(ct2g_ctx *ctx, bool pot) {
   constexpr int NL = (ct2g_ncomp(P) + 1) / 2;
   const size_t smem = sizeof(float2) * ((size_t)N + (size_t)NL * LineLayout<N, true>::LS);
   auto k = pot ? fftz_c2r_l2p_kernel<P, N, true> : fftz_c2r_l2p_kernel<P, N, false>;
-  CT2G_CUDA(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CT2G_TRY(ct2g_smem_attrs(ctx, k, smem));
   k<<<(unsigned)((size_t)N * N * ctx->nbox), 256, smem, ctx->stream>>>(
       ctx->spec, ctx->ldk, ctx->CK, ctx->CK * ctx->nbox, ctx->cell_start, ctx->src, ctx->mbits,
       ctx->box_gm, ctx->fx, ctx->fy, ctx->fz, ctx->pot, twiddle_ptr<float2>(ctx));
@@ -700,6 +842,20 @@ int ct2g_fft_r2c_f64(ct2g_ctx *ctx, const double *in, double2 *out, int N, int b
 }
 int ct2g_fft_c2r_f64(ct2g_ctx *ctx, double2 *in, double *out, int N, int batch, int ld) {
   return fft_c2r<double>(ctx, in, out, N, batch, ld);
+}
+
+// moments and forward transform in one: z pass fused with P2M, then Y and X
+int ct2g_fft_p2m_r2c(ct2g_ctx *ctx) {
+  CT2G_TRY(ct2g_twiddles(ctx, ctx->M));
+  switch (ctx->p) {
+    case 1: return p2m_r2c_p<1>(ctx);
+    case 2: return p2m_r2c_p<2>(ctx);
+    case 3: return p2m_r2c_p<3>(ctx);
+    case 4: return p2m_r2c_p<4>(ctx);
+    case 5: return p2m_r2c_p<5>(ctx);
+    case 6: return p2m_r2c_p<6>(ctx);
+  }
+  return ct2g_fail(ctx, CT2G_EINVAL, "unsupported order");
 }
 
 // inverse transform of the expansions (Y and X passes, then z fused with L2P)

@@ -333,7 +333,13 @@ int ct2g_p2m(ct2g_ctx *ctx);
 // mesh solve; fused_l2p: the inverse z pass evaluates the far field of every
 // particle of the current range straight into the force buffers (the
 // expansion grid is not written)
-int ct2g_mesh_solve(ct2g_ctx *ctx, bool fused_l2p, bool pot);
+// fused_p2m: the moments are computed inside the forward z pass (the grid
+// is not written; ctx->grid then holds no moments)
+int ct2g_mesh_solve(ct2g_ctx *ctx, bool fused_l2p, bool pot, bool fused_p2m = false);
+// forward z pass fused with P2M, then the Y and X passes (ct2g_fft.cu)
+int ct2g_fft_p2m_r2c(ct2g_ctx *ctx);
+// the learned correction will run on the next force computation
+bool ct2g_learned_active(const ct2g_ctx *ctx);
 // inverse z pass fused with L2P (ct2g_fft.cu)
 int ct2g_fft_c2r_l2p(ct2g_ctx *ctx, bool pot);
 // forces of the current range; pot: also the potential (diagnostics)
@@ -350,3 +356,13 @@ int ct2g_fft_r2c_f64(ct2g_ctx *ctx, const double *in, double2 *out, int N, int b
 int ct2g_fft_c2r_f64(ct2g_ctx *ctx, double2 *in, double *out, int N, int batch, int ld);
 
 static inline unsigned ct2g_div_up(size_t a, size_t b) { return (unsigned)((a + b - 1) / b); }
+
+// a kernel's dynamic shared memory, with all of the unified L1 offered as
+// shared memory so that the occupancy the launch sizes assume is reachable
+template <typename K>
+int ct2g_smem_attrs(ct2g_ctx *ctx, K kernel, size_t smem) {
+  CT2G_CUDA(ctx, cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CT2G_CUDA(ctx, cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                      (int)cudaSharedmemCarveoutMaxShared));
+  return CT2G_OK;
+}

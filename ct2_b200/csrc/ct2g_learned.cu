@@ -892,8 +892,7 @@ int infer(ct2g_ctx *ctx) {
   ct2g_learn *L = ctx->learn;
   const size_t nr = ctx->n - ctx->rung_begin;
   const size_t smem = sizeof(float) * NP;
-  CT2G_CUDA(ctx, cudaFuncSetAttribute(mlp_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem));
+  CT2G_TRY(ct2g_smem_attrs(ctx, mlp_infer_kernel, smem));
   const unsigned blocks = (unsigned)std::max<size_t>(
       1, std::min<size_t>((nr + 255) / 256, (size_t)ctx->num_sms * 4));
   mlp_infer_kernel<<<blocks, 256, smem, ctx->stream>>>(L->wbf, L->fmean, L->fstd, L->X, L->d_cnt,
@@ -1056,8 +1055,7 @@ int mlp_batch(ct2g_ctx *ctx, const float *X, const float *T, const uint32_t *idx
   ct2g_learn *L = ctx->learn;
   cudaStream_t st = ctx->stream;
   const size_t smem = sizeof(float) * NP;
-  CT2G_CUDA(ctx, cudaFuncSetAttribute(mlp_fwdbwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem));
+  CT2G_TRY(ct2g_smem_attrs(ctx, mlp_fwdbwd_kernel, smem));
   mlp_fwdbwd_kernel<<<ct2g_div_up(count, 128), 128, smem, st>>>(
       L->wbf, L->fmean, L->fstd, X, T, idx, start, count, L->stash, L->sloss);
   CT2G_LAUNCHED(ctx);
@@ -1080,6 +1078,10 @@ int mlp_batch(ct2g_ctx *ctx, const float *X, const float *T, const uint32_t *idx
 }
 
 }  // namespace
+
+bool ct2g_learned_active(const ct2g_ctx *ctx) {
+  return ctx->learn && ctx->learn->mode != CT2G_SELECT_NONE;
+}
 
 int ct2g_learned_resize(ct2g_ctx *ctx) {
   if (!ctx->learn) return CT2G_OK;
@@ -1221,7 +1223,13 @@ int ct2g_learned_collect(ct2g_ctx *ctx, size_t *ncells) {
   CT2G_TRY(learn_cells_alloc(ctx));
   const size_t nr = ctx->n - ctx->rung_begin;
   cudaStream_t st = ctx->stream;
-  // plain forces
+  // plain forces; the moment grid is formed first (the features and the
+  // shell's Taylor term read it), so the far field does not fuse P2M away
+  if (!ctx->moments_valid) {
+    CT2G_TRY(ct2g_p2m(ctx));
+    ctx->moments_valid = true;
+    ctx->expansions_valid = false;
+  }
   const int mode = L->mode;
   L->mode = CT2G_SELECT_NONE;
   int rc = ct2g_far_field(ctx, false);

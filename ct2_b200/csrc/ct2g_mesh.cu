@@ -494,10 +494,13 @@ int ct2g_p2m(ct2g_ctx *ctx) {
 
 // forward FFT of the moment grids, MG2L, inverse FFT into the expansions
 // (which overwrite the moments in ctx->grid)
-int ct2g_mesh_solve(ct2g_ctx *ctx, bool fused_l2p, bool pot) {
+int ct2g_mesh_solve(ct2g_ctx *ctx, bool fused_l2p, bool pot, bool fused_p2m) {
   CT2G_TRY(ct2g_build_greens(ctx));
   ct2g_mark(ctx, 2);
-  CT2G_TRY(ct2g_fft_r2c_f32(ctx, ctx->grid, ctx->spec, ctx->M, ctx->nc * ctx->nbox, ctx->ldk));
+  if (fused_p2m)
+    CT2G_TRY(ct2g_fft_p2m_r2c(ctx));
+  else
+    CT2G_TRY(ct2g_fft_r2c_f32(ctx, ctx->grid, ctx->spec, ctx->M, ctx->nc * ctx->nbox, ctx->ldk));
   ct2g_mark(ctx, 3);
   switch (ctx->p) {
     case 1: CT2G_TRY(launch_mg2l<1>(ctx)); break;

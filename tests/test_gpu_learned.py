@@ -92,7 +92,11 @@ def test_features_match_oracle(gpu):
     g.learned_select("fixed", 1e30)  # features and scores, nothing selected
     g.compute_forces()
     f1, _ = g.forces()
-    assert np.array_equal(f0, f1)
+    # with the correction on, P2M runs as its own pass (the features read the
+    # moment grid) instead of inside the forward z pass: same sums, different
+    # FP32 pairing in the transform
+    rel = np.linalg.norm(f1 - f0, axis=1) / np.linalg.norm(f0, axis=1)
+    assert rel.max() < 1e-5
     c = g.learned_cells()
     assert c["nselected"] == 0
     M = 1 << mbits
