@@ -160,6 +160,9 @@ __device__ __forceinline__ void near_chunk(
   // packed accumulators of the Plummer path (+d g and +1/r per pair half)
   f32x2 pax = 0ull, pay = 0ull, paz = 0ull, pap = 0ull;
   const f32x2 H2 = f2_pack(h2, h2);
+  // dense chunks: the sink in its own cell's frame (sources are shifted there)
+  const f32x2 SX = f2_pack(si.x, si.x), SY = f2_pack(si.y, si.y), SZ = f2_pack(si.z, si.z);
+  const f32x2 ONE = f2_pack(1.f, 1.f);
   uint32_t nsrc = 0;
   for (int o = 0; o < 27; o++) {
     const unsigned long long bits = __shfl_sync(0xffffffffu, word, o);
@@ -176,6 +179,65 @@ __device__ __forceinline__ void near_chunk(
         const uint32_t ck = (nb << 6) | (uint32_t)(32 * half + lane);
         jb = cs[ck];
         je = cs[ck + 1];
+      }
+      if constexpr (KERNEL == CT2G_SOFT_PLUMMER && !SPARSE) {
+        // Every candidate cell is in the stencil of every lane: the cells'
+        // sources form one stream (lane order), staged in full batches of 32,
+        // each source shifted into the sink cell's frame.
+        const uint32_t c = je - jb;
+        uint32_t incl = c;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+          const uint32_t t = __shfl_up_sync(0xffffffffu, incl, d);
+          if (lane >= d) incl += t;
+        }
+        const uint32_t excl = incl - c;
+        const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+        if (act) nsrc += total;
+        // source g of the stream, in the sink cell's frame
+        auto fetch = [&](uint32_t g) {
+          const uint32_t gg = min(g, total - 1);
+          int t = 0;  // owner: the last lane whose stream offset is <= gg
+#pragma unroll
+          for (int step = 16; step > 0; step >>= 1) {
+            const uint32_t e = __shfl_sync(0xffffffffu, excl, t + step);
+            if (e <= gg) t += step;
+          }
+          const uint32_t j = __shfl_sync(0xffffffffu, jb, t) + (gg - __shfl_sync(0xffffffffu, excl, t));
+          int bx, by, bz;
+          inblock(32 * half + t, bx, by, bz);
+          const float4 q = __ldg(src + j);
+          return make_float3(fmaf((float)(dX + bx), hc, q.x), fmaf((float)(dY + by), hc, q.y),
+                             fmaf((float)(dZ + bz), hc, q.z));
+        };
+        float *sbf = reinterpret_cast<float *>(sb);
+        const int rec = 4 * (lane >> 1) + (lane & 1);
+        float3 nq = fetch((uint32_t)lane);
+        for (uint32_t b0 = 0; b0 < total; b0 += 32) {
+          const int cnt = (int)min(32u, total - b0);
+          __syncwarp();
+          sbf[rec] = nq.x;
+          sbf[rec + 2] = nq.y;
+          sbf[64 + 2 * (lane >> 1) + (lane & 1)] = nq.z;
+          __syncwarp();
+          if (b0 + 32 < total) nq = fetch(b0 + 32 + (uint32_t)lane);
+          if (cnt == 32) {
+#pragma unroll 8
+            for (int pr = 0; pr < 16; pr++)
+              plummer_pair<POT, false>(sbf, pr, SX, SY, SZ, H2, ONE, pax, pay, paz, pap);
+          } else {
+#pragma unroll 2
+            for (int pr = 0; pr < (cnt >> 1); pr++)
+              plummer_pair<POT, false>(sbf, pr, SX, SY, SZ, H2, ONE, pax, pay, paz, pap);
+            if (cnt & 1) {  // the odd last source
+              const int pr = cnt >> 1;
+              const float qx = sbf[4 * pr], qy = sbf[4 * pr + 2], qz = sbf[64 + 2 * pr];
+              ct2g_pair_term<KERNEL, POT>(si.x - qx, si.y - qy, si.z - qz, h2, hinv, hinv3, nx,
+                                          ny, nz, np, true);
+            }
+          }
+        }
+        continue;
       }
       while (hb) {
         const int t = __ffs(hb) - 1;
