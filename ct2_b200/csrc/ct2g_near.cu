@@ -203,7 +203,9 @@ __device__ __forceinline__ void near_chunk(
             const uint32_t e = __shfl_sync(0xffffffffu, excl, t + step);
             if (e <= gg) t += step;
           }
-          const uint32_t j = __shfl_sync(0xffffffffu, jb, t) + (gg - __shfl_sync(0xffffffffu, excl, t));
+          const uint32_t jt = __shfl_sync(0xffffffffu, jb, t), et = __shfl_sync(0xffffffffu, je, t);
+          // j < et by the scan; the clamp keeps the load inside the owner cell regardless
+          const uint32_t j = min(jt + (gg - __shfl_sync(0xffffffffu, excl, t)), max(et, 1u) - 1u);
           int bx, by, bz;
           inblock(32 * half + t, bx, by, bz);
           const float4 q = __ldg(src + j);
