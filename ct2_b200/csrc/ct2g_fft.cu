@@ -737,24 +737,51 @@ __global__ void __launch_bounds__(256) fftz_c2r_l2p_kernel(
     s[LL::at(l, k, 0)] = make_float2(a.x - b.y, a.y + b.x);
   }
   __syncthreads();
+  // offsets of the cells' particles in the line's particle list (inclusive
+  // scan of the counts, off[0] = 0), built while nothing else needs the SM
+  constexpr int ZT = (N + 255) / 256;  // cells per thread
+  __shared__ uint32_t off[N + 1];
+  for (int z = threadIdx.x; z < N; z += 256) off[z + 1] = ce[z] - cb[z];
+  if (threadIdx.x == 0) off[0] = 0;
   tile_fft<N, true, float2, true>(s, NL, 0, stw);
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  for (int z = w; z < N; z += 8) {
-    const uint32_t b0 = cb[z], b1 = ce[z];
-    if (b0 == b1) continue;
+  __syncthreads();
+  for (int d = 1; d < N; d <<= 1) {
+    uint32_t add[ZT];
+#pragma unroll
+    for (int q = 0; q < ZT; q++) {
+      const int z = threadIdx.x + 256 * q;
+      add[q] = (z < N && z >= d) ? off[z + 1 - d] : 0u;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < ZT; q++) {
+      const int z = threadIdx.x + 256 * q;
+      if (z < N) off[z + 1] += add[q];
+    }
+    __syncthreads();
+  }
+  // every particle of the line, one per thread: its cell is the last z with
+  // off[z] <= q (that cell holds it: off[z] <= q < off[z + 1])
+  const uint32_t total = off[N];
+  for (uint32_t q = threadIdx.x; q < total; q += 256) {
+    int lo = 0, hi = N;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (off[mid] <= q) lo = mid; else hi = mid;
+    }
+    const int z = lo;
+    const uint32_t i = cb[z] + (q - off[z]);
     const auto acc = [&](int k) {
       const float2 v = s[LL::at(k >> 1, z, 0)];
       return (k & 1) ? v.y : v.x;
     };
-    for (uint32_t i = b0 + lane; i < b1; i += 32) {
-      const float4 t = src[i];
-      float fx, fy, fz, ph;
-      ct2g_l2p<P>(acc, t.x, t.y, t.z, fx, fy, fz, ph);
-      ofx[i] = GM * fx;
-      ofy[i] = GM * fy;
-      ofz[i] = GM * fz;
-      if (POT) opot[i] = GM * ph;
-    }
+    const float4 t = src[i];
+    float fx, fy, fz, ph;
+    ct2g_l2p<P>(acc, t.x, t.y, t.z, fx, fy, fz, ph);
+    ofx[i] = GM * fx;
+    ofy[i] = GM * fy;
+    ofz[i] = GM * fz;
+    if (POT) opot[i] = GM * ph;
   }
 }
 
