@@ -812,8 +812,14 @@ def main():
         sms = torch.cuda.get_device_properties(local).multi_processor_count
         peak = sms * 128 * 2 * peaks["sm_max_mhz"] * 1e6 / 1e12
         ach = flops / (st[k] * 1e-3) / 1e12
+        # DRAM bytes of the two near-field launches of one step, from the ncu
+        # capture summarised in profiles/near_kernel_128cubed_mesh256_bw4_ncu_full.md
+        # (default workload only)
+        default = (args.ngrid, args.mesh, args.bwidth, args.nspheres) == (128, 256, 4.0, 512)
         roof = {"kernel": "forces (direct sum)", "bound": "fp32", "achieved": ach, "peak": peak,
-                "unit": "TFLOP/s", "frac": ach / peak, "traffic": None,
+                "unit": "TFLOP/s", "frac": ach / peak,
+                "traffic": (44.171e6 + 0.504e6 + 116.976e6 + 11.257e6) if default else None,
+                "traffic_unit": "bytes per step (dense + sparse launch)",
                 "peak_source": "derived: SMs x 128 x 2 x max SM clock (no measured FP32 peak)"}
     else:
         ach = algo_bytes[dom] / (st[k] * 1e-3) / 1e9
