@@ -26,7 +26,8 @@ class Options(ctypes.Structure):
 
 class Tuning(ctypes.Structure):
     _fields_ = [("dense_cell", ctypes.c_int), ("near_blocks_per_sm", ctypes.c_int),
-                ("fft_tile", ctypes.c_int), ("reserved", ctypes.c_int * 5)]
+                ("fft_tile", ctypes.c_int), ("split_mg2l", ctypes.c_int),
+                ("reserved", ctypes.c_int * 4)]
 
 
 STEP_GRAPH = 1

@@ -224,6 +224,7 @@ int ct2g_alloc_mesh(ct2g_ctx *ctx) {
   CT2G_CUDA(ctx, cudaMalloc(&ctx->box_off, sizeof(uint32_t) * (nb + 1)));
   CT2G_CUDA(ctx, cudaMalloc(&ctx->box_gm, sizeof(float) * nb));
   CT2G_CUDA(ctx, cudaMalloc(&ctx->greens, sizeof(float) * ctx->nc * ctx->CK));
+  CT2G_CUDA(ctx, cudaMalloc(&ctx->greens_x, sizeof(float) * ct2g_greens_x_floats(ctx)));
   return CT2G_OK;
 }
 
@@ -371,7 +372,7 @@ int ct2g_destroy(ct2g_ctx *ctx) {
   if (ctx->self_batch) ct2g_batch_destroy(ctx->self_batch);
   ct2g_learned_free(ctx);
   void *ptrs[] = {ctx->cell_start, ctx->occ, ctx->stmask, ctx->grid, ctx->spec, ctx->greens,
-                  ctx->tw32, ctx->tw64, ctx->d_counts, ctx->box_off, ctx->box_gm, ctx->tc_tables,
+                  ctx->greens_x,                  ctx->tw32, ctx->tw64, ctx->d_counts, ctx->box_off, ctx->box_gm, ctx->tc_tables,
                   ctx->d_maxrung, ctx->d_inter, ctx->scan_tmp};
   for (void *p : ptrs)
     if (p) cudaFree(p);

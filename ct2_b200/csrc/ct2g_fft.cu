@@ -101,13 +101,15 @@ __device__ __forceinline__ void reg_dft(C2 (&v)[R]) {
 }
 
 // Line FFTs on smem lines.  Layout ROWS: element (l, r) at
-// l*(N + N/R1) + r + r/R1 (one pad every R1 points); layout COLS: element
+// l*(N + N/R1 + 1) + r + r/R1 (one pad every R1 points); layout COLS: element
 // (l, r) at r*W + l.
 template <int N, bool ROWS>
 struct LineLayout {
   static constexpr int R2 = N >= 4 ? (1 << (ilog2c(N) / 2)) : 1;
   static constexpr int R1 = N / R2;  // R1 >= R2
-  static constexpr int LS = N + N / R1;
+  // odd in complex units, so that the same point of consecutive lines falls
+  // in different banks
+  static constexpr int LS = N + N / R1 + 1;
   __device__ __forceinline__ static int at(int l, int r, int W) {
     return ROWS ? l * LS + r + r / R1 : r * W + l;
   }
@@ -551,6 +553,14 @@ int fft_c2r(ct2g_ctx *ctx, typename Cplx<T>::type *in, T *out, int N, int batch,
   return ct2g_fail(ctx, CT2G_EINVAL, "FFT size must be a power of two in [4, 512]");
 }
 
+// ---- the mesh solve's spectrum ------------------------------------------------
+// ctx->spec keeps the NC components of a k-point side by side,
+// [box][qi][qj][qk][NC] with qk < ldk, so that a (qi, qj) row is RS = ldk*NC
+// complex values (16-byte aligned rows: ldk is even; slots qk > N/2 hold
+// zeros).  The z passes write and read whole rows; the Y pass transforms tiles
+// of W contiguous (qk, c) columns; the X pass runs inside the MG2L kernel,
+// whose block holds every component of one (qj, qk) column.
+
 // ---- forward z pass fused with P2M -----------------------------------------
 // One block per (x, y) line of one box: the moments of the line's N cells
 // (FP64 sums about the cell centres, as p2m_kernel) go straight into shared
@@ -559,7 +569,8 @@ int fft_c2r(ct2g_ctx *ctx, typename Cplx<T>::type *in, T *out, int N, int batch,
 // components.  The moment grid is never written to HBM.  A thread sums a
 // cell of up to kWarpCell particles; bigger cells are summed by a warp
 // (lanes stride over the particles, partial moments reduced by shuffles), so
-// no block waits on one thread's long loop.
+// no block waits on one thread's long loop.  GRID: the moments are read from
+// the moment grid (component k of box b at grid + (k * nbox + b) * N^3).
 constexpr uint32_t kWarpCell = 32;
 
 template <int P>
@@ -585,74 +596,86 @@ __device__ __forceinline__ void p2m_accumulate(const uint32_t *__restrict__ px,
   for (int k = 0; k < NC; k++) acc[k] += qx[T.nx[k]] * qy[T.ny[k]] * qz[T.nz[k]];
 }
 
-template <int P, int N>
+template <int P, int N, bool GRID>
 __global__ void __launch_bounds__(256, 2) fftz_p2m_r2c_kernel(
     const uint32_t *__restrict__ px, const uint32_t *__restrict__ py,
     const uint32_t *__restrict__ pz, const uint32_t *__restrict__ cs, int mbits,
-    float2 *__restrict__ spec, int ld, int64_t CK, int64_t SK, const float2 *__restrict__ tw) {
+    const float *__restrict__ grid, int64_t CB, float2 *__restrict__ spec, int ldk,
+    const float2 *__restrict__ tw) {
   using LL = LineLayout<N, true>;
   constexpr int NC = ct2g_ncomp(P), NL = (NC + 1) / 2, NH = N / 2 + 1;
   extern __shared__ __align__(16) unsigned char smraw[];
   float2 *stw = reinterpret_cast<float2 *>(smraw);
   float2 *s = stw + N;
   float *sr = reinterpret_cast<float *>(s);
-  __shared__ uint32_t big[N], nbig;
+  __shared__ uint32_t big[GRID ? 1 : N], nbig;
   if (threadIdx.x == 0) nbig = 0;
   load_twiddles(stw, tw, N);
   __syncthreads();
   const size_t line = blockIdx.x % ((size_t)N * N);
   const uint32_t box = (uint32_t)(blockIdx.x / ((size_t)N * N));
-  const uint32_t cx = (uint32_t)(line / N), cy = (uint32_t)(line % N);
-  const int sh = 32 - mbits;
-  const uint32_t halfc = 1u << (sh - 1);
-  const uint32_t ux = (cx << sh) + halfc, uy = (cy << sh) + halfc;
-  for (int zc = threadIdx.x; zc < N; zc += 256) {
-    const uint32_t key = (box << (3 * mbits)) | ct2g_morton(cx, cy, (uint32_t)zc);
-    const uint32_t b = cs[key], e = cs[key + 1];
-    if (e - b > kWarpCell) {
-      big[atomicAdd(&nbig, 1u)] = (uint32_t)zc;
-      continue;
+  if constexpr (GRID) {
+    const float *g = grid + ((int64_t)box * N * N + (int64_t)line) * N;
+    for (int e = threadIdx.x; e < NC * N; e += 256) {
+      const int k = e / N, z = e % N;
+      sr[2 * LL::at(k >> 1, z, 0) + (k & 1)] = g[(int64_t)k * CB + z];
     }
-    const uint32_t uz = ((uint32_t)zc << sh) + halfc;
-    double acc[NC];
-#pragma unroll
-    for (int k = 0; k < NC; k++) acc[k] = 0.0;
-    for (uint32_t i = b; i < e; i++) p2m_accumulate<P>(px, py, pz, i, ux, uy, uz, acc);
-#pragma unroll
-    for (int k = 0; k < NC; k++) sr[2 * LL::at(k >> 1, zc, 0) + (k & 1)] = (float)acc[k];
-    if (NC & 1) sr[2 * LL::at(NL - 1, zc, 0) + 1] = 0.f;
-  }
-  __syncthreads();
-  {  // the big cells, a warp each
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (uint32_t q = warp; q < nbig; q += 8) {
-      const uint32_t zc = big[q];
-      const uint32_t key = (box << (3 * mbits)) | ct2g_morton(cx, cy, zc);
+    if (NC & 1)
+      for (int z = threadIdx.x; z < N; z += 256) sr[2 * LL::at(NL - 1, z, 0) + 1] = 0.f;
+  } else {
+    const uint32_t cx = (uint32_t)(line / N), cy = (uint32_t)(line % N);
+    const int sh = 32 - mbits;
+    const uint32_t halfc = 1u << (sh - 1);
+    const uint32_t ux = (cx << sh) + halfc, uy = (cy << sh) + halfc;
+    for (int zc = threadIdx.x; zc < N; zc += 256) {
+      const uint32_t key = (box << (3 * mbits)) | ct2g_morton(cx, cy, (uint32_t)zc);
       const uint32_t b = cs[key], e = cs[key + 1];
-      const uint32_t uz = (zc << sh) + halfc;
+      if (e - b > kWarpCell) {
+        big[atomicAdd(&nbig, 1u)] = (uint32_t)zc;
+        continue;
+      }
+      const uint32_t uz = ((uint32_t)zc << sh) + halfc;
       double acc[NC];
 #pragma unroll
       for (int k = 0; k < NC; k++) acc[k] = 0.0;
-      for (uint32_t i = b + lane; i < e; i += 32) p2m_accumulate<P>(px, py, pz, i, ux, uy, uz, acc);
+      for (uint32_t i = b; i < e; i++) p2m_accumulate<P>(px, py, pz, i, ux, uy, uz, acc);
 #pragma unroll
-      for (int k = 0; k < NC; k++) {
-        double v = acc[k];
+      for (int k = 0; k < NC; k++) sr[2 * LL::at(k >> 1, zc, 0) + (k & 1)] = (float)acc[k];
+      if (NC & 1) sr[2 * LL::at(NL - 1, zc, 0) + 1] = 0.f;
+    }
+    __syncthreads();
+    {  // the big cells, a warp each
+      const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+      for (uint32_t q = warp; q < nbig; q += 8) {
+        const uint32_t zc = big[q];
+        const uint32_t key = (box << (3 * mbits)) | ct2g_morton(cx, cy, zc);
+        const uint32_t b = cs[key], e = cs[key + 1];
+        const uint32_t uz = (zc << sh) + halfc;
+        double acc[NC];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        acc[k] = v;
-      }
-      if (lane == 0) {
+        for (int k = 0; k < NC; k++) acc[k] = 0.0;
+        for (uint32_t i = b + lane; i < e; i += 32) p2m_accumulate<P>(px, py, pz, i, ux, uy, uz, acc);
 #pragma unroll
-        for (int k = 0; k < NC; k++) sr[2 * LL::at(k >> 1, (int)zc, 0) + (k & 1)] = (float)acc[k];
-        if (NC & 1) sr[2 * LL::at(NL - 1, (int)zc, 0) + 1] = 0.f;
+        for (int k = 0; k < NC; k++) {
+          double v = acc[k];
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+          acc[k] = v;
+        }
+        if (lane == 0) {
+#pragma unroll
+          for (int k = 0; k < NC; k++) sr[2 * LL::at(k >> 1, (int)zc, 0) + (k & 1)] = (float)acc[k];
+          if (NC & 1) sr[2 * LL::at(NL - 1, (int)zc, 0) + 1] = 0.f;
+        }
       }
     }
   }
   __syncthreads();
   tile_fft<N, true, float2, false>(s, NL, 0, stw);
-  float2 *base = spec + (int64_t)box * CK + line * (size_t)ld;
-  for (int c = threadIdx.x; c < NL * ld; c += 256) {
-    const int l = c / ld, k = c % ld;
+  // row blockIdx.x = box * N^2 + line; k-point k's components at k * NC
+  float2 *row = spec + (int64_t)blockIdx.x * ((int64_t)ldk * NC);
+  for (int e = threadIdx.x; e < ldk * NL; e += 256) {
+    const int k = e / NL, l = e - k * NL;
     float2 a = make_float2(0.f, 0.f), bb = make_float2(0.f, 0.f);
     if (k < NH) {
       const float2 zk = s[LL::at(l, k & (N - 1), 0)];
@@ -661,36 +684,22 @@ __global__ void __launch_bounds__(256, 2) fftz_p2m_r2c_kernel(
       a = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
       bb = make_float2(0.5f * (zk.y + zn.y), 0.5f * (zn.x - zk.x));
     }
-    base[(int64_t)(2 * l) * SK + k] = a;
-    if (2 * l + 1 < NC) base[(int64_t)(2 * l + 1) * SK + k] = bb;
+    row[k * NC + 2 * l] = a;
+    if (2 * l + 1 < NC) row[k * NC + 2 * l + 1] = bb;
   }
 }
 
 template <int P, int N>
-int launch_p2m_r2c(ct2g_ctx *ctx) {
+int launch_p2m_r2c(ct2g_ctx *ctx, bool from_grid) {
   constexpr int NL = (ct2g_ncomp(P) + 1) / 2;
   const size_t smem = sizeof(float2) * ((size_t)N + (size_t)NL * LineLayout<N, true>::LS);
-  auto k = fftz_p2m_r2c_kernel<P, N>;
+  auto k = from_grid ? fftz_p2m_r2c_kernel<P, N, true> : fftz_p2m_r2c_kernel<P, N, false>;
   CT2G_TRY(ct2g_smem_attrs(ctx, k, smem));
   k<<<(unsigned)((size_t)N * N * ctx->nbox), 256, smem, ctx->stream>>>(
-      ctx->x, ctx->y, ctx->z, ctx->cell_start, ctx->mbits, ctx->spec, ctx->ldk, ctx->CK,
-      ctx->CK * ctx->nbox, twiddle_ptr<float2>(ctx));
+      ctx->x, ctx->y, ctx->z, ctx->cell_start, ctx->mbits, ctx->grid, ctx->CB, ctx->spec,
+      ctx->ldk, twiddle_ptr<float2>(ctx));
   CT2G_LAUNCHED(ctx);
-  return run_cols<float, N>(ctx, ctx->spec, ctx->nc * ctx->nbox, false, ctx->ldk);
-}
-
-template <int P>
-int p2m_r2c_p(ct2g_ctx *ctx) {
-  switch (ctx->M) {
-    case 8: return launch_p2m_r2c<P, 8>(ctx);
-    case 16: return launch_p2m_r2c<P, 16>(ctx);
-    case 32: return launch_p2m_r2c<P, 32>(ctx);
-    case 64: return launch_p2m_r2c<P, 64>(ctx);
-    case 128: return launch_p2m_r2c<P, 128>(ctx);
-    case 256: return launch_p2m_r2c<P, 256>(ctx);
-    case 512: return launch_p2m_r2c<P, 512>(ctx);
-  }
-  return ct2g_fail(ctx, CT2G_EINVAL, "mesh must be a power of two in [8, 512]");
+  return CT2G_OK;
 }
 
 // ---- inverse z pass fused with L2P ------------------------------------------
@@ -699,117 +708,279 @@ int p2m_r2c_p(ct2g_ctx *ctx) {
 // in shared memory, and the block then evaluates the far field of every
 // particle of the line's cells from the expansions in shared memory.  The
 // expansion grid itself is never written to HBM.  Block b is line b % N^2
-// of box b / N^2; component k of box q starts at spec + (k * nbox + q) * CK.
-template <int P, int N, bool POT>
+// of box b / N^2.  MODE 0: forces, 1: forces and potentials, 2: no L2P, the
+// expansions go to the expansion grid (layout as the moment grid).
+template <int P, int N, int MODE>
 __global__ void __launch_bounds__(256) fftz_c2r_l2p_kernel(
-    const float2 *__restrict__ spec, int ld, int64_t CK, int64_t SK,
-    const uint32_t *__restrict__ cs, const float4 *__restrict__ src, int mbits,
-    const float *__restrict__ box_gm, float *__restrict__ ofx, float *__restrict__ ofy,
-    float *__restrict__ ofz, float *__restrict__ opot, const float2 *__restrict__ tw) {
+    const float2 *__restrict__ spec, int ldk, const uint32_t *__restrict__ cs,
+    const float4 *__restrict__ src, int mbits, const float *__restrict__ box_gm,
+    float *__restrict__ ofx, float *__restrict__ ofy, float *__restrict__ ofz,
+    float *__restrict__ opot, float *__restrict__ grid, int64_t CB,
+    const float2 *__restrict__ tw) {
   using LL = LineLayout<N, true>;
   constexpr int NC = ct2g_ncomp(P), NL = (NC + 1) / 2, NH = N / 2 + 1;
+  constexpr bool L2P = MODE < 2;
   extern __shared__ __align__(16) unsigned char smraw[];
   float2 *stw = reinterpret_cast<float2 *>(smraw);
   float2 *s = stw + N;
-  __shared__ uint32_t cb[N + 1], ce[N];  // particle ranges of the line's cells
+  __shared__ uint32_t cb[L2P ? N + 1 : 1], ce[L2P ? N : 1];  // particle ranges of the line's cells
   load_twiddles(stw, tw, N);
   const size_t line = blockIdx.x % ((size_t)N * N);
   const uint32_t box = (uint32_t)(blockIdx.x / ((size_t)N * N));
   const uint32_t x = (uint32_t)(line / N), y = (uint32_t)(line % N);
-  // issue the range loads first: their latency hides behind the transform
-  for (int z = threadIdx.x; z < N; z += 256) {
-    const uint32_t key = (box << (3 * mbits)) | ct2g_morton(x, y, (uint32_t)z);
-    cb[z] = cs[key];
-    ce[z] = cs[key + 1];
-  }
-  const float GM = __ldg(box_gm + box);
-  const float2 *base = spec + (int64_t)box * CK + line * (size_t)ld;
-  for (int e = threadIdx.x; e < NL * N; e += 256) {
-    const int l = e / N, k = e % N;
-    const bool up = k >= NH;
-    const int kk = up ? N - k : k;
-    float2 a = base[(int64_t)(2 * l) * SK + kk];
-    float2 b = (2 * l + 1 < NC) ? base[(int64_t)(2 * l + 1) * SK + kk] : make_float2(0.f, 0.f);
-    if (up) {
-      a.y = -a.y;
-      b.y = -b.y;
+  if constexpr (L2P) {
+    // issue the range loads first: their latency hides behind the transform
+    for (int z = threadIdx.x; z < N; z += 256) {
+      const uint32_t key = (box << (3 * mbits)) | ct2g_morton(x, y, (uint32_t)z);
+      cb[z] = cs[key];
+      ce[z] = cs[key + 1];
     }
+  }
+  const float2 *row = spec + (int64_t)blockIdx.x * ((int64_t)ldk * NC);
+  for (int e = threadIdx.x; e < NH * NL; e += 256) {
+    const int k = e / NL, l = e - k * NL;
+    const float2 a = row[k * NC + 2 * l];
+    const float2 b = (2 * l + 1 < NC) ? row[k * NC + 2 * l + 1] : make_float2(0.f, 0.f);
+    // Z_k = A_k + i B_k; Z_{N-k} = conj(A_k) + i conj(B_k)
     s[LL::at(l, k, 0)] = make_float2(a.x - b.y, a.y + b.x);
+    if (k > 0 && k < N / 2) s[LL::at(l, N - k, 0)] = make_float2(a.x + b.y, b.x - a.y);
   }
   __syncthreads();
-  // offsets of the cells' particles in the line's particle list (inclusive
-  // scan of the counts, off[0] = 0), built while nothing else needs the SM
-  constexpr int ZT = (N + 255) / 256;  // cells per thread
-  __shared__ uint32_t off[N + 1];
-  for (int z = threadIdx.x; z < N; z += 256) off[z + 1] = ce[z] - cb[z];
-  if (threadIdx.x == 0) off[0] = 0;
-  tile_fft<N, true, float2, true>(s, NL, 0, stw);
-  __syncthreads();
-  for (int d = 1; d < N; d <<= 1) {
-    uint32_t add[ZT];
-#pragma unroll
-    for (int q = 0; q < ZT; q++) {
-      const int z = threadIdx.x + 256 * q;
-      add[q] = (z < N && z >= d) ? off[z + 1 - d] : 0u;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int q = 0; q < ZT; q++) {
-      const int z = threadIdx.x + 256 * q;
-      if (z < N) off[z + 1] += add[q];
-    }
-    __syncthreads();
-  }
-  // every particle of the line, one per thread: its cell is the last z with
-  // off[z] <= q (that cell holds it: off[z] <= q < off[z + 1])
-  const uint32_t total = off[N];
-  for (uint32_t q = threadIdx.x; q < total; q += 256) {
-    int lo = 0, hi = N;
-    while (hi - lo > 1) {
-      const int mid = (lo + hi) >> 1;
-      if (off[mid] <= q) lo = mid; else hi = mid;
-    }
-    const int z = lo;
-    const uint32_t i = cb[z] + (q - off[z]);
-    const auto acc = [&](int k) {
+  if constexpr (!L2P) {
+    tile_fft<N, true, float2, true>(s, NL, 0, stw);
+    float *g = grid + ((int64_t)box * N * N + (int64_t)line) * N;
+    for (int e = threadIdx.x; e < NC * N; e += 256) {
+      const int k = e / N, z = e % N;
       const float2 v = s[LL::at(k >> 1, z, 0)];
-      return (k & 1) ? v.y : v.x;
-    };
-    const float4 t = src[i];
-    float fx, fy, fz, ph;
-    ct2g_l2p<P>(acc, t.x, t.y, t.z, fx, fy, fz, ph);
-    ofx[i] = GM * fx;
-    ofy[i] = GM * fy;
-    ofz[i] = GM * fz;
-    if (POT) opot[i] = GM * ph;
+      g[(int64_t)k * CB + z] = (k & 1) ? v.y : v.x;
+    }
+    return;
+  } else {
+    // offsets of the cells' particles in the line's particle list (inclusive
+    // scan of the counts, off[0] = 0), built while nothing else needs the SM
+    constexpr int ZT = (N + 255) / 256;  // cells per thread
+    __shared__ uint32_t off[N + 1];
+    for (int z = threadIdx.x; z < N; z += 256) off[z + 1] = ce[z] - cb[z];
+    if (threadIdx.x == 0) off[0] = 0;
+    tile_fft<N, true, float2, true>(s, NL, 0, stw);
+    __syncthreads();
+    for (int d = 1; d < N; d <<= 1) {
+      uint32_t add[ZT];
+#pragma unroll
+      for (int q = 0; q < ZT; q++) {
+        const int z = threadIdx.x + 256 * q;
+        add[q] = (z < N && z >= d) ? off[z + 1 - d] : 0u;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int q = 0; q < ZT; q++) {
+        const int z = threadIdx.x + 256 * q;
+        if (z < N) off[z + 1] += add[q];
+      }
+      __syncthreads();
+    }
+    // every particle of the line, one per thread: its cell is the last z with
+    // off[z] <= q (that cell holds it: off[z] <= q < off[z + 1])
+    const float GM = __ldg(box_gm + box);
+    const uint32_t total = off[N];
+    for (uint32_t q = threadIdx.x; q < total; q += 256) {
+      int lo = 0, hi = N;
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (off[mid] <= q) lo = mid; else hi = mid;
+      }
+      const int z = lo;
+      const uint32_t i = cb[z] + (q - off[z]);
+      const auto acc = [&](int k) {
+        const float2 v = s[LL::at(k >> 1, z, 0)];
+        return (k & 1) ? v.y : v.x;
+      };
+      const float4 t = src[i];
+      float fx, fy, fz, ph;
+      ct2g_l2p<P>(acc, t.x, t.y, t.z, fx, fy, fz, ph);
+      ofx[i] = GM * fx;
+      ofy[i] = GM * fy;
+      ofz[i] = GM * fz;
+      if (MODE == 1) opot[i] = GM * ph;
+    }
   }
 }
 
 template <int P, int N>
-int launch_c2r_l2p(ct2g_ctx *ctx, bool pot) {
+int launch_c2r_l2p(ct2g_ctx *ctx, int mode) {
   constexpr int NL = (ct2g_ncomp(P) + 1) / 2;
   const size_t smem = sizeof(float2) * ((size_t)N + (size_t)NL * LineLayout<N, true>::LS);
-  auto k = pot ? fftz_c2r_l2p_kernel<P, N, true> : fftz_c2r_l2p_kernel<P, N, false>;
+  auto k = mode == 0 ? fftz_c2r_l2p_kernel<P, N, 0>
+           : mode == 1 ? fftz_c2r_l2p_kernel<P, N, 1> : fftz_c2r_l2p_kernel<P, N, 2>;
   CT2G_TRY(ct2g_smem_attrs(ctx, k, smem));
   k<<<(unsigned)((size_t)N * N * ctx->nbox), 256, smem, ctx->stream>>>(
-      ctx->spec, ctx->ldk, ctx->CK, ctx->CK * ctx->nbox, ctx->cell_start, ctx->src, ctx->mbits,
-      ctx->box_gm, ctx->fx, ctx->fy, ctx->fz, ctx->pot, twiddle_ptr<float2>(ctx));
+      ctx->spec, ctx->ldk, ctx->cell_start, ctx->src, ctx->mbits, ctx->box_gm, ctx->fx, ctx->fy,
+      ctx->fz, ctx->pot, ctx->grid, ctx->CB, twiddle_ptr<float2>(ctx));
   CT2G_LAUNCHED(ctx);
   return CT2G_OK;
 }
 
+// ---- X pass + MG2L + inverse X pass ------------------------------------------
+// One block per spectrum column (box, qj, qk): the column's N k-points with all
+// NC components, s[qi * NC + c], are transformed along x, contracted with the
+// Green's tensor (L_a = sum_b G_{a+b} M_b, src/particle.cpp:244-250) and
+// transformed back, so neither the transformed moments nor the expansions
+// make a round trip through HBM between the three steps.  The column's
+// moments and its Green's values ([c][qi], one contiguous run of the
+// column-ordered table) arrive by cp.async.
+template <int P, int N>
+struct FxShape {
+  static constexpr int NC = ct2g_ncomp(P), NH = N / 2 + 1;
+  static constexpr int GCOL = NC * N;  // floats per Green's column (a multiple of 8)
+  static constexpr size_t SMEM =
+      sizeof(float2) * (size_t)N + sizeof(float2) * (size_t)N * NC + sizeof(float) * (size_t)GCOL;
+  static constexpr bool FITS = SMEM <= 227 * 1024;
+  static constexpr int MINB = SMEM <= 112 * 1024 ? 2 : 1;
+  static constexpr bool GREG = NC <= 35;  // Green's values in registers
+};
+
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+
+template <int P, int N>
+__global__ void __launch_bounds__(256, FxShape<P, N>::MINB) fftx_mg2l_kernel(
+    float2 *__restrict__ spec, int ldk, const float *__restrict__ gx,
+    const float2 *__restrict__ tw) {
+  using S = FxShape<P, N>;
+  constexpr int NC = S::NC, NH = S::NH;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  float2 *stw = reinterpret_cast<float2 *>(smraw);
+  float2 *s = stw + N;
+  float *sg = reinterpret_cast<float *>(s + N * NC);
+  const int qk = (int)(blockIdx.x % NH);
+  const int qj = (int)((blockIdx.x / NH) % N);
+  const int box = (int)(blockIdx.x / ((unsigned)NH * N));
+  const int64_t RS = (int64_t)ldk * NC, XS = (int64_t)N * RS;
+  float2 *col = spec + (int64_t)box * N * XS + (int64_t)qj * RS + (int64_t)qk * NC;
+  for (int e = threadIdx.x; e < N * NC; e += 256) {
+    const int x = e / NC, c = e - x * NC;
+    cp_async8(s + e, col + x * XS + c);
+  }
+  const float *gcol = gx + ((int64_t)qj * NH + qk) * S::GCOL;
+  for (int e = threadIdx.x; e < S::GCOL / 4; e += 256) cp_async16(sg + 4 * e, gcol + 4 * e);
+  cp_async_commit();
+  load_twiddles(stw, tw, N);
+  cp_async_wait<0>();
+  __syncthreads();
+  tile_fft<N, false, float2, false>(s, NC, NC, stw);
+  for (int qi = threadIdx.x; qi < N; qi += 256) {
+    float2 m[NC];
+#pragma unroll
+    for (int k = 0; k < NC; k++) m[k] = s[qi * NC + k];
+    if constexpr (S::GREG) {
+      float g[NC];
+#pragma unroll
+      for (int k = 0; k < NC; k++) g[k] = sg[k * N + qi];
+      ct2g_mg2l_all<P, 1>(m, g, s + qi * NC, std::make_integer_sequence<int, Mg2lPairs<P>::NP>{});
+    } else {
+      ct2g_mg2l_all<P, N>(m, sg + qi, s + qi * NC,
+                          std::make_integer_sequence<int, Mg2lPairs<P>::NP>{});
+    }
+  }
+  __syncthreads();
+  tile_fft<N, false, float2, true>(s, NC, NC, stw);
+  for (int e = threadIdx.x; e < N * NC; e += 256) {
+    const int x = e / NC, c = e - x * NC;
+    col[x * XS + c] = s[e];
+  }
+}
+
+template <int P, int N>
+int launch_fx_mg2l(ct2g_ctx *ctx) {
+  using S = FxShape<P, N>;
+  if constexpr (!S::FITS) {
+    return ct2g_fail(ctx, CT2G_EINVAL, "fused X pass + MG2L does not fit in shared memory");
+  } else {
+    auto k = fftx_mg2l_kernel<P, N>;
+    CT2G_TRY(ct2g_smem_attrs(ctx, k, S::SMEM));
+    k<<<(unsigned)((size_t)ctx->nbox * N * S::NH), 256, S::SMEM, ctx->stream>>>(
+        ctx->spec, ctx->ldk, ctx->greens_x, twiddle_ptr<float2>(ctx));
+    CT2G_LAUNCHED(ctx);
+    return CT2G_OK;
+  }
+}
+
+// the Y pass (tiles of the (qk, c) columns of each (box, qi) plane) or the
+// split X pass (tiles of the (qj, qk, c) columns of each box)
+template <int N>
+int spec_cols(ct2g_ctx *ctx, bool inv, bool xpass) {
+  const size_t RS = (size_t)ctx->ldk * ctx->nc, nb = (size_t)ctx->nbox;
+  size_t nouter, ostride, rstride, ncols;
+  if (!xpass) {
+    nouter = nb * N;
+    ostride = (size_t)N * RS;
+    rstride = RS;
+    ncols = (size_t)(N / 2 + 1) * ctx->nc;
+  } else {
+    nouter = nb;
+    ostride = (size_t)N * N * RS;
+    rstride = (size_t)N * RS;
+    ncols = (size_t)N * RS;
+  }
+  if constexpr (N == 256 || N == 512) {
+    if (ctx->fft_tc)
+      return ct2g_fft_cols_tc(ctx, ctx->spec, N, nouter, ostride, rstride, ncols, inv);
+  }
+  if (inv) return launch_cols<float, N, true, true>(ctx, ctx->spec, nouter, ostride, rstride, ncols);
+  return launch_cols<float, N, false, true>(ctx, ctx->spec, nouter, ostride, rstride, ncols);
+}
+
 template <int P>
-int c2r_l2p_p(ct2g_ctx *ctx, bool pot) {
+bool fx_fits(int N) {
+  switch (N) {
+    case 8: return FxShape<P, 8>::FITS;
+    case 16: return FxShape<P, 16>::FITS;
+    case 32: return FxShape<P, 32>::FITS;
+    case 64: return FxShape<P, 64>::FITS;
+    case 128: return FxShape<P, 128>::FITS;
+    case 256: return FxShape<P, 256>::FITS;
+    case 512: return FxShape<P, 512>::FITS;
+  }
+  return false;
+}
+
+// order x mesh dispatch of the mesh-solve kernels
+template <int P>
+int spec_stage(ct2g_ctx *ctx, int stage, bool flag, int mode) {
   switch (ctx->M) {
-    case 8: return launch_c2r_l2p<P, 8>(ctx, pot);
-    case 16: return launch_c2r_l2p<P, 16>(ctx, pot);
-    case 32: return launch_c2r_l2p<P, 32>(ctx, pot);
-    case 64: return launch_c2r_l2p<P, 64>(ctx, pot);
-    case 128: return launch_c2r_l2p<P, 128>(ctx, pot);
-    case 256: return launch_c2r_l2p<P, 256>(ctx, pot);
-    case 512: return launch_c2r_l2p<P, 512>(ctx, pot);
+#define CT2G_SPEC_CASE(NN)                                                  \
+  case NN:                                                                  \
+    if (stage == 0) return launch_p2m_r2c<P, NN>(ctx, flag);                \
+    if (stage == 1) return launch_fx_mg2l<P, NN>(ctx);                      \
+    if (stage == 2) return launch_c2r_l2p<P, NN>(ctx, mode);                \
+    return spec_cols<NN>(ctx, flag, mode != 0);
+    CT2G_SPEC_CASE(8)
+    CT2G_SPEC_CASE(16)
+    CT2G_SPEC_CASE(32)
+    CT2G_SPEC_CASE(64)
+    CT2G_SPEC_CASE(128)
+    CT2G_SPEC_CASE(256)
+    CT2G_SPEC_CASE(512)
+#undef CT2G_SPEC_CASE
   }
   return ct2g_fail(ctx, CT2G_EINVAL, "mesh must be a power of two in [8, 512]");
+}
+
+// stage 0: z pass (flag: from the moment grid); 1: fused X + MG2L; 2: inverse
+// z pass (mode 0/1/2 as fftz_c2r_l2p_kernel); 3: Y pass (mode 0) or X pass
+// (mode 1), inverse when flag
+int spec_run(ct2g_ctx *ctx, int stage, bool flag, int mode) {
+  switch (ctx->p) {
+    case 1: return spec_stage<1>(ctx, stage, flag, mode);
+    case 2: return spec_stage<2>(ctx, stage, flag, mode);
+    case 3: return spec_stage<3>(ctx, stage, flag, mode);
+    case 4: return spec_stage<4>(ctx, stage, flag, mode);
+    case 5: return spec_stage<5>(ctx, stage, flag, mode);
+    case 6: return spec_stage<6>(ctx, stage, flag, mode);
+  }
+  return ct2g_fail(ctx, CT2G_EINVAL, "unsupported order");
 }
 
 }  // namespace
@@ -871,40 +1042,38 @@ int ct2g_fft_c2r_f64(ct2g_ctx *ctx, double2 *in, double *out, int N, int batch, 
   return fft_c2r<double>(ctx, in, out, N, batch, ld);
 }
 
-// moments and forward transform in one: z pass fused with P2M, then Y and X
-int ct2g_fft_p2m_r2c(ct2g_ctx *ctx) {
-  CT2G_TRY(ct2g_twiddles(ctx, ctx->M));
+bool ct2g_mg2l_fused(const ct2g_ctx *ctx) {
+  if (ctx->fft_tc || ctx->split_mg2l || !ctx->greens_x) return false;
   switch (ctx->p) {
-    case 1: return p2m_r2c_p<1>(ctx);
-    case 2: return p2m_r2c_p<2>(ctx);
-    case 3: return p2m_r2c_p<3>(ctx);
-    case 4: return p2m_r2c_p<4>(ctx);
-    case 5: return p2m_r2c_p<5>(ctx);
-    case 6: return p2m_r2c_p<6>(ctx);
+    case 1: return fx_fits<1>(ctx->M);
+    case 2: return fx_fits<2>(ctx->M);
+    case 3: return fx_fits<3>(ctx->M);
+    case 4: return fx_fits<4>(ctx->M);
+    case 5: return fx_fits<5>(ctx->M);
+    case 6: return fx_fits<6>(ctx->M);
   }
-  return ct2g_fail(ctx, CT2G_EINVAL, "unsupported order");
+  return false;
 }
 
-// inverse transform of the expansions (Y and X passes, then z fused with L2P)
-int ct2g_fft_c2r_l2p(ct2g_ctx *ctx, bool pot) {
+// z pass (P2M inside it, or from the moment grid), Y pass, X pass when split
+int ct2g_spec_forward(ct2g_ctx *ctx, bool p2m) {
   CT2G_TRY(ct2g_twiddles(ctx, ctx->M));
-  switch (ctx->M) {
-    case 8: CT2G_TRY((run_cols<float, 8>(ctx, ctx->spec, ctx->nc * ctx->nbox, true, ctx->ldk))); break;
-    case 16: CT2G_TRY((run_cols<float, 16>(ctx, ctx->spec, ctx->nc * ctx->nbox, true, ctx->ldk))); break;
-    case 32: CT2G_TRY((run_cols<float, 32>(ctx, ctx->spec, ctx->nc * ctx->nbox, true, ctx->ldk))); break;
-    case 64: CT2G_TRY((run_cols<float, 64>(ctx, ctx->spec, ctx->nc * ctx->nbox, true, ctx->ldk))); break;
-    case 128: CT2G_TRY((run_cols<float, 128>(ctx, ctx->spec, ctx->nc * ctx->nbox, true, ctx->ldk))); break;
-    case 256: CT2G_TRY((run_cols<float, 256>(ctx, ctx->spec, ctx->nc * ctx->nbox, true, ctx->ldk))); break;
-    case 512: CT2G_TRY((run_cols<float, 512>(ctx, ctx->spec, ctx->nc * ctx->nbox, true, ctx->ldk))); break;
-    default: return ct2g_fail(ctx, CT2G_EINVAL, "mesh must be a power of two in [8, 512]");
-  }
-  switch (ctx->p) {
-    case 1: return c2r_l2p_p<1>(ctx, pot);
-    case 2: return c2r_l2p_p<2>(ctx, pot);
-    case 3: return c2r_l2p_p<3>(ctx, pot);
-    case 4: return c2r_l2p_p<4>(ctx, pot);
-    case 5: return c2r_l2p_p<5>(ctx, pot);
-    case 6: return c2r_l2p_p<6>(ctx, pot);
-  }
-  return ct2g_fail(ctx, CT2G_EINVAL, "unsupported order");
+  CT2G_TRY(spec_run(ctx, 0, !p2m, 0));
+  CT2G_TRY(spec_run(ctx, 3, false, 0));
+  if (!ct2g_mg2l_fused(ctx)) CT2G_TRY(spec_run(ctx, 3, false, 1));
+  return CT2G_OK;
+}
+
+int ct2g_spec_mg2l(ct2g_ctx *ctx) {
+  if (ct2g_mg2l_fused(ctx)) return spec_run(ctx, 1, false, 0);
+  return ct2g_mg2l_split(ctx);
+}
+
+// inverse X pass when split, Y pass, z pass (L2P inside it, or into the
+// expansion grid)
+int ct2g_spec_inverse(ct2g_ctx *ctx, bool l2p, bool pot) {
+  CT2G_TRY(ct2g_twiddles(ctx, ctx->M));
+  if (!ct2g_mg2l_fused(ctx)) CT2G_TRY(spec_run(ctx, 3, true, 1));
+  CT2G_TRY(spec_run(ctx, 3, true, 0));
+  return spec_run(ctx, 2, false, l2p ? (pot ? 1 : 0) : 2);
 }

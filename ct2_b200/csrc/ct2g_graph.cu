@@ -339,17 +339,20 @@ int ct2g_get_tuning(const ct2g_ctx *ctx, ct2g_tuning *t) {
   t->dense_cell = (int)ctx->dense_cell;
   t->near_blocks_per_sm = ctx->near_blocks_per_sm;
   t->fft_tile = ctx->fft_tile;
+  t->split_mg2l = ctx->split_mg2l;
   return CT2G_OK;
 }
 
 int ct2g_set_tuning(ct2g_ctx *ctx, const ct2g_tuning *t) {
   if (!ctx || !t) return CT2G_EINVAL;
   if (t->dense_cell < 1 || t->dense_cell > 4096 || t->near_blocks_per_sm < 0 ||
-      t->near_blocks_per_sm > 32 || t->fft_tile < 0 || t->fft_tile > 512)
+      t->near_blocks_per_sm > 32 || t->fft_tile < 0 || t->fft_tile > 512 ||
+      (t->split_mg2l != 0 && t->split_mg2l != 1))
     return ct2g_fail(ctx, CT2G_EINVAL, "tuning out of range");
   ctx->dense_cell = (uint32_t)t->dense_cell;
   ctx->near_blocks_per_sm = t->near_blocks_per_sm;
   ctx->fft_tile = t->fft_tile;
+  ctx->split_mg2l = t->split_mg2l;
   ctx->epoch++;  // launch shapes are part of a recorded graph
   ctx->grid_valid = false;  // the chunk lists depend on dense_cell
   return CT2G_OK;

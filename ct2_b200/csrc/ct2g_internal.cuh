@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <cmath>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/ct2g.h"
@@ -170,6 +171,36 @@ struct Mg2lTab {
   static constexpr Mg2lPairs<P> t{};
 };
 
+// One (a, b) term of L_a = sum_b G_{a+b} M_b (src/particle.cpp:244-250).
+// G_n is real for even |n| and i*g for odd |n| (parity of D^n phi); g[n * GS]
+// is that real factor.  Every index is a compile-time constant, so m[], a
+// register g[] and acc stay in registers; L_a goes to out[a].
+template <int P, int GS, int I>
+__device__ __forceinline__ void ct2g_mg2l_term(const float2 *m, const float *g, float2 &acc,
+                                               float2 *out) {
+  constexpr int A = Mg2lTab<P>::t.a[I], B = Mg2lTab<P>::t.b[I], AB = Mg2lTab<P>::t.ab[I];
+  constexpr bool FIRST = Mg2lTab<P>::t.first[I] != 0, LAST = Mg2lTab<P>::t.last[I] != 0,
+                 ODD = Mg2lTab<P>::t.odd[I] != 0;
+  if constexpr (FIRST) acc = make_float2(0.f, 0.f);
+  const float gv = g[AB * GS];
+  const float2 mb = m[B];
+  if constexpr (!ODD) {
+    acc.x = fmaf(gv, mb.x, acc.x);
+    acc.y = fmaf(gv, mb.y, acc.y);
+  } else {  // i*g*(mx + i my) = (-g my, g mx)
+    acc.x = fmaf(-gv, mb.y, acc.x);
+    acc.y = fmaf(gv, mb.x, acc.y);
+  }
+  if constexpr (LAST) out[A] = acc;
+}
+
+template <int P, int GS, int... I>
+__device__ __forceinline__ void ct2g_mg2l_all(const float2 *m, const float *g, float2 *out,
+                                              std::integer_sequence<int, I...>) {
+  float2 acc = make_float2(0.f, 0.f);
+  (ct2g_mg2l_term<P, GS, I>(m, g, acc, out), ...);
+}
+
 // ---------------------------------------------------------------------------
 // Context
 // ---------------------------------------------------------------------------
@@ -222,6 +253,7 @@ struct ct2g_ctx {
   uint32_t dense_cell = 16;  // cells with at least this many particles get their own chunks
   int near_blocks_per_sm = 0;  // persistent near-field grid: blocks per SM (0: occupancy)
   int fft_tile = 0;            // y/x FFT pass tile width (0: default)
+  int split_mg2l = 0;          // 1: X passes and MG2L as three launches, not one
   struct ct2g_batch *self_batch = nullptr;  // graph of ct2g_kick_drift
   struct ct2g_learn *learn = nullptr;       // learned near-field correction
   bool fft_tc = false;                      // y/x FFT passes on the tensor cores
@@ -246,8 +278,13 @@ struct ct2g_ctx {
   uint32_t *h_pinned = nullptr;  // small pinned host scratch
   // mesh
   float *grid = nullptr;    // [nc][nbox][C] real: moments, then expansions
-  float2 *spec = nullptr;   // [nc][nbox][CK] complex
+  // spectrum of the mesh solve, all components of a k-point side by side:
+  // [box][qi][qj][qk][nc], qk < ldk (the slots qk > N/2 are zero padding)
+  float2 *spec = nullptr;
   float *greens = nullptr;  // [nc][CK] real-or-imag, shared by the boxes
+  // the same table in column order for the fused X pass + MG2L:
+  // [qj][qk <= N/2][nc][qi]
+  float *greens_x = nullptr;
   float2 *tw32 = nullptr;   // twiddles exp(-2 pi i k/M), k < M/2
   double2 *tw64 = nullptr;
   int tw_n = 0;
@@ -336,12 +373,23 @@ int ct2g_p2m(ct2g_ctx *ctx);
 // fused_p2m: the moments are computed inside the forward z pass (the grid
 // is not written; ctx->grid then holds no moments)
 int ct2g_mesh_solve(ct2g_ctx *ctx, bool fused_l2p, bool pot, bool fused_p2m = false);
-// forward z pass fused with P2M, then the Y and X passes (ct2g_fft.cu)
-int ct2g_fft_p2m_r2c(ct2g_ctx *ctx);
+// Mesh-solve transforms on ctx->spec (ct2g_fft.cu).  Forward: the z pass
+// (P2M inside it when p2m, else from the moment grid), the Y pass, and the X
+// pass unless the X passes are fused with MG2L.  ct2g_spec_mg2l: the fused X
+// pass + MG2L + inverse X pass, or MG2L alone.  Inverse: the inverse X pass
+// (when not fused), the Y pass and the z pass (L2P inside it when l2p, else
+// into the expansion grid).
+int ct2g_spec_forward(ct2g_ctx *ctx, bool p2m);
+int ct2g_spec_mg2l(ct2g_ctx *ctx);
+int ct2g_spec_inverse(ct2g_ctx *ctx, bool l2p, bool pot);
+// the X passes and MG2L run as one kernel for this context
+bool ct2g_mg2l_fused(const ct2g_ctx *ctx);
+// MG2L alone on ctx->spec (ct2g_mesh.cu)
+int ct2g_mg2l_split(ct2g_ctx *ctx);
+// floats of ctx->greens_x
+size_t ct2g_greens_x_floats(const ct2g_ctx *ctx);
 // the learned correction will run on the next force computation
 bool ct2g_learned_active(const ct2g_ctx *ctx);
-// inverse z pass fused with L2P (ct2g_fft.cu)
-int ct2g_fft_c2r_l2p(ct2g_ctx *ctx, bool pot);
 // forces of the current range; pot: also the potential (diagnostics)
 int ct2g_forces(ct2g_ctx *ctx, bool pot);
 int ct2g_update(ct2g_ctx *ctx, const ct2g_kick_params *p, int *max_rung, bool fuse_drift,

@@ -68,58 +68,57 @@ __global__ void __launch_bounds__(128) p2m_kernel(const uint32_t *__restrict__ x
 }
 
 // ---------------------------------------------------------------------------
-// MG2L: one thread per k-point, in place on the spectrum.
-// G_n is real for even |n| and i*g for odd |n| (parity of D^n phi).
+// MG2L alone (the precision form, and orders or meshes whose fused X pass
+// does not fit in shared memory): one thread per k-point, in place.  A block's
+// 128 k-points are one contiguous run of the spectrum ([k-point][nc]), staged
+// through shared memory so that both the load and the store are coalesced;
+// each thread's Green's values go to a private smem column.  blockIdx.y is
+// the box; the boxes share G.  The zero-padding slots qk > N/2 are skipped.
 // ---------------------------------------------------------------------------
-// one (a, b) term; every index is a compile-time constant, so m[] and acc
-// stay in registers
-template <int P, int I>
-__device__ __forceinline__ void mg2l_term(const float2 *m, const float *gcol, float2 &acc,
-                                          float2 *out, int64_t SK) {
-  constexpr int A = Mg2lTab<P>::t.a[I], B = Mg2lTab<P>::t.b[I], AB = Mg2lTab<P>::t.ab[I];
-  constexpr bool FIRST = Mg2lTab<P>::t.first[I] != 0, LAST = Mg2lTab<P>::t.last[I] != 0,
-                 ODD = Mg2lTab<P>::t.odd[I] != 0;
-  if constexpr (FIRST) acc = make_float2(0.f, 0.f);
-  const float gv = gcol[AB * 128];
-  const float2 mb = m[B];
-  if constexpr (!ODD) {
-    acc.x = fmaf(gv, mb.x, acc.x);
-    acc.y = fmaf(gv, mb.y, acc.y);
-  } else {  // i*g*(mx + i my) = (-g my, g mx)
-    acc.x = fmaf(-gv, mb.y, acc.x);
-    acc.y = fmaf(gv, mb.x, acc.y);
-  }
-  if constexpr (LAST) out[(int64_t)A * SK] = acc;
-}
-
-template <int P, int... I>
-__device__ __forceinline__ void mg2l_all(const float2 *m, const float *gcol, float2 *out,
-                                         int64_t SK, std::integer_sequence<int, I...>) {
-  float2 acc = make_float2(0.f, 0.f);
-  (mg2l_term<P, I>(m, gcol, acc, out, SK), ...);
-}
-
-// MG2L: one thread per k-point, in place on the spectrum.  G_n is real for
-// even |n| and i*g for odd |n| (parity of D^n phi).  The thread's Green's
-// values go to a private smem column (no sharing, so no barrier); the moments
-// stay in registers.  blockIdx.y is the box: the spectrum holds component k
-// of box b at (k * nbox + b) * CK, and the boxes share G.
 template <int P>
 __global__ void __launch_bounds__(128) mg2l_kernel(float2 *__restrict__ spec,
                                                    const float *__restrict__ G, int64_t CK,
-                                                   int64_t SK) {
+                                                   int ldk, int nh) {
   constexpr int NC = ct2g_ncomp(P);
-  __shared__ float gs[NC * 128];
-  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= CK) return;
-  float2 *sp = spec + (int64_t)blockIdx.y * CK + q;
-  float2 m[NC];
+  extern __shared__ __align__(16) unsigned char smraw[];
+  float2 *sm = reinterpret_cast<float2 *>(smraw);       // [128][NC]
+  float *gs = reinterpret_cast<float *>(sm + 128 * NC);  // [NC][128]
+  const int64_t q0 = (int64_t)blockIdx.x * 128;
+  const int np = (int)min((int64_t)128, CK - q0);
+  float2 *run = spec + ((int64_t)blockIdx.y * CK + q0) * NC;
+  for (int e = threadIdx.x; e < np * NC; e += 128) sm[e] = run[e];
+  const int64_t q = q0 + threadIdx.x;
+  if (threadIdx.x < np) {
 #pragma unroll
-  for (int k = 0; k < NC; k++) {
-    m[k] = sp[(int64_t)k * SK];
-    gs[k * 128 + threadIdx.x] = __ldg(G + (int64_t)k * CK + q);
+    for (int k = 0; k < NC; k++) gs[k * 128 + threadIdx.x] = __ldg(G + (int64_t)k * CK + q);
   }
-  mg2l_all<P>(m, gs + threadIdx.x, sp, SK, std::make_integer_sequence<int, Mg2lPairs<P>::NP>{});
+  __syncthreads();
+  if (threadIdx.x < np && (int)(q % ldk) < nh) {
+    float2 m[NC];
+#pragma unroll
+    for (int k = 0; k < NC; k++) m[k] = sm[threadIdx.x * NC + k];
+    ct2g_mg2l_all<P, 128>(m, gs + threadIdx.x, sm + threadIdx.x * NC,
+                          std::make_integer_sequence<int, Mg2lPairs<P>::NP>{});
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < np * NC; e += 128) run[e] = sm[e];
+}
+
+// ctx->greens [nc][CK] -> ctx->greens_x: column (qj, qk), qk <= N/2, holds
+// the column's values as [nc][qi]
+__global__ void greens_cols_kernel(const float *__restrict__ G, int64_t CK, int N, int ldk,
+                                   int nc, float *__restrict__ gx) {
+  const int nh = N / 2 + 1;
+  const int64_t gcol = (int64_t)nc * N;
+  const int64_t total = (int64_t)N * nh * gcol;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t colid = e / gcol;
+    const int r = (int)(e - colid * gcol);
+    const int qj = (int)(colid / nh), qk = (int)(colid % nh);
+    const int k = r / N, qi = r % N;
+    gx[e] = G[(int64_t)k * CK + ((int64_t)qi * N + qj) * ldk + qk];
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -326,10 +325,12 @@ int launch_p2m(ct2g_ctx *ctx) {
 
 template <int P>
 int launch_mg2l(ct2g_ctx *ctx) {
-  const unsigned T = 128;
-  const dim3 grid(ct2g_div_up(ctx->CK, T), (unsigned)ctx->nbox);
-  mg2l_kernel<P><<<grid, T, 0, ctx->stream>>>(ctx->spec, ctx->greens, ctx->CK,
-                                               ctx->CK * ctx->nbox);
+  constexpr int NC = ct2g_ncomp(P);
+  const size_t smem = (sizeof(float2) + sizeof(float)) * 128 * NC;
+  auto k = mg2l_kernel<P>;
+  CT2G_TRY(ct2g_smem_attrs(ctx, k, smem));
+  const dim3 grid(ct2g_div_up(ctx->CK, 128), (unsigned)ctx->nbox);
+  k<<<grid, 128, smem, ctx->stream>>>(ctx->spec, ctx->greens, ctx->CK, ctx->ldk, ctx->M / 2 + 1);
   CT2G_LAUNCHED(ctx);
   return CT2G_OK;
 }
@@ -472,12 +473,33 @@ int ct2g_build_greens(ct2g_ctx *ctx) {
     }
   } while (0);
   cleanup();
+  if (rc == CT2G_OK && ctx->greens_x) {
+    greens_cols_kernel<<<4 * ctx->num_sms, 256, 0, ctx->stream>>>(ctx->greens, ctx->CK, M,
+                                                                 ctx->ldk, nc, ctx->greens_x);
+    ctx->launches++;
+  }
   if (rc == CT2G_OK) {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return ct2g_cuda_fail(ctx, e, "greens build");
     ctx->greens_valid = true;
   }
   return rc;
+}
+
+size_t ct2g_greens_x_floats(const ct2g_ctx *ctx) {
+  return (size_t)ctx->M * (ctx->M / 2 + 1) * ctx->nc * ctx->M;
+}
+
+int ct2g_mg2l_split(ct2g_ctx *ctx) {
+  switch (ctx->p) {
+    case 1: return launch_mg2l<1>(ctx);
+    case 2: return launch_mg2l<2>(ctx);
+    case 3: return launch_mg2l<3>(ctx);
+    case 4: return launch_mg2l<4>(ctx);
+    case 5: return launch_mg2l<5>(ctx);
+    case 6: return launch_mg2l<6>(ctx);
+  }
+  return ct2g_fail(ctx, CT2G_EINVAL, "unsupported order");
 }
 
 int ct2g_p2m(ct2g_ctx *ctx) {
@@ -492,25 +514,14 @@ int ct2g_p2m(ct2g_ctx *ctx) {
   return ct2g_fail(ctx, CT2G_EINVAL, "unsupported order");
 }
 
-// forward FFT of the moment grids, MG2L, inverse FFT into the expansions
-// (which overwrite the moments in ctx->grid)
+// forward FFT of the moments, MG2L, inverse FFT into the expansions (the
+// expansion grid, or straight into the forces)
 int ct2g_mesh_solve(ct2g_ctx *ctx, bool fused_l2p, bool pot, bool fused_p2m) {
   CT2G_TRY(ct2g_build_greens(ctx));
   ct2g_mark(ctx, 2);
-  if (fused_p2m)
-    CT2G_TRY(ct2g_fft_p2m_r2c(ctx));
-  else
-    CT2G_TRY(ct2g_fft_r2c_f32(ctx, ctx->grid, ctx->spec, ctx->M, ctx->nc * ctx->nbox, ctx->ldk));
+  CT2G_TRY(ct2g_spec_forward(ctx, fused_p2m));
   ct2g_mark(ctx, 3);
-  switch (ctx->p) {
-    case 1: CT2G_TRY(launch_mg2l<1>(ctx)); break;
-    case 2: CT2G_TRY(launch_mg2l<2>(ctx)); break;
-    case 3: CT2G_TRY(launch_mg2l<3>(ctx)); break;
-    case 4: CT2G_TRY(launch_mg2l<4>(ctx)); break;
-    case 5: CT2G_TRY(launch_mg2l<5>(ctx)); break;
-    case 6: CT2G_TRY(launch_mg2l<6>(ctx)); break;
-    default: return ct2g_fail(ctx, CT2G_EINVAL, "unsupported order");
-  }
+  CT2G_TRY(ct2g_spec_mg2l(ctx));
   ct2g_mark(ctx, 4);
   if (fused_l2p) {
     // every particle of the range gets its far field; others read zero
@@ -519,10 +530,8 @@ int ct2g_mesh_solve(ct2g_ctx *ctx, bool fused_l2p, bool pot, bool fused_p2m) {
     CT2G_CUDA(ctx, cudaMemsetAsync(ctx->fy, 0, n * 4, ctx->stream));
     CT2G_CUDA(ctx, cudaMemsetAsync(ctx->fz, 0, n * 4, ctx->stream));
     if (pot) CT2G_CUDA(ctx, cudaMemsetAsync(ctx->pot, 0, n * 4, ctx->stream));
-    CT2G_TRY(ct2g_fft_c2r_l2p(ctx, pot));
-  } else {
-    CT2G_TRY(ct2g_fft_c2r_f32(ctx, ctx->spec, ctx->grid, ctx->M, ctx->nc * ctx->nbox, ctx->ldk));
   }
+  CT2G_TRY(ct2g_spec_inverse(ctx, fused_l2p, pot));
   ct2g_mark(ctx, 5);
   return CT2G_OK;
 }

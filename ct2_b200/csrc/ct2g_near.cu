@@ -460,7 +460,7 @@ int ct2g_upload_stencil(ct2g_ctx *ctx, const std::vector<int> &st4) {
 
 int ct2g_forces(ct2g_ctx *ctx, bool pot) {
   const size_t n = ctx->n;
-  // the far-field pass (ct2g_fft_c2r_l2p) has written the range's entries
+  // the far-field pass (the inverse z pass with L2P) has written the range's entries
   (void)n;
   CT2G_CUDA(ctx, cudaMemsetAsync(ctx->d_inter, 0, sizeof(unsigned long long), ctx->stream));
   CT2G_CUDA(ctx, cudaMemsetAsync(ctx->d_counts + 3, 0, 2 * sizeof(uint32_t), ctx->stream));

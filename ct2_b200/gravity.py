@@ -301,10 +301,10 @@ class Gravity:
         t = Tuning()
         self._chk(self._l.ct2g_get_tuning(self._h, ctypes.byref(t)))
         return dict(dense_cell=t.dense_cell, near_blocks_per_sm=t.near_blocks_per_sm,
-                    fft_tile=t.fft_tile)
+                    fft_tile=t.fft_tile, split_mg2l=t.split_mg2l)
 
-    def set_tuning(self, dense_cell=16, near_blocks_per_sm=0, fft_tile=0):
-        t = Tuning(dense_cell, near_blocks_per_sm, fft_tile)
+    def set_tuning(self, dense_cell=16, near_blocks_per_sm=0, fft_tile=0, split_mg2l=0):
+        t = Tuning(dense_cell, near_blocks_per_sm, fft_tile, split_mg2l)
         self._chk(self._l.ct2g_set_tuning(self._h, ctypes.byref(t)))
 
     def autotune(self, params: kick_params, dt: float, scale: float = 1.0, cache_path=None):
@@ -313,7 +313,7 @@ class Gravity:
         self._chk(self._l.ct2g_autotune(self._h, ctypes.byref(params._c()), dt, scale, cp,
                                         ctypes.byref(t)))
         return dict(dense_cell=t.dense_cell, near_blocks_per_sm=t.near_blocks_per_sm,
-                    fft_tile=t.fft_tile)
+                    fft_tile=t.fft_tile, split_mg2l=t.split_mg2l)
 
     def kick_step(self, minrung, max_rung, scale, adot, tau, t0, minrung0, nocrop=False):
         """Returns (max_rung, minrung) -- the reference returns max_rung and

@@ -207,12 +207,16 @@ int ct2g_batch_destroy(ct2g_batch *b);
  * dense_cell -- cells with at least this many particles get their own sink
  * chunks, the rest are chunked per 4x4x4 block; near_blocks_per_sm -- blocks
  * per SM of the persistent near-field grid (0: occupancy limit); fft_tile --
- * columns per tile of the y/x FFT passes (0: default). */
+ * columns per tile of the y/x FFT passes (0: default); split_mg2l -- 1 runs
+ * the X FFT passes and the Green's-function multiply as three kernels, 0 (the
+ * default) as one wherever a spectrum column of all components fits in
+ * shared memory. */
 typedef struct {
   int dense_cell;
   int near_blocks_per_sm;
   int fft_tile;
-  int reserved[5];
+  int split_mg2l;
+  int reserved[4];
 } ct2g_tuning;
 int ct2g_get_tuning(const ct2g_ctx *ctx, ct2g_tuning *t);
 int ct2g_set_tuning(ct2g_ctx *ctx, const ct2g_tuning *t);
