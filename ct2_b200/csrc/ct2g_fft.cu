@@ -72,7 +72,8 @@ constexpr int brevc(int v, int bits) {
 // In-register R-point DFT (R <= 32), natural order in and out.
 // Radix-2 DIF: span h from R/2 down to 1, butterfly (a, b) ->
 // (a + b, (a - b) W_{2h}^j); the result lands in bit-reversed order and is
-// permuted back at compile time.
+// permuted back at compile time.  W = -i (a quarter turn) is a swap and a
+// sign, not a complex product.
 template <int R, typename C2, bool INV>
 __device__ __forceinline__ void reg_dft(C2 (&v)[R]) {
 #pragma unroll
@@ -84,7 +85,11 @@ __device__ __forceinline__ void reg_dft(C2 (&v)[R]) {
         const C2 a = v[blk + j], b = v[blk + j + h];
         v[blk + j] = cadd(a, b);
         C2 d = csub(a, b);
-        if (j != 0) {
+        if (j * (32 / (2 * h)) == 8) {  // W = -i (forward), +i (inverse): a swap
+          const C2 e = d;
+          d.x = INV ? -e.y : e.y;
+          d.y = INV ? e.x : -e.x;
+        } else if (j != 0) {
           C2 w = w32<C2>(j * (32 / (2 * h)));
           if (INV) w.y = -w.y;
           d = cmul(d, w);
@@ -573,14 +578,14 @@ int fft_c2r(ct2g_ctx *ctx, typename Cplx<T>::type *in, T *out, int N, int batch,
 // the moment grid (component k of box b at grid + (k * nbox + b) * N^3).
 constexpr uint32_t kWarpCell = 32;
 
-template <int P>
+// components [K0, K1) of one particle's moments about the cell centre u
+template <int P, int K0, int K1>
 __device__ __forceinline__ void p2m_accumulate(const uint32_t *__restrict__ px,
                                                const uint32_t *__restrict__ py,
                                                const uint32_t *__restrict__ pz, uint32_t i,
                                                uint32_t ux, uint32_t uy, uint32_t uz,
                                                double *acc) {
   constexpr MiTable<P> T{};
-  constexpr int NC = ct2g_ncomp(P);
   const double sx = -(double)(int32_t)(px[i] - ux) * CT2G_TWO_M32;
   const double sy = -(double)(int32_t)(py[i] - uy) * CT2G_TWO_M32;
   const double sz = -(double)(int32_t)(pz[i] - uz) * CT2G_TWO_M32;
@@ -593,11 +598,41 @@ __device__ __forceinline__ void p2m_accumulate(const uint32_t *__restrict__ px,
     qz[q] = qz[q - 1] * sz * (1.0 / q);
   }
 #pragma unroll
-  for (int k = 0; k < NC; k++) acc[k] += qx[T.nx[k]] * qy[T.ny[k]] * qz[T.nz[k]];
+  for (int k = K0; k < K1; k++) acc[k - K0] += qx[T.nx[k]] * qy[T.ny[k]] * qz[T.nz[k]];
+}
+
+// the moments of cell particles b, b + step, ... < e (a thread: step 1; a
+// warp: lane offset, step 32, then summed over the warp) into the packed smem
+// lines at z, for components [K0, K1): the components go in two halves so
+// that only half of the FP64 sums are live at once
+template <int P, int N, int K0, int K1>
+__device__ __forceinline__ void p2m_half(const uint32_t *__restrict__ px,
+                                         const uint32_t *__restrict__ py,
+                                         const uint32_t *__restrict__ pz, uint32_t b, uint32_t e,
+                                         uint32_t step, bool warp_sum, uint32_t ux, uint32_t uy,
+                                         uint32_t uz, int z, float *sr, bool write) {
+  using LL = LineLayout<N, true>;
+  double acc[K1 - K0];
+#pragma unroll
+  for (int k = 0; k < K1 - K0; k++) acc[k] = 0.0;
+  for (uint32_t i = b; i < e; i += step) p2m_accumulate<P, K0, K1>(px, py, pz, i, ux, uy, uz, acc);
+  if (warp_sum) {
+#pragma unroll
+    for (int k = 0; k < K1 - K0; k++) {
+      double v = acc[k];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      acc[k] = v;
+    }
+  }
+  if (write) {
+#pragma unroll
+    for (int k = K0; k < K1; k++) sr[2 * LL::at(k >> 1, z, 0) + (k & 1)] = (float)acc[k - K0];
+  }
 }
 
 template <int P, int N, bool GRID>
-__global__ void __launch_bounds__(256, 2) fftz_p2m_r2c_kernel(
+__global__ void __launch_bounds__(256, P <= 4 ? 3 : 2) fftz_p2m_r2c_kernel(
     const uint32_t *__restrict__ px, const uint32_t *__restrict__ py,
     const uint32_t *__restrict__ pz, const uint32_t *__restrict__ cs, int mbits,
     const float *__restrict__ grid, int64_t CB, float2 *__restrict__ spec, int ldk,
@@ -635,12 +670,8 @@ __global__ void __launch_bounds__(256, 2) fftz_p2m_r2c_kernel(
         continue;
       }
       const uint32_t uz = ((uint32_t)zc << sh) + halfc;
-      double acc[NC];
-#pragma unroll
-      for (int k = 0; k < NC; k++) acc[k] = 0.0;
-      for (uint32_t i = b; i < e; i++) p2m_accumulate<P>(px, py, pz, i, ux, uy, uz, acc);
-#pragma unroll
-      for (int k = 0; k < NC; k++) sr[2 * LL::at(k >> 1, zc, 0) + (k & 1)] = (float)acc[k];
+      p2m_half<P, N, 0, NC / 2>(px, py, pz, b, e, 1, false, ux, uy, uz, zc, sr, true);
+      p2m_half<P, N, NC / 2, NC>(px, py, pz, b, e, 1, false, ux, uy, uz, zc, sr, true);
       if (NC & 1) sr[2 * LL::at(NL - 1, zc, 0) + 1] = 0.f;
     }
     __syncthreads();
@@ -651,22 +682,11 @@ __global__ void __launch_bounds__(256, 2) fftz_p2m_r2c_kernel(
         const uint32_t key = (box << (3 * mbits)) | ct2g_morton(cx, cy, zc);
         const uint32_t b = cs[key], e = cs[key + 1];
         const uint32_t uz = (zc << sh) + halfc;
-        double acc[NC];
-#pragma unroll
-        for (int k = 0; k < NC; k++) acc[k] = 0.0;
-        for (uint32_t i = b + lane; i < e; i += 32) p2m_accumulate<P>(px, py, pz, i, ux, uy, uz, acc);
-#pragma unroll
-        for (int k = 0; k < NC; k++) {
-          double v = acc[k];
-#pragma unroll
-          for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-          acc[k] = v;
-        }
-        if (lane == 0) {
-#pragma unroll
-          for (int k = 0; k < NC; k++) sr[2 * LL::at(k >> 1, (int)zc, 0) + (k & 1)] = (float)acc[k];
-          if (NC & 1) sr[2 * LL::at(NL - 1, (int)zc, 0) + 1] = 0.f;
-        }
+        p2m_half<P, N, 0, NC / 2>(px, py, pz, b + lane, e, 32, true, ux, uy, uz, (int)zc, sr,
+                                  lane == 0);
+        p2m_half<P, N, NC / 2, NC>(px, py, pz, b + lane, e, 32, true, ux, uy, uz, (int)zc, sr,
+                                   lane == 0);
+        if ((NC & 1) && lane == 0) sr[2 * LL::at(NL - 1, (int)zc, 0) + 1] = 0.f;
       }
     }
   }
