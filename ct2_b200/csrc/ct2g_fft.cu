@@ -61,6 +61,28 @@ __device__ __forceinline__ C2 csub(C2 a, C2 b) {
   r.y = a.y - b.y;
   return r;
 }
+// FP32 complex sums as one packed f32x2 instruction (two round-to-nearest
+// FP32 operations, the same results as the scalar pair)
+template <>
+__device__ __forceinline__ float2 cadd<float2>(float2 a, float2 b) {
+  unsigned long long pa, pb, pr;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(pa) : "f"(a.x), "f"(a.y));
+  asm("mov.b64 %0, {%1, %2};" : "=l"(pb) : "f"(b.x), "f"(b.y));
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(pr) : "l"(pa), "l"(pb));
+  float2 r;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(pr));
+  return r;
+}
+template <>
+__device__ __forceinline__ float2 csub<float2>(float2 a, float2 b) {
+  unsigned long long pa, pb, pr;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(pa) : "f"(a.x), "f"(a.y));
+  asm("mov.b64 %0, {%1, %2};" : "=l"(pb) : "f"(b.x), "f"(b.y));
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(pr) : "l"(pa), "l"(pb));
+  float2 r;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(pr));
+  return r;
+}
 
 constexpr int ilog2c(int n) { return n <= 1 ? 0 : 1 + ilog2c(n / 2); }
 constexpr int brevc(int v, int bits) {
@@ -845,9 +867,10 @@ int launch_c2r_l2p(ct2g_ctx *ctx, int mode) {
 // NC components, s[qi * NC + c], are transformed along x, contracted with the
 // Green's tensor (L_a = sum_b G_{a+b} M_b, src/particle.cpp:244-250) and
 // transformed back, so neither the transformed moments nor the expansions
-// make a round trip through HBM between the three steps.  The column's
-// moments and its Green's values ([c][qi], one contiguous run of the
-// column-ordered table) arrive by cp.async.
+// make a round trip through HBM between the three steps.  The first transform
+// step reads the column's moments from HBM into registers, the last one
+// writes the expansions back from registers; the Green's values ([c][qi], one
+// contiguous run of the column-ordered table) arrive by cp.async meanwhile.
 template <int P, int N>
 struct FxShape {
   static constexpr int NC = ct2g_ncomp(P), NH = N / 2 + 1;
@@ -857,11 +880,65 @@ struct FxShape {
   static constexpr bool FITS = SMEM <= 227 * 1024;
   static constexpr int MINB = SMEM <= 112 * 1024 ? 2 : 1;
   static constexpr bool GREG = NC <= 35;  // Green's values in registers
+  // (a persistent form with one 512-thread block per SM and the next
+  // column's data arriving by cp.async in a second buffer measured slower:
+  // 2.45 against 1.90 ms at N = 256, order 4)
 };
 
 __device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+
+// The two steps of tile_fft for NL lines in the COLS layout s[r * NL + l],
+// with the first step's input and the second step's output going through
+// functors, so that a line can come straight from HBM or go straight back
+// without a pass through shared memory.  cols_step1: jobs (l, n1), input
+// ld(l, r), Y[n1][k2] to smem.  cols_step2: jobs (l, k2), X[k2 + R2*k1] to
+// st(l, r, v); INPLACE when st writes the smem slots the step reads.
+template <int N, int NL, bool INV, int NT, typename LD>
+__device__ __forceinline__ void cols_step1(float2 *s, const float2 *stw, LD ld) {
+  using LL = LineLayout<N, false>;
+  constexpr int R1 = LL::R1, R2 = LL::R2;
+  for (int job = threadIdx.x; job < NL * R1; job += NT) {
+    const int l = job % NL, n1 = job / NL;
+    float2 v[R2];
+#pragma unroll
+    for (int n2 = 0; n2 < R2; n2++) v[n2] = ld(l, n1 + R1 * n2);
+    reg_dft<R2, float2, INV>(v);
+#pragma unroll
+    for (int k2 = 1; k2 < R2; k2++) {
+      float2 w = stw[(n1 * k2) & (N - 1)];
+      if (INV) w.y = -w.y;
+      v[k2] = cmul(v[k2], w);
+    }
+#pragma unroll
+    for (int k2 = 0; k2 < R2; k2++) s[(n1 + R1 * k2) * NL + l] = v[k2];
+  }
+}
+
+template <int N, int NL, bool INV, bool INPLACE, int NT, typename ST>
+__device__ __forceinline__ void cols_step2(const float2 *s, ST st) {
+  using LL = LineLayout<N, false>;
+  constexpr int R1 = LL::R1, R2 = LL::R2;
+  static_assert(NT % R2 == 0, "block size must be a multiple of R2");
+  constexpr int LW = NT / R2;
+  for (int l0 = 0; l0 < NL; l0 += LW) {
+    const int l = l0 + threadIdx.x % LW, k2 = threadIdx.x / LW;
+    const bool on = l < NL;
+    float2 v[R1];
+    if (on) {
+#pragma unroll
+      for (int n1 = 0; n1 < R1; n1++) v[n1] = s[(n1 + R1 * k2) * NL + l];
+      reg_dft<R1, float2, INV>(v);
+    }
+    if (INPLACE) __syncthreads();  // all reads of this round before any write
+    if (on) {
+#pragma unroll
+      for (int k1 = 0; k1 < R1; k1++) st(l, k2 + R2 * k1, v[k1]);
+    }
+    if (INPLACE) __syncthreads();
+  }
 }
 
 template <int P, int N>
@@ -879,17 +956,18 @@ __global__ void __launch_bounds__(256, FxShape<P, N>::MINB) fftx_mg2l_kernel(
   const int box = (int)(blockIdx.x / ((unsigned)NH * N));
   const int64_t RS = (int64_t)ldk * NC, XS = (int64_t)N * RS;
   float2 *col = spec + (int64_t)box * N * XS + (int64_t)qj * RS + (int64_t)qk * NC;
-  for (int e = threadIdx.x; e < N * NC; e += 256) {
-    const int x = e / NC, c = e - x * NC;
-    cp_async8(s + e, col + x * XS + c);
-  }
+  // the Green's values arrive while the forward transform runs
   const float *gcol = gx + ((int64_t)qj * NH + qk) * S::GCOL;
   for (int e = threadIdx.x; e < S::GCOL / 4; e += 256) cp_async16(sg + 4 * e, gcol + 4 * e);
   cp_async_commit();
   load_twiddles(stw, tw, N);
+  __syncthreads();
+  // forward: the first step reads the column from HBM
+  cols_step1<N, NC, false, 256>(s, stw, [&](int l, int r) { return col[r * XS + l]; });
+  __syncthreads();
+  cols_step2<N, NC, false, true, 256>(s, [&](int l, int r, float2 v) { s[r * NC + l] = v; });
   cp_async_wait<0>();
   __syncthreads();
-  tile_fft<N, false, float2, false>(s, NC, NC, stw);
   for (int qi = threadIdx.x; qi < N; qi += 256) {
     float2 m[NC];
 #pragma unroll
@@ -905,11 +983,10 @@ __global__ void __launch_bounds__(256, FxShape<P, N>::MINB) fftx_mg2l_kernel(
     }
   }
   __syncthreads();
-  tile_fft<N, false, float2, true>(s, NC, NC, stw);
-  for (int e = threadIdx.x; e < N * NC; e += 256) {
-    const int x = e / NC, c = e - x * NC;
-    col[x * XS + c] = s[e];
-  }
+  // inverse: the second step writes the column back to HBM
+  cols_step1<N, NC, true, 256>(s, stw, [&](int l, int r) { return s[r * NC + l]; });
+  __syncthreads();
+  cols_step2<N, NC, true, false, 256>(s, [&](int l, int r, float2 v) { col[r * XS + l] = v; });
 }
 
 template <int P, int N>
@@ -918,10 +995,11 @@ int launch_fx_mg2l(ct2g_ctx *ctx) {
   if constexpr (!S::FITS) {
     return ct2g_fail(ctx, CT2G_EINVAL, "fused X pass + MG2L does not fit in shared memory");
   } else {
+    const size_t ncol = (size_t)ctx->nbox * N * S::NH;
     auto k = fftx_mg2l_kernel<P, N>;
     CT2G_TRY(ct2g_smem_attrs(ctx, k, S::SMEM));
-    k<<<(unsigned)((size_t)ctx->nbox * N * S::NH), 256, S::SMEM, ctx->stream>>>(
-        ctx->spec, ctx->ldk, ctx->greens_x, twiddle_ptr<float2>(ctx));
+    k<<<(unsigned)ncol, 256, S::SMEM, ctx->stream>>>(ctx->spec, ctx->ldk, ctx->greens_x,
+                                                     twiddle_ptr<float2>(ctx));
     CT2G_LAUNCHED(ctx);
     return CT2G_OK;
   }
