@@ -596,9 +596,10 @@ int fft_c2r(ct2g_ctx *ctx, typename Cplx<T>::type *in, T *out, int N, int batch,
 // components.  The moment grid is never written to HBM.  A thread sums a
 // cell of up to kWarpCell particles; bigger cells are summed by a warp
 // (lanes stride over the particles, partial moments reduced by shuffles), so
-// no block waits on one thread's long loop.  GRID: the moments are read from
+// no block waits on one thread's long loop: a thread's FP64 sums are a serial
+// chain, and a block's transform waits for its slowest cell.  GRID: the moments are read from
 // the moment grid (component k of box b at grid + (k * nbox + b) * N^3).
-constexpr uint32_t kWarpCell = 32;
+constexpr uint32_t kWarpCell = 6;
 
 // components [K0, K1) of one particle's moments about the cell centre u
 template <int P, int K0, int K1>
@@ -779,13 +780,31 @@ __global__ void __launch_bounds__(256) fftz_c2r_l2p_kernel(
     }
   }
   const float2 *row = spec + (int64_t)blockIdx.x * ((int64_t)ldk * NC);
-  for (int e = threadIdx.x; e < NH * NL; e += 256) {
-    const int k = e / NL, l = e - k * NL;
-    const float2 a = row[k * NC + 2 * l];
-    const float2 b = (2 * l + 1 < NC) ? row[k * NC + 2 * l + 1] : make_float2(0.f, 0.f);
-    // Z_k = A_k + i B_k; Z_{N-k} = conj(A_k) + i conj(B_k)
-    s[LL::at(l, k, 0)] = make_float2(a.x - b.y, a.y + b.x);
-    if (k > 0 && k < N / 2) s[LL::at(l, N - k, 0)] = make_float2(a.x + b.y, b.x - a.y);
+  // the row's loads go out in batches of RB per thread before any of them is
+  // used, so that their latencies overlap
+  constexpr int RB = 5;
+  for (int e0 = threadIdx.x; e0 < NH * NL; e0 += RB * 256) {
+    float2 a[RB], b[RB];
+#pragma unroll
+    for (int u = 0; u < RB; u++) {
+      const int e = e0 + 256 * u;
+      const int k = e / NL, l = e - k * NL;
+      a[u] = b[u] = make_float2(0.f, 0.f);
+      if (e < NH * NL) {
+        a[u] = row[k * NC + 2 * l];
+        if (2 * l + 1 < NC) b[u] = row[k * NC + 2 * l + 1];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < RB; u++) {
+      const int e = e0 + 256 * u;
+      const int k = e / NL, l = e - k * NL;
+      if (e < NH * NL) {
+        // Z_k = A_k + i B_k; Z_{N-k} = conj(A_k) + i conj(B_k)
+        s[LL::at(l, k, 0)] = make_float2(a[u].x - b[u].y, a[u].y + b[u].x);
+        if (k > 0 && k < N / 2) s[LL::at(l, N - k, 0)] = make_float2(a[u].x + b[u].y, b[u].x - a[u].y);
+      }
+    }
   }
   __syncthreads();
   if constexpr (!L2P) {
