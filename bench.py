@@ -399,6 +399,9 @@ def run_fft512(args, rank, world, local):
     M = 512
     g = Gravity(mesh=M, order=1, bwidth=args.bwidth, hsoft=1.0 / (50 * args.ngrid),
                 GM=1.0 / n, device=local, max_particles=n)
+    # the x passes as their own launches, so that both modes' forward and
+    # inverse stages time all three passes of the transforms
+    g.set_tuning(**{**g.tuning(), "split_mg2l": 1})
     g.upload_dict(P)
     g.particle_to_grid()
     res = {}

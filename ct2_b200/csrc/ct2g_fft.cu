@@ -588,6 +588,15 @@ int fft_c2r(ct2g_ctx *ctx, typename Cplx<T>::type *in, T *out, int N, int batch,
 // of W contiguous (qk, c) columns; the X pass runs inside the MG2L kernel,
 // whose block holds every component of one (qj, qk) column.
 
+// (x, y) lines per block of a z pass that reads or writes the moment grid:
+// enough packed lines for a block's transform to fill its threads (one line
+// when the components alone give 16 packed lines or more)
+template <int P>
+constexpr int z_lines() {
+  constexpr int NL = (ct2g_ncomp(P) + 1) / 2;
+  return NL >= 8 ? 1 : NL >= 4 ? 2 : NL >= 2 ? 4 : 8;
+}
+
 // ---- forward z pass fused with P2M -----------------------------------------
 // One block per (x, y) line of one box: the moments of the line's N cells
 // (FP64 sums about the cell centres, as p2m_kernel) go straight into shared
@@ -662,6 +671,7 @@ __global__ void __launch_bounds__(256, P <= 4 ? 3 : 2) fftz_p2m_r2c_kernel(
     const float2 *__restrict__ tw) {
   using LL = LineLayout<N, true>;
   constexpr int NC = ct2g_ncomp(P), NL = (NC + 1) / 2, NH = N / 2 + 1;
+  constexpr int LB = GRID ? z_lines<P>() : 1;  // lines of this block
   extern __shared__ __align__(16) unsigned char smraw[];
   float2 *stw = reinterpret_cast<float2 *>(smraw);
   float2 *s = stw + N;
@@ -670,16 +680,20 @@ __global__ void __launch_bounds__(256, P <= 4 ? 3 : 2) fftz_p2m_r2c_kernel(
   if (threadIdx.x == 0) nbig = 0;
   load_twiddles(stw, tw, N);
   __syncthreads();
-  const size_t line = blockIdx.x % ((size_t)N * N);
-  const uint32_t box = (uint32_t)(blockIdx.x / ((size_t)N * N));
+  const size_t L0 = (size_t)blockIdx.x * LB;  // first line (box * N^2 + line)
+  const size_t line = L0 % ((size_t)N * N);
+  const uint32_t box = (uint32_t)(L0 / ((size_t)N * N));
   if constexpr (GRID) {
+    // line lb of the block: packed lines lb * NL ...; its grid rows follow
     const float *g = grid + ((int64_t)box * N * N + (int64_t)line) * N;
-    for (int e = threadIdx.x; e < NC * N; e += 256) {
-      const int k = e / N, z = e % N;
-      sr[2 * LL::at(k >> 1, z, 0) + (k & 1)] = g[(int64_t)k * CB + z];
+    for (int e = threadIdx.x; e < LB * NC * N; e += 256) {
+      const int lb = LB == 1 ? 0 : e / (NC * N), r = e - lb * NC * N;
+      const int k = r / N, z = r % N;
+      sr[2 * LL::at(lb * NL + (k >> 1), z, 0) + (k & 1)] = g[(int64_t)k * CB + lb * N + z];
     }
     if (NC & 1)
-      for (int z = threadIdx.x; z < N; z += 256) sr[2 * LL::at(NL - 1, z, 0) + 1] = 0.f;
+      for (int e = threadIdx.x; e < LB * N; e += 256)
+        sr[2 * LL::at((e / N) * NL + NL - 1, e % N, 0) + 1] = 0.f;
   } else {
     const uint32_t cx = (uint32_t)(line / N), cy = (uint32_t)(line % N);
     const int sh = 32 - mbits;
@@ -714,15 +728,18 @@ __global__ void __launch_bounds__(256, P <= 4 ? 3 : 2) fftz_p2m_r2c_kernel(
     }
   }
   __syncthreads();
-  tile_fft<N, true, float2, false>(s, NL, 0, stw);
-  // row blockIdx.x = box * N^2 + line; k-point k's components at k * NC
-  float2 *row = spec + (int64_t)blockIdx.x * ((int64_t)ldk * NC);
-  for (int e = threadIdx.x; e < ldk * NL; e += 256) {
-    const int k = e / NL, l = e - k * NL;
+  tile_fft<N, true, float2, false>(s, LB * NL, 0, stw);
+  // row L0 + lb = box * N^2 + line + lb; k-point k's components at k * NC
+  const int64_t RS = (int64_t)ldk * NC;
+  float2 *rows = spec + (int64_t)L0 * RS;
+  for (int e = threadIdx.x; e < LB * ldk * NL; e += 256) {
+    const int lb = LB == 1 ? 0 : e / (ldk * NL), r = e - lb * ldk * NL;
+    const int k = r / NL, l = r - k * NL;
+    float2 *row = rows + lb * RS;
     float2 a = make_float2(0.f, 0.f), bb = make_float2(0.f, 0.f);
     if (k < NH) {
-      const float2 zk = s[LL::at(l, k & (N - 1), 0)];
-      const float2 zn = s[LL::at(l, (N - k) & (N - 1), 0)];
+      const float2 zk = s[LL::at(lb * NL + l, k & (N - 1), 0)];
+      const float2 zn = s[LL::at(lb * NL + l, (N - k) & (N - 1), 0)];
       // A_k = (Z_k + conj Z_{N-k})/2, B_k = (Z_k - conj Z_{N-k})/(2i)
       a = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
       bb = make_float2(0.5f * (zk.y + zn.y), 0.5f * (zn.x - zk.x));
@@ -735,10 +752,11 @@ __global__ void __launch_bounds__(256, P <= 4 ? 3 : 2) fftz_p2m_r2c_kernel(
 template <int P, int N>
 int launch_p2m_r2c(ct2g_ctx *ctx, bool from_grid) {
   constexpr int NL = (ct2g_ncomp(P) + 1) / 2;
-  const size_t smem = sizeof(float2) * ((size_t)N + (size_t)NL * LineLayout<N, true>::LS);
+  const int LB = from_grid ? z_lines<P>() : 1;
+  const size_t smem = sizeof(float2) * ((size_t)N + (size_t)LB * NL * LineLayout<N, true>::LS);
   auto k = from_grid ? fftz_p2m_r2c_kernel<P, N, true> : fftz_p2m_r2c_kernel<P, N, false>;
   CT2G_TRY(ct2g_smem_attrs(ctx, k, smem));
-  k<<<(unsigned)((size_t)N * N * ctx->nbox), 256, smem, ctx->stream>>>(
+  k<<<(unsigned)((size_t)N * N * ctx->nbox / LB), 256, smem, ctx->stream>>>(
       ctx->x, ctx->y, ctx->z, ctx->cell_start, ctx->mbits, ctx->grid, ctx->CB, ctx->spec,
       ctx->ldk, twiddle_ptr<float2>(ctx));
   CT2G_LAUNCHED(ctx);
@@ -763,13 +781,15 @@ __global__ void __launch_bounds__(256) fftz_c2r_l2p_kernel(
   using LL = LineLayout<N, true>;
   constexpr int NC = ct2g_ncomp(P), NL = (NC + 1) / 2, NH = N / 2 + 1;
   constexpr bool L2P = MODE < 2;
+  constexpr int LB = L2P ? 1 : z_lines<P>();  // lines of this block
   extern __shared__ __align__(16) unsigned char smraw[];
   float2 *stw = reinterpret_cast<float2 *>(smraw);
   float2 *s = stw + N;
   __shared__ uint32_t cb[L2P ? N + 1 : 1], ce[L2P ? N : 1];  // particle ranges of the line's cells
   load_twiddles(stw, tw, N);
-  const size_t line = blockIdx.x % ((size_t)N * N);
-  const uint32_t box = (uint32_t)(blockIdx.x / ((size_t)N * N));
+  const size_t L0 = (size_t)blockIdx.x * LB;  // first line (box * N^2 + line)
+  const size_t line = L0 % ((size_t)N * N);
+  const uint32_t box = (uint32_t)(L0 / ((size_t)N * N));
   const uint32_t x = (uint32_t)(line / N), y = (uint32_t)(line % N);
   if constexpr (L2P) {
     // issue the range loads first: their latency hides behind the transform
@@ -779,41 +799,46 @@ __global__ void __launch_bounds__(256) fftz_c2r_l2p_kernel(
       ce[z] = cs[key + 1];
     }
   }
-  const float2 *row = spec + (int64_t)blockIdx.x * ((int64_t)ldk * NC);
+  const int64_t RS = (int64_t)ldk * NC;
+  const float2 *rows = spec + (int64_t)L0 * RS;
   // the row's loads go out in batches of RB per thread before any of them is
   // used, so that their latencies overlap
   constexpr int RB = 5;
-  for (int e0 = threadIdx.x; e0 < NH * NL; e0 += RB * 256) {
+  for (int e0 = threadIdx.x; e0 < LB * NH * NL; e0 += RB * 256) {
     float2 a[RB], b[RB];
 #pragma unroll
     for (int u = 0; u < RB; u++) {
       const int e = e0 + 256 * u;
-      const int k = e / NL, l = e - k * NL;
+      const int lb = LB == 1 ? 0 : e / (NH * NL), r = e - lb * NH * NL;
+      const int k = r / NL, l = r - k * NL;
       a[u] = b[u] = make_float2(0.f, 0.f);
-      if (e < NH * NL) {
-        a[u] = row[k * NC + 2 * l];
-        if (2 * l + 1 < NC) b[u] = row[k * NC + 2 * l + 1];
+      if (e < LB * NH * NL) {
+        a[u] = rows[lb * RS + k * NC + 2 * l];
+        if (2 * l + 1 < NC) b[u] = rows[lb * RS + k * NC + 2 * l + 1];
       }
     }
 #pragma unroll
     for (int u = 0; u < RB; u++) {
       const int e = e0 + 256 * u;
-      const int k = e / NL, l = e - k * NL;
-      if (e < NH * NL) {
+      const int lb = LB == 1 ? 0 : e / (NH * NL), r = e - lb * NH * NL;
+      const int k = r / NL, l = r - k * NL;
+      if (e < LB * NH * NL) {
         // Z_k = A_k + i B_k; Z_{N-k} = conj(A_k) + i conj(B_k)
-        s[LL::at(l, k, 0)] = make_float2(a[u].x - b[u].y, a[u].y + b[u].x);
-        if (k > 0 && k < N / 2) s[LL::at(l, N - k, 0)] = make_float2(a[u].x + b[u].y, b[u].x - a[u].y);
+        s[LL::at(lb * NL + l, k, 0)] = make_float2(a[u].x - b[u].y, a[u].y + b[u].x);
+        if (k > 0 && k < N / 2)
+          s[LL::at(lb * NL + l, N - k, 0)] = make_float2(a[u].x + b[u].y, b[u].x - a[u].y);
       }
     }
   }
   __syncthreads();
   if constexpr (!L2P) {
-    tile_fft<N, true, float2, true>(s, NL, 0, stw);
+    tile_fft<N, true, float2, true>(s, LB * NL, 0, stw);
     float *g = grid + ((int64_t)box * N * N + (int64_t)line) * N;
-    for (int e = threadIdx.x; e < NC * N; e += 256) {
-      const int k = e / N, z = e % N;
-      const float2 v = s[LL::at(k >> 1, z, 0)];
-      g[(int64_t)k * CB + z] = (k & 1) ? v.y : v.x;
+    for (int e = threadIdx.x; e < LB * NC * N; e += 256) {
+      const int lb = LB == 1 ? 0 : e / (NC * N), r = e - lb * NC * N;
+      const int k = r / N, z = r % N;
+      const float2 v = s[LL::at(lb * NL + (k >> 1), z, 0)];
+      g[(int64_t)k * CB + lb * N + z] = (k & 1) ? v.y : v.x;
     }
     return;
   } else {
@@ -870,11 +895,12 @@ __global__ void __launch_bounds__(256) fftz_c2r_l2p_kernel(
 template <int P, int N>
 int launch_c2r_l2p(ct2g_ctx *ctx, int mode) {
   constexpr int NL = (ct2g_ncomp(P) + 1) / 2;
-  const size_t smem = sizeof(float2) * ((size_t)N + (size_t)NL * LineLayout<N, true>::LS);
+  const int LB = mode == 2 ? z_lines<P>() : 1;
+  const size_t smem = sizeof(float2) * ((size_t)N + (size_t)LB * NL * LineLayout<N, true>::LS);
   auto k = mode == 0 ? fftz_c2r_l2p_kernel<P, N, 0>
            : mode == 1 ? fftz_c2r_l2p_kernel<P, N, 1> : fftz_c2r_l2p_kernel<P, N, 2>;
   CT2G_TRY(ct2g_smem_attrs(ctx, k, smem));
-  k<<<(unsigned)((size_t)N * N * ctx->nbox), 256, smem, ctx->stream>>>(
+  k<<<(unsigned)((size_t)N * N * ctx->nbox / LB), 256, smem, ctx->stream>>>(
       ctx->spec, ctx->ldk, ctx->cell_start, ctx->src, ctx->mbits, ctx->box_gm, ctx->fx, ctx->fy,
       ctx->fz, ctx->pot, ctx->grid, ctx->CB, twiddle_ptr<float2>(ctx));
   CT2G_LAUNCHED(ctx);
