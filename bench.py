@@ -216,6 +216,38 @@ def precision_form(args, g, P, n, local, kp, accuracy, stream):
             "fft": "y/x passes: tcgen05 DFT products, BF16 hi+lo operands, FP32 accumulation"}
 
 
+CAL_THRESHOLDS = (-4.4, -4.2, -4.0, -3.8, -3.6, -3.4, -3.2, -3.0)
+CAL_TARGET = 0.95e-4  # rms relative force error the calibration aims under
+
+
+def calibrate_threshold(gl, Pt, n, nsample, seed):
+    """The MLP threshold for the learned form, picked on the TRAINING state
+    (never on the state the form is judged on): the largest of CAL_THRESHOLDS
+    whose rms relative force error, against the FP64 Ewald sum on a seeded
+    sample of the training state's particles, is within CAL_TARGET (the
+    smallest threshold when none is).  Returns (threshold, table)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    sel = np.sort(rng.choice(n, size=min(n, nsample), replace=False))
+    truth = gl.ewald_direct(Pt["x"][sel], Pt["y"][sel], Pt["z"][sel])
+    tn = np.linalg.norm(truth, axis=1)
+    gl.upload_dict(Pt)
+    gl.particle_to_grid()
+    ids = gl.download()["id"]
+    inv = np.empty_like(ids)
+    inv[ids] = np.arange(len(ids), dtype=ids.dtype)
+    best, table = CAL_THRESHOLDS[0], []
+    for t in CAL_THRESHOLDS:
+        gl.learned_select("mlp", t)
+        gl.compute_forces()
+        f, _ = gl.forces()
+        rms = float(np.sqrt(np.mean((np.linalg.norm(f[inv[sel]] - truth, axis=1) / tn) ** 2)))
+        table.append({"threshold_log10": t, "rms_rel": rms,
+                      "cells_selected": int(gl.learned_cells()["nselected"])})
+        if rms <= CAL_TARGET:
+            best = t
+    return best, table
+
+
 def learned_form(args, P, n, soft, local, kp, accuracy):
     """Learned form: the plain stencil narrowed to --learned-base, and the
     cells an MLP selects widened back to --bwidth.  The MLP is trained first
@@ -237,8 +269,11 @@ def learned_form(args, P, n, soft, local, kp, accuracy):
     loss = gl.mlp_train(epochs=args.learned_epochs, batch=4096, lr=2e-3, seed=2)
     gl.synchronize()
     train_s = time.perf_counter() - t
+    thr, cal = args.learned_threshold, None
+    if thr is None:
+        thr, cal = calibrate_threshold(gl, Pt, n, 4096, args.seed + 101)
     gl.upload_dict(P)
-    gl.learned_select("mlp", args.learned_threshold)
+    gl.learned_select("mlp", thr)
     acc = accuracy(gl)
     nsel = gl.learned_cells()["nselected"]
     tune = gl.autotune(kp, args.dt, 1.0, cache_path=args.tune_cache)
@@ -257,7 +292,7 @@ def learned_form(args, P, n, soft, local, kp, accuracy):
     value, ms = replicas.job_throughput(n, e0.elapsed_time(e1) / args.steps, device="cuda")
     out = {"value": value, "ms_per_step": ms, "accuracy": acc, "tuning": tune,
            "base_bwidth": args.learned_base, "widened_to": args.bwidth,
-           "threshold_log10": args.learned_threshold, "cells_selected": int(nsel),
+           "threshold_log10": thr, "calibration": cal, "cells_selected": int(nsel),
            "training": {"cells": int(ncell), "epochs": args.learned_epochs, "mse": loss,
                         "seconds": train_s, "state": "same generator, seed + 100"}}
     gl.close()
@@ -338,17 +373,21 @@ def run_nfw(args, rank, world, local):
     t = time.perf_counter()
     Pt = ics.nfw_halos(n, seed=args.seed + 100 + rank)
     gl.upload_dict(Pt)
-    del Pt
     gl.particle_to_grid()
     ncell = gl.learned_collect()
     gl.mlp_init(seed=1)
     loss = gl.mlp_train(epochs=args.learned_epochs, batch=4096, lr=2e-3, seed=2)
     gl.synchronize()
     train_s = time.perf_counter() - t
+    thr, cal = args.learned_threshold, None
+    if thr is None:
+        thr, cal = calibrate_threshold(gl, Pt, n, max(1, int(round(0.2 * args.nfw_sample * n))),
+                                       args.seed + 101 + rank)
+    del Pt
     gl.learned_select("none")
     base_acc = errors(gl, truth)
     base_ms = timed(gl)
-    gl.learned_select("mlp", args.learned_threshold)
+    gl.learned_select("mlp", thr)
     learned_acc = errors(gl, truth)
     nsel = gl.learned_cells()["nselected"]
     learned_ms = timed(gl)
@@ -371,7 +410,7 @@ def run_nfw(args, rank, world, local):
                                           "accuracy": base_acc},
                           "learned": {"value": n / (learned_ms * 1e-3), "ms_per_step": learned_ms,
                                       "accuracy": learned_acc, "cells_selected": int(nsel),
-                                      "threshold_log10": args.learned_threshold,
+                                      "threshold_log10": thr, "calibration": cal,
                                       "training": {"cells": int(ncell), "mse": loss,
                                                    "seconds": train_s,
                                                    "state": "same generator, seed + 100"}}},
@@ -628,8 +667,9 @@ def main():
                     help="nfw256: fraction of particles judged against FP64 Ewald")
     ap.add_argument("--learned-base", type=float, default=3.0,
                     help="learned form: plain stencil of the base step (0: skip the form)")
-    ap.add_argument("--learned-threshold", type=float, default=-4.0,
-                    help="learned form: widen cells whose predicted log10 residual exceeds this")
+    ap.add_argument("--learned-threshold", type=float, default=None,
+                    help="learned form: widen cells whose predicted log10 residual exceeds "
+                         "this (default: calibrated on the training state)")
     ap.add_argument("--learned-epochs", type=int, default=30)
     ap.add_argument("--no-precision-form", dest="precision_form", action="store_false",
                     help="skip the tensor-core FFT form")

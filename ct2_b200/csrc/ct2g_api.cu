@@ -133,17 +133,16 @@ int ct2g_device_error(ct2g_ctx *ctx) {
 int ct2g_far_field(ct2g_ctx *ctx, bool pot) {
   CT2G_TRY(ensure_grid(ctx));
   ct2g_mark(ctx, 1);
-  if (ctx->moments_valid) return ct2g_mesh_solve(ctx, true, pot, false);
-  // the learned correction reads the moment grid; otherwise the moments are
-  // formed inside the forward z pass and never stored
-  if (ct2g_learned_active(ctx)) {
-    CT2G_TRY(ct2g_p2m(ctx));
-    ctx->moments_valid = true;
-    ctx->expansions_valid = false;
-    return ct2g_mesh_solve(ctx, true, pot, false);
-  }
+  if (ctx->moments_valid) return ct2g_mesh_solve(ctx, true, pot, CT2G_P2M_GRID);
+  // the moments are formed inside the forward z pass; the learned correction
+  // reads the moment grid, so then the pass stores them too
   ctx->expansions_valid = false;
-  return ct2g_mesh_solve(ctx, true, pot, true);
+  if (ct2g_learned_active(ctx)) {
+    CT2G_TRY(ct2g_mesh_solve(ctx, true, pot, CT2G_P2M_FUSED_STORE));
+    ctx->moments_valid = true;
+    return CT2G_OK;
+  }
+  return ct2g_mesh_solve(ctx, true, pot, CT2G_P2M_FUSED);
 }
 
 // upload the box table (offsets and GM) of the context

@@ -663,14 +663,15 @@ __device__ __forceinline__ void p2m_half(const uint32_t *__restrict__ px,
   }
 }
 
-template <int P, int N, bool GRID>
+template <int P, int N, int SRC>
 __global__ void __launch_bounds__(256, P <= 4 ? 3 : 2) fftz_p2m_r2c_kernel(
     const uint32_t *__restrict__ px, const uint32_t *__restrict__ py,
     const uint32_t *__restrict__ pz, const uint32_t *__restrict__ cs, int mbits,
-    const float *__restrict__ grid, int64_t CB, float2 *__restrict__ spec, int ldk,
+    float *__restrict__ grid, int64_t CB, float2 *__restrict__ spec, int ldk,
     const float2 *__restrict__ tw) {
   using LL = LineLayout<N, true>;
   constexpr int NC = ct2g_ncomp(P), NL = (NC + 1) / 2, NH = N / 2 + 1;
+  constexpr bool GRID = SRC == CT2G_P2M_GRID;
   constexpr int LB = GRID ? z_lines<P>() : 1;  // lines of this block
   extern __shared__ __align__(16) unsigned char smraw[];
   float2 *stw = reinterpret_cast<float2 *>(smraw);
@@ -728,6 +729,15 @@ __global__ void __launch_bounds__(256, P <= 4 ? 3 : 2) fftz_p2m_r2c_kernel(
     }
   }
   __syncthreads();
+  if constexpr (SRC == CT2G_P2M_FUSED_STORE) {
+    // the moments also go to the moment grid (for passes that read it)
+    float *g = grid + ((int64_t)box * N * N + (int64_t)line) * N;
+    for (int e = threadIdx.x; e < NC * N; e += 256) {
+      const int k = e / N, z = e % N;
+      g[(int64_t)k * CB + z] = sr[2 * LL::at(k >> 1, z, 0) + (k & 1)];
+    }
+    __syncthreads();
+  }
   tile_fft<N, true, float2, false>(s, LB * NL, 0, stw);
   // row L0 + lb = box * N^2 + line + lb; k-point k's components at k * NC
   const int64_t RS = (int64_t)ldk * NC;
@@ -750,11 +760,13 @@ __global__ void __launch_bounds__(256, P <= 4 ? 3 : 2) fftz_p2m_r2c_kernel(
 }
 
 template <int P, int N>
-int launch_p2m_r2c(ct2g_ctx *ctx, bool from_grid) {
+int launch_p2m_r2c(ct2g_ctx *ctx, int src) {
   constexpr int NL = (ct2g_ncomp(P) + 1) / 2;
-  const int LB = from_grid ? z_lines<P>() : 1;
+  const int LB = src == CT2G_P2M_GRID ? z_lines<P>() : 1;
   const size_t smem = sizeof(float2) * ((size_t)N + (size_t)LB * NL * LineLayout<N, true>::LS);
-  auto k = from_grid ? fftz_p2m_r2c_kernel<P, N, true> : fftz_p2m_r2c_kernel<P, N, false>;
+  auto k = src == CT2G_P2M_GRID    ? fftz_p2m_r2c_kernel<P, N, CT2G_P2M_GRID>
+           : src == CT2G_P2M_FUSED ? fftz_p2m_r2c_kernel<P, N, CT2G_P2M_FUSED>
+                                   : fftz_p2m_r2c_kernel<P, N, CT2G_P2M_FUSED_STORE>;
   CT2G_TRY(ct2g_smem_attrs(ctx, k, smem));
   k<<<(unsigned)((size_t)N * N * ctx->nbox / LB), 256, smem, ctx->stream>>>(
       ctx->x, ctx->y, ctx->z, ctx->cell_start, ctx->mbits, ctx->grid, ctx->CB, ctx->spec,
@@ -1095,7 +1107,7 @@ int spec_stage(ct2g_ctx *ctx, int stage, bool flag, int mode) {
   switch (ctx->M) {
 #define CT2G_SPEC_CASE(NN)                                                  \
   case NN:                                                                  \
-    if (stage == 0) return launch_p2m_r2c<P, NN>(ctx, flag);                \
+    if (stage == 0) return launch_p2m_r2c<P, NN>(ctx, mode);                \
     if (stage == 1) return launch_fx_mg2l<P, NN>(ctx);                      \
     if (stage == 2) return launch_c2r_l2p<P, NN>(ctx, mode);                \
     return spec_cols<NN>(ctx, flag, mode != 0);
@@ -1111,7 +1123,7 @@ int spec_stage(ct2g_ctx *ctx, int stage, bool flag, int mode) {
   return ct2g_fail(ctx, CT2G_EINVAL, "mesh must be a power of two in [8, 512]");
 }
 
-// stage 0: z pass (flag: from the moment grid); 1: fused X + MG2L; 2: inverse
+// stage 0: z pass (mode: CT2G_P2M_*); 1: fused X + MG2L; 2: inverse
 // z pass (mode 0/1/2 as fftz_c2r_l2p_kernel); 3: Y pass (mode 0) or X pass
 // (mode 1), inverse when flag
 int spec_run(ct2g_ctx *ctx, int stage, bool flag, int mode) {
@@ -1199,9 +1211,9 @@ bool ct2g_mg2l_fused(const ct2g_ctx *ctx) {
 }
 
 // z pass (P2M inside it, or from the moment grid), Y pass, X pass when split
-int ct2g_spec_forward(ct2g_ctx *ctx, bool p2m) {
+int ct2g_spec_forward(ct2g_ctx *ctx, int src) {
   CT2G_TRY(ct2g_twiddles(ctx, ctx->M));
-  CT2G_TRY(spec_run(ctx, 0, !p2m, 0));
+  CT2G_TRY(spec_run(ctx, 0, false, src));
   CT2G_TRY(spec_run(ctx, 3, false, 0));
   if (!ct2g_mg2l_fused(ctx)) CT2G_TRY(spec_run(ctx, 3, false, 1));
   return CT2G_OK;

@@ -360,6 +360,12 @@ void ct2g_learned_free(ct2g_ctx *ctx);
 int ct2g_near_window(ct2g_ctx *ctx, const uint2 *chunks, const uint32_t *nch, uint32_t *work,
                      const uint32_t *slist, const unsigned long long *stm, float lo2, float hi2,
                      bool pot, float *fx, float *fy, float *fz, float *po);
+// the same over the stencil masks stm for dense-style chunks (<= 32
+// consecutive sinks of one cell, (first particle, count)), persistent over
+// *nch / *work
+int ct2g_near_dense_window(ct2g_ctx *ctx, const uint2 *chunks, const uint32_t *nch,
+                           uint32_t *work, const unsigned long long *stm, bool pot, float *fx,
+                           float *fy, float *fz, float *po);
 // D^n phi_eps(-o h) for the offsets o (x,y,z triples) -> d_out[nshell][nc]
 int ct2g_shell_greens(ct2g_ctx *ctx, const std::vector<int> &offs3, float *d_out);
 // far field of the current range into the force buffers (P2M if needed, mesh
@@ -370,16 +376,20 @@ int ct2g_p2m(ct2g_ctx *ctx);
 // mesh solve; fused_l2p: the inverse z pass evaluates the far field of every
 // particle of the current range straight into the force buffers (the
 // expansion grid is not written)
-// fused_p2m: the moments are computed inside the forward z pass (the grid
-// is not written; ctx->grid then holds no moments)
-int ct2g_mesh_solve(ct2g_ctx *ctx, bool fused_l2p, bool pot, bool fused_p2m = false);
+// p2m: where the forward z pass takes the moments from --
+// CT2G_P2M_GRID the moment grid (already computed);
+// CT2G_P2M_FUSED computed inside the pass, not stored (ctx->grid then holds
+//   no moments);
+// CT2G_P2M_FUSED_STORE computed inside the pass and also written to the grid
+enum { CT2G_P2M_GRID = 0, CT2G_P2M_FUSED = 1, CT2G_P2M_FUSED_STORE = 2 };
+int ct2g_mesh_solve(ct2g_ctx *ctx, bool fused_l2p, bool pot, int p2m = CT2G_P2M_GRID);
 // Mesh-solve transforms on ctx->spec (ct2g_fft.cu).  Forward: the z pass
-// (P2M inside it when p2m, else from the moment grid), the Y pass, and the X
-// pass unless the X passes are fused with MG2L.  ct2g_spec_mg2l: the fused X
-// pass + MG2L + inverse X pass, or MG2L alone.  Inverse: the inverse X pass
-// (when not fused), the Y pass and the z pass (L2P inside it when l2p, else
-// into the expansion grid).
-int ct2g_spec_forward(ct2g_ctx *ctx, bool p2m);
+// (taking the moments as src says, CT2G_P2M_*), the Y pass, and the X pass
+// unless the X passes are fused with MG2L.  ct2g_spec_mg2l: the fused X pass
+// + MG2L + inverse X pass, or MG2L alone.  Inverse: the inverse X pass (when
+// not fused), the Y pass and the z pass (L2P inside it when l2p, else into
+// the expansion grid).
+int ct2g_spec_forward(ct2g_ctx *ctx, int src);
 int ct2g_spec_mg2l(ct2g_ctx *ctx);
 int ct2g_spec_inverse(ct2g_ctx *ctx, bool l2p, bool pot);
 // the X passes and MG2L run as one kernel for this context

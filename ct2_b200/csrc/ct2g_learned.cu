@@ -54,6 +54,8 @@ struct ct2g_learn {
   uint32_t *flags = nullptr;   // scratch
   uint32_t *scan = nullptr;    // scratch
   uint32_t *d_cnt = nullptr;   // [0] cells [1] selected cells [2] chunks [3] work counter
+                               // [4] sinks of the selected cells; widening: [5] dense
+                               // chunks [6] their work counter [7] sparse sinks
                                // [4] selected sinks [5] scan total scratch
   // block-walk form of the widening (bwidth_ext <= 4): stencil masks of the
   // shell per (in-block cell, neighbouring block), selected cells and sinks
@@ -73,6 +75,8 @@ struct ct2g_learn {
   float *pred = nullptr;       // MLP output
   uint8_t *sel = nullptr;      // selected
   uint2 *chunks = nullptr;     // (cell index, first sink << 8 | count)
+  uint2 *dchunks = nullptr;    // widening: dense-style chunks of selected dense cells
+  uint32_t *ssink2 = nullptr;  // widening: sinks of the selected sparse cells
   float *ex = nullptr, *ey = nullptr, *ez = nullptr;  // widened forces (training)
   // MLP
   float *params = nullptr, *grad = nullptr, *am = nullptr, *av = nullptr;
@@ -510,7 +514,7 @@ __global__ void sink_chunk_flag_kernel(const uint32_t *__restrict__ keys,
   cflag[q] = ((q - pscan[f]) % 32u) == 0u ? 1u : 0u;
 }
 
-__global__ void sink_chunk_fill_kernel(const uint32_t *__restrict__ cnt,
+__global__ void sink_chunk_fill_kernel(const uint32_t *__restrict__ nsink_ptr,
                                        const uint32_t *__restrict__ cflag,
                                        const uint32_t *__restrict__ cscan,
                                        const uint32_t *__restrict__ ssink,
@@ -519,12 +523,52 @@ __global__ void sink_chunk_fill_kernel(const uint32_t *__restrict__ cnt,
                                        const uint32_t *__restrict__ pscan, uint32_t begin,
                                        size_t nr, uint2 *__restrict__ chunks) {
   const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t nsink = cnt[4];
+  const uint32_t nsink = *nsink_ptr;
   if (q >= nsink || !cflag[q]) return;
   const uint32_t i = ssink[q] - begin;
   const uint32_t e = cs[(keys[i] | 63u) + 1] - begin;  // past the block
   const uint32_t qe = e < nr ? pscan[e] : nsink;
   chunks[cscan[q]] = make_uint2(q, min(32u, qe - q));
+}
+
+// the selected cells' sinks for the widened direct sum: cells of at least
+// dense_cell particles as dense-style chunks (every 32nd particle of the cell
+// starts one: dflag), the rest listed one by one (sflag)
+__global__ void shell_split_kernel(const uint32_t *__restrict__ cnt,
+                                   const uint32_t *__restrict__ sel_cells,
+                                   const uint32_t *__restrict__ cells,
+                                   const uint32_t *__restrict__ cs, uint32_t begin,
+                                   uint32_t dense_cell, uint32_t *__restrict__ dflag,
+                                   uint32_t *__restrict__ sflag) {
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= cnt[1]) return;
+  const uint32_t key = cells[sel_cells[j]];
+  const uint32_t c0 = cs[key], c1 = cs[key + 1];
+  if (c1 - c0 >= dense_cell) {
+    for (uint32_t i = c0; i < c1; i += 32) dflag[i - begin] = 1u;
+  } else {
+    for (uint32_t i = c0; i < c1; i++) sflag[i - begin] = 1u;
+  }
+}
+
+// (first particle, count) of each dense-style chunk
+__global__ void shell_dense_fill_kernel(const uint32_t *__restrict__ dflag,
+                                        const uint32_t *__restrict__ dscan,
+                                        const uint32_t *__restrict__ keys,
+                                        const uint32_t *__restrict__ cs, uint32_t begin, size_t nr,
+                                        uint2 *__restrict__ list) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nr || !dflag[i]) return;
+  const uint32_t g = begin + (uint32_t)i;
+  list[dscan[i]] = make_uint2(g, min(32u, cs[keys[i] + 1] - g));
+}
+
+// the listed (sparse) sinks, in particle order
+__global__ void shell_sparse_list_kernel(const uint32_t *__restrict__ sflag,
+                                         const uint32_t *__restrict__ sscan, uint32_t begin,
+                                         size_t nr, uint32_t *__restrict__ list) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nr && sflag[i]) list[sscan[i]] = begin + (uint32_t)i;
 }
 
 // the mesh's Taylor term of the shell, once per selected cell: warp per
@@ -778,10 +822,12 @@ __global__ void loss_sum_kernel(const float *__restrict__ l, int n, float *__res
 int free_learn_cells(ct2g_learn *L) {
   void *ptrs[] = {L->cells, L->flags, L->scan, L->X, L->score, L->pred, L->sel, L->chunks,
                   L->ex, L->ey, L->ez, L->sel_cells, L->pflag, L->pscan, L->ssink, L->scell,
-                  L->cflag, L->cscan, L->lsub};
+                  L->cflag, L->cscan, L->lsub, L->dchunks, L->ssink2};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   L->sel_cells = L->pflag = L->pscan = L->ssink = L->scell = L->cflag = L->cscan = nullptr;
+  L->dchunks = nullptr;
+  L->ssink2 = nullptr;
   L->lsub = nullptr;
   if (L->mc) cudaFree(L->mc);
   L->mc = nullptr;
@@ -807,6 +853,8 @@ int learn_cells_alloc(ct2g_ctx *ctx) {
   A(L->pred, cap * 4);
   A(L->sel, cap);
   A(L->chunks, cap * sizeof(uint2));
+  A(L->dchunks, cap * sizeof(uint2));
+  A(L->ssink2, cap * 4);
   A(L->ex, cap * 4);
   A(L->ey, cap * 4);
   A(L->ez, cap * 4);
@@ -979,21 +1027,41 @@ int widen_block_p(ct2g_ctx *ctx, bool pot, float *fx, float *fy, float *fz, floa
   sink_list_kernel<<<G, T, 0, st>>>(L->d_cnt, L->sel_cells, L->cells, ctx->cell_start, begin,
                                     L->pscan, L->ssink, L->scell);
   CT2G_LAUNCHED(ctx);
+  // the widened direct sum: selected dense cells through the near kernel's
+  // dense path (chunks of one cell, count d_cnt[5], work counter d_cnt[6]),
+  // the sinks of the other selected cells (count d_cnt[7]) in sparse-style
+  // chunks per 4x4x4 block (count d_cnt[2], work counter d_cnt[3]); flags,
+  // scan, pflag and pscan are free again here
+  CT2G_CUDA(ctx, cudaMemsetAsync(L->flags, 0, sizeof(uint32_t) * nr, st));
+  CT2G_CUDA(ctx, cudaMemsetAsync(L->pflag, 0, sizeof(uint32_t) * nr, st));
+  shell_split_kernel<<<G, T, 0, st>>>(L->d_cnt, L->sel_cells, L->cells, ctx->cell_start, begin,
+                                      ctx->dense_cell, L->flags, L->pflag);
+  CT2G_LAUNCHED(ctx);
+  CT2G_TRY(ct2g_scan_exclusive(ctx, L->flags, L->scan, nr, L->d_cnt + 5, 0));
+  shell_dense_fill_kernel<<<G, T, 0, st>>>(L->flags, L->scan, ctx->keys, ctx->cell_start, begin,
+                                           nr, L->dchunks);
+  CT2G_LAUNCHED(ctx);
+  CT2G_TRY(ct2g_scan_exclusive(ctx, L->pflag, L->pscan, nr, L->d_cnt + 7, 0));
+  shell_sparse_list_kernel<<<G, T, 0, st>>>(L->pflag, L->pscan, begin, nr, L->ssink2);
+  CT2G_LAUNCHED(ctx);
   CT2G_CUDA(ctx, cudaMemsetAsync(L->cflag, 0, sizeof(uint32_t) * nr, st));
   sink_chunk_flag_kernel<<<G, T, 0, st>>>(ctx->keys, ctx->cell_start, L->pflag, L->pscan, begin,
                                           nr, L->cflag);
   CT2G_LAUNCHED(ctx);
   CT2G_TRY(ct2g_scan_exclusive(ctx, L->cflag, L->cscan, nr, L->d_cnt + 2, 0));
-  sink_chunk_fill_kernel<<<G, T, 0, st>>>(L->d_cnt, L->cflag, L->cscan, L->ssink, ctx->keys,
+  sink_chunk_fill_kernel<<<G, T, 0, st>>>(L->d_cnt + 7, L->cflag, L->cscan, L->ssink2, ctx->keys,
                                           ctx->cell_start, L->pscan, begin, nr, L->chunks);
   CT2G_LAUNCHED(ctx);
   CT2G_CUDA(ctx, cudaMemsetAsync(L->d_cnt + 3, 0, sizeof(uint32_t), st));
+  CT2G_CUDA(ctx, cudaMemsetAsync(L->d_cnt + 6, 0, sizeof(uint32_t), st));
   shell_m2l_kernel<P><<<warp_grid(ctx, nr), 256, 0, st>>>(
       L->d_cnt, L->sel_cells, L->cells, L->mc, L->idx, geo_of(ctx), L->d_shell, L->d_shellG,
       L->nshell, L->lsub);
   CT2G_LAUNCHED(ctx);
   const float bw = ctx->opt.bwidth, bx = L->bw_ext;
-  CT2G_TRY(ct2g_near_window(ctx, L->chunks, L->d_cnt + 2, L->d_cnt + 3, L->ssink, L->d_stm,
+  CT2G_TRY(ct2g_near_dense_window(ctx, L->dchunks, L->d_cnt + 5, L->d_cnt + 6, L->d_stm, pot, fx,
+                                  fy, fz, po));
+  CT2G_TRY(ct2g_near_window(ctx, L->chunks, L->d_cnt + 2, L->d_cnt + 3, L->ssink2, L->d_stm,
                             bw * bw, bx * bx, pot, fx, fy, fz, po));
   if (pot)
     shell_l2p_kernel<P, true><<<G, T, 0, st>>>(L->d_cnt, L->ssink, L->scell, ctx->keys, begin,

@@ -516,10 +516,10 @@ int ct2g_p2m(ct2g_ctx *ctx) {
 
 // forward FFT of the moments, MG2L, inverse FFT into the expansions (the
 // expansion grid, or straight into the forces)
-int ct2g_mesh_solve(ct2g_ctx *ctx, bool fused_l2p, bool pot, bool fused_p2m) {
+int ct2g_mesh_solve(ct2g_ctx *ctx, bool fused_l2p, bool pot, int p2m) {
   CT2G_TRY(ct2g_build_greens(ctx));
   ct2g_mark(ctx, 2);
-  CT2G_TRY(ct2g_spec_forward(ctx, fused_p2m));
+  CT2G_TRY(ct2g_spec_forward(ctx, p2m));
   ct2g_mark(ctx, 3);
   CT2G_TRY(ct2g_spec_mg2l(ctx));
   ct2g_mark(ctx, 4);

@@ -440,6 +440,27 @@ int ct2g_near_window(ct2g_ctx *ctx, const uint2 *chunks, const uint32_t *nch, ui
                                                             nullptr);
 }
 
+// direct sum over the cells of the stencil masks stm for dense-style chunks
+// (<= 32 consecutive sinks of one cell), added into the given force buffers
+int ct2g_near_dense_window(ct2g_ctx *ctx, const uint2 *chunks, const uint32_t *nch,
+                           uint32_t *work, const unsigned long long *stm, bool pot, float *fx,
+                           float *fy, float *fz, float *po) {
+  const Walk walk = make_walk(ctx->mbits);
+  if (ctx->opt.kernel == CT2G_SOFT_SPHERE)
+    return pot ? launch_near1<CT2G_SOFT_SPHERE, true, false>(ctx, walk, chunks, nch, nullptr, work,
+                                                             nullptr, stm, -1.f, 0.f, fx, fy, fz,
+                                                             po, nullptr)
+               : launch_near1<CT2G_SOFT_SPHERE, false, false>(ctx, walk, chunks, nch, nullptr,
+                                                              work, nullptr, stm, -1.f, 0.f, fx,
+                                                              fy, fz, po, nullptr);
+  return pot ? launch_near1<CT2G_SOFT_PLUMMER, true, false>(ctx, walk, chunks, nch, nullptr, work,
+                                                            nullptr, stm, -1.f, 0.f, fx, fy, fz,
+                                                            po, nullptr)
+             : launch_near1<CT2G_SOFT_PLUMMER, false, false>(ctx, walk, chunks, nch, nullptr,
+                                                             work, nullptr, stm, -1.f, 0.f, fx, fy,
+                                                             fz, po, nullptr);
+}
+
 int ct2g_upload_stencil(ct2g_ctx *ctx, const std::vector<int> &st4) {
   CT2G_CUDA(ctx, cudaMemcpyToSymbolAsync(c_stencil, st4.data(), sizeof(int) * st4.size(), 0,
                                          cudaMemcpyHostToDevice, ctx->stream));

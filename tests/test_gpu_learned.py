@@ -92,9 +92,8 @@ def test_features_match_oracle(gpu):
     g.learned_select("fixed", 1e30)  # features and scores, nothing selected
     g.compute_forces()
     f1, _ = g.forces()
-    # with the correction on, P2M runs as its own pass (the features read the
-    # moment grid) instead of inside the forward z pass: same sums, different
-    # FP32 pairing in the transform
+    # with the correction on, the forward z pass also stores the moments (the
+    # features read the moment grid); the mesh arithmetic is the same
     rel = np.linalg.norm(f1 - f0, axis=1) / np.linalg.norm(f0, axis=1)
     assert rel.max() < 1e-5
     c = g.learned_cells()
