@@ -216,7 +216,7 @@ def precision_form(args, g, P, n, local, kp, accuracy, stream):
             "fft": "y/x passes: tcgen05 DFT products, BF16 hi+lo operands, FP32 accumulation"}
 
 
-CAL_THRESHOLDS = (-4.4, -4.2, -4.0, -3.8, -3.6, -3.4, -3.2, -3.0)
+CAL_THRESHOLDS = tuple(round(-4.5 + 0.1 * k, 1) for k in range(16))  # -4.5 .. -3.0
 CAL_TARGET = 0.95e-4  # rms relative force error the calibration aims under
 
 

@@ -205,17 +205,22 @@ __global__ void keys_kernel(const uint32_t *__restrict__ x, const uint32_t *__re
 
 // per-cell particle counts of the sorted range (cell_start = begin + their
 // exclusive scan)
+// particles per cell (counts, zero on entry) and the occupancy bit of every
+// occupied cell (occ, zero on entry), from the sorted keys: the first
+// particle of a run of equal keys subtracts its index, the last adds its
+// index + 1 (two atomics per occupied cell, none per particle, so a crowded
+// cell costs no more than an empty one)
 __global__ void cell_count_kernel(const uint32_t *__restrict__ skeys, size_t nr,
-                                  uint32_t *__restrict__ counts) {
+                                  uint32_t *__restrict__ counts,
+                                  unsigned long long *__restrict__ occ) {
   size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nr) return;
   const uint32_t k = skeys[i];
-  // one atomic per run of equal keys
   if (i == 0 || skeys[i - 1] != k) {
-    size_t e = i + 1;
-    while (e < nr && skeys[e] == k) e++;
-    counts[k] = (uint32_t)(e - i);
+    atomicAdd(counts + k, 0u - (uint32_t)i);
+    atomicOr(occ + (k >> 6), 1ull << (k & 63u));
   }
+  if (i + 1 == nr || skeys[i + 1] != k) atomicAdd(counts + k, (uint32_t)(i + 1));
 }
 
 // gather the active range into cell order; write the direct-sum source records
@@ -327,23 +332,6 @@ __global__ void chunk_fill_kernel(const uint32_t *__restrict__ flags,
   if (flags[i]) list[fscan[i]] = (uint32_t)(begin + i);
 }
 
-// occupancy of every 4x4x4 cell block: a block is 64 consecutive Morton keys,
-// bit b of word w set when cell 64w+b holds a particle of the range
-__global__ void occupancy_kernel(const uint32_t *__restrict__ cs, size_t nwords,
-                                 unsigned long long *__restrict__ occ) {
-  const size_t w = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (w >= nwords) return;
-  const uint32_t *c = cs + 64 * w;
-  unsigned long long bits = 0;
-  uint32_t prev = c[0];
-#pragma unroll 8
-  for (int b = 0; b < 64; b++) {
-    const uint32_t next = c[b + 1];
-    if (next > prev) bits |= 1ull << b;
-    prev = next;
-  }
-  occ[w] = bits;
-}
 
 // the gathered (cell-ordered) store goes back into the primary buffers, so
 // that every step reads and writes the same addresses (a recorded graph
@@ -450,7 +438,8 @@ int ct2g_bin_range(ct2g_ctx *ctx) {
       ctx->vals2 = t;
     }
     CT2G_CUDA(ctx, cudaMemsetAsync(ctx->cell_start, 0, sizeof(uint32_t) * (ctx->CB + 1), st));
-    cell_count_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(ctx->keys, nr, ctx->cell_start);
+    CT2G_CUDA(ctx, cudaMemsetAsync(ctx->occ, 0, sizeof(unsigned long long) * (ctx->CB / 64), st));
+    cell_count_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(ctx->keys, nr, ctx->cell_start, ctx->occ);
     CT2G_LAUNCHED(ctx);
     CT2G_TRY(ct2g_scan_exclusive(ctx, ctx->cell_start, ctx->cell_start, (size_t)ctx->CB + 1,
                                  nullptr, (uint32_t)begin));
@@ -462,9 +451,6 @@ int ct2g_bin_range(ct2g_ctx *ctx) {
     copy_back_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(
         begin, nr, ctx->x2, ctx->y2, ctx->z2, ctx->vx2, ctx->vy2, ctx->vz2, ctx->rung2, ctx->id2,
         ctx->x, ctx->y, ctx->z, ctx->vx, ctx->vy, ctx->vz, ctx->rung, ctx->id);
-    CT2G_LAUNCHED(ctx);
-    occupancy_kernel<<<ct2g_div_up(ctx->CB / 64, T), T, 0, st>>>(ctx->cell_start, ctx->CB / 64,
-                                                                ctx->occ);
     CT2G_LAUNCHED(ctx);
     // near-field work lists (scratch: flags, vals, vals2, x2, y2 are free here)
     chunk_flag_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(ctx->keys, ctx->cell_start, begin, nr,
