@@ -35,6 +35,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -66,7 +67,10 @@ class ClockSampler:
     def __init__(self, device):
         self.device = device
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", "clocks_rank%d.csv" % device)
+        # the raw samples: CT2G_CLOCKS_DIR when set (to keep them), else a
+        # temporary directory
+        out = os.environ.get("CT2G_CLOCKS_DIR") or tempfile.mkdtemp(prefix="ct2g_clocks_")
+        self.path = os.path.join(out, "clocks_rank%d.csv" % device)
 
     def start(self):
         try:
