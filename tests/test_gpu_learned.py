@@ -212,3 +212,31 @@ def test_learned_step_records_into_graph(gpu):
     for k in ("x", "y", "z", "vx", "vy", "vz", "rung", "id"):
         assert np.array_equal(da[k], db[k]), k
     assert a.learned_cells()["nselected"] == b.learned_cells()["nselected"]
+
+
+def test_widened_all_matches_wide_context_at_scale(gpu):
+    # 200k particles in 20 spheres on a 64^3 mesh: many cells hold more than
+    # one warp of sinks, so every widening path runs (dense-style chunks of
+    # one cell, several per crowded cell, and sparse-style chunks); widening
+    # every cell must give the forces of a context run with the wider stencil
+    mbits, p, bw, bwx = 6, 4, 3.0, 4.0
+    n = 200000
+    P = ics.plummer_spheres(n, seed=21, nspheres=20, a=2.0 / (1 << mbits))
+    soft, GM = 0.02 / (1 << mbits), 1.0 / n
+    wide = Gravity(mesh=1 << mbits, order=p, bwidth=bwx, hsoft=soft, GM=GM)
+    wide.upload_dict(P)
+    wide.particle_to_grid()
+    wide.compute_forces()
+    fw, _ = wide.forces()
+    g = Gravity(mesh=1 << mbits, order=p, bwidth=bw, hsoft=soft, GM=GM)
+    g.upload_dict(P)
+    g.learned_enable(bwx)
+    g.learned_select("all")
+    g.particle_to_grid()
+    g.compute_forces()
+    f, _ = g.forces()
+    assert np.array_equal(g.download()["id"], wide.download()["id"])
+    cs_b, cs_e = g.cells()
+    assert (cs_e - cs_b).max() > 64  # crowded cells exist
+    e = _rel(f, fw)
+    assert np.sqrt(np.mean(e ** 2)) < 1e-5 and e.max() < 1e-3
