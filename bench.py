@@ -849,9 +849,14 @@ def main():
     peaks = _peaks()
     M, nc = args.mesh, (args.order + 1) * (args.order + 2) * (args.order + 3) // 6
     CK = M * M * (M // 2 + 1)
-    algo_bytes = {"bin": 66.0 * n, "p2m": 12.0 * n + 4.0 * nc * M ** 3,
-                  "fft_fwd": nc * (4.0 * M ** 3 + 8.0 * CK), "mg2l": 20.0 * nc * CK,
-                  "fft_inv": nc * (4.0 * M ** 3 + 8.0 * CK), "update_drift": 61.0 * n}
+    # algorithmic HBM bytes per stage of the step as it runs here: fft_fwd =
+    # P2M inside the z pass (particles in, spectrum out) + the y pass (one
+    # read, one write); mg2l = the fused x pass + Green's multiply + inverse x
+    # pass (spectrum and Green's table in, spectrum out); fft_inv = the y pass
+    # + the z pass with L2P (spectrum in; particle offsets in, forces out)
+    algo_bytes = {"bin": 66.0 * n, "p2m": 0.0,
+                  "fft_fwd": 24.0 * nc * CK + 12.0 * n, "mg2l": 20.0 * nc * CK,
+                  "fft_inv": 24.0 * nc * CK + 28.0 * n, "update_drift": 61.0 * n}
     k = int(np.argmax(st))
     dom = names[k]
     if dom == "forces":
@@ -874,6 +879,11 @@ def main():
                 "unit": "GB/s", "frac": ach / peaks["hbm"], "traffic": None,
                 "peak_source": peaks["source"]}
     stages = {nm: float(t) for nm, t in zip(names, st)}
+    # the HBM-bound stages against the measured copy bandwidth
+    stage_roof = {nm: {"algorithmic_bytes": algo_bytes[nm],
+                       "achieved_gbs": algo_bytes[nm] / (st[i] * 1e-3) / 1e9,
+                       "frac": algo_bytes[nm] / (st[i] * 1e-3) / 1e9 / peaks["hbm"]}
+                  for i, nm in enumerate(names) if nm in ("fft_fwd", "mg2l", "fft_inv") and st[i] > 0}
 
     cb = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -889,7 +899,8 @@ def main():
                 "data": "synthetic: seeded Plummer spheres + uniform background",
                 "config": _config(args, world), "e2e": e2e, "gpu_launches": int(launches),
                 "roofline": roof, "cpu_baseline": cb, "clocks": ck, "accuracy": acc,
-                "forms": forms, "stage_ms": stages, "interactions_per_step": inter / args.steps}
+                "forms": forms, "stage_ms": stages, "stage_roofline": stage_roof,
+                "interactions_per_step": inter / args.steps}
         print(json.dumps(line), flush=True)
     g.close()
     if dist:
