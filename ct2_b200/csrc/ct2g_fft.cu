@@ -664,7 +664,7 @@ __device__ __forceinline__ void p2m_half(const uint32_t *__restrict__ px,
 }
 
 template <int P, int N, int SRC>
-__global__ void __launch_bounds__(256, P <= 4 ? 3 : 2) fftz_p2m_r2c_kernel(
+__global__ void __launch_bounds__(256, P <= 4 ? 4 : 2) fftz_p2m_r2c_kernel(
     const uint32_t *__restrict__ px, const uint32_t *__restrict__ py,
     const uint32_t *__restrict__ pz, const uint32_t *__restrict__ cs, int mbits,
     float *__restrict__ grid, int64_t CB, float2 *__restrict__ spec, int ldk,
@@ -708,8 +708,9 @@ __global__ void __launch_bounds__(256, P <= 4 ? 3 : 2) fftz_p2m_r2c_kernel(
         continue;
       }
       const uint32_t uz = ((uint32_t)zc << sh) + halfc;
-      p2m_half<P, N, 0, NC / 2>(px, py, pz, b, e, 1, false, ux, uy, uz, zc, sr, true);
-      p2m_half<P, N, NC / 2, NC>(px, py, pz, b, e, 1, false, ux, uy, uz, zc, sr, true);
+      p2m_half<P, N, 0, NC / 3>(px, py, pz, b, e, 1, false, ux, uy, uz, zc, sr, true);
+      p2m_half<P, N, NC / 3, 2 * NC / 3>(px, py, pz, b, e, 1, false, ux, uy, uz, zc, sr, true);
+      p2m_half<P, N, 2 * NC / 3, NC>(px, py, pz, b, e, 1, false, ux, uy, uz, zc, sr, true);
       if (NC & 1) sr[2 * LL::at(NL - 1, zc, 0) + 1] = 0.f;
     }
     __syncthreads();
@@ -720,10 +721,12 @@ __global__ void __launch_bounds__(256, P <= 4 ? 3 : 2) fftz_p2m_r2c_kernel(
         const uint32_t key = (box << (3 * mbits)) | ct2g_morton(cx, cy, zc);
         const uint32_t b = cs[key], e = cs[key + 1];
         const uint32_t uz = (zc << sh) + halfc;
-        p2m_half<P, N, 0, NC / 2>(px, py, pz, b + lane, e, 32, true, ux, uy, uz, (int)zc, sr,
+        p2m_half<P, N, 0, NC / 3>(px, py, pz, b + lane, e, 32, true, ux, uy, uz, (int)zc, sr,
                                   lane == 0);
-        p2m_half<P, N, NC / 2, NC>(px, py, pz, b + lane, e, 32, true, ux, uy, uz, (int)zc, sr,
-                                   lane == 0);
+        p2m_half<P, N, NC / 3, 2 * NC / 3>(px, py, pz, b + lane, e, 32, true, ux, uy, uz,
+                                           (int)zc, sr, lane == 0);
+        p2m_half<P, N, 2 * NC / 3, NC>(px, py, pz, b + lane, e, 32, true, ux, uy, uz, (int)zc,
+                                       sr, lane == 0);
         if ((NC & 1) && lane == 0) sr[2 * LL::at(NL - 1, (int)zc, 0) + 1] = 0.f;
       }
     }
@@ -784,7 +787,7 @@ int launch_p2m_r2c(ct2g_ctx *ctx, int src) {
 // of box b / N^2.  MODE 0: forces, 1: forces and potentials, 2: no L2P, the
 // expansions go to the expansion grid (layout as the moment grid).
 template <int P, int N, int MODE>
-__global__ void __launch_bounds__(256) fftz_c2r_l2p_kernel(
+__global__ void __launch_bounds__(256, 5) fftz_c2r_l2p_kernel(
     const float2 *__restrict__ spec, int ldk, const uint32_t *__restrict__ cs,
     const float4 *__restrict__ src, int mbits, const float *__restrict__ box_gm,
     float *__restrict__ ofx, float *__restrict__ ofy, float *__restrict__ ofz,
