@@ -663,8 +663,10 @@ __device__ __forceinline__ void p2m_half(const uint32_t *__restrict__ px,
   }
 }
 
+// occupancy: 4 blocks per SM up to order 4 (64 registers); at N = 512 the
+// 32-point in-register DFTs need more registers than that, so 2
 template <int P, int N, int SRC>
-__global__ void __launch_bounds__(256, P <= 4 ? 4 : 2) fftz_p2m_r2c_kernel(
+__global__ void __launch_bounds__(256, N >= 512 ? 2 : P <= 4 ? 4 : 2) fftz_p2m_r2c_kernel(
     const uint32_t *__restrict__ px, const uint32_t *__restrict__ py,
     const uint32_t *__restrict__ pz, const uint32_t *__restrict__ cs, int mbits,
     float *__restrict__ grid, int64_t CB, float2 *__restrict__ spec, int ldk,
@@ -786,8 +788,10 @@ int launch_p2m_r2c(ct2g_ctx *ctx, int src) {
 // expansion grid itself is never written to HBM.  Block b is line b % N^2
 // of box b / N^2.  MODE 0: forces, 1: forces and potentials, 2: no L2P, the
 // expansions go to the expansion grid (layout as the moment grid).
+// occupancy: 5 blocks per SM (48 registers) below N = 512, whose 32-point
+// in-register DFTs need more
 template <int P, int N, int MODE>
-__global__ void __launch_bounds__(256, 5) fftz_c2r_l2p_kernel(
+__global__ void __launch_bounds__(256, N >= 512 ? 1 : 5) fftz_c2r_l2p_kernel(
     const float2 *__restrict__ spec, int ldk, const uint32_t *__restrict__ cs,
     const float4 *__restrict__ src, int mbits, const float *__restrict__ box_gm,
     float *__restrict__ ofx, float *__restrict__ ofy, float *__restrict__ ofz,
