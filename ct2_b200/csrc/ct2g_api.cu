@@ -748,6 +748,12 @@ int ct2g_kick_step(ct2g_ctx *ctx, int *minrung_io, int max_rung, double scale, d
   CT2G_TRY(check(ctx));
   if (!minrung_io) return ct2g_fail(ctx, CT2G_EINVAL, "null minrung");
   int &minrung = *minrung_io;
+  // every level above minrung pops a range pushed by an earlier call's
+  // descending levels; refuse before any work if the stack is short (the
+  // reference would read an empty std::stack, particle.cpp:31-34)
+  if (max_rung > minrung && ctx->rung_stack.size() < (size_t)(max_rung - minrung))
+    return ct2g_fail(ctx, CT2G_ESTATE,
+                     "kick_step: the rung stack holds fewer levels than max_rung - minrung");
   std::vector<int> levels(std::max(max_rung - minrung, 0) + 1);
   int k = 0;
   for (int i = max_rung; i > minrung; i--) levels[k++] = i;
@@ -798,7 +804,10 @@ int ct2g_kick_step(ct2g_ctx *ctx, int *minrung_io, int max_rung, double scale, d
     if (ascending && !top) CT2G_TRY(ct2g_pop_rungs(ctx));
   }
   if (clip_top) minrung++;
-  if (out_max_rung) *out_max_rung = mr;
+  // the reference returns its max_rung argument: the max_rung declared in
+  // its loop body (main.cpp:68) shadows the parameter and is out of scope at
+  // the return (main.cpp:90)
+  if (out_max_rung) *out_max_rung = max_rung;
   return CT2G_OK;
 }
 

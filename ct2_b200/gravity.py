@@ -316,8 +316,10 @@ class Gravity:
                     fft_tile=t.fft_tile, split_mg2l=t.split_mg2l)
 
     def kick_step(self, minrung, max_rung, scale, adot, tau, t0, minrung0, nocrop=False):
-        """Returns (max_rung, minrung) -- the reference returns max_rung and
-        updates minrung through its reference argument."""
+        """Returns (value, minrung): the reference's return value, which is its
+        max_rung argument (main.cpp:68 shadows it, :90 returns the parameter),
+        and minrung as updated through its reference argument.  The highest
+        rung after the step is len(rung_counts()) - 1."""
         mr = ctypes.c_int(minrung)
         out = ctypes.c_int(0)
         self._chk(self._l.ct2g_kick_step(self._h, ctypes.byref(mr), max_rung, scale, adot, tau,

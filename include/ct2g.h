@@ -158,7 +158,14 @@ int ct2g_drift(ct2g_ctx *ctx, float dt, float scale);
  * double tau, double t0, int minrung0, bool nocrop) (cosmictiger/kick.hpp:23,
  * src/main.cpp:8-92): the rung-hierarchical KDK step, GPU-resident.
  * *minrung is updated like the reference's reference argument; the return
- * value of the reference goes to *out_max_rung. */
+ * value of the reference goes to *out_max_rung (may be NULL).  That value is
+ * the max_rung argument itself: in the reference the max_rung that each level
+ * declares from kick() (main.cpp:68) shadows the parameter and has gone out of
+ * scope at the return (main.cpp:90).  The highest rung after the step, which
+ * the next call's max_rung should be, is ct2g_rung_counts' *nrungs - 1.  The
+ * rung stack carries over between calls as in the reference: a call whose
+ * max_rung is above minrung pops one level per rung above it, pushed by the
+ * previous call's descending levels (CT2G_ESTATE if the stack runs out). */
 int ct2g_kick_step(ct2g_ctx *ctx, int *minrung, int max_rung, double scale, double adot,
                    double tau, double t0, int minrung0, int nocrop, int *out_max_rung);
 

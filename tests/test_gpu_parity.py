@@ -46,6 +46,29 @@ def test_binning_bit_exact(gpu, mbits, n):
     assert np.array_equal(g.download()["id"], d["id"])
 
 
+@pytest.mark.parametrize("n,ppcell", [(5000, 64), (32768, 16), (23000, 1)])
+def test_binning_matches_reference_fixture(gpu, n, ppcell):
+    """Against the reference's own compiled bisection (tests/golden/
+    ref_binning.npz): the same cells, in the same order, with the same
+    particles in each; only the order inside a cell (arbitrary in the
+    reference's Hoare partition) is the stable one."""
+    import os
+    g0 = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_binning.npz"))
+    order = g0["order_%d_%d" % (n, ppcell)].astype(np.int64)
+    mesh = int(g0["ncell_%d_%d" % (n, ppcell)])
+    mbits = mesh.bit_length() - 1
+    P = ics.plummer_spheres(n, seed=3, nspheres=4, a=0.02)
+    g = _ctx(mbits, 2, 1.0, 1e-3)
+    g.upload_dict(P)
+    g.particle_to_grid()
+    ids = g.download()["id"].astype(np.int64)
+    keys = O.cell_keys(P["x"], P["y"], P["z"], mbits).astype(np.int64)
+    assert np.array_equal(keys[ids], keys[order])
+    b, e = g.cells()
+    for c in np.flatnonzero(e > b):
+        assert np.array_equal(np.sort(ids[b[c]:e[c]]), np.sort(order[b[c]:e[c]]))
+
+
 def test_binning_empty_and_single(gpu):
     g = _ctx(3, 1, 1.0, 1e-3)
     one = ics.lattice(1, seed=0)
