@@ -104,6 +104,13 @@ SYMBOLS = [
     ("ct2g_fft_r2c_3d", _I, [_P, _P, _P, _I, _I]),
     ("ct2g_fft_c2r_3d", _I, [_P, _P, _P, _I, _I]),
     ("ct2g_fft3d_f32_dev", _I, [_P, _I, _P, _P, _I, _I]),
+    ("ct2g_fft1d_real", _I, [_P, _P, _I, _I, _I]),
+    ("ct2g_fft1d_complex", _I, [_P, _P, _I, _I, _I]),
+    ("ct2g_scramble", _I, [_P, _P, _I, _I, _I]),
+    ("ct2g_transpose_yz", _I, [_P, _P, _I]),
+    ("ct2g_transpose_r2c", _I, [_P, _P, _P, _I]),
+    ("ct2g_transpose_c2r", _I, [_P, _P, _P, _I]),
+    ("ct2g_twiddles", _I, [_P, _I, _I, _P]),
     ("ct2g_ewald_direct", _I, [_P, _P, _P, _P, _SZ, _D, _D, _I, _P, _P]),
     ("ct2g_ewald_direct_noalloc", _I, [_I, _P, _P, _P, _SZ, _P, _P, _P, _SZ, _I, _D, _D, _D, _D,
                                        _I, _P, _P, _P]),

@@ -12,6 +12,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <map>
 #include <mutex>
 #include <sstream>
 
@@ -291,6 +292,50 @@ void particles_init() {
   invalidate_caches();
 }
 
+// Raw SoA particle files (no counterpart in the reference, whose only
+// initial-condition path is particles_init): an 8-byte magic "CT2SOA1", the
+// count as uint64, then the x, y, z (uint32 fixed point), vx, vy, vz (float)
+// and rung (int8) arrays, little-endian, as ct2_b200/ics.py writes them.
+namespace {
+const char kSoaMagic[8] = {'C', 'T', '2', 'S', 'O', 'A', '1', 0};
+}
+
+void particles_save(const std::string &path) {
+  std::ofstream f(path, std::ios::binary);
+  if (!f) throw ct2_error(CT2G_EINVAL, "particles_save: cannot open " + path);
+  const uint64_t n = g_x.size();
+  f.write(kSoaMagic, 8);
+  f.write(reinterpret_cast<const char *>(&n), 8);
+  f.write(reinterpret_cast<const char *>(g_x.data()), 4 * n);
+  f.write(reinterpret_cast<const char *>(g_y.data()), 4 * n);
+  f.write(reinterpret_cast<const char *>(g_z.data()), 4 * n);
+  f.write(reinterpret_cast<const char *>(g_vx.data()), 4 * n);
+  f.write(reinterpret_cast<const char *>(g_vy.data()), 4 * n);
+  f.write(reinterpret_cast<const char *>(g_vz.data()), 4 * n);
+  f.write(g_rung.data(), n);
+  if (!f) throw ct2_error(CT2G_EINVAL, "particles_save: write failed for " + path);
+}
+
+void particles_load(const std::string &path) {
+  std::ifstream f(path, std::ios::binary);
+  if (!f) throw ct2_error(CT2G_EINVAL, "particles_load: cannot open " + path);
+  char magic[8];
+  uint64_t n = 0;
+  f.read(magic, 8);
+  f.read(reinterpret_cast<char *>(&n), 8);
+  if (!f || std::memcmp(magic, kSoaMagic, 8) != 0)
+    throw ct2_error(CT2G_EINVAL, "particles_load: not a particle file: " + path);
+  particle_allocate((size_t)n);
+  f.read(reinterpret_cast<char *>(g_x.data()), 4 * n);
+  f.read(reinterpret_cast<char *>(g_y.data()), 4 * n);
+  f.read(reinterpret_cast<char *>(g_z.data()), 4 * n);
+  f.read(reinterpret_cast<char *>(g_vx.data()), 4 * n);
+  f.read(reinterpret_cast<char *>(g_vy.data()), 4 * n);
+  f.read(reinterpret_cast<char *>(g_vz.data()), 4 * n);
+  f.read(g_rung.data(), n);
+  if (!f) throw ct2_error(CT2G_EINVAL, "particles_load: file too short: " + path);
+}
+
 size_t particle_count() { return g_x.size(); }
 pos_fixed &particle_x(int i) { g_host_dirty = true; return g_x[i]; }
 pos_fixed &particle_y(int i) { g_host_dirty = true; return g_y[i]; }
@@ -438,6 +483,58 @@ void fft_r2c_3d(fft_float *xin, fft_float *xout, int N) {
 void fft_c2r_3d(fft_float *xin, fft_float *xout, int N) {
   check(ct2g_fft_c2r_3d(ctx(), xin, xout, N, 1), "fft_c2r_3d");
 }
+
+// ---------------------------------------------------------------- 1D FFT --
+static_assert(sizeof(fft_simd) == 4 * sizeof(double), "fft_simd is four doubles");
+static_assert(sizeof(ct2::complex<fft_simd>) == 8 * sizeof(double), "complex<fft_simd> layout");
+
+void fft_real(fft_float *X, int N, int dir) {
+  check(ct2g_fft1d_real(ctx(), X, N, 1, dir), "fft_real");
+}
+
+void fft_real(fft_simd *X, int N, int dir) {
+  check(ct2g_fft1d_real(ctx(), reinterpret_cast<double *>(X), N, 4, dir), "fft_real");
+}
+
+void fft_complex(ct2::complex<fft_simd> *X, int N, int dir) {
+  check(ct2g_fft1d_complex(ctx(), reinterpret_cast<double *>(X), N, 4, dir), "fft_complex");
+}
+
+void scramble(fft_float *X, int N1, int N2, int N3) {
+  check(ct2g_scramble(ctx(), X, N1, N2, N3), "scramble");
+}
+
+void transpose_yz(fft_float *X, int N) { check(ct2g_transpose_yz(ctx(), X, N), "transpose_yz"); }
+
+void transpose_r2c(fft_float *xin, fft_float *xout, int N) {
+  check(ct2g_transpose_r2c(ctx(), xin, xout, N), "transpose_r2c");
+}
+
+void transpose_c2r(fft_float *xin, fft_float *xout, int N) {
+  check(ct2g_transpose_c2r(ctx(), xin, xout, N), "transpose_c2r");
+}
+
+// twiddle tables, cached per N like the reference's (src/fft/twiddles.cpp);
+// the references stay valid for the life of the process
+namespace {
+const std::vector<fft_float> &twiddle_table(int which, int N) {
+  static std::mutex mu;
+  static std::map<std::pair<int, int>, std::vector<fft_float>> tables;
+  std::lock_guard<std::mutex> lk(mu);
+  auto key = std::make_pair(which, N);
+  auto it = tables.find(key);
+  if (it == tables.end()) {
+    std::vector<fft_float> w((size_t)std::max(N, 0));
+    if (N > 0) check(ct2g_twiddles(ctx(), which, N, w.data()), "twiddles");
+    it = tables.emplace(key, std::move(w)).first;
+  }
+  return it->second;
+}
+}  // namespace
+
+const std::vector<fft_float> &cos_twiddles(int N) { return twiddle_table(0, N); }
+const std::vector<fft_float> &sin_twiddles(int N) { return twiddle_table(1, N); }
+const std::vector<fft_float> &inv_sin_twiddles(int N) { return twiddle_table(2, N); }
 
 // ---------------------------------------------------------------- cosmology --
 // src/cosmology.cpp restated: Friedmann expansion rate, an SSP-RK3 update of

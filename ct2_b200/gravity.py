@@ -351,6 +351,41 @@ class Gravity:
         return c[:nr.value].astype(np.int64)
 
     # -- FFT ----------------------------------------------------------------
+    def fft1d_real(self, X, N, lanes=1, dir=1):
+        """fft_real (fft.hpp:25-26) in place on a float64 array: input in
+        bit-reversed order, output halfcomplex; lanes interleaved."""
+        assert X.dtype == np.float64 and X.flags.c_contiguous and X.size >= N * lanes
+        self._chk(self._l.ct2g_fft1d_real(self._h, _ptr(X), N, lanes, dir))
+
+    def fft1d_complex(self, X, N, lanes=1, dir=1):
+        """fft_complex (fft.hpp:27) in place: element n of lane l at
+        X[(2n)*lanes + l] (real) and X[(2n+1)*lanes + l] (imaginary)."""
+        assert X.dtype == np.float64 and X.flags.c_contiguous and X.size >= 2 * N * lanes
+        self._chk(self._l.ct2g_fft1d_complex(self._h, _ptr(X), N, lanes, dir))
+
+    def scramble(self, X, N1, N2, N3):
+        assert X.dtype == np.float64 and X.flags.c_contiguous and X.size >= N1 * N2 * N3
+        self._chk(self._l.ct2g_scramble(self._h, _ptr(X), N1, N2, N3))
+
+    def transpose_yz(self, X, N):
+        assert X.dtype == np.float64 and X.flags.c_contiguous and X.size >= N ** 3
+        self._chk(self._l.ct2g_transpose_yz(self._h, _ptr(X), N))
+
+    def transpose_r2c(self, xin, xout, N):
+        xin = np.ascontiguousarray(xin, np.float64)
+        assert xout.dtype == np.float64 and xout.size >= 2 * N * N * (N // 2 + 1)
+        self._chk(self._l.ct2g_transpose_r2c(self._h, _ptr(xin), _ptr(xout), N))
+
+    def transpose_c2r(self, xin, xout, N):
+        xin = np.ascontiguousarray(xin, np.float64)
+        assert xout.dtype == np.float64 and xout.size >= N ** 3
+        self._chk(self._l.ct2g_transpose_c2r(self._h, _ptr(xin), _ptr(xout), N))
+
+    def twiddles(self, which, N):
+        out = np.zeros(N, np.float64)
+        self._chk(self._l.ct2g_twiddles(self._h, which, N, _ptr(out)))
+        return out
+
     def fft_r2c_3d(self, x):
         """x: float64 [batch,]N,N,N -> split planes float64 [batch,] 2*N*N*(N/2+1)."""
         x = np.ascontiguousarray(x, np.float64)

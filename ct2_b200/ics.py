@@ -129,3 +129,35 @@ def batch_boxes(nboxes: int = 96, seed: int = 0, log2_min: float = 12.0,
         box["mesh"] = mesh
         out.append(box)
     return out
+
+
+SOA_MAGIC = b"CT2SOA1\x00"
+
+
+def save_soa(path, d):
+    """Write particles as the raw SoA file the C++ layer's particles_save /
+    particles_load use: magic, uint64 count, x y z (uint32), vx vy vz
+    (float32), rung (int8)."""
+    n = len(d["x"])
+    with open(path, "wb") as f:
+        f.write(SOA_MAGIC)
+        f.write(np.uint64(n).tobytes())
+        for k, t in (("x", np.uint32), ("y", np.uint32), ("z", np.uint32), ("vx", np.float32),
+                     ("vy", np.float32), ("vz", np.float32)):
+            f.write(np.ascontiguousarray(d[k], t).tobytes())
+        f.write(np.ascontiguousarray(d.get("rung", np.zeros(n, np.int8)), np.int8).tobytes())
+
+
+def load_soa(path):
+    with open(path, "rb") as f:
+        if f.read(8) != SOA_MAGIC:
+            raise ValueError("not a particle file: %s" % path)
+        n = int(np.frombuffer(f.read(8), np.uint64)[0])
+        out = {}
+        for k, t in (("x", np.uint32), ("y", np.uint32), ("z", np.uint32), ("vx", np.float32),
+                     ("vy", np.float32), ("vz", np.float32), ("rung", np.int8)):
+            b = f.read(n * np.dtype(t).itemsize)
+            if len(b) != n * np.dtype(t).itemsize:
+                raise ValueError("file too short: %s" % path)
+            out[k] = np.frombuffer(b, t).copy()
+    return out

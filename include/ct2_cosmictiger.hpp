@@ -77,6 +77,8 @@ struct kick_params {
   float scale;
 };
 
+// returns its max_rung argument, as the reference does (the max_rung its
+// loop body declares, main.cpp:68, shadows the parameter returned at :90)
 int kick_step(int &minrung, int max_rung, double scale, double adot, double tau, double t0,
               int minrung0, bool nocrop);             // kick.hpp:23, main.cpp:8-92
 int kick(const kick_params &params);                  // kick.hpp:24, kick.cpp:105-125
@@ -84,6 +86,42 @@ void drift(float dt, float scale);                    // drift.hpp:12, drift.cpp
 
 void fft_r2c_3d(fft_float *xin, fft_float *xout, int N);  // fft.hpp:28
 void fft_c2r_3d(fft_float *xin, fft_float *xout, int N);  // fft.hpp:29
+
+// The 1D FFT surface, cosmictiger/fft.hpp:18-27.  The reference's fft_simd is
+// sfmm::simd_f64 with FFT_SIMD_SIZE = 4 lanes (cosmictiger/cosmictiger.hpp:12,19)
+// and its complex type sfmm::complex<T>; sfmm is not part of the reference
+// tree, so these are layout-compatible stand-ins: fft_simd is four doubles,
+// ct2::complex<fft_simd> the four real lanes followed by the four imaginary
+// lanes (an sfmm array of the same shape can be passed by reinterpret_cast).
+// Inputs of fft_real / fft_complex are in bit-reversed order (scramble
+// first); dir = -1 is the transform with exp(+2 pi i n k / N).  Computed on
+// the GPU in FP64 (ct2g_fft1d_real / ct2g_fft1d_complex).
+namespace ct2 {
+struct simd_f64 {
+  double v[4];
+  double &operator[](int i) { return v[i]; }
+  double operator[](int i) const { return v[i]; }
+};
+template <class T>
+struct complex {
+  T re, im;
+  T &real() { return re; }
+  T &imag() { return im; }
+  const T &real() const { return re; }
+  const T &imag() const { return im; }
+};
+}  // namespace ct2
+using fft_simd = ct2::simd_f64;                                       // cosmictiger.hpp:19
+void transpose_yz(fft_float *X, int N);                               // fft.hpp:18
+void transpose_r2c(fft_float *xin, fft_float *xout, int N);           // fft.hpp:19
+void transpose_c2r(fft_float *xin, fft_float *xout, int N);           // fft.hpp:20
+void scramble(fft_float *X, int N1, int N2, int N3);                  // fft.hpp:21
+const std::vector<fft_float> &cos_twiddles(int N);                    // fft.hpp:22
+const std::vector<fft_float> &sin_twiddles(int N);                    // fft.hpp:23
+const std::vector<fft_float> &inv_sin_twiddles(int N);                // fft.hpp:24
+void fft_real(fft_float *X, int N, int dir = 1);                      // fft.hpp:25
+void fft_real(fft_simd *X, int N, int dir = 1);                       // fft.hpp:26
+void fft_complex(ct2::complex<fft_simd> *X, int N, int dir = 1);      // fft.hpp:27
 
 // cosmictiger/particle.hpp:22-73 and src/particle.cpp
 void particle_allocate(size_t count);                 // particle.cpp:273
@@ -107,6 +145,11 @@ std::vector<std::pair<size_t, size_t>> particle_cell_neighbors(int i, int j, int
 int particle_cell_dim();                              // particle.hpp:69
 std::pair<size_t, size_t> particle_get_cell(int i, int j, int k);  // particle.hpp:70
 std::vector<double> particle_get_expansion(int i, int j, int k);   // particle.hpp:71
+// Raw SoA particle files: no counterpart in the reference (its only initial
+// conditions come from particles_init).  Magic "CT2SOA1\0", uint64 count,
+// then x, y, z (uint32), vx, vy, vz (float), rung (int8) arrays.
+void particles_save(const std::string &path);
+void particles_load(const std::string &path);
 
 // cosmictiger/cosmology.hpp:13-16
 double cosmos_conformal_time(double a0, double a1);

@@ -306,6 +306,49 @@ int ct2g_rung_counts(ct2g_ctx *ctx, size_t *counts, int nmax, int *nrungs);
  * batch transforms of consecutive arrays.  N: power of two, 4..512. */
 int ct2g_fft_r2c_3d(ct2g_ctx *ctx, const double *xin, double *xout, int N, int batch);
 int ct2g_fft_c2r_3d(ct2g_ctx *ctx, const double *xin, double *xout, int N, int batch);
+/* The reference's 1D FFT surface (cosmictiger/fft.hpp:18-27), computed on the
+ * GPU in FP64; host arrays, transformed in place.  Several independent
+ * sequences ("lanes") interleave element by element like the reference's
+ * 4-lane SIMD type: real element n of lane l at X[n*lanes + l]; complex
+ * element n at X[(2n)*lanes + l] (real part) and X[(2n+1)*lanes + l]
+ * (imaginary part).  Inputs arrive in bit-reversed order (scrambled, as
+ * src/fft/fft_test.cpp:81-159 prepares them); dir = +1 is the forward DFT
+ * sum_n x(n) exp(-2 pi i n k/N), dir = -1 the same with exp(+2 pi i n k/N)
+ * (the reference's dir = -1 path is not a usable transform; this is the one
+ * its inverse twiddle table, src/fft/twiddles.cpp:44-56, describes).
+ * N: power of two, 2..8192.
+ *   ct2g_fft1d_real:    fft_real(fft_float*, N, dir) with lanes = 1 and
+ *                       fft_real(fft_simd*, N, dir) with lanes = 4
+ *                       (fft.hpp:25-26, src/fft/fft_real_scalar.cpp,
+ *                       fft_real_vector.cpp); output in halfcomplex order:
+ *                       X[0], Re X(1)..Re X(N/2), Im X(N/2-1)..Im X(1).
+ *   ct2g_fft1d_complex: fft_complex(complex<fft_simd>*, N, dir) with lanes =
+ *                       4 (fft.hpp:27, src/fft/fft_complex_vector.cpp);
+ *                       output in natural order. */
+int ct2g_fft1d_real(ct2g_ctx *ctx, double *X, int N, int lanes, int dir);
+int ct2g_fft1d_complex(ct2g_ctx *ctx, double *X, int N, int lanes, int dir);
+/* scramble(X, N1, N2, N3) (fft.hpp:21, src/fft/scramble.cpp:26-43): in each
+ * of N1 blocks of N2 rows of N3 values, row j trades places with row
+ * bitrev(j).  N2: power of two. */
+int ct2g_scramble(ct2g_ctx *ctx, double *X, int N1, int N2, int N3);
+/* transpose_yz(X, N) (fft.hpp:18, src/fft/transpose.cpp:7-31,118-120): X[ix][iy][iz]
+ * becomes X[ix][iz][iy].  (The reference swaps every pair twice, which leaves
+ * X unchanged; this is the transpose its 3D drivers rely on.)  N <= 512. */
+int ct2g_transpose_yz(ct2g_ctx *ctx, double *X, int N);
+/* transpose_r2c(xin, xout, N) (fft.hpp:19, src/fft/transpose.cpp:33-72):
+ * xin[N][N][N] holds halfcomplex rows along y; xout receives the split planes,
+ * re[(ix*N+iz)*(N/2+1)+iy] = xin[ix][iy][iz] and im[same] = xin[ix][N-iy][iz]
+ * (0 at iy = 0, N/2) at offset N*N*(N/2+1).  N even, <= 512. */
+int ct2g_transpose_r2c(ct2g_ctx *ctx, const double *xin, double *xout, int N);
+/* transpose_c2r(xin, xout, N) (fft.hpp:20, src/fft/transpose.cpp:74-116):
+ * the inverse of ct2g_transpose_r2c.  (The reference reads its input with a
+ * row stride of N where transpose_r2c writes N/2+1, and starts its z loop at
+ * the block's y coordinate; this is the inverse both are meant to be.) */
+int ct2g_transpose_c2r(ct2g_ctx *ctx, const double *xin, double *xout, int N);
+/* cos_twiddles / sin_twiddles / inv_sin_twiddles (fft.hpp:22-24,
+ * src/fft/twiddles.cpp): out[n] = cos(-2 pi n/N) (which 0), sin(-2 pi n/N)
+ * (which 1), sin(2 pi n/N) (which 2), n < N. */
+int ct2g_twiddles(ct2g_ctx *ctx, int which, int N, double *out);
 /* FP32 device-pointer variant on the context stream, interleaved complex
  * output (float2[batch][N][N][N/2+1]); dir = +1 forward r2c, -1 inverse c2r */
 int ct2g_fft3d_f32_dev(ct2g_ctx *ctx, int dir, void *d_real, void *d_complex, int N,

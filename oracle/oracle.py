@@ -311,6 +311,11 @@ def ref_fft_lib():
     L.ref_fft_real.argtypes = [_f64p, _int, _int]
     L.ref_scramble.argtypes = [_f64p, _int, _int, _int]
     L.ref_fft_complex4.argtypes = [_f64p, _int, _int]
+    L.ref_fft_real4.argtypes = [_f64p, _int, _int]
+    L.ref_transpose_yz.argtypes = [_f64p, _int]
+    L.ref_transpose_r2c.argtypes = [_f64p, _f64p, _int]
+    L.ref_transpose_c2r.argtypes = [_f64p, _f64p, _int]
+    L.ref_twiddles.argtypes = [_int, _int, _f64p]
     _REF = L
     return L
 

@@ -43,7 +43,7 @@ def test_library_exports_reference_cxx_interface():
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
     src = re.sub(r"//[^\n]*", "", src)
     names = set(re.findall(r"^\s*[\w:&<>, *]+?\b(\w+)\(", src, flags=re.M))
-    names -= {"ct2_error"}
+    names -= {"ct2_error", "real", "imag"}  # constructor, inline accessors of ct2::complex
     out = subprocess.run(["nm", "-DC", "--defined-only", _lib.LIB_PATH], capture_output=True,
                          text=True, check=True).stdout
     for n in sorted(names):
@@ -91,3 +91,17 @@ def test_drop_in_program_compiles(tmp_path):
                     "drop_in.cpp"), "-L" + os.path.dirname(_lib.LIB_PATH), "-lct2g",
                     "-Wl,-rpath," + os.path.dirname(_lib.LIB_PATH), "-o", str(exe)], check=True)
     assert exe.exists()
+
+
+def test_reference_fft_surface_signatures():
+    """The C++ names of the reference's 1D FFT surface (fft.hpp:18-27) are
+    exported with their argument types."""
+    out = subprocess.run(["nm", "-DC", "--defined-only", _lib.LIB_PATH], capture_output=True,
+                         text=True, check=True).stdout
+    for sig in ("fft_real(double*, int, int)", "fft_real(ct2::simd_f64*, int, int)",
+                "fft_complex(ct2::complex<ct2::simd_f64>*, int, int)",
+                "scramble(double*, int, int, int)", "transpose_yz(double*, int)",
+                "transpose_r2c(double*, double*, int)", "transpose_c2r(double*, double*, int)",
+                "cos_twiddles(int)", "sin_twiddles(int)", "inv_sin_twiddles(int)",
+                "fft_r2c_3d(double*, double*, int)", "fft_c2r_3d(double*, double*, int)"):
+        assert sig in out, sig

@@ -40,10 +40,13 @@ def config1():
     GM = float(np.float32(1.0 / n))
     g = Gravity(mesh=1 << MBITS, order=ORDER, bwidth=BW, hsoft=soft, GM=GM)
     g.upload_dict(P)
+    # the cell ranges of the initial positions (kick_step bins them again:
+    # the stable sort of a sorted store is the identity)
+    g.particle_to_grid()
+    b, e = g.cells()
     val, minrung = g.kick_step(0, 0, 1.0, 1.0, 1.0, DT, 0)
     d = g.download()
     f, _ = g.forces()
-    b, e = g.cells()
     g.close()
     r = O.method_forces(P["x"], P["y"], P["z"], MBITS, ORDER, 0, soft, BW, GM)
     return dict(P=P, n=n, soft=soft, GM=GM, val=val, minrung=minrung, d=d, f=f, b=b, e=e, r=r)

@@ -143,3 +143,32 @@ def test_reference_rung_partition_and_stack():
     counts = (ctypes.c_size_t * 16)()
     m = L.ref_rung_counts(counts, 16)
     assert list(counts[:m]) == [int(c) for c in a.rung_counts()]
+
+
+@pytest.mark.skipif(O.ref_fft_lib() is None, reason="oracle/_ref not built here")
+def test_reference_transposes_as_compiled():
+    """What the reference's layout helpers compute (src/fft/transpose.cpp),
+    next to what the library implements: transpose_r2c is the documented
+    gather; transpose_yz swaps every pair twice and leaves X unchanged;
+    transpose_c2r does not invert transpose_r2c (row stride N instead of
+    N/2+1 on its input, z loop started at the block's y)."""
+    L = O.ref_fft_lib()
+    N = 8
+    rng = np.random.Generator(np.random.PCG64(9))
+    x = rng.uniform(size=N ** 3)
+    X = x.copy()
+    L.ref_transpose_yz(X, N)
+    assert np.array_equal(X, x)
+    Y = np.zeros(2 * N * N * (N // 2 + 1))
+    L.ref_transpose_r2c(np.ascontiguousarray(x), Y, N)
+    h = N // 2 + 1
+    xr = x.reshape(N, N, N)
+    re = Y[: N * N * h].reshape(N, N, h)
+    im = Y[N * N * h:].reshape(N, N, h)
+    for iy in range(h):
+        assert np.array_equal(re[:, :, iy], xr[:, iy, :])
+        want = 0.0 if iy in (0, N // 2) else xr[:, N - iy, :]
+        assert np.array_equal(im[:, :, iy], np.broadcast_to(want, (N, N)))
+    back = np.zeros(N ** 3)
+    L.ref_transpose_c2r(Y, back, N)
+    assert not np.array_equal(back, x)
