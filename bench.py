@@ -117,40 +117,73 @@ def workload(args, rank):
     return P, n
 
 
-def cpu_baseline(args):
-    """CPU oracle (C + numpy, all host threads) on a bounded sample of the
-    workload: the same generator scaled to 1/64 of the particles and mesh
-    cells (same particles per cell and sphere size in cells)."""
-    from ct2_b200 import ics
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
+def _oracle_step_seconds(P, mbits, order, soft, bwidth, dt, reps=2):
+    """Best-of-reps wall time of one CPU-oracle kick+drift (forces, update,
+    drift) on particles P; the Green's table is built first and not timed (it
+    is cached per mesh in the reference's design and here)."""
     from oracle import oracle as O
-    ng = args.ngrid // 4
-    mesh = args.mesh // 4
-    mbits = int(np.log2(mesh))
-    nsph = max(1, args.nspheres // 64)
-    P = ics.plummer_spheres(ng ** 3, seed=args.seed, nspheres=nsph, a=args.a * 4)
-    n = ng ** 3
-    soft = 1.0 / (50 * args.ngrid) * 4
-    Gk = O.greens_k(mbits, args.order, 0, soft, args.bwidth)  # cached per mesh, not timed
+    n = len(P["x"])
+    Gk = O.greens_k(mbits, order, 0, soft, bwidth)
     times = []
-    for _ in range(2):
+    for _ in range(reps):
         t = time.perf_counter()
-        r = O.method_forces(P["x"], P["y"], P["z"], mbits, args.order, 0, soft, args.bwidth,
-                            1.0 / n, Gk=Gk)
+        r = O.method_forces(P["x"], P["y"], P["z"], mbits, order, 0, soft, bwidth, 1.0 / n, Gk=Gk)
         f = (r["ffar"] + r["fnear"]).astype(np.float32)
         perm = r["perm"]
         vx, vy, vz, rung, mr = O.kick_update(P["vx"][perm], P["vy"][perm], P["vz"][perm],
                                              P["rung"][perm], f[:, 0], f[:, 1], f[:, 2],
                                              ascending=1, descending=1, top=1, first=0, prung=0,
-                                             t0=args.dt, eta=0.15, max_dt=0.01, scale=1.0,
+                                             t0=dt, eta=0.15, max_dt=0.01, scale=1.0,
                                              hsoft=soft)
-        O.drift(r["xs"], r["ys"], r["zs"], vx, vy, vz, args.dt, 1.0)
+        O.drift(r["xs"], r["ys"], r["zs"], vx, vy, vz, dt, 1.0)
         times.append(time.perf_counter() - t)
+    return min(times)
+
+
+def _sample_shape(args):
+    """The bounded CPU sample of the workload: the same generator scaled to
+    1/64 of the particles and mesh cells (same particles per cell, sphere
+    size in cells and softening in cells)."""
+    ng, mesh = args.ngrid // 4, args.mesh // 4
+    return ng, mesh, max(1, args.nspheres // 64)
+
+
+def cpu_baseline(args, config1=True):
+    """CPU oracle (C + numpy, all host threads) on a bounded sample of the
+    workload (_sample_shape), and on the CPU parity configuration (32^3
+    lattice + 0.1-spacing noise, 64^3 mesh, bwidth 3, order 4, eps = 1/1600)."""
+    from ct2_b200 import ics
+    ng, mesh, nsph = _sample_shape(args)
+    P = ics.plummer_spheres(ng ** 3, seed=args.seed, nspheres=nsph, a=args.a * 4)
+    n = ng ** 3
+    soft = 1.0 / (50 * args.ngrid) * 4
+    sec = _oracle_step_seconds(P, int(np.log2(mesh)), args.order, soft, args.bwidth, args.dt)
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count()))
-    return {"value": n / min(times), "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": "CPU oracle, one full kick+drift on the workload generator scaled to "
-                      "%d^3 particles, %d spheres, %d^3 mesh, order %d, bwidth %g (1/64 of the "
-                      "particles and cells); Green's table excluded (cached per mesh)"
-                      % (ng, nsph, mesh, args.order, args.bwidth)}
+    out = {"value": n / sec, "unit": UNIT, "cores": cores, "kind": "port",
+           "cpu_model": cpu_model(),
+           "sample": "CPU oracle, one full kick+drift (best of 2) on the workload generator "
+                     "scaled to %d^3 particles, %d spheres, %d^3 mesh, order %d, bwidth %g (1/64 "
+                     "of the particles and cells; particles/s extrapolates per particle); "
+                     "Green's table excluded (cached per mesh)"
+                     % (ng, nsph, mesh, args.order, args.bwidth)}
+    if config1:
+        L = ics.lattice(32, seed=0, sigma_cells=0.1)
+        s1 = _oracle_step_seconds(L, 6, 4, float(np.float32(1.0 / 1600)), 3.0, 1e-3)
+        out["config1"] = {"workload": "lattice_32cubed_mesh64 (32^3 lattice + 0.1-spacing noise, "
+                                      "64^3 mesh, bwidth 3, order 4, eps 1/1600, dt 1e-3)",
+                          "particles_per_s": 32768 / s1, "seconds_per_step": s1}
+    return out
 
 
 def run_reference(args, rank, world):
@@ -161,17 +194,26 @@ def run_reference(args, rank, world):
         return
     os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
     for _ in range(args.warmup):
-        cpu_baseline(args)
+        cpu_baseline(args, config1=False)
     vals = []
     for _ in range(args.steps):
-        vals.append(cpu_baseline(args))
+        vals.append(cpu_baseline(args, config1=False))
     v = min(x["value"] for x in vals)
     cb = dict(vals[0])
     cb["value"] = v
+    ng, mesh, nsph = _sample_shape(args)
+    cfg = dict(_config(args, world))
+    cfg.update({"workload": "plummer_spheres_%dcubed_mesh%d" % (ng, mesh),
+                "particles_per_gpu": ng ** 3, "mesh": mesh, "spheres": nsph,
+                "softening": "plummer eps=1/(50*%d) (the same in cells)" % ng,
+                "sample_of": _config(args, world)["workload"],
+                "sample": "1/64 of the particles and mesh cells of the GPU workload (same "
+                          "particles per cell, sphere size and softening in cells); value is "
+                          "particles/s of this sample"})
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": _config(args, world), "cpu_baseline": cb,
+            "config": cfg, "cpu_baseline": cb,
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -864,14 +906,10 @@ def main():
         sms = torch.cuda.get_device_properties(local).multi_processor_count
         peak = sms * 128 * 2 * peaks["sm_max_mhz"] * 1e6 / 1e12
         ach = flops / (st[k] * 1e-3) / 1e12
-        # DRAM bytes of the two near-field launches of one step, from the ncu
-        # capture summarised in profiles/near_kernel_128cubed_mesh256_bw4_ncu_full.md
-        # (default workload only)
-        default = (args.ngrid, args.mesh, args.bwidth, args.nspheres) == (128, 256, 4.0, 512)
+        # DRAM traffic is not measured inside this run (no profiler here):
+        # null, with the ncu figures kept beside the kernel's profile
         roof = {"kernel": "forces (direct sum)", "bound": "fp32", "achieved": ach, "peak": peak,
-                "unit": "TFLOP/s", "frac": ach / peak,
-                "traffic": (44.171e6 + 0.504e6 + 116.976e6 + 11.257e6) if default else None,
-                "traffic_unit": "bytes per step (dense + sparse launch)",
+                "unit": "TFLOP/s", "frac": ach / peak, "traffic": None,
                 "peak_source": "derived: SMs x 128 x 2 x max SM clock (no measured FP32 peak)"}
     else:
         ach = algo_bytes[dom] / (st[k] * 1e-3) / 1e9

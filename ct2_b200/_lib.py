@@ -27,7 +27,7 @@ class Options(ctypes.Structure):
 class Tuning(ctypes.Structure):
     _fields_ = [("dense_cell", ctypes.c_int), ("near_blocks_per_sm", ctypes.c_int),
                 ("fft_tile", ctypes.c_int), ("split_mg2l", ctypes.c_int),
-                ("reserved", ctypes.c_int * 4)]
+                ("sparse_path", ctypes.c_int), ("reserved", ctypes.c_int * 3)]
 
 
 STEP_GRAPH = 1
@@ -115,6 +115,7 @@ SYMBOLS = [
     ("ct2g_ewald_direct_noalloc", _I, [_I, _P, _P, _P, _SZ, _P, _P, _P, _SZ, _I, _D, _D, _D, _D,
                                        _I, _P, _P, _P]),
     ("ct2g_tc_selftest", _I, [_I, _P, _P, _I, _I, _P]),
+    ("ct2g_wait_selftest", _I, [_P, ctypes.c_uint32]),
     ("ct2g_set_fft_mode", _I, [_P, _I]),
     ("ct2g_stream", _P, [_P]),
     ("ct2g_synchronize", _I, [_P]),

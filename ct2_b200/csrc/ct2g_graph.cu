@@ -340,6 +340,7 @@ int ct2g_get_tuning(const ct2g_ctx *ctx, ct2g_tuning *t) {
   t->near_blocks_per_sm = ctx->near_blocks_per_sm;
   t->fft_tile = ctx->fft_tile;
   t->split_mg2l = ctx->split_mg2l;
+  t->sparse_path = ctx->sparse_path;
   return CT2G_OK;
 }
 
@@ -347,12 +348,13 @@ int ct2g_set_tuning(ct2g_ctx *ctx, const ct2g_tuning *t) {
   if (!ctx || !t) return CT2G_EINVAL;
   if (t->dense_cell < 1 || t->dense_cell > 4096 || t->near_blocks_per_sm < 0 ||
       t->near_blocks_per_sm > 32 || t->fft_tile < 0 || t->fft_tile > 512 ||
-      (t->split_mg2l != 0 && t->split_mg2l != 1))
+      (t->split_mg2l != 0 && t->split_mg2l != 1) || (t->sparse_path != 0 && t->sparse_path != 1))
     return ct2g_fail(ctx, CT2G_EINVAL, "tuning out of range");
   ctx->dense_cell = (uint32_t)t->dense_cell;
   ctx->near_blocks_per_sm = t->near_blocks_per_sm;
   ctx->fft_tile = t->fft_tile;
   ctx->split_mg2l = t->split_mg2l;
+  ctx->sparse_path = t->sparse_path;
   ctx->epoch++;  // launch shapes are part of a recorded graph
   ctx->grid_valid = false;  // the chunk lists depend on dense_cell
   return CT2G_OK;
@@ -375,7 +377,8 @@ int ct2g_autotune(ct2g_ctx *ctx, const ct2g_kick_params *p, float dt, float scal
       ct2g_tuning t;
       std::memset(&t, 0, sizeof(t));
       double ms = 0;
-      if (ls >> k >> t.dense_cell >> t.near_blocks_per_sm >> t.fft_tile >> ms && k == key &&
+      if (ls >> k >> t.dense_cell >> t.near_blocks_per_sm >> t.fft_tile >> t.sparse_path >> ms &&
+          k == key &&
           ct2g_set_tuning(ctx, &t) == CT2G_OK) {
         if (out) *out = t;
         return CT2G_OK;
@@ -402,16 +405,20 @@ int ct2g_autotune(ct2g_ctx *ctx, const ct2g_kick_params *p, float dt, float scal
     return CT2G_OK;
   };
   if (rc == CT2G_OK) rc = time_one(best, best_ms);
-  // coordinate descent over the three shapes
+  // coordinate descent over the four shapes
   const int W = ctx->M >= 256 ? 16 : 4096 / ctx->M;
   std::vector<std::vector<int>> cand = {
       {8, 12, 16, 24, 32, 48},  // dense_cell
       {0, 1, 2},                // near_blocks_per_sm
-      ctx->M >= 64 ? std::vector<int>{0, W / 2, 2 * W} : std::vector<int>{0}};
-  for (int dim = 0; dim < 3 && rc == CT2G_OK; dim++) {
+      ctx->M >= 64 ? std::vector<int>{0, W / 2, 2 * W} : std::vector<int>{0},
+      {0, 1}};                  // sparse_path
+  for (int dim = 0; dim < 4 && rc == CT2G_OK; dim++) {
     for (int v : cand[dim]) {
       ct2g_tuning t = best;
-      int *field = dim == 0 ? &t.dense_cell : dim == 1 ? &t.near_blocks_per_sm : &t.fft_tile;
+      int *field = dim == 0 ? &t.dense_cell
+                   : dim == 1 ? &t.near_blocks_per_sm
+                   : dim == 2 ? &t.fft_tile
+                              : &t.sparse_path;
       if (*field == v) continue;
       *field = v;
       float ms = 0.f;
@@ -433,7 +440,9 @@ int ct2g_autotune(ct2g_ctx *ctx, const ct2g_kick_params *p, float dt, float scal
   if (rc != CT2G_OK) return rc;
   if (cache_path) {
     std::ofstream f(cache_path, std::ios::app);
-    if (f) f << key << ' ' << best.dense_cell << ' ' << best.near_blocks_per_sm << ' ' << best.fft_tile << ' ' << best_ms << '\n';
+    if (f)
+      f << key << ' ' << best.dense_cell << ' ' << best.near_blocks_per_sm << ' ' << best.fft_tile
+        << ' ' << best.sparse_path << ' ' << best_ms << '\n';
   }
   if (out) *out = best;
   return CT2G_OK;

@@ -254,6 +254,7 @@ struct ct2g_ctx {
   int near_blocks_per_sm = 0;  // persistent near-field grid: blocks per SM (0: occupancy)
   int fft_tile = 0;            // y/x FFT pass tile width (0: default)
   int split_mg2l = 0;          // 1: X passes and MG2L as three launches, not one
+  int sparse_path = 0;         // sparse sinks: 0 one per lane, 1 per-block warp chunks
   struct ct2g_batch *self_batch = nullptr;  // graph of ct2g_kick_drift
   struct ct2g_learn *learn = nullptr;       // learned near-field correction
   bool fft_tc = false;                      // y/x FFT passes on the tensor cores

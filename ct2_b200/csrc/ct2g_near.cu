@@ -370,6 +370,138 @@ __global__ void __launch_bounds__(256, 4) near_kernel(
   }
 }
 
+// Sparse sinks, one per lane: the warp takes 32 consecutive entries of the
+// sparse sink list (cell order, so the lanes are neighbours) and every lane
+// walks the stencil of its own cell -- the 27 neighbouring 4x4x4 blocks,
+// occupancy & its own stencil mask, the ranges of the occupied cells -- and
+// sums its own sources, read through the read-only cache, two at a time with
+// the packed f32x2 arithmetic.  No lane evaluates a source outside its
+// stencil, and a warp is not bound to one cell block, so sparse regions fill
+// whole warps.  The work counter hands out groups of 32 sinks until the
+// device-held sparse count is covered.
+template <int KERNEL, bool POT>
+__global__ void __launch_bounds__(256, 4) near_lane_kernel(
+    const uint32_t *__restrict__ nsparse_ptr, uint32_t *__restrict__ work,
+    const uint32_t *__restrict__ sparse_list, const uint32_t *__restrict__ cs,
+    const unsigned long long *__restrict__ occ, const unsigned long long *__restrict__ stmask,
+    Walk walk, const uint32_t *__restrict__ skeys, uint32_t rbegin,
+    const float4 *__restrict__ src, int mbits, float soft, const float *__restrict__ box_gm,
+    float *__restrict__ ofx, float *__restrict__ ofy, float *__restrict__ ofz,
+    float *__restrict__ opot, unsigned long long *__restrict__ inter) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t ns = *nsparse_ptr;
+  const int M = 1 << mbits;
+  const float hc = 1.0f / (float)M;
+  const float h2 = soft * soft, hinv = 1.f / soft, hinv3 = hinv * hinv * hinv;
+  const f32x2 H2 = f2_pack(h2, h2);
+  for (;;) {
+    uint32_t ch = 0;
+    if (lane == 0) ch = atomicAdd(work, 1u);
+    ch = __shfl_sync(0xffffffffu, ch, 0);
+    if ((size_t)ch * 32 >= ns) break;
+    const uint32_t r = ch * 32 + (uint32_t)lane;
+    const bool act = r < ns;
+    uint32_t nsrc = 0;
+    if (act) {
+      const uint32_t i = sparse_list[r];
+      const uint32_t key = skeys[i - rbegin];
+      const float4 si = src[i];
+      const uint32_t p = key & 63u, blk = key >> 6;
+      const float GM = __ldg(box_gm + (key >> (3 * mbits)));
+      int px, py, pz;
+      inblock((int)p, px, py, pz);
+      float nx = 0.f, ny = 0.f, nz = 0.f, np = 0.f;
+      f32x2 pax = 0ull, pay = 0ull, paz = 0ull, pap = 0ull;
+      const unsigned long long *sm = stmask + p * 27;
+#pragma unroll 1
+      for (int o = 0; o < 27; o++) {
+        const unsigned long long m = __ldg(sm + o);
+        if (!m) continue;
+        const uint32_t nb = walk.add(blk, o);
+        unsigned long long word = __ldg(occ + nb) & m;
+        const int dX = 4 * (o / 9 - 1) - px, dY = 4 * ((o / 3) % 3 - 1) - py,
+                  dZ = 4 * (o % 3 - 1) - pz;
+        while (word) {
+          const int c = __ffsll((long long)word) - 1;
+          word &= word - 1;
+          const uint32_t ck = (nb << 6) | (uint32_t)c;
+          const uint32_t j0 = __ldg(cs + ck), j1 = __ldg(cs + ck + 1);
+          nsrc += j1 - j0;
+          int bx, by, bz;
+          inblock(c, bx, by, bz);
+          // the sink relative to the source cell's centre
+          const float xs = si.x - (float)(dX + bx) * hc, ys = si.y - (float)(dY + by) * hc,
+                      zs = si.z - (float)(dZ + bz) * hc;
+          uint32_t j = j0;
+          if constexpr (KERNEL == CT2G_SOFT_PLUMMER) {
+            const f32x2 X = f2_pack(xs, xs), Y = f2_pack(ys, ys), Z = f2_pack(zs, zs);
+            for (; j + 1 < j1; j += 2) {
+              const float4 a = __ldg(src + j), b = __ldg(src + j + 1);
+              const f32x2 dx = f2_sub(X, f2_pack(a.x, b.x));
+              const f32x2 dy = f2_sub(Y, f2_pack(a.y, b.y));
+              const f32x2 dz = f2_sub(Z, f2_pack(a.z, b.z));
+              const f32x2 r2 = f2_fma(dz, dz, f2_fma(dy, dy, f2_fma(dx, dx, H2)));
+              float r0, r1;
+              f2_unpack(r2, r0, r1);
+              const f32x2 ri = f2_pack(rsqrtf(r0), rsqrtf(r1));
+              const f32x2 g = f2_mul(f2_mul(ri, ri), ri);
+              pax = f2_fma(dx, g, pax);
+              pay = f2_fma(dy, g, pay);
+              paz = f2_fma(dz, g, paz);
+              if (POT) pap = f2_sub(pap, ri);
+            }
+          }
+          for (; j < j1; j++) {
+            const float4 q = __ldg(src + j);
+            ct2g_pair_term<KERNEL, POT>(xs - q.x, ys - q.y, zs - q.z, h2, hinv, hinv3, nx, ny,
+                                        nz, np, true);
+          }
+        }
+      }
+      if constexpr (KERNEL == CT2G_SOFT_PLUMMER) {
+        float a0, a1;
+        f2_unpack(pax, a0, a1);
+        nx -= a0 + a1;
+        f2_unpack(pay, a0, a1);
+        ny -= a0 + a1;
+        f2_unpack(paz, a0, a1);
+        nz -= a0 + a1;
+        if (POT) {
+          f2_unpack(pap, a0, a1);
+          np += a0 + a1;
+        }
+      }
+      // the far field (L2P, with GM) is already in the force buffers
+      ofx[i] += GM * nx;
+      ofy[i] += GM * ny;
+      ofz[i] += GM * nz;
+      if (POT) opot[i] += GM * np;
+    }
+    unsigned long long c = nsrc;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if (lane == 0 && c && inter) atomicAdd(inter, c);
+  }
+}
+
+template <int K, bool POT>
+int launch_near_lanes(ct2g_ctx *ctx, const Walk &walk) {
+  auto k = near_lane_kernel<K, POT>;
+  int per_sm = 0;
+  CT2G_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 256, 0));
+  const size_t nr = ctx->n - ctx->rung_begin;
+  if (ctx->near_blocks_per_sm > 0) per_sm = std::min(per_sm, ctx->near_blocks_per_sm);
+  size_t blocks = (size_t)std::max(1, per_sm) * ctx->num_sms;
+  blocks = std::max<size_t>(1, std::min(blocks, (nr + 255) / 256));
+  uint32_t *c = ctx->d_counts;
+  k<<<(unsigned)blocks, 256, 0, ctx->stream>>>(
+      c + 1, c + 4, ctx->sparse_list, ctx->cell_start, ctx->occ, ctx->stmask, walk, ctx->keys,
+      (uint32_t)ctx->rung_begin, ctx->src, ctx->mbits, ctx->opt.hsoft, ctx->box_gm, ctx->fx,
+      ctx->fy, ctx->fz, ctx->pot, ctx->d_inter);
+  CT2G_LAUNCHED(ctx);
+  return CT2G_OK;
+}
+
 Walk make_walk(int mbits) {
   Walk w{0u, 0u, 0u};
   for (int i = 0; i < mbits - 2; i++) {
@@ -402,8 +534,9 @@ int launch_near1(ct2g_ctx *ctx, const Walk &walk, const uint2 *chunks, const uin
   return CT2G_OK;
 }
 
-// dense chunks (counts[0], work counter counts[3]), then sparse chunks
-// (counts[2], stored after the dense ones, work counter counts[4])
+// dense chunks (counts[0], work counter counts[3]), then the sparse sinks
+// (counts[1] of them; work counter counts[4]): one per lane (sparse_path 0) or
+// as the per-block chunks stored after the dense ones (counts[2], sparse_path 1)
 template <int K, bool POT>
 int launch_near(ct2g_ctx *ctx) {
   const Walk walk = make_walk(ctx->mbits);
@@ -412,6 +545,7 @@ int launch_near(ct2g_ctx *ctx) {
   CT2G_TRY((launch_near1<K, POT, false>(ctx, walk, ctx->chunks, c + 0, nullptr, c + 3,
                                         ctx->sparse_list, ctx->stmask, -1.f, bw2, ctx->fx,
                                         ctx->fy, ctx->fz, ctx->pot, ctx->d_inter)));
+  if (ctx->sparse_path == 0) return launch_near_lanes<K, POT>(ctx, walk);
   return launch_near1<K, POT, true>(ctx, walk, ctx->chunks, c + 2, c + 0, c + 4,
                                     ctx->sparse_list, ctx->stmask, -1.f, bw2, ctx->fx, ctx->fy,
                                     ctx->fz, ctx->pot, ctx->d_inter);

@@ -82,7 +82,31 @@ int run_test(ct2g_ctx *ctx, const float *dA, const float *dB, float *dD, int *dS
   return cudaGetLastError() == cudaSuccess ? CT2G_OK : CT2G_ECUDA;
 }
 
+// The bounded wait and its error report, with nothing to wait for: an
+// mbarrier that expects one arrival and never gets it.  Each thread polls it
+// `polls` times (tc::mbar_wait), then the first thread records CT2G_ETIMEOUT
+// in the context's device error word, exactly as the tensor-core passes do
+// when their MMA completion does not arrive, and the kernel returns.
+__global__ void __launch_bounds__(128) wait_selftest_kernel(uint32_t polls,
+                                                            uint32_t *__restrict__ status) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) tc::mbar_init(&bar, 1);
+  __syncthreads();
+  const bool ok = tc::mbar_wait(&bar, 0, polls);
+  if (!ok && threadIdx.x == 0) atomicExch(status, (uint32_t)CT2G_ETIMEOUT);
+}
+
 }  // namespace
+
+extern "C" int ct2g_wait_selftest(ct2g_ctx *ctx, uint32_t polls) {
+  CT2G_TRY(ct2g_check(ctx));
+  if (polls < 1 || polls > (1u << 22))
+    return ct2g_fail(ctx, CT2G_EINVAL, "wait_selftest: polls in [1, 2^22]");
+  if (!ctx->d_counts) return ct2g_fail(ctx, CT2G_ESTATE, "wait_selftest: context has no device state");
+  wait_selftest_kernel<<<1, 128, 0, ctx->stream>>>(polls, ctx->d_counts + 6);
+  CT2G_LAUNCHED(ctx);
+  return CT2G_OK;
+}
 
 extern "C" int ct2g_tc_selftest(int device, const float *A, const float *B, int N, int K,
                                 float *D) {

@@ -212,18 +212,22 @@ int ct2g_batch_destroy(ct2g_batch *b);
 
 /* Tunable launch shapes of a context (no counterpart in the reference):
  * dense_cell -- cells with at least this many particles get their own sink
- * chunks, the rest are chunked per 4x4x4 block; near_blocks_per_sm -- blocks
- * per SM of the persistent near-field grid (0: occupancy limit); fft_tile --
- * columns per tile of the y/x FFT passes (0: default); split_mg2l -- 1 runs
- * the X FFT passes and the Green's-function multiply as three kernels, 0 (the
- * default) as one wherever a spectrum column of all components fits in
- * shared memory. */
+ * chunks, the sinks of sparser cells take the sparse path; near_blocks_per_sm
+ * -- blocks per SM of the persistent near-field grid (0: occupancy limit);
+ * fft_tile -- columns per tile of the y/x FFT passes (0: default); split_mg2l
+ * -- 1 runs the X FFT passes and the Green's-function multiply as three
+ * kernels, 0 (the default) as one wherever a spectrum column of all
+ * components fits in shared memory; sparse_path -- 0 (the default): one
+ * sparse sink per warp lane, each lane walking its own stencil; 1: the sparse
+ * sinks of a 4x4x4 cell block share a warp that walks the union of their
+ * stencils. */
 typedef struct {
   int dense_cell;
   int near_blocks_per_sm;
   int fft_tile;
   int split_mg2l;
-  int reserved[4];
+  int sparse_path;
+  int reserved[3];
 } ct2g_tuning;
 int ct2g_get_tuning(const ct2g_ctx *ctx, ct2g_tuning *t);
 int ct2g_set_tuning(ct2g_ctx *ctx, const ct2g_tuning *t);
@@ -387,6 +391,15 @@ int ct2g_ewald_direct_noalloc(int device, const uint32_t *qx, const uint32_t *qy
  * N in {32, 64}, K in {16, 32, 64, 96}.  CT2G_ETIMEOUT if the MMA did not
  * complete within the kernel's bounded wait. */
 int ct2g_tc_selftest(int device, const float *A, const float *B, int N, int K, float *D);
+
+/* Failure-path self-test.  No counterpart in the reference.  Queues on the
+ * context's stream a kernel whose threads wait, `polls` times each (1..2^22,
+ * a few ns apart), on an mbarrier that nothing arrives at; the wait gives up
+ * and the kernel records CT2G_ETIMEOUT in the context's device error word,
+ * the path the tensor-core passes take when an MMA completion does not
+ * arrive.  The next ct2g_synchronize reports CT2G_ETIMEOUT and clears it; the
+ * context stays usable. */
+int ct2g_wait_selftest(ct2g_ctx *ctx, uint32_t polls);
 
 /* FFT arithmetic of the mesh solve (precision form).  No counterpart in the
  * reference.  CT2G_FFT_FP32 (default): every pass on the CUDA cores in FP32.
