@@ -345,11 +345,11 @@ def learned_form(args, P, n, soft, local, kp, accuracy):
     return out
 
 
-FFT_METRIC = "3D FFT of 4 x 512^3 moment grids (grid points/s, forward + inverse)"
+FFT_METRIC = "complex 3D FFT of 4 x 512^3 CIC grids (grid points/s, forward)"
 NFW_METRIC = "particles/s per kick+drift, 256^3 NFW halos on a 512^3 mesh"
 
 
-def run_nfw(args, rank, world, local):
+def run_nfw(args, rank, world, local, emit=True):
     """--workload nfw256: the learned form's configuration.  256^3 particles in
     2000 NFW halos (c ~ U[5,15], dN/dM ~ M^-1.9 over two decades, r_vir ~
     M^(1/3)), 512^3 mesh, Plummer eps = cell/25, order --order.  plain: the
@@ -462,86 +462,145 @@ def run_nfw(args, rank, world, local):
                                                    "state": "same generator, seed + 100"}}},
                 "timings_s": {"generate": gen_s, "ewald_truth": truth_s},
                 "e2e": None, "gpu_launches": None, "roofline": None, "cpu_baseline": None}
-        print(json.dumps(line), flush=True)
+        if emit:
+            print(json.dumps(line), flush=True)
+        return line
+    return None
 
 
 
-def run_fft512(args, rank, world, local):
-    """--workload fft512: the precision form's configuration.  The 128^3
-    Plummer particles deposited on a 512^3 mesh as their four order-1 moment
-    grids (monopole and dipole about the cell centres: the method's own
-    deposit); the mesh solve's forward r2c and inverse c2r 3D FFTs of the four
-    grids timed with CUDA events, FP32 CUDA-core passes against tensor-core
-    y/x passes (BF16 hi+lo); the spectrum of the monopole grid checked against
-    the FP64 transform in both modes."""
-    import ctypes
-
+def fft512_form(args, P, n, local, with_forces=True):
+    """The precision form's configuration: the 128^3 Plummer particles'
+    cloud-in-cell deposit on a 512^3 mesh as four complex grids (the CIC mass
+    and its three first moments about the mesh points, imaginary parts zero),
+    transformed forward and back as one batch of complex 3D FFTs -- FP32
+    CUDA-core passes against tensor-core y/x passes (radix-16/32 DFT products,
+    BF16 hi+lo operands, FP32 accumulation); times by CUDA events on the
+    context's stream, each spectrum checked against the FP64 transform of the
+    mass grid; and the end force error of a mesh-512 solve with the
+    tensor-core passes against the FP64 Ewald sum."""
     import torch
 
-    from ct2_b200 import _lib
     from ct2_b200.gravity import Gravity
-    P, n = workload(args, rank)
     M = 512
+    peaks = _peaks()
     g = Gravity(mesh=M, order=1, bwidth=args.bwidth, hsoft=1.0 / (50 * args.ngrid),
                 GM=1.0 / n, device=local, max_particles=n)
-    # the x passes as their own launches, so that both modes' forward and
-    # inverse stages time all three passes of the transforms
-    g.set_tuning(**{**g.tuning(), "split_mg2l": 1})
     g.upload_dict(P)
-    g.particle_to_grid()
+    stream = torch.cuda.ExternalStream(g.stream(), device=local)
+    grid = torch.empty(4 * M ** 3 * 2, dtype=torch.float32, device="cuda")
+    work = torch.empty_like(grid)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e2 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    g.cic_deposit(M, grid.data_ptr())
+    e1.record(stream)
+    e1.synchronize()
+    deposit_ms = e0.elapsed_time(e1)
+    # FP64 reference: the r2c transform of the mass grid on the GPU in FP64
+    m0 = grid.view(4, M, M, M, 2)[0, ..., 0].double().cpu().numpy()
+    ref = g.fft_r2c_3d(np.ascontiguousarray(m0))
+    dim = M * M * (M // 2 + 1)
+    ref = (ref[:dim] + 1j * ref[dim:]).reshape(M, M, M // 2 + 1)
+    del m0
     res = {}
     for mode in ("fp32", "tc"):
         g.set_fft_mode(mode)
         fw, iv = [], []
         for it in range(args.warmup + args.steps):
-            g.compute_multipoles()
-            g.compute_expansions()  # r2c, MG2L, c2r of the 4 grids
-            st = g.stage_times()
+            work.copy_(grid)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            g.fft3d_c2c_dev(work.data_ptr(), M, 4, 1)
+            e1.record(stream)
+            g.fft3d_c2c_dev(work.data_ptr(), M, 4, -1)
+            e2.record(stream)
+            e2.synchronize()
             if it >= args.warmup:
-                fw.append(float(st[2]))
-                iv.append(float(st[4]))
-        res[mode] = {"fft_fwd_ms": float(np.median(fw)), "fft_inv_ms": float(np.median(iv))}
-    # spectrum accuracy on the monopole grid against FP64
-    g.compute_multipoles()
-    m0 = np.ascontiguousarray(g.multipoles()[0])
-    ref = g.fft_r2c_3d(m0.astype(np.float64))  # FP64 on the GPU, split planes
-    dim = M * M * (M // 2 + 1)
-    ref = (ref[:dim] + 1j * ref[dim:]).reshape(M, M, M // 2 + 1)
-    scale = np.sqrt(np.mean(np.abs(ref) ** 2))
-    lib = _lib.load()
-    xin = torch.from_numpy(m0).cuda()
-    out = torch.empty((M, M, M // 2 + 1), dtype=torch.complex64, device="cuda")
-    for mode in ("fp32", "tc"):
-        g.set_fft_mode(mode)
-        torch.cuda.synchronize()
-        rc = lib.ct2g_fft3d_f32_dev(g.handle, 1, ctypes.c_void_p(xin.data_ptr()),
-                                    ctypes.c_void_p(out.data_ptr()), M, 1)
-        assert rc == 0
+                fw.append(e0.elapsed_time(e1))
+                iv.append(e1.elapsed_time(e2))
+        work.copy_(grid)
+        g.fft3d_c2c_dev(work.data_ptr(), M, 4, 1)
         g.synchronize()
-        y = out.cpu().numpy()
-        res[mode]["spectrum_rms_rel_err"] = float(np.sqrt(np.mean(np.abs(y - ref) ** 2)) / scale)
-    points = 4.0 * M ** 3
-    best = res["tc"]
-    ms = best["fft_fwd_ms"] + best["fft_inv_ms"]
+        z = work.view(4, M, M, M, 2)[0, :, :, : M // 2 + 1, :].cpu().numpy()
+        z = z[..., 0].astype(np.float64) + 1j * z[..., 1]
+        err = float(np.linalg.norm(z - ref) / np.linalg.norm(ref))
+        del z
+        f_ms, i_ms = float(np.median(fw)), float(np.median(iv))
+        # algorithmic bytes: one read and one write of the batch per 3D
+        # transform (4 x 16 x 512^3); the three passes move three times that
+        algo = 4 * 16.0 * M ** 3
+        res[mode] = {"fft_fwd_ms": f_ms, "fft_inv_ms": i_ms, "spectrum_rms_rel_err": err,
+                     "algorithmic_bytes_per_transform": algo,
+                     "passes_bytes_per_transform": 3 * algo,
+                     "achieved_gbs_passes": 3 * algo / (f_ms * 1e-3) / 1e9,
+                     "frac_of_measured_hbm": 3 * algo / (f_ms * 1e-3) / 1e9 / peaks["hbm"]}
+    g.set_fft_mode("fp32")
+    g.close()
+    del grid, work
+    torch.cuda.empty_cache()
+    out = {"deposit_ms": deposit_ms, "grids": 4, "mesh": M, "forms": res,
+           "fft": "batch of 4 complex 512^3 grids; tc: y/x passes as tcgen05 DFT products, "
+                  "BF16 hi+lo operands, FP32 accumulation"}
+    if with_forces:
+        # the end force error of the tensor-core passes on a 512^3 mesh solve
+        gf = Gravity(mesh=M, order=args.order, bwidth=args.bwidth, hsoft=1.0 / (50 * args.ngrid),
+                     GM=1.0 / n, device=local, max_particles=n)
+        gf.upload_dict(P)
+        rng = np.random.Generator(np.random.PCG64(123))
+        sel = np.sort(rng.choice(n, size=min(args.accuracy_sinks, n), replace=False))
+        truth = gf.ewald_direct(P["x"][sel], P["y"][sel], P["z"][sel])
+        acc = {}
+        for mode in ("fp32", "tc"):
+            gf.set_fft_mode(mode)
+            gf.upload_dict(P)
+            gf.particle_to_grid()
+            gf.compute_forces()
+            f, _ = gf.forces()
+            ids = gf.download()["id"]
+            inv = np.empty_like(ids)
+            inv[ids] = np.arange(n, dtype=ids.dtype)
+            d = np.linalg.norm(f[inv[sel]] - truth, axis=1)
+            tn = np.linalg.norm(truth, axis=1)
+            acc[mode] = {"rms_rel": float(np.sqrt(np.mean((d / tn) ** 2))),
+                         "max_rel": float((d / tn).max()), "sinks": int(len(sel))}
+        gf.close()
+        out["force_accuracy_mesh512"] = {"order": args.order, "bwidth": args.bwidth,
+                                         "vs": "FP64 Ewald direct sum", **acc}
+    return out
+
+
+def run_fft512(args, rank, world, local):
+    """--workload fft512: the precision form's configuration on its own line
+    (fft512_form)."""
+    P, n = workload(args, rank)
+    out = fft512_form(args, P, n, local)
+    best = out["forms"]["tc"]
+    ms = best["fft_fwd_ms"]
+    points = 4.0 * 512 ** 3
     if rank == 0:
         line = {"metric": FFT_METRIC, "value": points / (ms * 1e-3), "unit": "grid points/s",
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "bf16x3 (tensor cores) / f32",
-                "data": "synthetic: moments of the seeded 128^3 Plummer workload",
-                "config": {"workload": "fft512x4", "mesh": M, "grids": 4,
+                "data": "synthetic: CIC deposit of the seeded 128^3 Plummer workload",
+                "config": {"workload": "cic512x4_c2c", "mesh": 512, "grids": 4,
                            "particles": n, "l2": "inputs larger than L2 (4.3 GB)"},
-                "forms": res, "gpu_launches": None, "roofline": None, "cpu_baseline": None,
-                "e2e": None}
+                "result": out, "gpu_launches": None, "roofline": {
+                    "kernel": "tensor-core y/x passes + z pass, forward batch", "bound": "hbm",
+                    "achieved": best["achieved_gbs_passes"], "peak": _peaks()["hbm"],
+                    "unit": "GB/s", "frac": best["frac_of_measured_hbm"], "traffic": None},
+                "cpu_baseline": None, "e2e": None}
         print(json.dumps(line), flush=True)
-    g.close()
 
 
 BOX_METRIC = ("particles/s per kick+drift over 96 independent periodic boxes "
               "(16^3..128^3 particles, meshes 32^3..256^3)")
 
 
-def run_boxes(args, rank, world, local):
+def run_boxes(args, rank, world, local, emit=True):
     """--workload boxes96: 96 independent boxes (particle counts 2^U[12,21],
     mesh = nearest power of two to 2 N^(1/3) clipped to [32, 256], Plummer +
     background generator seeded per box, softening = cell/25, GM = 1/N per
@@ -685,9 +744,11 @@ def run_boxes(args, rank, world, local):
                 "forms": {"plain_box_by_box": {"value": plain_value, "ms_per_step": plain_ms},
                           "batched_graph": {"value": value, "ms_per_step": ms,
                                             "tuning": {str(k): v for k, v in tunings.items()}}}}
-        print(json.dumps(line), flush=True)
+        if emit:
+            print(json.dumps(line), flush=True)
     for g, _, _ in ctxs:
         g.close()
+    return line if rank == 0 else None
 
 
 def main():
@@ -719,6 +780,10 @@ def main():
     ap.add_argument("--learned-epochs", type=int, default=30)
     ap.add_argument("--no-precision-form", dest="precision_form", action="store_false",
                     help="skip the tensor-core FFT form")
+    ap.add_argument("--no-extra-forms", action="store_true",
+                    help="skip the fft512, boxes96 and nfw256 forms of the default run")
+    ap.add_argument("--form-steps", type=int, default=5,
+                    help="timed steps of the extra forms in the default run")
     ap.add_argument("--tune-cache", default=None,
                     help="autotuner cache file (default: tune on every run)")
     args = ap.parse_args()
@@ -922,6 +987,25 @@ def main():
                        "achieved_gbs": algo_bytes[nm] / (st[i] * 1e-3) / 1e9,
                        "frac": algo_bytes[nm] / (st[i] * 1e-3) / 1e9 / peaks["hbm"]}
                   for i, nm in enumerate(names) if nm in ("fft_fwd", "mg2l", "fft_inv") and st[i] > 0}
+
+    # the configurations of the precision, batching and learned forms, each on
+    # its own workload, with fewer timed steps (their own lines come from
+    # --workload fft512 / boxes96 / nfw256)
+    if not args.no_extra_forms:
+        import copy
+        a2 = copy.copy(args)
+        a2.steps, a2.warmup = min(args.steps, args.form_steps), min(args.warmup, 3)
+        forms["precision_fft512"] = fft512_form(a2, P, n, local)
+        bl = run_boxes(a2, rank, world, local, emit=False)
+        if bl is not None:
+            forms["batched_boxes96"] = {k: bl[k] for k in ("metric", "value", "unit", "ms_per_step",
+                                                          "config", "accuracy", "forms", "e2e",
+                                                          "gpu_launches")}
+        nl = run_nfw(a2, rank, world, local, emit=False)
+        if nl is not None:
+            forms["learned_nfw256"] = {k: nl[k] for k in ("metric", "value", "unit", "ms_per_step",
+                                                         "config", "accuracy", "forms",
+                                                         "interactions_per_step", "timings_s")}
 
     cb = None
     if rank == 0 and not args.no_cpu_baseline:

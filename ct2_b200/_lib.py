@@ -104,6 +104,8 @@ SYMBOLS = [
     ("ct2g_fft_r2c_3d", _I, [_P, _P, _P, _I, _I]),
     ("ct2g_fft_c2r_3d", _I, [_P, _P, _P, _I, _I]),
     ("ct2g_fft3d_f32_dev", _I, [_P, _I, _P, _P, _I, _I]),
+    ("ct2g_fft3d_c2c_f32_dev", _I, [_P, _I, _P, _I, _I]),
+    ("ct2g_cic_deposit", _I, [_P, _I, _P]),
     ("ct2g_fft1d_real", _I, [_P, _P, _I, _I, _I]),
     ("ct2g_fft1d_complex", _I, [_P, _P, _I, _I, _I]),
     ("ct2g_scramble", _I, [_P, _P, _I, _I, _I]),

@@ -10,6 +10,8 @@ namespace {
 
 constexpr int kSinkThreads = 128;
 constexpr int kSrcChunk = 4096;
+// source chunks ride on grid.y (at most 65535), which bounds the source count
+constexpr size_t kMaxSources = (size_t)65535 * kSrcChunk;
 
 __global__ void ewald_real_kernel(const uint32_t *__restrict__ sx, const uint32_t *__restrict__ sy,
                                   const uint32_t *__restrict__ sz, size_t ns,
@@ -157,6 +159,7 @@ extern "C" int ct2g_ewald_direct(ct2g_ctx *ctx, const uint32_t *sx, const uint32
   if (!ctx->has_particles) return ct2g_fail(ctx, CT2G_ESTATE, "no particles uploaded");
   if (!(alpha > 0) || !(rcut > 0) || rcut > 0.5 || kmax < 1 || kmax > 64)
     return ct2g_fail(ctx, CT2G_EINVAL, "ewald: bad split parameters");
+  if (ctx->n > kMaxSources) return ct2g_fail(ctx, CT2G_EINVAL, "ewald: more than 65535*4096 sources");
   std::vector<int> kv;
   for (int kx = 0; kx <= kmax; kx++)
     for (int ky = -kmax; ky <= kmax; ky++)
@@ -346,9 +349,25 @@ extern "C" int ct2g_ewald_direct_noalloc(int device, const uint32_t *qx, const u
   if (!qx || !qy || !qz || !sx || !sy || !sz || !f || !pot || nq == 0 || ns == 0)
     return CT2G_EINVAL;
   if (kmax < 1 || kmax > CT2G_NOALLOC_KMAX) return CT2G_EINVAL;  // scratch holds kmax <= 24
+  if (nq > kMaxSources) return CT2G_EINVAL;
   if (!(alpha > 0) || !(rcut > 0) || rcut > 0.5 || !(soft > 0)) return CT2G_EINVAL;
   if (kernel != CT2G_SOFT_PLUMMER && kernel != CT2G_SOFT_SPHERE) return CT2G_EINVAL;
   if (device < 0 || device >= 128) return CT2G_EINVAL;
+  // an error the caller's own work left pending is theirs: report it without
+  // clearing it, and run nothing
+  if (cudaPeekAtLastError() != cudaSuccess) return CT2G_ECUDA;
+  // the caller's current device is put back on every return
+  int prev = -1;
+  if (cudaGetDevice(&prev) != cudaSuccess) {
+    cudaGetLastError();
+    return CT2G_ENODEV;
+  }
+  struct Restore {
+    int dev;
+    ~Restore() {
+      if (dev >= 0) cudaSetDevice(dev);
+    }
+  } restore{prev};
   if (cudaSetDevice(device) != cudaSuccess) {
     cudaGetLastError();
     return CT2G_ENODEV;
@@ -369,6 +388,7 @@ extern "C" int ct2g_ewald_direct_noalloc(int device, const uint32_t *qx, const u
   cudaStream_t st = (cudaStream_t)stream;
   const int nbox = (kmax + 1) * (2 * kmax + 1) * (2 * kmax + 1);
   // the outputs accumulate, and S keeps the previous call's sums: clear all
+  // (no error was pending on entry, so any error here is this call's own)
   if (cudaMemsetAsync(S, 0, sizeof(double2) * nbox, st) != cudaSuccess ||
       cudaMemsetAsync(f, 0, sizeof(double) * 3 * ns, st) != cudaSuccess ||
       cudaMemsetAsync(pot, 0, sizeof(double) * ns, st) != cudaSuccess) {

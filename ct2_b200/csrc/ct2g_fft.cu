@@ -480,11 +480,14 @@ int launch_cols(ct2g_ctx *ctx, typename Cplx<T>::type *spec, size_t nouter, size
   return CT2G_OK;
 }
 
-// Y and X passes over a spectrum whose qk rows hold ld >= N/2+1 elements
+// Y and X passes over a spectrum whose qk rows hold ld >= N/2+1 elements (a
+// half spectrum: the Y pass transforms its first N/2+1 columns) or, `full`,
+// N elements (a complex grid: every column)
 template <typename T, int N>
-int run_cols(ct2g_ctx *ctx, typename Cplx<T>::type *spec, int batch, bool inv, size_t ld) {
+int run_cols(ct2g_ctx *ctx, typename Cplx<T>::type *spec, int batch, bool inv, size_t ld,
+             bool full = false) {
   using C2 = typename Cplx<T>::type;
-  const size_t NH = N / 2 + 1;
+  const size_t NH = full ? (size_t)N : (size_t)N / 2 + 1;
   const bool vec = (ld * sizeof(C2)) % 16 == 0;
   for (int pass = 0; pass < 2; pass++) {
     const bool ypass = (pass == 0) != inv;
@@ -576,6 +579,66 @@ int fft_c2r(ct2g_ctx *ctx, typename Cplx<T>::type *in, T *out, int N, int batch,
     case 128: return fft_c2r_n<T, 128>(ctx, in, out, batch, ld);
     case 256: return fft_c2r_n<T, 256>(ctx, in, out, batch, ld);
     case 512: return fft_c2r_n<T, 512>(ctx, in, out, batch, ld);
+  }
+  return ct2g_fail(ctx, CT2G_EINVAL, "FFT size must be a power of two in [4, 512]");
+}
+
+// ---- complex-to-complex 3D FFT ------------------------------------------------
+// Pass Z of a complex grid a[b][i][j][k] (k contiguous, N per row): LP rows
+// per block through shared memory, moved in 16-byte chunks (two complex
+// values); the Y and X passes are the column passes of the real transforms
+// over every column (run_cols, `full`).
+template <int N, bool INV>
+__global__ void __launch_bounds__(256, 3) fftz_c2c_kernel(float2 *__restrict__ a, size_t nrows,
+                                                          int LP, const float2 *__restrict__ tw) {
+  using LL = LineLayout<N, true>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  float2 *stw = reinterpret_cast<float2 *>(smraw);
+  float2 *s = stw + N;
+  load_twiddles(stw, tw, N);
+  const size_t row0 = (size_t)blockIdx.x * LP;
+  const int nr = (int)min((size_t)LP, nrows - row0);
+  float2 *g = a + row0 * N;
+  for (int c = threadIdx.x; c < nr * N / 2; c += 256) {
+    const int e = 2 * c, l = e / N, r = e % N;
+    const float4 v = *reinterpret_cast<const float4 *>(g + e);
+    s[LL::at(l, r, 0)] = make_float2(v.x, v.y);
+    s[LL::at(l, r + 1, 0)] = make_float2(v.z, v.w);
+  }
+  __syncthreads();
+  tile_fft<N, true, float2, INV>(s, nr, 0, stw);
+  for (int c = threadIdx.x; c < nr * N / 2; c += 256) {
+    const int e = 2 * c, l = e / N, r = e % N;
+    const float2 u = s[LL::at(l, r, 0)], w = s[LL::at(l, r + 1, 0)];
+    *reinterpret_cast<float4 *>(g + e) = make_float4(u.x, u.y, w.x, w.y);
+  }
+}
+
+template <int N>
+int fft_c2c_n(ct2g_ctx *ctx, float2 *a, int batch, bool inv) {
+  const size_t nrows = (size_t)batch * N * N;
+  const int LP = std::max(1, 4096 / N);
+  const size_t smem = sizeof(float2) * ((size_t)N + (size_t)LP * LineLayout<N, true>::LS);
+  auto kern = inv ? fftz_c2c_kernel<N, true> : fftz_c2c_kernel<N, false>;
+  if (inv) CT2G_TRY((run_cols<float, N>(ctx, a, batch, true, N, true)));
+  CT2G_TRY(ct2g_smem_attrs(ctx, kern, smem));
+  kern<<<ct2g_div_up(nrows, LP), 256, smem, ctx->stream>>>(a, nrows, LP, twiddle_ptr<float2>(ctx));
+  CT2G_LAUNCHED(ctx);
+  if (!inv) CT2G_TRY((run_cols<float, N>(ctx, a, batch, false, N, true)));
+  return CT2G_OK;
+}
+
+int fft_c2c(ct2g_ctx *ctx, float2 *a, int N, int batch, bool inv) {
+  CT2G_TRY(ct2g_twiddles(ctx, N));
+  switch (N) {
+    case 4: return fft_c2c_n<4>(ctx, a, batch, inv);
+    case 8: return fft_c2c_n<8>(ctx, a, batch, inv);
+    case 16: return fft_c2c_n<16>(ctx, a, batch, inv);
+    case 32: return fft_c2c_n<32>(ctx, a, batch, inv);
+    case 64: return fft_c2c_n<64>(ctx, a, batch, inv);
+    case 128: return fft_c2c_n<128>(ctx, a, batch, inv);
+    case 256: return fft_c2c_n<256>(ctx, a, batch, inv);
+    case 512: return fft_c2c_n<512>(ctx, a, batch, inv);
   }
   return ct2g_fail(ctx, CT2G_EINVAL, "FFT size must be a power of two in [4, 512]");
 }
@@ -1196,6 +1259,9 @@ int ct2g_fft_r2c_f32(ct2g_ctx *ctx, const float *in, float2 *out, int N, int bat
 }
 int ct2g_fft_c2r_f32(ct2g_ctx *ctx, float2 *in, float *out, int N, int batch, int ld) {
   return fft_c2r<float>(ctx, in, out, N, batch, ld);
+}
+int ct2g_fft_c2c_f32(ct2g_ctx *ctx, float2 *a, int N, int batch, bool inv) {
+  return fft_c2c(ctx, a, N, batch, inv);
 }
 int ct2g_fft_r2c_f64(ct2g_ctx *ctx, const double *in, double2 *out, int N, int batch, int ld) {
   return fft_r2c<double>(ctx, in, out, N, batch, ld);

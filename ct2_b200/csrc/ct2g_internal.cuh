@@ -254,7 +254,7 @@ struct ct2g_ctx {
   int near_blocks_per_sm = 0;  // persistent near-field grid: blocks per SM (0: occupancy)
   int fft_tile = 0;            // y/x FFT pass tile width (0: default)
   int split_mg2l = 0;          // 1: X passes and MG2L as three launches, not one
-  int sparse_path = 0;         // sparse sinks: 0 one per lane, 1 per-block warp chunks
+  int sparse_path = 1;         // sparse sinks: 0 one per lane, 1 per-block warp chunks
   struct ct2g_batch *self_batch = nullptr;  // graph of ct2g_kick_drift
   struct ct2g_learn *learn = nullptr;       // learned near-field correction
   bool fft_tc = false;                      // y/x FFT passes on the tensor cores
@@ -411,6 +411,7 @@ int ct2g_twiddles(ct2g_ctx *ctx, int N);
 // halved axis) hold ld >= N/2+1 complex values
 int ct2g_fft_r2c_f32(ct2g_ctx *ctx, const float *in, float2 *out, int N, int batch, int ld);
 int ct2g_fft_c2r_f32(ct2g_ctx *ctx, float2 *in, float *out, int N, int batch, int ld);
+int ct2g_fft_c2c_f32(ct2g_ctx *ctx, float2 *a, int N, int batch, bool inv);
 int ct2g_fft_r2c_f64(ct2g_ctx *ctx, const double *in, double2 *out, int N, int batch, int ld);
 int ct2g_fft_c2r_f64(ct2g_ctx *ctx, double2 *in, double *out, int N, int batch, int ld);
 

@@ -304,7 +304,7 @@ class Gravity:
                     fft_tile=t.fft_tile, split_mg2l=t.split_mg2l, sparse_path=t.sparse_path)
 
     def set_tuning(self, dense_cell=16, near_blocks_per_sm=0, fft_tile=0, split_mg2l=0,
-                   sparse_path=0):
+                   sparse_path=1):
         t = Tuning(dense_cell, near_blocks_per_sm, fft_tile, split_mg2l, sparse_path)
         self._chk(self._l.ct2g_set_tuning(self._h, ctypes.byref(t)))
 
@@ -352,6 +352,22 @@ class Gravity:
         return c[:nr.value].astype(np.int64)
 
     # -- FFT ----------------------------------------------------------------
+    def fft3d_c2c_dev(self, ptr, N, batch, dir=1):
+        """In-place complex 3D FFT of `batch` device grids (a device pointer,
+        e.g. a torch tensor's data_ptr()) on the context's stream."""
+        self._chk(self._l.ct2g_fft3d_c2c_f32_dev(self._h, dir, ctypes.c_void_p(ptr), N, batch))
+
+    def fft3d_r2c_dev(self, real_ptr, cplx_ptr, N, batch, dir=1):
+        """The real <-> half-spectrum 3D FFT on device pointers (dir +1 r2c,
+        -1 c2r), FP32."""
+        self._chk(self._l.ct2g_fft3d_f32_dev(self._h, dir, ctypes.c_void_p(real_ptr),
+                                             ctypes.c_void_p(cplx_ptr), N, batch))
+
+    def cic_deposit(self, N, ptr):
+        """CIC mass and first moments of the particles onto four complex
+        device grids float2[4][N][N][N] at `ptr`."""
+        self._chk(self._l.ct2g_cic_deposit(self._h, N, ctypes.c_void_p(ptr)))
+
     def fft1d_real(self, X, N, lanes=1, dir=1):
         """fft_real (fft.hpp:25-26) in place on a float64 array: input in
         bit-reversed order, output halfcomplex; lanes interleaved."""

@@ -217,10 +217,12 @@ int ct2g_batch_destroy(ct2g_batch *b);
  * fft_tile -- columns per tile of the y/x FFT passes (0: default); split_mg2l
  * -- 1 runs the X FFT passes and the Green's-function multiply as three
  * kernels, 0 (the default) as one wherever a spectrum column of all
- * components fits in shared memory; sparse_path -- 0 (the default): one
- * sparse sink per warp lane, each lane walking its own stencil; 1: the sparse
- * sinks of a 4x4x4 cell block share a warp that walks the union of their
- * stencils. */
+ * components fits in shared memory; sparse_path -- 1 (the default): the
+ * sparse sinks of a 4x4x4 cell block share a warp that walks the union of
+ * their stencils, each source batch staged once in shared memory; 0: one
+ * sparse sink per warp lane, each lane walking its own stencil and reading
+ * its own sources (no masked work, but every lane gathers its own sources
+ * through the L1 cache). */
 typedef struct {
   int dense_cell;
   int near_blocks_per_sm;
@@ -357,6 +359,20 @@ int ct2g_twiddles(ct2g_ctx *ctx, int which, int N, double *out);
  * output (float2[batch][N][N][N/2+1]); dir = +1 forward r2c, -1 inverse c2r */
 int ct2g_fft3d_f32_dev(ct2g_ctx *ctx, int dir, void *d_real, void *d_complex, int N,
                        int batch);
+/* Complex-to-complex 3D FFT of `batch` device grids float2[batch][N][N][N]
+ * (k contiguous), in place, FP32, on the context's stream: dir = +1 forward
+ * (exp(-2 pi i q.r/N)), -1 the unnormalised inverse.  With CT2G_FFT_TC_BF16X3
+ * set (and N equal to the context's mesh) the y and x passes run on the
+ * tensor cores.  No counterpart in the reference.  N: power of two, 4..512;
+ * the grid 16-byte aligned. */
+int ct2g_fft3d_c2c_f32_dev(ct2g_ctx *ctx, int dir, void *d_data, int N, int batch);
+/* Cloud-in-cell deposit of the context's particles (unit mass) onto four
+ * complex device grids float2[4][N][N][N] (zeroed first): the real parts hold
+ * the CIC mass and the three first moments about each mesh point (offsets in
+ * mesh units), the imaginary parts zero.  A particle at x lies between mesh
+ * points floor(xN - 1/2) and the next, with linear weights per axis.  No
+ * counterpart in the reference. */
+int ct2g_cic_deposit(ct2g_ctx *ctx, int N, void *d_grid);
 
 /* FP64 Ewald direct sum over ALL particles of the context as sources, at the
  * given sink positions (host, fixed32): the force truth.  f: host double[3*ns]
@@ -374,10 +390,14 @@ int ct2g_ewald_direct(ct2g_ctx *ctx, const uint32_t *sx, const uint32_t *sy,
  * (both required) -- and the only scratch, the structure factor, lives in a
  * static device array of the library (about 0.94 MB per GPU, held until the
  * process exits).  kmax must be <= 24, the size that array holds; larger
- * values return CT2G_EINVAL.  The first call on a device looks the array up
- * (cudaGetSymbolAddress), so make it before any stream capture.  Calls share
- * the array: calls that overlap on the GPU race.  Work is queued on `stream`
- * (a cudaStream_t, or NULL for the default stream); nothing is allocated. */
+ * values return CT2G_EINVAL, as do more than 65535*4096 sources.  The first
+ * call on a device looks the array up (cudaGetSymbolAddress), so make it
+ * before any stream capture.  Calls share the array: calls that overlap on
+ * the GPU race.  Work is queued on `stream` (a cudaStream_t, or NULL for the
+ * default stream); nothing is allocated.  The calling thread's current device
+ * is the same on return as on entry; an error already pending from the
+ * caller's own work is left in place and the call returns CT2G_ECUDA without
+ * running. */
 int ct2g_ewald_direct_noalloc(int device, const uint32_t *qx, const uint32_t *qy,
                               const uint32_t *qz, size_t nq, const uint32_t *sx,
                               const uint32_t *sy, const uint32_t *sz, size_t ns, int kernel,

@@ -352,3 +352,26 @@ def halfcomplex_to_complex(X):
     k = np.arange(1, N // 2)
     out.imag[k] = X[N - k]
     return out
+
+
+# --------------------------------------------------------------------------
+# Cloud-in-cell deposit (no counterpart in the reference; the published CIC
+# scheme, as ct2g_cic_deposit states it): four grids, the CIC mass and the
+# first moments about each mesh point, in FP64
+# --------------------------------------------------------------------------
+def cic_deposit(x, y, z, N):
+    pos = np.stack([x, y, z], 1).astype(np.float64) * 2.0 ** -32
+    u = pos * N - 0.5
+    m = np.floor(u).astype(np.int64)
+    f = u - m
+    out = np.zeros((4, N, N, N), np.float64)
+    for corner in range(8):
+        b = np.array([(corner >> 2) & 1, (corner >> 1) & 1, corner & 1])
+        w = np.prod(np.where(b[None, :] == 1, f, 1.0 - f), axis=1)
+        s = np.where(b[None, :] == 1, f - 1.0, f)
+        idx = (m + b[None, :]) & (N - 1)
+        flat = (idx[:, 0] * N + idx[:, 1]) * N + idx[:, 2]
+        np.add.at(out[0].reshape(-1), flat, w)
+        for d in range(3):
+            np.add.at(out[1 + d].reshape(-1), flat, w * s[:, d])
+    return out
