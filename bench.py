@@ -336,7 +336,24 @@ def learned_form(args, P, n, soft, local, kp, accuracy):
     e1.record(stream)
     e1.synchronize()
     value, ms = replicas.job_throughput(n, e0.elapsed_time(e1) / args.steps, device="cuda")
+    # the same context with the correction off: the narrow base step alone,
+    # so that the correction's own cost (learned - base) is on the line
+    gl.learned_select("none")
+    base_acc = accuracy(gl)
+    gl.upload_dict(P)
+    for _ in range(args.warmup):
+        gl.kick_drift(kp, args.dt, 1.0, graph=True, wait=False)
+    gl.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        gl.kick_drift(kp, args.dt, 1.0, graph=True, wait=False)
+    e1.record(stream)
+    e1.synchronize()
+    base_ms = e0.elapsed_time(e1) / args.steps
     out = {"value": value, "ms_per_step": ms, "accuracy": acc, "tuning": tune,
+           "base_narrow": {"bwidth": args.learned_base, "ms_per_step": base_ms,
+                           "accuracy": base_acc},
+           "correction_ms": ms - base_ms,
            "base_bwidth": args.learned_base, "widened_to": args.bwidth,
            "threshold_log10": thr, "calibration": cal, "cells_selected": int(nsel),
            "training": {"cells": int(ncell), "epochs": args.learned_epochs, "mse": loss,

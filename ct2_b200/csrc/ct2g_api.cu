@@ -78,7 +78,7 @@ void free_particles(ct2g_ctx *ctx) {
                   ctx->keys, ctx->keys2, ctx->vals, ctx->vals2, ctx->hist, ctx->src,
                   ctx->chunks, ctx->sparse_list, ctx->flags, ctx->fx,
                   ctx->fy, ctx->fz,
-                  ctx->pot};
+                  ctx->pot, ctx->nfx, ctx->nfy, ctx->nfz, ctx->npot};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   ctx->x = ctx->y = ctx->z = ctx->id = nullptr;
@@ -92,6 +92,7 @@ void free_particles(ct2g_ctx *ctx) {
   ctx->chunks = nullptr;
   ctx->sparse_list = ctx->flags = nullptr;
   ctx->fx = ctx->fy = ctx->fz = ctx->pot = nullptr;
+  ctx->nfx = ctx->nfy = ctx->nfz = ctx->npot = nullptr;
   ctx->cap = 0;
 }
 
@@ -195,6 +196,10 @@ int ct2g_alloc_particles(ct2g_ctx *ctx, size_t n) {
   A(ctx->fy, cap * 4);
   A(ctx->fz, cap * 4);
   A(ctx->pot, cap * 4);
+  A(ctx->nfx, cap * 4);
+  A(ctx->nfy, cap * 4);
+  A(ctx->nfz, cap * 4);
+  A(ctx->npot, cap * 4);
 #undef A
   ctx->cap = cap;
   // scan scratch for the largest scan of a step (radix histograms, cell
@@ -302,6 +307,12 @@ int ct2g_create_boxes(const ct2g_options *opt, int nbox, ct2g_ctx **out) {
   do {
     if (cudaSetDevice(ctx->device) != cudaSuccess) { rc = CT2G_ENODEV; break; }
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) { rc = CT2G_ECUDA; break; }
+    if (cudaStreamCreateWithFlags(&ctx->stream2, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+      rc = CT2G_ECUDA;
+      break;
+    }
     for (auto &e : ctx->ev)
       if (cudaEventCreate(&e) != cudaSuccess) { rc = CT2G_ECUDA; break; }
     if (rc) break;
@@ -378,6 +389,10 @@ int ct2g_destroy(ct2g_ctx *ctx) {
   if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
   for (auto &e : ctx->ev)
     if (e) cudaEventDestroy(e);
+  if (ctx->stream2) cudaStreamSynchronize(ctx->stream2);
+  if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+  if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
+  if (ctx->stream2) cudaStreamDestroy(ctx->stream2);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return CT2G_OK;
@@ -574,8 +589,7 @@ int ct2g_download_greens(ct2g_ctx *ctx, float *out) {
 
 int ct2g_compute_forces(ct2g_ctx *ctx) {
   CT2G_TRY(check(ctx));
-  CT2G_TRY(ct2g_far_field(ctx, true));
-  CT2G_TRY(ct2g_forces(ctx, true));
+  CT2G_TRY(ct2g_all_forces(ctx, true));
   ctx->forces_valid = true;
   ctx->pot_valid = true;
   return CT2G_OK;
@@ -618,8 +632,7 @@ int ct2g_kick(ct2g_ctx *ctx, const ct2g_kick_params *p, int *max_rung) {
   CT2G_TRY(check(ctx));
   if (!p) return ct2g_fail(ctx, CT2G_EINVAL, "null kick params");
   if (p->rung < 0 || p->rung > 30) return ct2g_fail(ctx, CT2G_EINVAL, "rung out of range");
-  CT2G_TRY(ct2g_far_field(ctx, false));
-  CT2G_TRY(ct2g_forces(ctx, false));
+  CT2G_TRY(ct2g_all_forces(ctx, false));
   ctx->pot_valid = false;
   ct2g_mark(ctx, 6);
   ctx->forces_valid = true;

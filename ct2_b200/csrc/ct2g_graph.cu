@@ -44,8 +44,7 @@ int step_body(ct2g_ctx *ctx, const ct2g_kick_params *p, float dt, float scale) {
   if (!ctx->has_particles) return ct2g_fail(ctx, CT2G_ESTATE, "no particles uploaded");
   ct2g_mark(ctx, 0);
   CT2G_TRY(ct2g_bin_range(ctx));
-  CT2G_TRY(ct2g_far_field(ctx, false));
-  CT2G_TRY(ct2g_forces(ctx, false));
+  CT2G_TRY(ct2g_all_forces(ctx, false));
   ctx->pot_valid = false;
   ctx->forces_valid = true;
   ct2g_mark(ctx, 6);
@@ -341,6 +340,7 @@ int ct2g_get_tuning(const ct2g_ctx *ctx, ct2g_tuning *t) {
   t->fft_tile = ctx->fft_tile;
   t->split_mg2l = ctx->split_mg2l;
   t->sparse_path = ctx->sparse_path;
+  t->overlap = ctx->overlap;
   return CT2G_OK;
 }
 
@@ -348,13 +348,15 @@ int ct2g_set_tuning(ct2g_ctx *ctx, const ct2g_tuning *t) {
   if (!ctx || !t) return CT2G_EINVAL;
   if (t->dense_cell < 1 || t->dense_cell > 4096 || t->near_blocks_per_sm < 0 ||
       t->near_blocks_per_sm > 32 || t->fft_tile < 0 || t->fft_tile > 512 ||
-      (t->split_mg2l != 0 && t->split_mg2l != 1) || (t->sparse_path != 0 && t->sparse_path != 1))
+      (t->split_mg2l != 0 && t->split_mg2l != 1) || (t->sparse_path != 0 && t->sparse_path != 1) ||
+      (t->overlap != 0 && t->overlap != 1))
     return ct2g_fail(ctx, CT2G_EINVAL, "tuning out of range");
   ctx->dense_cell = (uint32_t)t->dense_cell;
   ctx->near_blocks_per_sm = t->near_blocks_per_sm;
   ctx->fft_tile = t->fft_tile;
   ctx->split_mg2l = t->split_mg2l;
   ctx->sparse_path = t->sparse_path;
+  ctx->overlap = t->overlap;
   ctx->epoch++;  // launch shapes are part of a recorded graph
   ctx->grid_valid = false;  // the chunk lists depend on dense_cell
   return CT2G_OK;
@@ -377,7 +379,8 @@ int ct2g_autotune(ct2g_ctx *ctx, const ct2g_kick_params *p, float dt, float scal
       ct2g_tuning t;
       std::memset(&t, 0, sizeof(t));
       double ms = 0;
-      if (ls >> k >> t.dense_cell >> t.near_blocks_per_sm >> t.fft_tile >> t.sparse_path >> ms &&
+      if (ls >> k >> t.dense_cell >> t.near_blocks_per_sm >> t.fft_tile >> t.sparse_path >>
+              t.overlap >> ms &&
           k == key &&
           ct2g_set_tuning(ctx, &t) == CT2G_OK) {
         if (out) *out = t;
@@ -405,20 +408,25 @@ int ct2g_autotune(ct2g_ctx *ctx, const ct2g_kick_params *p, float dt, float scal
     return CT2G_OK;
   };
   if (rc == CT2G_OK) rc = time_one(best, best_ms);
-  // coordinate descent over the four shapes
+  // coordinate descent over the five shapes
   const int W = ctx->M >= 256 ? 16 : 4096 / ctx->M;
   std::vector<std::vector<int>> cand = {
       {8, 12, 16, 24, 32, 48},  // dense_cell
-      {0, 1, 2},                // near_blocks_per_sm
+      {0, 1, 2, 3},             // near_blocks_per_sm
       ctx->M >= 64 ? std::vector<int>{0, W / 2, 2 * W} : std::vector<int>{0},
-      {0, 1}};                  // sparse_path
-  for (int dim = 0; dim < 4 && rc == CT2G_OK; dim++) {
+      {0, 1},                   // sparse_path
+      {0, 1}};                  // overlap
+  // the overlap first: it changes which near-field footprint is best
+  const int dims[5] = {4, 1, 0, 2, 3};
+  for (int di = 0; di < 5 && rc == CT2G_OK; di++) {
+    const int dim = dims[di];
     for (int v : cand[dim]) {
       ct2g_tuning t = best;
-      int *field = dim == 0 ? &t.dense_cell
+      int *field = dim == 0   ? &t.dense_cell
                    : dim == 1 ? &t.near_blocks_per_sm
                    : dim == 2 ? &t.fft_tile
-                              : &t.sparse_path;
+                   : dim == 3 ? &t.sparse_path
+                              : &t.overlap;
       if (*field == v) continue;
       *field = v;
       float ms = 0.f;
@@ -442,7 +450,7 @@ int ct2g_autotune(ct2g_ctx *ctx, const ct2g_kick_params *p, float dt, float scal
     std::ofstream f(cache_path, std::ios::app);
     if (f)
       f << key << ' ' << best.dense_cell << ' ' << best.near_blocks_per_sm << ' ' << best.fft_tile
-        << ' ' << best.sparse_path << ' ' << best_ms << '\n';
+        << ' ' << best.sparse_path << ' ' << best.overlap << ' ' << best_ms << '\n';
   }
   if (out) *out = best;
   return CT2G_OK;

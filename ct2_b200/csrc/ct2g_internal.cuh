@@ -218,6 +218,10 @@ struct ct2g_ctx {
   int device = 0;
   int num_sms = 0;
   cudaStream_t stream = nullptr;
+  // the near field's own stream when it overlaps the mesh solve, and the
+  // events that fork it from and join it back to `stream`
+  cudaStream_t stream2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaEvent_t ev[8] = {};
   float stage_ms[8] = {};
   std::string err;
@@ -255,6 +259,7 @@ struct ct2g_ctx {
   int fft_tile = 0;            // y/x FFT pass tile width (0: default)
   int split_mg2l = 0;          // 1: X passes and MG2L as three launches, not one
   int sparse_path = 1;         // sparse sinks: 0 one per lane, 1 per-block warp chunks
+  int overlap = 0;             // 1: near field on stream2, concurrent with the mesh solve
   struct ct2g_batch *self_batch = nullptr;  // graph of ct2g_kick_drift
   struct ct2g_learn *learn = nullptr;       // learned near-field correction
   bool fft_tc = false;                      // y/x FFT passes on the tensor cores
@@ -274,6 +279,8 @@ struct ct2g_ctx {
   bool capturing = false;            // recording a CUDA graph: no events, no host reads
   // forces
   float *fx = nullptr, *fy = nullptr, *fz = nullptr, *pot = nullptr;
+  // near-field accelerations while they run beside the mesh solve (overlap)
+  float *nfx = nullptr, *nfy = nullptr, *nfz = nullptr, *npot = nullptr;
   int *d_maxrung = nullptr;
   unsigned long long *d_inter = nullptr;
   uint32_t *h_pinned = nullptr;  // small pinned host scratch
@@ -401,8 +408,12 @@ int ct2g_mg2l_split(ct2g_ctx *ctx);
 size_t ct2g_greens_x_floats(const ct2g_ctx *ctx);
 // the learned correction will run on the next force computation
 bool ct2g_learned_active(const ct2g_ctx *ctx);
-// forces of the current range; pot: also the potential (diagnostics)
+// near-field forces of the current range added to the far field already in
+// the force buffers; pot: also the potential (diagnostics)
 int ct2g_forces(ct2g_ctx *ctx, bool pot);
+// far field and near field of the current range (the mesh solve, then or
+// beside it the near field, per ctx->overlap)
+int ct2g_all_forces(ct2g_ctx *ctx, bool pot);
 int ct2g_update(ct2g_ctx *ctx, const ct2g_kick_params *p, int *max_rung, bool fuse_drift,
                 float drift_dt, float drift_scale);
 int ct2g_drift_all(ct2g_ctx *ctx, float dt, float scale);

@@ -1300,8 +1300,7 @@ int ct2g_learned_collect(ct2g_ctx *ctx, size_t *ncells) {
   }
   const int mode = L->mode;
   L->mode = CT2G_SELECT_NONE;
-  int rc = ct2g_far_field(ctx, false);
-  if (rc == CT2G_OK) rc = ct2g_forces(ctx, false);
+  int rc = ct2g_all_forces(ctx, false);
   L->mode = mode;
   CT2G_TRY(rc);
   ctx->forces_valid = true;

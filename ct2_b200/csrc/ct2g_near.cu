@@ -125,7 +125,8 @@ __device__ __forceinline__ void near_chunk(
     const uint32_t *__restrict__ skeys, uint32_t rbegin, const float4 *__restrict__ src,
     int mbits, float soft, float lo2, float bw2, const float *__restrict__ box_gm,
     float *__restrict__ ofx, float *__restrict__ ofy, float *__restrict__ ofz,
-    float *__restrict__ opot, unsigned long long *__restrict__ inter, float4 *sb, int lane) {
+    float *__restrict__ opot, bool store, unsigned long long *__restrict__ inter, float4 *sb,
+    int lane) {
   const int M = 1 << mbits;
   const bool act = (uint32_t)lane < cd.y;
   const uint32_t slot = cd.x + (act ? (uint32_t)lane : 0u);
@@ -327,12 +328,23 @@ __device__ __forceinline__ void near_chunk(
       np += a0 + a1;
     }
   }
-  // the far field (L2P, with GM) is already in the force buffers
+  // added to the far field (L2P, with GM) already in the force buffers, or
+  // stored into the near-field buffers when the two run side by side; the
+  // product is rounded on its own (no fused multiply-add into the far
+  // field), so that both forms add the same two values
   if (act) {
-    ofx[i] += GM * nx;
-    ofy[i] += GM * ny;
-    ofz[i] += GM * nz;
-    if (POT) opot[i] += GM * np;
+    const float gx = __fmul_rn(GM, nx), gy = __fmul_rn(GM, ny), gz = __fmul_rn(GM, nz);
+    if (store) {
+      ofx[i] = gx;
+      ofy[i] = gy;
+      ofz[i] = gz;
+      if (POT) opot[i] = __fmul_rn(GM, np);
+    } else {
+      ofx[i] += gx;
+      ofy[i] += gy;
+      ofz[i] += gz;
+      if (POT) opot[i] += __fmul_rn(GM, np);
+    }
   }
   unsigned long long c = nsrc;
 #pragma unroll
@@ -354,7 +366,8 @@ __global__ void __launch_bounds__(256, 4) near_kernel(
     Walk walk, const uint32_t *__restrict__ skeys, uint32_t rbegin,
     const float4 *__restrict__ src, int mbits, float soft, float lo2, float bw2,
     const float *__restrict__ box_gm, float *__restrict__ ofx, float *__restrict__ ofy,
-    float *__restrict__ ofz, float *__restrict__ opot, unsigned long long *__restrict__ inter) {
+    float *__restrict__ ofz, float *__restrict__ opot, bool store,
+    unsigned long long *__restrict__ inter) {
   __shared__ float4 sbuf[8][32];  // one batch of 32 sources per warp
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const uint32_t nch = *nch_ptr;
@@ -366,7 +379,7 @@ __global__ void __launch_bounds__(256, 4) near_kernel(
     if (ch >= nch) break;
     near_chunk<KERNEL, POT, SPARSE>(list[ch], sparse_list, cs, occ, stmask, walk, skeys, rbegin,
                                     src, mbits, soft, lo2, bw2, box_gm, ofx, ofy, ofz, opot,
-                                    inter, sbuf[wib], lane);
+                                    store, inter, sbuf[wib], lane);
   }
 }
 
@@ -387,7 +400,7 @@ __global__ void __launch_bounds__(256, 4) near_lane_kernel(
     Walk walk, const uint32_t *__restrict__ skeys, uint32_t rbegin,
     const float4 *__restrict__ src, int mbits, float soft, const float *__restrict__ box_gm,
     float *__restrict__ ofx, float *__restrict__ ofy, float *__restrict__ ofz,
-    float *__restrict__ opot, unsigned long long *__restrict__ inter) {
+    float *__restrict__ opot, bool store, unsigned long long *__restrict__ inter) {
   const int lane = threadIdx.x & 31;
   const uint32_t ns = *nsparse_ptr;
   const int M = 1 << mbits;
@@ -471,11 +484,20 @@ __global__ void __launch_bounds__(256, 4) near_lane_kernel(
           np += a0 + a1;
         }
       }
-      // the far field (L2P, with GM) is already in the force buffers
-      ofx[i] += GM * nx;
-      ofy[i] += GM * ny;
-      ofz[i] += GM * nz;
-      if (POT) opot[i] += GM * np;
+      // added to the far field already in the force buffers, or stored (the
+      // product rounded on its own, as in near_chunk)
+      const float gx = __fmul_rn(GM, nx), gy = __fmul_rn(GM, ny), gz = __fmul_rn(GM, nz);
+      if (store) {
+        ofx[i] = gx;
+        ofy[i] = gy;
+        ofz[i] = gz;
+        if (POT) opot[i] = __fmul_rn(GM, np);
+      } else {
+        ofx[i] += gx;
+        ofy[i] += gy;
+        ofz[i] += gz;
+        if (POT) opot[i] += __fmul_rn(GM, np);
+      }
     }
     unsigned long long c = nsrc;
 #pragma unroll
@@ -485,7 +507,8 @@ __global__ void __launch_bounds__(256, 4) near_lane_kernel(
 }
 
 template <int K, bool POT>
-int launch_near_lanes(ct2g_ctx *ctx, const Walk &walk) {
+int launch_near_lanes(ct2g_ctx *ctx, const Walk &walk, cudaStream_t st, float *fx, float *fy,
+                      float *fz, float *pot, bool store) {
   auto k = near_lane_kernel<K, POT>;
   int per_sm = 0;
   CT2G_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 256, 0));
@@ -494,10 +517,10 @@ int launch_near_lanes(ct2g_ctx *ctx, const Walk &walk) {
   size_t blocks = (size_t)std::max(1, per_sm) * ctx->num_sms;
   blocks = std::max<size_t>(1, std::min(blocks, (nr + 255) / 256));
   uint32_t *c = ctx->d_counts;
-  k<<<(unsigned)blocks, 256, 0, ctx->stream>>>(
+  k<<<(unsigned)blocks, 256, 0, st>>>(
       c + 1, c + 4, ctx->sparse_list, ctx->cell_start, ctx->occ, ctx->stmask, walk, ctx->keys,
-      (uint32_t)ctx->rung_begin, ctx->src, ctx->mbits, ctx->opt.hsoft, ctx->box_gm, ctx->fx,
-      ctx->fy, ctx->fz, ctx->pot, ctx->d_inter);
+      (uint32_t)ctx->rung_begin, ctx->src, ctx->mbits, ctx->opt.hsoft, ctx->box_gm, fx, fy, fz,
+      pot, store, ctx->d_inter);
   CT2G_LAUNCHED(ctx);
   return CT2G_OK;
 }
@@ -518,18 +541,20 @@ template <int K, bool POT, bool SPARSE>
 int launch_near1(ct2g_ctx *ctx, const Walk &walk, const uint2 *chunks, const uint32_t *nch,
                  const uint32_t *off, uint32_t *work, const uint32_t *slist,
                  const unsigned long long *stm, float lo2, float bw2, float *fx, float *fy,
-                 float *fz, float *pot, unsigned long long *inter) {
+                 float *fz, float *pot, unsigned long long *inter, cudaStream_t st = nullptr,
+                 bool store = false) {
   auto k = near_kernel<K, POT, SPARSE>;
+  if (!st) st = ctx->stream;
   int per_sm = 0;
   CT2G_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 256, 0));
   const size_t nr = ctx->n - ctx->rung_begin;
   if (ctx->near_blocks_per_sm > 0) per_sm = std::min(per_sm, ctx->near_blocks_per_sm);
   size_t blocks = (size_t)std::max(1, per_sm) * ctx->num_sms;
   blocks = std::max<size_t>(1, std::min(blocks, (nr + 255) / 256));
-  k<<<(unsigned)blocks, 256, 0, ctx->stream>>>(
+  k<<<(unsigned)blocks, 256, 0, st>>>(
       chunks, nch, off, work, slist, ctx->cell_start, ctx->occ, stm, walk, ctx->keys,
       (uint32_t)ctx->rung_begin, ctx->src, ctx->mbits, ctx->opt.hsoft, lo2, bw2, ctx->box_gm, fx,
-      fy, fz, pot, inter);
+      fy, fz, pot, store, inter);
   CT2G_LAUNCHED(ctx);
   return CT2G_OK;
 }
@@ -538,17 +563,41 @@ int launch_near1(ct2g_ctx *ctx, const Walk &walk, const uint2 *chunks, const uin
 // (counts[1] of them; work counter counts[4]): one per lane (sparse_path 0) or
 // as the per-block chunks stored after the dense ones (counts[2], sparse_path 1)
 template <int K, bool POT>
-int launch_near(ct2g_ctx *ctx) {
+int launch_near(ct2g_ctx *ctx, cudaStream_t st, float *fx, float *fy, float *fz, float *pot,
+                bool store) {
   const Walk walk = make_walk(ctx->mbits);
   const float bw2 = ctx->opt.bwidth * ctx->opt.bwidth;
   uint32_t *c = ctx->d_counts;
   CT2G_TRY((launch_near1<K, POT, false>(ctx, walk, ctx->chunks, c + 0, nullptr, c + 3,
-                                        ctx->sparse_list, ctx->stmask, -1.f, bw2, ctx->fx,
-                                        ctx->fy, ctx->fz, ctx->pot, ctx->d_inter)));
-  if (ctx->sparse_path == 0) return launch_near_lanes<K, POT>(ctx, walk);
+                                        ctx->sparse_list, ctx->stmask, -1.f, bw2, fx, fy, fz, pot,
+                                        ctx->d_inter, st, store)));
+  if (ctx->sparse_path == 0) return launch_near_lanes<K, POT>(ctx, walk, st, fx, fy, fz, pot, store);
   return launch_near1<K, POT, true>(ctx, walk, ctx->chunks, c + 2, c + 0, c + 4,
-                                    ctx->sparse_list, ctx->stmask, -1.f, bw2, ctx->fx, ctx->fy,
-                                    ctx->fz, ctx->pot, ctx->d_inter);
+                                    ctx->sparse_list, ctx->stmask, -1.f, bw2, fx, fy, fz, pot,
+                                    ctx->d_inter, st, store);
+}
+
+int near_all(ct2g_ctx *ctx, bool pot, cudaStream_t st, float *fx, float *fy, float *fz,
+             float *po, bool store) {
+  if (ctx->opt.kernel == CT2G_SOFT_SPHERE)
+    return pot ? launch_near<CT2G_SOFT_SPHERE, true>(ctx, st, fx, fy, fz, po, store)
+               : launch_near<CT2G_SOFT_SPHERE, false>(ctx, st, fx, fy, fz, po, store);
+  return pot ? launch_near<CT2G_SOFT_PLUMMER, true>(ctx, st, fx, fy, fz, po, store)
+             : launch_near<CT2G_SOFT_PLUMMER, false>(ctx, st, fx, fy, fz, po, store);
+}
+
+// far field + near field, added in that order: f = far + GM * near
+__global__ void combine_kernel(size_t b, size_t n, float *__restrict__ fx, float *__restrict__ fy,
+                               float *__restrict__ fz, const float *__restrict__ nfx,
+                               const float *__restrict__ nfy, const float *__restrict__ nfz,
+                               float *__restrict__ po, const float *__restrict__ npo) {
+  for (size_t i = b + blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    fx[i] += nfx[i];
+    fy[i] += nfy[i];
+    fz[i] += nfz[i];
+    if (po) po[i] += npo[i];
+  }
 }
 
 }  // namespace
@@ -614,18 +663,43 @@ int ct2g_upload_stencil(ct2g_ctx *ctx, const std::vector<int> &st4) {
 }
 
 int ct2g_forces(ct2g_ctx *ctx, bool pot) {
-  const size_t n = ctx->n;
   // the far-field pass (the inverse z pass with L2P) has written the range's entries
-  (void)n;
   CT2G_CUDA(ctx, cudaMemsetAsync(ctx->d_inter, 0, sizeof(unsigned long long), ctx->stream));
   CT2G_CUDA(ctx, cudaMemsetAsync(ctx->d_counts + 3, 0, 2 * sizeof(uint32_t), ctx->stream));
   if (ctx->n == ctx->rung_begin) return CT2G_OK;
-  int rc;
-  if (ctx->opt.kernel == CT2G_SOFT_SPHERE)
-    rc = pot ? launch_near<CT2G_SOFT_SPHERE, true>(ctx) : launch_near<CT2G_SOFT_SPHERE, false>(ctx);
-  else
-    rc = pot ? launch_near<CT2G_SOFT_PLUMMER, true>(ctx) : launch_near<CT2G_SOFT_PLUMMER, false>(ctx);
+  CT2G_TRY(near_all(ctx, pot, ctx->stream, ctx->fx, ctx->fy, ctx->fz, ctx->pot, false));
+  return ct2g_learned_apply(ctx, pot);
+}
+
+// Far field and near field of the current range.  Serial (ctx->overlap 0):
+// the mesh solve writes the far field, then the near field adds to it.
+// Overlapped: the near field forks onto stream2 as soon as binning is done
+// and stores into its own buffers while the mesh solve runs on the context
+// stream (the near kernels are issue-bound, the mesh passes bound by memory
+// latency, so the two fill each other's idle cycles); the context stream then
+// joins it and adds the two, in the serial order (far + GM near), so both
+// forms give the same forces bit for bit.
+int ct2g_all_forces(ct2g_ctx *ctx, bool pot) {
+  if (!ctx->overlap || ctx->n == ctx->rung_begin) {
+    CT2G_TRY(ct2g_far_field(ctx, pot));
+    return ct2g_forces(ctx, pot);
+  }
+  cudaStream_t st = ctx->stream;
+  CT2G_CUDA(ctx, cudaMemsetAsync(ctx->d_inter, 0, sizeof(unsigned long long), st));
+  CT2G_CUDA(ctx, cudaMemsetAsync(ctx->d_counts + 3, 0, 2 * sizeof(uint32_t), st));
+  CT2G_CUDA(ctx, cudaEventRecord(ctx->ev_fork, st));
+  CT2G_CUDA(ctx, cudaStreamWaitEvent(ctx->stream2, ctx->ev_fork, 0));
+  CT2G_TRY(near_all(ctx, pot, ctx->stream2, ctx->nfx, ctx->nfy, ctx->nfz, ctx->npot, true));
+  CT2G_CUDA(ctx, cudaEventRecord(ctx->ev_join, ctx->stream2));
+  const int rc = ct2g_far_field(ctx, pot);
+  // join before any return, so that stream2 never outlives a recording
+  CT2G_CUDA(ctx, cudaStreamWaitEvent(st, ctx->ev_join, 0));
   CT2G_TRY(rc);
+  const size_t b = ctx->rung_begin, nr = ctx->n - b;
+  combine_kernel<<<(unsigned)std::min<size_t>((nr + 255) / 256, (size_t)ctx->num_sms * 16), 256, 0,
+                   st>>>(b, ctx->n, ctx->fx, ctx->fy, ctx->fz, ctx->nfx, ctx->nfy, ctx->nfz,
+                         pot ? ctx->pot : nullptr, ctx->npot);
+  CT2G_LAUNCHED(ctx);
   return ct2g_learned_apply(ctx, pot);
 }
 

@@ -222,14 +222,20 @@ int ct2g_batch_destroy(ct2g_batch *b);
  * their stencils, each source batch staged once in shared memory; 0: one
  * sparse sink per warp lane, each lane walking its own stencil and reading
  * its own sources (no masked work, but every lane gathers its own sources
- * through the L1 cache). */
+ * through the L1 cache); overlap -- 1: the near field runs on a second stream
+ * beside the mesh solve (from the end of binning to the L2P pass) into its
+ * own buffers, added to the far field afterwards in the same order as the
+ * serial form (0), so both give the same forces bit for bit; the per-stage
+ * times then show only the part of the near field the mesh solve did not
+ * hide. */
 typedef struct {
   int dense_cell;
   int near_blocks_per_sm;
   int fft_tile;
   int split_mg2l;
   int sparse_path;
-  int reserved[3];
+  int overlap;
+  int reserved[2];
 } ct2g_tuning;
 int ct2g_get_tuning(const ct2g_ctx *ctx, ct2g_tuning *t);
 int ct2g_set_tuning(ct2g_ctx *ctx, const ct2g_tuning *t);
