@@ -117,6 +117,28 @@ void ct2g_mark(ct2g_ctx *ctx, int k) {
 
 int ct2g_check(ct2g_ctx *ctx) { return check(ctx); }
 
+// resident blocks per SM of a kernel from its registers, its shared memory
+// (static + dynamic + the 1 KB the system reserves per block) against the
+// SM's maximum carveout, and its threads
+int ct2g_blocks_per_sm(ct2g_ctx *ctx, const void *kernel, int threads, size_t dyn_smem) {
+  cudaFuncAttributes fa;
+  if (cudaFuncGetAttributes(&fa, kernel) != cudaSuccess) {
+    cudaGetLastError();
+    return 1;
+  }
+  int smem_sm = 0, regs_sm = 0, threads_sm = 0;
+  cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->device);
+  cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, ctx->device);
+  cudaDeviceGetAttribute(&threads_sm, cudaDevAttrMaxThreadsPerMultiProcessor, ctx->device);
+  // registers are allocated per warp in units of 256
+  const int regs_warp = ((std::max(1, fa.numRegs) * 32 + 255) / 256) * 256;
+  const int warps = (threads + 31) / 32;
+  const int by_regs = regs_sm / std::max(1, regs_warp * warps);
+  const int by_smem = smem_sm / (int)std::max<size_t>(1, dyn_smem + fa.sharedSizeBytes + 1024);
+  const int by_threads = threads_sm / std::max(1, threads);
+  return std::max(1, std::min(std::min(by_regs, by_smem), by_threads));
+}
+
 int ct2g_device_error(ct2g_ctx *ctx) {
   uint32_t e = 0;
   CT2G_CUDA(ctx, cudaStreamSynchronize(ctx->stream));

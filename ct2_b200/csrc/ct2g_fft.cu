@@ -442,6 +442,9 @@ int launch_pipe(ct2g_ctx *ctx, C2 *spec, size_t nouter, size_t ostride, size_t r
   CT2G_TRY(ct2g_smem_attrs(ctx, k, smem));
   int per_sm = 0;
   CT2G_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 256, smem));
+  // the query can miss the maximum carveout the attributes ask for: count
+  // from the kernel's registers and shared memory as well, keep the larger
+  per_sm = std::max(per_sm, ct2g_blocks_per_sm(ctx, (const void *)k, 256, smem));
   const int ntiles = (int)((ncols + W - 1) / W);
   const size_t ntot = nouter * ntiles;
   const size_t grid = std::min(ntot, (size_t)std::max(1, per_sm) * ctx->num_sms);
@@ -998,15 +1001,21 @@ int launch_c2r_l2p(ct2g_ctx *ctx, int mode) {
 // step reads the column's moments from HBM into registers, the last one
 // writes the expansions back from registers; the Green's values ([c][qi], one
 // contiguous run of the column-ordered table) arrive by cp.async meanwhile.
-template <int P, int N>
+// GD: the Green's values are read straight from HBM by the contraction (no
+// shared-memory copy of the Green's column, so one more block fits per SM)
+template <int P, int N, bool GD = false>
 struct FxShape {
   static constexpr int NC = ct2g_ncomp(P), NH = N / 2 + 1;
   static constexpr int GCOL = NC * N;  // floats per Green's column (a multiple of 8)
-  static constexpr size_t SMEM =
-      sizeof(float2) * (size_t)N + sizeof(float2) * (size_t)N * NC + sizeof(float) * (size_t)GCOL;
+  static constexpr size_t SMEM = sizeof(float2) * (size_t)N + sizeof(float2) * (size_t)N * NC +
+                                 (GD ? 0 : sizeof(float) * (size_t)GCOL);
   static constexpr bool FITS = SMEM <= 227 * 1024;
-  static constexpr int MINB = SMEM <= 112 * 1024 ? 2 : 1;
-  static constexpr bool GREG = NC <= 35;  // Green's values in registers
+  // three blocks per SM only where the contraction fits 85 registers
+  // (orders up to 4 with the Green's values read directly)
+  static constexpr int MINB = (GD && NC <= 35 && SMEM <= 75 * 1024) ? 3
+                              : SMEM <= 112 * 1024                  ? 2
+                                                                    : 1;
+  static constexpr bool GREG = !GD && NC <= 35;  // Green's values in registers
   // (a persistent form with one 512-thread block per SM and the next
   // column's data arriving by cp.async in a second buffer measured slower:
   // 2.45 against 1.90 ms at N = 256, order 4)
@@ -1068,11 +1077,11 @@ __device__ __forceinline__ void cols_step2(const float2 *s, ST st) {
   }
 }
 
-template <int P, int N>
-__global__ void __launch_bounds__(256, FxShape<P, N>::MINB) fftx_mg2l_kernel(
+template <int P, int N, bool GD>
+__global__ void __launch_bounds__(256, FxShape<P, N, GD>::MINB) fftx_mg2l_kernel(
     float2 *__restrict__ spec, int ldk, const float *__restrict__ gx,
     const float2 *__restrict__ tw) {
-  using S = FxShape<P, N>;
+  using S = FxShape<P, N, GD>;
   constexpr int NC = S::NC, NH = S::NH;
   extern __shared__ __align__(16) unsigned char smraw[];
   float2 *stw = reinterpret_cast<float2 *>(smraw);
@@ -1083,23 +1092,29 @@ __global__ void __launch_bounds__(256, FxShape<P, N>::MINB) fftx_mg2l_kernel(
   const int box = (int)(blockIdx.x / ((unsigned)NH * N));
   const int64_t RS = (int64_t)ldk * NC, XS = (int64_t)N * RS;
   float2 *col = spec + (int64_t)box * N * XS + (int64_t)qj * RS + (int64_t)qk * NC;
-  // the Green's values arrive while the forward transform runs
+  // the Green's values arrive while the forward transform runs (or, GD, are
+  // read by the contraction itself)
   const float *gcol = gx + ((int64_t)qj * NH + qk) * S::GCOL;
-  for (int e = threadIdx.x; e < S::GCOL / 4; e += 256) cp_async16(sg + 4 * e, gcol + 4 * e);
-  cp_async_commit();
+  if constexpr (!GD) {
+    for (int e = threadIdx.x; e < S::GCOL / 4; e += 256) cp_async16(sg + 4 * e, gcol + 4 * e);
+    cp_async_commit();
+  }
   load_twiddles(stw, tw, N);
   __syncthreads();
   // forward: the first step reads the column from HBM
   cols_step1<N, NC, false, 256>(s, stw, [&](int l, int r) { return col[r * XS + l]; });
   __syncthreads();
   cols_step2<N, NC, false, true, 256>(s, [&](int l, int r, float2 v) { s[r * NC + l] = v; });
-  cp_async_wait<0>();
+  if constexpr (!GD) cp_async_wait<0>();
   __syncthreads();
   for (int qi = threadIdx.x; qi < N; qi += 256) {
     float2 m[NC];
 #pragma unroll
     for (int k = 0; k < NC; k++) m[k] = s[qi * NC + k];
-    if constexpr (S::GREG) {
+    if constexpr (GD) {
+      ct2g_mg2l_all<P, N>(m, gcol + qi, s + qi * NC,
+                          std::make_integer_sequence<int, Mg2lPairs<P>::NP>{});
+    } else if constexpr (S::GREG) {
       float g[NC];
 #pragma unroll
       for (int k = 0; k < NC; k++) g[k] = sg[k * N + qi];
@@ -1116,20 +1131,26 @@ __global__ void __launch_bounds__(256, FxShape<P, N>::MINB) fftx_mg2l_kernel(
   cols_step2<N, NC, true, false, 256>(s, [&](int l, int r, float2 v) { col[r * XS + l] = v; });
 }
 
-template <int P, int N>
-int launch_fx_mg2l(ct2g_ctx *ctx) {
-  using S = FxShape<P, N>;
+template <int P, int N, bool GD>
+int launch_fx_mg2l_g(ct2g_ctx *ctx) {
+  using S = FxShape<P, N, GD>;
   if constexpr (!S::FITS) {
     return ct2g_fail(ctx, CT2G_EINVAL, "fused X pass + MG2L does not fit in shared memory");
   } else {
     const size_t ncol = (size_t)ctx->nbox * N * S::NH;
-    auto k = fftx_mg2l_kernel<P, N>;
+    auto k = fftx_mg2l_kernel<P, N, GD>;
     CT2G_TRY(ct2g_smem_attrs(ctx, k, S::SMEM));
     k<<<(unsigned)ncol, 256, S::SMEM, ctx->stream>>>(ctx->spec, ctx->ldk, ctx->greens_x,
                                                      twiddle_ptr<float2>(ctx));
     CT2G_LAUNCHED(ctx);
     return CT2G_OK;
   }
+}
+
+template <int P, int N>
+int launch_fx_mg2l(ct2g_ctx *ctx) {
+  return ctx->mg2l_greens_direct ? launch_fx_mg2l_g<P, N, true>(ctx)
+                                 : launch_fx_mg2l_g<P, N, false>(ctx);
 }
 
 // the Y pass (tiles of the (qk, c) columns of each (box, qi) plane) or the

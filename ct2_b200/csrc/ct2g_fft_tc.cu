@@ -336,9 +336,13 @@ int launch_tc(ct2g_ctx *ctx, float2 *spec, size_t nouter, size_t ostride, size_t
   // all of the unified L1 as shared memory, so that several CTAs fit per SM
   CT2G_CUDA(ctx, cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
                                       (int)cudaSharedmemCarveoutMaxShared));
-  int per_sm = 0;
-  CT2G_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 128, S::SMEM));
-  per_sm = std::max(1, std::min(per_sm, (int)(512 / S::TCOLS)));  // tensor memory columns
+  // CTAs per SM from the kernel's own limits -- registers, shared memory at
+  // the maximum carveout, tensor-memory columns -- rather than from the
+  // occupancy query, which reported one CTA per SM here (it does not apply
+  // the carveout preference set above)
+  int per_sm = std::min(ct2g_blocks_per_sm(ctx, (const void *)k, 128, S::SMEM),
+                        (int)(512 / S::TCOLS));
+  per_sm = std::max(1, per_sm);
   const uint32_t ntiles = (uint32_t)((ncols + TW - 1) / TW);
   const size_t ntot = nouter * ntiles;
   const size_t grid = std::min(ntot, (size_t)per_sm * ctx->num_sms);

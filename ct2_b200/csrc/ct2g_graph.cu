@@ -341,6 +341,7 @@ int ct2g_get_tuning(const ct2g_ctx *ctx, ct2g_tuning *t) {
   t->split_mg2l = ctx->split_mg2l;
   t->sparse_path = ctx->sparse_path;
   t->overlap = ctx->overlap;
+  t->mg2l_greens_direct = ctx->mg2l_greens_direct;
   return CT2G_OK;
 }
 
@@ -349,7 +350,8 @@ int ct2g_set_tuning(ct2g_ctx *ctx, const ct2g_tuning *t) {
   if (t->dense_cell < 1 || t->dense_cell > 4096 || t->near_blocks_per_sm < 0 ||
       t->near_blocks_per_sm > 32 || t->fft_tile < 0 || t->fft_tile > 512 ||
       (t->split_mg2l != 0 && t->split_mg2l != 1) || (t->sparse_path != 0 && t->sparse_path != 1) ||
-      (t->overlap != 0 && t->overlap != 1))
+      (t->overlap != 0 && t->overlap != 1) ||
+      (t->mg2l_greens_direct != 0 && t->mg2l_greens_direct != 1))
     return ct2g_fail(ctx, CT2G_EINVAL, "tuning out of range");
   ctx->dense_cell = (uint32_t)t->dense_cell;
   ctx->near_blocks_per_sm = t->near_blocks_per_sm;
@@ -357,6 +359,7 @@ int ct2g_set_tuning(ct2g_ctx *ctx, const ct2g_tuning *t) {
   ctx->split_mg2l = t->split_mg2l;
   ctx->sparse_path = t->sparse_path;
   ctx->overlap = t->overlap;
+  ctx->mg2l_greens_direct = t->mg2l_greens_direct;
   ctx->epoch++;  // launch shapes are part of a recorded graph
   ctx->grid_valid = false;  // the chunk lists depend on dense_cell
   return CT2G_OK;
@@ -380,7 +383,7 @@ int ct2g_autotune(ct2g_ctx *ctx, const ct2g_kick_params *p, float dt, float scal
       std::memset(&t, 0, sizeof(t));
       double ms = 0;
       if (ls >> k >> t.dense_cell >> t.near_blocks_per_sm >> t.fft_tile >> t.sparse_path >>
-              t.overlap >> ms &&
+              t.overlap >> t.mg2l_greens_direct >> ms &&
           k == key &&
           ct2g_set_tuning(ctx, &t) == CT2G_OK) {
         if (out) *out = t;
@@ -408,17 +411,18 @@ int ct2g_autotune(ct2g_ctx *ctx, const ct2g_kick_params *p, float dt, float scal
     return CT2G_OK;
   };
   if (rc == CT2G_OK) rc = time_one(best, best_ms);
-  // coordinate descent over the five shapes
+  // coordinate descent over the six shapes
   const int W = ctx->M >= 256 ? 16 : 4096 / ctx->M;
   std::vector<std::vector<int>> cand = {
       {8, 12, 16, 24, 32, 48},  // dense_cell
       {0, 1, 2, 3},             // near_blocks_per_sm
       ctx->M >= 64 ? std::vector<int>{0, W / 2, 2 * W} : std::vector<int>{0},
       {0, 1},                   // sparse_path
-      {0, 1}};                  // overlap
+      {0, 1},                   // overlap
+      {0, 1}};                  // mg2l_greens_direct
   // the overlap first: it changes which near-field footprint is best
-  const int dims[5] = {4, 1, 0, 2, 3};
-  for (int di = 0; di < 5 && rc == CT2G_OK; di++) {
+  const int dims[6] = {4, 1, 0, 2, 3, 5};
+  for (int di = 0; di < 6 && rc == CT2G_OK; di++) {
     const int dim = dims[di];
     for (int v : cand[dim]) {
       ct2g_tuning t = best;
@@ -426,7 +430,8 @@ int ct2g_autotune(ct2g_ctx *ctx, const ct2g_kick_params *p, float dt, float scal
                    : dim == 1 ? &t.near_blocks_per_sm
                    : dim == 2 ? &t.fft_tile
                    : dim == 3 ? &t.sparse_path
-                              : &t.overlap;
+                   : dim == 4 ? &t.overlap
+                              : &t.mg2l_greens_direct;
       if (*field == v) continue;
       *field = v;
       float ms = 0.f;
@@ -450,7 +455,8 @@ int ct2g_autotune(ct2g_ctx *ctx, const ct2g_kick_params *p, float dt, float scal
     std::ofstream f(cache_path, std::ios::app);
     if (f)
       f << key << ' ' << best.dense_cell << ' ' << best.near_blocks_per_sm << ' ' << best.fft_tile
-        << ' ' << best.sparse_path << ' ' << best.overlap << ' ' << best_ms << '\n';
+        << ' ' << best.sparse_path << ' ' << best.overlap << ' ' << best.mg2l_greens_direct << ' '
+        << best_ms << '\n';
   }
   if (out) *out = best;
   return CT2G_OK;

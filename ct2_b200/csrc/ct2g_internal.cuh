@@ -260,6 +260,7 @@ struct ct2g_ctx {
   int split_mg2l = 0;          // 1: X passes and MG2L as three launches, not one
   int sparse_path = 1;         // sparse sinks: 0 one per lane, 1 per-block warp chunks
   int overlap = 0;             // 1: near field on stream2, concurrent with the mesh solve
+  int mg2l_greens_direct = 0;  // 1: the fused x pass reads the Green's values from HBM
   struct ct2g_batch *self_batch = nullptr;  // graph of ct2g_kick_drift
   struct ct2g_learn *learn = nullptr;       // learned near-field correction
   bool fft_tc = false;                      // y/x FFT passes on the tensor cores
@@ -352,6 +353,9 @@ size_t ct2g_scan_scratch_words(size_t n);
 void ct2g_mark(ct2g_ctx *ctx, int k);
 int ct2g_bin_range(ct2g_ctx *ctx);
 int ct2g_check(ct2g_ctx *ctx);  // valid context; selects its device
+// resident blocks per SM of `kernel` (threads, dynamic shared memory) from its
+// own registers and shared memory at the maximum carveout
+int ct2g_blocks_per_sm(ct2g_ctx *ctx, const void *kernel, int threads, size_t dyn_smem);
 // waits for the stream, then reports a status a kernel left in d_counts[6]
 int ct2g_device_error(ct2g_ctx *ctx);
 // tensor-core FFT passes (ct2g_fft_tc.cu)

@@ -227,7 +227,10 @@ int ct2g_batch_destroy(ct2g_batch *b);
  * own buffers, added to the far field afterwards in the same order as the
  * serial form (0), so both give the same forces bit for bit; the per-stage
  * times then show only the part of the near field the mesh solve did not
- * hide. */
+ * hide; mg2l_greens_direct -- 1: the fused x pass + Green's multiply reads
+ * the Green's values straight from HBM inside the contraction instead of
+ * staging each column in shared memory first (one more block per SM; the
+ * same results). */
 typedef struct {
   int dense_cell;
   int near_blocks_per_sm;
@@ -235,7 +238,8 @@ typedef struct {
   int split_mg2l;
   int sparse_path;
   int overlap;
-  int reserved[2];
+  int mg2l_greens_direct;
+  int reserved[1];
 } ct2g_tuning;
 int ct2g_get_tuning(const ct2g_ctx *ctx, ct2g_tuning *t);
 int ct2g_set_tuning(ct2g_ctx *ctx, const ct2g_tuning *t);
