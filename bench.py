@@ -339,6 +339,7 @@ def learned_form(args, P, n, soft, local, kp, accuracy):
     # the same context with the correction off: the narrow base step alone,
     # so that the correction's own cost (learned - base) is on the line
     gl.learned_select("none")
+    gl.upload_dict(P)
     base_acc = accuracy(gl)
     gl.upload_dict(P)
     for _ in range(args.warmup):

@@ -86,3 +86,21 @@ def test_fullsize_forces_momentum_and_accuracy(gpu, full):
     scale = np.abs(f).astype(np.float64).sum()
     print("sum F / sum |F| =", tot / scale)
     assert np.all(np.abs(tot) < 1e-4 * scale)
+
+
+def test_binning_at_the_largest_mesh(gpu):
+    """mesh 512 (the largest the context takes: 134 M cells, 27-bit keys) on
+    the same 2.1 M particles: order and cell ranges bit-exact."""
+    n = N_SIDE ** 3
+    P = ics.plummer_spheres(n, seed=2, nspheres=512, a=0.005)
+    g = Gravity(mesh=512, order=1, bwidth=1.0, hsoft=1.0 / (50 * N_SIDE), GM=1.0 / n,
+                max_particles=n)
+    g.upload_dict(P)
+    g.particle_to_grid()
+    ids = g.download()["id"].astype(np.int64)
+    perm, cs = O.bin_stable(P["x"], P["y"], P["z"], 9)
+    assert np.array_equal(ids, perm)
+    b, e = g.cells()
+    ob, oe = O.cell_ranges_rowmajor(cs, 9)
+    assert np.array_equal(b, ob) and np.array_equal(e, oe)
+    g.close()
