@@ -328,8 +328,12 @@ int ct2g_create_boxes(const ct2g_options *opt, int nbox, ct2g_ctx **out) {
   int rc = CT2G_OK;
   do {
     if (cudaSetDevice(ctx->device) != cudaSuccess) { rc = CT2G_ENODEV; break; }
-    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) { rc = CT2G_ECUDA; break; }
-    if (cudaStreamCreateWithFlags(&ctx->stream2, cudaStreamNonBlocking) != cudaSuccess ||
+    // the context stream at the highest priority, the near field's own stream
+    // at the lowest: when both have blocks waiting, the mesh solve's go first
+    int prio_least = 0, prio_greatest = 0;
+    cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest);
+    if (cudaStreamCreateWithPriority(&ctx->stream, cudaStreamNonBlocking, prio_greatest) != cudaSuccess) { rc = CT2G_ECUDA; break; }
+    if (cudaStreamCreateWithPriority(&ctx->stream2, cudaStreamNonBlocking, prio_least) != cudaSuccess ||
         cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming) != cudaSuccess) {
       rc = CT2G_ECUDA;

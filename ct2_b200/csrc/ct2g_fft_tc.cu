@@ -23,7 +23,16 @@
 namespace {
 
 constexpr int TW = 8;   // lines per tile
-constexpr int TP = 9;   // tile row pitch (complex): odd, so strided reads spread over the banks
+constexpr int TP = 9;   // tile buffer size per row (complex; the row view uses 8 of them)
+
+// Row view of the tile buffer: element (row r, line c) at r * 8 + (c ^
+// ((r >> 1) & 7)).  The XOR spreads the accesses of a half-warp over all 16
+// complex-wide bank slots in the three patterns that use this view: a row
+// run of (line pairs x 4 rows) when the tile moves in and out, 16 rows of one
+// line for the stage-1 operand, and 16 rows of one line for the stage-2
+// result (a plain pitch of 9 left 2-way conflicts on the first, of 8 made
+// the second 8-way).
+__device__ __forceinline__ int tidx(int r, int c) { return r * 8 + (c ^ ((r >> 1) & 7)); }
 constexpr int R1 = 16;  // radix of stage 2
 constexpr uint32_t kWaitLimit = 1u << 22;
 
@@ -85,7 +94,7 @@ __global__ void __launch_bounds__(128) fft_cols_tc_kernel(float2 *__restrict__ a
   const uint32_t lane_base = (uint32_t)(32 * warp) << 16;
   unsigned char *A = sm;
   const float2 *tw = reinterpret_cast<const float2 *>(sm + S::OFF_TW);
-  float2 *T = reinterpret_cast<float2 *>(sm + S::OFF_T);  // [N][TP], TW used
+  float2 *T = reinterpret_cast<float2 *>(sm + S::OFF_T);  // rows of TW lines (tidx)
   const uint32_t sA = tc::smem_addr(A), sB1 = tc::smem_addr(sm + S::OFF_B1),
                  sB2 = tc::smem_addr(sm + S::OFF_B2);
   uint32_t phase = 0;
@@ -129,8 +138,8 @@ __global__ void __launch_bounds__(128) fft_cols_tc_kernel(float2 *__restrict__ a
 #pragma unroll
     for (int j = 0; j < CH; j++) {
       const int e = tid + 128 * j, r = e >> 2, c = (e & 3) * 2;
-      T[r * TP + c] = make_float2(pre[j].x, pre[j].y);
-      T[r * TP + c + 1] = make_float2(pre[j].z, pre[j].w);
+      T[tidx(r, c)] = make_float2(pre[j].x, pre[j].y);
+      T[tidx(r, c + 1)] = make_float2(pre[j].z, pre[j].w);
     }
     if (tile + gridDim.x < ntot) fetch(tile + gridDim.x);
     __syncthreads();
@@ -140,7 +149,7 @@ __global__ void __launch_bounds__(128) fft_cols_tc_kernel(float2 *__restrict__ a
       float hr[R2], lr[R2], hi_[R2], li[R2];
 #pragma unroll
       for (int n2 = 0; n2 < R2; n2++) {
-        const float2 x = T[(n1 + R1 * n2) * TP + w];
+        const float2 x = T[tidx(n1 + R1 * n2, w)];
         split_bf16(x.x, hr[n2], lr[n2]);
         split_bf16(x.y, hi_[n2], li[n2]);
       }
@@ -245,12 +254,12 @@ __global__ void __launch_bounds__(128) fft_cols_tc_kernel(float2 *__restrict__ a
       float v[32];
       tc::tmem_ld32(tmem + lane_base + (uint32_t)(S::N1 + mt * S::N2), v);
 #pragma unroll
-      for (int k1 = 0; k1 < R1; k1++) T[(k2 + R2 * k1) * TP + w] = make_float2(v[k1], v[R1 + k1]);
+      for (int k1 = 0; k1 < R1; k1++) T[tidx(k2 + R2 * k1, w)] = make_float2(v[k1], v[R1 + k1]);
     }
     __syncthreads();
     for (int e = tid; e < N * 4; e += 128) {
       const int r = e >> 2, c = (e & 3) * 2;
-      const float2 u0 = T[r * TP + c], u1 = T[r * TP + c + 1];
+      const float2 u0 = T[tidx(r, c)], u1 = T[tidx(r, c + 1)];
       const float4 v = make_float4(u0.x, u0.y, u1.x, u1.y);
       if (VEC && c + 1 < wv) {
         *reinterpret_cast<float4 *>(base + (size_t)r * rstride + c) = v;

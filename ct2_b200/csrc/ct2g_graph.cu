@@ -342,6 +342,7 @@ int ct2g_get_tuning(const ct2g_ctx *ctx, ct2g_tuning *t) {
   t->sparse_path = ctx->sparse_path;
   t->overlap = ctx->overlap;
   t->mg2l_greens_direct = ctx->mg2l_greens_direct;
+  t->near_chunks_per_warp = ctx->near_chunks_per_warp;
   return CT2G_OK;
 }
 
@@ -351,7 +352,8 @@ int ct2g_set_tuning(ct2g_ctx *ctx, const ct2g_tuning *t) {
       t->near_blocks_per_sm > 32 || t->fft_tile < 0 || t->fft_tile > 512 ||
       (t->split_mg2l != 0 && t->split_mg2l != 1) || (t->sparse_path != 0 && t->sparse_path != 1) ||
       (t->overlap != 0 && t->overlap != 1) ||
-      (t->mg2l_greens_direct != 0 && t->mg2l_greens_direct != 1))
+      (t->mg2l_greens_direct != 0 && t->mg2l_greens_direct != 1) ||
+      t->near_chunks_per_warp < 0 || t->near_chunks_per_warp > 4096)
     return ct2g_fail(ctx, CT2G_EINVAL, "tuning out of range");
   ctx->dense_cell = (uint32_t)t->dense_cell;
   ctx->near_blocks_per_sm = t->near_blocks_per_sm;
@@ -360,6 +362,7 @@ int ct2g_set_tuning(ct2g_ctx *ctx, const ct2g_tuning *t) {
   ctx->sparse_path = t->sparse_path;
   ctx->overlap = t->overlap;
   ctx->mg2l_greens_direct = t->mg2l_greens_direct;
+  ctx->near_chunks_per_warp = t->near_chunks_per_warp;
   ctx->epoch++;  // launch shapes are part of a recorded graph
   ctx->grid_valid = false;  // the chunk lists depend on dense_cell
   return CT2G_OK;
@@ -383,7 +386,7 @@ int ct2g_autotune(ct2g_ctx *ctx, const ct2g_kick_params *p, float dt, float scal
       std::memset(&t, 0, sizeof(t));
       double ms = 0;
       if (ls >> k >> t.dense_cell >> t.near_blocks_per_sm >> t.fft_tile >> t.sparse_path >>
-              t.overlap >> t.mg2l_greens_direct >> ms &&
+              t.overlap >> t.mg2l_greens_direct >> t.near_chunks_per_warp >> ms &&
           k == key &&
           ct2g_set_tuning(ctx, &t) == CT2G_OK) {
         if (out) *out = t;
@@ -411,7 +414,7 @@ int ct2g_autotune(ct2g_ctx *ctx, const ct2g_kick_params *p, float dt, float scal
     return CT2G_OK;
   };
   if (rc == CT2G_OK) rc = time_one(best, best_ms);
-  // coordinate descent over the six shapes
+  // coordinate descent over the seven shapes
   const int W = ctx->M >= 256 ? 16 : 4096 / ctx->M;
   std::vector<std::vector<int>> cand = {
       {8, 12, 16, 24, 32, 48},  // dense_cell
@@ -419,10 +422,12 @@ int ct2g_autotune(ct2g_ctx *ctx, const ct2g_kick_params *p, float dt, float scal
       ctx->M >= 64 ? std::vector<int>{0, W / 2, 2 * W} : std::vector<int>{0},
       {0, 1},                   // sparse_path
       {0, 1},                   // overlap
-      {0, 1}};                  // mg2l_greens_direct
-  // the overlap first: it changes which near-field footprint is best
-  const int dims[6] = {4, 1, 0, 2, 3, 5};
-  for (int di = 0; di < 6 && rc == CT2G_OK; di++) {
+      {0, 1},                   // mg2l_greens_direct
+      {0, 4, 16, 64}};          // near_chunks_per_warp (with overlap)
+  // the overlap first, then how the near field shares the SMs with the mesh
+  // solve: they change which near-field footprint is best
+  const int dims[7] = {4, 6, 1, 0, 2, 3, 5};
+  for (int di = 0; di < 7 && rc == CT2G_OK; di++) {
     const int dim = dims[di];
     for (int v : cand[dim]) {
       ct2g_tuning t = best;
@@ -431,7 +436,8 @@ int ct2g_autotune(ct2g_ctx *ctx, const ct2g_kick_params *p, float dt, float scal
                    : dim == 2 ? &t.fft_tile
                    : dim == 3 ? &t.sparse_path
                    : dim == 4 ? &t.overlap
-                              : &t.mg2l_greens_direct;
+                   : dim == 5 ? &t.mg2l_greens_direct
+                              : &t.near_chunks_per_warp;
       if (*field == v) continue;
       *field = v;
       float ms = 0.f;
@@ -456,7 +462,7 @@ int ct2g_autotune(ct2g_ctx *ctx, const ct2g_kick_params *p, float dt, float scal
     if (f)
       f << key << ' ' << best.dense_cell << ' ' << best.near_blocks_per_sm << ' ' << best.fft_tile
         << ' ' << best.sparse_path << ' ' << best.overlap << ' ' << best.mg2l_greens_direct << ' '
-        << best_ms << '\n';
+        << best.near_chunks_per_warp << ' ' << best_ms << '\n';
   }
   if (out) *out = best;
   return CT2G_OK;

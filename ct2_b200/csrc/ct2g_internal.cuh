@@ -261,6 +261,7 @@ struct ct2g_ctx {
   int sparse_path = 1;         // sparse sinks: 0 one per lane, 1 per-block warp chunks
   int overlap = 0;             // 1: near field on stream2, concurrent with the mesh solve
   int mg2l_greens_direct = 0;  // 1: the fused x pass reads the Green's values from HBM
+  int near_chunks_per_warp = 0;  // overlap: chunks a near-field warp takes before its block exits
   struct ct2g_batch *self_batch = nullptr;  // graph of ct2g_kick_drift
   struct ct2g_learn *learn = nullptr;       // learned near-field correction
   bool fft_tc = false;                      // y/x FFT passes on the tensor cores

@@ -366,13 +366,15 @@ __global__ void __launch_bounds__(256, 4) near_kernel(
     Walk walk, const uint32_t *__restrict__ skeys, uint32_t rbegin,
     const float4 *__restrict__ src, int mbits, float soft, float lo2, float bw2,
     const float *__restrict__ box_gm, float *__restrict__ ofx, float *__restrict__ ofy,
-    float *__restrict__ ofz, float *__restrict__ opot, bool store,
+    float *__restrict__ ofz, float *__restrict__ opot, bool store, uint32_t maxch,
     unsigned long long *__restrict__ inter) {
   __shared__ float4 sbuf[8][32];  // one batch of 32 sources per warp
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const uint32_t nch = *nch_ptr;
   const uint2 *list = off_ptr ? chunks + *off_ptr : chunks;
-  for (;;) {
+  // maxch > 0: a warp takes at most maxch chunks and the block then exits,
+  // so that blocks of kernels on other streams get the SM in between
+  for (uint32_t taken = 0; maxch == 0 || taken < maxch; taken++) {
     uint32_t ch = 0;
     if (lane == 0) ch = atomicAdd(work, 1u);
     ch = __shfl_sync(0xffffffffu, ch, 0);
@@ -542,7 +544,7 @@ int launch_near1(ct2g_ctx *ctx, const Walk &walk, const uint2 *chunks, const uin
                  const uint32_t *off, uint32_t *work, const uint32_t *slist,
                  const unsigned long long *stm, float lo2, float bw2, float *fx, float *fy,
                  float *fz, float *pot, unsigned long long *inter, cudaStream_t st = nullptr,
-                 bool store = false) {
+                 bool store = false, uint32_t maxch = 0) {
   auto k = near_kernel<K, POT, SPARSE>;
   if (!st) st = ctx->stream;
   int per_sm = 0;
@@ -551,10 +553,13 @@ int launch_near1(ct2g_ctx *ctx, const Walk &walk, const uint2 *chunks, const uin
   if (ctx->near_blocks_per_sm > 0) per_sm = std::min(per_sm, ctx->near_blocks_per_sm);
   size_t blocks = (size_t)std::max(1, per_sm) * ctx->num_sms;
   blocks = std::max<size_t>(1, std::min(blocks, (nr + 255) / 256));
+  // capped warps: enough blocks for every chunk the range can have (one per
+  // sink at most); blocks past the device-held chunk count exit at once
+  if (maxch) blocks = std::max<size_t>(1, (nr + 8 * (size_t)maxch - 1) / (8 * (size_t)maxch));
   k<<<(unsigned)blocks, 256, 0, st>>>(
       chunks, nch, off, work, slist, ctx->cell_start, ctx->occ, stm, walk, ctx->keys,
       (uint32_t)ctx->rung_begin, ctx->src, ctx->mbits, ctx->opt.hsoft, lo2, bw2, ctx->box_gm, fx,
-      fy, fz, pot, store, inter);
+      fy, fz, pot, store, maxch, inter);
   CT2G_LAUNCHED(ctx);
   return CT2G_OK;
 }
@@ -568,13 +573,16 @@ int launch_near(ct2g_ctx *ctx, cudaStream_t st, float *fx, float *fy, float *fz,
   const Walk walk = make_walk(ctx->mbits);
   const float bw2 = ctx->opt.bwidth * ctx->opt.bwidth;
   uint32_t *c = ctx->d_counts;
+  // capped warps only beside the mesh solve (overlap), where they let the
+  // mesh kernels' blocks in
+  const uint32_t maxch = store ? (uint32_t)ctx->near_chunks_per_warp : 0u;
   CT2G_TRY((launch_near1<K, POT, false>(ctx, walk, ctx->chunks, c + 0, nullptr, c + 3,
                                         ctx->sparse_list, ctx->stmask, -1.f, bw2, fx, fy, fz, pot,
-                                        ctx->d_inter, st, store)));
+                                        ctx->d_inter, st, store, maxch)));
   if (ctx->sparse_path == 0) return launch_near_lanes<K, POT>(ctx, walk, st, fx, fy, fz, pot, store);
   return launch_near1<K, POT, true>(ctx, walk, ctx->chunks, c + 2, c + 0, c + 4,
                                     ctx->sparse_list, ctx->stmask, -1.f, bw2, fx, fy, fz, pot,
-                                    ctx->d_inter, st, store);
+                                    ctx->d_inter, st, store, maxch);
 }
 
 int near_all(ct2g_ctx *ctx, bool pot, cudaStream_t st, float *fx, float *fy, float *fz,

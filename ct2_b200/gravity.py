@@ -73,6 +73,7 @@ class Gravity:
             raise CT2GError(rc, "ct2g_create_boxes(mesh=%d, order=%d, bwidth=%g, nbox=%d)"
                             % (mesh, order, bwidth, nbox))
         self._h = h
+        self.device = int(device)
         self.mesh, self.order, self.bwidth, self.kernel = mesh, order, bwidth, kernel
         self.nbox = int(nbox)
         self.nc = ncomp(order)
@@ -302,12 +303,13 @@ class Gravity:
         self._chk(self._l.ct2g_get_tuning(self._h, ctypes.byref(t)))
         return dict(dense_cell=t.dense_cell, near_blocks_per_sm=t.near_blocks_per_sm,
                     fft_tile=t.fft_tile, split_mg2l=t.split_mg2l, sparse_path=t.sparse_path,
-                    overlap=t.overlap, mg2l_greens_direct=t.mg2l_greens_direct)
+                    overlap=t.overlap, mg2l_greens_direct=t.mg2l_greens_direct,
+                    near_chunks_per_warp=t.near_chunks_per_warp)
 
     def set_tuning(self, dense_cell=16, near_blocks_per_sm=0, fft_tile=0, split_mg2l=0,
-                   sparse_path=1, overlap=0, mg2l_greens_direct=0):
+                   sparse_path=1, overlap=0, mg2l_greens_direct=0, near_chunks_per_warp=0):
         t = Tuning(dense_cell, near_blocks_per_sm, fft_tile, split_mg2l, sparse_path, overlap,
-                   mg2l_greens_direct)
+                   mg2l_greens_direct, near_chunks_per_warp)
         self._chk(self._l.ct2g_set_tuning(self._h, ctypes.byref(t)))
 
     def autotune(self, params: kick_params, dt: float, scale: float = 1.0, cache_path=None):
@@ -317,7 +319,8 @@ class Gravity:
                                         ctypes.byref(t)))
         return dict(dense_cell=t.dense_cell, near_blocks_per_sm=t.near_blocks_per_sm,
                     fft_tile=t.fft_tile, split_mg2l=t.split_mg2l, sparse_path=t.sparse_path,
-                    overlap=t.overlap, mg2l_greens_direct=t.mg2l_greens_direct)
+                    overlap=t.overlap, mg2l_greens_direct=t.mg2l_greens_direct,
+                    near_chunks_per_warp=t.near_chunks_per_warp)
 
     def kick_step(self, minrung, max_rung, scale, adot, tau, t0, minrung0, nocrop=False):
         """Returns (value, minrung): the reference's return value, which is its
@@ -355,21 +358,44 @@ class Gravity:
         return c[:nr.value].astype(np.int64)
 
     # -- FFT ----------------------------------------------------------------
+    def _on_torch_order(self, call):
+        """Run `call` (work on device buffers that torch owns) on the context's
+        stream, ordered after the work already queued on torch's current
+        stream, and make torch's current stream wait for it: the buffers are
+        written by torch and read back by torch, and the context's stream is
+        a non-blocking stream of its own, so without the two waits the
+        kernels could read a buffer before torch's copy into it has finished
+        (the context's stream also runs at a higher priority)."""
+        import sys
+        torch = sys.modules.get("torch")
+        if torch is None or not torch.cuda.is_initialized():
+            return call()
+        ext = torch.cuda.ExternalStream(self.stream(), device=self.device)
+        cur = torch.cuda.current_stream(self.device)
+        ext.wait_stream(cur)
+        r = call()
+        cur.wait_stream(ext)
+        return r
+
     def fft3d_c2c_dev(self, ptr, N, batch, dir=1):
         """In-place complex 3D FFT of `batch` device grids (a device pointer,
-        e.g. a torch tensor's data_ptr()) on the context's stream."""
-        self._chk(self._l.ct2g_fft3d_c2c_f32_dev(self._h, dir, ctypes.c_void_p(ptr), N, batch))
+        e.g. a torch tensor's data_ptr()) on the context's stream, ordered
+        with torch's current stream both ways."""
+        self._on_torch_order(lambda: self._chk(self._l.ct2g_fft3d_c2c_f32_dev(
+            self._h, dir, ctypes.c_void_p(ptr), N, batch)))
 
     def fft3d_r2c_dev(self, real_ptr, cplx_ptr, N, batch, dir=1):
         """The real <-> half-spectrum 3D FFT on device pointers (dir +1 r2c,
-        -1 c2r), FP32."""
-        self._chk(self._l.ct2g_fft3d_f32_dev(self._h, dir, ctypes.c_void_p(real_ptr),
-                                             ctypes.c_void_p(cplx_ptr), N, batch))
+        -1 c2r), FP32, ordered with torch's current stream both ways."""
+        self._on_torch_order(lambda: self._chk(self._l.ct2g_fft3d_f32_dev(
+            self._h, dir, ctypes.c_void_p(real_ptr), ctypes.c_void_p(cplx_ptr), N, batch)))
 
     def cic_deposit(self, N, ptr):
         """CIC mass and first moments of the particles onto four complex
-        device grids float2[4][N][N][N] at `ptr`."""
-        self._chk(self._l.ct2g_cic_deposit(self._h, N, ctypes.c_void_p(ptr)))
+        device grids float2[4][N][N][N] at `ptr`, ordered with torch's current
+        stream both ways."""
+        self._on_torch_order(lambda: self._chk(self._l.ct2g_cic_deposit(
+            self._h, N, ctypes.c_void_p(ptr))))
 
     def fft1d_real(self, X, N, lanes=1, dir=1):
         """fft_real (fft.hpp:25-26) in place on a float64 array: input in

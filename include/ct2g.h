@@ -230,7 +230,10 @@ int ct2g_batch_destroy(ct2g_batch *b);
  * hide; mg2l_greens_direct -- 1: the fused x pass + Green's multiply reads
  * the Green's values straight from HBM inside the contraction instead of
  * staging each column in shared memory first (one more block per SM; the
- * same results). */
+ * same results); near_chunks_per_warp -- with overlap, > 0: a near-field warp
+ * takes at most this many sink chunks before its block exits, so that the
+ * mesh solve's blocks (on the context stream, which has the higher priority)
+ * get SMs in between; 0: the near-field grid is persistent. */
 typedef struct {
   int dense_cell;
   int near_blocks_per_sm;
@@ -239,7 +242,7 @@ typedef struct {
   int sparse_path;
   int overlap;
   int mg2l_greens_direct;
-  int reserved[1];
+  int near_chunks_per_warp;
 } ct2g_tuning;
 int ct2g_get_tuning(const ct2g_ctx *ctx, ct2g_tuning *t);
 int ct2g_set_tuning(ct2g_ctx *ctx, const ct2g_tuning *t);
@@ -365,6 +368,12 @@ int ct2g_transpose_c2r(ct2g_ctx *ctx, const double *xin, double *xout, int N);
  * src/fft/twiddles.cpp): out[n] = cos(-2 pi n/N) (which 0), sin(-2 pi n/N)
  * (which 1), sin(2 pi n/N) (which 2), n < N. */
 int ct2g_twiddles(ct2g_ctx *ctx, int which, int N, double *out);
+/* The device-pointer entry points below queue their kernels on the context's
+ * stream (ct2g_stream), a non-blocking stream created at the highest stream
+ * priority: it is not ordered with the legacy default stream nor with the
+ * caller's streams.  A caller that fills or reads the buffers on a stream of
+ * its own makes the context's stream wait for that stream first (an event)
+ * and its own stream wait for the context's afterwards. */
 /* FP32 device-pointer variant on the context stream, interleaved complex
  * output (float2[batch][N][N][N/2+1]); dir = +1 forward r2c, -1 inverse c2r */
 int ct2g_fft3d_f32_dev(ct2g_ctx *ctx, int dir, void *d_real, void *d_complex, int N,
