@@ -247,6 +247,7 @@ int ct2g_alloc_mesh(ct2g_ctx *ctx) {
   CT2G_CUDA(ctx, cudaMalloc(&ctx->spec, sizeof(float2) * ctx->nc * nb * ctx->CK));
   CT2G_CUDA(ctx, cudaMalloc(&ctx->d_counts, sizeof(uint32_t) * 8));
   CT2G_CUDA(ctx, cudaMemset(ctx->d_counts, 0, sizeof(uint32_t) * 8));
+  CT2G_CUDA(ctx, cudaMalloc(&ctx->pipe_sync, sizeof(uint32_t) * 2 * (2 + nb * ctx->M)));
   CT2G_CUDA(ctx, cudaMalloc(&ctx->box_off, sizeof(uint32_t) * (nb + 1)));
   CT2G_CUDA(ctx, cudaMalloc(&ctx->box_gm, sizeof(float) * nb));
   CT2G_CUDA(ctx, cudaMalloc(&ctx->greens, sizeof(float) * ctx->nc * ctx->CK));
@@ -409,7 +410,7 @@ int ct2g_destroy(ct2g_ctx *ctx) {
   ct2g_learned_free(ctx);
   void *ptrs[] = {ctx->cell_start, ctx->occ, ctx->stmask, ctx->grid, ctx->spec, ctx->greens,
                   ctx->greens_x,                  ctx->tw32, ctx->tw64, ctx->d_counts, ctx->box_off, ctx->box_gm, ctx->tc_tables,
-                  ctx->d_maxrung, ctx->d_inter, ctx->scan_tmp};
+                  ctx->d_maxrung, ctx->d_inter, ctx->scan_tmp, ctx->pipe_sync};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);

@@ -729,6 +729,81 @@ __device__ __forceinline__ void p2m_half(const uint32_t *__restrict__ px,
   }
 }
 
+// The moments of the N cells of line `line` (x * N + y) of box `box`, from
+// the particles, into the packed smem lines sr (line l = components 2l, 2l+1
+// as .x, .y).  big / nbig: smem list of the cells summed by a warp.  Ends
+// with the block synchronised.
+template <int P, int N>
+__device__ __forceinline__ void p2m_line(const uint32_t *__restrict__ px,
+                                         const uint32_t *__restrict__ py,
+                                         const uint32_t *__restrict__ pz,
+                                         const uint32_t *__restrict__ cs, int mbits, uint32_t box,
+                                         size_t line, float *sr, uint32_t *big, uint32_t &nbig) {
+  using LL = LineLayout<N, true>;
+  constexpr int NC = ct2g_ncomp(P), NL = (NC + 1) / 2;
+  const uint32_t cx = (uint32_t)(line / N), cy = (uint32_t)(line % N);
+  const int sh = 32 - mbits;
+  const uint32_t halfc = 1u << (sh - 1);
+  const uint32_t ux = (cx << sh) + halfc, uy = (cy << sh) + halfc;
+  for (int zc = threadIdx.x; zc < N; zc += 256) {
+    const uint32_t key = (box << (3 * mbits)) | ct2g_morton(cx, cy, (uint32_t)zc);
+    const uint32_t b = cs[key], e = cs[key + 1];
+    if (e - b > kWarpCell) {
+      big[atomicAdd(&nbig, 1u)] = (uint32_t)zc;
+      continue;
+    }
+    const uint32_t uz = ((uint32_t)zc << sh) + halfc;
+    p2m_half<P, N, 0, NC / 3>(px, py, pz, b, e, 1, false, ux, uy, uz, zc, sr, true);
+    p2m_half<P, N, NC / 3, 2 * NC / 3>(px, py, pz, b, e, 1, false, ux, uy, uz, zc, sr, true);
+    p2m_half<P, N, 2 * NC / 3, NC>(px, py, pz, b, e, 1, false, ux, uy, uz, zc, sr, true);
+    if (NC & 1) sr[2 * LL::at(NL - 1, zc, 0) + 1] = 0.f;
+  }
+  __syncthreads();
+  {  // the big cells, a warp each
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (uint32_t q = warp; q < nbig; q += 8) {
+      const uint32_t zc = big[q];
+      const uint32_t key = (box << (3 * mbits)) | ct2g_morton(cx, cy, zc);
+      const uint32_t b = cs[key], e = cs[key + 1];
+      const uint32_t uz = (zc << sh) + halfc;
+      p2m_half<P, N, 0, NC / 3>(px, py, pz, b + lane, e, 32, true, ux, uy, uz, (int)zc, sr,
+                                lane == 0);
+      p2m_half<P, N, NC / 3, 2 * NC / 3>(px, py, pz, b + lane, e, 32, true, ux, uy, uz,
+                                         (int)zc, sr, lane == 0);
+      p2m_half<P, N, 2 * NC / 3, NC>(px, py, pz, b + lane, e, 32, true, ux, uy, uz, (int)zc,
+                                     sr, lane == 0);
+      if ((NC & 1) && lane == 0) sr[2 * LL::at(NL - 1, (int)zc, 0) + 1] = 0.f;
+    }
+  }
+  __syncthreads();
+}
+
+// The transformed packed lines of LB mesh lines, split into the half spectra
+// of their two components, written as LB spectrum rows from `rows` on (row
+// lb at rows + lb * ldk * NC; k-point k's components at k * NC; the slots
+// k > N/2 get zeros).
+template <int P, int N, int LB>
+__device__ __forceinline__ void store_half_spectra(const float2 *s, float2 *rows, int ldk) {
+  using LL = LineLayout<N, true>;
+  constexpr int NC = ct2g_ncomp(P), NL = (NC + 1) / 2, NH = N / 2 + 1;
+  const int64_t RS = (int64_t)ldk * NC;
+  for (int e = threadIdx.x; e < LB * ldk * NL; e += 256) {
+    const int lb = LB == 1 ? 0 : e / (ldk * NL), r = e - lb * ldk * NL;
+    const int k = r / NL, l = r - k * NL;
+    float2 *row = rows + lb * RS;
+    float2 a = make_float2(0.f, 0.f), bb = make_float2(0.f, 0.f);
+    if (k < NH) {
+      const float2 zk = s[LL::at(lb * NL + l, k & (N - 1), 0)];
+      const float2 zn = s[LL::at(lb * NL + l, (N - k) & (N - 1), 0)];
+      // A_k = (Z_k + conj Z_{N-k})/2, B_k = (Z_k - conj Z_{N-k})/(2i)
+      a = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
+      bb = make_float2(0.5f * (zk.y + zn.y), 0.5f * (zn.x - zk.x));
+    }
+    row[k * NC + 2 * l] = a;
+    if (2 * l + 1 < NC) row[k * NC + 2 * l + 1] = bb;
+  }
+}
+
 // occupancy: 4 blocks per SM up to order 4 (64 registers); at N = 512 the
 // 32-point in-register DFTs need more registers than that, so 2
 template <int P, int N, int SRC>
@@ -764,40 +839,7 @@ __global__ void __launch_bounds__(256, N >= 512 ? 2 : P <= 4 ? 4 : 2) fftz_p2m_r
       for (int e = threadIdx.x; e < LB * N; e += 256)
         sr[2 * LL::at((e / N) * NL + NL - 1, e % N, 0) + 1] = 0.f;
   } else {
-    const uint32_t cx = (uint32_t)(line / N), cy = (uint32_t)(line % N);
-    const int sh = 32 - mbits;
-    const uint32_t halfc = 1u << (sh - 1);
-    const uint32_t ux = (cx << sh) + halfc, uy = (cy << sh) + halfc;
-    for (int zc = threadIdx.x; zc < N; zc += 256) {
-      const uint32_t key = (box << (3 * mbits)) | ct2g_morton(cx, cy, (uint32_t)zc);
-      const uint32_t b = cs[key], e = cs[key + 1];
-      if (e - b > kWarpCell) {
-        big[atomicAdd(&nbig, 1u)] = (uint32_t)zc;
-        continue;
-      }
-      const uint32_t uz = ((uint32_t)zc << sh) + halfc;
-      p2m_half<P, N, 0, NC / 3>(px, py, pz, b, e, 1, false, ux, uy, uz, zc, sr, true);
-      p2m_half<P, N, NC / 3, 2 * NC / 3>(px, py, pz, b, e, 1, false, ux, uy, uz, zc, sr, true);
-      p2m_half<P, N, 2 * NC / 3, NC>(px, py, pz, b, e, 1, false, ux, uy, uz, zc, sr, true);
-      if (NC & 1) sr[2 * LL::at(NL - 1, zc, 0) + 1] = 0.f;
-    }
-    __syncthreads();
-    {  // the big cells, a warp each
-      const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-      for (uint32_t q = warp; q < nbig; q += 8) {
-        const uint32_t zc = big[q];
-        const uint32_t key = (box << (3 * mbits)) | ct2g_morton(cx, cy, zc);
-        const uint32_t b = cs[key], e = cs[key + 1];
-        const uint32_t uz = (zc << sh) + halfc;
-        p2m_half<P, N, 0, NC / 3>(px, py, pz, b + lane, e, 32, true, ux, uy, uz, (int)zc, sr,
-                                  lane == 0);
-        p2m_half<P, N, NC / 3, 2 * NC / 3>(px, py, pz, b + lane, e, 32, true, ux, uy, uz,
-                                           (int)zc, sr, lane == 0);
-        p2m_half<P, N, 2 * NC / 3, NC>(px, py, pz, b + lane, e, 32, true, ux, uy, uz, (int)zc,
-                                       sr, lane == 0);
-        if ((NC & 1) && lane == 0) sr[2 * LL::at(NL - 1, (int)zc, 0) + 1] = 0.f;
-      }
-    }
+    p2m_line<P, N>(px, py, pz, cs, mbits, box, line, sr, big, nbig);
   }
   __syncthreads();
   if constexpr (SRC == CT2G_P2M_FUSED_STORE) {
@@ -810,24 +852,7 @@ __global__ void __launch_bounds__(256, N >= 512 ? 2 : P <= 4 ? 4 : 2) fftz_p2m_r
     __syncthreads();
   }
   tile_fft<N, true, float2, false>(s, LB * NL, 0, stw);
-  // row L0 + lb = box * N^2 + line + lb; k-point k's components at k * NC
-  const int64_t RS = (int64_t)ldk * NC;
-  float2 *rows = spec + (int64_t)L0 * RS;
-  for (int e = threadIdx.x; e < LB * ldk * NL; e += 256) {
-    const int lb = LB == 1 ? 0 : e / (ldk * NL), r = e - lb * ldk * NL;
-    const int k = r / NL, l = r - k * NL;
-    float2 *row = rows + lb * RS;
-    float2 a = make_float2(0.f, 0.f), bb = make_float2(0.f, 0.f);
-    if (k < NH) {
-      const float2 zk = s[LL::at(lb * NL + l, k & (N - 1), 0)];
-      const float2 zn = s[LL::at(lb * NL + l, (N - k) & (N - 1), 0)];
-      // A_k = (Z_k + conj Z_{N-k})/2, B_k = (Z_k - conj Z_{N-k})/(2i)
-      a = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
-      bb = make_float2(0.5f * (zk.y + zn.y), 0.5f * (zn.x - zk.x));
-    }
-    row[k * NC + 2 * l] = a;
-    if (2 * l + 1 < NC) row[k * NC + 2 * l + 1] = bb;
-  }
+  store_half_spectra<P, N, LB>(s, spec + (int64_t)L0 * ldk * NC, ldk);
 }
 
 template <int P, int N>
@@ -847,6 +872,106 @@ int launch_p2m_r2c(ct2g_ctx *ctx, int src) {
 }
 
 // ---- inverse z pass fused with L2P ------------------------------------------
+// LB spectrum rows from `rows` on (layout as store_half_spectra) unpacked
+// into packed complex lines in smem: Z = A + iB for the components 2l, 2l+1,
+// both halves of the line from the k <= N/2 slots.  ld(q) loads one value
+// (a plain load, or one that bypasses L1).  The row's loads go out in batches
+// of RB per thread before any of them is used, so that their latencies
+// overlap.
+template <int P, int N, int LB, typename LD>
+__device__ __forceinline__ void load_half_spectra(const float2 *rows, int ldk, float2 *s, LD ld) {
+  using LL = LineLayout<N, true>;
+  constexpr int NC = ct2g_ncomp(P), NL = (NC + 1) / 2, NH = N / 2 + 1;
+  const int64_t RS = (int64_t)ldk * NC;
+  constexpr int RB = 5;
+  for (int e0 = threadIdx.x; e0 < LB * NH * NL; e0 += RB * 256) {
+    float2 a[RB], b[RB];
+#pragma unroll
+    for (int u = 0; u < RB; u++) {
+      const int e = e0 + 256 * u;
+      const int lb = LB == 1 ? 0 : e / (NH * NL), r = e - lb * NH * NL;
+      const int k = r / NL, l = r - k * NL;
+      a[u] = b[u] = make_float2(0.f, 0.f);
+      if (e < LB * NH * NL) {
+        a[u] = ld(rows + lb * RS + k * NC + 2 * l);
+        if (2 * l + 1 < NC) b[u] = ld(rows + lb * RS + k * NC + 2 * l + 1);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < RB; u++) {
+      const int e = e0 + 256 * u;
+      const int lb = LB == 1 ? 0 : e / (NH * NL), r = e - lb * NH * NL;
+      const int k = r / NL, l = r - k * NL;
+      if (e < LB * NH * NL) {
+        // Z_k = A_k + i B_k; Z_{N-k} = conj(A_k) + i conj(B_k)
+        s[LL::at(lb * NL + l, k, 0)] = make_float2(a[u].x - b[u].y, a[u].y + b[u].x);
+        if (k > 0 && k < N / 2)
+          s[LL::at(lb * NL + l, N - k, 0)] = make_float2(a[u].x + b[u].y, b[u].x - a[u].y);
+      }
+    }
+  }
+}
+
+// Inverse transform of one line's packed expansion lines in smem (s, loaded
+// and synchronised), then the far field of every particle of the line's
+// cells: cb / ce hold the cells' particle ranges (smem, written before the
+// caller's last barrier), off is smem scratch of N + 1 words.
+template <int P, int N, bool POT>
+__device__ __forceinline__ void l2p_line(float2 *s, const float2 *stw, const uint32_t *cb,
+                                         const uint32_t *ce, uint32_t *off,
+                                         const float4 *__restrict__ src, float GM,
+                                         float *__restrict__ ofx, float *__restrict__ ofy,
+                                         float *__restrict__ ofz, float *__restrict__ opot) {
+  using LL = LineLayout<N, true>;
+  constexpr int NL = (ct2g_ncomp(P) + 1) / 2;
+  // offsets of the cells' particles in the line's particle list (inclusive
+  // scan of the counts, off[0] = 0), built while nothing else needs the SM
+  constexpr int ZT = (N + 255) / 256;  // cells per thread
+  for (int z = threadIdx.x; z < N; z += 256) off[z + 1] = ce[z] - cb[z];
+  if (threadIdx.x == 0) off[0] = 0;
+  tile_fft<N, true, float2, true>(s, NL, 0, stw);
+  __syncthreads();
+  for (int d = 1; d < N; d <<= 1) {
+    uint32_t add[ZT];
+#pragma unroll
+    for (int q = 0; q < ZT; q++) {
+      const int z = threadIdx.x + 256 * q;
+      add[q] = (z < N && z >= d) ? off[z + 1 - d] : 0u;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < ZT; q++) {
+      const int z = threadIdx.x + 256 * q;
+      if (z < N) off[z + 1] += add[q];
+    }
+    __syncthreads();
+  }
+  // every particle of the line, one per thread: its cell is the last z with
+  // off[z] <= q (that cell holds it: off[z] <= q < off[z + 1])
+  const uint32_t total = off[N];
+  for (uint32_t q = threadIdx.x; q < total; q += 256) {
+    int lo = 0, hi = N;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (off[mid] <= q) lo = mid; else hi = mid;
+    }
+    const int z = lo;
+    const uint32_t i = cb[z] + (q - off[z]);
+    const auto acc = [&](int k) {
+      const float2 v = s[LL::at(k >> 1, z, 0)];
+      return (k & 1) ? v.y : v.x;
+    };
+    const float4 t = src[i];
+    float fx, fy, fz, ph;
+    ct2g_l2p<P>(acc, t.x, t.y, t.z, fx, fy, fz, ph);
+    ofx[i] = GM * fx;
+    ofy[i] = GM * fy;
+    ofz[i] = GM * fz;
+    if (POT) opot[i] = GM * ph;
+  }
+}
+
+
 // One block per (x, y) line of the mesh, all NC expansion components: pairs of
 // components are packed into complex lines (A + iB), transformed back along z
 // in shared memory, and the block then evaluates the far field of every
@@ -884,37 +1009,8 @@ __global__ void __launch_bounds__(256, N >= 512 ? 1 : 5) fftz_c2r_l2p_kernel(
       ce[z] = cs[key + 1];
     }
   }
-  const int64_t RS = (int64_t)ldk * NC;
-  const float2 *rows = spec + (int64_t)L0 * RS;
-  // the row's loads go out in batches of RB per thread before any of them is
-  // used, so that their latencies overlap
-  constexpr int RB = 5;
-  for (int e0 = threadIdx.x; e0 < LB * NH * NL; e0 += RB * 256) {
-    float2 a[RB], b[RB];
-#pragma unroll
-    for (int u = 0; u < RB; u++) {
-      const int e = e0 + 256 * u;
-      const int lb = LB == 1 ? 0 : e / (NH * NL), r = e - lb * NH * NL;
-      const int k = r / NL, l = r - k * NL;
-      a[u] = b[u] = make_float2(0.f, 0.f);
-      if (e < LB * NH * NL) {
-        a[u] = rows[lb * RS + k * NC + 2 * l];
-        if (2 * l + 1 < NC) b[u] = rows[lb * RS + k * NC + 2 * l + 1];
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < RB; u++) {
-      const int e = e0 + 256 * u;
-      const int lb = LB == 1 ? 0 : e / (NH * NL), r = e - lb * NH * NL;
-      const int k = r / NL, l = r - k * NL;
-      if (e < LB * NH * NL) {
-        // Z_k = A_k + i B_k; Z_{N-k} = conj(A_k) + i conj(B_k)
-        s[LL::at(lb * NL + l, k, 0)] = make_float2(a[u].x - b[u].y, a[u].y + b[u].x);
-        if (k > 0 && k < N / 2)
-          s[LL::at(lb * NL + l, N - k, 0)] = make_float2(a[u].x + b[u].y, b[u].x - a[u].y);
-      }
-    }
-  }
+  load_half_spectra<P, N, LB>(spec + (int64_t)L0 * ldk * NC, ldk, s,
+                              [](const float2 *q) { return *q; });
   __syncthreads();
   if constexpr (!L2P) {
     tile_fft<N, true, float2, true>(s, LB * NL, 0, stw);
@@ -927,53 +1023,9 @@ __global__ void __launch_bounds__(256, N >= 512 ? 1 : 5) fftz_c2r_l2p_kernel(
     }
     return;
   } else {
-    // offsets of the cells' particles in the line's particle list (inclusive
-    // scan of the counts, off[0] = 0), built while nothing else needs the SM
-    constexpr int ZT = (N + 255) / 256;  // cells per thread
     __shared__ uint32_t off[N + 1];
-    for (int z = threadIdx.x; z < N; z += 256) off[z + 1] = ce[z] - cb[z];
-    if (threadIdx.x == 0) off[0] = 0;
-    tile_fft<N, true, float2, true>(s, NL, 0, stw);
-    __syncthreads();
-    for (int d = 1; d < N; d <<= 1) {
-      uint32_t add[ZT];
-#pragma unroll
-      for (int q = 0; q < ZT; q++) {
-        const int z = threadIdx.x + 256 * q;
-        add[q] = (z < N && z >= d) ? off[z + 1 - d] : 0u;
-      }
-      __syncthreads();
-#pragma unroll
-      for (int q = 0; q < ZT; q++) {
-        const int z = threadIdx.x + 256 * q;
-        if (z < N) off[z + 1] += add[q];
-      }
-      __syncthreads();
-    }
-    // every particle of the line, one per thread: its cell is the last z with
-    // off[z] <= q (that cell holds it: off[z] <= q < off[z + 1])
-    const float GM = __ldg(box_gm + box);
-    const uint32_t total = off[N];
-    for (uint32_t q = threadIdx.x; q < total; q += 256) {
-      int lo = 0, hi = N;
-      while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (off[mid] <= q) lo = mid; else hi = mid;
-      }
-      const int z = lo;
-      const uint32_t i = cb[z] + (q - off[z]);
-      const auto acc = [&](int k) {
-        const float2 v = s[LL::at(k >> 1, z, 0)];
-        return (k & 1) ? v.y : v.x;
-      };
-      const float4 t = src[i];
-      float fx, fy, fz, ph;
-      ct2g_l2p<P>(acc, t.x, t.y, t.z, fx, fy, fz, ph);
-      ofx[i] = GM * fx;
-      ofy[i] = GM * fy;
-      ofz[i] = GM * fz;
-      if (MODE == 1) opot[i] = GM * ph;
-    }
+    l2p_line<P, N, MODE == 1>(s, stw, cb, ce, off, src, __ldg(box_gm + box), ofx, ofy, ofz,
+                              opot);
   }
 }
 
@@ -990,6 +1042,281 @@ int launch_c2r_l2p(ct2g_ctx *ctx, int mode) {
       ctx->fz, ctx->pot, ctx->grid, ctx->CB, twiddle_ptr<float2>(ctx));
   CT2G_LAUNCHED(ctx);
   return CT2G_OK;
+}
+
+// ---- z and y passes plane by plane: one persistent kernel per direction -----
+// The z pass and the y pass both work plane by plane (an x plane of a box is
+// N spectrum rows, N * ldk * NC complex values: 9.3 MB at N = 256, order 4),
+// so the y pass of a plane can start as soon as the z pass has written the
+// plane, while it is still in L2.  One persistent kernel hands out the items
+// of both passes in plane order from a device counter: the z lines of plane
+// t, then the y tiles of plane t - 1, then the z lines of plane t + 1, ...;
+// a y tile first waits (bounded) for the count of finished z lines of its
+// plane.  The spectrum then crosses HBM once per direction instead of three
+// times: forward, the y tiles read the rows from L2 and overwrite them in
+// place, so only the final values are written back; inverse, the z lines
+// read the y pass's output from L2 and (`discard`) drop the lines they have
+// read, which nothing reads again, without writing them back.
+//
+// Waiting is deadlock free whatever the number of resident blocks: a block
+// takes an item only while it runs, items are taken in order, and a waiting
+// item waits only for items of the other pass taken before it, which never
+// wait themselves.
+
+// Item order of a plane pipeline over T planes with a lag of D planes: A(t),
+// the first pass's NA items of plane t, and B(t), the second pass's NB items,
+// in the order A(0) ... A(D-1), then A(t) B(t-D) for t = D ... T-1, then
+// B(T-D) ... B(T-1).  The lag is how long a plane's first-pass items have
+// to finish before its second-pass items are handed out; D + 1 planes are in
+// flight at a time.
+struct PipeOrder {
+  uint32_t NA, NB, T, D;  // 1 <= D <= T
+  __device__ __forceinline__ uint32_t total() const { return T * (NA + NB); }
+  // true for an item of the first pass
+  __device__ __forceinline__ bool decode(uint32_t i, uint32_t &plane, uint32_t &sub) const {
+    if (i < D * NA) {
+      plane = i / NA;
+      sub = i - plane * NA;
+      return true;
+    }
+    i -= D * NA;
+    const uint32_t R = NA + NB;
+    if (i < (T - D) * R) {
+      const uint32_t t = i / R, o = i - t * R;
+      plane = o < NA ? t + D : t;
+      sub = o < NA ? o : o - NA;
+      return o < NA;
+    }
+    i -= (T - D) * R;
+    plane = T - D + i / NB;
+    sub = i - (plane - (T - D)) * NB;
+    return false;
+  }
+};
+
+constexpr uint32_t kPipeWaitLimit = 1u << 21;  // polls of a plane count (about a second)
+constexpr int kPipeW = 16;                     // y tile width (complex columns)
+
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t *p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Thread 0 waits until *count reaches target (the producers' row stores are
+// then visible to the block); false for every thread when the wait gave up,
+// after the status word was set to CT2G_ETIMEOUT.
+__device__ __forceinline__ bool pipe_wait(const uint32_t *count, uint32_t target,
+                                          uint32_t *status) {
+  int good = 1;
+  if (threadIdx.x == 0) {
+    uint32_t polls = 0;
+    while (ld_acquire(count) < target) {
+      if (++polls > kPipeWaitLimit) {
+        atomicExch(status, (uint32_t)CT2G_ETIMEOUT);
+        good = 0;
+        break;
+      }
+      __nanosleep(64);
+    }
+    __threadfence();
+  }
+  return __syncthreads_and(good) != 0;
+}
+
+// After the block's stores: the item is counted as finished in *count.
+__device__ __forceinline__ void pipe_done(uint32_t *count) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(count, 1u);
+  }
+}
+
+// One y tile: columns [c0, c0 + wv) of the N rows of a plane (row r at
+// plane + r * RS), copied into smem by cp.async past L1 (other blocks of the
+// kernel wrote them; the whole tile is in flight at once, without staging
+// registers), transformed along y in smem (column layout, W columns) and
+// written back.  Columns go in 16-byte pairs; a pair that starts below wv
+// moves whole (its second column, when past the last one, is a zero slot of
+// the row); the smem columns of pairs past wv are left as they are (columns
+// transform independently).
+template <int N, int W, bool INV>
+__device__ __forceinline__ void y_tile(float2 *plane, int64_t RS, int c0, int wv, float2 *s,
+                                       const float2 *stw) {
+  constexpr int CH = W / 2;  // 16-byte chunks per tile row
+  static_assert(N * CH % 256 == 0, "tile chunks per thread");
+#pragma unroll 4
+  for (int e = threadIdx.x; e < N * CH; e += 256) {
+    const int r = e / CH, c = (e % CH) * 2;
+    if (c < wv) cp_async16(s + r * W + c, plane + r * RS + c0 + c);
+  }
+  cp_async_commit();
+  cp_async_wait<0>();
+  __syncthreads();
+  tile_fft<N, false, float2, INV>(s, W, W, stw);
+#pragma unroll 4
+  for (int e = threadIdx.x; e < N * CH; e += 256) {
+    const int r = e / CH, c = (e % CH) * 2;
+    if (c < wv)
+      *reinterpret_cast<float4 *>(plane + r * RS + c0 + c) =
+          *reinterpret_cast<const float4 *>(s + r * W + c);
+  }
+}
+
+template <int P, int N>
+struct PipeShape {
+  static constexpr int NC = ct2g_ncomp(P), NL = (NC + 1) / 2, NH = N / 2 + 1;
+  static constexpr size_t ZS = (size_t)NL * LineLayout<N, true>::LS;  // a z line's packed lines
+  static constexpr size_t YS = (size_t)N * kPipeW;                    // a y tile
+  static constexpr size_t SMEM = sizeof(float2) * ((size_t)N + (ZS > YS ? ZS : YS));
+  // the z kernels' register budgets: 64 per thread up to order 4
+  static constexpr int MINB = P <= 4 ? 4 : 2;
+  static constexpr bool OK = N >= 64 && N <= 256;
+};
+
+// Forward: z lines (P2M from the particles + r2c along z, store_half_spectra)
+// and y tiles.  sync[0]: item counter; sync[2 + t]: finished z lines of plane t.
+template <int P, int N>
+__global__ void __launch_bounds__(256, PipeShape<P, N>::MINB) zy_forward_kernel(
+    const uint32_t *__restrict__ px, const uint32_t *__restrict__ py,
+    const uint32_t *__restrict__ pz, const uint32_t *__restrict__ cs, int mbits,
+    float2 *__restrict__ spec, int ldk, const float2 *__restrict__ tw, uint32_t nplanes,
+    uint32_t lag, uint32_t *__restrict__ sync, uint32_t *__restrict__ status) {
+  using S = PipeShape<P, N>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  float2 *stw = reinterpret_cast<float2 *>(smraw);
+  float2 *s = stw + N;
+  __shared__ uint32_t big[N], nbig, item_s;
+  load_twiddles(stw, tw, N);
+  const int64_t RS = (int64_t)ldk * S::NC;
+  const uint32_t ncols = (uint32_t)(S::NH * S::NC);
+  const PipeOrder ord{(uint32_t)N, (ncols + kPipeW - 1) / kPipeW, nplanes, min(lag, nplanes)};
+  if (threadIdx.x == 0) item_s = atomicAdd(sync, 1u);
+  __syncthreads();
+  for (;;) {
+    const uint32_t item = item_s;
+    if (item >= ord.total()) break;
+    uint32_t next = 0;
+    if (threadIdx.x == 0) {
+      next = atomicAdd(sync, 1u);  // the next item, asked for early
+      nbig = 0;
+    }
+    __syncthreads();
+    uint32_t plane, sub;
+    if (ord.decode(item, plane, sub)) {
+      const size_t L0 = (size_t)plane * N + sub;  // box * N^2 + x * N + y
+      p2m_line<P, N>(px, py, pz, cs, mbits, plane / N, L0 % ((size_t)N * N),
+                     reinterpret_cast<float *>(s), big, nbig);
+      tile_fft<N, true, float2, false>(s, S::NL, 0, stw);
+      store_half_spectra<P, N, 1>(s, spec + (int64_t)L0 * RS, ldk);
+      pipe_done(sync + 2 + plane);
+    } else {
+      if (!pipe_wait(sync + 2 + plane, (uint32_t)N, status)) break;
+      const int c0 = (int)sub * kPipeW;
+      y_tile<N, kPipeW, false>(spec + (int64_t)plane * N * RS, RS, c0,
+                               (int)min((uint32_t)kPipeW, ncols - (uint32_t)c0), s, stw);
+    }
+    if (threadIdx.x == 0) item_s = next;
+    __syncthreads();
+  }
+}
+
+// Inverse: y tiles and z lines (c2r along z + L2P); with `discard` a z line
+// drops the L2 lines that lie wholly inside the row it has read.  sync[0]:
+// item counter; sync[2 + t]: finished y tiles of plane t.
+template <int P, int N, bool POT>
+__global__ void __launch_bounds__(256, PipeShape<P, N>::MINB) yz_inverse_kernel(
+    float2 *__restrict__ spec, int ldk, const uint32_t *__restrict__ cs,
+    const float4 *__restrict__ src, int mbits, const float *__restrict__ box_gm,
+    float *__restrict__ ofx, float *__restrict__ ofy, float *__restrict__ ofz,
+    float *__restrict__ opot, const float2 *__restrict__ tw, uint32_t nplanes, uint32_t lag,
+    int discard, uint32_t *__restrict__ sync, uint32_t *__restrict__ status) {
+  using S = PipeShape<P, N>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  float2 *stw = reinterpret_cast<float2 *>(smraw);
+  float2 *s = stw + N;
+  __shared__ uint32_t cb[N + 1], ce[N], off[N + 1], item_s;
+  load_twiddles(stw, tw, N);
+  const int64_t RS = (int64_t)ldk * S::NC;
+  const uint32_t ncols = (uint32_t)(S::NH * S::NC), NT = (ncols + kPipeW - 1) / kPipeW;
+  const PipeOrder ord{NT, (uint32_t)N, nplanes, min(lag, nplanes)};
+  if (threadIdx.x == 0) item_s = atomicAdd(sync, 1u);
+  __syncthreads();
+  for (;;) {
+    const uint32_t item = item_s;
+    if (item >= ord.total()) break;
+    uint32_t next = 0;
+    if (threadIdx.x == 0) next = atomicAdd(sync, 1u);
+    uint32_t plane, sub;
+    if (ord.decode(item, plane, sub)) {
+      const int c0 = (int)sub * kPipeW;
+      y_tile<N, kPipeW, true>(spec + (int64_t)plane * N * RS, RS, c0,
+                              (int)min((uint32_t)kPipeW, ncols - (uint32_t)c0), s, stw);
+      pipe_done(sync + 2 + plane);
+    } else {
+      const size_t L0 = (size_t)plane * N + sub;
+      const uint32_t box = plane / N, x = plane % N, y = sub;
+      // the cells' particle ranges first: their latency hides behind the wait
+      for (int z = threadIdx.x; z < N; z += 256) {
+        const uint32_t key = (box << (3 * mbits)) | ct2g_morton(x, y, (uint32_t)z);
+        cb[z] = cs[key];
+        ce[z] = cs[key + 1];
+      }
+      if (!pipe_wait(sync + 2 + plane, NT, status)) break;
+      const float2 *row = spec + (int64_t)L0 * RS;
+      load_half_spectra<P, N, 1>(row, ldk, s, [](const float2 *q) { return __ldcg(q); });
+      __syncthreads();
+      if (discard) {
+        // the row's own 128-byte lines: every value of them is in smem now
+        const uintptr_t a = reinterpret_cast<uintptr_t>(row), e = a + (uintptr_t)RS * 8;
+        for (uintptr_t q = ((a + 127) & ~(uintptr_t)127) + 128 * threadIdx.x; q + 128 <= e;
+             q += 128 * 256)
+          asm volatile("discard.global.L2 [%0], 128;" ::"l"(q) : "memory");
+      }
+      l2p_line<P, N, POT>(s, stw, cb, ce, off, src, __ldg(box_gm + box), ofx, ofy, ofz, opot);
+    }
+    if (threadIdx.x == 0) item_s = next;
+    __syncthreads();
+  }
+}
+
+// the plane pipeline of one direction, when the configuration has one
+// (FP32 passes, the meshes it is built for, P2M from the particles or L2P
+// into the forces); *done = false otherwise, nothing launched
+template <int P, int N>
+int launch_plane_pipe(ct2g_ctx *ctx, bool inverse, int mode, bool *done) {
+  using S = PipeShape<P, N>;
+  *done = false;
+  if constexpr (!S::OK) {
+    return CT2G_OK;
+  } else {
+    if (!ctx->plane_pipe || ctx->fft_tc || !ctx->pipe_sync) return CT2G_OK;
+    if (inverse ? mode > 1 : mode != CT2G_P2M_FUSED) return CT2G_OK;
+    const uint32_t nplanes = (uint32_t)(ctx->nbox * N);
+    const void *kf = inverse ? (mode == 1 ? (const void *)yz_inverse_kernel<P, N, true>
+                                          : (const void *)yz_inverse_kernel<P, N, false>)
+                             : (const void *)zy_forward_kernel<P, N>;
+    CT2G_TRY(ct2g_smem_attrs(ctx, kf, S::SMEM));
+    const unsigned grid = (unsigned)(ct2g_blocks_per_sm(ctx, kf, 256, S::SMEM) * ctx->num_sms);
+    uint32_t *sync = ctx->pipe_sync + (inverse ? 2 + nplanes : 0);
+    CT2G_CUDA(ctx, cudaMemsetAsync(sync, 0, sizeof(uint32_t) * (2 + nplanes), ctx->stream));
+    if (inverse) {
+      auto k = mode == 1 ? yz_inverse_kernel<P, N, true> : yz_inverse_kernel<P, N, false>;
+      k<<<grid, 256, S::SMEM, ctx->stream>>>(ctx->spec, ctx->ldk, ctx->cell_start, ctx->src,
+                                             ctx->mbits, ctx->box_gm, ctx->fx, ctx->fy, ctx->fz,
+                                             ctx->pot, twiddle_ptr<float2>(ctx), nplanes,
+                                             (uint32_t)ctx->plane_pipe, ctx->pipe_discard, sync,
+                                             ctx->d_counts + 6);
+    } else {
+      zy_forward_kernel<P, N><<<grid, 256, S::SMEM, ctx->stream>>>(
+          ctx->x, ctx->y, ctx->z, ctx->cell_start, ctx->mbits, ctx->spec, ctx->ldk,
+          twiddle_ptr<float2>(ctx), nplanes, (uint32_t)ctx->plane_pipe, sync, ctx->d_counts + 6);
+    }
+    CT2G_LAUNCHED(ctx);
+    *done = true;
+    return CT2G_OK;
+  }
 }
 
 // ---- X pass + MG2L + inverse X pass ------------------------------------------
@@ -1229,6 +1556,32 @@ int spec_run(ct2g_ctx *ctx, int stage, bool flag, int mode) {
   return ct2g_fail(ctx, CT2G_EINVAL, "unsupported order");
 }
 
+template <int P>
+int spec_pipe_p(ct2g_ctx *ctx, bool inverse, int mode, bool *done) {
+  switch (ctx->M) {
+    case 64: return launch_plane_pipe<P, 64>(ctx, inverse, mode, done);
+    case 128: return launch_plane_pipe<P, 128>(ctx, inverse, mode, done);
+    case 256: return launch_plane_pipe<P, 256>(ctx, inverse, mode, done);
+  }
+  *done = false;
+  return CT2G_OK;
+}
+
+// the z and y passes of one direction as the plane pipeline, when the
+// context's configuration has one (*done tells)
+int spec_pipe(ct2g_ctx *ctx, bool inverse, int mode, bool *done) {
+  switch (ctx->p) {
+    case 1: return spec_pipe_p<1>(ctx, inverse, mode, done);
+    case 2: return spec_pipe_p<2>(ctx, inverse, mode, done);
+    case 3: return spec_pipe_p<3>(ctx, inverse, mode, done);
+    case 4: return spec_pipe_p<4>(ctx, inverse, mode, done);
+    case 5: return spec_pipe_p<5>(ctx, inverse, mode, done);
+    case 6: return spec_pipe_p<6>(ctx, inverse, mode, done);
+  }
+  *done = false;
+  return CT2G_OK;
+}
+
 }  // namespace
 
 // constant twiddles of the in-register DFTs, once per context (device)
@@ -1307,8 +1660,12 @@ bool ct2g_mg2l_fused(const ct2g_ctx *ctx) {
 // z pass (P2M inside it, or from the moment grid), Y pass, X pass when split
 int ct2g_spec_forward(ct2g_ctx *ctx, int src) {
   CT2G_TRY(ct2g_twiddles(ctx, ctx->M));
-  CT2G_TRY(spec_run(ctx, 0, false, src));
-  CT2G_TRY(spec_run(ctx, 3, false, 0));
+  bool piped = false;
+  CT2G_TRY(spec_pipe(ctx, false, src, &piped));
+  if (!piped) {
+    CT2G_TRY(spec_run(ctx, 0, false, src));
+    CT2G_TRY(spec_run(ctx, 3, false, 0));
+  }
   if (!ct2g_mg2l_fused(ctx)) CT2G_TRY(spec_run(ctx, 3, false, 1));
   return CT2G_OK;
 }
@@ -1323,6 +1680,10 @@ int ct2g_spec_mg2l(ct2g_ctx *ctx) {
 int ct2g_spec_inverse(ct2g_ctx *ctx, bool l2p, bool pot) {
   CT2G_TRY(ct2g_twiddles(ctx, ctx->M));
   if (!ct2g_mg2l_fused(ctx)) CT2G_TRY(spec_run(ctx, 3, true, 1));
+  const int mode = l2p ? (pot ? 1 : 0) : 2;
+  bool piped = false;
+  CT2G_TRY(spec_pipe(ctx, true, mode, &piped));
+  if (piped) return CT2G_OK;
   CT2G_TRY(spec_run(ctx, 3, true, 0));
-  return spec_run(ctx, 2, false, l2p ? (pot ? 1 : 0) : 2);
+  return spec_run(ctx, 2, false, mode);
 }

@@ -262,6 +262,8 @@ struct ct2g_ctx {
   int overlap = 0;             // 1: near field on stream2, concurrent with the mesh solve
   int mg2l_greens_direct = 0;  // 1: the fused x pass reads the Green's values from HBM
   int near_chunks_per_warp = 0;  // overlap: chunks a near-field warp takes before its block exits
+  int plane_pipe = 0;          // > 0: z and y passes as one plane pipeline, this lag in planes
+  int pipe_discard = 1;        // the pipeline's inverse z lines drop the L2 lines they read
   struct ct2g_batch *self_batch = nullptr;  // graph of ct2g_kick_drift
   struct ct2g_learn *learn = nullptr;       // learned near-field correction
   bool fft_tc = false;                      // y/x FFT passes on the tensor cores
@@ -283,6 +285,9 @@ struct ct2g_ctx {
   float *fx = nullptr, *fy = nullptr, *fz = nullptr, *pot = nullptr;
   // near-field accelerations while they run beside the mesh solve (overlap)
   float *nfx = nullptr, *nfy = nullptr, *nfz = nullptr, *npot = nullptr;
+  // plane pipeline counters: per direction an item counter, a spare word and
+  // one count per plane (nbox * mesh planes)
+  uint32_t *pipe_sync = nullptr;
   int *d_maxrung = nullptr;
   unsigned long long *d_inter = nullptr;
   uint32_t *h_pinned = nullptr;  // small pinned host scratch

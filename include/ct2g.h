@@ -233,7 +233,15 @@ int ct2g_batch_destroy(ct2g_batch *b);
  * same results); near_chunks_per_warp -- with overlap, > 0: a near-field warp
  * takes at most this many sink chunks before its block exits, so that the
  * mesh solve's blocks (on the context stream, which has the higher priority)
- * get SMs in between; 0: the near-field grid is persistent. */
+ * get SMs in between; 0: the near-field grid is persistent; plane_pipe --
+ * D > 0 (up to 16): the forward z pass (with P2M) and y pass run as one
+ * persistent kernel that hands out the z lines and y tiles of the x planes
+ * in turn, the y tiles of a plane D planes after its z lines, each waiting
+ * (bounded) for its plane's z lines, so that the y pass reads the plane from
+ * L2; the inverse y pass and z pass (with L2P) likewise, the z lines dropping
+ * the L2 lines they have read (PTX discard.global.L2) instead of letting them
+ * be written back; the same results as 0 (separate passes); meshes 64-256
+ * with the FP32 passes (others run the separate passes). */
 typedef struct {
   int dense_cell;
   int near_blocks_per_sm;
@@ -243,13 +251,15 @@ typedef struct {
   int overlap;
   int mg2l_greens_direct;
   int near_chunks_per_warp;
+  int plane_pipe;
 } ct2g_tuning;
 int ct2g_get_tuning(const ct2g_ctx *ctx, ct2g_tuning *t);
 int ct2g_set_tuning(ct2g_ctx *ctx, const ct2g_tuning *t);
 /* Autotuner: times ct2g_kick_drift (graph replays) on the context's current
  * particles for candidate tunings, keeps the fastest and restores the
  * particles afterwards.  cache_path (may be NULL): a text file of
- * "key dense_cell near_blocks_per_sm fft_tile ms" lines; a hit for this
+ * "key dense_cell near_blocks_per_sm fft_tile sparse_path overlap
+ * mg2l_greens_direct near_chunks_per_warp plane_pipe ms" lines; a hit for this
  * context's key (mesh, order, bwidth, boxes, particle-count octave) is used
  * without timing, a miss is appended.  *out (may be NULL) gets the choice. */
 int ct2g_autotune(ct2g_ctx *ctx, const ct2g_kick_params *p, float dt, float scale,
