@@ -258,7 +258,9 @@ struct ct2g_ctx {
   int near_blocks_per_sm = 0;  // persistent near-field grid: blocks per SM (0: occupancy)
   int fft_tile = 0;            // y/x FFT pass tile width (0: default)
   int split_mg2l = 0;          // 1: X passes and MG2L as three launches, not one
-  int sparse_path = 1;         // sparse sinks: 0 one per lane, 1 per-block warp chunks
+  int sparse_path = 2;         // sparse sinks: 0 one per lane, 1 per-block warp chunks, 2 the
+                               // same chunks with their sources streamed in windows (Plummer;
+                               // the sphere kernel takes 1)
   int overlap = 0;             // 1: near field on stream2, concurrent with the mesh solve
   int mg2l_greens_direct = 0;  // 1: the fused x pass reads the Green's values from HBM
   int near_chunks_per_warp = 0;  // overlap: chunks a near-field warp takes before its block exits

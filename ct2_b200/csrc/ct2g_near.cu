@@ -117,7 +117,169 @@ __device__ __forceinline__ void inblock(int b, int &x, int &y, int &z) {
   z = (b & 1) | ((b >> 2) & 2);
 }
 
-template <int KERNEL, bool POT, bool SPARSE>
+// index of the r-th set bit (r < popcount) of w
+__device__ __forceinline__ int nth_set_bit(unsigned long long w, uint32_t r) {
+  int base = 0;
+  uint32_t c = __popc((uint32_t)w);
+  if (r >= c) {
+    r -= c;
+    w >>= 32;
+    base = 32;
+  }
+  uint32_t v = (uint32_t)w;
+#pragma unroll
+  for (int h = 16; h >= 1; h >>= 1) {
+    c = __popc(v & ((1u << h) - 1u));
+    if (r >= c) {
+      r -= c;
+      v >>= h;
+      base += h;
+    }
+  }
+  return base;
+}
+
+// two masked Plummer interactions from a streamed pair record: (x0 x1 y0 y1)
+// at sbf[4 pr], (z0 z1 t0 t1) at sbf[64 + 4 pr], t the source's window cell
+// (its bits as a float) and tb[t] this lane's 1 / 0 for that cell
+template <bool POT>
+__device__ __forceinline__ void plummer_pair_window(const float *sbf, const float *tb, int pr,
+                                                    f32x2 X, f32x2 Y, f32x2 Z, f32x2 H2,
+                                                    f32x2 &ax, f32x2 &ay, f32x2 &az,
+                                                    f32x2 &ap) {
+  const float4 a = reinterpret_cast<const float4 *>(sbf)[pr];
+  const float4 b = reinterpret_cast<const float4 *>(sbf + 64)[pr];
+  const f32x2 MASK = f2_pack(tb[__float_as_int(b.z)], tb[__float_as_int(b.w)]);
+  const f32x2 dx = f2_sub(X, f2_pack(a.x, a.y));
+  const f32x2 dy = f2_sub(Y, f2_pack(a.z, a.w));
+  const f32x2 dz = f2_sub(Z, f2_pack(b.x, b.y));
+  const f32x2 r2 = f2_fma(dz, dz, f2_fma(dy, dy, f2_fma(dx, dx, H2)));
+  float r0, r1;
+  f2_unpack(r2, r0, r1);
+  const f32x2 ri = f2_mul(f2_pack(rsqrtf(r0), rsqrtf(r1)), MASK);
+  const f32x2 g = f2_mul(f2_mul(ri, ri), ri);
+  ax = f2_fma(dx, g, ax);
+  ay = f2_fma(dy, g, ay);
+  az = f2_fma(dz, g, az);
+  if (POT) ap = f2_sub(ap, ri);
+}
+
+// Sparse chunk, streamed (Plummer): the candidate cells of the chunk (the set
+// bits of `word`, lane o < 27 holding neighbouring block o's) go in windows of
+// 32, a cell per lane; every lane first tabulates, for each cell of the
+// window, whether it lies in its own sink's stencil window (lo2 < |o|^2 <=
+// bw2: tb[t] = 1 or 0, slot 32 always 0); the sources of the window's cells
+// then form one stream, staged in full batches of 32 in the chunk block's
+// frame with the cell slot of each source, and every lane evaluates every
+// staged source, multiplied by its table entry.  Unlike the cell-by-cell walk
+// this keeps the batches full where the candidate cells hold a few particles
+// each.
+template <bool POT>
+__device__ __forceinline__ void sparse_stream(
+    unsigned long long word, uint32_t nblk, const uint32_t *__restrict__ cs,
+    const float4 *__restrict__ src, int px, int py, int pz, float hc, float lo2, float bw2,
+    bool act, f32x2 SX, f32x2 SY, f32x2 SZ, f32x2 H2, float *sbf, float *tb, int lane,
+    f32x2 &pax, f32x2 &pay, f32x2 &paz, f32x2 &pap, uint32_t &nsrc) {
+  const uint32_t c1 = (uint32_t)__popcll(word);
+  uint32_t in1 = c1;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t t = __shfl_up_sync(0xffffffffu, in1, d);
+    if (lane >= d) in1 += t;
+  }
+  const uint32_t ex1 = in1 - c1, C = __shfl_sync(0xffffffffu, in1, 31);
+  tb[32] = 0.f;
+  const int rec = 4 * (lane >> 1) + (lane & 1);
+  for (uint32_t w0 = 0; w0 < C; w0 += 32) {
+    const uint32_t nw = min(32u, C - w0);
+    // window cell of this lane: the (g - ex1[o])-th candidate cell of block o
+    const uint32_t g = min(w0 + (uint32_t)lane, C - 1);
+    int o = 0;
+#pragma unroll
+    for (int step = 16; step > 0; step >>= 1) {
+      const uint32_t e = __shfl_sync(0xffffffffu, ex1, o + step);
+      if (e <= g) o += step;
+    }
+    const unsigned long long wo = __shfl_sync(0xffffffffu, word, o);
+    const uint32_t nbo = __shfl_sync(0xffffffffu, nblk, o);
+    const uint32_t exo = __shfl_sync(0xffffffffu, ex1, o);
+    const int q = nth_set_bit(wo, g - exo);
+    int bx, by, bz;
+    inblock(q, bx, by, bz);
+    // cell offset from the chunk block's cell (0,0,0), biased by 8 per axis
+    const int cpk = (4 * (o / 9 - 1) + bx + 8) | ((4 * ((o / 3) % 3 - 1) + by + 8) << 8) |
+                    ((4 * (o % 3 - 1) + bz + 8) << 16);
+    uint32_t jb = 0, je = 0;
+    if ((uint32_t)lane < nw) {
+      const uint32_t ck = (nbo << 6) | (uint32_t)q;
+      jb = cs[ck];
+      je = cs[ck + 1];
+    }
+    const uint32_t c = je - jb;
+    // this lane's stencil entries for the window's cells
+    for (uint32_t t = 0; t < nw; t++) {
+      const int ct = __shfl_sync(0xffffffffu, cpk, (int)t);
+      const uint32_t nt = __shfl_sync(0xffffffffu, c, (int)t);
+      const int ox = (ct & 255) - 8 - px, oy = ((ct >> 8) & 255) - 8 - py,
+                oz = (ct >> 16) - 8 - pz;
+      const float d2 = (float)(ox * ox + oy * oy + oz * oz);
+      const bool in = d2 > lo2 && d2 <= bw2;
+      tb[t] = in ? 1.f : 0.f;
+      if (in && act) nsrc += nt;
+    }
+    // the window's sources as one stream (lane order)
+    uint32_t incl = c;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, incl, d);
+      if (lane >= d) incl += t;
+    }
+    const uint32_t excl = incl - c;
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    // source gs of the stream in the block frame, and its window slot (32
+    // past the end of the stream: masked for every lane)
+    auto fetch = [&](uint32_t gs, float4 &v) {
+      const uint32_t gg = min(gs, max(total, 1u) - 1);
+      int t = 0;
+#pragma unroll
+      for (int step = 16; step > 0; step >>= 1) {
+        const uint32_t e = __shfl_sync(0xffffffffu, excl, t + step);
+        if (e <= gg) t += step;
+      }
+      const uint32_t jt = __shfl_sync(0xffffffffu, jb, t), et = __shfl_sync(0xffffffffu, je, t);
+      const int ct = __shfl_sync(0xffffffffu, cpk, t);
+      const uint32_t j = min(jt + (gg - __shfl_sync(0xffffffffu, excl, t)), max(et, 1u) - 1u);
+      const float4 s = __ldg(src + j);
+      v = make_float4(fmaf((float)((ct & 255) - 8), hc, s.x),
+                      fmaf((float)(((ct >> 8) & 255) - 8), hc, s.y),
+                      fmaf((float)((ct >> 16) - 8), hc, s.z), __int_as_float(gs < total ? t : 32));
+    };
+    if (total == 0) continue;
+    float4 nq;
+    fetch((uint32_t)lane, nq);
+    for (uint32_t b0 = 0; b0 < total; b0 += 32) {
+      __syncwarp();
+      sbf[rec] = nq.x;
+      sbf[rec + 2] = nq.y;
+      sbf[64 + rec] = nq.z;
+      sbf[64 + rec + 2] = nq.w;
+      __syncwarp();
+      if (b0 + 32 < total) fetch(b0 + 32 + (uint32_t)lane, nq);
+      const int npair = (int)((min(32u, total - b0) + 1) >> 1);
+      if (npair == 16) {
+#pragma unroll 8
+        for (int pr = 0; pr < 16; pr++)
+          plummer_pair_window<POT>(sbf, tb, pr, SX, SY, SZ, H2, pax, pay, paz, pap);
+      } else {
+#pragma unroll 2
+        for (int pr = 0; pr < npair; pr++)
+          plummer_pair_window<POT>(sbf, tb, pr, SX, SY, SZ, H2, pax, pay, paz, pap);
+      }
+    }
+  }
+}
+
+template <int KERNEL, bool POT, bool SPARSE, bool STREAM>
 __device__ __forceinline__ void near_chunk(
     const uint2 cd, const uint32_t *__restrict__ sparse_list,
     const uint32_t *__restrict__ cs, const unsigned long long *__restrict__ occ,
@@ -126,7 +288,7 @@ __device__ __forceinline__ void near_chunk(
     int mbits, float soft, float lo2, float bw2, const float *__restrict__ box_gm,
     float *__restrict__ ofx, float *__restrict__ ofy, float *__restrict__ ofz,
     float *__restrict__ opot, bool store, unsigned long long *__restrict__ inter, float4 *sb,
-    int lane) {
+    float *tbl, int lane) {
   const int M = 1 << mbits;
   const bool act = (uint32_t)lane < cd.y;
   const uint32_t slot = cd.x + (act ? (uint32_t)lane : 0u);
@@ -165,6 +327,16 @@ __device__ __forceinline__ void near_chunk(
   const f32x2 SX = f2_pack(si.x, si.x), SY = f2_pack(si.y, si.y), SZ = f2_pack(si.z, si.z);
   const f32x2 ONE = f2_pack(1.f, 1.f);
   uint32_t nsrc = 0;
+  if constexpr (STREAM) {
+    static_assert(SPARSE && KERNEL == CT2G_SOFT_PLUMMER, "streamed sparse chunks: Plummer only");
+    // the sink in the chunk block's frame (from the centre of its cell (0,0,0))
+    const float sx = fmaf((float)px, hc, si.x), sy = fmaf((float)py, hc, si.y),
+                sz = fmaf((float)pz, hc, si.z);
+    sparse_stream<POT>(word, nblk, cs, src, px, py, pz, hc, lo2, bw2, act,
+                       f2_pack(sx, sx), f2_pack(sy, sy), f2_pack(sz, sz), H2,
+                       reinterpret_cast<float *>(sb), tbl + 33 * lane, lane, pax, pay, paz, pap,
+                       nsrc);
+  } else {
   for (int o = 0; o < 27; o++) {
     const unsigned long long bits = __shfl_sync(0xffffffffu, word, o);
     if (!bits) continue;
@@ -315,6 +487,7 @@ __device__ __forceinline__ void near_chunk(
       }
     }
   }
+  }  // not STREAM
   if constexpr (KERNEL == CT2G_SOFT_PLUMMER) {
     float a0, a1;
     f2_unpack(pax, a0, a1);
@@ -357,7 +530,7 @@ __device__ __forceinline__ void near_chunk(
 // Sparse-style chunks (SPARSE) list sinks through slist and take only the
 // source cells with lo2 < |o|^2 <= bw2 of each lane's own cell; the stencil
 // masks stm must cover that window.
-template <int KERNEL, bool POT, bool SPARSE>
+template <int KERNEL, bool POT, bool SPARSE, bool STREAM = false>
 __global__ void __launch_bounds__(256, 4) near_kernel(
     const uint2 *__restrict__ chunks, const uint32_t *__restrict__ nch_ptr,
     const uint32_t *__restrict__ off_ptr, uint32_t *__restrict__ work,
@@ -369,6 +542,8 @@ __global__ void __launch_bounds__(256, 4) near_kernel(
     float *__restrict__ ofz, float *__restrict__ opot, bool store, uint32_t maxch,
     unsigned long long *__restrict__ inter) {
   __shared__ float4 sbuf[8][32];  // one batch of 32 sources per warp
+  // streamed sparse chunks: per warp, per lane a row of 33 window-cell entries
+  __shared__ float tbl[STREAM ? 8 * 32 * 33 : 1];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const uint32_t nch = *nch_ptr;
   const uint2 *list = off_ptr ? chunks + *off_ptr : chunks;
@@ -379,9 +554,10 @@ __global__ void __launch_bounds__(256, 4) near_kernel(
     if (lane == 0) ch = atomicAdd(work, 1u);
     ch = __shfl_sync(0xffffffffu, ch, 0);
     if (ch >= nch) break;
-    near_chunk<KERNEL, POT, SPARSE>(list[ch], sparse_list, cs, occ, stmask, walk, skeys, rbegin,
-                                    src, mbits, soft, lo2, bw2, box_gm, ofx, ofy, ofz, opot,
-                                    store, inter, sbuf[wib], lane);
+    near_chunk<KERNEL, POT, SPARSE, STREAM>(list[ch], sparse_list, cs, occ, stmask, walk, skeys,
+                                            rbegin, src, mbits, soft, lo2, bw2, box_gm, ofx, ofy,
+                                            ofz, opot, store, inter, sbuf[wib],
+                                            tbl + (STREAM ? wib * 32 * 33 : 0), lane);
   }
 }
 
@@ -539,16 +715,23 @@ Walk make_walk(int mbits) {
 
 // persistent grid: the resident blocks of every SM (or the tuned count), and
 // no more than one block per 256 sinks of the range
-template <int K, bool POT, bool SPARSE>
+template <int K, bool POT, bool SPARSE, bool STREAM = false>
 int launch_near1(ct2g_ctx *ctx, const Walk &walk, const uint2 *chunks, const uint32_t *nch,
                  const uint32_t *off, uint32_t *work, const uint32_t *slist,
                  const unsigned long long *stm, float lo2, float bw2, float *fx, float *fy,
                  float *fz, float *pot, unsigned long long *inter, cudaStream_t st = nullptr,
                  bool store = false, uint32_t maxch = 0) {
-  auto k = near_kernel<K, POT, SPARSE>;
+  auto k = near_kernel<K, POT, SPARSE, STREAM>;
   if (!st) st = ctx->stream;
   int per_sm = 0;
-  CT2G_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 256, 0));
+  if constexpr (STREAM) {
+    // 38 KB of static shared memory a block: the whole L1 as shared memory,
+    // and the resident blocks counted from the kernel's own limits
+    CT2G_TRY(ct2g_smem_attrs(ctx, k, 0));
+    per_sm = ct2g_blocks_per_sm(ctx, (const void *)k, 256, 0);
+  } else {
+    CT2G_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 256, 0));
+  }
   const size_t nr = ctx->n - ctx->rung_begin;
   if (ctx->near_blocks_per_sm > 0) per_sm = std::min(per_sm, ctx->near_blocks_per_sm);
   size_t blocks = (size_t)std::max(1, per_sm) * ctx->num_sms;
@@ -580,6 +763,12 @@ int launch_near(ct2g_ctx *ctx, cudaStream_t st, float *fx, float *fy, float *fz,
                                         ctx->sparse_list, ctx->stmask, -1.f, bw2, fx, fy, fz, pot,
                                         ctx->d_inter, st, store, maxch)));
   if (ctx->sparse_path == 0) return launch_near_lanes<K, POT>(ctx, walk, st, fx, fy, fz, pot, store);
+  if constexpr (K == CT2G_SOFT_PLUMMER) {
+    if (ctx->sparse_path == 2)
+      return launch_near1<K, POT, true, true>(ctx, walk, ctx->chunks, c + 2, c + 0, c + 4,
+                                              ctx->sparse_list, ctx->stmask, -1.f, bw2, fx, fy,
+                                              fz, pot, ctx->d_inter, st, store, maxch);
+  }
   return launch_near1<K, POT, true>(ctx, walk, ctx->chunks, c + 2, c + 0, c + 4,
                                     ctx->sparse_list, ctx->stmask, -1.f, bw2, fx, fy, fz, pot,
                                     ctx->d_inter, st, store, maxch);
@@ -623,6 +812,13 @@ int ct2g_near_window(ct2g_ctx *ctx, const uint2 *chunks, const uint32_t *nch, ui
                : launch_near1<CT2G_SOFT_SPHERE, false, true>(ctx, walk, chunks, nch, nullptr,
                                                              work, slist, stm, lo2, hi2, fx, fy,
                                                              fz, po, nullptr);
+  if (ctx->sparse_path == 2)
+    return pot ? launch_near1<CT2G_SOFT_PLUMMER, true, true, true>(
+                     ctx, walk, chunks, nch, nullptr, work, slist, stm, lo2, hi2, fx, fy, fz, po,
+                     nullptr)
+               : launch_near1<CT2G_SOFT_PLUMMER, false, true, true>(
+                     ctx, walk, chunks, nch, nullptr, work, slist, stm, lo2, hi2, fx, fy, fz, po,
+                     nullptr);
   return pot ? launch_near1<CT2G_SOFT_PLUMMER, true, true>(ctx, walk, chunks, nch, nullptr, work,
                                                            slist, stm, lo2, hi2, fx, fy, fz, po,
                                                            nullptr)

@@ -217,12 +217,16 @@ int ct2g_batch_destroy(ct2g_batch *b);
  * fft_tile -- columns per tile of the y/x FFT passes (0: default); split_mg2l
  * -- 1 runs the X FFT passes and the Green's-function multiply as three
  * kernels, 0 (the default) as one wherever a spectrum column of all
- * components fits in shared memory; sparse_path -- 1 (the default): the
- * sparse sinks of a 4x4x4 cell block share a warp that walks the union of
- * their stencils, each source batch staged once in shared memory; 0: one
- * sparse sink per warp lane, each lane walking its own stencil and reading
- * its own sources (no masked work, but every lane gathers its own sources
- * through the L1 cache); overlap -- 1: the near field runs on a second stream
+ * components fits in shared memory; sparse_path -- 2 (the default): the
+ * sparse sinks of a 4x4x4 cell block share a warp; the candidate cells of
+ * the union of their stencils go in windows of 32, every lane tabulates
+ * which of them lie in its own stencil, and the window's sources are
+ * streamed in full batches of 32 staged in shared memory, each evaluated by
+ * every lane times its table entry (the Plummer kernel; the sphere kernel
+ * takes 1); 1: the same chunks, the union walked cell by cell, each cell's
+ * sources staged as their own batch; 0: one sparse sink per warp lane, each
+ * lane walking its own stencil and reading its own sources (no masked work,
+ * but every lane gathers its own sources through the L1 cache); overlap -- 1: the near field runs on a second stream
  * beside the mesh solve (from the end of binning to the L2P pass) into its
  * own buffers, added to the far field afterwards in the same order as the
  * serial form (0), so both give the same forces bit for bit; the per-stage

@@ -9,8 +9,10 @@ bit-identical to the eager single-box path on the same particles:
   * FFT tile widths and the near-field grid size change which block does the
     work, not its arithmetic.  The sink chunking (dense_cell) moves a sink
     between the dense path (sources shifted into the sink cell's frame) and
-    the sparse path (the sink shifted into each source cell's frame): the
-    same sums with different FP32 rounding, checked to 1e-5 relative.
+    the sparse path (the sink shifted into each source cell's frame), and
+    the streamed sparse path (sparse_path 2) evaluates its sinks and sources
+    in the chunk block's frame: the same sums with different FP32 rounding,
+    checked to 1e-5 relative, with the same interaction count.
 """
 import numpy as np
 import pytest
@@ -153,6 +155,7 @@ def test_batch_of_meshes_matches_eager(gpu):
 
 
 @pytest.mark.parametrize("tuning", [dict(dense_cell=8), dict(dense_cell=48),
+                                    dict(sparse_path=2), dict(sparse_path=2, dense_cell=48),
                                     dict(near_blocks_per_sm=1), dict(fft_tile=32),
                                     dict(fft_tile=128)])
 def test_tuning_keeps_results(gpu, tuning):
@@ -165,9 +168,10 @@ def test_tuning_keeps_results(gpu, tuning):
         g.compute_forces()
     fa, pa = a.forces()
     fb, pb = b.forces()
-    if "dense_cell" in tuning:
+    if "dense_cell" in tuning or "sparse_path" in tuning:
         rel = np.linalg.norm(fa - fb, axis=1) / np.linalg.norm(fa, axis=1)
         assert rel.max() < 1e-5 and np.sqrt(np.mean(rel ** 2)) < 1e-6
+        assert a.interaction_count() == b.interaction_count() > 0
         return
     assert np.array_equal(fa, fb) and np.array_equal(pa, pb)
     a.kick_drift(KP, DT, graph=True)
