@@ -24,7 +24,10 @@
 // exchange patterns are free of bank conflicts.
 #include <type_traits>
 
+#include <cuda.h>  // CUtensorMap and the cuTensorMapEncodeTiled signature (called through the runtime's entry point)
+
 #include "ct2g_internal.cuh"
+#include "ct2g_tc.cuh"
 
 namespace {
 
@@ -452,6 +455,141 @@ int launch_pipe(ct2g_ctx *ctx, C2 *spec, size_t nouter, size_t ostride, size_t r
                                                 twiddle_ptr<C2>(ctx));
   CT2G_LAUNCHED(ctx);
   return CT2G_OK;
+}
+
+// ---- y pass with tiles moved by TMA --------------------------------------------
+// The same column transform as fft_cols_pipe_kernel on the spectrum's y pass,
+// with each tile (N rows x W complex columns of one plane) brought into shared
+// memory by one tiled bulk tensor copy and written back by another: a
+// persistent block keeps S tiles in flight (S - 1 loading while one is
+// transformed), completion through one mbarrier per stage (bounded waits), and
+// no thread spends issue slots on addresses or copies.  The tensor map views
+// the spectrum as floats [plane][y][2 * ldk * NC]; x coordinates are
+// multiples of 2W floats (16-byte aligned), and the last tile of a row reads
+// zeros past its end and stores nothing there.
+constexpr uint32_t kTmaWaitLimit = 1u << 22;
+
+template <int N, int W, bool INV, int S>
+__global__ void __launch_bounds__(256, 1) fft_cols_tma_kernel(
+    const __grid_constant__ CUtensorMap map, uint32_t ntiles, uint32_t ntot,
+    const float2 *__restrict__ tw, uint32_t *__restrict__ status) {
+  // the tensor copies need 128-byte aligned shared memory: the tiles start at
+  // the first 128-byte boundary of the dynamic region (128 bytes reserved for
+  // it), whatever offset the static variables leave that region at
+  extern __shared__ __align__(128) unsigned char smraw[];
+  const uint32_t pad = (128u - (tc::smem_addr(smraw) & 127u)) & 127u;
+  float2 *buf = reinterpret_cast<float2 *>(smraw + pad);  // S tiles of N * W
+  float2 *stw = buf + S * N * W;
+  __shared__ uint64_t bar[S];
+  const int tid = threadIdx.x;
+  if (tc::smem_addr(buf) & 127u) {  // not reached: checked before any copy
+    if (tid == 0) atomicExch(status, (uint32_t)CT2G_ECUDA);
+    return;
+  }
+  load_twiddles(stw, tw, N);
+  if (tid == 0)
+    for (int k = 0; k < S; k++) tc::mbar_init(&bar[k], 1);
+  __syncthreads();
+  auto issue = [&](uint32_t t, int k) {  // thread 0
+    tc::mbar_arrive_expect_tx(&bar[k], (uint32_t)(N * W * sizeof(float2)));
+    tc::tma_load_3d(buf + k * N * W, &map, (int)(2 * W * (t % ntiles)), 0, (int)(t / ntiles),
+                    &bar[k]);
+  };
+  uint32_t t = blockIdx.x;
+  if (tid == 0)
+    for (int k = 0; k < S - 1; k++)
+      if (t + k * gridDim.x < ntot) issue(t + k * gridDim.x, k);
+  uint32_t parity = 0;
+  bool ok = true;
+  for (int it = 0; t < ntot; t += gridDim.x, it++) {
+    const int k = it % S;
+    if (tid == 0) {
+      // the next tile goes into the previous tile's stage once its store has
+      // read it
+      const uint32_t tn = t + (S - 1) * gridDim.x;
+      if (tn < ntot) {
+        tc::bulk_wait_read();
+        issue(tn, (it + S - 1) % S);
+      }
+    }
+    ok = tc::mbar_wait(&bar[k], (parity >> k) & 1u, kTmaWaitLimit);
+    parity ^= 1u << k;
+    if (!__syncthreads_and(ok)) break;
+    float2 *s = buf + k * N * W;
+    tile_fft<N, false, float2, INV>(s, W, W, stw);
+    tc::fence_async_smem();  // this thread's writes, before the bulk store reads them
+    __syncthreads();
+    if (tid == 0) {
+      tc::tma_store_3d(&map, (int)(2 * W * (t % ntiles)), 0, (int)(t / ntiles), s);
+      tc::bulk_commit();
+    }
+  }
+  if (tid == 0) {
+    if (!ok) {
+      atomicExch(status, (uint32_t)CT2G_ETIMEOUT);
+      // loads still in flight land before the block's shared memory goes away
+      for (int k = 0; k < S; k++) tc::mbar_wait(&bar[k], (parity >> k) & 1u, kTmaWaitLimit);
+    }
+    tc::bulk_wait_all();
+  }
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                  const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                  const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// the y-pass tensor map of the context's spectrum for tiles W complex wide
+int ymap_build(ct2g_ctx *ctx, int W) {
+  if (ctx->ymap_w == W) return CT2G_OK;
+  static EncodeTiledFn encode = nullptr;
+  if (!encode) {
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn) {
+      cudaGetLastError();
+      return ct2g_fail(ctx, CT2G_ECUDA, "cuTensorMapEncodeTiled not available");
+    }
+    encode = reinterpret_cast<EncodeTiledFn>(fn);
+  }
+  const cuuint64_t RS = (cuuint64_t)ctx->ldk * ctx->nc, N = (cuuint64_t)ctx->M;
+  const cuuint64_t dims[3] = {2 * RS, N, (cuuint64_t)ctx->nbox * N};
+  const cuuint64_t strides[2] = {RS * sizeof(float2), N * RS * sizeof(float2)};
+  const cuuint32_t box[3] = {(cuuint32_t)(2 * W), (cuuint32_t)N, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  CUtensorMap *m = reinterpret_cast<CUtensorMap *>(ctx->ymap);
+  if (encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, ctx->spec, dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return ct2g_fail(ctx, CT2G_ECUDA, "y-pass tensor map");
+  ctx->ymap_w = W;
+  return CT2G_OK;
+}
+
+template <int N, bool INV>
+int launch_cols_tma(ct2g_ctx *ctx) {
+  if constexpr (N < 64 || N > 256) {
+    return ct2g_fail(ctx, CT2G_EINVAL, "TMA y pass: meshes 64-256");
+  } else {
+    // W 32 with three stages (one block per SM), or 16 with three (two)
+    const bool narrow = ctx->fft_tile == 16;
+    const int W = narrow ? 16 : 32;
+    CT2G_TRY(ymap_build(ctx, W));
+    const uint32_t ncols = (uint32_t)((N / 2 + 1) * ctx->nc);
+    const uint32_t ntiles = (ncols + W - 1) / W, ntot = ntiles * (uint32_t)(ctx->nbox * N);
+    auto k = narrow ? fft_cols_tma_kernel<N, 16, INV, 3> : fft_cols_tma_kernel<N, 32, INV, 3>;
+    const size_t smem = sizeof(float2) * (3 * (size_t)N * W + N) + 128;
+    CT2G_TRY(ct2g_smem_attrs(ctx, k, smem));
+    const int per_sm = ct2g_blocks_per_sm(ctx, (const void *)k, 256, smem);
+    const uint32_t grid = std::min(ntot, (uint32_t)(per_sm * ctx->num_sms));
+    const CUtensorMap *m = reinterpret_cast<const CUtensorMap *>(ctx->ymap);
+    k<<<grid, 256, smem, ctx->stream>>>(*m, ntiles, ntot, twiddle_ptr<float2>(ctx),
+                                        ctx->d_counts + 6);
+    CT2G_LAUNCHED(ctx);
+    return CT2G_OK;
+  }
 }
 
 // column tile widths: the default W, and W/2 or 2W (FP32 only) when the
@@ -1500,6 +1638,10 @@ int spec_cols(ct2g_ctx *ctx, bool inv, bool xpass) {
   if constexpr (N == 256 || N == 512) {
     if (ctx->fft_tc)
       return ct2g_fft_cols_tc(ctx, ctx->spec, N, nouter, ostride, rstride, ncols, inv);
+  }
+  if constexpr (N >= 64 && N <= 256) {
+    if (ctx->cols_tma && !xpass)
+      return inv ? launch_cols_tma<N, true>(ctx) : launch_cols_tma<N, false>(ctx);
   }
   if (inv) return launch_cols<float, N, true, true>(ctx, ctx->spec, nouter, ostride, rstride, ncols);
   return launch_cols<float, N, false, true>(ctx, ctx->spec, nouter, ostride, rstride, ncols);

@@ -265,6 +265,10 @@ struct ct2g_ctx {
   int mg2l_greens_direct = 0;  // 1: the fused x pass reads the Green's values from HBM
   int near_chunks_per_warp = 0;  // overlap: chunks a near-field warp takes before its block exits
   int plane_pipe = 0;          // > 0: z and y passes as one plane pipeline, this lag in planes
+  int cols_tma = 1;            // 1: the mesh y passes move their tiles by TMA
+  // tensor map of the spectrum's y-pass tiles (a CUtensorMap, built once)
+  alignas(64) unsigned char ymap[128] = {};
+  int ymap_w = 0;              // tile width the map was built for (0: none)
   int pipe_discard = 1;        // the pipeline's inverse z lines drop the L2 lines they read
   struct ct2g_batch *self_batch = nullptr;  // graph of ct2g_kick_drift
   struct ct2g_learn *learn = nullptr;       // learned near-field correction

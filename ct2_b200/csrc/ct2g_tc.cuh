@@ -115,6 +115,60 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32
   return mbar_test(bar, parity);
 }
 
+// the mbarrier's current phase gets one arrival and expects `bytes` more
+// transaction bytes (bulk copies that complete on it)
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+}
+// bulk copy global -> this CTA's shared memory (16-byte aligned addresses, a
+// multiple of 16 bytes), completing `bytes` transaction bytes on bar
+__device__ __forceinline__ void bulk_load(void *sdst, const void *gsrc, uint32_t bytes,
+                                          uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+          smem_addr(sdst)),
+      "l"(gsrc), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+// bulk copy shared -> global in the thread's current bulk group
+__device__ __forceinline__ void bulk_store(void *gdst, const void *ssrc, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n" ::"l"(gdst),
+               "r"(smem_addr(ssrc)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() {
+  asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+}
+// this thread's bulk stores have finished reading shared memory
+__device__ __forceinline__ void bulk_wait_read() {
+  asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");
+}
+// this thread's bulk stores are complete
+__device__ __forceinline__ void bulk_wait_all() {
+  asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
+}
+
+// tiled bulk tensor copies through a tensor map (3D, no multicast): the box
+// at coordinates (x, y, z) into / out of this CTA's shared memory
+__device__ __forceinline__ void tma_load_3d(void *sdst, const void *map, int x, int y, int z,
+                                            uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], "
+      "[%1, {%2, %3, %4}], [%5];\n" ::"r"(smem_addr(sdst)),
+      "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_addr(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tma_store_3d(const void *map, int x, int y, int z,
+                                             const void *ssrc) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];\n" ::"l"(
+          map),
+      "r"(x), "r"(y), "r"(z), "r"(smem_addr(ssrc))
+      : "memory");
+}
+
 // 32 consecutive FP32 columns of this thread's lane (warp w reads lanes
 // 32 (w % 4) .. +31); taddr carries the warp's lane base in bits 16-31
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {

@@ -245,7 +245,12 @@ int ct2g_batch_destroy(ct2g_batch *b);
  * L2; the inverse y pass and z pass (with L2P) likewise, the z lines dropping
  * the L2 lines they have read (PTX discard.global.L2) instead of letting them
  * be written back; the same results as 0 (separate passes); meshes 64-256
- * with the FP32 passes (others run the separate passes). */
+ * with the FP32 passes (others run the separate passes); cols_tma -- 1: the
+ * mesh's y FFT passes move each tile (all rows of a plane x 32 complex
+ * columns; 16 with fft_tile 16) by one tiled bulk tensor copy (TMA) in and
+ * one out, three tiles in flight per block (meshes 64-256, FP32 passes; the
+ * default); 0: every thread copies its share of each tile (cp.async, two
+ * tiles in flight); the same results. */
 typedef struct {
   int dense_cell;
   int near_blocks_per_sm;
@@ -256,6 +261,7 @@ typedef struct {
   int mg2l_greens_direct;
   int near_chunks_per_warp;
   int plane_pipe;
+  int cols_tma;
 } ct2g_tuning;
 int ct2g_get_tuning(const ct2g_ctx *ctx, ct2g_tuning *t);
 int ct2g_set_tuning(ct2g_ctx *ctx, const ct2g_tuning *t);
@@ -263,7 +269,7 @@ int ct2g_set_tuning(ct2g_ctx *ctx, const ct2g_tuning *t);
  * particles for candidate tunings, keeps the fastest and restores the
  * particles afterwards.  cache_path (may be NULL): a text file of
  * "key dense_cell near_blocks_per_sm fft_tile sparse_path overlap
- * mg2l_greens_direct near_chunks_per_warp plane_pipe ms" lines; a hit for this
+ * mg2l_greens_direct near_chunks_per_warp plane_pipe cols_tma ms" lines; a hit for this
  * context's key (mesh, order, bwidth, boxes, particle-count octave) is used
  * without timing, a miss is appended.  *out (may be NULL) gets the choice. */
 int ct2g_autotune(ct2g_ctx *ctx, const ct2g_kick_params *p, float dt, float scale,
