@@ -539,9 +539,8 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t
                                   const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
-// the y-pass tensor map of the context's spectrum for tiles W complex wide
-int ymap_build(ct2g_ctx *ctx, int W) {
-  if (ctx->ymap_w == W) return CT2G_OK;
+// the driver's tensor-map encoder, looked up once through the runtime
+int tensor_map_encoder(ct2g_ctx *ctx, EncodeTiledFn *out) {
   static EncodeTiledFn encode = nullptr;
   if (!encode) {
     void *fn = nullptr;
@@ -554,6 +553,15 @@ int ymap_build(ct2g_ctx *ctx, int W) {
     }
     encode = reinterpret_cast<EncodeTiledFn>(fn);
   }
+  *out = encode;
+  return CT2G_OK;
+}
+
+// the y-pass tensor map of the context's spectrum for tiles W complex wide
+int ymap_build(ct2g_ctx *ctx, int W) {
+  if (ctx->ymap_w == W) return CT2G_OK;
+  EncodeTiledFn encode = nullptr;
+  CT2G_TRY(tensor_map_encoder(ctx, &encode));
   const cuuint64_t RS = (cuuint64_t)ctx->ldk * ctx->nc, N = (cuuint64_t)ctx->M;
   const cuuint64_t dims[3] = {2 * RS, N, (cuuint64_t)ctx->nbox * N};
   const cuuint64_t strides[2] = {RS * sizeof(float2), N * RS * sizeof(float2)};
@@ -1497,8 +1505,8 @@ __device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
 // without a pass through shared memory.  cols_step1: jobs (l, n1), input
 // ld(l, r), Y[n1][k2] to smem.  cols_step2: jobs (l, k2), X[k2 + R2*k1] to
 // st(l, r, v); INPLACE when st writes the smem slots the step reads.
-template <int N, int NL, bool INV, int NT, typename LD>
-__device__ __forceinline__ void cols_step1(float2 *s, const float2 *stw, LD ld) {
+template <int N, int NL, bool INV, int NT, int PITCH = NL, typename LD>
+__device__ __forceinline__ void cols_step1(float2 *s, const float2 *stw, LD ld, int off = 0) {
   using LL = LineLayout<N, false>;
   constexpr int R1 = LL::R1, R2 = LL::R2;
   for (int job = threadIdx.x; job < NL * R1; job += NT) {
@@ -1514,12 +1522,12 @@ __device__ __forceinline__ void cols_step1(float2 *s, const float2 *stw, LD ld) 
       v[k2] = cmul(v[k2], w);
     }
 #pragma unroll
-    for (int k2 = 0; k2 < R2; k2++) s[(n1 + R1 * k2) * NL + l] = v[k2];
+    for (int k2 = 0; k2 < R2; k2++) s[(n1 + R1 * k2) * PITCH + off + l] = v[k2];
   }
 }
 
-template <int N, int NL, bool INV, bool INPLACE, int NT, typename ST>
-__device__ __forceinline__ void cols_step2(const float2 *s, ST st) {
+template <int N, int NL, bool INV, bool INPLACE, int NT, int PITCH = NL, typename ST>
+__device__ __forceinline__ void cols_step2(const float2 *s, ST st, int off = 0) {
   using LL = LineLayout<N, false>;
   constexpr int R1 = LL::R1, R2 = LL::R2;
   static_assert(NT % R2 == 0, "block size must be a multiple of R2");
@@ -1530,7 +1538,7 @@ __device__ __forceinline__ void cols_step2(const float2 *s, ST st) {
     float2 v[R1];
     if (on) {
 #pragma unroll
-      for (int n1 = 0; n1 < R1; n1++) v[n1] = s[(n1 + R1 * k2) * NL + l];
+      for (int n1 = 0; n1 < R1; n1++) v[n1] = s[(n1 + R1 * k2) * PITCH + off + l];
       reg_dft<R1, float2, INV>(v);
     }
     if (INPLACE) __syncthreads();  // all reads of this round before any write
@@ -1596,6 +1604,98 @@ __global__ void __launch_bounds__(256, FxShape<P, N, GD>::MINB) fftx_mg2l_kernel
   cols_step2<N, NC, true, false, 256>(s, [&](int l, int r, float2 v) { col[r * XS + l] = v; });
 }
 
+// The fused x pass + MG2L with its inputs brought in by bulk copies: the
+// column (every qi row's NC components) by one tiled tensor copy, its rows
+// PITCH complex apart (the copy starts on the 16-byte boundary at or below
+// the column: `off` = 0 or 1 complex into each row), and the Green's column
+// (contiguous) by one bulk copy, both completing on one mbarrier (bounded
+// wait) while the twiddles load.  The transforms run in place in the copied
+// tile; the inverse's last step writes the column back from registers (a
+// tensor store would also write the neighbouring column's element that the
+// tile carries, which another block owns).
+template <int P, int N>
+struct FxTma {
+  static constexpr int NC = ct2g_ncomp(P), NH = N / 2 + 1;
+  static constexpr int BW = (2 * NC + 3) / 4 * 4;  // floats per tile row (16-byte multiple)
+  static constexpr int PITCH = BW / 2;             // complex per tile row
+  static constexpr int GCOL = NC * N;
+  static constexpr size_t SMEM = 128 + sizeof(float2) * (size_t)N * PITCH +
+                                 sizeof(float) * (size_t)GCOL + sizeof(float2) * (size_t)N;
+  static constexpr bool OK = N >= 64 && N <= 256 && SMEM <= 227 * 1024;
+};
+
+template <int P, int N>
+__global__ void __launch_bounds__(256, FxShape<P, N>::MINB) fftx_mg2l_tma_kernel(
+    const __grid_constant__ CUtensorMap xmap, float2 *__restrict__ spec, int ldk,
+    const float *__restrict__ gx, const float2 *__restrict__ tw, uint32_t *__restrict__ status) {
+  using S = FxTma<P, N>;
+  constexpr int NC = S::NC, NH = S::NH, PITCH = S::PITCH;
+  // the tensor copy needs a 128-byte aligned destination: the tile starts at
+  // the first 128-byte boundary of the dynamic region (128 bytes reserved)
+  extern __shared__ __align__(128) unsigned char smraw[];
+  const uint32_t pad = (128u - (tc::smem_addr(smraw) & 127u)) & 127u;
+  float2 *s = reinterpret_cast<float2 *>(smraw + pad);  // N rows of PITCH
+  float *sg = reinterpret_cast<float *>(s + N * PITCH);
+  float2 *stw = reinterpret_cast<float2 *>(sg + S::GCOL);
+  __shared__ uint64_t bar;
+  const int qk = (int)(blockIdx.x % NH);
+  const int qj = (int)((blockIdx.x / NH) % N);
+  const int box = (int)(blockIdx.x / ((unsigned)NH * N));
+  const int64_t RS = (int64_t)ldk * NC, XS = (int64_t)N * RS;
+  const int f0 = 2 * qk * NC, x0 = f0 & ~3, off = (f0 - x0) / 2;
+  if (tc::smem_addr(s) & 127u) {  // not reached: checked before any copy
+    if (threadIdx.x == 0) atomicExch(status, (uint32_t)CT2G_ECUDA);
+    return;
+  }
+  if (threadIdx.x == 0) tc::mbar_init(&bar, 1);
+  __syncthreads();  // the barrier is initialised before any thread polls it
+  if (threadIdx.x == 0) {
+    tc::mbar_arrive_expect_tx(
+        &bar, (uint32_t)(sizeof(float2) * N * PITCH + sizeof(float) * S::GCOL));
+    tc::tma_load_4d(s, &xmap, x0, qj, 0, box, &bar);
+    tc::bulk_load(sg, gx + ((int64_t)qj * NH + qk) * S::GCOL, (uint32_t)(sizeof(float) * S::GCOL),
+                  &bar);
+  }
+  load_twiddles(stw, tw, N);
+  const bool ok = tc::mbar_wait(&bar, 0, kTmaWaitLimit);
+  if (!__syncthreads_and(ok)) {
+    if (threadIdx.x == 0) {
+      atomicExch(status, (uint32_t)CT2G_ETIMEOUT);
+      tc::mbar_wait(&bar, 0, kTmaWaitLimit);  // copies in flight land before the block exits
+    }
+    return;
+  }
+  // forward transform in place in the tile
+  cols_step1<N, NC, false, 256, PITCH>(
+      s, stw, [&](int l, int r) { return s[r * PITCH + off + l]; }, off);
+  __syncthreads();
+  cols_step2<N, NC, false, true, 256, PITCH>(
+      s, [&](int l, int r, float2 v) { s[r * PITCH + off + l] = v; }, off);
+  __syncthreads();
+  for (int qi = threadIdx.x; qi < N; qi += 256) {
+    float2 *row = s + qi * PITCH + off;
+    float2 m[NC];
+#pragma unroll
+    for (int k = 0; k < NC; k++) m[k] = row[k];
+    if constexpr (FxShape<P, N>::GREG) {
+      float g[NC];
+#pragma unroll
+      for (int k = 0; k < NC; k++) g[k] = sg[k * N + qi];
+      ct2g_mg2l_all<P, 1>(m, g, row, std::make_integer_sequence<int, Mg2lPairs<P>::NP>{});
+    } else {
+      ct2g_mg2l_all<P, N>(m, sg + qi, row, std::make_integer_sequence<int, Mg2lPairs<P>::NP>{});
+    }
+  }
+  __syncthreads();
+  // inverse: the second step writes the column back to HBM
+  float2 *col = spec + (int64_t)box * N * XS + (int64_t)qj * RS + (int64_t)qk * NC;
+  cols_step1<N, NC, true, 256, PITCH>(
+      s, stw, [&](int l, int r) { return s[r * PITCH + off + l]; }, off);
+  __syncthreads();
+  cols_step2<N, NC, true, false, 256, PITCH>(
+      s, [&](int l, int r, float2 v) { col[r * XS + l] = v; }, off);
+}
+
 template <int P, int N, bool GD>
 int launch_fx_mg2l_g(ct2g_ctx *ctx) {
   using S = FxShape<P, N, GD>;
@@ -1612,8 +1712,50 @@ int launch_fx_mg2l_g(ct2g_ctx *ctx) {
   }
 }
 
+// the x-pass tensor map: the spectrum as floats [box][qi][qj][2 * ldk * NC],
+// a box of BW floats x all N rows qi of one (qj, box)
+int xmap_build(ct2g_ctx *ctx, int BW) {
+  if (ctx->xmap_bw == BW) return CT2G_OK;
+  EncodeTiledFn encode = nullptr;
+  CT2G_TRY(tensor_map_encoder(ctx, &encode));
+  const cuuint64_t RS = (cuuint64_t)ctx->ldk * ctx->nc, N = (cuuint64_t)ctx->M;
+  const cuuint64_t dims[4] = {2 * RS, N, N, (cuuint64_t)ctx->nbox};
+  const cuuint64_t strides[3] = {RS * sizeof(float2), N * RS * sizeof(float2),
+                                 N * N * RS * sizeof(float2)};
+  const cuuint32_t box[4] = {(cuuint32_t)BW, 1, (cuuint32_t)N, 1};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  CUtensorMap *m = reinterpret_cast<CUtensorMap *>(ctx->xmap);
+  if (encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, ctx->spec, dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return ct2g_fail(ctx, CT2G_ECUDA, "x-pass tensor map");
+  ctx->xmap_bw = BW;
+  return CT2G_OK;
+}
+
+template <int P, int N>
+int launch_fx_mg2l_tma(ct2g_ctx *ctx) {
+  using S = FxTma<P, N>;
+  if constexpr (!S::OK) {
+    return ct2g_fail(ctx, CT2G_EINVAL, "TMA x pass: meshes 64-256");
+  } else {
+    CT2G_TRY(xmap_build(ctx, S::BW));
+    const size_t ncol = (size_t)ctx->nbox * N * S::NH;
+    auto k = fftx_mg2l_tma_kernel<P, N>;
+    CT2G_TRY(ct2g_smem_attrs(ctx, k, S::SMEM));
+    const CUtensorMap *m = reinterpret_cast<const CUtensorMap *>(ctx->xmap);
+    k<<<(unsigned)ncol, 256, S::SMEM, ctx->stream>>>(*m, ctx->spec, ctx->ldk, ctx->greens_x,
+                                                     twiddle_ptr<float2>(ctx), ctx->d_counts + 6);
+    CT2G_LAUNCHED(ctx);
+    return CT2G_OK;
+  }
+}
+
 template <int P, int N>
 int launch_fx_mg2l(ct2g_ctx *ctx) {
+  if constexpr (FxTma<P, N>::OK) {
+    if (ctx->x_tma) return launch_fx_mg2l_tma<P, N>(ctx);
+  }
   return ctx->mg2l_greens_direct ? launch_fx_mg2l_g<P, N, true>(ctx)
                                  : launch_fx_mg2l_g<P, N, false>(ctx);
 }

@@ -269,6 +269,10 @@ struct ct2g_ctx {
   // tensor map of the spectrum's y-pass tiles (a CUtensorMap, built once)
   alignas(64) unsigned char ymap[128] = {};
   int ymap_w = 0;              // tile width the map was built for (0: none)
+  int x_tma = 1;               // 1: the fused x pass's inputs arrive by bulk copies
+  // tensor map of the spectrum's x-pass columns (a CUtensorMap, built once)
+  alignas(64) unsigned char xmap[128] = {};
+  int xmap_bw = 0;             // box width (floats) the map was built for (0: none)
   int pipe_discard = 1;        // the pipeline's inverse z lines drop the L2 lines they read
   struct ct2g_batch *self_batch = nullptr;  // graph of ct2g_kick_drift
   struct ct2g_learn *learn = nullptr;       // learned near-field correction

@@ -160,6 +160,14 @@ __device__ __forceinline__ void tma_load_3d(void *sdst, const void *map, int x, 
       "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_addr(bar))
       : "memory");
 }
+__device__ __forceinline__ void tma_load_4d(void *sdst, const void *map, int x, int y, int z,
+                                            int w, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], "
+      "[%1, {%2, %3, %4, %5}], [%6];\n" ::"r"(smem_addr(sdst)),
+      "l"(map), "r"(x), "r"(y), "r"(z), "r"(w), "r"(smem_addr(bar))
+      : "memory");
+}
 __device__ __forceinline__ void tma_store_3d(const void *map, int x, int y, int z,
                                              const void *ssrc) {
   asm volatile(

@@ -250,7 +250,11 @@ int ct2g_batch_destroy(ct2g_batch *b);
  * columns; 16 with fft_tile 16) by one tiled bulk tensor copy (TMA) in and
  * one out, three tiles in flight per block (meshes 64-256, FP32 passes; the
  * default); 0: every thread copies its share of each tile (cp.async, two
- * tiles in flight); the same results. */
+ * tiles in flight); the same results; x_tma -- 1 (the default): the fused x
+ * pass + Green's multiply brings each spectrum column in by one tiled bulk
+ * tensor copy and its Green's column by one bulk copy (meshes 64-256, FP32
+ * passes; mg2l_greens_direct then does not apply); 0: per-thread loads; the
+ * same results. */
 typedef struct {
   int dense_cell;
   int near_blocks_per_sm;
@@ -262,6 +266,7 @@ typedef struct {
   int near_chunks_per_warp;
   int plane_pipe;
   int cols_tma;
+  int x_tma;
 } ct2g_tuning;
 int ct2g_get_tuning(const ct2g_ctx *ctx, ct2g_tuning *t);
 int ct2g_set_tuning(ct2g_ctx *ctx, const ct2g_tuning *t);
@@ -269,7 +274,7 @@ int ct2g_set_tuning(ct2g_ctx *ctx, const ct2g_tuning *t);
  * particles for candidate tunings, keeps the fastest and restores the
  * particles afterwards.  cache_path (may be NULL): a text file of
  * "key dense_cell near_blocks_per_sm fft_tile sparse_path overlap
- * mg2l_greens_direct near_chunks_per_warp plane_pipe cols_tma ms" lines; a hit for this
+ * mg2l_greens_direct near_chunks_per_warp plane_pipe cols_tma x_tma ms" lines; a hit for this
  * context's key (mesh, order, bwidth, boxes, particle-count octave) is used
  * without timing, a miss is appended.  *out (may be NULL) gets the choice. */
 int ct2g_autotune(ct2g_ctx *ctx, const ct2g_kick_params *p, float dt, float scale,

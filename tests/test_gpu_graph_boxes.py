@@ -6,9 +6,9 @@ bit-identical to the eager single-box path on the same particles:
   * a box context sorts each box's particles exactly as a one-box context
     does (the box index sits above the Morton key of a stable sort), runs the
     same per-grid FFT and the same per-sink near-field sequence;
-  * FFT tile widths, the y pass's tile transport (TMA or per-thread copies)
-    and the near-field grid size change which block does the work, not its
-    arithmetic.  The sink chunking (dense_cell) moves a sink
+  * FFT tile widths, the y and x passes' transport (TMA or per-thread
+    copies) and the near-field grid size change which block does the work,
+    not its arithmetic.  The sink chunking (dense_cell) moves a sink
     between the dense path (sources shifted into the sink cell's frame) and
     the sparse path (the sink shifted into each source cell's frame), and
     the streamed sparse path (sparse_path 2) evaluates its sinks and sources
@@ -158,8 +158,9 @@ def test_batch_of_meshes_matches_eager(gpu):
 @pytest.mark.parametrize("tuning", [dict(dense_cell=8), dict(dense_cell=48),
                                     dict(sparse_path=2), dict(sparse_path=2, dense_cell=48),
                                     dict(near_blocks_per_sm=1), dict(fft_tile=32),
-                                    dict(fft_tile=128), dict(cols_tma=1),
-                                    dict(cols_tma=1, fft_tile=16)])
+                                    dict(fft_tile=128), dict(cols_tma=0),
+                                    dict(cols_tma=1, fft_tile=16), dict(x_tma=0),
+                                    dict(x_tma=0, mg2l_greens_direct=1)])
 def test_tuning_keeps_results(gpu, tuning):
     P = _box(40000, 5, 64)
     a, b = _mk(64, order=4), _mk(64, order=4)
