@@ -1607,61 +1607,71 @@ __global__ void __launch_bounds__(256, FxShape<P, N, GD>::MINB) fftx_mg2l_kernel
 // The fused x pass + MG2L with its inputs brought in by bulk copies: the
 // column (every qi row's NC components) by one tiled tensor copy, its rows
 // PITCH complex apart (the copy starts on the 16-byte boundary at or below
-// the column: `off` = 0 or 1 complex into each row), and the Green's column
-// (contiguous) by one bulk copy, both completing on one mbarrier (bounded
-// wait) while the twiddles load.  The transforms run in place in the copied
-// tile; the inverse's last step writes the column back from registers (a
-// tensor store would also write the neighbouring column's element that the
-// tile carries, which another block owns).
-template <int P, int N>
+// the column: `off` = 0 or 1 complex into each row), and, unless GD, the
+// Green's column (contiguous) by one bulk copy, completing on one mbarrier
+// (bounded wait) while the twiddles load; GD: the contraction reads the
+// Green's values from HBM, and the smaller block (no Green's column, no
+// static shared memory, so the dynamic region starts 128-byte aligned) fits
+// three to an SM.  The transforms run in place in the copied tile; the
+// inverse's last step writes the column back from registers (a tensor store
+// would also write the neighbouring column's element that the tile carries,
+// which another block owns).
+template <int P, int N, bool GD>
 struct FxTma {
   static constexpr int NC = ct2g_ncomp(P), NH = N / 2 + 1;
   static constexpr int BW = (2 * NC + 3) / 4 * 4;  // floats per tile row (16-byte multiple)
   static constexpr int PITCH = BW / 2;             // complex per tile row
   static constexpr int GCOL = NC * N;
-  static constexpr size_t SMEM = 128 + sizeof(float2) * (size_t)N * PITCH +
-                                 sizeof(float) * (size_t)GCOL + sizeof(float2) * (size_t)N;
+  // GD: tile, twiddles, the mbarrier; else 128 bytes of alignment slack,
+  // tile, Green's column, twiddles, the mbarrier
+  static constexpr size_t SMEM = (GD ? 0 : 128) + sizeof(float2) * (size_t)N * PITCH +
+                                 (GD ? 0 : sizeof(float) * (size_t)GCOL) +
+                                 sizeof(float2) * (size_t)N + 16;
   static constexpr bool OK = N >= 64 && N <= 256 && SMEM <= 227 * 1024;
+  // three blocks per SM where the contraction fits 85 registers (GD, orders
+  // up to 4) and three blocks' shared memory fit
+  static constexpr int MINB = (GD && NC <= 35 && 3 * (SMEM + 1024) <= 228 * 1024) ? 3
+                              : 2 * (SMEM + 1024) <= 228 * 1024               ? 2
+                                                                              : 1;
 };
 
-template <int P, int N>
-__global__ void __launch_bounds__(256, FxShape<P, N>::MINB) fftx_mg2l_tma_kernel(
+template <int P, int N, bool GD>
+__global__ void __launch_bounds__(256, FxTma<P, N, GD>::MINB) fftx_mg2l_tma_kernel(
     const __grid_constant__ CUtensorMap xmap, float2 *__restrict__ spec, int ldk,
     const float *__restrict__ gx, const float2 *__restrict__ tw, uint32_t *__restrict__ status) {
-  using S = FxTma<P, N>;
+  using S = FxTma<P, N, GD>;
   constexpr int NC = S::NC, NH = S::NH, PITCH = S::PITCH;
-  // the tensor copy needs a 128-byte aligned destination: the tile starts at
-  // the first 128-byte boundary of the dynamic region (128 bytes reserved)
+  // the tensor copy needs a 128-byte aligned destination
   extern __shared__ __align__(128) unsigned char smraw[];
-  const uint32_t pad = (128u - (tc::smem_addr(smraw) & 127u)) & 127u;
+  const uint32_t pad = GD ? 0u : (128u - (tc::smem_addr(smraw) & 127u)) & 127u;
   float2 *s = reinterpret_cast<float2 *>(smraw + pad);  // N rows of PITCH
   float *sg = reinterpret_cast<float *>(s + N * PITCH);
-  float2 *stw = reinterpret_cast<float2 *>(sg + S::GCOL);
-  __shared__ uint64_t bar;
+  float2 *stw = reinterpret_cast<float2 *>(sg + (GD ? 0 : S::GCOL));
+  uint64_t *bar = reinterpret_cast<uint64_t *>(stw + N);
   const int qk = (int)(blockIdx.x % NH);
   const int qj = (int)((blockIdx.x / NH) % N);
   const int box = (int)(blockIdx.x / ((unsigned)NH * N));
   const int64_t RS = (int64_t)ldk * NC, XS = (int64_t)N * RS;
   const int f0 = 2 * qk * NC, x0 = f0 & ~3, off = (f0 - x0) / 2;
-  if (tc::smem_addr(s) & 127u) {  // not reached: checked before any copy
+  const float *gcol = gx + ((int64_t)qj * NH + qk) * S::GCOL;
+  if (tc::smem_addr(s) & 127u) {  // checked before any copy
     if (threadIdx.x == 0) atomicExch(status, (uint32_t)CT2G_ECUDA);
     return;
   }
-  if (threadIdx.x == 0) tc::mbar_init(&bar, 1);
+  if (threadIdx.x == 0) tc::mbar_init(bar, 1);
   __syncthreads();  // the barrier is initialised before any thread polls it
   if (threadIdx.x == 0) {
     tc::mbar_arrive_expect_tx(
-        &bar, (uint32_t)(sizeof(float2) * N * PITCH + sizeof(float) * S::GCOL));
-    tc::tma_load_4d(s, &xmap, x0, qj, 0, box, &bar);
-    tc::bulk_load(sg, gx + ((int64_t)qj * NH + qk) * S::GCOL, (uint32_t)(sizeof(float) * S::GCOL),
-                  &bar);
+        bar, (uint32_t)(sizeof(float2) * N * PITCH + (GD ? 0 : sizeof(float) * S::GCOL)));
+    tc::tma_load_4d(s, &xmap, x0, qj, 0, box, bar);
+    if constexpr (!GD) tc::bulk_load(sg, gcol, (uint32_t)(sizeof(float) * S::GCOL), bar);
   }
   load_twiddles(stw, tw, N);
-  const bool ok = tc::mbar_wait(&bar, 0, kTmaWaitLimit);
+  const bool ok = tc::mbar_wait(bar, 0, kTmaWaitLimit);
   if (!__syncthreads_and(ok)) {
     if (threadIdx.x == 0) {
       atomicExch(status, (uint32_t)CT2G_ETIMEOUT);
-      tc::mbar_wait(&bar, 0, kTmaWaitLimit);  // copies in flight land before the block exits
+      tc::mbar_wait(bar, 0, kTmaWaitLimit);  // copies in flight land before the block exits
     }
     return;
   }
@@ -1677,7 +1687,9 @@ __global__ void __launch_bounds__(256, FxShape<P, N>::MINB) fftx_mg2l_tma_kernel
     float2 m[NC];
 #pragma unroll
     for (int k = 0; k < NC; k++) m[k] = row[k];
-    if constexpr (FxShape<P, N>::GREG) {
+    if constexpr (GD) {
+      ct2g_mg2l_all<P, N>(m, gcol + qi, row, std::make_integer_sequence<int, Mg2lPairs<P>::NP>{});
+    } else if constexpr (FxShape<P, N>::GREG) {
       float g[NC];
 #pragma unroll
       for (int k = 0; k < NC; k++) g[k] = sg[k * N + qi];
@@ -1733,15 +1745,15 @@ int xmap_build(ct2g_ctx *ctx, int BW) {
   return CT2G_OK;
 }
 
-template <int P, int N>
+template <int P, int N, bool GD>
 int launch_fx_mg2l_tma(ct2g_ctx *ctx) {
-  using S = FxTma<P, N>;
+  using S = FxTma<P, N, GD>;
   if constexpr (!S::OK) {
     return ct2g_fail(ctx, CT2G_EINVAL, "TMA x pass: meshes 64-256");
   } else {
     CT2G_TRY(xmap_build(ctx, S::BW));
     const size_t ncol = (size_t)ctx->nbox * N * S::NH;
-    auto k = fftx_mg2l_tma_kernel<P, N>;
+    auto k = fftx_mg2l_tma_kernel<P, N, GD>;
     CT2G_TRY(ct2g_smem_attrs(ctx, k, S::SMEM));
     const CUtensorMap *m = reinterpret_cast<const CUtensorMap *>(ctx->xmap);
     k<<<(unsigned)ncol, 256, S::SMEM, ctx->stream>>>(*m, ctx->spec, ctx->ldk, ctx->greens_x,
@@ -1753,8 +1765,11 @@ int launch_fx_mg2l_tma(ct2g_ctx *ctx) {
 
 template <int P, int N>
 int launch_fx_mg2l(ct2g_ctx *ctx) {
-  if constexpr (FxTma<P, N>::OK) {
-    if (ctx->x_tma) return launch_fx_mg2l_tma<P, N>(ctx);
+  if (ctx->x_tma) {
+    if constexpr (FxTma<P, N, true>::OK) {
+      if (ctx->mg2l_greens_direct) return launch_fx_mg2l_tma<P, N, true>(ctx);
+    }
+    if constexpr (FxTma<P, N, false>::OK) return launch_fx_mg2l_tma<P, N, false>(ctx);
   }
   return ctx->mg2l_greens_direct ? launch_fx_mg2l_g<P, N, true>(ctx)
                                  : launch_fx_mg2l_g<P, N, false>(ctx);

@@ -253,7 +253,8 @@ int ct2g_batch_destroy(ct2g_batch *b);
  * tiles in flight); the same results; x_tma -- 1 (the default): the fused x
  * pass + Green's multiply brings each spectrum column in by one tiled bulk
  * tensor copy and its Green's column by one bulk copy (meshes 64-256, FP32
- * passes; mg2l_greens_direct then does not apply); 0: per-thread loads; the
+ * passes; with mg2l_greens_direct the Green's values are read by the
+ * contraction instead, and three blocks fit per SM); 0: per-thread loads; the
  * same results. */
 typedef struct {
   int dense_cell;

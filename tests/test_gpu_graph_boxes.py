@@ -160,7 +160,8 @@ def test_batch_of_meshes_matches_eager(gpu):
                                     dict(near_blocks_per_sm=1), dict(fft_tile=32),
                                     dict(fft_tile=128), dict(cols_tma=0),
                                     dict(cols_tma=1, fft_tile=16), dict(x_tma=0),
-                                    dict(x_tma=0, mg2l_greens_direct=1)])
+                                    dict(x_tma=0, mg2l_greens_direct=1),
+                                    dict(mg2l_greens_direct=1)])
 def test_tuning_keeps_results(gpu, tuning):
     P = _box(40000, 5, 64)
     a, b = _mk(64, order=4), _mk(64, order=4)
