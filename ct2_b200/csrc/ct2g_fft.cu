@@ -1612,15 +1612,21 @@ __global__ void __launch_bounds__(256, FxShape<P, N, GD>::MINB) fftx_mg2l_kernel
 // (bounded wait) while the twiddles load; GD: the contraction reads the
 // Green's values from HBM, and the smaller block (no Green's column, no
 // static shared memory, so the dynamic region starts 128-byte aligned) fits
-// three to an SM.  The transforms run in place in the copied tile; the
-// inverse's last step writes the column back from registers (a tensor store
-// would also write the neighbouring column's element that the tile carries,
-// which another block owns).
-template <int P, int N, bool GD>
+// three to an SM.  CPA: the column arrives instead by per-thread 8-byte
+// cp.async copies, all in flight at once, into rows NC complex apart: the
+// tensor copy's rows are a 16-byte multiple apart (36 complex at order 4),
+// which puts the rows that the contraction's threads read (a k-point each,
+// all NC components) into only four bank groups (an 8-way conflict on every
+// component); NC apart (odd at order 4) they spread over all banks.  The
+// transforms run in place in the copied tile; the inverse's last step
+// writes the column back from registers (a tensor store would also write the
+// neighbouring column's element that the tile carries, which another block
+// owns).
+template <int P, int N, bool GD, bool CPA = false>
 struct FxTma {
   static constexpr int NC = ct2g_ncomp(P), NH = N / 2 + 1;
-  static constexpr int BW = (2 * NC + 3) / 4 * 4;  // floats per tile row (16-byte multiple)
-  static constexpr int PITCH = BW / 2;             // complex per tile row
+  static constexpr int BW = (2 * NC + 3) / 4 * 4;    // floats per tensor-copy row (16-byte multiple)
+  static constexpr int PITCH = CPA ? NC : BW / 2;    // complex per tile row
   static constexpr int GCOL = NC * N;
   // GD: tile, twiddles, the mbarrier; else 128 bytes of alignment slack,
   // tile, Green's column, twiddles, the mbarrier
@@ -1635,11 +1641,11 @@ struct FxTma {
                                                                               : 1;
 };
 
-template <int P, int N, bool GD>
-__global__ void __launch_bounds__(256, FxTma<P, N, GD>::MINB) fftx_mg2l_tma_kernel(
+template <int P, int N, bool GD, bool CPA>
+__global__ void __launch_bounds__(256, FxTma<P, N, GD, CPA>::MINB) fftx_mg2l_tma_kernel(
     const __grid_constant__ CUtensorMap xmap, float2 *__restrict__ spec, int ldk,
     const float *__restrict__ gx, const float2 *__restrict__ tw, uint32_t *__restrict__ status) {
-  using S = FxTma<P, N, GD>;
+  using S = FxTma<P, N, GD, CPA>;
   constexpr int NC = S::NC, NH = S::NH, PITCH = S::PITCH;
   // the tensor copy needs a 128-byte aligned destination
   extern __shared__ __align__(128) unsigned char smraw[];
@@ -1652,21 +1658,32 @@ __global__ void __launch_bounds__(256, FxTma<P, N, GD>::MINB) fftx_mg2l_tma_kern
   const int qj = (int)((blockIdx.x / NH) % N);
   const int box = (int)(blockIdx.x / ((unsigned)NH * N));
   const int64_t RS = (int64_t)ldk * NC, XS = (int64_t)N * RS;
-  const int f0 = 2 * qk * NC, x0 = f0 & ~3, off = (f0 - x0) / 2;
+  const int f0 = 2 * qk * NC, x0 = f0 & ~3, off = CPA ? 0 : (f0 - x0) / 2;
   const float *gcol = gx + ((int64_t)qj * NH + qk) * S::GCOL;
-  if (tc::smem_addr(s) & 127u) {  // checked before any copy
+  float2 *col = spec + (int64_t)box * N * XS + (int64_t)qj * RS + (int64_t)qk * NC;
+  if (!CPA && (tc::smem_addr(s) & 127u)) {  // checked before any tensor copy
     if (threadIdx.x == 0) atomicExch(status, (uint32_t)CT2G_ECUDA);
     return;
   }
   if (threadIdx.x == 0) tc::mbar_init(bar, 1);
   __syncthreads();  // the barrier is initialised before any thread polls it
   if (threadIdx.x == 0) {
-    tc::mbar_arrive_expect_tx(
-        bar, (uint32_t)(sizeof(float2) * N * PITCH + (GD ? 0 : sizeof(float) * S::GCOL)));
-    tc::tma_load_4d(s, &xmap, x0, qj, 0, box, bar);
+    tc::mbar_arrive_expect_tx(bar, (uint32_t)((CPA ? 0 : sizeof(float2) * N * PITCH) +
+                                              (GD ? 0 : sizeof(float) * S::GCOL)));
+    if constexpr (!CPA) tc::tma_load_4d(s, &xmap, x0, qj, 0, box, bar);
     if constexpr (!GD) tc::bulk_load(sg, gcol, (uint32_t)(sizeof(float) * S::GCOL), bar);
   }
+  if constexpr (CPA) {
+    for (int e = threadIdx.x; e < N * NC; e += 256) {
+      const int r = e / NC, l = e - r * NC;
+      const unsigned sa = tc::smem_addr(s + e);
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(col + r * XS + l)
+                   : "memory");
+    }
+    cp_async_commit();
+  }
   load_twiddles(stw, tw, N);
+  if constexpr (CPA) cp_async_wait<0>();
   const bool ok = tc::mbar_wait(bar, 0, kTmaWaitLimit);
   if (!__syncthreads_and(ok)) {
     if (threadIdx.x == 0) {
@@ -1700,7 +1717,6 @@ __global__ void __launch_bounds__(256, FxTma<P, N, GD>::MINB) fftx_mg2l_tma_kern
   }
   __syncthreads();
   // inverse: the second step writes the column back to HBM
-  float2 *col = spec + (int64_t)box * N * XS + (int64_t)qj * RS + (int64_t)qk * NC;
   cols_step1<N, NC, true, 256, PITCH>(
       s, stw, [&](int l, int r) { return s[r * PITCH + off + l]; }, off);
   __syncthreads();
@@ -1745,15 +1761,15 @@ int xmap_build(ct2g_ctx *ctx, int BW) {
   return CT2G_OK;
 }
 
-template <int P, int N, bool GD>
+template <int P, int N, bool GD, bool CPA>
 int launch_fx_mg2l_tma(ct2g_ctx *ctx) {
-  using S = FxTma<P, N, GD>;
+  using S = FxTma<P, N, GD, CPA>;
   if constexpr (!S::OK) {
     return ct2g_fail(ctx, CT2G_EINVAL, "TMA x pass: meshes 64-256");
   } else {
     CT2G_TRY(xmap_build(ctx, S::BW));
     const size_t ncol = (size_t)ctx->nbox * N * S::NH;
-    auto k = fftx_mg2l_tma_kernel<P, N, GD>;
+    auto k = fftx_mg2l_tma_kernel<P, N, GD, CPA>;
     CT2G_TRY(ct2g_smem_attrs(ctx, k, S::SMEM));
     const CUtensorMap *m = reinterpret_cast<const CUtensorMap *>(ctx->xmap);
     k<<<(unsigned)ncol, 256, S::SMEM, ctx->stream>>>(*m, ctx->spec, ctx->ldk, ctx->greens_x,
@@ -1765,11 +1781,17 @@ int launch_fx_mg2l_tma(ct2g_ctx *ctx) {
 
 template <int P, int N>
 int launch_fx_mg2l(ct2g_ctx *ctx) {
-  if (ctx->x_tma) {
+  if (ctx->x_tma == 1) {
     if constexpr (FxTma<P, N, true>::OK) {
-      if (ctx->mg2l_greens_direct) return launch_fx_mg2l_tma<P, N, true>(ctx);
+      if (ctx->mg2l_greens_direct) return launch_fx_mg2l_tma<P, N, true, false>(ctx);
     }
-    if constexpr (FxTma<P, N, false>::OK) return launch_fx_mg2l_tma<P, N, false>(ctx);
+    if constexpr (FxTma<P, N, false>::OK) return launch_fx_mg2l_tma<P, N, false, false>(ctx);
+  }
+  if (ctx->x_tma == 2) {
+    if constexpr (FxTma<P, N, true, true>::OK) {
+      if (ctx->mg2l_greens_direct) return launch_fx_mg2l_tma<P, N, true, true>(ctx);
+    }
+    if constexpr (FxTma<P, N, false, true>::OK) return launch_fx_mg2l_tma<P, N, false, true>(ctx);
   }
   return ctx->mg2l_greens_direct ? launch_fx_mg2l_g<P, N, true>(ctx)
                                  : launch_fx_mg2l_g<P, N, false>(ctx);

@@ -358,7 +358,7 @@ int ct2g_set_tuning(ct2g_ctx *ctx, const ct2g_tuning *t) {
       (t->mg2l_greens_direct != 0 && t->mg2l_greens_direct != 1) ||
       t->near_chunks_per_warp < 0 || t->near_chunks_per_warp > 4096 || t->plane_pipe < 0 ||
       t->plane_pipe > 16 || (t->cols_tma != 0 && t->cols_tma != 1) ||
-      (t->x_tma != 0 && t->x_tma != 1))
+      t->x_tma < 0 || t->x_tma > 2)
     return ct2g_fail(ctx, CT2G_EINVAL, "tuning out of range");
   ctx->dense_cell = (uint32_t)t->dense_cell;
   ctx->near_blocks_per_sm = t->near_blocks_per_sm;
@@ -434,7 +434,7 @@ int ct2g_autotune(ct2g_ctx *ctx, const ct2g_kick_params *p, float dt, float scal
       {0, 4, 16, 64},           // near_chunks_per_warp (with overlap)
       {0, 8},                   // plane_pipe
       ctx->M >= 64 && ctx->M <= 256 ? std::vector<int>{0, 1} : std::vector<int>{0},   // cols_tma
-      ctx->M >= 64 && ctx->M <= 256 ? std::vector<int>{0, 1} : std::vector<int>{0}};  // x_tma
+      ctx->M >= 64 && ctx->M <= 256 ? std::vector<int>{0, 1, 2} : std::vector<int>{0}};  // x_tma
   // the overlap and the mesh solve's form first, then how the near field
   // shares the SMs with the mesh solve: they change which near-field
   // footprint is best

@@ -269,7 +269,8 @@ struct ct2g_ctx {
   // tensor map of the spectrum's y-pass tiles (a CUtensorMap, built once)
   alignas(64) unsigned char ymap[128] = {};
   int ymap_w = 0;              // tile width the map was built for (0: none)
-  int x_tma = 1;               // 1: the fused x pass's inputs arrive by bulk copies
+  int x_tma = 2;               // fused x pass inputs: 1 tensor + bulk copies, 2 cp.async
+                               // column + bulk Green's copy, 0 per-thread loads
   // tensor map of the spectrum's x-pass columns (a CUtensorMap, built once)
   alignas(64) unsigned char xmap[128] = {};
   int xmap_bw = 0;             // box width (floats) the map was built for (0: none)

@@ -309,7 +309,7 @@ class Gravity:
 
     def set_tuning(self, dense_cell=16, near_blocks_per_sm=0, fft_tile=0, split_mg2l=0,
                    sparse_path=2, overlap=0, mg2l_greens_direct=0, near_chunks_per_warp=0,
-                   plane_pipe=0, cols_tma=1, x_tma=1):
+                   plane_pipe=0, cols_tma=1, x_tma=2):
         t = Tuning(dense_cell, near_blocks_per_sm, fft_tile, split_mg2l, sparse_path, overlap,
                    mg2l_greens_direct, near_chunks_per_warp, plane_pipe, cols_tma, x_tma)
         self._chk(self._l.ct2g_set_tuning(self._h, ctypes.byref(t)))

@@ -254,8 +254,11 @@ int ct2g_batch_destroy(ct2g_batch *b);
  * pass + Green's multiply brings each spectrum column in by one tiled bulk
  * tensor copy and its Green's column by one bulk copy (meshes 64-256, FP32
  * passes; with mg2l_greens_direct the Green's values are read by the
- * contraction instead, and three blocks fit per SM); 0: per-thread loads; the
- * same results. */
+ * contraction instead, and three blocks fit per SM); 2: the column by
+ * per-thread cp.async copies, all in flight at once, into rows NC complex
+ * apart (the tensor copy's 16-byte-multiple rows put the contraction's
+ * shared-memory reads into a few banks); 0: per-thread loads inside the
+ * first transform step; the same results. */
 typedef struct {
   int dense_cell;
   int near_blocks_per_sm;

@@ -161,7 +161,8 @@ def test_batch_of_meshes_matches_eager(gpu):
                                     dict(fft_tile=128), dict(cols_tma=0),
                                     dict(cols_tma=1, fft_tile=16), dict(x_tma=0),
                                     dict(x_tma=0, mg2l_greens_direct=1),
-                                    dict(mg2l_greens_direct=1)])
+                                    dict(mg2l_greens_direct=1), dict(x_tma=2),
+                                    dict(x_tma=2, mg2l_greens_direct=1)])
 def test_tuning_keeps_results(gpu, tuning):
     P = _box(40000, 5, 64)
     a, b = _mk(64, order=4), _mk(64, order=4)
