@@ -250,12 +250,12 @@ int ct2g_batch_destroy(ct2g_batch *b);
  * columns; 16 with fft_tile 16) by one tiled bulk tensor copy (TMA) in and
  * one out, three tiles in flight per block (meshes 64-256, FP32 passes; the
  * default); 0: every thread copies its share of each tile (cp.async, two
- * tiles in flight); the same results; x_tma -- 1 (the default): the fused x
+ * tiles in flight); the same results; x_tma -- 1: the fused x
  * pass + Green's multiply brings each spectrum column in by one tiled bulk
  * tensor copy and its Green's column by one bulk copy (meshes 64-256, FP32
  * passes; with mg2l_greens_direct the Green's values are read by the
- * contraction instead, and three blocks fit per SM); 2: the column by
- * per-thread cp.async copies, all in flight at once, into rows NC complex
+ * contraction instead, and three blocks fit per SM); 2 (the default): the
+ * column by per-thread cp.async copies, all in flight at once, into rows NC complex
  * apart (the tensor copy's 16-byte-multiple rows put the contraction's
  * shared-memory reads into a few banks); 0: per-thread loads inside the
  * first transform step; the same results. */
