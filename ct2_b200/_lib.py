@@ -30,7 +30,7 @@ class Tuning(ctypes.Structure):
                 ("sparse_path", ctypes.c_int), ("overlap", ctypes.c_int),
                 ("mg2l_greens_direct", ctypes.c_int), ("near_chunks_per_warp", ctypes.c_int),
                 ("plane_pipe", ctypes.c_int), ("cols_tma", ctypes.c_int),
-                ("x_tma", ctypes.c_int)]
+                ("x_tma", ctypes.c_int), ("p2m_compact", ctypes.c_int)]
 
 
 STEP_GRAPH = 1

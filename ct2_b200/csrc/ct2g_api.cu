@@ -78,7 +78,7 @@ void free_particles(ct2g_ctx *ctx) {
                   ctx->keys, ctx->keys2, ctx->vals, ctx->vals2, ctx->hist, ctx->src,
                   ctx->chunks, ctx->sparse_list, ctx->flags, ctx->fx,
                   ctx->fy, ctx->fz,
-                  ctx->pot, ctx->nfx, ctx->nfy, ctx->nfz, ctx->npot};
+                  ctx->pot, ctx->nfx, ctx->nfy, ctx->nfz, ctx->npot, ctx->cmom, ctx->p2m_big};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   ctx->x = ctx->y = ctx->z = ctx->id = nullptr;
@@ -93,6 +93,8 @@ void free_particles(ct2g_ctx *ctx) {
   ctx->sparse_list = ctx->flags = nullptr;
   ctx->fx = ctx->fy = ctx->fz = ctx->pot = nullptr;
   ctx->nfx = ctx->nfy = ctx->nfz = ctx->npot = nullptr;
+  ctx->cmom = nullptr;
+  ctx->p2m_big = nullptr;
   ctx->cap = 0;
 }
 
@@ -116,6 +118,23 @@ void ct2g_mark(ct2g_ctx *ctx, int k) {
 }
 
 int ct2g_check(ct2g_ctx *ctx) { return check(ctx); }
+
+// compact P2M records for the particle capacity: NC floats per occupied
+// cell (at most one cell per particle) and the big-cell list (count first;
+// a big cell holds more than 6 particles, so at most cap / 7 of them)
+int ct2g_alloc_p2m_compact(ct2g_ctx *ctx) {
+  if (ctx->cmom || ctx->cap == 0) return CT2G_OK;
+  if (ctx->capturing) return ct2g_fail(ctx, CT2G_ESTATE, "compact P2M records not allocated before recording");
+  CT2G_CUDA(ctx, cudaMalloc(&ctx->cmom, sizeof(float) * ctx->nc * ctx->cap));
+  cudaError_t e = cudaMalloc(&ctx->p2m_big, sizeof(uint32_t) * (ctx->cap / 7 + 2));
+  if (e != cudaSuccess) {
+    cudaFree(ctx->cmom);
+    ctx->cmom = nullptr;
+    return ct2g_cuda_fail(ctx, e, "compact P2M big-cell list");
+  }
+  ctx->epoch++;
+  return CT2G_OK;
+}
 
 // resident blocks per SM of a kernel from its registers, its shared memory
 // (static + dynamic + the 1 KB the system reserves per block) against the
@@ -224,6 +243,7 @@ int ct2g_alloc_particles(ct2g_ctx *ctx, size_t n) {
   A(ctx->npot, cap * 4);
 #undef A
   ctx->cap = cap;
+  if (ctx->p2m_compact) CT2G_TRY(ct2g_alloc_p2m_compact(ctx));
   // scan scratch for the largest scan of a step (radix histograms, cell
   // ranges, per-particle flags), so that no step allocates
   const size_t words = ct2g_scan_scratch_words(
@@ -250,6 +270,7 @@ int ct2g_alloc_mesh(ct2g_ctx *ctx) {
   CT2G_CUDA(ctx, cudaMalloc(&ctx->d_counts, sizeof(uint32_t) * 8));
   CT2G_CUDA(ctx, cudaMemset(ctx->d_counts, 0, sizeof(uint32_t) * 8));
   CT2G_CUDA(ctx, cudaMalloc(&ctx->pipe_sync, sizeof(uint32_t) * 2 * (2 + nb * ctx->M)));
+  CT2G_CUDA(ctx, cudaMalloc(&ctx->blk_rank, sizeof(uint32_t) * (ctx->CB / 64)));
   CT2G_CUDA(ctx, cudaMalloc(&ctx->box_off, sizeof(uint32_t) * (nb + 1)));
   CT2G_CUDA(ctx, cudaMalloc(&ctx->box_gm, sizeof(float) * nb));
   CT2G_CUDA(ctx, cudaMalloc(&ctx->greens, sizeof(float) * ctx->nc * ctx->CK));
@@ -412,7 +433,7 @@ int ct2g_destroy(ct2g_ctx *ctx) {
   ct2g_learned_free(ctx);
   void *ptrs[] = {ctx->cell_start, ctx->occ, ctx->stmask, ctx->grid, ctx->spec, ctx->greens,
                   ctx->greens_x,                  ctx->tw32, ctx->tw64, ctx->d_counts, ctx->box_off, ctx->box_gm, ctx->tc_tables,
-                  ctx->d_maxrung, ctx->d_inter, ctx->scan_tmp, ctx->pipe_sync};
+                  ctx->d_maxrung, ctx->d_inter, ctx->scan_tmp, ctx->pipe_sync, ctx->blk_rank};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);

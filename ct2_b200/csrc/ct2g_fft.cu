@@ -849,13 +849,12 @@ __device__ __forceinline__ void p2m_accumulate(const uint32_t *__restrict__ px,
 // warp: lane offset, step 32, then summed over the warp) into the packed smem
 // lines at z, for components [K0, K1): the components go in two halves so
 // that only half of the FP64 sums are live at once
-template <int P, int N, int K0, int K1>
-__device__ __forceinline__ void p2m_half(const uint32_t *__restrict__ px,
-                                         const uint32_t *__restrict__ py,
-                                         const uint32_t *__restrict__ pz, uint32_t b, uint32_t e,
-                                         uint32_t step, bool warp_sum, uint32_t ux, uint32_t uy,
-                                         uint32_t uz, int z, float *sr, bool write) {
-  using LL = LineLayout<N, true>;
+template <int P, int K0, int K1, typename ST>
+__device__ __forceinline__ void p2m_group(const uint32_t *__restrict__ px,
+                                          const uint32_t *__restrict__ py,
+                                          const uint32_t *__restrict__ pz, uint32_t b, uint32_t e,
+                                          uint32_t step, bool warp_sum, uint32_t ux, uint32_t uy,
+                                          uint32_t uz, bool write, ST st) {
   double acc[K1 - K0];
 #pragma unroll
   for (int k = 0; k < K1 - K0; k++) acc[k] = 0.0;
@@ -871,7 +870,117 @@ __device__ __forceinline__ void p2m_half(const uint32_t *__restrict__ px,
   }
   if (write) {
 #pragma unroll
-    for (int k = K0; k < K1; k++) sr[2 * LL::at(k >> 1, z, 0) + (k & 1)] = (float)acc[k - K0];
+    for (int k = K0; k < K1; k++) st(k, (float)acc[k - K0]);
+  }
+}
+
+// the same sums into the packed smem lines at z
+template <int P, int N, int K0, int K1>
+__device__ __forceinline__ void p2m_half(const uint32_t *__restrict__ px,
+                                         const uint32_t *__restrict__ py,
+                                         const uint32_t *__restrict__ pz, uint32_t b, uint32_t e,
+                                         uint32_t step, bool warp_sum, uint32_t ux, uint32_t uy,
+                                         uint32_t uz, int z, float *sr, bool write) {
+  using LL = LineLayout<N, true>;
+  p2m_group<P, K0, K1>(px, py, pz, b, e, step, warp_sum, ux, uy, uz, write,
+                       [&](int k, float v) { sr[2 * LL::at(k >> 1, z, 0) + (k & 1)] = v; });
+}
+
+// ---- P2M into compact per-cell records ---------------------------------------
+// The moments of every occupied cell (the same FP64 sums about the cell
+// centre as the fused z pass, term for term, stored FP32) as NC floats at
+// cmom + rank * NC, where rank is the cell's index among the occupied cells
+// in key order: blk_rank[block] (an exclusive scan of the occupancy words'
+// populations) plus the occupied cells before it in its 4x4x4 block's word.
+// A thread per particle of the binned range: the first particle of each
+// cell's run (in the sorted keys) sums the cell; cells of more than
+// kWarpCell particles are listed (by key) for p2m_compact_big_kernel, a warp
+// each.  The z pass then reads the records instead of summing particles, so
+// its blocks no longer wait on the slowest cell of a line.
+__device__ __forceinline__ uint32_t occ_rank(const unsigned long long *__restrict__ occ,
+                                             const uint32_t *__restrict__ blk_rank, uint32_t key,
+                                             bool &on) {
+  const unsigned long long w = occ[key >> 6];
+  on = (w >> (key & 63u)) & 1ull;
+  return blk_rank[key >> 6] + (uint32_t)__popcll(w & ((1ull << (key & 63u)) - 1ull));
+}
+
+__global__ void occ_popc_kernel(const unsigned long long *__restrict__ occ, size_t nw,
+                                uint32_t *__restrict__ out) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nw) out[i] = (uint32_t)__popcll(occ[i]);
+}
+
+// the cell coordinates of a Morton key's low 3 * mbits bits (the inverse of
+// ct2g_morton: bit 3b + 2 is x's bit b, 3b + 1 y's, 3b z's)
+__device__ __forceinline__ void demorton(uint32_t key, int mbits, uint32_t &x, uint32_t &y,
+                                         uint32_t &z) {
+  x = y = z = 0;
+  for (int b = 0; b < mbits; b++) {
+    z |= ((key >> (3 * b)) & 1u) << b;
+    y |= ((key >> (3 * b + 1)) & 1u) << b;
+    x |= ((key >> (3 * b + 2)) & 1u) << b;
+  }
+}
+
+// the moments of the cell `key` (particles b .. e) into out (a thread: step
+// 1; a warp: lanes strided, summed over the warp, lane 0 writes)
+template <int P>
+__device__ __forceinline__ void p2m_cell(const uint32_t *__restrict__ px,
+                                         const uint32_t *__restrict__ py,
+                                         const uint32_t *__restrict__ pz, uint32_t key, int mbits,
+                                         uint32_t b, uint32_t e, bool warp, int lane,
+                                         float *out) {
+  constexpr int NC = ct2g_ncomp(P);
+  uint32_t cx, cy, cz;
+  demorton(key, mbits, cx, cy, cz);
+  const int sh = 32 - mbits;
+  const uint32_t halfc = 1u << (sh - 1);
+  const uint32_t ux = (cx << sh) + halfc, uy = (cy << sh) + halfc, uz = (cz << sh) + halfc;
+  const uint32_t b0 = warp ? b + (uint32_t)lane : b, step = warp ? 32u : 1u;
+  const bool write = !warp || lane == 0;
+  auto st = [&](int k, float v) { out[k] = v; };
+  p2m_group<P, 0, NC / 3>(px, py, pz, b0, e, step, warp, ux, uy, uz, write, st);
+  p2m_group<P, NC / 3, 2 * NC / 3>(px, py, pz, b0, e, step, warp, ux, uy, uz, write, st);
+  p2m_group<P, 2 * NC / 3, NC>(px, py, pz, b0, e, step, warp, ux, uy, uz, write, st);
+}
+
+// a thread per particle j of the range (absolute index rbegin + j, key
+// skeys[j]); the first of its cell's run sums the cell
+template <int P>
+__global__ void __launch_bounds__(256) p2m_compact_kernel(
+    const uint32_t *__restrict__ px, const uint32_t *__restrict__ py,
+    const uint32_t *__restrict__ pz, const uint32_t *__restrict__ cs,
+    const unsigned long long *__restrict__ occ, const uint32_t *__restrict__ blk_rank, int mbits,
+    const uint32_t *__restrict__ skeys, uint32_t rbegin, uint32_t nr, float *__restrict__ cmom,
+    uint32_t *__restrict__ big) {
+  const uint32_t j = blockIdx.x * 256 + threadIdx.x;
+  if (j >= nr) return;
+  const uint32_t key = skeys[j];
+  if (j > 0 && skeys[j - 1] == key) return;  // not the first of its cell
+  const uint32_t b = rbegin + j, e = cs[key + 1];
+  if (e - b > kWarpCell) {
+    big[1 + atomicAdd(big, 1u)] = key;
+    return;
+  }
+  bool on;
+  float *out = cmom + (size_t)occ_rank(occ, blk_rank, key, on) * ct2g_ncomp(P);
+  p2m_cell<P>(px, py, pz, key, mbits, b, e, false, 0, out);
+}
+
+template <int P>
+__global__ void __launch_bounds__(256) p2m_compact_big_kernel(
+    const uint32_t *__restrict__ px, const uint32_t *__restrict__ py,
+    const uint32_t *__restrict__ pz, const uint32_t *__restrict__ cs,
+    const unsigned long long *__restrict__ occ, const uint32_t *__restrict__ blk_rank, int mbits,
+    float *__restrict__ cmom, const uint32_t *__restrict__ big) {
+  const uint32_t nbig = big[0];
+  const int lane = threadIdx.x & 31;
+  for (uint32_t q = (blockIdx.x * 256 + threadIdx.x) >> 5; q < nbig; q += gridDim.x * 8) {
+    const uint32_t key = big[1 + q];
+    bool on;
+    float *out = cmom + (size_t)occ_rank(occ, blk_rank, key, on) * ct2g_ncomp(P);
+    p2m_cell<P>(px, py, pz, key, mbits, cs[key], cs[key + 1], true, lane, out);
   }
 }
 
@@ -924,6 +1033,37 @@ __device__ __forceinline__ void p2m_line(const uint32_t *__restrict__ px,
   __syncthreads();
 }
 
+// The moments of the N cells of line `line` of box `box` from the compact
+// per-cell records (zeros for empty cells) into the packed smem lines sr.
+// Ends with the block synchronised.
+template <int P, int N>
+__device__ __forceinline__ void cmom_line(const float *__restrict__ cmom,
+                                          const unsigned long long *__restrict__ occ,
+                                          const uint32_t *__restrict__ blk_rank, int mbits,
+                                          uint32_t box, size_t line, float *sr) {
+  using LL = LineLayout<N, true>;
+  constexpr int NC = ct2g_ncomp(P), NL = (NC + 1) / 2;
+  const uint32_t cx = (uint32_t)(line / N), cy = (uint32_t)(line % N);
+  for (int zc = threadIdx.x; zc < N; zc += 256) {
+    const uint32_t key = (box << (3 * mbits)) | ct2g_morton(cx, cy, (uint32_t)zc);
+    bool on;
+    const uint32_t rank = occ_rank(occ, blk_rank, key, on);
+    float v[NC];
+    if (on) {
+      const float *m = cmom + (size_t)rank * NC;
+#pragma unroll
+      for (int k = 0; k < NC; k++) v[k] = __ldg(m + k);
+    } else {
+#pragma unroll
+      for (int k = 0; k < NC; k++) v[k] = 0.f;
+    }
+#pragma unroll
+    for (int k = 0; k < NC; k++) sr[2 * LL::at(k >> 1, zc, 0) + (k & 1)] = v[k];
+    if (NC & 1) sr[2 * LL::at(NL - 1, zc, 0) + 1] = 0.f;
+  }
+  __syncthreads();
+}
+
 // The transformed packed lines of LB mesh lines, split into the half spectra
 // of their two components, written as LB spectrum rows from `rows` on (row
 // lb at rows + lb * ldk * NC; k-point k's components at k * NC; the slots
@@ -957,7 +1097,8 @@ __global__ void __launch_bounds__(256, N >= 512 ? 2 : P <= 4 ? 4 : 2) fftz_p2m_r
     const uint32_t *__restrict__ px, const uint32_t *__restrict__ py,
     const uint32_t *__restrict__ pz, const uint32_t *__restrict__ cs, int mbits,
     float *__restrict__ grid, int64_t CB, float2 *__restrict__ spec, int ldk,
-    const float2 *__restrict__ tw) {
+    const float2 *__restrict__ tw, const float *__restrict__ cmom,
+    const unsigned long long *__restrict__ occ, const uint32_t *__restrict__ blk_rank) {
   using LL = LineLayout<N, true>;
   constexpr int NC = ct2g_ncomp(P), NL = (NC + 1) / 2, NH = N / 2 + 1;
   constexpr bool GRID = SRC == CT2G_P2M_GRID;
@@ -984,6 +1125,8 @@ __global__ void __launch_bounds__(256, N >= 512 ? 2 : P <= 4 ? 4 : 2) fftz_p2m_r
     if (NC & 1)
       for (int e = threadIdx.x; e < LB * N; e += 256)
         sr[2 * LL::at((e / N) * NL + NL - 1, e % N, 0) + 1] = 0.f;
+  } else if constexpr (SRC == CT2G_P2M_COMPACT) {
+    cmom_line<P, N>(cmom, occ, blk_rank, mbits, box, line, sr);
   } else {
     p2m_line<P, N>(px, py, pz, cs, mbits, box, line, sr, big, nbig);
   }
@@ -1001,18 +1144,42 @@ __global__ void __launch_bounds__(256, N >= 512 ? 2 : P <= 4 ? 4 : 2) fftz_p2m_r
   store_half_spectra<P, N, LB>(s, spec + (int64_t)L0 * ldk * NC, ldk);
 }
 
+// the compact per-cell moment records of the current binning: the occupied
+// cells' ranks, then a thread per small cell and a warp per listed big cell
+template <int P>
+int launch_p2m_compact(ct2g_ctx *ctx) {
+  const size_t nw = (size_t)ctx->CB / 64;
+  occ_popc_kernel<<<ct2g_div_up(nw, 256), 256, 0, ctx->stream>>>(ctx->occ, nw, ctx->blk_rank);
+  CT2G_LAUNCHED(ctx);
+  CT2G_TRY(ct2g_scan_exclusive(ctx, ctx->blk_rank, ctx->blk_rank, nw, nullptr, 0));
+  CT2G_CUDA(ctx, cudaMemsetAsync(ctx->p2m_big, 0, sizeof(uint32_t), ctx->stream));
+  const size_t nr = ctx->n - ctx->rung_begin;  // the binned range, as ct2g_bin_range sorted it
+  p2m_compact_kernel<P><<<(unsigned)std::max<size_t>(1, ct2g_div_up(nr, 256)), 256, 0,
+                          ctx->stream>>>(ctx->x, ctx->y, ctx->z, ctx->cell_start, ctx->occ,
+                                         ctx->blk_rank, ctx->mbits, ctx->keys,
+                                         (uint32_t)ctx->rung_begin, (uint32_t)nr, ctx->cmom,
+                                         ctx->p2m_big);
+  CT2G_LAUNCHED(ctx);
+  p2m_compact_big_kernel<P><<<(unsigned)(4 * ctx->num_sms), 256, 0, ctx->stream>>>(
+      ctx->x, ctx->y, ctx->z, ctx->cell_start, ctx->occ, ctx->blk_rank, ctx->mbits, ctx->cmom,
+      ctx->p2m_big);
+  CT2G_LAUNCHED(ctx);
+  return CT2G_OK;
+}
+
 template <int P, int N>
 int launch_p2m_r2c(ct2g_ctx *ctx, int src) {
   constexpr int NL = (ct2g_ncomp(P) + 1) / 2;
   const int LB = src == CT2G_P2M_GRID ? z_lines<P>() : 1;
   const size_t smem = sizeof(float2) * ((size_t)N + (size_t)LB * NL * LineLayout<N, true>::LS);
-  auto k = src == CT2G_P2M_GRID    ? fftz_p2m_r2c_kernel<P, N, CT2G_P2M_GRID>
-           : src == CT2G_P2M_FUSED ? fftz_p2m_r2c_kernel<P, N, CT2G_P2M_FUSED>
-                                   : fftz_p2m_r2c_kernel<P, N, CT2G_P2M_FUSED_STORE>;
+  auto k = src == CT2G_P2M_GRID      ? fftz_p2m_r2c_kernel<P, N, CT2G_P2M_GRID>
+           : src == CT2G_P2M_FUSED   ? fftz_p2m_r2c_kernel<P, N, CT2G_P2M_FUSED>
+           : src == CT2G_P2M_COMPACT ? fftz_p2m_r2c_kernel<P, N, CT2G_P2M_COMPACT>
+                                     : fftz_p2m_r2c_kernel<P, N, CT2G_P2M_FUSED_STORE>;
   CT2G_TRY(ct2g_smem_attrs(ctx, k, smem));
   k<<<(unsigned)((size_t)N * N * ctx->nbox / LB), 256, smem, ctx->stream>>>(
       ctx->x, ctx->y, ctx->z, ctx->cell_start, ctx->mbits, ctx->grid, ctx->CB, ctx->spec,
-      ctx->ldk, twiddle_ptr<float2>(ctx));
+      ctx->ldk, twiddle_ptr<float2>(ctx), ctx->cmom, ctx->occ, ctx->blk_rank);
   CT2G_LAUNCHED(ctx);
   return CT2G_OK;
 }
@@ -1846,6 +2013,8 @@ int spec_stage(ct2g_ctx *ctx, int stage, bool flag, int mode) {
   switch (ctx->M) {
 #define CT2G_SPEC_CASE(NN)                                                  \
   case NN:                                                                  \
+    if (stage == 0 && mode == CT2G_P2M_COMPACT)                             \
+      CT2G_TRY(launch_p2m_compact<P>(ctx));                                 \
     if (stage == 0) return launch_p2m_r2c<P, NN>(ctx, mode);                \
     if (stage == 1) return launch_fx_mg2l<P, NN>(ctx);                      \
     if (stage == 2) return launch_c2r_l2p<P, NN>(ctx, mode);                \
@@ -1984,6 +2153,8 @@ int ct2g_spec_forward(ct2g_ctx *ctx, int src) {
   bool piped = false;
   CT2G_TRY(spec_pipe(ctx, false, src, &piped));
   if (!piped) {
+    // P2M into compact per-cell records first, read by the z pass
+    if (src == CT2G_P2M_FUSED && ctx->p2m_compact && ctx->cmom) src = CT2G_P2M_COMPACT;
     CT2G_TRY(spec_run(ctx, 0, false, src));
     CT2G_TRY(spec_run(ctx, 3, false, 0));
   }

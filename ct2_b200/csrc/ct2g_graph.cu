@@ -346,6 +346,7 @@ int ct2g_get_tuning(const ct2g_ctx *ctx, ct2g_tuning *t) {
   t->plane_pipe = ctx->plane_pipe;
   t->cols_tma = ctx->cols_tma;
   t->x_tma = ctx->x_tma;
+  t->p2m_compact = ctx->p2m_compact;
   return CT2G_OK;
 }
 
@@ -358,7 +359,7 @@ int ct2g_set_tuning(ct2g_ctx *ctx, const ct2g_tuning *t) {
       (t->mg2l_greens_direct != 0 && t->mg2l_greens_direct != 1) ||
       t->near_chunks_per_warp < 0 || t->near_chunks_per_warp > 4096 || t->plane_pipe < 0 ||
       t->plane_pipe > 16 || (t->cols_tma != 0 && t->cols_tma != 1) ||
-      t->x_tma < 0 || t->x_tma > 2)
+      t->x_tma < 0 || t->x_tma > 2 || (t->p2m_compact != 0 && t->p2m_compact != 1))
     return ct2g_fail(ctx, CT2G_EINVAL, "tuning out of range");
   ctx->dense_cell = (uint32_t)t->dense_cell;
   ctx->near_blocks_per_sm = t->near_blocks_per_sm;
@@ -371,6 +372,8 @@ int ct2g_set_tuning(ct2g_ctx *ctx, const ct2g_tuning *t) {
   ctx->plane_pipe = t->plane_pipe;
   ctx->cols_tma = t->cols_tma;
   ctx->x_tma = t->x_tma;
+  ctx->p2m_compact = t->p2m_compact;
+  if (ctx->p2m_compact) CT2G_TRY(ct2g_alloc_p2m_compact(ctx));
   ctx->epoch++;  // launch shapes are part of a recorded graph
   ctx->grid_valid = false;  // the chunk lists depend on dense_cell
   return CT2G_OK;
@@ -394,7 +397,7 @@ int ct2g_autotune(ct2g_ctx *ctx, const ct2g_kick_params *p, float dt, float scal
       std::memset(&t, 0, sizeof(t));
       double ms = 0;
       if (ls >> k >> t.dense_cell >> t.near_blocks_per_sm >> t.fft_tile >> t.sparse_path >>
-              t.overlap >> t.mg2l_greens_direct >> t.near_chunks_per_warp >> t.plane_pipe >> t.cols_tma >> t.x_tma >> ms &&
+              t.overlap >> t.mg2l_greens_direct >> t.near_chunks_per_warp >> t.plane_pipe >> t.cols_tma >> t.x_tma >> t.p2m_compact >> ms &&
           k == key &&
           ct2g_set_tuning(ctx, &t) == CT2G_OK) {
         if (out) *out = t;
@@ -422,7 +425,7 @@ int ct2g_autotune(ct2g_ctx *ctx, const ct2g_kick_params *p, float dt, float scal
     return CT2G_OK;
   };
   if (rc == CT2G_OK) rc = time_one(best, best_ms);
-  // coordinate descent over the ten shapes
+  // coordinate descent over the eleven shapes
   const int W = ctx->M >= 256 ? 16 : 4096 / ctx->M;
   std::vector<std::vector<int>> cand = {
       {8, 12, 16, 24, 32, 48},  // dense_cell
@@ -434,16 +437,17 @@ int ct2g_autotune(ct2g_ctx *ctx, const ct2g_kick_params *p, float dt, float scal
       {0, 4, 16, 64},           // near_chunks_per_warp (with overlap)
       {0, 8},                   // plane_pipe
       ctx->M >= 64 && ctx->M <= 256 ? std::vector<int>{0, 1} : std::vector<int>{0},   // cols_tma
-      ctx->M >= 64 && ctx->M <= 256 ? std::vector<int>{0, 1, 2} : std::vector<int>{0}};  // x_tma
+      ctx->M >= 64 && ctx->M <= 256 ? std::vector<int>{0, 1, 2} : std::vector<int>{0},  // x_tma
+      {0, 1}};                  // p2m_compact
   // the overlap and the mesh solve's form first, then how the near field
   // shares the SMs with the mesh solve: they change which near-field
   // footprint is best
-  const int dims[10] = {4, 7, 8, 9, 6, 1, 0, 2, 3, 5};
+  const int dims[11] = {4, 7, 10, 8, 9, 6, 1, 0, 2, 3, 5};
   // two sweeps: a shape chosen late can change which value of an earlier
   // one is best (the second sweep re-times each dimension around the first's
   // choice; the replays' minimum keeps the comparison to within about 1%)
-  for (int di = 0; di < 20 && rc == CT2G_OK; di++) {
-    const int dim = dims[di % 10];
+  for (int di = 0; di < 22 && rc == CT2G_OK; di++) {
+    const int dim = dims[di % 11];
     for (int v : cand[dim]) {
       ct2g_tuning t = best;
       int *field = dim == 0   ? &t.dense_cell
@@ -455,7 +459,8 @@ int ct2g_autotune(ct2g_ctx *ctx, const ct2g_kick_params *p, float dt, float scal
                    : dim == 6 ? &t.near_chunks_per_warp
                    : dim == 7 ? &t.plane_pipe
                    : dim == 8 ? &t.cols_tma
-                              : &t.x_tma;
+                   : dim == 9 ? &t.x_tma
+                              : &t.p2m_compact;
       if (*field == v) continue;
       *field = v;
       float ms = 0.f;
@@ -482,7 +487,7 @@ int ct2g_autotune(ct2g_ctx *ctx, const ct2g_kick_params *p, float dt, float scal
     if (f)
       f << key << ' ' << best.dense_cell << ' ' << best.near_blocks_per_sm << ' ' << best.fft_tile
         << ' ' << best.sparse_path << ' ' << best.overlap << ' ' << best.mg2l_greens_direct << ' '
-        << best.near_chunks_per_warp << ' ' << best.plane_pipe << ' ' << best.cols_tma << ' ' << best.x_tma << ' ' << best_ms << '\n';
+        << best.near_chunks_per_warp << ' ' << best.plane_pipe << ' ' << best.cols_tma << ' ' << best.x_tma << ' ' << best.p2m_compact << ' ' << best_ms << '\n';
   }
   if (out) *out = best;
   return CT2G_OK;

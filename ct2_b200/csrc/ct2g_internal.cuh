@@ -269,6 +269,7 @@ struct ct2g_ctx {
   // tensor map of the spectrum's y-pass tiles (a CUtensorMap, built once)
   alignas(64) unsigned char ymap[128] = {};
   int ymap_w = 0;              // tile width the map was built for (0: none)
+  int p2m_compact = 0;         // 1: P2M into compact per-cell records before the z pass
   int x_tma = 2;               // fused x pass inputs: 1 tensor + bulk copies, 2 cp.async
                                // column + bulk Green's copy, 0 per-thread loads
   // tensor map of the spectrum's x-pass columns (a CUtensorMap, built once)
@@ -299,6 +300,12 @@ struct ct2g_ctx {
   // plane pipeline counters: per direction an item counter, a spare word and
   // one count per plane (nbox * mesh planes)
   uint32_t *pipe_sync = nullptr;
+  // compact P2M: per occupied cell NC floats (capacity: one cell per
+  // particle), the occupied cells' rank per 4x4x4 block, and the list of
+  // cells summed by a warp (count first)
+  float *cmom = nullptr;
+  uint32_t *blk_rank = nullptr;
+  uint32_t *p2m_big = nullptr;
   int *d_maxrung = nullptr;
   unsigned long long *d_inter = nullptr;
   uint32_t *h_pinned = nullptr;  // small pinned host scratch
@@ -370,6 +377,8 @@ size_t ct2g_scan_scratch_words(size_t n);
 void ct2g_mark(ct2g_ctx *ctx, int k);
 int ct2g_bin_range(ct2g_ctx *ctx);
 int ct2g_check(ct2g_ctx *ctx);  // valid context; selects its device
+// the compact P2M records for the particle capacity (no-op when present)
+int ct2g_alloc_p2m_compact(ct2g_ctx *ctx);
 // resident blocks per SM of `kernel` (threads, dynamic shared memory) from its
 // own registers and shared memory at the maximum carveout
 int ct2g_blocks_per_sm(ct2g_ctx *ctx, const void *kernel, int threads, size_t dyn_smem);
@@ -410,7 +419,9 @@ int ct2g_p2m(ct2g_ctx *ctx);
 // CT2G_P2M_FUSED computed inside the pass, not stored (ctx->grid then holds
 //   no moments);
 // CT2G_P2M_FUSED_STORE computed inside the pass and also written to the grid
-enum { CT2G_P2M_GRID = 0, CT2G_P2M_FUSED = 1, CT2G_P2M_FUSED_STORE = 2 };
+// CT2G_P2M_COMPACT computed by a cell-parallel pass into compact per-cell
+// records (ctx->cmom) that the z pass reads (tuning p2m_compact)
+enum { CT2G_P2M_GRID = 0, CT2G_P2M_FUSED = 1, CT2G_P2M_FUSED_STORE = 2, CT2G_P2M_COMPACT = 3 };
 int ct2g_mesh_solve(ct2g_ctx *ctx, bool fused_l2p, bool pot, int p2m = CT2G_P2M_GRID);
 // Mesh-solve transforms on ctx->spec (ct2g_fft.cu).  Forward: the z pass
 // (taking the moments as src says, CT2G_P2M_*), the Y pass, and the X pass

@@ -305,13 +305,14 @@ class Gravity:
                     fft_tile=t.fft_tile, split_mg2l=t.split_mg2l, sparse_path=t.sparse_path,
                     overlap=t.overlap, mg2l_greens_direct=t.mg2l_greens_direct,
                     near_chunks_per_warp=t.near_chunks_per_warp, plane_pipe=t.plane_pipe,
-                    cols_tma=t.cols_tma, x_tma=t.x_tma)
+                    cols_tma=t.cols_tma, x_tma=t.x_tma, p2m_compact=t.p2m_compact)
 
     def set_tuning(self, dense_cell=16, near_blocks_per_sm=0, fft_tile=0, split_mg2l=0,
                    sparse_path=2, overlap=0, mg2l_greens_direct=0, near_chunks_per_warp=0,
-                   plane_pipe=0, cols_tma=1, x_tma=2):
+                   plane_pipe=0, cols_tma=1, x_tma=2, p2m_compact=0):
         t = Tuning(dense_cell, near_blocks_per_sm, fft_tile, split_mg2l, sparse_path, overlap,
-                   mg2l_greens_direct, near_chunks_per_warp, plane_pipe, cols_tma, x_tma)
+                   mg2l_greens_direct, near_chunks_per_warp, plane_pipe, cols_tma, x_tma,
+                   p2m_compact)
         self._chk(self._l.ct2g_set_tuning(self._h, ctypes.byref(t)))
 
     def autotune(self, params: kick_params, dt: float, scale: float = 1.0, cache_path=None):
@@ -323,7 +324,7 @@ class Gravity:
                     fft_tile=t.fft_tile, split_mg2l=t.split_mg2l, sparse_path=t.sparse_path,
                     overlap=t.overlap, mg2l_greens_direct=t.mg2l_greens_direct,
                     near_chunks_per_warp=t.near_chunks_per_warp, plane_pipe=t.plane_pipe,
-                    cols_tma=t.cols_tma, x_tma=t.x_tma)
+                    cols_tma=t.cols_tma, x_tma=t.x_tma, p2m_compact=t.p2m_compact)
 
     def kick_step(self, minrung, max_rung, scale, adot, tau, t0, minrung0, nocrop=False):
         """Returns (value, minrung): the reference's return value, which is its

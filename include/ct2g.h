@@ -258,7 +258,13 @@ int ct2g_batch_destroy(ct2g_batch *b);
  * column by per-thread cp.async copies, all in flight at once, into rows NC complex
  * apart (the tensor copy's 16-byte-multiple rows put the contraction's
  * shared-memory reads into a few banks); 0: per-thread loads inside the
- * first transform step; the same results. */
+ * first transform step; the same results; p2m_compact -- 1: the cells'
+ * multipole moments are summed by a cell-parallel pass (the thread of a
+ * cell's first particle, a warp per cell of more than 6 particles) into
+ * compact records
+ * of the occupied cells (capacity: NC floats per particle), which the
+ * forward z pass then reads; 0 (the default): the z pass sums them itself,
+ * a line's cells at a time; the same results. */
 typedef struct {
   int dense_cell;
   int near_blocks_per_sm;
@@ -271,6 +277,7 @@ typedef struct {
   int plane_pipe;
   int cols_tma;
   int x_tma;
+  int p2m_compact;
 } ct2g_tuning;
 int ct2g_get_tuning(const ct2g_ctx *ctx, ct2g_tuning *t);
 int ct2g_set_tuning(ct2g_ctx *ctx, const ct2g_tuning *t);
@@ -278,7 +285,8 @@ int ct2g_set_tuning(ct2g_ctx *ctx, const ct2g_tuning *t);
  * particles for candidate tunings, keeps the fastest and restores the
  * particles afterwards.  cache_path (may be NULL): a text file of
  * "key dense_cell near_blocks_per_sm fft_tile sparse_path overlap
- * mg2l_greens_direct near_chunks_per_warp plane_pipe cols_tma x_tma ms" lines; a hit for this
+ * mg2l_greens_direct near_chunks_per_warp plane_pipe cols_tma x_tma p2m_compact ms"
+ * lines; a hit for this
  * context's key (mesh, order, bwidth, boxes, particle-count octave) is used
  * without timing, a miss is appended.  *out (may be NULL) gets the choice. */
 int ct2g_autotune(ct2g_ctx *ctx, const ct2g_kick_params *p, float dt, float scale,

@@ -7,8 +7,9 @@ bit-identical to the eager single-box path on the same particles:
     does (the box index sits above the Morton key of a stable sort), runs the
     same per-grid FFT and the same per-sink near-field sequence;
   * FFT tile widths, the y and x passes' transport (TMA or per-thread
-    copies) and the near-field grid size change which block does the work,
-    not its arithmetic.  The sink chunking (dense_cell) moves a sink
+    copies), where the cells' moments are summed (a cell-parallel pass into
+    compact records, or inside the z pass) and the near-field grid size
+    change which block does the work, not its arithmetic.  The sink chunking (dense_cell) moves a sink
     between the dense path (sources shifted into the sink cell's frame) and
     the sparse path (the sink shifted into each source cell's frame), and
     the streamed sparse path (sparse_path 2) evaluates its sinks and sources
@@ -162,7 +163,7 @@ def test_batch_of_meshes_matches_eager(gpu):
                                     dict(cols_tma=1, fft_tile=16), dict(x_tma=0),
                                     dict(x_tma=0, mg2l_greens_direct=1),
                                     dict(mg2l_greens_direct=1), dict(x_tma=2),
-                                    dict(x_tma=2, mg2l_greens_direct=1)])
+                                    dict(x_tma=2, mg2l_greens_direct=1), dict(p2m_compact=1)])
 def test_tuning_keeps_results(gpu, tuning):
     P = _box(40000, 5, 64)
     a, b = _mk(64, order=4), _mk(64, order=4)
