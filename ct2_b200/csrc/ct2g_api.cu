@@ -265,8 +265,7 @@ int ct2g_alloc_mesh(ct2g_ctx *ctx) {
   CT2G_CUDA(ctx, cudaMalloc(&ctx->stmask, sizeof(unsigned long long) * 64 * 27));
   CT2G_CUDA(ctx, cudaMalloc(&ctx->grid, sizeof(float) * ctx->nc * nb * ctx->C));
   CT2G_CUDA(ctx, cudaMalloc(&ctx->spec, sizeof(float2) * ctx->nc * nb * ctx->CK));
-  ctx->ymap_w = 0;  // the tensor maps describe the spectrum's address
-  ctx->xmap_bw = 0;
+  ctx->xmap_bw = 0;  // the x-pass tensor map describes the spectrum's address
   CT2G_CUDA(ctx, cudaMalloc(&ctx->d_counts, sizeof(uint32_t) * 8));
   CT2G_CUDA(ctx, cudaMemset(ctx->d_counts, 0, sizeof(uint32_t) * 8));
   CT2G_CUDA(ctx, cudaMalloc(&ctx->pipe_sync, sizeof(uint32_t) * 2 * (2 + nb * ctx->M)));

@@ -490,10 +490,14 @@ __global__ void __launch_bounds__(256, 1) fft_cols_tma_kernel(
   if (tid == 0)
     for (int k = 0; k < S; k++) tc::mbar_init(&bar[k], 1);
   __syncthreads();
+  // a tensor copy's box holds at most 256 rows: N = 512 moves as two boxes
+  constexpr int NB = (N + 255) / 256, BR = N / NB;
   auto issue = [&](uint32_t t, int k) {  // thread 0
     tc::mbar_arrive_expect_tx(&bar[k], (uint32_t)(N * W * sizeof(float2)));
-    tc::tma_load_3d(buf + k * N * W, &map, (int)(2 * W * (t % ntiles)), 0, (int)(t / ntiles),
-                    &bar[k]);
+#pragma unroll
+    for (int b = 0; b < NB; b++)
+      tc::tma_load_3d(buf + k * N * W + b * BR * W, &map, (int)(2 * W * (t % ntiles)), b * BR,
+                      (int)(t / ntiles), &bar[k]);
   };
   uint32_t t = blockIdx.x;
   if (tid == 0)
@@ -520,7 +524,10 @@ __global__ void __launch_bounds__(256, 1) fft_cols_tma_kernel(
     tc::fence_async_smem();  // this thread's writes, before the bulk store reads them
     __syncthreads();
     if (tid == 0) {
-      tc::tma_store_3d(&map, (int)(2 * W * (t % ntiles)), 0, (int)(t / ntiles), s);
+#pragma unroll
+      for (int b = 0; b < NB; b++)
+        tc::tma_store_3d(&map, (int)(2 * W * (t % ntiles)), b * BR, (int)(t / ntiles),
+                         s + b * BR * W);
       tc::bulk_commit();
     }
   }
@@ -557,43 +564,47 @@ int tensor_map_encoder(ct2g_ctx *ctx, EncodeTiledFn *out) {
   return CT2G_OK;
 }
 
-// the y-pass tensor map of the context's spectrum for tiles W complex wide
-int ymap_build(ct2g_ctx *ctx, int W) {
-  if (ctx->ymap_w == W) return CT2G_OK;
+// The tensor map of a column pass over complex FP32 data: `nouter` blocks
+// (ostride complex apart) of N rows (rstride complex apart), seen as floats
+// [outer][row][2 * rstride]; a box is W complex columns x N / NB rows.
+int cols_map(ct2g_ctx *ctx, void *base, size_t nouter, size_t ostride, size_t rstride, int N,
+             int W, CUtensorMap *m) {
   EncodeTiledFn encode = nullptr;
   CT2G_TRY(tensor_map_encoder(ctx, &encode));
-  const cuuint64_t RS = (cuuint64_t)ctx->ldk * ctx->nc, N = (cuuint64_t)ctx->M;
-  const cuuint64_t dims[3] = {2 * RS, N, (cuuint64_t)ctx->nbox * N};
-  const cuuint64_t strides[2] = {RS * sizeof(float2), N * RS * sizeof(float2)};
-  const cuuint32_t box[3] = {(cuuint32_t)(2 * W), (cuuint32_t)N, 1};
+  const cuuint64_t dims[3] = {2 * (cuuint64_t)rstride, (cuuint64_t)N, (cuuint64_t)nouter};
+  const cuuint64_t strides[2] = {rstride * sizeof(float2), ostride * sizeof(float2)};
+  const cuuint32_t box[3] = {(cuuint32_t)(2 * W), (cuuint32_t)(N > 256 ? 256 : N), 1};
   const cuuint32_t estr[3] = {1, 1, 1};
-  CUtensorMap *m = reinterpret_cast<CUtensorMap *>(ctx->ymap);
-  if (encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, ctx->spec, dims, strides, box, estr,
+  if (encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, estr,
              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-    return ct2g_fail(ctx, CT2G_ECUDA, "y-pass tensor map");
-  ctx->ymap_w = W;
+    return ct2g_fail(ctx, CT2G_ECUDA, "column-pass tensor map");
   return CT2G_OK;
 }
 
+// a column pass (y pass, or an x pass over whole planes) with its tiles moved
+// by TMA: N rows x W columns per tile (W 32, or 16 with fft_tile 16 and at
+// N = 512), three tiles in flight per block; the data 16-byte aligned with
+// rstride and ostride even (the callers' vector condition)
 template <int N, bool INV>
-int launch_cols_tma(ct2g_ctx *ctx) {
-  if constexpr (N < 64 || N > 256) {
-    return ct2g_fail(ctx, CT2G_EINVAL, "TMA y pass: meshes 64-256");
+int launch_cols_tma(ct2g_ctx *ctx, float2 *data, size_t nouter, size_t ostride, size_t rstride,
+                    size_t ncols) {
+  if constexpr (N < 64 || N > 512) {
+    return ct2g_fail(ctx, CT2G_EINVAL, "TMA column pass: sizes 64-512");
   } else {
-    // W 32 with three stages (one block per SM), or 16 with three (two)
-    const bool narrow = ctx->fft_tile == 16;
+    const bool narrow = N > 256 || ctx->fft_tile == 16;
     const int W = narrow ? 16 : 32;
-    CT2G_TRY(ymap_build(ctx, W));
-    const uint32_t ncols = (uint32_t)((N / 2 + 1) * ctx->nc);
-    const uint32_t ntiles = (ncols + W - 1) / W, ntot = ntiles * (uint32_t)(ctx->nbox * N);
-    auto k = narrow ? fft_cols_tma_kernel<N, 16, INV, 3> : fft_cols_tma_kernel<N, 32, INV, 3>;
+    alignas(64) CUtensorMap map;
+    CT2G_TRY(cols_map(ctx, data, nouter, ostride, rstride, N, W, &map));
+    const uint32_t ntiles = (uint32_t)((ncols + W - 1) / W), ntot = ntiles * (uint32_t)nouter;
+    auto k = fft_cols_tma_kernel<N, 16, INV, 3>;
+    if constexpr (N <= 256)
+      if (!narrow) k = fft_cols_tma_kernel<N, 32, INV, 3>;
     const size_t smem = sizeof(float2) * (3 * (size_t)N * W + N) + 128;
     CT2G_TRY(ct2g_smem_attrs(ctx, k, smem));
     const int per_sm = ct2g_blocks_per_sm(ctx, (const void *)k, 256, smem);
     const uint32_t grid = std::min(ntot, (uint32_t)(per_sm * ctx->num_sms));
-    const CUtensorMap *m = reinterpret_cast<const CUtensorMap *>(ctx->ymap);
-    k<<<grid, 256, smem, ctx->stream>>>(*m, ntiles, ntot, twiddle_ptr<float2>(ctx),
+    k<<<grid, 256, smem, ctx->stream>>>(map, ntiles, ntot, twiddle_ptr<float2>(ctx),
                                         ctx->d_counts + 6);
     CT2G_LAUNCHED(ctx);
     return CT2G_OK;
@@ -606,6 +617,11 @@ template <typename T, int N, bool INV, bool VEC>
 int launch_cols(ct2g_ctx *ctx, typename Cplx<T>::type *spec, size_t nouter, size_t ostride,
                 size_t rstride, size_t ncols) {
   using C2 = typename Cplx<T>::type;
+  if constexpr (sizeof(C2) == 8 && N >= 64 && N <= 512) {
+    // FP32 columns with 16-byte aligned rows: tiles moved by TMA (tuning cols_tma)
+    if (VEC && ctx->cols_tma)
+      return launch_cols_tma<N, INV>(ctx, spec, nouter, ostride, rstride, ncols);
+  }
   // 16-column tiles from N = 256 on; FP64 at N = 512 takes 8 so that the
   // double-buffered tile fits in shared memory
   constexpr int W = N >= 256 ? (sizeof(C2) == 16 && N >= 512 ? 8 : 16) : 4096 / N;
@@ -1984,10 +2000,6 @@ int spec_cols(ct2g_ctx *ctx, bool inv, bool xpass) {
   if constexpr (N == 256 || N == 512) {
     if (ctx->fft_tc)
       return ct2g_fft_cols_tc(ctx, ctx->spec, N, nouter, ostride, rstride, ncols, inv);
-  }
-  if constexpr (N >= 64 && N <= 256) {
-    if (ctx->cols_tma && !xpass)
-      return inv ? launch_cols_tma<N, true>(ctx) : launch_cols_tma<N, false>(ctx);
   }
   if (inv) return launch_cols<float, N, true, true>(ctx, ctx->spec, nouter, ostride, rstride, ncols);
   return launch_cols<float, N, false, true>(ctx, ctx->spec, nouter, ostride, rstride, ncols);

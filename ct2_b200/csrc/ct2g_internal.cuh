@@ -265,10 +265,7 @@ struct ct2g_ctx {
   int mg2l_greens_direct = 0;  // 1: the fused x pass reads the Green's values from HBM
   int near_chunks_per_warp = 0;  // overlap: chunks a near-field warp takes before its block exits
   int plane_pipe = 0;          // > 0: z and y passes as one plane pipeline, this lag in planes
-  int cols_tma = 1;            // 1: the mesh y passes move their tiles by TMA
-  // tensor map of the spectrum's y-pass tiles (a CUtensorMap, built once)
-  alignas(64) unsigned char ymap[128] = {};
-  int ymap_w = 0;              // tile width the map was built for (0: none)
+  int cols_tma = 1;            // 1: FP32 column FFT passes move their tiles by TMA
   int p2m_compact = 0;         // 1: P2M into compact per-cell records before the z pass
   int x_tma = 2;               // fused x pass inputs: 1 tensor + bulk copies, 2 cp.async
                                // column + bulk Green's copy, 0 per-thread loads
