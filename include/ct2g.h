@@ -245,12 +245,13 @@ int ct2g_batch_destroy(ct2g_batch *b);
  * L2; the inverse y pass and z pass (with L2P) likewise, the z lines dropping
  * the L2 lines they have read (PTX discard.global.L2) instead of letting them
  * be written back; the same results as 0 (separate passes); meshes 64-256
- * with the FP32 passes (others run the separate passes); cols_tma -- 1: the
- * mesh's y FFT passes move each tile (all rows of a plane x 32 complex
- * columns; 16 with fft_tile 16) by one tiled bulk tensor copy (TMA) in and
- * one out, three tiles in flight per block (meshes 64-256, FP32 passes; the
- * default); 0: every thread copies its share of each tile (cp.async, two
- * tiles in flight); the same results; x_tma -- 1: the fused x
+ * with the FP32 passes (others run the separate passes); cols_tma -- 1 (the
+ * default): every FP32 column FFT pass with 16-byte aligned rows (the mesh's
+ * y passes, the r2c / c2r / complex 3D FFT entry points) moves each tile
+ * (all N rows x 32 complex columns; 16 with fft_tile 16 or at N = 512) by
+ * tiled bulk tensor copies (TMA) in and out, three tiles in flight per
+ * block (N 64-512); 0: every thread copies its share of each tile
+ * (cp.async, two tiles in flight); the same results; x_tma -- 1: the fused x
  * pass + Green's multiply brings each spectrum column in by one tiled bulk
  * tensor copy and its Green's column by one bulk copy (meshes 64-256, FP32
  * passes; with mg2l_greens_direct the Green's values are read by the
