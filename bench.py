@@ -19,9 +19,9 @@ Two forms of the same step are timed on the same particles:
           launch per step.
 `value` is the graph form's whole-job particles/s (device time, CUDA events,
 max over ranks); `forms` holds both.  `e2e` is the same metric through the
-public API (ct2g_upload_particles, ct2g_kick_drift, ct2g_download_particles)
-with the particle state copied host->device before and device->host after
-every step.  `roofline` is for the
+public API's host-state step (ct2g_kick_drift_host: the particle state copied
+host->device, the step, the state copied device->host, every step; the
+velocity and rung upload overlaps binning and the force solve).  `roofline` is for the
 kernel with the largest share of the step; `cpu_baseline` is the CPU oracle
 timed on a bounded sample.  Under torchrun (N>1) every rank runs an
 independent box (replicas; the step has no exchange), value = all particles /
@@ -830,7 +830,7 @@ def main():
             dist.destroy_process_group()
         return
 
-    from ct2_b200 import _lib, replicas
+    from ct2_b200 import replicas
     from ct2_b200.gravity import Gravity
 
     P, n = workload(args, rank)
@@ -943,17 +943,11 @@ def main():
         outn = {k: v.numpy() for k, v in outb.items()}
         for k in ("x", "y", "z"):
             outn[k] = outn[k].view(np.uint32)
-        import ctypes
-        lib = _lib.load()
 
         def e2e_step():
-            g.upload(pin["x"], pin["y"], pin["z"], pin["vx"], pin["vy"], pin["vz"], pin["rung"])
-            g.kick_drift(kp, args.dt, 1.0, graph=True, wait=True)
-            vp = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
-            rc = lib.ct2g_download_particles(g.handle, vp(outn["x"]), vp(outn["y"]), vp(outn["z"]),
-                                             vp(outn["vx"]), vp(outn["vy"]), vp(outn["vz"]),
-                                             vp(outn["rung"]), None)
-            assert rc == 0
+            # ct2g_kick_drift_host: positions in, the step (its velocity and
+            # rung upload beside binning and the force solve), state out
+            g.kick_drift_host(kp, args.dt, pin, outn, graph=True)
         for _ in range(2):
             e2e_step()
         if dist:

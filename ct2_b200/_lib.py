@@ -76,6 +76,7 @@ SYMBOLS = [
     ("ct2g_kick", _I, [_P, _P, _P]),
     ("ct2g_drift", _I, [_P, _F, _F]),
     ("ct2g_kick_drift", _I, [_P, _P, _F, _F, _I, _P]),
+    ("ct2g_kick_drift_host", _I, [_P, _P, _F, _F, _I] + [_P] * 7 + [_SZ] + [_P] * 9),
     ("ct2g_create_boxes", _I, [_P, _I, _P]),
     ("ct2g_set_boxes", _I, [_P, _P, _P]),
     ("ct2g_box_count", _I, [_P]),

@@ -358,10 +358,16 @@ int ct2g_create_boxes(const ct2g_options *opt, int nbox, ct2g_ctx **out) {
     if (cudaStreamCreateWithPriority(&ctx->stream, cudaStreamNonBlocking, prio_greatest) != cudaSuccess) { rc = CT2G_ECUDA; break; }
     if (cudaStreamCreateWithPriority(&ctx->stream2, cudaStreamNonBlocking, prio_least) != cudaSuccess ||
         cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->ev_pos, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->ev_vel, cudaEventDisableTiming) != cudaSuccess) {
       rc = CT2G_ECUDA;
       break;
     }
+    // ev_vel always holds a record: a step that waits on it without a
+    // host-state upload finds it complete
+    if (cudaEventRecord(ctx->ev_vel, ctx->copy_stream) != cudaSuccess) { rc = CT2G_ECUDA; break; }
     for (auto &e : ctx->ev)
       if (cudaEventCreate(&e) != cudaSuccess) { rc = CT2G_ECUDA; break; }
     if (rc) break;
@@ -441,6 +447,10 @@ int ct2g_destroy(ct2g_ctx *ctx) {
   if (ctx->stream2) cudaStreamSynchronize(ctx->stream2);
   if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
   if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
+  if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
+  if (ctx->ev_pos) cudaEventDestroy(ctx->ev_pos);
+  if (ctx->ev_vel) cudaEventDestroy(ctx->ev_vel);
+  if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
   if (ctx->stream2) cudaStreamDestroy(ctx->stream2);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -550,6 +560,65 @@ int ct2g_download_particles(ct2g_ctx *ctx, uint32_t *x, uint32_t *y, uint32_t *z
   if (rung) CT2G_CUDA(ctx, cudaMemcpyAsync(rung, ctx->rung, n, cudaMemcpyDeviceToHost, st));
   if (ids) CT2G_CUDA(ctx, cudaMemcpyAsync(ids, ctx->id, n * 4, cudaMemcpyDeviceToHost, st));
   CT2G_CUDA(ctx, cudaStreamSynchronize(st));
+  return CT2G_OK;
+}
+
+// One kick + drift from host state to host state.  Positions and ids go
+// first on the context stream (binning needs them at once); the velocities
+// and rungs follow on copy_stream while binning and the force solve run,
+// and the step waits for them (ev_vel) only where it gathers them into cell
+// order, just before the update.  Then the state comes back.
+int ct2g_kick_drift_host(ct2g_ctx *ctx, const ct2g_kick_params *p, float dt, float scale,
+                         int flags, const uint32_t *x, const uint32_t *y, const uint32_t *z,
+                         const float *vx, const float *vy, const float *vz, const int8_t *rung,
+                         size_t n, uint32_t *xo, uint32_t *yo, uint32_t *zo, float *vxo,
+                         float *vyo, float *vzo, int8_t *rungo, uint32_t *ido, int *max_rung) {
+  CT2G_TRY(check(ctx));
+  if (!p) return ct2g_fail(ctx, CT2G_EINVAL, "null kick params");
+  if (!x || !y || !z || !vx || !vy || !vz) return ct2g_fail(ctx, CT2G_EINVAL, "null particle array");
+  if (!ctx->has_particles || n != ctx->n)
+    return ct2g_fail(ctx, CT2G_ESTATE, "host-state step: n must equal the uploaded particle count");
+  cudaStream_t st = ctx->stream, cs = ctx->copy_stream;
+  CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->x, x, n * 4, cudaMemcpyHostToDevice, st));
+  CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->y, y, n * 4, cudaMemcpyHostToDevice, st));
+  CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->z, z, n * 4, cudaMemcpyHostToDevice, st));
+  if (n) {
+    iota_kernel<<<ct2g_div_up(n, 256), 256, 0, st>>>(ctx->id, n);
+    CT2G_LAUNCHED(ctx);
+  }
+  // the velocity upload starts once everything queued before it on the
+  // context stream (earlier steps included) and the position upload are done
+  CT2G_CUDA(ctx, cudaEventRecord(ctx->ev_pos, st));
+  CT2G_CUDA(ctx, cudaStreamWaitEvent(cs, ctx->ev_pos, 0));
+  CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->vx, vx, n * 4, cudaMemcpyHostToDevice, cs));
+  CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->vy, vy, n * 4, cudaMemcpyHostToDevice, cs));
+  CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->vz, vz, n * 4, cudaMemcpyHostToDevice, cs));
+  if (rung)
+    CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->rung, rung, n, cudaMemcpyHostToDevice, cs));
+  else
+    CT2G_CUDA(ctx, cudaMemsetAsync(ctx->rung, 0, n, cs));
+  CT2G_CUDA(ctx, cudaEventRecord(ctx->ev_vel, cs));
+  // what an upload resets
+  ctx->rung_begin = 0;
+  ctx->rung_stack.clear();
+  ctx->grid_valid = ctx->moments_valid = ctx->expansions_valid = ctx->forces_valid = false;
+  const int rc = ct2g_kick_drift(ctx, p, dt, scale, flags, nullptr);
+  if (rc != CT2G_OK) {
+    cudaStreamSynchronize(cs);  // the host arrays stay in use until the copies end
+    return rc;
+  }
+  if (xo) CT2G_CUDA(ctx, cudaMemcpyAsync(xo, ctx->x, n * 4, cudaMemcpyDeviceToHost, st));
+  if (yo) CT2G_CUDA(ctx, cudaMemcpyAsync(yo, ctx->y, n * 4, cudaMemcpyDeviceToHost, st));
+  if (zo) CT2G_CUDA(ctx, cudaMemcpyAsync(zo, ctx->z, n * 4, cudaMemcpyDeviceToHost, st));
+  if (vxo) CT2G_CUDA(ctx, cudaMemcpyAsync(vxo, ctx->vx, n * 4, cudaMemcpyDeviceToHost, st));
+  if (vyo) CT2G_CUDA(ctx, cudaMemcpyAsync(vyo, ctx->vy, n * 4, cudaMemcpyDeviceToHost, st));
+  if (vzo) CT2G_CUDA(ctx, cudaMemcpyAsync(vzo, ctx->vz, n * 4, cudaMemcpyDeviceToHost, st));
+  if (rungo) CT2G_CUDA(ctx, cudaMemcpyAsync(rungo, ctx->rung, n, cudaMemcpyDeviceToHost, st));
+  if (ido) CT2G_CUDA(ctx, cudaMemcpyAsync(ido, ctx->id, n * 4, cudaMemcpyDeviceToHost, st));
+  CT2G_CUDA(ctx, cudaMemcpyAsync(ctx->h_pinned, ctx->d_maxrung, sizeof(int),
+                                 cudaMemcpyDeviceToHost, st));
+  CT2G_CUDA(ctx, cudaStreamSynchronize(st));
+  if (max_rung) *max_rung = (int)ctx->h_pinned[0];
   return CT2G_OK;
 }
 

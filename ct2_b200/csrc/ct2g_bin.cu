@@ -233,7 +233,8 @@ __global__ void gather_kernel(const uint32_t *__restrict__ perm, size_t begin, s
                               uint32_t *__restrict__ y2, uint32_t *__restrict__ z2,
                               float *__restrict__ vx2, float *__restrict__ vy2,
                               float *__restrict__ vz2, int8_t *__restrict__ rung2,
-                              uint32_t *__restrict__ id2, float4 *__restrict__ src) {
+                              uint32_t *__restrict__ id2, float4 *__restrict__ src,
+                              bool vel) {
   size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nr) return;
   size_t s = begin + perm[i], d = begin + i;
@@ -241,10 +242,16 @@ __global__ void gather_kernel(const uint32_t *__restrict__ perm, size_t begin, s
   x2[d] = px;
   y2[d] = py;
   z2[d] = pz;
-  vx2[d] = vx[s];
-  vy2[d] = vy[s];
-  vz2[d] = vz[s];
-  rung2[d] = rung[s];
+  if (vel) {
+    vx2[d] = vx[s];
+    vy2[d] = vy[s];
+    vz2[d] = vz[s];
+    rung2[d] = rung[s];
+  } else {
+    // velocities and rungs follow later (gather_vel_kernel): keep the source
+    // index in their gather target
+    reinterpret_cast<uint32_t *>(vx2)[d] = (uint32_t)s;
+  }
   id2[d] = id[s];
   // offset from the cell centre: low (32-mbits) bits minus half a cell,
   // exact in float (|value| < 2^(31-mbits) <= 2^24)
@@ -344,17 +351,50 @@ __global__ void copy_back_kernel(size_t begin, size_t nr, const uint32_t *__rest
                                  uint32_t *__restrict__ y, uint32_t *__restrict__ z,
                                  float *__restrict__ vx, float *__restrict__ vy,
                                  float *__restrict__ vz, int8_t *__restrict__ rung,
-                                 uint32_t *__restrict__ id) {
+                                 uint32_t *__restrict__ id, bool vel) {
   const size_t i = begin + (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= begin + nr) return;
   x[i] = x2[i];
   y[i] = y2[i];
   z[i] = z2[i];
+  if (vel) {
+    vx[i] = vx2[i];
+    vy[i] = vy2[i];
+    vz[i] = vz2[i];
+    rung[i] = rung2[i];
+  }
+  id[i] = id2[i];
+}
+
+// the deferred half of the gather: velocities and rungs into cell order,
+// from the source indices the position gather left in vx2
+__global__ void gather_vel_kernel(size_t begin, size_t nr, const float *__restrict__ vx,
+                                  const float *__restrict__ vy, const float *__restrict__ vz,
+                                  const int8_t *__restrict__ rung, float *__restrict__ vx2,
+                                  float *__restrict__ vy2, float *__restrict__ vz2,
+                                  int8_t *__restrict__ rung2) {
+  const size_t d = begin + (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (d >= begin + nr) return;
+  const uint32_t s = reinterpret_cast<const uint32_t *>(vx2)[d];
+  if (s < begin || s >= begin + nr) return;  // the position gather wrote every index in range
+  vx2[d] = vx[s];
+  vy2[d] = vy[s];
+  vz2[d] = vz[s];
+  rung2[d] = rung[s];
+}
+
+__global__ void copy_back_vel_kernel(size_t begin, size_t nr, const float *__restrict__ vx2,
+                                     const float *__restrict__ vy2,
+                                     const float *__restrict__ vz2,
+                                     const int8_t *__restrict__ rung2, float *__restrict__ vx,
+                                     float *__restrict__ vy, float *__restrict__ vz,
+                                     int8_t *__restrict__ rung) {
+  const size_t i = begin + (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= begin + nr) return;
   vx[i] = vx2[i];
   vy[i] = vy2[i];
   vz[i] = vz2[i];
   rung[i] = rung2[i];
-  id[i] = id2[i];
 }
 
 __global__ void fill_kernel(uint32_t *__restrict__ a, size_t n, uint32_t v) {
@@ -446,12 +486,13 @@ int ct2g_bin_range(ct2g_ctx *ctx) {
     gather_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(
         ctx->vals, begin, nr, mbits, ctx->x, ctx->y, ctx->z, ctx->vx, ctx->vy, ctx->vz,
         ctx->rung, ctx->id, ctx->x2, ctx->y2, ctx->z2, ctx->vx2, ctx->vy2, ctx->vz2, ctx->rung2,
-        ctx->id2, ctx->src);
+        ctx->id2, ctx->src, !ctx->defer_vel);
     CT2G_LAUNCHED(ctx);
     copy_back_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(
         begin, nr, ctx->x2, ctx->y2, ctx->z2, ctx->vx2, ctx->vy2, ctx->vz2, ctx->rung2, ctx->id2,
-        ctx->x, ctx->y, ctx->z, ctx->vx, ctx->vy, ctx->vz, ctx->rung, ctx->id);
+        ctx->x, ctx->y, ctx->z, ctx->vx, ctx->vy, ctx->vz, ctx->rung, ctx->id, !ctx->defer_vel);
     CT2G_LAUNCHED(ctx);
+    ctx->vel_pending = ctx->defer_vel;
     // near-field work lists (scratch: flags, vals, vals2, x2, y2 are free here)
     chunk_flag_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(ctx->keys, ctx->cell_start, begin, nr,
                                                         ctx->dense_cell, ctx->flags, ctx->vals);
@@ -487,5 +528,29 @@ int ct2g_bin_range(ct2g_ctx *ctx) {
   ctx->moments_valid = false;
   ctx->expansions_valid = false;
   ctx->forces_valid = false;
+  return CT2G_OK;
+}
+
+// The second half of a deferred gather (ctx->defer_vel at binning): the
+// velocities and rungs of the binned range into cell order, after `stream`
+// has waited for ctx->ev_vel (the host-state step's velocity upload; a no-op
+// wait otherwise).  Bitwise the same store as the one-pass gather.
+int ct2g_gather_velocities(ct2g_ctx *ctx) {
+  if (!ctx->vel_pending) return CT2G_OK;
+  ctx->vel_pending = false;
+  const size_t begin = ctx->rung_begin, nr = ctx->n - ctx->rung_begin;
+  cudaStream_t st = ctx->stream;
+  CT2G_CUDA(ctx, cudaStreamWaitEvent(st, ctx->ev_vel,
+                                     ctx->capturing ? cudaEventWaitExternal : 0));
+  if (nr == 0) return CT2G_OK;
+  const unsigned T = 256;
+  gather_vel_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(begin, nr, ctx->vx, ctx->vy, ctx->vz,
+                                                      ctx->rung, ctx->vx2, ctx->vy2, ctx->vz2,
+                                                      ctx->rung2);
+  CT2G_LAUNCHED(ctx);
+  copy_back_vel_kernel<<<ct2g_div_up(nr, T), T, 0, st>>>(begin, nr, ctx->vx2, ctx->vy2,
+                                                         ctx->vz2, ctx->rung2, ctx->vx, ctx->vy,
+                                                         ctx->vz, ctx->rung);
+  CT2G_LAUNCHED(ctx);
   return CT2G_OK;
 }

@@ -44,11 +44,23 @@ int check_params(ct2g_ctx *ctx, const ct2g_kick_params *p, float scale) {
 int step_body(ct2g_ctx *ctx, const ct2g_kick_params *p, float dt, float scale) {
   if (!ctx->has_particles) return ct2g_fail(ctx, CT2G_ESTATE, "no particles uploaded");
   ct2g_mark(ctx, 0);
-  CT2G_TRY(ct2g_bin_range(ctx));
-  CT2G_TRY(ct2g_all_forces(ctx, false));
+  // binning moves positions and ids into cell order; the velocities and
+  // rungs, which only the update reads, follow just before it, so that a
+  // host-state step's velocity upload overlaps binning and the force solve
+  ctx->defer_vel = true;
+  int rc = ct2g_bin_range(ctx);
+  ctx->defer_vel = false;
+  if (rc == CT2G_OK) rc = ct2g_all_forces(ctx, false);
+  if (rc != CT2G_OK) {
+    // leave no half-gathered store behind (best effort: the step has failed)
+    if (ctx->vel_pending) ct2g_gather_velocities(ctx);
+    ctx->vel_pending = false;
+    return rc;
+  }
   ctx->pot_valid = false;
   ctx->forces_valid = true;
   ct2g_mark(ctx, 6);
+  CT2G_TRY(ct2g_gather_velocities(ctx));
   CT2G_TRY(ct2g_update(ctx, p, nullptr, false, 0.f, 1.f));
   CT2G_TRY(ct2g_drift_all(ctx, dt, scale));
   ct2g_mark(ctx, 7);

@@ -222,6 +222,13 @@ struct ct2g_ctx {
   // events that fork it from and join it back to `stream`
   cudaStream_t stream2 = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // host-state steps (ct2g_kick_drift_host): the velocity and rung upload
+  // runs on copy_stream after ev_pos (positions landed) and signals ev_vel,
+  // which the step waits for just before it gathers the velocities
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_pos = nullptr, ev_vel = nullptr;
+  bool defer_vel = false;    // binning leaves the velocity/rung gather for later
+  bool vel_pending = false;  // ... and that gather has not run yet
   cudaEvent_t ev[8] = {};
   float stage_ms[8] = {};
   std::string err;
@@ -373,6 +380,8 @@ size_t ct2g_scan_scratch_words(size_t n);
 // stage-time event k, skipped while a graph is recorded
 void ct2g_mark(ct2g_ctx *ctx, int k);
 int ct2g_bin_range(ct2g_ctx *ctx);
+// the velocity/rung half of a gather that binning deferred (ctx->defer_vel)
+int ct2g_gather_velocities(ct2g_ctx *ctx);
 int ct2g_check(ct2g_ctx *ctx);  // valid context; selects its device
 // the compact P2M records for the particle capacity (no-op when present)
 int ct2g_alloc_p2m_compact(ct2g_ctx *ctx);

@@ -221,6 +221,29 @@ class Gravity:
                                           ctypes.byref(mr) if wait else None))
         return mr.value if wait else None
 
+    def kick_drift_host(self, params: kick_params, dt: float, state, out, scale: float = 1.0,
+                        graph=True):
+        """One kick+drift from host arrays to host arrays (ct2g_kick_drift_host):
+        `state` holds x, y, z (uint32), vx, vy, vz (float32) and optionally
+        rung (int8) of the uploaded particle count; `out` the preallocated
+        arrays to fill (any key may be missing; "id" maps the new order back
+        to input order).  Pinned arrays give the copies their full rate.
+        Returns the max rung."""
+        n = len(state["x"])
+        ins = [state[k] for k in ("x", "y", "z", "vx", "vy", "vz")] + [state.get("rung")]
+        for a, t in zip(ins, (np.uint32,) * 3 + (np.float32,) * 3 + (np.int8,)):
+            if a is not None and (a.dtype != t or len(a) != n or not a.flags["C_CONTIGUOUS"]):
+                raise ValueError("state arrays: %d contiguous values of %s" % (n, np.dtype(t)))
+        outs = [out.get(k) for k in ("x", "y", "z", "vx", "vy", "vz", "rung", "id")]
+        for a, t in zip(outs, (np.uint32,) * 3 + (np.float32,) * 3 + (np.int8, np.uint32)):
+            if a is not None and (a.dtype != t or len(a) != n or not a.flags["C_CONTIGUOUS"]):
+                raise ValueError("output arrays: %d contiguous values of %s" % (n, np.dtype(t)))
+        mr = ctypes.c_int(0)
+        self._chk(self._l.ct2g_kick_drift_host(
+            self._h, ctypes.byref(params._c()), dt, scale, _lib.STEP_GRAPH if graph else 0,
+            *[_ptr(a) for a in ins], n, *[_ptr(a) for a in outs], ctypes.byref(mr)))
+        return mr.value
+
     # -- learned near-field correction ---------------------------------------
     def learned_enable(self, bwidth_ext):
         self._chk(self._l.ct2g_learned_enable(self._h, float(bwidth_ext)))

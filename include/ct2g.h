@@ -181,6 +181,25 @@ int ct2g_kick_step(ct2g_ctx *ctx, int *minrung, int max_rung, double scale, doub
 int ct2g_kick_drift(ct2g_ctx *ctx, const ct2g_kick_params *p, float dt, float scale, int flags,
                     int *max_rung);
 
+/* One kick + drift from host state to host state: the same step as
+ * ct2g_upload_particles (same n as the last upload), ct2g_kick_drift and
+ * ct2g_download_particles in a row, with the same results bit for bit, but
+ * with the velocity and rung upload overlapping binning and the force solve
+ * (they are gathered into cell order just before the update).  No
+ * counterpart in the reference, whose particles live in host memory.
+ * Inputs: host arrays of n particles (rung may be NULL: all 0); ids are set
+ * to 0..n-1 in input order, as an upload does, and the box counts of a box
+ * context stay as set.  Outputs: host arrays in the new (cell-sorted) order,
+ * any may be NULL; ids_out maps them back to input order.  Pinned host
+ * memory gives the copies their full rate.  *max_rung (may be NULL) gets
+ * kick()'s return value.  Returns once the outputs are written. */
+int ct2g_kick_drift_host(ct2g_ctx *ctx, const ct2g_kick_params *p, float dt, float scale,
+                         int flags, const uint32_t *x, const uint32_t *y, const uint32_t *z,
+                         const float *vx, const float *vy, const float *vz, const int8_t *rung,
+                         size_t n, uint32_t *x_out, uint32_t *y_out, uint32_t *z_out,
+                         float *vx_out, float *vy_out, float *vz_out, int8_t *rung_out,
+                         uint32_t *ids_out, int *max_rung);
+
 /* Many independent periodic boxes.  No counterpart in the reference (one box
  * per process there).  A box context holds nbox unit boxes that share the
  * mesh, order, stencil and softening of *opt (so they share one Green's
