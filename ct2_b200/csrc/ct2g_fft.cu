@@ -1254,27 +1254,41 @@ __device__ __forceinline__ void l2p_line(float2 *s, const float2 *stw, const uin
   using LL = LineLayout<N, true>;
   constexpr int NL = (ct2g_ncomp(P) + 1) / 2;
   // offsets of the cells' particles in the line's particle list (inclusive
-  // scan of the counts, off[0] = 0), built while nothing else needs the SM
+  // scan of the counts, off[0] = 0): thread t holds cells [t ZT, t ZT + ZT),
+  // scans its sum across its warp by shuffles before the transform and
+  // across the block's warps after it (one barrier of its own)
   constexpr int ZT = (N + 255) / 256;  // cells per thread
-  for (int z = threadIdx.x; z < N; z += 256) off[z + 1] = ce[z] - cb[z];
-  if (threadIdx.x == 0) off[0] = 0;
+  static_assert(N % 256 == 0 || N < 256, "cells per thread");
+  __shared__ uint32_t wsum[8];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t c[ZT], tsum = 0;
+#pragma unroll
+  for (int q = 0; q < ZT; q++) {
+    const int z = threadIdx.x * ZT + q;
+    c[q] = z < N ? ce[z] - cb[z] : 0u;
+    tsum += c[q];
+  }
+  uint32_t inc = tsum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += t;
+  }
+  if (lane == 31) wsum[warp] = inc;
   tile_fft<N, true, float2, true>(s, NL, 0, stw);
   __syncthreads();
-  for (int d = 1; d < N; d <<= 1) {
-    uint32_t add[ZT];
+  {
+    uint32_t run = inc - tsum;
+    for (int w = 0; w < warp; w++) run += wsum[w];
 #pragma unroll
     for (int q = 0; q < ZT; q++) {
-      const int z = threadIdx.x + 256 * q;
-      add[q] = (z < N && z >= d) ? off[z + 1 - d] : 0u;
+      const int z = threadIdx.x * ZT + q;
+      run += c[q];
+      if (z < N) off[z + 1] = run;
     }
-    __syncthreads();
-#pragma unroll
-    for (int q = 0; q < ZT; q++) {
-      const int z = threadIdx.x + 256 * q;
-      if (z < N) off[z + 1] += add[q];
-    }
-    __syncthreads();
+    if (threadIdx.x == 0) off[0] = 0;
   }
+  __syncthreads();
   // every particle of the line, one per thread: its cell is the last z with
   // off[z] <= q (that cell holds it: off[z] <= q < off[z + 1])
   const uint32_t total = off[N];
